@@ -1,0 +1,192 @@
+/*
+ * msolve_gpu.h -- C ABI of the B200 (sm_100a) Hexa8 linear-elastic solve path.
+ *
+ * The drop-in boundary for MSolve's Hexa8 static solve and its Monte Carlo
+ * realization loop. Every entry point is extern "C", Cdecl, takes plain
+ * pointers and sizes, and returns an int status (0 = ok; negative codes below,
+ * message through MSG_LAST_ERROR). It is written to be bound from C# with
+ * [DllImport("msolve_gpu", CallingConvention = CallingConvention.Cdecl)], the
+ * convention the reference already uses for its native element library
+ * (ISAAR.MSolve.PreProcessor/Elements/Hexa8.cs:26-62).
+ *
+ * Conventions
+ *  - Host pointers unless an entry point says "device". Host buffers are
+ *    caller-owned and only read/written during the call.
+ *  - Element node order and packed 24x24 layout are the reference's:
+ *    nodes (-,-,-),(+,-,-),(+,+,-),(-,+,-),(-,-,+),(+,-,+),(+,+,+),(-,+,+)
+ *    (FEMElements/FEMElements/rElHexa8.f90:43-68), element DOFs node-major x,y,z,
+ *    packed row-wise upper triangle of 300 entries
+ *    (ISAAR.MSolve.Matrices/SymmetricMatrix2D.cs:22-49).
+ *  - DOF numbering is the caller's (Model/Subdomain numbering, constrained = -1,
+ *    ISAAR.MSolve.PreProcessor/Subdomain.cs:77-135). Vectors of length n_dofs are
+ *    in that numbering.
+ *  - Handles are bound to the context (one CUDA device, one stream). Calls on
+ *    one context are serialised by an internal mutex; different contexts may be
+ *    used from different threads.
+ */
+#ifndef MSOLVE_GPU_H
+#define MSOLVE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes. The first three reuse FEMElements/FEMElements/hCommon.h:18-29. */
+#define MSG_OK                    0
+#define MSG_ERR_UNKNOWN          (-1)     /* iErrUnknown */
+#define MSG_ERR_OUT_OF_MEMORY    (-100)   /* iErrNotEnoughMemory (device or memory budget) */
+#define MSG_ERR_NEG_DET          (-1001)  /* iErrNegDet: Jacobian determinant < 1e-8 */
+#define MSG_ERR_NOT_CONVERGED    (-2001)  /* PCG hit max iterations above tolerance */
+#define MSG_ERR_BREAKDOWN        (-2002)  /* p.q <= 0 or NaN in PCG */
+#define MSG_ERR_TIMEOUT          (-2003)  /* a bounded device/host wait gave up */
+#define MSG_ERR_CANCELLED        (-2004)  /* serving request cancelled */
+#define MSG_ERR_INVALID_ARGUMENT (-2005)
+#define MSG_ERR_CUDA             (-2006)  /* CUDA runtime error (message has the text) */
+#define MSG_ERR_NOT_STRUCTURED   (-2007)  /* batched matrix-free path needs a structured cube lattice */
+#define MSG_ERR_NO_DEVICE        (-2008)
+
+/* ---- solver modes for MSG_MC_SOLVE_BATCH */
+#define MSG_MODE_FP64_BSR        0  /* plain FP64: per realization assemble BSR + Jacobi-PCG (the drop-in) */
+#define MSG_MODE_MIXED_BATCHED   1  /* all realizations at once: matrix-free FP32 PCG + FP64 refinement */
+
+typedef struct msg_context* MSG_CTX;
+typedef struct msg_mesh* MSG_MESH;
+typedef struct msg_matrix* MSG_MAT;
+
+/* ------------------------------------------------------------------ context */
+/* Create a context on CUDA device `device`. mem_budget_bytes = 0 means no budget
+ * beyond the device's free memory. No counterpart in the reference (which has no
+ * device); the C# shim creates one per solver instance. */
+int MSG_CREATE(int device, uint64_t mem_budget_bytes, MSG_CTX* out);
+int MSG_DESTROY(MSG_CTX ctx);
+/* Text of the last error on this context (valid until the next call on it). */
+const char* MSG_LAST_ERROR(MSG_CTX ctx);
+/* ABI version (major*10000 + minor*100 + patch). */
+int MSG_VERSION(void);
+
+/* ------------------------------------------------------------------ element kernels */
+/* Batched twin of CALCH8GAUSSMATRICES + CALCH8K
+ * (FEMElements/FEMElements/rElHexa8.f90:422-464, 489-543; called from
+ * Hexa8WithStochasticMaterial.StiffnessMatrix, Hexa8WithStochasticMaterial.cs:61-110):
+ * for each of n elements, isotropic D(E[e], nu) at every 2x2x2 Gauss point,
+ * K_e = sum_gp w B^T D B, packed 300 entries.
+ * xyz [n][8][3], E [n], Ke [n][300]. Returns MSG_ERR_NEG_DET if any element has
+ * detJ < 1e-8 at a Gauss point (Ke is still written, as the Fortran does). */
+int MSG_H8_KE_BATCH(MSG_CTX ctx, int n, const double* xyz, const double* E, double nu, double* Ke);
+
+/* Batched consistent mass, Hexa8.CalculateConsistentMass
+ * (ISAAR.MSolve.PreProcessor/Elements/Hexa8.cs:403-435): xyz [n][8][3], Me [n][300]. */
+int MSG_H8_ME_BATCH(MSG_CTX ctx, int n, const double* xyz, double rho, double* Me);
+
+/* ------------------------------------------------------------------ mesh */
+/* Upload a Hexa8 mesh: xyz [n_nodes][3], conn [n_elems][8] (0-based node
+ * indices), dof [n_nodes][3] (free DOF number or -1 if constrained, the
+ * Subdomain.NodalDOFsDictionary numbering). Builds the 3x3-block sparsity
+ * pattern (replacing GlobalMatrixAssemblerSkyline.CalculateRowIndex,
+ * GlobalMatrixAssemblerSkyline.cs:14-42) and detects whether the mesh is a
+ * structured lattice of equal cubes in generator order
+ * (Hexa8MeshGenerator.BuildNodes / element loop, Hexa8MeshGenerator.cs:508-568,
+ * 1075-1089), which enables MSG_MODE_MIXED_BATCHED. */
+int MSG_MESH_CREATE(MSG_CTX ctx, int n_nodes, const double* xyz, int n_elems, const int* conn,
+                    const int* dof, int n_dofs, MSG_MESH* out);
+/* info[0]=structured(0/1) info[1..3]=nx,ny,nz info[4]=n_dofs info[5]=n_block_rows
+ * info[6]=nnz_blocks info[7]=n_elems. (8 ints) */
+int MSG_MESH_INFO(MSG_MESH mesh, int64_t* info8);
+int MSG_MESH_DESTROY(MSG_MESH mesh);
+
+/* ------------------------------------------------------------------ assembled FP64 operator */
+/* Assemble the global stiffness in 3x3 block sparse form on the device from
+ * per-element Young's moduli E [n_elems] and nu: element matrices by the
+ * MSG_H8_KE_BATCH kernel, summed per block in a fixed order (deterministic).
+ * Replaces ProblemStructural.BuildKs -> GlobalMatrixAssemblerSkyline.CalculateGlobalMatrix
+ * (ProblemStructural.cs:63-89; GlobalMatrixAssemblerSkyline.cs:51-103). */
+int MSG_ASSEMBLE_BSR(MSG_MESH mesh, const double* E, double nu, MSG_MAT* out);
+/* Same, from caller-supplied element matrices Ke [n_elems][300] (host), the
+ * IElementMatrixProvider seam (ISAAR.MSolve.PreProcessor/Interfaces/IElementMatrixProvider.cs:9-12). */
+int MSG_ASSEMBLE_BSR_KE(MSG_MESH mesh, const double* Ke, MSG_MAT* out);
+/* y = K x in DOF numbering (IMatrix2D.Multiply parity, SkylineMatrix2D.cs:224-286). */
+int MSG_MAT_MULTIPLY(MSG_MAT mat, const double* x, double* y);
+/* diag [n_dofs] = K_jj (the Jacobi preconditioner's source,
+ * PolynomialChaosSolverPCGMatrixCalculator.cs:467-495). */
+int MSG_MAT_DIAGONAL(MSG_MAT mat, double* diag);
+int MSG_MAT_DESTROY(MSG_MAT mat);
+
+/* Jacobi-preconditioned PCG with the reference's semantics
+ * (ISAAR.MSolve.Solvers/PCG/SolverPCG.cs:105-149, simple search vector
+ * SolverPCGSimpleSearchVectorCalculator.cs:18-41): x0 = 0, r0 = b, stop when
+ * ||r_k|| / ||b|| < tol on the recursively updated r, skip if ||b|| <= 1e-25.
+ * The whole loop runs on the device (no host round trip per iteration).
+ * iterations = the reference's count (loop index at the break); rel_res = last
+ * ||r||/||b||. Returns MSG_ERR_NOT_CONVERGED if max_it was reached. */
+int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
+                  double* rel_res);
+
+/* ------------------------------------------------------------------ stochastic field */
+/* Separable Karhunen-Loeve table of a lognormal Young's modulus, the content of
+ * the eigen-data file read by LognormalFileStochasticCoefficientsProvider
+ * (ISAAR.MSolve.PreProcessor/Stochastic/LognormalFileStochasticCoefficientsProvider.cs:71-118):
+ * per term k and axis a: frequency w3[k][a], amplitude amp3[k][a], 1-based 1-D
+ * mode index idx3[k][a] (odd -> cos, even -> sin), eigenvalue eig[k].
+ * E(x) = exp(ln(mean) - mc*sigma^2/2 + sum_k xi_k sigma sqrt(eig_k)
+ *            prod_a amp * {cos|sin}(w * (x_a - domain_a/2)))   (GetCoefficient :173-193)
+ * evaluated at each element's bounding-box centre (Hexa8WithStochasticMaterial.cs:112-140). */
+typedef struct {
+  int n_terms;          /* 1..64 */
+  const double* w3;
+  const double* amp3;
+  const int* idx3;
+  const double* eig;
+  double domain[3];
+  double mean;
+  double sigma;
+  int mean_correction; /* 1: reference form ln(mean) - sigma^2/2; 0: exp(sigma g) */
+} MSG_KL;
+
+/* Build the KL table of the separable exponential kernel exp(-sum|dx_a|/corr_len)
+ * on [0,domain] (analytic 1-D eigen-pairs, n1d modes per axis, the n_terms
+ * largest 3-D products). Outputs into the caller's arrays w3/amp3/idx3 [n_terms][3], eig [n_terms]. */
+int MSG_KL_TABLE(const double* domain3, double corr_len, int n_terms, int n1d, double* w3, double* amp3,
+                 int* idx3, double* eig);
+/* E [R][n_elems] for xi [R][n_terms] (the MC loop's RandomVariables,
+ * MonteCarloAnalyzerWithStochasticMaterial.cs:258-261). */
+int MSG_KL_FIELD(MSG_MESH mesh, const MSG_KL* kl, int R, const double* xi, double* E);
+
+/* ------------------------------------------------------------------ Monte Carlo batch */
+/* The realization loop of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
+ * (ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:232-296):
+ * for each realization r: E field from xi[r], rebuild K, solve K x_r = b.
+ *   mode MSG_MODE_FP64_BSR: realizations one after another, FP64 BSR + Jacobi PCG
+ *     (recursive-residual stop as MSG_PCG_SOLVE).
+ *   mode MSG_MODE_MIXED_BATCHED: all realizations in one batch on a structured
+ *     cube lattice: matrix-free FP32 element-by-element operator inside
+ *     Jacobi-PCG, FP64 true residual r = b - K x and FP64 solution update
+ *     (iterative refinement); stop when ||b - K x||/||b|| < tol in FP64.
+ * xi [R][kl->n_terms], b [n_dofs]. Outputs (each may be NULL): X [R][n_dofs],
+ * tip [R] = X[r][tip_dof], iterations [R] (matrix products per realization),
+ * rel_res [R] (final FP64 ||b - K x||/||b||). */
+int MSG_MC_SOLVE_BATCH(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const double* xi, const double* b,
+                       int mode, int max_it, double tol, int tip_dof, double* X, double* tip, int* iterations,
+                       double* rel_res);
+/* Device-pointer variant (xi_dev, b_dev, X_dev on this context's device; X_dev may
+ * be NULL). Host outputs tip/iterations/rel_res as above. For callers that keep
+ * inputs and results resident in device memory. */
+int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const double* xi_dev,
+                              const double* b_dev, int mode, int max_it, double tol, int tip_dof, double* X_dev,
+                              double* tip, int* iterations, double* rel_res);
+
+/* Tunables of the mixed solver on this context: "inner_tol" (relative residual
+ * of each inner FP32 solve, default 1e-4), "inner_max" (inner iterations per
+ * refinement step), "chunk" (inner iterations per CUDA-graph launch, even). */
+int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
+
+/* Kernel launch counter of this context (kernels launched since creation),
+ * and per-phase device timings of the last MC batch in ms:
+ * t[0]=field, t[1]=inner operator, t[2]=inner update, t[3]=FP64 residual, t[4]=total. */
+int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,20 @@
+"""msolve_b200: B200-native (sm_100a) Hexa8 linear-elastic solve path of MSolve.
+
+The product is ``libmsolve_gpu.so`` (C ABI in ``include/msolve_gpu.h``); this
+package is its host-side mirror of the reference's preprocessor, provider,
+solver and analyzer interfaces, bound through ctypes.
+"""
+from ._native import (ArgumentError, Context, InvalidOperationError, MSolveError, MSG_MODE_FP64_BSR,
+                      MSG_MODE_MIXED_BATCHED, lib)
+from .analyzers import (GpuMatrix, GpuMesh, LinearAnalyzer, LognormalStochasticCoefficientsProvider,
+                        MonteCarloAnalyzerWithStochasticMaterial, ProblemStructural, SolverPCG, StaticAnalyzer,
+                        h8_mass_batch, h8_stiffness_batch)
+from .model import Hexa8MeshGenerator, Model, cantilever_model, clamped_block_model, tip_dof
+
+__all__ = [
+    "ArgumentError", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
+    "lib", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
+    "MonteCarloAnalyzerWithStochasticMaterial", "ProblemStructural", "SolverPCG", "StaticAnalyzer",
+    "h8_mass_batch", "h8_stiffness_batch", "Hexa8MeshGenerator", "Model", "cantilever_model",
+    "clamped_block_model", "tip_dof",
+]

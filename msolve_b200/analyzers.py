@@ -1,0 +1,291 @@
+"""Host mirror of the reference's solver / provider / analyzer interfaces on
+top of the C ABI, so code written against MSolve's StaticAnalyzer ->
+LinearAnalyzer -> ISolver chain and its Monte Carlo analyzer can drive the
+GPU path with the same call sequence:
+
+    model = clamped_block_model(32)
+    ctx = Context(0)
+    solver = SolverPCG(ctx, model)                  # ISolver (SolverPCG<T>)
+    provider = ProblemStructural(ctx, model)        # IStaticProvider
+    static = StaticAnalyzer(provider, LinearAnalyzer(solver))
+    static.BuildMatrices(); static.Initialize(); static.Solve()
+    model.subdomains[0].Solution
+
+References: IAnalyzer (ISAAR.MSolve.Analyzers/Interfaces/IAnalyzer.cs:9-17),
+StaticAnalyzer.cs:10-75, LinearAnalyzer.cs:12-69, ProblemStructural.cs:16-221,
+ISolver (ISAAR.MSolve.Solvers/Interfaces/ISolver.cs:8-12),
+SolverPCGSkyline.cs:75-108 (Initialize / Solve(20000, 1e-7)),
+MonteCarloAnalyzerWithStochasticMaterial.cs:55-296.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .model import tip_dof as _tip_dof
+
+
+class GpuMatrix:
+    """Assembled FP64 global stiffness on the device (IMatrix2D analogue)."""
+
+    def __init__(self, mesh, handle):
+        self.mesh, self.handle = mesh, handle
+
+    def Multiply(self, x):
+        x = N.f64(x)
+        y = np.zeros(self.mesh.model.n_dofs)
+        N.check(N.lib().MSG_MAT_MULTIPLY(self.handle, N.ptr(x), N.ptr(y)), self.mesh.ctx.handle, "Multiply")
+        return y
+
+    def Diagonal(self):
+        d = np.zeros(self.mesh.model.n_dofs)
+        N.check(N.lib().MSG_MAT_DIAGONAL(self.handle, N.ptr(d)), self.mesh.ctx.handle, "Diagonal")
+        return d
+
+    def close(self):
+        if self.handle:
+            N.lib().MSG_MAT_DESTROY(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuMesh:
+    """Device copy of a model's mesh and DOF map (MSG_MESH_CREATE)."""
+
+    def __init__(self, ctx, model):
+        if model.dof is None:
+            model.ConnectDataStructures()
+        self.ctx, self.model = ctx, model
+        h = N._vp()
+        N.check(N.lib().MSG_MESH_CREATE(ctx.handle, model.n_nodes, N.ptr(model.xyz), model.n_elems,
+                                        N.ptr(model.conn, N._i), N.ptr(N.i32(model.dof), N._i), model.n_dofs,
+                                        C.byref(h)), ctx.handle, "MSG_MESH_CREATE")
+        self.handle = h
+
+    def info(self):
+        a = np.zeros(8, dtype=np.int64)
+        N.check(N.lib().MSG_MESH_INFO(self.handle, N.ptr(a, N._i64)))
+        return dict(structured=bool(a[0]), nx=int(a[1]), ny=int(a[2]), nz=int(a[3]), n_dofs=int(a[4]),
+                    n_block_rows=int(a[5]), nnzb=int(a[6]), n_elems=int(a[7]))
+
+    def assemble(self, E_elem, nu):
+        h = N._vp()
+        E_elem = N.f64(E_elem)
+        N.check(N.lib().MSG_ASSEMBLE_BSR(self.handle, N.ptr(E_elem), float(nu), C.byref(h)), self.ctx.handle,
+                "MSG_ASSEMBLE_BSR")
+        return GpuMatrix(self, h)
+
+    def assemble_from_element_matrices(self, Ke):
+        h = N._vp()
+        Ke = N.f64(Ke)
+        N.check(N.lib().MSG_ASSEMBLE_BSR_KE(self.handle, N.ptr(Ke), C.byref(h)), self.ctx.handle,
+                "MSG_ASSEMBLE_BSR_KE")
+        return GpuMatrix(self, h)
+
+    def close(self):
+        if self.handle:
+            N.lib().MSG_MESH_DESTROY(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def h8_stiffness_batch(ctx, xyz, E, nu):
+    """MSG_H8_KE_BATCH: packed K_e [n][300] (CalcH8GaussMatrices + CalcH8K)."""
+    xyz = N.f64(xyz).reshape(-1, 24)
+    n = xyz.shape[0]
+    E = N.f64(np.broadcast_to(np.asarray(E, dtype=np.float64), (n,)))
+    K = np.zeros((n, 300))
+    N.check(N.lib().MSG_H8_KE_BATCH(ctx.handle, n, N.ptr(xyz), N.ptr(E), float(nu), N.ptr(K)), ctx.handle,
+            "MSG_H8_KE_BATCH")
+    return K
+
+
+def h8_mass_batch(ctx, xyz, rho):
+    """MSG_H8_ME_BATCH: packed consistent mass [n][300] (Hexa8.CalculateConsistentMass)."""
+    xyz = N.f64(xyz).reshape(-1, 24)
+    M = np.zeros((xyz.shape[0], 300))
+    N.check(N.lib().MSG_H8_ME_BATCH(ctx.handle, xyz.shape[0], N.ptr(xyz), float(rho), N.ptr(M)), ctx.handle,
+            "MSG_H8_ME_BATCH")
+    return M
+
+
+class ProblemStructural:
+    """IStaticProvider: builds the global stiffness on the device
+    (ProblemStructural.BuildKs / CalculateMatrix, ProblemStructural.cs:63-89, 217-221)."""
+
+    def __init__(self, ctx, model):
+        self.ctx, self.model = ctx, model
+        self.mesh = GpuMesh(ctx, model)
+        self.K = None
+
+    def Reset(self):
+        if self.K is not None:
+            self.K.close()
+        self.K = None
+
+    def CalculateMatrix(self, subdomain=None):
+        if self.K is None:
+            self.K = self.mesh.assemble(self.model.E_elem, self.model.poisson)
+        return self.K
+
+
+class SolverPCG:
+    """ISolver over the device Jacobi-PCG (SolverPCG.Solve, PCG/SolverPCG.cs:105-149).
+    Solve() uses (20000, 1e-7) as SolverPCG<T>.Solve() does (SolverPCGSkyline.cs:102-108)."""
+
+    def __init__(self, ctx, model, max_iterations=20000, tolerance=1e-7):
+        self.ctx, self.model = ctx, model
+        self.max_iterations, self.tolerance = max_iterations, tolerance
+        self.matrix = None
+        self.iterations = 0
+        self.rel_res = None
+
+    def Initialize(self):
+        if self.matrix is None:
+            raise N.InvalidOperationError(N.MSG_ERR_INVALID_ARGUMENT, "no matrix: call BuildMatrices first")
+
+    def Solve(self, max_iterations=None, tolerance=None):
+        s = self.model.subdomains[0]
+        b = N.f64(s.RHS)
+        x = np.zeros(self.model.n_dofs)
+        it, rr = C.c_int(0), C.c_double(0)
+        st = N.lib().MSG_PCG_SOLVE(self.matrix.handle, N.ptr(b), N.ptr(x), int(max_iterations or self.max_iterations),
+                                   float(tolerance or self.tolerance), C.byref(it), C.byref(rr))
+        self.iterations, self.rel_res = it.value, rr.value
+        s.Solution = x
+        N.check(st, self.ctx.handle, "MSG_PCG_SOLVE")
+        return x
+
+
+class LinearAnalyzer:
+    """IAnalyzer child: Initialize -> solver.Initialize, Solve -> solver.Solve (LinearAnalyzer.cs:57-69)."""
+
+    def __init__(self, solver):
+        self.solver = solver
+        self.ParentAnalyzer = None
+
+    def BuildMatrices(self):
+        if self.ParentAnalyzer is None:
+            raise N.InvalidOperationError(N.MSG_ERR_INVALID_ARGUMENT, "linear analyzer needs a parent")
+        self.ParentAnalyzer.BuildMatrices()
+
+    def Initialize(self):
+        self.solver.Initialize()
+
+    def Solve(self):
+        self.solver.Solve()
+
+
+class StaticAnalyzer:
+    """IAnalyzer parent (StaticAnalyzer.cs:18-75)."""
+
+    def __init__(self, provider, child):
+        self.provider, self.ChildAnalyzer = provider, child
+        child.ParentAnalyzer = self
+
+    def BuildMatrices(self):
+        self.ChildAnalyzer.solver.matrix = self.provider.CalculateMatrix(self.provider.model.subdomains[0])
+
+    def Initialize(self):
+        self.ChildAnalyzer.Initialize()
+
+    def Solve(self):
+        self.ChildAnalyzer.Solve()
+
+
+class LognormalStochasticCoefficientsProvider:
+    """KL lognormal Young's modulus (LognormalFileStochasticCoefficientsProvider.cs:43-193).
+    The eigen-data table the reference reads from a file is built analytically
+    for the separable exponential kernel (MSG_KL_TABLE)."""
+
+    def __init__(self, domain, corr_len, n_terms=50, n1d=16, mean=1.0, sigma=0.3, mean_correction=False):
+        self.domain = np.asarray(domain, dtype=np.float64)
+        self.n_terms, self.mean, self.sigma, self.mean_correction = n_terms, mean, sigma, mean_correction
+        self.w = np.zeros((n_terms, 3))
+        self.amp = np.zeros((n_terms, 3))
+        self.idx = np.zeros((n_terms, 3), dtype=np.int32)
+        self.eig = np.zeros(n_terms)
+        N.check(N.lib().MSG_KL_TABLE(N.ptr(N.f64(self.domain)), float(corr_len), n_terms, n1d, N.ptr(self.w),
+                                     N.ptr(self.amp), N.ptr(self.idx, N._i), N.ptr(self.eig)), None, "MSG_KL_TABLE")
+        self.RandomVariables = None
+
+    def struct(self):
+        s = N.MSG_KL()
+        s.n_terms = self.n_terms
+        s.w3, s.amp3, s.eig = N.ptr(self.w), N.ptr(self.amp), N.ptr(self.eig)
+        s.idx3 = N.ptr(self.idx, N._i)
+        for a in range(3):
+            s.domain[a] = float(self.domain[a])
+        s.mean, s.sigma, s.mean_correction = float(self.mean), float(self.sigma), int(bool(self.mean_correction))
+        return s
+
+    def table(self):
+        return dict(w=self.w, amp=self.amp, idx=self.idx, eig=self.eig)
+
+    def field(self, mesh, xi):
+        xi = N.f64(np.atleast_2d(xi))
+        E = np.zeros((xi.shape[0], mesh.model.n_elems))
+        s = self.struct()
+        N.check(N.lib().MSG_KL_FIELD(mesh.handle, C.byref(s), xi.shape[0], N.ptr(xi), N.ptr(E)), mesh.ctx.handle,
+                "MSG_KL_FIELD")
+        return E
+
+
+class MonteCarloAnalyzerWithStochasticMaterial:
+    """The realization loop (MonteCarloAnalyzerWithStochasticMaterial.cs:55-296).
+    Initialize() draws xi[simulations][expansion_order] ~ N(0,1) from a seeded
+    generator (the reference draws with Troschuetz.Random; the stream is not part
+    of parity, the same table feeds every implementation). Solve() runs all
+    realizations through MSG_MC_SOLVE_BATCH in `mode` ("mixed": one batched
+    mixed-precision launch sequence; "fp64": the plain FP64 drop-in, one
+    realization after another). Results: Solutions [R][n_dofs] (if keep_solutions),
+    TipValues [R], Iterations [R], Residuals [R]."""
+
+    def __init__(self, ctx, model, coefficients_provider, expansion_order=50, simulations=1, seed=12345,
+                 mode="mixed", max_iterations=20000, tolerance=1e-8, keep_solutions=True, tip_dof=None):
+        self.ctx, self.model, self.kl = ctx, model, coefficients_provider
+        self.expansion_order, self.simulations, self.seed = expansion_order, simulations, seed
+        self.mode = N.MSG_MODE_MIXED_BATCHED if mode == "mixed" else N.MSG_MODE_FP64_BSR
+        self.max_iterations, self.tolerance = max_iterations, tolerance
+        self.keep_solutions = keep_solutions
+        self.tip_dof = _tip_dof(model) if tip_dof is None else tip_dof
+        self.mesh = GpuMesh(ctx, model)
+        self.RandomNumbers = None
+
+    def Initialize(self):
+        rng = np.random.default_rng(self.seed)
+        self.RandomNumbers = rng.standard_normal((self.simulations, self.expansion_order))
+
+    def Solve(self):
+        if self.RandomNumbers is None:
+            self.Initialize()
+        R = self.simulations
+        xi = N.f64(self.RandomNumbers)
+        b = N.f64(self.model.subdomains[0].RHS)
+        X = np.zeros((R, self.model.n_dofs)) if self.keep_solutions else None
+        tip = np.zeros(R)
+        its = np.zeros(R, dtype=np.int32)
+        res = np.zeros(R)
+        s = self.kl.struct()
+        st = N.lib().MSG_MC_SOLVE_BATCH(self.mesh.handle, float(self.model.poisson), C.byref(s), R, N.ptr(xi), N.ptr(b),
+                                        self.mode, int(self.max_iterations), float(self.tolerance), int(self.tip_dof),
+                                        N.ptr(X) if X is not None else None, N.ptr(tip), N.ptr(its, N._i), N.ptr(res))
+        self.Solutions, self.TipValues, self.Iterations, self.Residuals = X, tip, its, res
+        N.check(st, self.ctx.handle, "MSG_MC_SOLVE_BATCH")
+        return tip
+
+    def statistics(self):
+        t = self.TipValues
+        return dict(mean=float(np.mean(t)), variance=float(np.var(t, ddof=1)) if len(t) > 1 else 0.0)

@@ -1,0 +1,415 @@
+// Assembled FP64 path: 3x3 block sliced-ELL (SELL-32) stiffness built on the
+// device from element matrices, its SpMV, and a Jacobi-PCG whose whole loop
+// runs on the device.
+//
+// Replaces the skyline assembler (GlobalMatrixAssemblerSkyline.cs:51-103), the
+// skyline product (SkylineMatrix2D.Multiply :224-286) and the PCG loop of
+// SolverPCG.Solve (PCG/SolverPCG.cs:105-149) with the simple search vector
+// (SolverPCGSimpleSearchVectorCalculator.cs:18-41) and the diagonal
+// preconditioner z_j = r_j / K_jj (PolynomialChaosSolverPCGMatrixCalculator.cs:467-495).
+//
+// Layout: block row = mesh node; vectors in node layout v[3*node + comp]
+// (constrained components hold 0 and their matrix rows/columns are identity).
+// SELL values: val[((slot)*9 + k)*32 + lane], k = 3*row_comp + col_comp, so a
+// warp reads each of the 9 block entries of 32 consecutive rows as one 256-byte
+// coalesced load; the matrix stream is the whole HBM traffic of the product.
+#include <algorithm>
+
+#include "msg_internal.h"
+
+namespace msg {
+namespace {
+
+constexpr int kSpmvThreads = 128;
+
+// One thread per (flat position, block entry k): sum the element
+// contributions (e, a, b) of this block in their fixed order, then apply the
+// Dirichlet mask (identity on constrained rows/columns).
+__global__ void k_bsr_assemble(int64_t n_pos, const int* __restrict__ /*col*/, const int64_t* __restrict__ cptr,
+                               const int* __restrict__ contrib, const double* __restrict__ Ke,
+                               double* __restrict__ val) {
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (tid >= n_pos * 9) return;
+  const int64_t pos = tid / 9;
+  const int k = (int)(tid - pos * 9);
+  const int64_t slot = pos >> 5;
+  const int lane = (int)(pos & 31);
+  const int cr = k / 3, cc = k - 3 * cr;
+  double acc = 0.0;
+  for (int64_t q = cptr[pos]; q < cptr[pos + 1]; ++q) {
+    const int code = contrib[q];
+    const int e = code >> 6, a = (code >> 3) & 7, b = code & 7;
+    acc += Ke[(size_t)e * 300 + packed_index(3 * a + cr, 3 * b + cc)];
+  }
+  val[(slot * 9 + k) * 32 + lane] = acc;
+}
+
+// Dirichlet masking pass: row node = slice*32 + lane, column node = col[pos].
+__global__ void k_bsr_mask(int n_rows, const int64_t* __restrict__ slice_ptr, const int* __restrict__ col,
+                           const uint8_t* __restrict__ mask, double* __restrict__ val) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  const int slice = row >> 5, lane = row & 31;
+  const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
+  const uint8_t mr = mask[row];
+  for (int64_t s = s0; s < s1; ++s) {
+    const int c = col[s * 32 + lane];
+    if (c < 0) break;
+    const uint8_t mc = mask[c];
+    if ((mr | mc) == 0) continue;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int cr = k / 3, cc = k % 3;
+      if (((mr >> cr) & 1) || ((mc >> cc) & 1)) val[(s * 9 + k) * 32 + lane] = (c == row && cr == cc) ? 1.0 : 0.0;
+    }
+  }
+}
+
+__global__ void k_bsr_diag_inv(int n_rows, const int* __restrict__ diag_pos, const double* __restrict__ val,
+                               double* __restrict__ dinv) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  const int64_t pos = diag_pos[row];
+  const int64_t slot = pos >> 5;
+  const int lane = (int)(pos & 31);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dinv[3 * row + c] = 1.0 / val[(slot * 9 + 4 * c) * 32 + lane];
+}
+
+__device__ __forceinline__ void sell_row(int row, const int64_t* __restrict__ slice_ptr, const int* __restrict__ col,
+                                         const double* __restrict__ val, const double* __restrict__ x, double* y3) {
+  const int slice = row >> 5, lane = row & 31;
+  const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
+  double y0 = 0, y1 = 0, y2 = 0;
+  for (int64_t s = s0; s < s1; ++s) {
+    const int c = __ldg(col + s * 32 + lane);
+    if (c < 0) break;
+    const double* v = val + s * 9 * 32 + lane;
+    const double x0 = __ldg(x + 3 * c), x1 = __ldg(x + 3 * c + 1), x2 = __ldg(x + 3 * c + 2);
+    y0 += __ldg(v + 0 * 32) * x0 + __ldg(v + 1 * 32) * x1 + __ldg(v + 2 * 32) * x2;
+    y1 += __ldg(v + 3 * 32) * x0 + __ldg(v + 4 * 32) * x1 + __ldg(v + 5 * 32) * x2;
+    y2 += __ldg(v + 6 * 32) * x0 + __ldg(v + 7 * 32) * x1 + __ldg(v + 8 * 32) * x2;
+  }
+  y3[0] = y0; y3[1] = y1; y3[2] = y2;
+}
+
+__global__ void __launch_bounds__(kSpmvThreads) k_bsr_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
+                                                           const int* __restrict__ col, const double* __restrict__ val,
+                                                           const double* __restrict__ x, double* __restrict__ y) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  double y3[3];
+  sell_row(row, slice_ptr, col, val, x, y3);
+  y[3 * row] = y3[0]; y[3 * row + 1] = y3[1]; y[3 * row + 2] = y3[2];
+}
+
+__global__ void k_dof_to_node(int n_dofs, const int* __restrict__ free_rows, const double* __restrict__ in,
+                              double* __restrict__ out, int64_t in_stride, int64_t out_stride) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = blockIdx.y;
+  if (i >= n_dofs) return;
+  out[v * out_stride + free_rows[i]] = in[v * in_stride + i];
+}
+
+__global__ void k_node_to_dof(int n_dofs, const int* __restrict__ free_rows, const double* __restrict__ in,
+                              double* __restrict__ out, int64_t in_stride, int64_t out_stride) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = blockIdx.y;
+  if (i >= n_dofs) return;
+  out[v * out_stride + i] = in[v * in_stride + free_rows[i]];
+}
+
+// ------------------------------------------------------------------ PCG
+// Device-resident Jacobi-PCG. Two kernels per iteration, each ending with a
+// last-block-done reduction that updates the scalar state in fixed block order
+// (deterministic results):
+//   k_pcg_dir_spmv: p_new = dinv.r + beta p_old (recomputed for gathered
+//     columns, written for own rows), q = K p_new, partial p.q
+//     -> last block: alpha = z.r / p.q (breakdown check)
+//   k_pcg_update:   r -= alpha q, x += alpha p_new, partials r.r and (dinv r).r
+//     -> last block: err = ||r||/||b||, convergence / iteration bookkeeping, beta
+// p is double-buffered by iteration parity so gathered columns are never read
+// while being overwritten.
+
+constexpr int kPcgThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sh[i];
+  return s;  // valid in thread 0
+}
+
+// Returns true in thread 0 of the last block to finish.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    const unsigned int ticket = atomicAdd(counter, 1u);
+    is_last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  return is_last;
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n_rows, const double* __restrict__ b,
+                                                          const double* __restrict__ dinv, double* __restrict__ r,
+                                                          double* __restrict__ x, double* __restrict__ p0,
+                                                          double* __restrict__ p1, double* __restrict__ partial,
+                                                          PcgState* st) {
+  __shared__ double sh[32];
+  double bb = 0, zr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
+    const double bi = b[i];
+    r[i] = bi; x[i] = 0; p0[i] = 0; p1[i] = 0;
+    bb += bi * bi;
+    zr += bi * dinv[i] * bi;
+  }
+  double s1 = block_sum(bb, sh);
+  double s2 = block_sum(zr, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
+  if (last_block(&st->counter) && threadIdx.x == 0) {
+    double tb = 0, tz = 0;
+    for (unsigned int i = 0; i < gridDim.x; ++i) { tb += __ldcg(partial + 2 * i); tz += __ldcg(partial + 2 * i + 1); }
+    st->bnorm = sqrt(tb);
+    st->zr = tz;
+    st->beta = 0; st->alpha = 0; st->err = 0;
+    st->it = 0; st->iterations = 0; st->matvecs = 0; st->status = 0;
+    st->done = (st->bnorm > 1e-25) ? 0 : 1;  // SolverPCG.cs:112
+    st->counter = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_dir_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
+                                                              const int* __restrict__ col,
+                                                              const double* __restrict__ val,
+                                                              const double* __restrict__ dinv,
+                                                              const double* __restrict__ r, double* p0, double* p1,
+                                                              double* __restrict__ q, double* __restrict__ partial,
+                                                              PcgState* st) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  const int it = st->it;
+  const double beta = st->beta;
+  const double* __restrict__ pold = (it & 1) ? p1 : p0;
+  double* __restrict__ pnew = (it & 1) ? p0 : p1;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double pq = 0;
+  if (row < n_rows) {
+    const int slice = row >> 5, lane = row & 31;
+    const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
+    double y0 = 0, y1 = 0, y2 = 0;
+    for (int64_t s = s0; s < s1; ++s) {
+      const int c = __ldg(col + s * 32 + lane);
+      if (c < 0) break;
+      const double* v = val + s * 9 * 32 + lane;
+      const double x0 = dinv[3 * c] * r[3 * c] + beta * pold[3 * c];
+      const double x1 = dinv[3 * c + 1] * r[3 * c + 1] + beta * pold[3 * c + 1];
+      const double x2 = dinv[3 * c + 2] * r[3 * c + 2] + beta * pold[3 * c + 2];
+      y0 += __ldg(v + 0 * 32) * x0 + __ldg(v + 1 * 32) * x1 + __ldg(v + 2 * 32) * x2;
+      y1 += __ldg(v + 3 * 32) * x0 + __ldg(v + 4 * 32) * x1 + __ldg(v + 5 * 32) * x2;
+      y2 += __ldg(v + 6 * 32) * x0 + __ldg(v + 7 * 32) * x1 + __ldg(v + 8 * 32) * x2;
+    }
+    double pn[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      pn[c] = dinv[3 * row + c] * r[3 * row + c] + beta * pold[3 * row + c];
+      pnew[3 * row + c] = pn[c];
+    }
+    q[3 * row] = y0; q[3 * row + 1] = y1; q[3 * row + 2] = y2;
+    pq = pn[0] * y0 + pn[1] * y1 + pn[2] * y2;
+  }
+  const double s = block_sum(pq, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  if (last_block(&st->counter) && threadIdx.x == 0) {
+    double t = 0;
+    for (unsigned int i = 0; i < gridDim.x; ++i) t += __ldcg(partial + i);
+    st->pq = t;
+    st->matvecs += 1;
+    if (!(t > 0) || isnan(t)) {  // breakdown: p.q <= 0 or NaN
+      st->status = MSG_ERR_BREAKDOWN; st->done = 1; st->iterations = it;
+    } else {
+      st->alpha = st->zr / t;
+    }
+    st->counter = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const double* __restrict__ dinv,
+                                                            double* __restrict__ r, double* __restrict__ x,
+                                                            const double* __restrict__ p0,
+                                                            const double* __restrict__ p1,
+                                                            const double* __restrict__ q, double* __restrict__ partial,
+                                                            PcgState* st) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  const int it = st->it;
+  const double alpha = st->alpha;
+  const double* __restrict__ pnew = (it & 1) ? p0 : p1;
+  double rr = 0, zr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
+    const double ri = r[i] - alpha * q[i];
+    r[i] = ri;
+    x[i] = x[i] + alpha * pnew[i];
+    rr += ri * ri;
+    zr += dinv[i] * ri * ri;
+  }
+  double s1 = block_sum(rr, sh);
+  double s2 = block_sum(zr, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
+  if (last_block(&st->counter) && threadIdx.x == 0) {
+    double tr = 0, tz = 0;
+    for (unsigned int i = 0; i < gridDim.x; ++i) { tr += __ldcg(partial + 2 * i); tz += __ldcg(partial + 2 * i + 1); }
+    st->err = sqrt(tr) / st->bnorm;
+    if (st->err < st->tol) {
+      st->done = 1; st->iterations = it;
+    } else if (it + 1 >= st->max_it) {
+      st->done = 1; st->iterations = st->max_it; st->status = MSG_ERR_NOT_CONVERGED;
+    } else {
+      st->beta = tz / st->zr;
+      st->zr = tz;
+      st->it = it + 1;
+    }
+    st->counter = 0;
+  }
+}
+
+}  // namespace
+
+int launch_bsr_assemble(Context* ctx, const Mesh* m, const double* d_Ke, double* d_val) {
+  const int64_t n_pos = m->pat.n_slots * 32;
+  if (n_pos == 0) return MSG_OK;
+  const int64_t nt = n_pos * 9;
+  k_bsr_assemble<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(
+      n_pos, m->d_col.as<int>(), m->d_contrib_ptr.as<int64_t>(), m->d_contrib.as<int>(), d_Ke, d_val);
+  k_bsr_mask<<<(m->n_nodes + 127) / 128, 128, 0, ctx->stream>>>(m->n_nodes, m->d_slice_ptr.as<int64_t>(),
+                                                                m->d_col.as<int>(), m->d_mask.as<uint8_t>(), d_val);
+  count_launch(ctx, 2);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+int launch_bsr_diag_inv(Context* ctx, const Mesh* m, const double* d_val, double* d_dinv) {
+  k_bsr_diag_inv<<<(m->n_nodes + 127) / 128, 128, 0, ctx->stream>>>(m->n_nodes, m->d_diag_pos.as<int>(), d_val,
+                                                                    d_dinv);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+int launch_bsr_spmv(Context* ctx, const Mesh* m, const double* d_val, const double* d_x, double* d_y) {
+  k_bsr_spmv<<<(m->n_nodes + kSpmvThreads - 1) / kSpmvThreads, kSpmvThreads, 0, ctx->stream>>>(
+      m->n_nodes, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), d_val, d_x, d_y);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+int launch_dof_to_node(Context* ctx, const Mesh* m, const double* d_in, double* d_out, int n_vec, int64_t in_stride,
+                       int64_t out_stride) {
+  if (m->n_dofs == 0 || n_vec == 0) return MSG_OK;
+  dim3 grid((m->n_dofs + 255) / 256, n_vec);
+  k_dof_to_node<<<grid, 256, 0, ctx->stream>>>(m->n_dofs, m->d_free_rows.as<int>(), d_in, d_out, in_stride,
+                                               out_stride);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* d_out, int n_vec, int64_t in_stride,
+                       int64_t out_stride) {
+  if (m->n_dofs == 0 || n_vec == 0) return MSG_OK;
+  dim3 grid((m->n_dofs + 255) / 256, n_vec);
+  k_node_to_dof<<<grid, 256, 0, ctx->stream>>>(m->n_dofs, m->d_free_rows.as<int>(), d_in, d_out, in_stride,
+                                               out_stride);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+// Runs the device PCG on node-layout vectors. The loop body (2 kernels) is
+// captured once per matrix as a CUDA graph of `chunk` iterations; the host
+// launches the graph and reads back the 4-byte `done` flag after each chunk.
+// Kernels after convergence return immediately, so the recorded iteration
+// count is exact.
+int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, int max_it, double tol, int* iterations,
+                     double* rel_res, int* status) {
+  Mesh* m = A->mesh;
+  const int nr = m->n_nodes;
+  const int n = 3 * nr;
+  if (!A->d_r.ptr) {
+    MSG_TRY(A->d_r.alloc(ctx, sizeof(double) * n));
+    MSG_TRY(A->d_p0.alloc(ctx, sizeof(double) * n));
+    MSG_TRY(A->d_p1.alloc(ctx, sizeof(double) * n));
+    MSG_TRY(A->d_q.alloc(ctx, sizeof(double) * n));
+    MSG_TRY(A->d_partial.alloc(ctx, sizeof(double) * 2 * 4096));
+    MSG_TRY(A->d_state.alloc(ctx, sizeof(PcgState)));
+    MSG_CUDA(ctx, cudaMemsetAsync(A->d_state.ptr, 0, sizeof(PcgState), ctx->stream));
+  }
+  PcgState* st = A->d_state.as<PcgState>();
+  const int grid_v = std::min(4096, std::max(1, std::min((n + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 8)));
+  const int grid_s = (nr + kPcgThreads - 1) / kPcgThreads;
+  // the partial buffer holds 8192 doubles: grid_s (SpMV) and 2*grid_v (update) entries
+  if (grid_s > 8192) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh too large for the PCG partial buffer");
+
+  k_pcg_init<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, d_b, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
+                                                      A->d_p0.as<double>(), A->d_p1.as<double>(),
+                                                      A->d_partial.as<double>(), st);
+  count_launch(ctx);
+  // tol / max_it into the state (after init so the counter reset does not race)
+  {
+    struct { double tol; } h{tol};
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &h.tol, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->max_it, &max_it, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  const int chunk = 8;
+  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x) {
+    if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
+    cudaGraph_t g;
+    MSG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < chunk; ++k) {
+      k_pcg_dir_spmv<<<grid_s, kPcgThreads, 0, ctx->stream>>>(
+          nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val.as<double>(), A->d_dinv.as<double>(),
+          A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
+          A->d_partial.as<double>(), st);
+      k_pcg_update<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
+                                                            A->d_p0.as<double>(), A->d_p1.as<double>(),
+                                                            A->d_q.as<double>(), A->d_partial.as<double>(), st);
+    }
+    MSG_CUDA(ctx, cudaStreamEndCapture(ctx->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&A->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphInstantiate");
+    A->graph_chunk = chunk;
+    A->graph_x = d_x;
+  }
+  int* h_done = nullptr;
+  MSG_CUDA(ctx, cudaMallocHost(&h_done, sizeof(int)));
+  int done = 0;
+  const int max_chunks = max_it / chunk + 2;
+  for (int c = 0; c < max_chunks && !done; ++c) {
+    cudaError_t e = cudaGraphLaunch(A->graph, ctx->stream);
+    if (e != cudaSuccess) { cudaFreeHost(h_done); return cuda_error(ctx, e, "cudaGraphLaunch"); }
+    count_launch(ctx, 2 * chunk);
+    e = cudaMemcpyAsync(h_done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { cudaFreeHost(h_done); return cuda_error(ctx, e, "pcg chunk"); }
+    done = *h_done;
+  }
+  cudaFreeHost(h_done);
+  PcgState hs;
+  MSG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (iterations) *iterations = hs.iterations;
+  if (rel_res) *rel_res = hs.err;
+  if (status) *status = hs.status;
+  return MSG_OK;
+}
+
+}  // namespace msg

@@ -1,0 +1,111 @@
+// Lognormal Young's-modulus field from a separable Karhunen-Loeve table, the
+// device twin of LognormalFileStochasticCoefficientsProvider.GetCoefficient
+// (ISAAR.MSolve.PreProcessor/Stochastic/LognormalFileStochasticCoefficientsProvider.cs:134-193)
+// evaluated at element bounding-box centres (Hexa8WithStochasticMaterial.cs:112-140).
+//
+// psi[k][e] = sigma sqrt(eig_k) prod_a amp_ka {cos|sin}(w_ka (x_ea - L_a/2)) is
+// built once per mesh and table (FP64). The field for R realizations is then
+// the product [R x K] . [K x n_e] followed by exp:
+//   E[e][r] = exp(mu + sum_k xi[r][k] psi[k][e]).
+// A CTA stages a 32-realization x 32-element tile of xi and psi in shared
+// memory; each thread produces four (element, realization) values, written
+// realization-innermost (coalesced) in FP64 and FP32, and optionally in the
+// per-realization layout [r][e] used by the assembled FP64 path.
+#include "msg_internal.h"
+
+namespace msg {
+namespace {
+
+constexpr int kMaxTerms = 64;  // 2 x 64 x 33 doubles of shared memory
+
+__global__ void k_kl_psi(int ne, int K, const double* __restrict__ cen, const double* __restrict__ tab,
+                         double L0, double L1, double L2, double sigma, double* __restrict__ psi) {
+  // tab rows: [w0 w1 w2 a0 a1 a2 idx0 idx1 idx2 eig] per term
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (e >= ne) return;
+  const double* t = tab + 10 * k;
+  double f = sigma * sqrt(t[9]);
+  const double L[3] = {L0, L1, L2};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double x = cen[3 * e + a] - L[a] / 2;
+    const int idx = (int)t[6 + a];
+    f *= (idx % 2 == 0) ? t[3 + a] * sin(t[a] * x) : t[3 + a] * cos(t[a] * x);
+  }
+  psi[(size_t)k * ne + e] = f;
+}
+
+__global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, const double* __restrict__ xi,
+                                                  const double* __restrict__ psi, double mu,
+                                                  double* __restrict__ E64_er, float* __restrict__ E32_er,
+                                                  double* __restrict__ E64_re) {
+  __shared__ double s_xi[kMaxTerms][33];
+  __shared__ double s_psi[kMaxTerms][33];
+  const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+  const int e0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = ty; k < K; k += 8) {
+    const int r = r0 + tx;
+    s_xi[k][tx] = (r < R) ? xi[(size_t)r * K + k] : 0.0;
+    const int e = e0 + tx;
+    s_psi[k][tx] = (e < ne) ? psi[(size_t)k * ne + e] : 0.0;
+  }
+  __syncthreads();
+  const int r = r0 + tx;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int le = ty + 8 * q, e = e0 + le;
+    if (e >= ne) continue;
+    double s = mu;
+    for (int k = 0; k < K; ++k) s += s_xi[k][tx] * s_psi[k][le];
+    const double E = (r < R) ? exp(s) : 1.0;
+    if (E64_er) E64_er[(size_t)e * Rp + r] = E;
+    if (E32_er) E32_er[(size_t)e * Rp + r] = (float)E;
+    if (E64_re && r < R) E64_re[(size_t)r * ne + e] = E;
+  }
+}
+
+}  // namespace
+
+int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
+  const int K = kl->n_terms;
+  if (K <= 0 || K > kMaxTerms) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "n_terms must be in 1..%d", kMaxTerms);
+  if (!(kl->mean > 0)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "KL mean must be > 0");
+  std::vector<double> tab(10 * (size_t)K);
+  for (int k = 0; k < K; ++k) {
+    for (int a = 0; a < 3; ++a) {
+      tab[10 * k + a] = kl->w3[3 * k + a];
+      tab[10 * k + 3 + a] = kl->amp3[3 * k + a];
+      tab[10 * k + 6 + a] = (double)kl->idx3[3 * k + a];
+    }
+    tab[10 * k + 9] = kl->eig[k];
+    if (!(kl->eig[k] >= 0)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "KL eigenvalue %d is negative", k);
+  }
+  DevMem d_tab;
+  MSG_TRY(d_tab.alloc(ctx, sizeof(double) * tab.size()));
+  MSG_TRY(out->d_psi.alloc(ctx, sizeof(double) * (size_t)K * m->n_elems));
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_tab.ptr, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice,
+                                ctx->stream));
+  dim3 grid((m->n_elems + 127) / 128, K);
+  k_kl_psi<<<grid, 128, 0, ctx->stream>>>(m->n_elems, K, m->d_centroid.as<double>(), d_tab.as<double>(),
+                                          kl->domain[0], kl->domain[1], kl->domain[2], kl->sigma,
+                                          out->d_psi.as<double>());
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // d_tab is released on return
+  out->n_terms = K;
+  out->mu = std::log(kl->mean) - (kl->mean_correction ? 0.5 * kl->sigma * kl->sigma : 0.0);
+  return MSG_OK;
+}
+
+int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int Rp, const double* d_xi,
+                    double* d_E64_er, float* d_E32_er, double* d_E64_re) {
+  dim3 grid((m->n_elems + 31) / 32, Rp / 32);
+  k_kl_field<<<grid, dim3(32, 8), 0, ctx->stream>>>(m->n_elems, kl->n_terms, R, Rp, d_xi, kl->d_psi.as<double>(),
+                                                    kl->mu, d_E64_er, d_E32_er, d_E64_re);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+}  // namespace msg

@@ -1,0 +1,715 @@
+// Host runtime of libmsolve_gpu.so: the extern "C" entry points of
+// include/msolve_gpu.h, context and handle management, mesh analysis (3x3
+// block sparsity pattern, assembly contribution map, structured-lattice
+// detection) and the Monte Carlo batch driver.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "msg_internal.h"
+
+namespace msg {
+
+// ------------------------------------------------------------------ errors, memory
+int set_error(Context* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return code;
+}
+
+int cuda_error(Context* ctx, cudaError_t e, const char* where) {
+  const int code = (e == cudaErrorMemoryAllocation) ? MSG_ERR_OUT_OF_MEMORY : MSG_ERR_CUDA;
+  return set_error(ctx, code, "CUDA error in %s: %s (%s)", where, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+DevMem::~DevMem() { release(); }
+
+void DevMem::release() {
+  if (ptr) {
+    cudaFree(ptr);
+    if (ctx) ctx->used -= bytes;
+  }
+  ptr = nullptr;
+  bytes = 0;
+}
+
+int DevMem::alloc(Context* c, size_t n) {
+  release();
+  ctx = c;
+  if (n == 0) n = 16;
+  if (c->budget && c->used + n > c->budget)
+    return set_error(c, MSG_ERR_OUT_OF_MEMORY, "memory budget exceeded: %llu + %llu > %llu bytes",
+                     (unsigned long long)c->used.load(), (unsigned long long)n, (unsigned long long)c->budget);
+  cudaError_t e = cudaMalloc(&ptr, n);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    cudaGetLastError();
+    return cuda_error(c, e, "cudaMalloc");
+  }
+  bytes = n;
+  c->used += n;
+  return MSG_OK;
+}
+
+Matrix::~Matrix() {
+  if (graph) cudaGraphExecDestroy(graph);
+}
+
+template <class T>
+static int upload(Context* ctx, DevMem& dst, const T* src, size_t n) {
+  MSG_TRY(dst.alloc(ctx, sizeof(T) * n));
+  if (n) MSG_CUDA(ctx, cudaMemcpyAsync(dst.ptr, src, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+  return MSG_OK;
+}
+
+// Element stiffness of one cube of side h, E = 1, through the K1 kernel; full 24x24.
+int unit_cube_khat(Context* ctx, double h, double nu, double* K576) {
+  double xyz[24];
+  for (int a = 0; a < 8; ++a) {
+    const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
+    xyz[3 * a] = ax * h; xyz[3 * a + 1] = ay * h; xyz[3 * a + 2] = az * h;
+  }
+  DevMem dx, dk, ds;
+  MSG_TRY(upload(ctx, dx, xyz, 24));
+  MSG_TRY(dk.alloc(ctx, sizeof(double) * 300));
+  MSG_TRY(ds.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(ds.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_ke(ctx, 1, dx.as<double>(), nullptr, 1.0, nu, dk.as<double>(), ds.as<int>()));
+  double k300[300];
+  MSG_CUDA(ctx, cudaMemcpyAsync(k300, dk.ptr, sizeof(k300), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < 24; ++i)
+    for (int j = 0; j < 24; ++j) K576[i * 24 + j] = k300[packed_index(i, j)];
+  for (int i = 1; i < 24; ++i)
+    if (std::fabs(K576[i * 25] - K576[0]) > 1e-12 * std::fabs(K576[0]))
+      return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "cube stiffness has unequal diagonal entries");
+  return MSG_OK;
+}
+
+// ------------------------------------------------------------------ mesh analysis
+static int build_pattern(Mesh* m) {
+  const int nn = m->n_nodes, ne = m->n_elems;
+  // node adjacency through elements (CSR, sorted unique)
+  std::vector<int64_t> cnt(nn + 1, 0);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) cnt[m->conn[8 * e + a] + 1] += 8;
+  for (int i = 0; i < nn; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int> adj(cnt[nn]);
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) adj[fill[m->conn[8 * e + a]]++] = m->conn[8 * e + b];
+  std::vector<int> rowlen(nn);
+  std::vector<int64_t> rowstart(nn);
+  for (int i = 0; i < nn; ++i) {
+    auto b = adj.begin() + cnt[i], en = adj.begin() + cnt[i + 1];
+    std::sort(b, en);
+    rowlen[i] = (int)(std::unique(b, en) - b);
+    rowstart[i] = cnt[i];
+  }
+  BlockPattern& P = m->pat;
+  P.n_rows = nn;
+  P.n_slices = (nn + 31) / 32;
+  P.slice_ptr.assign(P.n_slices + 1, 0);
+  P.nnzb = 0;
+  for (int z = 0; z < P.n_slices; ++z) {
+    int w = 0;
+    for (int l = 0; l < 32 && 32 * z + l < nn; ++l) w = std::max(w, rowlen[32 * z + l]);
+    P.slice_ptr[z + 1] = P.slice_ptr[z] + w;
+  }
+  P.n_slots = P.slice_ptr[P.n_slices];
+  P.col.assign(P.n_slots * 32, -1);
+  P.diag_pos.assign(nn, -1);
+  for (int row = 0; row < nn; ++row) {
+    const int z = row / 32, lane = row % 32;
+    for (int s = 0; s < rowlen[row]; ++s) {
+      const int c = adj[rowstart[row] + s];
+      const int64_t pos = (P.slice_ptr[z] + s) * 32 + lane;
+      P.col[pos] = c;
+      if (c == row) P.diag_pos[row] = (int)pos;
+    }
+    P.nnzb += rowlen[row];
+  }
+  // contribution lists in element order (deterministic summation order)
+  const int64_t npos = P.n_slots * 32;
+  P.contrib_ptr.assign(npos + 1, 0);
+  std::vector<int64_t> where((size_t)ne * 64);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) {
+      const int row = m->conn[8 * e + a];
+      const int z = row / 32, lane = row % 32;
+      const int* rb = adj.data() + rowstart[row];
+      for (int b = 0; b < 8; ++b) {
+        const int c = m->conn[8 * e + b];
+        const int s = (int)(std::lower_bound(rb, rb + rowlen[row], c) - rb);
+        const int64_t pos = (P.slice_ptr[z] + s) * 32 + lane;
+        where[(size_t)e * 64 + a * 8 + b] = pos;
+        P.contrib_ptr[pos + 1]++;
+      }
+    }
+  for (int64_t p = 0; p < npos; ++p) P.contrib_ptr[p + 1] += P.contrib_ptr[p];
+  P.contrib.assign(P.contrib_ptr[npos], 0);
+  std::vector<int64_t> f2(P.contrib_ptr.begin(), P.contrib_ptr.end() - 1);
+  for (int e = 0; e < ne; ++e)
+    for (int ab = 0; ab < 64; ++ab) P.contrib[f2[where[(size_t)e * 64 + ab]]++] = e * 64 + ab;
+  return MSG_OK;
+}
+
+// Structured cube lattice in generator order (Hexa8MeshGenerator.cs:508-568 node
+// IDs x fastest, :1075-1089 element corners).
+static void detect_structured(Mesh* m) {
+  m->structured = false;
+  const int nn = m->n_nodes, ne = m->n_elems;
+  if (nn < 8 || ne < 1) return;
+  const double* X = m->xyz.data();
+  // axis extents from node 0 and the lattice size from the element count per axis
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) { lo[a] = hi[a] = X[a]; }
+  for (int i = 0; i < nn; ++i)
+    for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], X[3 * i + a]); hi[a] = std::max(hi[a], X[3 * i + a]); }
+  // element 0 edge length
+  const int* c0 = m->conn.data();
+  const double h = X[3 * c0[1]] - X[3 * c0[0]];
+  if (!(h > 0)) return;
+  int n[3];
+  for (int a = 0; a < 3; ++a) {
+    const double v = (hi[a] - lo[a]) / h;
+    n[a] = (int)std::lround(v);
+    if (n[a] < 1 || std::fabs(v - n[a]) > 1e-9 * std::max(1.0, v)) return;
+  }
+  const int NX = n[0] + 1, NY = n[1] + 1, NZ = n[2] + 1;
+  if ((int64_t)NX * NY * NZ != nn || (int64_t)n[0] * n[1] * n[2] != ne) return;
+  const double tol = 1e-9 * h;
+  for (int k = 0, id = 0; k < NZ; ++k)
+    for (int j = 0; j < NY; ++j)
+      for (int i = 0; i < NX; ++i, ++id) {
+        if (std::fabs(X[3 * id] - (lo[0] + i * h)) > tol || std::fabs(X[3 * id + 1] - (lo[1] + j * h)) > tol ||
+            std::fabs(X[3 * id + 2] - (lo[2] + k * h)) > tol)
+          return;
+      }
+  for (int k = 0, e = 0; k < n[2]; ++k)
+    for (int j = 0; j < n[1]; ++j)
+      for (int i = 0; i < n[0]; ++i, ++e) {
+        const int b = i + NX * (j + NY * k);
+        const int ref[8] = {b, b + 1, b + NX + 1, b + NX, b + NX * NY, b + NX * NY + 1, b + NX * NY + NX + 1,
+                            b + NX * NY + NX};
+        for (int a = 0; a < 8; ++a)
+          if (m->conn[8 * e + a] != ref[a]) return;
+      }
+  m->structured = true;
+  m->nx = n[0]; m->ny = n[1]; m->nz = n[2];
+  m->h = h;
+  for (int a = 0; a < 3; ++a) m->origin[a] = lo[a];
+}
+
+static int create_mesh(Context* ctx, int n_nodes, const double* xyz, int n_elems, const int* conn, const int* dof,
+                       int n_dofs, Mesh** out) {
+  if (n_nodes <= 0 || n_elems <= 0 || !xyz || !conn || !dof || n_dofs < 0 || !out)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh: invalid sizes or null pointers");
+  std::unique_ptr<msg_mesh> m(new msg_mesh());
+  m->ctx = ctx;
+  m->n_nodes = n_nodes; m->n_elems = n_elems; m->n_dofs = n_dofs;
+  m->xyz.assign(xyz, xyz + 3 * (size_t)n_nodes);
+  m->conn.assign(conn, conn + 8 * (size_t)n_elems);
+  m->dof.assign(dof, dof + 3 * (size_t)n_nodes);
+  for (size_t i = 0; i < m->conn.size(); ++i)
+    if (m->conn[i] < 0 || m->conn[i] >= n_nodes)
+      return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh: element node index out of range");
+  std::vector<int> free_rows(n_dofs, -1);
+  std::vector<uint8_t> mask(n_nodes, 0);
+  for (int i = 0; i < n_nodes; ++i)
+    for (int c = 0; c < 3; ++c) {
+      const int d = m->dof[3 * i + c];
+      if (d == -1) { mask[i] |= (uint8_t)(1 << c); continue; }
+      if (d < 0 || d >= n_dofs || free_rows[d] != -1)
+        return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh: DOF numbering is not a bijection onto 0..n_dofs-1");
+      free_rows[d] = 3 * i + c;
+    }
+  for (int d = 0; d < n_dofs; ++d)
+    if (free_rows[d] < 0) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh: DOF %d unused", d);
+  MSG_TRY(build_pattern(m.get()));
+  detect_structured(m.get());
+  std::vector<double> exyz(24 * (size_t)n_elems), cen(3 * (size_t)n_elems);
+  for (int e = 0; e < n_elems; ++e) {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int a = 0; a < 8; ++a)
+      for (int c = 0; c < 3; ++c) {
+        const double v = m->xyz[3 * (size_t)m->conn[8 * e + a] + c];
+        exyz[24 * (size_t)e + 3 * a + c] = v;
+        lo[c] = std::min(lo[c], v);
+        hi[c] = std::max(hi[c], v);
+      }
+    // Hexa8WithStochasticMaterial.GetStochasticPoints: min + extent/2
+    for (int c = 0; c < 3; ++c) cen[3 * (size_t)e + c] = lo[c] + (hi[c] - lo[c]) / 2;
+  }
+  const BlockPattern& P = m->pat;
+  MSG_TRY(upload(ctx, m->d_exyz, exyz.data(), exyz.size()));
+  MSG_TRY(upload(ctx, m->d_centroid, cen.data(), cen.size()));
+  MSG_TRY(upload(ctx, m->d_dof, m->dof.data(), m->dof.size()));
+  MSG_TRY(upload(ctx, m->d_mask, mask.data(), mask.size()));
+  MSG_TRY(upload(ctx, m->d_free_rows, free_rows.data(), free_rows.size()));
+  MSG_TRY(upload(ctx, m->d_col, P.col.data(), P.col.size()));
+  MSG_TRY(upload(ctx, m->d_slice_ptr, P.slice_ptr.data(), P.slice_ptr.size()));
+  MSG_TRY(upload(ctx, m->d_contrib_ptr, P.contrib_ptr.data(), P.contrib_ptr.size()));
+  MSG_TRY(upload(ctx, m->d_contrib, P.contrib.data(), P.contrib.size()));
+  MSG_TRY(upload(ctx, m->d_diag_pos, P.diag_pos.data(), P.diag_pos.size()));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *out = m.release();
+  return MSG_OK;
+}
+
+static int assemble_from_device_ke(Context* ctx, Mesh* m, const double* d_Ke, Matrix* A) {
+  if (!A->d_val.ptr) {
+    MSG_TRY(A->d_val.alloc(ctx, sizeof(double) * (size_t)m->pat.n_slots * 32 * 9));
+    MSG_TRY(A->d_dinv.alloc(ctx, sizeof(double) * (size_t)m->n_nodes * 3));
+  }
+  MSG_TRY(launch_bsr_assemble(ctx, m, d_Ke, A->d_val.as<double>()));
+  MSG_TRY(launch_bsr_diag_inv(ctx, m, A->d_val.as<double>(), A->d_dinv.as<double>()));
+  return MSG_OK;
+}
+
+// Element matrices for per-element E (device), then assembly into A.
+static int assemble_from_device_E(Context* ctx, Mesh* m, const double* d_E, double nu, Matrix* A, DevMem& ke,
+                                  DevMem& st, int* neg_det) {
+  if (!ke.ptr) MSG_TRY(ke.alloc(ctx, sizeof(double) * 300 * (size_t)m->n_elems));
+  if (!st.ptr) MSG_TRY(st.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(st.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_ke(ctx, m->n_elems, m->d_exyz.as<double>(), d_E, 0.0, nu, ke.as<double>(), st.as<int>()));
+  MSG_TRY(assemble_from_device_ke(ctx, m, ke.as<double>(), A));
+  if (neg_det) {
+    MSG_CUDA(ctx, cudaMemcpyAsync(neg_det, st.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return MSG_OK;
+}
+
+// Monte Carlo batch, device inputs.
+static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, const double* d_xi, const double* d_b,
+                    int mode, int max_it, double tol, int tip_dof, double* d_X, double* tip, int* iterations,
+                    double* rel_res) {
+  if (R <= 0 || !kl || !d_xi || !d_b || max_it <= 0 || !(tol > 0))
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "MC batch: invalid arguments");
+  if (tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
+  const int Rp = (R + 31) / 32 * 32;
+  cudaEvent_t e0, e1;
+  MSG_CUDA(ctx, cudaEventCreate(&e0));
+  MSG_CUDA(ctx, cudaEventCreate(&e1));
+  cudaEventRecord(e0, ctx->stream);
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, m, kl, &kd));
+  int status = MSG_OK;
+  if (mode == MSG_MODE_MIXED_BATCHED) {
+    if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mixed batched mode needs a structured cube lattice");
+    DevMem E64, E32;
+    MSG_TRY(E64.alloc(ctx, sizeof(double) * (size_t)m->n_elems * Rp));
+    MSG_TRY(E32.alloc(ctx, sizeof(float) * (size_t)m->n_elems * Rp));
+    cudaEvent_t f0, f1;
+    cudaEventCreate(&f0); cudaEventCreate(&f1);
+    cudaEventRecord(f0, ctx->stream);
+    MSG_TRY(launch_kl_field(ctx, m, &kd, R, Rp, d_xi, E64.as<double>(), E32.as<float>(), nullptr));
+    cudaEventRecord(f1, ctx->stream);
+    BatchOut o;
+    std::vector<double> htip(R);
+    o.tip = tip ? htip.data() : nullptr;
+    o.iterations = iterations;
+    o.rel_res = rel_res;
+    status = block_mixed_solve(ctx, m, nu, E64.as<double>(), E32.as<float>(), R, Rp, d_b, max_it, tol, tip_dof, d_X, o);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, f0, f1);
+    ctx->t_phase[0] = ms;
+    cudaEventDestroy(f0); cudaEventDestroy(f1);
+    if (tip) std::copy(htip.begin(), htip.end(), tip);
+  } else if (mode == MSG_MODE_FP64_BSR) {
+    DevMem E64re, ke, st, bnode, xnode, tipd;
+    MSG_TRY(E64re.alloc(ctx, sizeof(double) * (size_t)m->n_elems * R));
+    MSG_TRY(launch_kl_field(ctx, m, &kd, R, Rp, d_xi, nullptr, nullptr, E64re.as<double>()));
+    std::unique_ptr<msg_matrix> A(new msg_matrix());
+    A->mesh = m;
+    MSG_TRY(bnode.alloc(ctx, sizeof(double) * 3 * (size_t)m->n_nodes));
+    MSG_TRY(xnode.alloc(ctx, sizeof(double) * 3 * (size_t)m->n_nodes));
+    MSG_CUDA(ctx, cudaMemsetAsync(bnode.ptr, 0, sizeof(double) * 3 * (size_t)m->n_nodes, ctx->stream));
+    MSG_TRY(launch_dof_to_node(ctx, m, d_b, bnode.as<double>(), 1, 0, 0));
+    DevMem xdof;
+    MSG_TRY(xdof.alloc(ctx, sizeof(double) * (size_t)std::max(1, m->n_dofs)));
+    for (int r = 0; r < R; ++r) {
+      int neg = 0;
+      MSG_TRY(assemble_from_device_E(ctx, m, E64re.as<double>() + (size_t)r * m->n_elems, nu, A.get(), ke, st, nullptr));
+      int its = 0, pst = 0;
+      double rr = 0;
+      MSG_TRY(pcg_solve_device(ctx, A.get(), bnode.as<double>(), xnode.as<double>(), max_it, tol, &its, &rr, &pst));
+      double* xout = d_X ? d_X + (size_t)r * m->n_dofs : xdof.as<double>();
+      MSG_TRY(launch_node_to_dof(ctx, m, xnode.as<double>(), xout, 1, 0, 0));
+      if (tip && tip_dof >= 0) {
+        MSG_CUDA(ctx, cudaMemcpyAsync(tip + r, xout + tip_dof, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      }
+      if (iterations) iterations[r] = its + (pst == MSG_OK ? 1 : 0);  // matrix products
+      if (rel_res) rel_res[r] = rr;
+      if (pst != MSG_OK && status == MSG_OK) status = pst;
+      (void)neg;
+    }
+    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (status != MSG_OK) set_error(ctx, status, "FP64 batch: a realization did not converge");
+  } else {
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown mode %d", mode);
+  }
+  cudaEventRecord(e1, ctx->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  ctx->t_phase[4] = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return status;
+}
+
+// KL 1-D eigen-pairs of exp(-|x-y|/l) on [-A, A]: roots of
+// c cos(wA) - w sin(wA) (cos modes, odd index) and w cos(wA) + c sin(wA) (sin
+// modes, even index), c = 1/l, by safeguarded Newton inside the bracket.
+static double kl_root(double A, double c, bool is_sin, double lo, double hi) {
+  auto f = [&](double w) { return is_sin ? w * std::cos(w * A) + c * std::sin(w * A) : c * std::cos(w * A) - w * std::sin(w * A); };
+  auto df = [&](double w) {
+    return is_sin ? std::cos(w * A) - w * A * std::sin(w * A) + c * A * std::cos(w * A)
+                  : -c * A * std::sin(w * A) - std::sin(w * A) - w * A * std::cos(w * A);
+  };
+  double flo = f(lo);
+  double w = 0.5 * (lo + hi);
+  for (int it = 0; it < 200; ++it) {
+    const double fw = f(w);
+    if (fw == 0) return w;
+    if ((fw > 0) == (flo > 0)) { lo = w; flo = fw; } else { hi = w; }
+    const double d = df(w);
+    double wn = (d != 0) ? w - fw / d : 0.5 * (lo + hi);
+    if (!(wn > lo && wn < hi)) wn = 0.5 * (lo + hi);
+    if (std::fabs(wn - w) <= 1e-16 * std::fabs(w) || hi - lo <= 4e-16 * hi) { w = wn; break; }
+    w = wn;
+  }
+  return w;
+}
+
+}  // namespace msg
+
+using namespace msg;
+
+#define CTX_GUARD(ctx)                                        \
+  if (!(ctx)) return MSG_ERR_INVALID_ARGUMENT;                \
+  std::lock_guard<std::recursive_mutex> _lk((ctx)->mu);       \
+  cudaSetDevice((ctx)->device)
+
+extern "C" {
+
+int MSG_VERSION(void) { return 100; }
+
+int MSG_CREATE(int device, uint64_t mem_budget_bytes, MSG_CTX* out) {
+  if (!out) return MSG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return MSG_ERR_NO_DEVICE; }
+  if (device < 0 || device >= n) return MSG_ERR_INVALID_ARGUMENT;
+  std::unique_ptr<msg_context> c(new msg_context());
+  c->device = device;
+  c->budget = mem_budget_bytes;
+  if (cudaSetDevice(device) != cudaSuccess) return MSG_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return MSG_ERR_CUDA;
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  *out = c.release();
+  return MSG_OK;
+}
+
+int MSG_DESTROY(MSG_CTX ctx) {
+  if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return MSG_OK;
+}
+
+const char* MSG_LAST_ERROR(MSG_CTX ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
+  CTX_GUARD(ctx);
+  if (!key) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "null option key");
+  if (!std::strcmp(key, "inner_tol") && value > 0 && value < 1) { ctx->inner_tol = value; return MSG_OK; }
+  if (!std::strcmp(key, "inner_max") && value >= 1) { ctx->inner_max = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
+  return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
+}
+
+int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t5) {
+  if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
+  if (launches) *launches = ctx->launches.load();
+  if (t5)
+    for (int i = 0; i < 5; ++i) t5[i] = ctx->t_phase[i];
+  return MSG_OK;
+}
+
+int MSG_H8_KE_BATCH(MSG_CTX ctx, int n, const double* xyz, const double* E, double nu, double* Ke) {
+  CTX_GUARD(ctx);
+  if (n < 0 || (n > 0 && (!xyz || !E || !Ke))) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "KE batch: bad args");
+  if (n == 0) return MSG_OK;
+  if (!(nu > -1.0 && nu < 0.5)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Poisson ratio out of (-1, 0.5)");
+  DevMem dx, dE, dK, ds;
+  MSG_TRY(upload(ctx, dx, xyz, 24 * (size_t)n));
+  MSG_TRY(upload(ctx, dE, E, (size_t)n));
+  MSG_TRY(dK.alloc(ctx, sizeof(double) * 300 * (size_t)n));
+  MSG_TRY(ds.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(ds.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_ke(ctx, n, dx.as<double>(), dE.as<double>(), 0.0, nu, dK.as<double>(), ds.as<int>()));
+  int st = 0;
+  MSG_CUDA(ctx, cudaMemcpyAsync(Ke, dK.ptr, sizeof(double) * 300 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&st, ds.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (st != 0) return set_error(ctx, st, "negative or tiny Jacobian determinant (H8)");
+  return MSG_OK;
+}
+
+int MSG_H8_ME_BATCH(MSG_CTX ctx, int n, const double* xyz, double rho, double* Me) {
+  CTX_GUARD(ctx);
+  if (n < 0 || (n > 0 && (!xyz || !Me))) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "ME batch: bad args");
+  if (n == 0) return MSG_OK;
+  DevMem dx, dM, ds;
+  MSG_TRY(upload(ctx, dx, xyz, 24 * (size_t)n));
+  MSG_TRY(dM.alloc(ctx, sizeof(double) * 300 * (size_t)n));
+  MSG_TRY(ds.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(ds.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_me(ctx, n, dx.as<double>(), rho, dM.as<double>(), ds.as<int>()));
+  int st = 0;
+  MSG_CUDA(ctx, cudaMemcpyAsync(Me, dM.ptr, sizeof(double) * 300 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&st, ds.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (st != 0) return set_error(ctx, st, "negative or tiny Jacobian determinant (H8)");
+  return MSG_OK;
+}
+
+int MSG_MESH_CREATE(MSG_CTX ctx, int n_nodes, const double* xyz, int n_elems, const int* conn, const int* dof,
+                    int n_dofs, MSG_MESH* out) {
+  CTX_GUARD(ctx);
+  Mesh* m = nullptr;
+  MSG_TRY(create_mesh(ctx, n_nodes, xyz, n_elems, conn, dof, n_dofs, &m));
+  *out = static_cast<msg_mesh*>(m);
+  return MSG_OK;
+}
+
+int MSG_MESH_INFO(MSG_MESH m, int64_t* info) {
+  if (!m || !info) return MSG_ERR_INVALID_ARGUMENT;
+  info[0] = m->structured; info[1] = m->nx; info[2] = m->ny; info[3] = m->nz;
+  info[4] = m->n_dofs; info[5] = m->pat.n_rows; info[6] = m->pat.nnzb; info[7] = m->n_elems;
+  return MSG_OK;
+}
+
+int MSG_MESH_DESTROY(MSG_MESH m) {
+  if (!m) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  delete m;
+  return MSG_OK;
+}
+
+int MSG_ASSEMBLE_BSR(MSG_MESH m, const double* E, double nu, MSG_MAT* out) {
+  if (!m || !E || !out) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  if (!(nu > -1.0 && nu < 0.5)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Poisson ratio out of (-1, 0.5)");
+  std::unique_ptr<msg_matrix> A(new msg_matrix());
+  A->mesh = m;
+  DevMem dE, ke, st;
+  MSG_TRY(upload(ctx, dE, E, (size_t)m->n_elems));
+  int neg = 0;
+  MSG_TRY(assemble_from_device_E(ctx, m, dE.as<double>(), nu, A.get(), ke, st, &neg));
+  if (neg != 0) return set_error(ctx, neg, "negative or tiny Jacobian determinant (H8)");
+  *out = A.release();
+  return MSG_OK;
+}
+
+int MSG_ASSEMBLE_BSR_KE(MSG_MESH m, const double* Ke, MSG_MAT* out) {
+  if (!m || !Ke || !out) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  std::unique_ptr<msg_matrix> A(new msg_matrix());
+  A->mesh = m;
+  DevMem dK;
+  MSG_TRY(upload(ctx, dK, Ke, 300 * (size_t)m->n_elems));
+  MSG_TRY(assemble_from_device_ke(ctx, m, dK.as<double>(), A.get()));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *out = A.release();
+  return MSG_OK;
+}
+
+int MSG_MAT_MULTIPLY(MSG_MAT A, const double* x, double* y) {
+  if (!A || !x || !y) return MSG_ERR_INVALID_ARGUMENT;
+  Mesh* m = A->mesh;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  const size_t n3 = 3 * (size_t)m->n_nodes;
+  DevMem dxd, dxn, dyn, dyd;
+  MSG_TRY(upload(ctx, dxd, x, (size_t)m->n_dofs));
+  MSG_TRY(dxn.alloc(ctx, sizeof(double) * n3));
+  MSG_TRY(dyn.alloc(ctx, sizeof(double) * n3));
+  MSG_TRY(dyd.alloc(ctx, sizeof(double) * std::max(1, m->n_dofs)));
+  MSG_CUDA(ctx, cudaMemsetAsync(dxn.ptr, 0, sizeof(double) * n3, ctx->stream));
+  MSG_TRY(launch_dof_to_node(ctx, m, dxd.as<double>(), dxn.as<double>(), 1, 0, 0));
+  MSG_TRY(launch_bsr_spmv(ctx, m, A->d_val.as<double>(), dxn.as<double>(), dyn.as<double>()));
+  MSG_TRY(launch_node_to_dof(ctx, m, dyn.as<double>(), dyd.as<double>(), 1, 0, 0));
+  MSG_CUDA(ctx, cudaMemcpyAsync(y, dyd.ptr, sizeof(double) * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MSG_OK;
+}
+
+int MSG_MAT_DIAGONAL(MSG_MAT A, double* diag) {
+  if (!A || !diag) return MSG_ERR_INVALID_ARGUMENT;
+  Mesh* m = A->mesh;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  std::vector<double> dinv(3 * (size_t)m->n_nodes);
+  MSG_CUDA(ctx, cudaMemcpyAsync(dinv.data(), A->d_dinv.ptr, sizeof(double) * dinv.size(), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < m->n_nodes; ++i)
+    for (int c = 0; c < 3; ++c) {
+      const int d = m->dof[3 * i + c];
+      if (d >= 0) diag[d] = 1.0 / dinv[3 * i + c];
+    }
+  return MSG_OK;
+}
+
+int MSG_MAT_DESTROY(MSG_MAT A) {
+  if (!A) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = A->mesh->ctx;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  delete A;
+  return MSG_OK;
+}
+
+int MSG_PCG_SOLVE(MSG_MAT A, const double* b, double* x, int max_it, double tol, int* iterations, double* rel_res) {
+  if (!A || !b || !x || max_it <= 0 || !(tol > 0)) return MSG_ERR_INVALID_ARGUMENT;
+  Mesh* m = A->mesh;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  const size_t n3 = 3 * (size_t)m->n_nodes;
+  DevMem dbd, dbn, dxn, dxd;
+  MSG_TRY(upload(ctx, dbd, b, (size_t)m->n_dofs));
+  MSG_TRY(dbn.alloc(ctx, sizeof(double) * n3));
+  MSG_TRY(dxn.alloc(ctx, sizeof(double) * n3));
+  MSG_TRY(dxd.alloc(ctx, sizeof(double) * std::max(1, m->n_dofs)));
+  MSG_CUDA(ctx, cudaMemsetAsync(dbn.ptr, 0, sizeof(double) * n3, ctx->stream));
+  MSG_TRY(launch_dof_to_node(ctx, m, dbd.as<double>(), dbn.as<double>(), 1, 0, 0));
+  int its = 0, st = 0;
+  double rr = 0;
+  MSG_TRY(pcg_solve_device(ctx, A, dbn.as<double>(), dxn.as<double>(), max_it, tol, &its, &rr, &st));
+  A->graph_x = nullptr;  // dxn is released on return; force a re-capture next time
+  if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
+  MSG_TRY(launch_node_to_dof(ctx, m, dxn.as<double>(), dxd.as<double>(), 1, 0, 0));
+  MSG_CUDA(ctx, cudaMemcpyAsync(x, dxd.ptr, sizeof(double) * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (iterations) *iterations = its;
+  if (rel_res) *rel_res = rr;
+  if (st != MSG_OK)
+    return set_error(ctx, st, st == MSG_ERR_BREAKDOWN ? "PCG breakdown (p.q <= 0 or NaN)" : "PCG did not converge");
+  return MSG_OK;
+}
+
+int MSG_KL_TABLE(const double* L, double l, int n_terms, int n1d, double* w3, double* amp3, int* idx3, double* eig) {
+  if (!L || !(l > 0) || n_terms <= 0 || n1d <= 0 || !w3 || !amp3 || !idx3 || !eig) return MSG_ERR_INVALID_ARGUMENT;
+  if ((int64_t)n1d * n1d * n1d < n_terms) return MSG_ERR_INVALID_ARGUMENT;
+  const double pi = 3.14159265358979323846;
+  const double c = 1.0 / l;
+  std::vector<double> w[3], a[3], lam[3];
+  for (int ax = 0; ax < 3; ++ax) {
+    if (!(L[ax] > 0)) return MSG_ERR_INVALID_ARGUMENT;
+    const double A = 0.5 * L[ax];
+    for (int k = 1; k <= n1d; ++k) {
+      const bool is_sin = (k % 2 == 0);
+      const int i = k / 2;
+      const double lo = is_sin ? (i - 0.5) * pi / A : i * pi / A;
+      const double hi = is_sin ? i * pi / A : (i + 0.5) * pi / A;
+      const double ww = kl_root(A, c, is_sin, lo, hi);
+      const double s = std::sin(2.0 * ww * A) / (2.0 * ww);
+      w[ax].push_back(ww);
+      lam[ax].push_back(2.0 * c / (ww * ww + c * c));
+      a[ax].push_back(1.0 / std::sqrt(is_sin ? A - s : A + s));
+    }
+  }
+  struct Term { int64_t key; int i, j, k; double e; };
+  std::vector<Term> t;
+  t.reserve((size_t)n1d * n1d * n1d);
+  const double emax = lam[0][0] * lam[1][0] * lam[2][0];
+  for (int i = 0; i < n1d; ++i)
+    for (int j = 0; j < n1d; ++j)
+      for (int k = 0; k < n1d; ++k) {
+        const double e = (lam[0][i] * lam[1][j]) * lam[2][k];
+        t.push_back({(int64_t)std::llround(e / emax * 1099511627776.0), i, j, k, e});  // 2^-40 quantised key
+      }
+  std::sort(t.begin(), t.end(), [](const Term& x, const Term& y) {
+    if (x.key != y.key) return x.key > y.key;
+    if (x.i != y.i) return x.i < y.i;
+    if (x.j != y.j) return x.j < y.j;
+    return x.k < y.k;
+  });
+  for (int q = 0; q < n_terms; ++q) {
+    const int id[3] = {t[q].i, t[q].j, t[q].k};
+    for (int ax = 0; ax < 3; ++ax) {
+      w3[3 * q + ax] = w[ax][id[ax]];
+      amp3[3 * q + ax] = a[ax][id[ax]];
+      idx3[3 * q + ax] = id[ax] + 1;
+    }
+    eig[q] = t[q].e;
+  }
+  return MSG_OK;
+}
+
+int MSG_KL_FIELD(MSG_MESH m, const MSG_KL* kl, int R, const double* xi, double* E) {
+  if (!m || !kl || R <= 0 || !xi || !E) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, m, kl, &kd));
+  const int Rp = (R + 31) / 32 * 32;
+  DevMem dxi, dE;
+  MSG_TRY(upload(ctx, dxi, xi, (size_t)R * kl->n_terms));
+  MSG_TRY(dE.alloc(ctx, sizeof(double) * (size_t)R * m->n_elems));
+  MSG_TRY(launch_kl_field(ctx, m, &kd, R, Rp, dxi.as<double>(), nullptr, nullptr, dE.as<double>()));
+  MSG_CUDA(ctx, cudaMemcpyAsync(E, dE.ptr, sizeof(double) * (size_t)R * m->n_elems, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MSG_OK;
+}
+
+int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH m, double nu, const MSG_KL* kl, int R, const double* xi_dev, const double* b_dev,
+                              int mode, int max_it, double tol, int tip_dof, double* X_dev, double* tip,
+                              int* iterations, double* rel_res) {
+  if (!m) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  return mc_batch(ctx, m, nu, kl, R, xi_dev, b_dev, mode, max_it, tol, tip_dof, X_dev, tip, iterations, rel_res);
+}
+
+int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const double* xi, const double* b, int mode,
+                       int max_it, double tol, int tip_dof, double* X, double* tip, int* iterations, double* rel_res) {
+  if (!m || !kl || !xi || !b || R <= 0) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  DevMem dxi, db, dX;
+  MSG_TRY(upload(ctx, dxi, xi, (size_t)R * kl->n_terms));
+  MSG_TRY(upload(ctx, db, b, (size_t)m->n_dofs));
+  if (X) MSG_TRY(dX.alloc(ctx, sizeof(double) * (size_t)R * m->n_dofs));
+  int st = mc_batch(ctx, m, nu, kl, R, dxi.as<double>(), db.as<double>(), mode, max_it, tol, tip_dof,
+                    X ? dX.as<double>() : nullptr, tip, iterations, rel_res);
+  if (X && (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED)) {
+    MSG_CUDA(ctx, cudaMemcpyAsync(X, dX.ptr, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+// Internal declarations shared by the host runtime (msg_api.cpp) and the
+// CUDA kernels (*.cu) of libmsolve_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "msolve_gpu.h"
+
+namespace msg {
+
+// Packed row-wise upper index of a 24x24 symmetric matrix (SymmetricMatrix2D.IndexOf).
+__host__ __device__ inline int packed_index(int i, int j) {
+  int r = i < j ? i : j, c = i < j ? j : i;
+  return r * (47 - r) / 2 + c;
+}
+
+// Hexa8 local corner numbering of (ax, ay, az) in {0,1}^3 (rElHexa8.f90:43-68).
+__host__ __device__ constexpr int corner_id(int ax, int ay, int az) {
+  return az * 4 + (ay ? (ax ? 2 : 3) : (ax ? 1 : 0));
+}
+
+struct Context;
+
+// Device allocation charged against the context's memory budget.
+struct DevMem {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  Context* ctx = nullptr;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem();
+  int alloc(Context* c, size_t n);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint64_t budget = 0;           // 0 = unlimited
+  std::atomic<uint64_t> used{0};
+  std::recursive_mutex mu;
+  std::string last_error;
+  std::atomic<int64_t> launches{0};
+  double t_phase[5] = {0, 0, 0, 0, 0};
+  int sm_count = 148;
+  // mixed-solver tunables (MSG_SET_OPTION)
+  double inner_tol = 1e-4;   // inner FP32 PCG relative residual per refinement step
+  int inner_max = 100000;    // inner iterations per refinement step
+  int chunk = 16;            // inner iterations per captured graph launch
+};
+
+int set_error(Context* ctx, int code, const char* fmt, ...);
+int cuda_error(Context* ctx, cudaError_t e, const char* where);
+
+#define MSG_CUDA(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return ::msg::cuda_error((ctx), _e, #call); \
+  } while (0)
+
+#define MSG_TRY(call)            \
+  do {                           \
+    int _s = (call);             \
+    if (_s != MSG_OK) return _s; \
+  } while (0)
+
+// Kernels launched counter (the bench reports how many of this library's
+// kernels ran inside its timed region).
+inline void count_launch(Context* ctx, int n = 1) { ctx->launches += n; }
+
+// 3x3-block sliced-ELL (SELL-32) pattern of the global stiffness over all
+// mesh nodes. Block row = node. Slices of 32 rows; slot s of slice z holds
+// one block column per row. Layouts: col[(slot_base + s)*32 + lane],
+// val[((slot_base + s)*9 + k)*32 + lane] with k = 3*row_comp + col_comp.
+struct BlockPattern {
+  int n_rows = 0;                       // nodes
+  int n_slices = 0;
+  int64_t n_slots = 0;                  // total slots (each 32 lanes)
+  int64_t nnzb = 0;                     // true blocks
+  std::vector<int64_t> slice_ptr;       // n_slices + 1, in slots
+  std::vector<int> col;                 // n_slots*32, -1 = padding
+  std::vector<int> diag_pos;            // per row: flat lane position of its diagonal block
+  // assembly contributions: per flat position, list of (e*64 + a*8 + b)
+  std::vector<int64_t> contrib_ptr;     // n_slots*32 + 1
+  std::vector<int> contrib;
+};
+
+struct Mesh {
+  Context* ctx = nullptr;
+  int n_nodes = 0, n_elems = 0, n_dofs = 0;
+  std::vector<double> xyz;   // [n_nodes][3]
+  std::vector<int> conn;     // [n_elems][8]
+  std::vector<int> dof;      // [n_nodes][3]
+  BlockPattern pat;
+  // structured cube lattice (generator order) -> matrix-free batched path
+  bool structured = false;
+  int nx = 0, ny = 0, nz = 0;
+  double h = 0, origin[3] = {0, 0, 0};
+  // device copies
+  DevMem d_exyz;       // [n_elems][24] element coordinates
+  DevMem d_dof;        // [n_nodes][3]
+  DevMem d_col, d_slice_ptr, d_contrib_ptr, d_contrib, d_diag_pos;
+  DevMem d_mask;       // [n_nodes] uint8 bit c = component c constrained
+  DevMem d_centroid;   // [n_elems][3]
+  DevMem d_free_rows;  // [n_dofs] int: node*3+c for each free DOF (DOF -> node layout)
+};
+
+struct PcgState {
+  double zr, pq, rr, bnorm, alpha, beta, err;
+  int it, done, status, iterations, matvecs, max_it;
+  double tol;
+  unsigned int counter;
+  int pad;
+};
+
+struct Matrix {
+  Mesh* mesh = nullptr;
+  DevMem d_val;   // SELL values FP64
+  DevMem d_dinv;  // [n_nodes*3]
+  // PCG workspace (node layout, 3 per node)
+  DevMem d_r, d_p0, d_p1, d_q, d_partial, d_state, d_tmp, d_tmp2;
+  cudaGraphExec_t graph = nullptr;
+  int graph_chunk = 0;
+  const void* graph_x = nullptr;  // output vector the captured graph writes (not owned)
+  ~Matrix();
+};
+
+// ---------------------------------------------------------------- kernel launchers (kernels_*.cu)
+int launch_h8_ke(Context* ctx, int n, const double* d_xyz, const double* d_E, double E_scalar, double nu,
+                 double* d_K, int* d_status);
+int launch_h8_me(Context* ctx, int n, const double* d_xyz, double rho, double* d_M, int* d_status);
+int launch_bsr_assemble(Context* ctx, const Mesh* m, const double* d_Ke, double* d_val);
+int launch_bsr_diag_inv(Context* ctx, const Mesh* m, const double* d_val, double* d_dinv);
+int launch_bsr_spmv(Context* ctx, const Mesh* m, const double* d_val, const double* d_x, double* d_y);
+int launch_dof_to_node(Context* ctx, const Mesh* m, const double* d_in, double* d_out, int n_vec, int64_t in_stride,
+                       int64_t out_stride);
+int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* d_out, int n_vec, int64_t in_stride,
+                       int64_t out_stride);
+int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b_node, double* d_x_node, int max_it, double tol,
+                     int* iterations, double* rel_res, int* status);
+
+// KL field: E64/E32 [n_elems][Rp] (realization innermost) and/or E64 [R][n_elems].
+struct KLDevice {
+  int n_terms = 0;
+  DevMem d_psi;   // [K][n_elems]
+  double mu = 0;
+};
+int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out);
+int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int Rp, const double* d_xi,
+                    double* d_E64_er, float* d_E32_er, double* d_E64_re);
+
+// batched mixed-precision solve on a structured lattice (kernels_block.cu)
+struct BatchOut {
+  double* tip = nullptr;
+  int* iterations = nullptr;
+  double* rel_res = nullptr;
+};
+int block_mixed_solve(Context* ctx, Mesh* m, double nu, const double* d_E64_er, const float* d_E32_er, int R,
+                      int Rp, const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
+
+// Element stiffness of one cube of side h at E=1 (host, via the K1 kernel): K[24][24] full.
+int unit_cube_khat(Context* ctx, double h, double nu, double* K576);
+
+}  // namespace msg
+
+struct msg_context : msg::Context {};
+struct msg_mesh : msg::Mesh {};
+struct msg_matrix : msg::Matrix {};

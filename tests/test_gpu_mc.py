@@ -1,0 +1,122 @@
+"""GPU parity of the Monte Carlo path: KL field, the plain FP64 drop-in
+(realization by realization, assembled BSR + Jacobi-PCG) and the batched
+mixed-precision matrix-free solve, against per-realization FP64 oracle solves.
+
+Tolerances: E field 1e-13 relative; FP64 drop-in displacements 1e-10 relative
+to the oracle at the same stopping rule; mixed-precision displacements 1e-8
+relative (max-norm) to an FP64 oracle solve converged to 1e-13."""
+import numpy as np
+import pytest
+
+import msolve_b200 as M
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(n, R, seed=1, n_terms=20):
+    model = M.clamped_block_model(n)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, n_terms, 8)
+    xi = np.random.default_rng(seed).standard_normal((R, n_terms))
+    return model, kl, xi
+
+
+def oracle_fields(model, kl, xi, n):
+    cen = O.centroids(model.xyz, model.conn)
+    return O.kl_field(cen, [n, n, n], kl.table(), xi, mean=kl.mean, sigma=kl.sigma,
+                      mean_correction=kl.mean_correction)
+
+
+def oracle_solve(model, n, E, tol=1e-13):
+    cons = (model.dof < 0).astype(np.uint8)
+    x, info = O.block_solve_pcg(n, n, n, cons, E, model.poisson, model.subdomains[0].RHS, tol=tol, max_it=100000)
+    assert info["status"] == 0
+    return x, info
+
+
+def test_kl_field_matches_oracle(ctx):
+    for mc in (False, True):
+        model, kl, xi = setup(8, 70, n_terms=30)
+        kl.mean_correction = mc
+        mesh = M.GpuMesh(ctx, model)
+        E = kl.field(mesh, xi)
+        Eo = oracle_fields(model, kl, xi, 8)
+        assert np.abs(E - Eo).max() <= 1e-13 * np.abs(Eo).max()
+
+
+def test_fp64_dropin_matches_oracle_pcg(ctx):
+    n, R = 6, 3
+    model, kl, xi = setup(n, R)
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R, mode="fp64",
+                                                    tolerance=1e-8)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    E = oracle_fields(model, kl, xi, n)
+    for r in range(R):
+        xo, info = oracle_solve(model, n, E[r], tol=1e-8)
+        assert abs(mc.Iterations[r] - info["iterations"] - 1) <= 1
+        assert np.abs(mc.Solutions[r] - xo).max() <= 1e-10 * np.abs(xo).max()
+        assert mc.TipValues[r] == mc.Solutions[r][mc.tip_dof]
+
+
+@pytest.mark.parametrize("n,R", [(4, 5), (8, 40), (12, 64)])
+def test_mixed_batched_matches_fp64_oracle(ctx, n, R):
+    model, kl, xi = setup(n, R, seed=n)
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R, mode="mixed",
+                                                    tolerance=1e-10)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    assert (mc.Residuals < 1e-10).all()
+    E = oracle_fields(model, kl, xi, n)
+    for r in sorted({0, R // 2, R - 1}):
+        xo, _ = oracle_solve(model, n, E[r])
+        err = np.abs(mc.Solutions[r] - xo).max() / np.abs(xo).max()
+        assert err <= 1e-8, (r, err)
+        # residual reported by the GPU is the FP64 true residual of the returned x
+        C = O.CSR(model.n_nodes, model.conn, model.dof, model.n_dofs)
+        C.assemble(O.h8_stiffness_batch(model.element_xyz(), E[r], 0.3)[0])
+        b = model.subdomains[0].RHS
+        rr = np.linalg.norm(b - C.multiply(mc.Solutions[r])) / np.linalg.norm(b)
+        assert abs(rr - mc.Residuals[r]) <= 1e-3 * mc.Residuals[r] + 1e-15
+
+
+def test_mixed_result_is_independent_of_the_batch(ctx):
+    """A realization solved alone and inside a batch gives the same answer
+    (realization-innermost layout: no cross-realization arithmetic)."""
+    n, R = 6, 33
+    model, kl, xi = setup(n, R, seed=3)
+    runs = []
+    for rows in (slice(0, R), slice(5, 6)):
+        mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20,
+                                                        simulations=xi[rows].shape[0], mode="mixed", tolerance=1e-10)
+        mc.RandomNumbers = xi[rows]
+        mc.Solve()
+        runs.append(mc)
+    a, b = runs[0].Solutions[5], runs[1].Solutions[0]
+    assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
+
+
+def test_mixed_needs_structured_mesh(ctx):
+    model = M.clamped_block_model(3)
+    model.xyz[5] += 0.01  # break the lattice
+    kl = M.LognormalStochasticCoefficientsProvider([3, 3, 3], 0.6, 5, 4)
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=5, simulations=2, mode="mixed")
+    with pytest.raises(M.InvalidOperationError) as e:
+        mc.Solve()
+    assert e.value.code == -2007
+
+
+def test_mixed_32cube_sample_against_oracle(ctx):
+    """Config 3 geometry (32^3, 50-term KL, l = 6.4, sigma = 0.3), a 64-realization batch."""
+    n, R = 32, 64
+    model, kl, xi = setup(n, R, seed=2024, n_terms=50)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, 50, 16)
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=50, simulations=R, mode="mixed",
+                                                    tolerance=1e-10)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    assert (mc.Residuals < 1e-10).all()
+    E = oracle_fields(model, kl, xi, n)
+    xo, _ = oracle_solve(model, n, E[7], tol=1e-12)
+    err = np.abs(mc.Solutions[7] - xo).max() / np.abs(xo).max()
+    assert err <= 1e-8, err
