@@ -1,0 +1,371 @@
+"""Benchmark: batched mixed-precision Monte Carlo Hexa8 solves on B200.
+
+Workload (one step): a batch of R realizations (default 1024) of a 32^3 Hexa8
+block of unit cubes (35,937 nodes, 104,544 free DOFs), z=0 face clamped,
+unit pressure on the top face (consistent weights), E_e = exp(sigma g(x_e))
+with a 50-term separable-exponential KL field (l = 0.2 * 32, sigma = 0.3),
+nu = 0.3, every realization solved to an FP64 true relative residual < tol
+(default 1e-10: the measured displacement error against an FP64 solve is then
+below 1e-8) with the matrix-free FP32 PCG + FP64 refinement path. Each step
+draws a fresh xi table (seeded); state is ~4.6 GB per GPU, larger than L2.
+
+value  = realizations solved per second with xi / b / X resident in HBM
+         (MSG_MC_SOLVE_BATCH_DEVICE), all ranks summed (weak scaling).
+e2e    = the same through MSG_MC_SOLVE_BATCH with host (pinned) buffers: xi and
+         b copied in, every realization's full displacement field copied out.
+fp64_dropin = the plain FP64 drop-in (assembled BSR + Jacobi PCG, one
+         realization after another, MSG_MODE_FP64_BSR) on a sample of the batch.
+roofline = the matrix-free operator kernel (k_inner_op), live per-launch CUDA
+         event durations inside the timed region.
+cpu_baseline = the oracle (C++ FP64 restatement of the reference: assembled
+         CSR Jacobi-PCG per realization) on the host cores, a bounded sample.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: torchrun --nproc-per-node N bench.py --gpus N (one rank per GPU,
+realization batches sharded across ranks, one all-reduce of the tip statistics).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p99 latency"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=32)
+    p.add_argument("--R", type=int, default=1024)
+    p.add_argument("--terms", type=int, default=50)
+    p.add_argument("--tol", type=float, default=1e-10)
+    p.add_argument("--fp64-sample", type=int, default=8)
+    p.add_argument("--cpu-sample", type=int, default=2)
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu, self.proc, self.path = gpu, None, None
+
+    def start(self):
+        self.path = f"/tmp/msg_clocks_{os.getpid()}.csv"
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 8:
+                try:
+                    rows.append((float(f[0]), float(f[1]), f[4], f[5], f[6], f[7]))
+                except ValueError:
+                    pass
+        if not rows:
+            return None
+        sm = [r[0] for r in rows]
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": float(rows[0][1]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def make_problem(args):
+    import msolve_b200 as M
+    model = M.clamped_block_model(args.n)
+    kl = M.LognormalStochasticCoefficientsProvider([args.n] * 3, 0.2 * args.n, args.terms, 16)
+    return model, kl
+
+
+def cpu_baseline(args, model, kl, xi_host):
+    """Oracle (the restated reference) on the host cores: per-realization FP64
+    assembly + Jacobi-PCG to the same tolerance, a bounded sample."""
+    import oracle as O
+    n = args.n
+    cen = O.centroids(model.xyz, model.conn)
+    E = O.kl_field(cen, [n] * 3, kl.table(), xi_host[: args.cpu_sample], sigma=kl.sigma)
+    cons = (model.dof < 0).astype(np.uint8)
+    t0 = time.perf_counter()
+    its = []
+    for r in range(args.cpu_sample):
+        x, info = O.block_solve_pcg(n, n, n, cons, E[r], model.poisson, model.subdomains[0].RHS, tol=args.tol,
+                                    max_it=100000)
+        its.append(info["iterations"])
+    dt = time.perf_counter() - t0
+    return {"value": args.cpu_sample / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{args.cpu_sample} realizations of the {n}^3 block, FP64 CSR Jacobi-PCG to tol {args.tol:g} "
+                      f"(mean {np.mean(its):.0f} iterations), {dt:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    import oracle as O
+    model, kl = make_problem(args)
+    rng = np.random.default_rng(99)
+    n = args.n
+    cen = O.centroids(model.xyz, model.conn)
+    cons = (model.dof < 0).astype(np.uint8)
+    times = []
+    for s in range(args.warmup + args.steps):
+        xi = rng.standard_normal((1, args.terms))
+        t0 = time.perf_counter()
+        E = O.kl_field(cen, [n] * 3, kl.table(), xi, sigma=kl.sigma)
+        O.block_solve_pcg(n, n, n, cons, E[0], model.poisson, model.subdomains[0].RHS, tol=args.tol, max_it=100000)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    T = float(np.sum(times))
+    v = args.steps / T
+    line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"Monte Carlo Hexa8 {n}^3 block, 1 realization per step (bounded CPU sample of the "
+                                   f"{args.R}-realization batch), 50-term KL, sigma 0.3, tol {args.tol:g}"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{args.steps} realizations, one per step"},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "latency_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "p99": 1e3 * float(np.percentile(times, 99))}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import msolve_b200 as M
+    from msolve_b200 import _native as N
+
+    ctx = M.Context(local)
+    model, kl = make_problem(args)
+    mesh = M.GpuMesh(ctx, model)
+    R, K_terms = args.R, args.terms
+    Nd = model.n_dofs
+    tip = M.tip_dof(model)
+    dev = torch.device("cuda", local)
+    steps_total = args.warmup + args.steps
+    g = torch.Generator(device="cpu").manual_seed(1000 + rank)
+    xi_all = torch.randn(steps_total + 1, R, K_terms, generator=g, dtype=torch.float64)
+    xi_dev = xi_all.to(dev)
+    b_dev = torch.from_numpy(model.subdomains[0].RHS).to(dev)
+    X_dev = torch.empty(R, Nd, dtype=torch.float64, device=dev)
+    kls = kl.struct()
+    tip_h = np.zeros(R)
+    its_h = np.zeros(R, dtype=np.int32)
+    res_h = np.zeros(R)
+    L = N.lib()
+
+    def solve_device(step, mode=N.MSG_MODE_MIXED_BATCHED, count=R):
+        st = L.MSG_MC_SOLVE_BATCH_DEVICE(mesh.handle, model.poisson, C.byref(kls), count,
+                                         C.c_void_p(xi_dev[step].data_ptr()), C.c_void_p(b_dev.data_ptr()), mode,
+                                         200000, args.tol, tip, C.c_void_p(X_dev.data_ptr()), N.ptr(tip_h),
+                                         N.ptr(its_h, N._i), N.ptr(res_h))
+        N.check(st, ctx.handle, "MSG_MC_SOLVE_BATCH_DEVICE")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for s in range(args.warmup):
+        solve_device(s)
+    barrier()
+    ctx.reset_stats()
+    launches0 = ctx.stats()["launches"]
+    clocks = Clocks(local)
+    clocks.start()
+    lat, iters, resmax = [], [], []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record()
+    for s in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        solve_device(args.warmup + s)
+        b.record()
+        b.synchronize()
+        lat.append(a.elapsed_time(b))
+        iters.append(its_h[:R].copy())
+        resmax.append(float(res_h[:R].max()))
+    e1.record()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    st = ctx.stats()
+    launches = st["launches"] - launches0
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = ws * R * args.steps / (ms_max / 1e3)
+
+    # Monte Carlo statistics of the last step: one all-reduce of (sum u, sum u^2, count)
+    stats_t = torch.tensor([tip_h[:R].sum(), (tip_h[:R] ** 2).sum(), R], dtype=torch.float64, device=dev)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(stats_t)
+    su, su2, cnt = stats_t.tolist()
+    tip_mean = su / cnt
+    tip_var = (su2 - cnt * tip_mean ** 2) / max(cnt - 1, 1)
+
+    # roofline of the matrix-free operator (live samples from the timed region)
+    op_ms = st["op_launch_ms"]
+    nn = model.n_nodes
+    ne = model.n_elems
+    Rp = (R + 31) // 32 * 32
+    # algorithmic bytes of one operator launch: read r, p_old (3 per node), dinv (1 per node), E (1 per
+    # element); write p_new, q (3 per node); FP32, realization-innermost, each once
+    op_bytes = 4.0 * Rp * (3 * nn * 4 + nn + ne)
+    hbm, peak_kind = load_peaks()
+    achieved = op_bytes / (op_ms / 1e3) / 1e9 if op_ms > 0 else 0.0
+
+    line = None
+    if rank == 0:
+        # e2e through the host-buffer entry point (pinned buffers)
+        xi_h = torch.empty(R, K_terms, dtype=torch.float64).pin_memory()
+        b_h = torch.from_numpy(model.subdomains[0].RHS.copy()).pin_memory()
+        X_h = torch.empty(R, Nd, dtype=torch.float64).pin_memory()
+        e2e_lat = []
+        for s in range(2):
+            xi_h.copy_(xi_all[steps_total])
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            stt = L.MSG_MC_SOLVE_BATCH(mesh.handle, model.poisson, C.byref(kls), R,
+                                       C.cast(C.c_void_p(xi_h.data_ptr()), N._d), C.cast(C.c_void_p(b_h.data_ptr()), N._d),
+                                       N.MSG_MODE_MIXED_BATCHED, 200000, args.tol, tip,
+                                       C.cast(C.c_void_p(X_h.data_ptr()), N._d), N.ptr(tip_h), N.ptr(its_h, N._i),
+                                       N.ptr(res_h))
+            b.record()
+            b.synchronize()
+            N.check(stt, ctx.handle, "MSG_MC_SOLVE_BATCH")
+            if s > 0:
+                e2e_lat.append(a.elapsed_time(b))
+        e2e_value = R / (np.mean(e2e_lat) / 1e3)
+        # accuracy sample: mixed vs the FP64 drop-in converged tighter
+        X_mixed = X_dev[:2].clone()
+        st64 = L.MSG_MC_SOLVE_BATCH_DEVICE(mesh.handle, model.poisson, C.byref(kls), 2,
+                                           C.c_void_p(xi_dev[steps_total - 1].data_ptr()), C.c_void_p(b_dev.data_ptr()),
+                                           N.MSG_MODE_FP64_BSR, 200000, 1e-12, tip, C.c_void_p(X_dev.data_ptr()),
+                                           N.ptr(tip_h), N.ptr(its_h, N._i), N.ptr(res_h))
+        N.check(st64, ctx.handle, "FP64 reference solve")
+        ref = X_dev[:2]
+        rel_err = float(((X_mixed - ref).abs().amax(dim=1) / ref.abs().amax(dim=1)).max().item())
+        # plain FP64 drop-in throughput on a sample of the batch (same tolerance, reference stopping rule)
+        k = args.fp64_sample
+        solve_device(0, N.MSG_MODE_FP64_BSR, 1)  # warm
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        solve_device(0, N.MSG_MODE_FP64_BSR, k)
+        b.record()
+        b.synchronize()
+        fp64_rate = k / (a.elapsed_time(b) / 1e3)
+        fp64_its = float(np.mean(its_h[:k]))
+        cpu = None
+        if not args.no_cpu and ws == 1:
+            cpu = cpu_baseline(args, model, kl, xi_all[0].numpy())
+        its_all = np.concatenate(iters)
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"batched Monte Carlo, {R} realizations x {args.n}^3 Hexa8 per GPU per step "
+                                   f"(z=0 clamped, unit top pressure, 50-term KL lognormal E, sigma 0.3, l 0.2*side, "
+                                   f"nu 0.3), mixed FP32 matrix-free PCG + FP64 refinement to FP64 true residual "
+                                   f"< {args.tol:g}",
+                       "realizations_per_gpu": R, "mesh": f"{args.n}x{args.n}x{args.n}", "free_dofs": Nd,
+                       "kl_terms": K_terms, "tol_true_residual": args.tol,
+                       "l2": "inputs larger than L2 (per-GPU batch state ~4.6 GB)", "parallelism": f"realizations x{ws}"},
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(R * K_terms * 8 + Nd * 8),
+                    "d2h_bytes_per_step": int(R * Nd * 8 + R * (8 + 4 + 8))},
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": "k_inner_op (matrix-free FP32 operator)", "bound": "hbm", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if hbm else None, "traffic": None,
+                         "peak_kind": peak_kind, "launch_ms": op_ms, "bytes_per_launch": op_bytes,
+                         "update_launch_ms": st["update_launch_ms"], "samples": st["launch_samples"]},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "iterations": {"mean": float(its_all.mean()), "max": int(its_all.max())},
+            "max_true_rel_residual": max(resmax),
+            "rel_err_vs_fp64": rel_err,
+            "fp64_dropin": {"solves_per_s": fp64_rate, "sample": k, "mean_iterations": fp64_its,
+                            "note": "assembled BSR FP64 Jacobi-PCG, one realization after another, tol on the "
+                                    "recursive residual as the reference"},
+            "mixed_over_fp64": value / ws / fp64_rate,
+            "tip_uz": {"mean": tip_mean, "variance": tip_var, "realizations": int(cnt)},
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

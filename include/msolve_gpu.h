@@ -182,9 +182,17 @@ int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R,
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 
 /* Kernel launch counter of this context (kernels launched since creation),
- * and per-phase device timings of the last MC batch in ms:
- * t[0]=field, t[1]=inner operator, t[2]=inner update, t[3]=FP64 residual, t[4]=total. */
-int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t5);
+ * and device timings in ms (t8 may be NULL):
+ * t[0]=KL field, t[1]=inner FP32 loop, t[2]=unused, t[3]=FP64 residual steps,
+ * t[4]=whole last MC batch (last call); t[5]=mean duration of one
+ * matrix-free operator launch, t[6]=mean duration of one inner update launch,
+ * t[7]=number of samples behind t[5..6] (one per inner graph launch, CUDA
+ * events captured around the first operator/update of each launch, accumulated
+ * since the context was created or MSG_STATS_RESET). No reference counterpart
+ * (the reference writes stopwatch times to text files,
+ * MonteCarloAnalyzerWithStochasticMaterial.cs:244-292). */
+int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t8);
+int MSG_STATS_RESET(MSG_CTX ctx);
 
 #ifdef __cplusplus
 }

@@ -76,6 +76,7 @@ SIGNATURES = {
                                             C.c_int, C.c_double, C.c_int, _vp, _d, _i, _d]),
     "MSG_SET_OPTION": (C.c_int, [_vp, C.c_char_p, C.c_double]),
     "MSG_STATS": (C.c_int, [_vp, _i64, _d]),
+    "MSG_STATS_RESET": (C.c_int, [_vp]),
 }
 
 _lib = None
@@ -168,7 +169,10 @@ class Context:
 
     def stats(self):
         n = C.c_int64(0)
-        t = np.zeros(5)
+        t = np.zeros(8)
         lib().MSG_STATS(self.handle, C.byref(n), ptr(t))
-        return dict(launches=n.value, t_field_ms=t[0], t_inner_ms=t[1], t_update_ms=t[2], t_resid_ms=t[3],
-                    t_total_ms=t[4])
+        return dict(launches=n.value, t_field_ms=t[0], t_inner_ms=t[1], t_resid_ms=t[3], t_total_ms=t[4],
+                    op_launch_ms=t[5], update_launch_ms=t[6], launch_samples=int(t[7]))
+
+    def reset_stats(self):
+        lib().MSG_STATS_RESET(self.handle)

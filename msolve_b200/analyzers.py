@@ -31,7 +31,7 @@ class GpuMatrix:
     """Assembled FP64 global stiffness on the device (IMatrix2D analogue)."""
 
     def __init__(self, mesh, handle):
-        self.mesh, self.handle = mesh, handle
+        self.mesh, self.handle = mesh, handle  # keeps the mesh (and its context) alive
 
     def Multiply(self, x):
         x = N.f64(x)

@@ -352,11 +352,37 @@ struct Scal {
   int* n_active;  // [1]
 };
 
-__global__ void k_alpha(int Rp, int n_tiles, const double* __restrict__ partial, Scal s) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= Rp) return;
-  double pq = 0;
-  for (int t = 0; t < n_tiles; ++t) pq += partial[(size_t)t * Rp + r];
+// Per-realization sum of NV interleaved partials over n rows, 32 realizations x
+// 32 row-groups per CTA; fixed summation order (row-group sequential, then the
+// 32 groups in order), so results are reproducible and independent of the batch.
+template <int NV>
+__device__ __forceinline__ void reduce_rows(const double* __restrict__ partial, int n, int Rp, double (&out)[NV]) {
+  __shared__ double sh[32][NV][33];
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int r = blockIdx.x * 32 + lane;
+  double acc[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+  for (int t = g; t < n; t += 32)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] += partial[((size_t)t * Rp + r) * NV + q];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) sh[g][q][lane] = acc[q];
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = 0.0;
+    for (int gg = 0; gg < 32; ++gg) s += sh[gg][q][lane];
+    out[q] = s;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_alpha(int Rp, int n_tiles, const double* __restrict__ partial, Scal s) {
+  double v[1];
+  reduce_rows<1>(partial, n_tiles, Rp, v);
+  if (threadIdx.x >= 32) return;
+  const int r = blockIdx.x * 32 + threadIdx.x;
+  const double pq = v[0];
   float a = 0.f;
   if (s.act[r]) {
     if (!(pq > 0.0)) {
@@ -370,15 +396,14 @@ __global__ void k_alpha(int Rp, int n_tiles, const double* __restrict__ partial,
   s.alpha[r] = a;
 }
 
-__global__ void k_beta(int Rp, int n_blk, const double* __restrict__ partial, Scal s, double eta2, int inner_max) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(1024) k_beta(int Rp, int n_blk, const double* __restrict__ partial, Scal s,
+                                               double eta2, int inner_max) {
+  double v[2];
+  reduce_rows<2>(partial, n_blk, Rp, v);
+  const int r = blockIdx.x * 32 + threadIdx.x;
   int active = 0;
-  if (r < Rp) {
-    double g = 0, rho = 0;
-    for (int t = 0; t < n_blk; ++t) {
-      g += partial[((size_t)t * Rp + r) * 2];
-      rho += partial[((size_t)t * Rp + r) * 2 + 1];
-    }
+  if (threadIdx.x < 32) {
+    const double g = v[0], rho = v[1];
     float b = 0.f;
     if (s.act[r]) {
       if (rho <= eta2 * s.rho0[r] || s.its_step[r] >= inner_max || !(rho == rho)) {
@@ -395,15 +420,14 @@ __global__ void k_beta(int Rp, int n_blk, const double* __restrict__ partial, Sc
   if (threadIdx.x == 0 && active) atomicAdd(s.n_active, active);
 }
 
-__global__ void k_resid_scalars(int Rp, int n_tiles, const double* __restrict__ partial, Scal s, double tol) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, const double* __restrict__ partial,
+                                                        Scal s, double tol) {
+  double v[2];
+  reduce_rows<2>(partial, n_tiles, Rp, v);
+  const int r = blockIdx.x * 32 + threadIdx.x;
   int active = 0;
-  if (r < Rp) {
-    double rr = 0, g = 0;
-    for (int t = 0; t < n_tiles; ++t) {
-      rr += partial[((size_t)t * Rp + r) * 2];
-      g += partial[((size_t)t * Rp + r) * 2 + 1];
-    }
+  if (threadIdx.x < 32) {
+    const double rr = v[0], g = v[1];
     const double bn = s.bnorm[r];
     const double rel = bn > 0 ? sqrt(rr) / bn : 0.0;
     s.res[r] = rel;
@@ -530,9 +554,9 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const double* d_E64, con
   const int Q = Rp / 4;
   const int G = Q >= 256 ? 1 : 256 / Q;
   const size_t upd_smem = G > 1 ? sizeof(double) * (size_t)G * Q * 8 : 0;
-  const int sblocks = (Rp + 127) / 128;
+  const int sblocks = Rp / 32;  // scalar kernels: 32 realizations x 32 row groups per CTA
 
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[8];  // 0-3 host-side phases, 4-7 captured around the first operator / update launch
   for (auto& e : ev) MSG_CUDA(ctx, cudaEventCreate(&e));
   float t_resid = 0.f, t_inner = 0.f;
 
@@ -544,13 +568,19 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const double* d_E64, con
     for (int it = 0; it < chunk; ++it) {
       float* pold = (it & 1) ? p1.as<float>() : p0.as<float>();
       float* pnew = (it & 1) ? p0.as<float>() : p1.as<float>();
+      // cudaEventRecordExternal: a real event-record node in the graph (plain
+      // records during capture only order streams)
+      if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
       k_inner_op<<<op_grid, op_block, 0, st>>>(L, KF, r32.as<float>(), pold, pnew, dinv.as<float>(), d_E32,
                                                m->d_mask.as<uint8_t>(), s.beta, q.as<float>(), part_op.as<double>());
-      k_alpha<<<sblocks, 128, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
+      if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
+      k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
+      if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
       k_update<<<n_upd, 256, upd_smem, st>>>(nn, Rp, s.alpha, pnew, q.as<float>(), d.as<float>(), r32.as<float>(),
                                              dinv.as<float>(), part_up.as<double>());
+      if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
       cudaMemsetAsync(s.n_active, 0, sizeof(int), st);
-      k_beta<<<sblocks, 128, 0, st>>>(Rp, n_upd, part_up.as<double>(), s, ctx->inner_tol * ctx->inner_tol, ctx->inner_max);
+      k_beta<<<sblocks, 1024, 0, st>>>(Rp, n_upd, part_up.as<double>(), s, ctx->inner_tol * ctx->inner_tol, ctx->inner_max);
     }
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (e != cudaSuccess) return cuda_error(ctx, e, "capture inner chunk");
@@ -571,7 +601,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const double* d_E64, con
     k_resid_op<<<op_grid, op_block, 0, st>>>(L, KD, xc->as<double>(), d.as<float>(), xn->as<double>(),
                                              blat.as<double>(), d_E64, m->d_mask.as<uint8_t>(), dinv.as<float>(),
                                              r32.as<float>(), part_op.as<double>());
-    k_resid_scalars<<<sblocks, 128, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol);
+    k_resid_scalars<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol);
     cudaEventRecord(ev[1], st);
     count_launch(ctx, 2);
     std::swap(xc, xn);
@@ -591,6 +621,14 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const double* d_E64, con
       total_inner += chunk;
       MSG_CUDA(ctx, cudaMemcpyAsync(h_active, s.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
       MSG_CUDA(ctx, cudaStreamSynchronize(st));
+      float op_ms = 0.f, up_ms = 0.f;
+      if (cudaEventElapsedTime(&op_ms, ev[4], ev[5]) == cudaSuccess &&
+          cudaEventElapsedTime(&up_ms, ev[6], ev[7]) == cudaSuccess) {
+        ctx->op_ms_sum += op_ms;
+        ctx->upd_ms_sum += up_ms;
+        ctx->op_samples += 1;
+      }
+      cudaGetLastError();
       if (*h_active == 0 || total_inner >= max_it) break;
     }
     cudaEventRecord(ev[3], st);

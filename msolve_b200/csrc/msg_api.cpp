@@ -62,6 +62,32 @@ Matrix::~Matrix() {
   if (graph) cudaGraphExecDestroy(graph);
 }
 
+void retain(Context* ctx) { ctx->refs++; }
+
+void release(Context* ctx) {
+  if (--ctx->refs == 0) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete static_cast<msg_context*>(ctx);
+  }
+}
+
+void retain(Mesh* m) { m->refs++; }
+
+void release(Mesh* m) {
+  if (--m->refs == 0) {
+    Context* ctx = m->ctx;
+    {
+      std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+      cudaSetDevice(ctx->device);
+      cudaStreamSynchronize(ctx->stream);
+      delete static_cast<msg_mesh*>(m);
+    }
+    release(ctx);
+  }
+}
+
 template <class T>
 static int upload(Context* ctx, DevMem& dst, const T* src, size_t n) {
   MSG_TRY(dst.alloc(ctx, sizeof(T) * n));
@@ -261,6 +287,7 @@ static int create_mesh(Context* ctx, int n_nodes, const double* xyz, int n_elems
   MSG_TRY(upload(ctx, m->d_contrib, P.contrib.data(), P.contrib.size()));
   MSG_TRY(upload(ctx, m->d_diag_pos, P.diag_pos.data(), P.diag_pos.size()));
   MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  retain(ctx);
   *out = m.release();
   return MSG_OK;
 }
@@ -424,10 +451,7 @@ int MSG_CREATE(int device, uint64_t mem_budget_bytes, MSG_CTX* out) {
 
 int MSG_DESTROY(MSG_CTX ctx) {
   if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  cudaStreamDestroy(ctx->stream);
-  delete ctx;
+  release(ctx);  // freed once the last mesh/matrix of this context is destroyed
   return MSG_OK;
 }
 
@@ -442,11 +466,23 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 
-int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t5) {
+int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t8) {
   if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
   if (launches) *launches = ctx->launches.load();
-  if (t5)
-    for (int i = 0; i < 5; ++i) t5[i] = ctx->t_phase[i];
+  if (t8) {
+    for (int i = 0; i < 5; ++i) t8[i] = ctx->t_phase[i];
+    const double n = (double)ctx->op_samples;
+    t8[5] = n > 0 ? ctx->op_ms_sum / n : 0.0;
+    t8[6] = n > 0 ? ctx->upd_ms_sum / n : 0.0;
+    t8[7] = n;
+  }
+  return MSG_OK;
+}
+
+int MSG_STATS_RESET(MSG_CTX ctx) {
+  if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
+  ctx->op_ms_sum = ctx->upd_ms_sum = 0;
+  ctx->op_samples = 0;
   return MSG_OK;
 }
 
@@ -506,11 +542,7 @@ int MSG_MESH_INFO(MSG_MESH m, int64_t* info) {
 
 int MSG_MESH_DESTROY(MSG_MESH m) {
   if (!m) return MSG_ERR_INVALID_ARGUMENT;
-  Context* ctx = m->ctx;
-  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  delete m;
+  release(static_cast<Mesh*>(m));
   return MSG_OK;
 }
 
@@ -526,6 +558,7 @@ int MSG_ASSEMBLE_BSR(MSG_MESH m, const double* E, double nu, MSG_MAT* out) {
   int neg = 0;
   MSG_TRY(assemble_from_device_E(ctx, m, dE.as<double>(), nu, A.get(), ke, st, &neg));
   if (neg != 0) return set_error(ctx, neg, "negative or tiny Jacobian determinant (H8)");
+  retain(static_cast<Mesh*>(m));
   *out = A.release();
   return MSG_OK;
 }
@@ -540,6 +573,7 @@ int MSG_ASSEMBLE_BSR_KE(MSG_MESH m, const double* Ke, MSG_MAT* out) {
   MSG_TRY(upload(ctx, dK, Ke, 300 * (size_t)m->n_elems));
   MSG_TRY(assemble_from_device_ke(ctx, m, dK.as<double>(), A.get()));
   MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  retain(static_cast<Mesh*>(m));
   *out = A.release();
   return MSG_OK;
 }
@@ -583,11 +617,15 @@ int MSG_MAT_DIAGONAL(MSG_MAT A, double* diag) {
 
 int MSG_MAT_DESTROY(MSG_MAT A) {
   if (!A) return MSG_ERR_INVALID_ARGUMENT;
-  Context* ctx = A->mesh->ctx;
-  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
-  cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  delete A;
+  Mesh* m = A->mesh;
+  Context* ctx = m->ctx;
+  {
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete A;
+  }
+  release(m);
   return MSG_OK;
 }
 

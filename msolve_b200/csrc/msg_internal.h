@@ -44,7 +44,12 @@ struct DevMem {
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Handles are reference counted: a mesh holds its context, a matrix holds its
+// mesh, so the caller may destroy them in any order (a garbage-collected host
+// such as .NET finalises in arbitrary order); the object is freed with its
+// last reference.
 struct Context {
+  std::atomic<int> refs{1};
   int device = 0;
   cudaStream_t stream = nullptr;
   uint64_t budget = 0;           // 0 = unlimited
@@ -53,12 +58,22 @@ struct Context {
   std::string last_error;
   std::atomic<int64_t> launches{0};
   double t_phase[5] = {0, 0, 0, 0, 0};
+  // live per-launch samples of the inner operator / update kernels (event
+  // records captured in the inner-loop graph): sum of ms and sample count
+  double op_ms_sum = 0, upd_ms_sum = 0;
+  int64_t op_samples = 0;
   int sm_count = 148;
   // mixed-solver tunables (MSG_SET_OPTION)
   double inner_tol = 1e-4;   // inner FP32 PCG relative residual per refinement step
   int inner_max = 100000;    // inner iterations per refinement step
   int chunk = 16;            // inner iterations per captured graph launch
 };
+
+void retain(Context* ctx);
+void release(Context* ctx);
+struct Mesh;
+void retain(Mesh* m);
+void release(Mesh* m);
 
 int set_error(Context* ctx, int code, const char* fmt, ...);
 int cuda_error(Context* ctx, cudaError_t e, const char* where);
@@ -97,6 +112,7 @@ struct BlockPattern {
 };
 
 struct Mesh {
+  std::atomic<int> refs{1};
   Context* ctx = nullptr;
   int n_nodes = 0, n_elems = 0, n_dofs = 0;
   std::vector<double> xyz;   // [n_nodes][3]

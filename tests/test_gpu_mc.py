@@ -45,18 +45,24 @@ def test_kl_field_matches_oracle(ctx):
 
 
 def test_fp64_dropin_matches_oracle_pcg(ctx):
+    """Same stopping rule -> same iteration count (+-1 from summation order);
+    tightly converged -> same displacements to 1e-10."""
     n, R = 6, 3
     model, kl, xi = setup(n, R)
-    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R, mode="fp64",
-                                                    tolerance=1e-8)
-    mc.RandomNumbers = xi
-    mc.Solve()
     E = oracle_fields(model, kl, xi, n)
-    for r in range(R):
-        xo, info = oracle_solve(model, n, E[r], tol=1e-8)
-        assert abs(mc.Iterations[r] - info["iterations"] - 1) <= 1
-        assert np.abs(mc.Solutions[r] - xo).max() <= 1e-10 * np.abs(xo).max()
-        assert mc.TipValues[r] == mc.Solutions[r][mc.tip_dof]
+    for tol in (1e-8, 1e-12):
+        mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R,
+                                                        mode="fp64", tolerance=tol)
+        mc.RandomNumbers = xi
+        mc.Solve()
+        for r in range(R):
+            xo, info = oracle_solve(model, n, E[r], tol=tol)
+            assert abs(mc.Iterations[r] - info["iterations"] - 1) <= 1
+            assert mc.TipValues[r] == mc.Solutions[r][mc.tip_dof]
+            if tol == 1e-12:
+                assert np.abs(mc.Solutions[r] - xo).max() <= 1e-10 * np.abs(xo).max()
+            else:
+                assert np.abs(mc.Solutions[r] - xo).max() <= 1e-6 * np.abs(xo).max()
 
 
 @pytest.mark.parametrize("n,R", [(4, 5), (8, 40), (12, 64)])
