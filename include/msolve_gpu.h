@@ -176,9 +176,10 @@ int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R,
                               const double* b_dev, int mode, int max_it, double tol, int tip_dof, double* X_dev,
                               double* tip, int* iterations, double* rel_res);
 
-/* Tunables of the mixed solver on this context: "inner_tol" (relative residual
- * of each inner FP32 solve, default 1e-4), "inner_max" (inner iterations per
- * refinement step), "chunk" (inner iterations per CUDA-graph launch, even). */
+/* Tunables of the mixed solver on this context: "reliable_delta" (the FP32
+ * recursive residual may fall by this factor before it is replaced by the FP64
+ * true residual, default 0.1), "chunk" (FP32 iterations per CUDA-graph launch,
+ * even, default 16). */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 
 /* Kernel launch counter of this context (kernels launched since creation),

@@ -103,6 +103,32 @@ __global__ void __launch_bounds__(kSpmvThreads) k_bsr_spmv(int n_rows, const int
   y[3 * row] = y3[0]; y[3 * row + 1] = y3[1]; y[3 * row + 2] = y3[2];
 }
 
+// One warp per (32-row slice, output component): 3x the threads of a
+// row-per-thread product, each warp still reading its 3 block entries per
+// slot as coalesced 256-byte lines.
+__device__ __forceinline__ double sell_row_comp(int slice, int lane, int c, const int64_t* __restrict__ slice_ptr,
+                                                const int* __restrict__ col, const double* __restrict__ val,
+                                                const double* __restrict__ x) {
+  const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
+  double acc = 0;
+  for (int64_t s = s0; s < s1; ++s) {
+    const int cc = __ldg(col + s * 32 + lane);
+    if (cc < 0) break;
+    const double* v = val + (s * 9 + 3 * c) * 32 + lane;
+    acc += __ldg(v) * __ldg(x + 3 * cc) + __ldg(v + 32) * __ldg(x + 3 * cc + 1) + __ldg(v + 64) * __ldg(x + 3 * cc + 2);
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(96) k_bsr_spmv3(int n_rows, const int64_t* __restrict__ slice_ptr,
+                                                  const int* __restrict__ col, const double* __restrict__ val,
+                                                  const double* __restrict__ x, double* __restrict__ y) {
+  const int slice = blockIdx.x, c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = slice * 32 + lane;
+  if (row >= n_rows) return;
+  y[3 * row + c] = sell_row_comp(slice, lane, c, slice_ptr, col, val, x);
+}
+
 __global__ void k_dof_to_node(int n_dofs, const int* __restrict__ free_rows, const double* __restrict__ in,
                               double* __restrict__ out, int64_t in_stride, int64_t out_stride) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -186,44 +212,39 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n_rows, const doub
   }
 }
 
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_dir_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
+__global__ void __launch_bounds__(96) k_pcg_dir_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
                                                               const int* __restrict__ col,
                                                               const double* __restrict__ val,
                                                               const double* __restrict__ dinv,
                                                               const double* __restrict__ r, double* p0, double* p1,
                                                               double* __restrict__ q, double* __restrict__ partial,
                                                               PcgState* st) {
+  // one CTA = one 32-row slice; warp c computes output component c
   __shared__ double sh[32];
   if (st->done) return;
   const int it = st->it;
   const double beta = st->beta;
   const double* __restrict__ pold = (it & 1) ? p1 : p0;
   double* __restrict__ pnew = (it & 1) ? p0 : p1;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slice = blockIdx.x, c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = slice * 32 + lane;
   double pq = 0;
   if (row < n_rows) {
-    const int slice = row >> 5, lane = row & 31;
     const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
-    double y0 = 0, y1 = 0, y2 = 0;
+    double yc = 0;
     for (int64_t s = s0; s < s1; ++s) {
-      const int c = __ldg(col + s * 32 + lane);
-      if (c < 0) break;
-      const double* v = val + s * 9 * 32 + lane;
-      const double x0 = dinv[3 * c] * r[3 * c] + beta * pold[3 * c];
-      const double x1 = dinv[3 * c + 1] * r[3 * c + 1] + beta * pold[3 * c + 1];
-      const double x2 = dinv[3 * c + 2] * r[3 * c + 2] + beta * pold[3 * c + 2];
-      y0 += __ldg(v + 0 * 32) * x0 + __ldg(v + 1 * 32) * x1 + __ldg(v + 2 * 32) * x2;
-      y1 += __ldg(v + 3 * 32) * x0 + __ldg(v + 4 * 32) * x1 + __ldg(v + 5 * 32) * x2;
-      y2 += __ldg(v + 6 * 32) * x0 + __ldg(v + 7 * 32) * x1 + __ldg(v + 8 * 32) * x2;
+      const int cc = __ldg(col + s * 32 + lane);
+      if (cc < 0) break;
+      const double* v = val + (s * 9 + 3 * c) * 32 + lane;
+      const double x0 = dinv[3 * cc] * r[3 * cc] + beta * pold[3 * cc];
+      const double x1 = dinv[3 * cc + 1] * r[3 * cc + 1] + beta * pold[3 * cc + 1];
+      const double x2 = dinv[3 * cc + 2] * r[3 * cc + 2] + beta * pold[3 * cc + 2];
+      yc += __ldg(v) * x0 + __ldg(v + 32) * x1 + __ldg(v + 64) * x2;
     }
-    double pn[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      pn[c] = dinv[3 * row + c] * r[3 * row + c] + beta * pold[3 * row + c];
-      pnew[3 * row + c] = pn[c];
-    }
-    q[3 * row] = y0; q[3 * row + 1] = y1; q[3 * row + 2] = y2;
-    pq = pn[0] * y0 + pn[1] * y1 + pn[2] * y2;
+    const double pn = dinv[3 * row + c] * r[3 * row + c] + beta * pold[3 * row + c];
+    pnew[3 * row + c] = pn;
+    q[3 * row + c] = yc;
+    pq = pn * yc;
   }
   const double s = block_sum(pq, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
@@ -304,8 +325,8 @@ int launch_bsr_diag_inv(Context* ctx, const Mesh* m, const double* d_val, double
 }
 
 int launch_bsr_spmv(Context* ctx, const Mesh* m, const double* d_val, const double* d_x, double* d_y) {
-  k_bsr_spmv<<<(m->n_nodes + kSpmvThreads - 1) / kSpmvThreads, kSpmvThreads, 0, ctx->stream>>>(
-      m->n_nodes, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), d_val, d_x, d_y);
+  k_bsr_spmv3<<<m->pat.n_slices, 96, 0, ctx->stream>>>(m->n_nodes, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
+                                                        d_val, d_x, d_y);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
@@ -348,15 +369,14 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     MSG_TRY(A->d_p0.alloc(ctx, sizeof(double) * n));
     MSG_TRY(A->d_p1.alloc(ctx, sizeof(double) * n));
     MSG_TRY(A->d_q.alloc(ctx, sizeof(double) * n));
-    MSG_TRY(A->d_partial.alloc(ctx, sizeof(double) * 2 * 4096));
+    // partials: one per SpMV CTA (slice) or two per update CTA
+    MSG_TRY(A->d_partial.alloc(ctx, sizeof(double) * std::max<size_t>(2 * 4096, m->pat.n_slices)));
     MSG_TRY(A->d_state.alloc(ctx, sizeof(PcgState)));
     MSG_CUDA(ctx, cudaMemsetAsync(A->d_state.ptr, 0, sizeof(PcgState), ctx->stream));
   }
   PcgState* st = A->d_state.as<PcgState>();
   const int grid_v = std::min(4096, std::max(1, std::min((n + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 8)));
-  const int grid_s = (nr + kPcgThreads - 1) / kPcgThreads;
-  // the partial buffer holds 8192 doubles: grid_s (SpMV) and 2*grid_v (update) entries
-  if (grid_s > 8192) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh too large for the PCG partial buffer");
+  const int grid_s = m->pat.n_slices;  // 96-thread CTAs, one 32-row slice each
 
   k_pcg_init<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, d_b, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
                                                       A->d_p0.as<double>(), A->d_p1.as<double>(),
@@ -374,7 +394,7 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
-      k_pcg_dir_spmv<<<grid_s, kPcgThreads, 0, ctx->stream>>>(
+      k_pcg_dir_spmv<<<grid_s, 96, 0, ctx->stream>>>(
           nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val.as<double>(), A->d_dinv.as<double>(),
           A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
           A->d_partial.as<double>(), st);

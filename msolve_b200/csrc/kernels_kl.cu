@@ -39,7 +39,7 @@ __global__ void k_kl_psi(int ne, int K, const double* __restrict__ cen, const do
 __global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, const double* __restrict__ xi,
                                                   const double* __restrict__ psi, double mu,
                                                   double* __restrict__ E64_er, float* __restrict__ E32_er,
-                                                  double* __restrict__ E64_re) {
+                                                  double* __restrict__ E64_re, const int* __restrict__ elem_row) {
   __shared__ double s_xi[kMaxTerms][33];
   __shared__ double s_psi[kMaxTerms][33];
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
@@ -59,8 +59,9 @@ __global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, 
     double s = mu;
     for (int k = 0; k < K; ++k) s += s_xi[k][tx] * s_psi[k][le];
     const double E = (r < R) ? exp(s) : 1.0;
-    if (E64_er) E64_er[(size_t)e * Rp + r] = E;
-    if (E32_er) E32_er[(size_t)e * Rp + r] = (float)E;
+    const size_t row = elem_row ? (size_t)elem_row[e] : (size_t)e;
+    if (E64_er) E64_er[row * Rp + r] = E;
+    if (E32_er) E32_er[row * Rp + r] = (float)E;
     if (E64_re && r < R) E64_re[(size_t)r * ne + e] = E;
   }
 }
@@ -99,10 +100,10 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
 }
 
 int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int Rp, const double* d_xi,
-                    double* d_E64_er, float* d_E32_er, double* d_E64_re) {
+                    double* d_E64_er, float* d_E32_er, double* d_E64_re, const int* d_elem_row) {
   dim3 grid((m->n_elems + 31) / 32, Rp / 32);
   k_kl_field<<<grid, dim3(32, 8), 0, ctx->stream>>>(m->n_elems, kl->n_terms, R, Rp, d_xi, kl->d_psi.as<double>(),
-                                                    kl->mu, d_E64_er, d_E32_er, d_E64_re);
+                                                    kl->mu, d_E64_er, d_E32_er, d_E64_re, d_elem_row);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;

@@ -235,6 +235,38 @@ static void detect_structured(Mesh* m) {
   for (int a = 0; a < 3; ++a) m->origin[a] = lo[a];
 }
 
+// Index maps of the padded lattice used by the batched matrix-free path.
+static int build_padded_maps(Context* ctx, Mesh* m) {
+  const int NX = m->nx + 1, NY = m->ny + 1, NZ = m->nz + 1;
+  m->NXp = NX + 2; m->NYp = NY + 2; m->NZp = NZ + 2;
+  const int64_t npad = (int64_t)m->NXp * m->NYp * m->NZp;
+  if (npad * 3 > INT32_MAX) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "lattice too large");
+  auto pad = [&](int i, int j, int k) { return (i + 1) + m->NXp * ((j + 1) + m->NYp * (k + 1)); };
+  std::vector<int> interior((size_t)NX * NY * NZ), elem_row(m->n_elems), rows(m->n_dofs);
+  std::vector<uint8_t> pmask(npad, 7);
+  for (int k = 0, t = 0; k < NZ; ++k)
+    for (int j = 0; j < NY; ++j)
+      for (int i = 0; i < NX; ++i, ++t) {
+        const int p = pad(i, j, k);
+        interior[t] = p;
+        uint8_t mk = 0;
+        for (int c = 0; c < 3; ++c) {
+          const int d = m->dof[3 * (size_t)t + c];
+          if (d < 0) mk |= (uint8_t)(1 << c);
+          else rows[d] = 3 * p + c;
+        }
+        pmask[p] = mk;
+      }
+  for (int k = 0, e = 0; k < m->nz; ++k)
+    for (int j = 0; j < m->ny; ++j)
+      for (int i = 0; i < m->nx; ++i, ++e) elem_row[e] = pad(i, j, k);
+  MSG_TRY(upload(ctx, m->d_pad_interior, interior.data(), interior.size()));
+  MSG_TRY(upload(ctx, m->d_pad_elem_row, elem_row.data(), elem_row.size()));
+  MSG_TRY(upload(ctx, m->d_pad_free_rows, rows.data(), rows.size()));
+  MSG_TRY(upload(ctx, m->d_pad_mask, pmask.data(), pmask.size()));
+  return MSG_OK;
+}
+
 static int create_mesh(Context* ctx, int n_nodes, const double* xyz, int n_elems, const int* conn, const int* dof,
                        int n_dofs, Mesh** out) {
   if (n_nodes <= 0 || n_elems <= 0 || !xyz || !conn || !dof || n_dofs < 0 || !out)
@@ -262,6 +294,7 @@ static int create_mesh(Context* ctx, int n_nodes, const double* xyz, int n_elems
     if (free_rows[d] < 0) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "mesh: DOF %d unused", d);
   MSG_TRY(build_pattern(m.get()));
   detect_structured(m.get());
+  if (m->structured) MSG_TRY(build_padded_maps(ctx, m.get()));
   std::vector<double> exyz(24 * (size_t)n_elems), cen(3 * (size_t)n_elems);
   for (int e = 0; e < n_elems; ++e) {
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -334,24 +367,12 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
   int status = MSG_OK;
   if (mode == MSG_MODE_MIXED_BATCHED) {
     if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mixed batched mode needs a structured cube lattice");
-    DevMem E64, E32;
-    MSG_TRY(E64.alloc(ctx, sizeof(double) * (size_t)m->n_elems * Rp));
-    MSG_TRY(E32.alloc(ctx, sizeof(float) * (size_t)m->n_elems * Rp));
-    cudaEvent_t f0, f1;
-    cudaEventCreate(&f0); cudaEventCreate(&f1);
-    cudaEventRecord(f0, ctx->stream);
-    MSG_TRY(launch_kl_field(ctx, m, &kd, R, Rp, d_xi, E64.as<double>(), E32.as<float>(), nullptr));
-    cudaEventRecord(f1, ctx->stream);
     BatchOut o;
     std::vector<double> htip(R);
     o.tip = tip ? htip.data() : nullptr;
     o.iterations = iterations;
     o.rel_res = rel_res;
-    status = block_mixed_solve(ctx, m, nu, E64.as<double>(), E32.as<float>(), R, Rp, d_b, max_it, tol, tip_dof, d_X, o);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, f0, f1);
-    ctx->t_phase[0] = ms;
-    cudaEventDestroy(f0); cudaEventDestroy(f1);
+    status = block_mixed_solve(ctx, m, nu, &kd, d_xi, R, Rp, d_b, max_it, tol, tip_dof, d_X, o);
     if (tip) std::copy(htip.begin(), htip.end(), tip);
   } else if (mode == MSG_MODE_FP64_BSR) {
     DevMem E64re, ke, st, bnode, xnode, tipd;
@@ -460,8 +481,7 @@ const char* MSG_LAST_ERROR(MSG_CTX ctx) { return ctx ? ctx->last_error.c_str() :
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   CTX_GUARD(ctx);
   if (!key) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "null option key");
-  if (!std::strcmp(key, "inner_tol") && value > 0 && value < 1) { ctx->inner_tol = value; return MSG_OK; }
-  if (!std::strcmp(key, "inner_max") && value >= 1) { ctx->inner_max = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "reliable_delta") && value > 0 && value < 1) { ctx->reliable_delta = value; return MSG_OK; }
   if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }

@@ -64,9 +64,8 @@ struct Context {
   int64_t op_samples = 0;
   int sm_count = 148;
   // mixed-solver tunables (MSG_SET_OPTION)
-  double inner_tol = 1e-4;   // inner FP32 PCG relative residual per refinement step
-  int inner_max = 100000;    // inner iterations per refinement step
-  int chunk = 16;            // inner iterations per captured graph launch
+  double reliable_delta = 0.1;  // FP64 residual replacement when ||r|| drops by this factor
+  int chunk = 16;               // inner iterations per captured graph launch
 };
 
 void retain(Context* ctx);
@@ -130,6 +129,14 @@ struct Mesh {
   DevMem d_mask;       // [n_nodes] uint8 bit c = component c constrained
   DevMem d_centroid;   // [n_elems][3]
   DevMem d_free_rows;  // [n_dofs] int: node*3+c for each free DOF (DOF -> node layout)
+  // padded lattice of a structured mesh (one ghost node layer per side):
+  // NXp = nx+3 nodes per x row etc.; element (i,j,k) is stored at the padded
+  // node of its lower corner, so nodes and elements share one index space.
+  int NXp = 0, NYp = 0, NZp = 0;
+  DevMem d_pad_free_rows;  // [n_dofs] padded node*3 + c
+  DevMem d_pad_elem_row;   // [n_elems] padded row of the element
+  DevMem d_pad_mask;       // [padded nodes] constrained bits, ghosts = 7
+  DevMem d_pad_interior;   // [interior nodes] padded index of interior node t (generator order)
 };
 
 struct PcgState {
@@ -173,8 +180,9 @@ struct KLDevice {
   double mu = 0;
 };
 int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out);
+// d_elem_row (nullable): output row of element e in the [row][Rp] layouts.
 int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int Rp, const double* d_xi,
-                    double* d_E64_er, float* d_E32_er, double* d_E64_re);
+                    double* d_E64_er, float* d_E32_er, double* d_E64_re, const int* d_elem_row = nullptr);
 
 // batched mixed-precision solve on a structured lattice (kernels_block.cu)
 struct BatchOut {
@@ -182,8 +190,8 @@ struct BatchOut {
   int* iterations = nullptr;
   double* rel_res = nullptr;
 };
-int block_mixed_solve(Context* ctx, Mesh* m, double nu, const double* d_E64_er, const float* d_E32_er, int R,
-                      int Rp, const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
+int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
+                      const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
 
 // Element stiffness of one cube of side h at E=1 (host, via the K1 kernel): K[24][24] full.
 int unit_cube_khat(Context* ctx, double h, double nu, double* K576);
