@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--fp64-sample", type=int, default=8)
     p.add_argument("--cpu-sample", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--reliable-delta", type=float, default=None, help="MSG_SET_OPTION reliable_delta")
+    p.add_argument("--chunk", type=int, default=None, help="MSG_SET_OPTION chunk")
     return p.parse_args()
 
 
@@ -197,6 +199,10 @@ def main():
     from msolve_b200 import _native as N
 
     ctx = M.Context(local)
+    if args.reliable_delta is not None:
+        ctx.set_option("reliable_delta", args.reliable_delta)
+    if args.chunk is not None:
+        ctx.set_option("chunk", args.chunk)
     model, kl = make_problem(args)
     mesh = M.GpuMesh(ctx, model)
     R, K_terms = args.R, args.terms
@@ -351,7 +357,8 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-            "iterations": {"mean": float(its_all.mean()), "max": int(its_all.max())},
+            "iterations": {"mean": float(its_all.mean()), "max": int(its_all.max()),
+                           "reliable_updates_last_step": st["reliable_updates"]},
             "max_true_rel_residual": max(resmax),
             "rel_err_vs_fp64": rel_err,
             "fp64_dropin": {"solves_per_s": fp64_rate, "sample": k, "mean_iterations": fp64_its,

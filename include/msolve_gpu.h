@@ -184,7 +184,8 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 
 /* Kernel launch counter of this context (kernels launched since creation),
  * and device timings in ms (t8 may be NULL):
- * t[0]=KL field, t[1]=inner FP32 loop, t[2]=unused, t[3]=FP64 residual steps,
+ * t[0]=KL field, t[1]=inner FP32 loop, t[2]=number of FP64 true-residual
+ * (reliable) updates of the last mixed batch, t[3]=FP64 residual steps,
  * t[4]=whole last MC batch (last call); t[5]=mean duration of one
  * matrix-free operator launch, t[6]=mean duration of one inner update launch,
  * t[7]=number of samples behind t[5..6] (one per inner graph launch, CUDA

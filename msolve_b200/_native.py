@@ -171,8 +171,9 @@ class Context:
         n = C.c_int64(0)
         t = np.zeros(8)
         lib().MSG_STATS(self.handle, C.byref(n), ptr(t))
-        return dict(launches=n.value, t_field_ms=t[0], t_inner_ms=t[1], t_resid_ms=t[3], t_total_ms=t[4],
-                    op_launch_ms=t[5], update_launch_ms=t[6], launch_samples=int(t[7]))
+        return dict(launches=n.value, t_field_ms=t[0], t_inner_ms=t[1], reliable_updates=int(t[2]),
+                    t_resid_ms=t[3], t_total_ms=t[4], op_launch_ms=t[5], update_launch_ms=t[6],
+                    launch_samples=int(t[7]))
 
     def reset_stats(self):
         lib().MSG_STATS_RESET(self.handle)

@@ -19,8 +19,10 @@
 // of p: each plane (3x3 nodes x 3 components, 27 coalesced loads) and the 4 new
 // elements of its slab feed the partial outputs of the three nodes P-1, P, P+1
 // through the two adjacent element slabs, 8 x (4 x 9) FMAs per plane against
-// Khat (a __grid_constant__ parameter: every Khat operand is a warp-uniform
-// constant-bank read). Only one plane, three partial outputs and two E slabs
+// Khat. Khat enters as its 10 value classes held in registers; the class and
+// sign of every entry are compile-time constants (khat_classes.h), so each
+// FMA takes a register operand with a free sign modifier and no constant-bank
+// traffic. Only one plane, three partial outputs and two E slabs
 // are live in registers. Each output is written once: no atomics; results are
 // deterministic and independent of the batch mix.
 //
@@ -39,6 +41,9 @@
 #include <cmath>
 #include <cstring>
 
+#include <utility>
+
+#include "khat_classes.h"
 #include "msg_internal.h"
 
 namespace msg {
@@ -46,8 +51,21 @@ namespace {
 
 constexpr int kTJ = 2, kTK = 2, kWarps = kTJ * kTK;  // pencils per CTA (2 x 2 in (j,k))
 
-struct KhatF { float k[576]; };
-struct KhatD { double k[576]; };
+// The unit-cube stiffness as its value classes (khat_classes.h): entry
+// (row, col) = sign * v[class], both compile-time constants of (row, col).
+template <class T> struct KhatClasses { T v[kKhatClasses]; };
+using KhatF = KhatClasses<float>;
+using KhatD = KhatClasses<double>;
+
+template <int... Is, class F>
+__device__ __forceinline__ void static_for_impl(std::integer_sequence<int, Is...>, F&& f) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+// f(std::integral_constant<int, i>) for i = 0..N-1, each index a constant expression
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  static_for_impl(std::make_integer_sequence<int, N>{}, f);
+}
 
 struct Lattice {
   int NX, NY, NZ;     // interior nodes per axis (nx+1 ...)
@@ -70,28 +88,32 @@ __device__ __forceinline__ T ldv(const T* p) { return __ldg(p); }
 // with an = corner(AX, 1-ey, 1-ez) (output node in the element) and
 // bn = corner(BX, by, bz) (input node in the element).
 template <class T, int AX, int BX>
-__device__ __forceinline__ void slab_apply(const typename KhatOf<T>::type& K, const T (&u)[3][3][3],
-                                           const T (&E)[2][2], T (&y)[3]) {
-#pragma unroll
-  for (int ey = 0; ey < 2; ++ey)
-#pragma unroll
-    for (int ez = 0; ez < 2; ++ez) {
-      const int an = corner_id(AX, 1 - ey, 1 - ez);
+__device__ __forceinline__ void slab_apply(const T (&kv)[kKhatClasses], const T (&u)[3][3][3], const T (&E)[2][2],
+                                           T (&y)[3]) {
+  static_for<2>([&](auto EY) {
+    static_for<2>([&](auto EZ) {
+      constexpr int ey = decltype(EY)::value, ez = decltype(EZ)::value;
+      constexpr int an = corner_id(AX, 1 - ey, 1 - ez);
       T t[3] = {T(0), T(0), T(0)};
-#pragma unroll
-      for (int by = 0; by < 2; ++by)
-#pragma unroll
-        for (int bz = 0; bz < 2; ++bz) {
-          const int bn = corner_id(BX, by, bz);
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int c2 = 0; c2 < 3; ++c2)
-              t[c] = fma(K.k[(3 * an + c) * 24 + 3 * bn + c2], u[ey + by][ez + bz][c2], t[c]);
-        }
+      static_for<2>([&](auto BY) {
+        static_for<2>([&](auto BZ) {
+          constexpr int by = decltype(BY)::value, bz = decltype(BZ)::value;
+          constexpr int bn = corner_id(BX, by, bz);
+          static_for<3>([&](auto C) {
+            static_for<3>([&](auto C2) {
+              constexpr int c = decltype(C)::value, c2 = decltype(C2)::value;
+              constexpr int code = kKhatClass[(3 * an + c) * 24 + 3 * bn + c2];
+              constexpr int cls = (code > 0 ? code : -code) - 1;
+              const T k = code > 0 ? kv[cls] : -kv[cls];
+              t[c] = fma(k, u[ey + by][ez + bz][c2], t[c]);
+            });
+          });
+        });
+      });
 #pragma unroll
       for (int c = 0; c < 3; ++c) y[c] = fma(E[ey][ez], t[c], y[c]);
-    }
+    });
+  });
 }
 
 // Sweep the interior pencil (J, K) (padded coordinates, 1-based) for one
@@ -104,6 +126,9 @@ template <class T, class Emit>
 __device__ __forceinline__ void pencil_sweep(const Lattice& L, const typename KhatOf<T>::type& K, int J, int Kz,
                                              const T* __restrict__ u, const T* __restrict__ E, Emit emit) {
   const int Rp = L.Rp;
+  T kv[kKhatClasses];  // class values in registers
+#pragma unroll
+  for (int i = 0; i < kKhatClasses; ++i) kv[i] = K.v[i];
   const size_t sxy = (size_t)L.NXp, sxz = (size_t)L.NXp * L.NYp;
   const size_t row0 = (size_t)(J + L.NYp * Kz) * L.NXp;  // padded node index of x = 0
   T ym[3] = {T(0), T(0), T(0)}, y0[3] = {T(0), T(0), T(0)}, yp[3];  // outputs at P-1, P, P+1
@@ -128,10 +153,10 @@ __device__ __forceinline__ void pencil_sweep(const Lattice& L, const typename Kh
       for (int ez = 0; ez < 2; ++ez) Ecur[ey][ez] = ldv(E + (node + (ey - 1) * sxy + (ez - 1) * sxz) * Rp);
 #pragma unroll
     for (int c = 0; c < 3; ++c) yp[c] = T(0);
-    slab_apply<T, 1, 0>(K, pl, Ecur, yp);   // slab P, output P+1
-    slab_apply<T, 0, 0>(K, pl, Ecur, y0);   // slab P, output P
-    slab_apply<T, 1, 1>(K, pl, Eprev, y0);  // slab P-1, output P
-    slab_apply<T, 0, 1>(K, pl, Eprev, ym);  // slab P-1, output P-1
+    slab_apply<T, 1, 0>(kv, pl, Ecur, yp);   // slab P, output P+1
+    slab_apply<T, 0, 0>(kv, pl, Ecur, y0);   // slab P, output P
+    slab_apply<T, 1, 1>(kv, pl, Eprev, y0);  // slab P-1, output P
+    slab_apply<T, 0, 1>(kv, pl, Eprev, ym);  // slab P-1, output P-1
     if (P > 1) emit(node - 1, own_m, ym);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -560,7 +585,16 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   MSG_TRY(unit_cube_khat(ctx, m->h, nu, K576));
   KhatF KF;
   KhatD KD;
-  for (int i = 0; i < 576; ++i) { KD.k[i] = K576[i]; KF.k[i] = (float)K576[i]; }
+  for (int c = 0; c < kKhatClasses; ++c) {
+    KD.v[c] = K576[kKhatRep[c]];
+    KF.v[c] = (float)KD.v[c];
+  }
+  for (int i = 0; i < 576; ++i) {  // the element must have the cube's class structure
+    const int code = kKhatClass[i];
+    const double v = code > 0 ? KD.v[code - 1] : -KD.v[-code - 1];
+    if (std::fabs(v - K576[i]) > 1e-12 * std::fabs(KD.v[0]))
+      return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element stiffness does not have the unit-cube structure");
+  }
   const double kdiag = K576[0];
 
   DevMem x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;

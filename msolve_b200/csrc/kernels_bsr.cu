@@ -172,7 +172,16 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;  // valid in thread 0
 }
 
-// Returns true in thread 0 of the last block to finish.
+// Whole-block sum of partial[i*stride + off], i < n, in a fixed order (thread
+// t takes i = t, t + blockDim, ...; then the block tree): called by every
+// thread of the last block, result valid in thread 0.
+__device__ __forceinline__ double sum_partials(const double* partial, int n, int stride, int off, double* sh) {
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += __ldcg(partial + (size_t)i * stride + off);
+  return block_sum(s, sh);
+}
+
+// Returns true in every thread of the last block to finish.
 __device__ __forceinline__ bool last_block(unsigned int* counter) {
   __shared__ bool is_last;
   __threadfence();
@@ -200,9 +209,10 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n_rows, const doub
   double s1 = block_sum(bb, sh);
   double s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
-  if (last_block(&st->counter) && threadIdx.x == 0) {
-    double tb = 0, tz = 0;
-    for (unsigned int i = 0; i < gridDim.x; ++i) { tb += __ldcg(partial + 2 * i); tz += __ldcg(partial + 2 * i + 1); }
+  if (!last_block(&st->counter)) return;
+  const double tb = sum_partials(partial, gridDim.x, 2, 0, sh);
+  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  if (threadIdx.x == 0) {
     st->bnorm = sqrt(tb);
     st->zr = tz;
     st->beta = 0; st->alpha = 0; st->err = 0;
@@ -248,9 +258,9 @@ __global__ void __launch_bounds__(96) k_pcg_dir_spmv(int n_rows, const int64_t* 
   }
   const double s = block_sum(pq, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
-  if (last_block(&st->counter) && threadIdx.x == 0) {
-    double t = 0;
-    for (unsigned int i = 0; i < gridDim.x; ++i) t += __ldcg(partial + i);
+  if (!last_block(&st->counter)) return;
+  const double t = sum_partials(partial, gridDim.x, 1, 0, sh);
+  if (threadIdx.x == 0) {
     st->pq = t;
     st->matvecs += 1;
     if (!(t > 0) || isnan(t)) {  // breakdown: p.q <= 0 or NaN
@@ -284,9 +294,10 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const do
   double s1 = block_sum(rr, sh);
   double s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
-  if (last_block(&st->counter) && threadIdx.x == 0) {
-    double tr = 0, tz = 0;
-    for (unsigned int i = 0; i < gridDim.x; ++i) { tr += __ldcg(partial + 2 * i); tz += __ldcg(partial + 2 * i + 1); }
+  if (!last_block(&st->counter)) return;
+  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
+  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  if (threadIdx.x == 0) {
     st->err = sqrt(tr) / st->bnorm;
     if (st->err < st->tol) {
       st->done = 1; st->iterations = it;
