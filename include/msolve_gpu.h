@@ -123,6 +123,22 @@ int MSG_MAT_DESTROY(MSG_MAT mat);
 int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
                   double* rel_res);
 
+/* MSG_PCG_SOLVE without device allocation. No counterpart in the reference.
+ * For callers that must not allocate device memory while solving: cudaMalloc
+ * and cudaFree synchronise the whole device (a caller overlapping other GPU
+ * work would stall), and a host that hands the library a fixed share of device
+ * memory may forbid allocations outside it. b_dev and x_dev are the caller's
+ * device buffers (n_dofs doubles, DOF numbering); the solve's working vectors
+ * live in one fixed device array of the library (about 9.5 MB, held on every
+ * GPU that loads the library until the process exits), which limits the mesh
+ * to 65536 nodes (larger meshes: MSG_ERR_INVALID_ARGUMENT). The first call on
+ * a device looks up that array's device address; make the first call before
+ * any stream capture. All calls share the array: calls whose GPU work
+ * overlaps (two host threads on two contexts of the same device) race and must
+ * be serialised by the caller. Semantics, kernels and results as MSG_PCG_SOLVE. */
+int MSG_PCG_SOLVE_NOALLOC(MSG_MAT mat, const double* b_dev, double* x_dev, int max_it, double tol, int* iterations,
+                          double* rel_res);
+
 /* ------------------------------------------------------------------ stochastic field */
 /* Separable Karhunen-Loeve table of a lognormal Young's modulus, the content of
  * the eigen-data file read by LognormalFileStochasticCoefficientsProvider

@@ -443,4 +443,100 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
   return MSG_OK;
 }
 
+// ------------------------------------------------------------------ PCG without allocation
+// Scratch of MSG_PCG_SOLVE_NOALLOC: a fixed array in device memory, so the call
+// needs no cudaMalloc. Sized for meshes of up to kNoAllocMaxNodes nodes: six
+// node-layout FP64 vectors (b, x, r, two search directions, K p), the per-CTA
+// partial sums and the scalar state, about 9.5 MB. Every GPU that loads the
+// library holds this array until the process exits.
+constexpr int kNoAllocMaxNodes = 65536;
+constexpr size_t kNoAllocVecBytes = sizeof(double) * 3 * (size_t)kNoAllocMaxNodes;
+constexpr size_t kNoAllocPartials = 2 * 4096;  // >= max(2 * update CTAs, slices of 65536 nodes)
+constexpr size_t kNoAllocStateOff = 6 * kNoAllocVecBytes + sizeof(double) * kNoAllocPartials;
+constexpr size_t kNoAllocBytes = kNoAllocStateOff + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of the scratch array on the current device, looked up once per
+// device (host code cannot use the array's name as a device address).
+static int noalloc_scratch(Context* ctx, unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* addr[64] = {nullptr};
+  if (ctx->device < 0 || ctx->device >= 64) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "device index >= 64");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[ctx->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    addr[ctx->device] = static_cast<unsigned char*>(p);
+  }
+  *out = addr[ctx->device];
+  return MSG_OK;
+}
+
 }  // namespace msg
+
+using namespace msg;
+
+// The device Jacobi-PCG of MSG_PCG_SOLVE, for callers that must not allocate
+// device memory during the solve: the solve's working vectors live in the
+// fixed scratch array above instead of buffers from cudaMalloc, and the
+// right-hand side and solution are the caller's device buffers. Kernels and
+// their order are those of MSG_PCG_SOLVE, launched one by one.
+extern "C" int MSG_PCG_SOLVE_NOALLOC(MSG_MAT A, const double* b_dev, double* x_dev, int max_it, double tol,
+                                     int* iterations, double* rel_res) {
+  if (!A || !b_dev || !x_dev || max_it <= 0 || !(tol > 0)) return MSG_ERR_INVALID_ARGUMENT;
+  Mesh* m = A->mesh;
+  Context* ctx = m->ctx;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const int nr = m->n_nodes;
+  if (nr > kNoAllocMaxNodes)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT,
+                     "MSG_PCG_SOLVE_NOALLOC: mesh has %d nodes, the fixed scratch holds at most %d", nr,
+                     kNoAllocMaxNodes);
+  unsigned char* base = nullptr;
+  MSG_TRY(noalloc_scratch(ctx, &base));
+  const size_t n = 3 * (size_t)nr;
+  double* bn = reinterpret_cast<double*>(base);
+  double* xn = reinterpret_cast<double*>(base + kNoAllocVecBytes);
+  double* r = reinterpret_cast<double*>(base + 2 * kNoAllocVecBytes);
+  double* p0 = reinterpret_cast<double*>(base + 3 * kNoAllocVecBytes);
+  double* p1 = reinterpret_cast<double*>(base + 4 * kNoAllocVecBytes);
+  double* q = reinterpret_cast<double*>(base + 5 * kNoAllocVecBytes);
+  double* partial = reinterpret_cast<double*>(base + 6 * kNoAllocVecBytes);
+  PcgState* st = reinterpret_cast<PcgState*>(base + kNoAllocStateOff);
+  cudaStream_t s = ctx->stream;
+  // the array keeps the previous call's contents: clear what must start at zero
+  MSG_CUDA(ctx, cudaMemsetAsync(bn, 0, sizeof(double) * n, s));
+  MSG_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(PcgState), s));
+  MSG_TRY(launch_dof_to_node(ctx, m, b_dev, bn, 1, 0, 0));
+  const int grid_v = std::min(4096, std::max(1, std::min((int)((n + kPcgThreads - 1) / kPcgThreads), ctx->sm_count * 8)));
+  const int grid_s = m->pat.n_slices;
+  k_pcg_init<<<grid_v, kPcgThreads, 0, s>>>(nr, bn, A->d_dinv.as<double>(), r, xn, p0, p1, partial, st);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &tol, sizeof(double), cudaMemcpyHostToDevice, s));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&st->max_it, &max_it, sizeof(int), cudaMemcpyHostToDevice, s));
+  int done = 0;
+  for (int it = 0; it < max_it + 8 && !done; it += 8) {
+    for (int k = 0; k < 8; ++k) {
+      k_pcg_dir_spmv<<<grid_s, 96, 0, s>>>(nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
+                                           A->d_val.as<double>(), A->d_dinv.as<double>(), r, p0, p1, q, partial, st);
+      k_pcg_update<<<grid_v, kPcgThreads, 0, s>>>(nr, A->d_dinv.as<double>(), r, xn, p0, p1, q, partial, st);
+    }
+    count_launch(ctx, 16);
+    MSG_CUDA(ctx, cudaMemcpyAsync(&done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MSG_CUDA(ctx, cudaStreamSynchronize(s));
+  }
+  MSG_CUDA(ctx, cudaGetLastError());
+  MSG_TRY(launch_node_to_dof(ctx, m, xn, x_dev, 1, 0, 0));
+  PcgState hs;
+  MSG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+  MSG_CUDA(ctx, cudaStreamSynchronize(s));
+  if (iterations) *iterations = hs.iterations;
+  if (rel_res) *rel_res = hs.err;
+  if (hs.status != MSG_OK)
+    return set_error(ctx, hs.status,
+                     hs.status == MSG_ERR_BREAKDOWN ? "PCG breakdown (p.q <= 0 or NaN)" : "PCG did not converge");
+  return MSG_OK;
+}
