@@ -26,15 +26,16 @@
 // are live in registers. Each output is written once: no atomics; results are
 // deterministic and independent of the batch mix.
 //
-// Solver: FP32 Jacobi-PCG with reliable updates. Per iteration
-//   k_dir    : p = dinv.r + beta p                      (elementwise)
-//   k_op     : q = K p (FP32, masked), partial p.q
-//   k_alpha  : alpha = (z.r)/(p.q) per realization
-//   k_update : d += alpha p, r -= alpha q, partials (dinv r).r and r.r
+// Solver: FP32 Jacobi-PCG with reliable updates. Per iteration k
+//   k_dir    : d += alpha_{k-1} p_{k-1}, p_k = dinv.r + beta_k p_{k-1} (in place)
+//   k_op     : q = K p_k (FP32, masked), partial p.q
+//   k_alpha  : alpha_k = (z.r)/(p.q) per realization
+//   k_update : r -= alpha_k q, partials (dinv r).r and r.r
 //   k_beta   : beta, and a request for a reliable update when ||r|| has
 //              dropped by `reliable_delta` since the last true residual
 // captured as one CUDA graph of `chunk` iterations. Reliable update (FP64):
-//   x += d, d = 0, r = b - K x with the FP64 operator (k_resid), true
+//   x += d + alpha p (the pending term), d = 0, r = b - K x with the FP64
+//   operator (k_resid), true
 //   ||r||/||b|| < tol ends a realization; otherwise the search direction is
 //   kept (beta = gamma_new / gamma_prev), so the Krylov progress survives.
 #include <algorithm>
@@ -120,11 +121,13 @@ __device__ __forceinline__ void slab_apply(const T (&kv)[kKhatClasses], const T 
 // realization lane, streaming x-planes: plane P feeds the output nodes P-1, P
 // and P+1 through the element slabs with lower corner x = P-1 and x = P, so
 // only the current plane (27 values), three partial outputs and two E slabs
-// are live. Node P-1 is complete (and emitted) after plane P. Emit(node,
-// own3, y3) receives the input and the operator output at the node.
-template <class T, class Emit>
+// are live. Node P-1 is complete (and emitted) after plane P. Load(node, v3)
+// produces the operator input at a node, Own(node, v3) runs once per node of
+// the pencil with its input, Emit(node, own3, y3) receives the input and the
+// operator output at the node.
+template <class T, class Load, class Own, class Emit>
 __device__ __forceinline__ void pencil_sweep(const Lattice& L, const typename KhatOf<T>::type& K, int J, int Kz,
-                                             const T* __restrict__ u, const T* __restrict__ E, Emit emit) {
+                                             const T* __restrict__ E, Load load, Own own, Emit emit) {
   const int Rp = L.Rp;
   T kv[kKhatClasses];  // class values in registers
 #pragma unroll
@@ -142,10 +145,9 @@ __device__ __forceinline__ void pencil_sweep(const Lattice& L, const typename Kh
     for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
       for (int dz = 0; dz < 3; ++dz) {
-        const T* src = u + ((node + (dy - 1) * sxy + (dz - 1) * sxz) * 3) * Rp;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) pl[dy][dz][c] = ldv(src + c * Rp);
+        load(node + (dy - 1) * sxy + (dz - 1) * sxz, pl[dy][dz]);
       }
+    own(node, pl[1][1]);  // side effects at the plane's centre node (x = P)
     T Ecur[2][2];
 #pragma unroll
     for (int ey = 0; ey < 2; ++ey)
@@ -211,21 +213,23 @@ __global__ void __launch_bounds__(128, 4)
   const int rr = blockIdx.y * 32 + threadIdx.x;
   double pq[1] = {0.0};
   if (valid) {
-    const float* pu = p + rr;
-    const float* Eu = E + rr;
-    float* qu = q + rr;
-    auto emit = [&](size_t node, const float* own, const float* y) {
+    auto load = [&](size_t node, float* o) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o[c] = ldv(p + (node * 3 + c) * Rp + rr);
+    };
+    auto own = [](size_t, const float*) {};
+    auto emit = [&](size_t node, const float* ownv, const float* y) {
       const uint8_t m = mask[node];
       float acc = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float qc = ((m >> c) & 1) ? 0.f : y[c];
-        qu[(node * 3 + c) * Rp] = qc;
-        acc = fmaf(own[c], qc, acc);
+        q[(node * 3 + c) * Rp + rr] = qc;
+        acc = fmaf(ownv[c], qc, acc);
       }
       pq[0] += (double)acc;
     };
-    pencil_sweep<float>(L, K, J, Kz, pu, Eu, emit);
+    pencil_sweep<float>(L, K, J, Kz, E + rr, load, own, emit);
   }
   cta_partial<1>(pq, partial, blockIdx.x, Rp, rr);
 }
@@ -255,7 +259,12 @@ __global__ void __launch_bounds__(128)
         acc[1] += dv * (double)rf * (double)rf;
       }
     };
-    pencil_sweep<double>(L, K, J, Kz, x + rr, E + rr, emit);
+    auto load = [&](size_t node, double* o) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o[c] = ldv(x + (node * 3 + c) * Rp + rr);
+    };
+    auto own = [](size_t, const double*) {};
+    pencil_sweep<double>(L, K, J, Kz, E + rr, load, own, emit);
   }
   cta_partial<2>(acc, partial, blockIdx.x, Rp, rr);
 }
@@ -290,15 +299,18 @@ struct Quad {
   __device__ bool live() const { return Q >= 256 || (int)threadIdx.x < G * Q; }
 };
 
-// p = dinv.r + beta p (in place; interior nodes)
+// Start of PCG iteration k (interior nodes, in place): d += alpha_{k-1} p_{k-1}
+// (the previous iteration's correction) and p_k = dinv.r_k + beta_k p_{k-1}.
 __global__ void __launch_bounds__(256) k_dir(int n_int, int Rp, const int* __restrict__ interior,
-                                             const float* __restrict__ beta, const float* __restrict__ r,
-                                             const float* __restrict__ dinv, float* __restrict__ p) {
+                                             const float* __restrict__ alpha, const float* __restrict__ beta,
+                                             const float* __restrict__ r, const float* __restrict__ dinv,
+                                             float* __restrict__ p, float* __restrict__ d) {
   Quad qd(Rp);
   if (!qd.live()) return;
   const int per = (n_int + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(n_int, t0 + per);
   for (int qb = qd.qb0; qb < qd.Q; qb += qd.qstep) {
+    const float4 a4 = reinterpret_cast<const float4*>(alpha)[qb];
     const float4 b4 = reinterpret_cast<const float4*>(beta)[qb];
     for (int t = t0 + qd.g; t < t1; t += qd.G) {
       const size_t n = (size_t)interior[t];
@@ -308,20 +320,21 @@ __global__ void __launch_bounds__(256) k_dir(int n_int, int Rp, const int* __res
         const size_t o = (n * 3 + c) * Rp;
         const float4 rv = reinterpret_cast<const float4*>(r + o)[qb];
         float4 pv = reinterpret_cast<const float4*>(p + o)[qb];
-        pv.x = fmaf(dv.x, rv.x, b4.x * pv.x);
-        pv.y = fmaf(dv.y, rv.y, b4.y * pv.y);
-        pv.z = fmaf(dv.z, rv.z, b4.z * pv.z);
-        pv.w = fmaf(dv.w, rv.w, b4.w * pv.w);
+        float4 dd = reinterpret_cast<const float4*>(d + o)[qb];
+        dd.x = fmaf(a4.x, pv.x, dd.x); dd.y = fmaf(a4.y, pv.y, dd.y);
+        dd.z = fmaf(a4.z, pv.z, dd.z); dd.w = fmaf(a4.w, pv.w, dd.w);
+        pv.x = fmaf(dv.x, rv.x, b4.x * pv.x); pv.y = fmaf(dv.y, rv.y, b4.y * pv.y);
+        pv.z = fmaf(dv.z, rv.z, b4.z * pv.z); pv.w = fmaf(dv.w, rv.w, b4.w * pv.w);
         reinterpret_cast<float4*>(p + o)[qb] = pv;
+        reinterpret_cast<float4*>(d + o)[qb] = dd;
       }
     }
   }
 }
 
-// d += alpha p, r -= alpha q; partials (dinv r).r and r.r per realization.
+// r -= alpha q; partials (dinv r).r and r.r per realization (interior nodes).
 __global__ void __launch_bounds__(256) k_update(int n_int, int Rp, const int* __restrict__ interior,
-                                                const float* __restrict__ alpha, const float* __restrict__ p,
-                                                const float* __restrict__ q, float* __restrict__ d,
+                                                const float* __restrict__ alpha, const float* __restrict__ q,
                                                 float* __restrict__ r, const float* __restrict__ dinv,
                                                 double* __restrict__ partial) {
   Quad qd(Rp);
@@ -338,15 +351,10 @@ __global__ void __launch_bounds__(256) k_update(int n_int, int Rp, const int* __
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const size_t o = (n * 3 + c) * Rp;
-          const float4 pv = reinterpret_cast<const float4*>(p + o)[qb];
           const float4 qv = reinterpret_cast<const float4*>(q + o)[qb];
-          float4 dd = reinterpret_cast<const float4*>(d + o)[qb];
           float4 rv = reinterpret_cast<const float4*>(r + o)[qb];
-          dd.x = fmaf(a4.x, pv.x, dd.x); dd.y = fmaf(a4.y, pv.y, dd.y);
-          dd.z = fmaf(a4.z, pv.z, dd.z); dd.w = fmaf(a4.w, pv.w, dd.w);
           rv.x = fmaf(-a4.x, qv.x, rv.x); rv.y = fmaf(-a4.y, qv.y, rv.y);
           rv.z = fmaf(-a4.z, qv.z, rv.z); rv.w = fmaf(-a4.w, qv.w, rv.w);
-          reinterpret_cast<float4*>(d + o)[qb] = dd;
           reinterpret_cast<float4*>(r + o)[qb] = rv;
           acc[0] += (double)(dv.x * rv.x * rv.x); acc[4] += (double)(rv.x * rv.x);
           acc[1] += (double)(dv.y * rv.y * rv.y); acc[5] += (double)(rv.y * rv.y);
@@ -384,8 +392,10 @@ __global__ void __launch_bounds__(256) k_update(int n_int, int Rp, const int* __
   }
 }
 
-// x += d, d = 0 (interior nodes, FP64 solution, FP32 correction)
+// x += d + alpha p (the correction, with the last iteration's term still
+// pending), d = 0 (interior nodes; FP64 solution, FP32 correction)
 __global__ void __launch_bounds__(256) k_xupdate(int n_int, int Rp, const int* __restrict__ interior,
+                                                 const float* __restrict__ alpha, const float* __restrict__ p,
                                                  double* __restrict__ x, float* __restrict__ d) {
   const int Q = Rp >> 1;  // float2 / double2 per thread
   const size_t total = (size_t)n_int * 3 * Q;
@@ -394,10 +404,12 @@ __global__ void __launch_bounds__(256) k_xupdate(int n_int, int Rp, const int* _
     const int qb = (int)(i - row * Q);
     const size_t node = (size_t)interior[row / 3];
     const size_t o = (node * 3 + row % 3) * Rp;
-    float2 dv = reinterpret_cast<float2*>(d + o)[qb];
+    const float2 a2 = reinterpret_cast<const float2*>(alpha)[qb];
+    const float2 pv = reinterpret_cast<const float2*>(p + o)[qb];
+    const float2 dv = reinterpret_cast<const float2*>(d + o)[qb];
     double2 xv = reinterpret_cast<double2*>(x + o)[qb];
-    xv.x += (double)dv.x;
-    xv.y += (double)dv.y;
+    xv.x += (double)fmaf(a2.x, pv.x, dv.x);
+    xv.y += (double)fmaf(a2.y, pv.y, dv.y);
     reinterpret_cast<double2*>(x + o)[qb] = xv;
     reinterpret_cast<float2*>(d + o)[qb] = make_float2(0.f, 0.f);
   }
@@ -517,6 +529,7 @@ __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, con
     s.beta[r] = (a && !first && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
     s.gamma[r] = g;
     s.rho_ref[r] = rr;
+    s.alpha[r] = 0.f;  // the pending alpha p term was folded into x
     active = a;
   }
   active = __syncthreads_count(active);
@@ -670,8 +683,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   const int G = Q >= 256 ? 1 : 256 / Q;
   const size_t upd_smem = G > 1 ? sizeof(double) * (size_t)G * Q * 8 : 0;
   const int sblocks = Rp / 32;  // scalar kernels: 32 realizations x 32 row groups per CTA
-  const int n_dir = std::min(L.n_int, ctx->sm_count * 8);
   const int n_xu = ctx->sm_count * 8;
+  const int n_dir = std::min(L.n_int, ctx->sm_count * 8);
   const double delta2 = ctx->reliable_delta * ctx->reliable_delta;
   const double tol2 = 0.25 * tol * tol;  // ask for a check once the recursive residual is at tol/2
 
@@ -685,7 +698,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < chunk; ++it) {
-      k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.beta, r32.as<float>(), dinv.as<float>(), p.as<float>());
+      k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
+                                   p.as<float>(), d.as<float>());
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
       if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
@@ -694,8 +708,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
       k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
       if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-      k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, s.alpha, p.as<float>(), q.as<float>(),
-                                             d.as<float>(), r32.as<float>(), dinv.as<float>(), part_up.as<double>());
+      k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, s.alpha, q.as<float>(), r32.as<float>(),
+                                             dinv.as<float>(), part_up.as<double>());
       if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
       cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
       k_beta<<<sblocks, 1024, 0, st>>>(Rp, n_upd, part_up.as<double>(), s, delta2, tol2);
@@ -718,7 +732,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       // reliable update: x += d; d = 0; r = b - K x (FP64)
       cudaEventRecord(ev[0], st);
       if (!first) {
-        k_xupdate<<<n_xu, 256, 0, st>>>(L.n_int, Rp, interior, x.as<double>(), d.as<float>());
+        k_xupdate<<<n_xu, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, p.as<float>(), x.as<double>(), d.as<float>());
         count_launch(ctx);
       }
       k_resid<<<op_grid, op_block, 0, st>>>(L, KD, x.as<double>(), blat.as<double>(), E64.as<double>(), mask,
