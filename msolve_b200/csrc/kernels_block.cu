@@ -42,6 +42,9 @@
 #include <cmath>
 #include <cstring>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <utility>
 
 #include "khat_classes.h"
@@ -231,6 +234,185 @@ __global__ void __launch_bounds__(128, 4)
     };
     pencil_sweep<float>(L, K, J, Kz, E + rr, load, own, emit);
   }
+  cta_partial<1>(pq, partial, blockIdx.x, Rp, rr);
+}
+
+// ---------------------------------------------------------------- TMA-staged FP32 operator
+// The production FP32 operator. A CTA owns a 2x2 tile of pencils (one warp
+// each) for 32 realizations. For every x-plane P one thread issues two TMA
+// tensor loads (no multicast) into a 4-stage shared-memory ring: the plane's
+// 4x4 node patch (32 realizations x 3 components, 6 KB: the tile plus its
+// one-node halo) and the 3x3 element patch of the slab with lower corner x = P
+// (1.1 KB). A "full" mbarrier per stage counts the bytes; an "empty" mbarrier
+// per stage collects one arrival per warp once the warp has read the stage, and
+// the producer refills a stage one plane after it was consumed. Warps read
+// their 3x3 neighbours at compile-time shared-memory offsets. Every wait is
+// bounded: on expiry the kernel raises *err and stops streaming.
+constexpr int kStages = 4;
+constexpr int kPJ = kTJ + 2, kPK = kTK + 2;              // plane patch (nodes)
+constexpr int kEJ = kTJ + 1, kEK = kTK + 1;              // element patch
+constexpr int kPlaneFloats = 32 * 3 * kPJ * kPK;         // 1536
+constexpr int kEFloats = 32 * kEJ * kEK;                 // 288
+constexpr int kStageFloats = kPlaneFloats + kEFloats;    // 7296 bytes, a multiple of 128
+constexpr uint32_t kStageBytes = kStageFloats * 4;
+constexpr size_t kOpSmem = 128 + (size_t)kStages * kStageBytes + 2 * kStages * sizeof(uint64_t);
+constexpr long kWaitLimit = 1L << 24;                    // try_wait polls before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(128, 4)
+    k_op_tma(Lattice L, const __grid_constant__ KhatF K, const __grid_constant__ CUtensorMap tm_p,
+             const __grid_constant__ CUtensorMap tm_e, const float* __restrict__ p, const uint8_t* __restrict__ mask,
+             float* __restrict__ q, double* __restrict__ partial, int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  // 128-byte aligned stage ring (TMA destinations), then the mbarriers
+  float* smem = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageFloats);
+  uint64_t* empty = full + kStages;
+  const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+  const int tile = blockIdx.x;
+  const int tj = tile % L.tiles_j, tk = tile / L.tiles_j;
+  const int J0 = 1 + tj * kTJ, K0 = 1 + tk * kTK;   // padded coordinates of the tile's first pencil
+  const int jy = w % kTJ, kz = w / kTJ;
+  const int J = J0 + jy, Kz = K0 + kz;
+  const bool valid = J <= L.NY && Kz <= L.NZ;
+  const int Rp = L.Rp, g32 = blockIdx.y * 32, rr = g32 + lane;
+  const int NX = L.NX;
+  if (tid == 0) {
+    for (int st = 0; st < kStages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int P) {  // plane P into stage (P-1) % kStages
+    const int st = (P - 1) % kStages;
+    float* dst = smem + st * kStageFloats;
+    mbar_expect_tx(&full[st], kStageBytes);
+    tma_load_5d(dst, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+    tma_load_4d(dst + kPlaneFloats, &tm_e, g32, P, J0 - 1, K0 - 1, &full[st]);
+  };
+  if (tid == 0)
+    for (int P = 1; P <= NX && P <= kStages; ++P) issue(P);
+
+  float kv[kKhatClasses];
+#pragma unroll
+  for (int i = 0; i < kKhatClasses; ++i) kv[i] = K.v[i];
+  const size_t row0 = (size_t)(J + L.NYp * Kz) * L.NXp;
+  float ym[3] = {0.f, 0.f, 0.f}, y0[3] = {0.f, 0.f, 0.f}, yp[3];
+  float Eprev[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+  float own_m[3] = {0.f, 0.f, 0.f};
+  double pq[1] = {0.0};
+  bool ok = true;
+  auto emit = [&](size_t node, const float* ownv, const float* y) {
+    const uint8_t m = mask[node];
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float qc = ((m >> c) & 1) ? 0.f : y[c];
+      q[(node * 3 + c) * Rp + rr] = qc;
+      acc = fmaf(ownv[c], qc, acc);
+    }
+    pq[0] += (double)acc;
+  };
+#pragma unroll 1
+  for (int P = 1; P <= NX; ++P) {
+    // refill the stage consumed one plane ago (the other warps have had a plane to release it)
+    if (tid == 0 && P >= 2 && P - 1 + kStages <= NX) {
+      const int prev = P - 1;
+      if (!mbar_wait(&empty[(prev - 1) % kStages], ((prev - 1) / kStages) & 1)) { atomicExch(err, 1); ok = false; }
+      else issue(prev + kStages);
+    }
+    const int st = (P - 1) % kStages;
+    if (!mbar_wait(&full[st], ((P - 1) / kStages) & 1)) { atomicExch(err, 1); ok = false; }
+    if (!ok) break;
+    const float* pt = smem + st * kStageFloats;
+    const float* et = pt + kPlaneFloats;
+    float pl[3][3][3];
+#pragma unroll
+    for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+      for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pl[dy][dz][c] = pt[(((kz + dz) * kPJ + (jy + dy)) * 3 + c) * 32 + lane];
+    float Ecur[2][2];
+#pragma unroll
+    for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+      for (int ez = 0; ez < 2; ++ez) Ecur[ey][ez] = et[((kz + ez) * kEJ + (jy + ey)) * 32 + lane];
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[st]);
+    if (valid) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) yp[c] = 0.f;
+      slab_apply<float, 1, 0>(kv, pl, Ecur, yp);
+      slab_apply<float, 0, 0>(kv, pl, Ecur, y0);
+      slab_apply<float, 1, 1>(kv, pl, Eprev, y0);
+      slab_apply<float, 0, 1>(kv, pl, Eprev, ym);
+      if (P > 1) emit(row0 + P - 1, own_m, ym);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ym[c] = y0[c];
+        y0[c] = yp[c];
+        own_m[c] = pl[1][1][c];
+      }
+#pragma unroll
+      for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+        for (int ez = 0; ez < 2; ++ez) Eprev[ey][ez] = Ecur[ey][ez];
+    }
+  }
+  if (ok && valid) emit(row0 + NX, own_m, ym);
+  if (!ok && tid == 0) {
+    // let copies already issued land before the CTA's shared memory goes away (bounded)
+    for (int P = 1; P <= NX; ++P) {
+      const int st = (P - 1) % kStages;
+      if (!mbar_wait(&full[st], ((P - 1) / kStages) & 1)) break;
+    }
+  }
+  (void)p;
   cta_partial<1>(pq, partial, blockIdx.x, Rp, rr);
 }
 
@@ -429,6 +611,7 @@ struct Scal {
   int* breakdown;      // [Rp]
   int* n_active;       // [1] active count after the last k_beta / k_resid_scalars
   int* n_update;       // [1] active realizations requesting a reliable update
+  int* err;            // [1] sticky: a bounded device wait expired
 };
 
 // Per-realization sum of NV interleaved partials over n rows, 32 realizations x
@@ -641,7 +824,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     s.its = (int*)base; base += sizeof(int) * Rp;
     s.breakdown = (int*)base; base += sizeof(int) * Rp;
     s.n_active = (int*)base; base += 16;
-    s.n_update = (int*)base;
+    s.n_update = (int*)base; base += 16;
+    s.err = (int*)base;  // outside the 32 bytes the iterations clear
   }
   // zero every padded vector once: ghost entries must stay zero
   MSG_CUDA(ctx, cudaMemsetAsync(x.ptr, 0, sizeof(double) * nvec, st));
@@ -692,6 +876,38 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   for (auto& e : ev) MSG_CUDA(ctx, cudaEventCreate(&e));
   float t_resid = 0.f, t_inner = 0.f;
 
+  // TMA descriptors of p (5-D: realization, component, x, y, z) and of the
+  // FP32 element field (4-D: realization, x, y, z) for the staged operator
+  CUtensorMap tm_p, tm_e;
+  {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+      void* f = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+          q == cudaDriverEntryPointSuccess)
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    if (!encode) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t fb = sizeof(float);
+    const cuuint64_t pd[5] = {(cuuint64_t)Rp, 3, (cuuint64_t)L.NXp, (cuuint64_t)L.NYp, (cuuint64_t)L.NZp};
+    const cuuint64_t ps[4] = {Rp * fb, 3 * Rp * fb, 3 * Rp * fb * L.NXp, 3 * Rp * fb * L.NXp * L.NYp};
+    const cuuint32_t pb[5] = {32, 3, 1, kPJ, kPK};
+    const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+    CUresult e1 = encode(&tm_p, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, p.ptr, pd, ps, pb, one,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const cuuint64_t ed[4] = {(cuuint64_t)Rp, (cuuint64_t)L.NXp, (cuuint64_t)L.NYp, (cuuint64_t)L.NZp};
+    const cuuint64_t es[3] = {Rp * fb, Rp * fb * L.NXp, Rp * fb * L.NXp * L.NYp};
+    const cuuint32_t eb[4] = {32, 1, kEJ, kEK};
+    CUresult e2 = encode(&tm_e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, E32.ptr, ed, es, eb, one,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (e1 != CUDA_SUCCESS || e2 != CUDA_SUCCESS)
+      return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d, %d)", (int)e1, (int)e2);
+  }
+
   const int chunk = std::max(2, ctx->chunk & ~1);
   cudaGraphExec_t gexec = nullptr;
   {
@@ -703,8 +919,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
       if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-      k_op<<<op_grid, op_block, 0, st>>>(L, KF, p.as<float>(), E32.as<float>(), mask, q.as<float>(),
-                                         part_op.as<double>());
+      k_op_tma<<<op_grid, op_block, kOpSmem, st>>>(L, KF, tm_p, tm_e, p.as<float>(), mask, q.as<float>(),
+                                                   part_op.as<double>(), s.err);
       if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
       k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
       if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
@@ -722,7 +938,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   }
 
   int* h_flags = nullptr;  // [0] active, [4] update requests (16-byte apart as in Scal)
-  MSG_CUDA(ctx, cudaMallocHost(&h_flags, 32));
+  MSG_CUDA(ctx, cudaMallocHost(&h_flags, 64));
   int status = MSG_OK;
   int total_inner = 0;
   int n_updates = 0;
@@ -741,7 +957,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       k_resid_scalars<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol, first ? 1 : 0);
       cudaEventRecord(ev[1], st);
       count_launch(ctx, 2);
-      MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 32, cudaMemcpyDeviceToHost, st));
+      MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
       MSG_CUDA(ctx, cudaStreamSynchronize(st));
       float ms = 0.f;
       cudaEventElapsedTime(&ms, ev[0], ev[1]);
@@ -761,7 +977,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     count_launch(ctx, 5 * chunk);
     total_inner += chunk;
     cudaEventRecord(ev[3], st);
-    MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 32, cudaMemcpyDeviceToHost, st));
+    MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     float ms = 0.f, op_ms = 0.f, up_ms = 0.f;
     cudaEventElapsedTime(&ms, ev[2], ev[3]);
@@ -774,6 +990,10 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     }
     cudaGetLastError();
     // a realization that stopped iterating (breakdown) or asks for a check triggers an update
+    if (h_flags[8]) {
+      status = set_error(ctx, MSG_ERR_TIMEOUT, "a bounded wait of the staged operator expired");
+      break;
+    }
     need_update = (h_flags[4] > 0) || (h_flags[0] == 0);
   }
   cudaFreeHost(h_flags);
