@@ -793,21 +793,25 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   }
   const double kdiag = K576[0];
 
-  DevMem x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;
-  MSG_TRY(x.alloc(ctx, sizeof(double) * nvec));
-  MSG_TRY(r32.alloc(ctx, sizeof(float) * nvec));
-  MSG_TRY(p.alloc(ctx, sizeof(float) * nvec));
-  MSG_TRY(q.alloc(ctx, sizeof(float) * nvec));
-  MSG_TRY(d.alloc(ctx, sizeof(float) * nvec));
-  MSG_TRY(dinv.alloc(ctx, sizeof(float) * npad * Rp));
-  MSG_TRY(E64.alloc(ctx, sizeof(double) * npad * Rp));
-  MSG_TRY(E32.alloc(ctx, sizeof(float) * npad * Rp));
-  MSG_TRY(blat.alloc(ctx, sizeof(double) * npad * 3));
+  // workspace of the batch (context slots 0-11, reused by the next batch)
+  struct WS {
+    void* ptr = nullptr;
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+  } x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;
+  MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &x.ptr));
+  MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &r32.ptr));
+  MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &p.ptr));
+  MSG_TRY(workspace(ctx, 3, sizeof(float) * nvec, &q.ptr));
+  MSG_TRY(workspace(ctx, 4, sizeof(float) * nvec, &d.ptr));
+  MSG_TRY(workspace(ctx, 5, sizeof(float) * npad * Rp, &dinv.ptr));
+  MSG_TRY(workspace(ctx, 6, sizeof(double) * npad * Rp, &E64.ptr));
+  MSG_TRY(workspace(ctx, 7, sizeof(float) * npad * Rp, &E32.ptr));
+  MSG_TRY(workspace(ctx, 8, sizeof(double) * npad * 3, &blat.ptr));
   const int n_upd = std::min(L.n_int, ctx->sm_count * 4);
-  MSG_TRY(part_op.alloc(ctx, sizeof(double) * (size_t)n_tiles * Rp * 2));
-  MSG_TRY(part_up.alloc(ctx, sizeof(double) * (size_t)n_upd * Rp * 2));
+  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)n_tiles * Rp * 2, &part_op.ptr));
+  MSG_TRY(workspace(ctx, 10, sizeof(double) * (size_t)n_upd * Rp * 2, &part_up.ptr));
   const size_t scal_bytes = (sizeof(float) * 2 + sizeof(double) * 5 + sizeof(int) * 4) * (size_t)Rp + 64;
-  MSG_TRY(scal.alloc(ctx, scal_bytes));
+  MSG_TRY(workspace(ctx, 11, scal_bytes, &scal.ptr));
   MSG_CUDA(ctx, cudaMemsetAsync(scal.ptr, 0, scal_bytes, st));
   Scal s;
   {

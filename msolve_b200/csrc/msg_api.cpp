@@ -62,6 +62,22 @@ Matrix::~Matrix() {
   if (graph) cudaGraphExecDestroy(graph);
 }
 
+Context::~Context() {
+  for (auto& w : work) {
+    delete w;
+    w = nullptr;
+  }
+}
+
+int workspace(Context* ctx, int slot, size_t bytes, void** out) {
+  if (slot < 0 || slot >= 32) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "workspace slot");
+  DevMem*& w = ctx->work[slot];
+  if (!w) w = new DevMem();
+  if (w->bytes < bytes) MSG_TRY(w->alloc(ctx, bytes));
+  *out = w->ptr;
+  return MSG_OK;
+}
+
 void retain(Context* ctx) { ctx->refs++; }
 
 void release(Context* ctx) {
@@ -756,15 +772,17 @@ int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const dou
   if (!m || !kl || !xi || !b || R <= 0) return MSG_ERR_INVALID_ARGUMENT;
   Context* ctx = m->ctx;
   CTX_GUARD(ctx);
-  DevMem dxi, db, dX;
-  MSG_TRY(upload(ctx, dxi, xi, (size_t)R * kl->n_terms));
-  MSG_TRY(upload(ctx, db, b, (size_t)m->n_dofs));
-  if (X) MSG_TRY(dX.alloc(ctx, sizeof(double) * (size_t)R * m->n_dofs));
-  int st = mc_batch(ctx, m, nu, kl, R, dxi.as<double>(), db.as<double>(), mode, max_it, tol, tip_dof,
-                    X ? dX.as<double>() : nullptr, tip, iterations, rel_res);
+  // staging buffers kept in the context (slots 12-14) across calls
+  void *dxi = nullptr, *db = nullptr, *dX = nullptr;
+  MSG_TRY(workspace(ctx, 12, sizeof(double) * (size_t)R * kl->n_terms, &dxi));
+  MSG_TRY(workspace(ctx, 13, sizeof(double) * (size_t)std::max(1, m->n_dofs), &db));
+  if (X) MSG_TRY(workspace(ctx, 14, sizeof(double) * (size_t)R * m->n_dofs, &dX));
+  MSG_CUDA(ctx, cudaMemcpyAsync(dxi, xi, sizeof(double) * (size_t)R * kl->n_terms, cudaMemcpyHostToDevice, ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(db, b, sizeof(double) * (size_t)m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
+  int st = mc_batch(ctx, m, nu, kl, R, static_cast<double*>(dxi), static_cast<double*>(db), mode, max_it, tol, tip_dof,
+                    X ? static_cast<double*>(dX) : nullptr, tip, iterations, rel_res);
   if (X && (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED)) {
-    MSG_CUDA(ctx, cudaMemcpyAsync(X, dX.ptr, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost,
-                                  ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(X, dX, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return st;

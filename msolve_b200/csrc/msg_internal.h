@@ -66,7 +66,15 @@ struct Context {
   // mixed-solver tunables (MSG_SET_OPTION)
   double reliable_delta = 0.1;  // FP64 residual replacement when ||r|| drops by this factor
   int chunk = 16;               // inner iterations per captured graph launch
+  // Workspace kept across calls (allocation and cudaFree synchronise the
+  // device; a batch reuses the previous batch's buffers when they are large
+  // enough). Slots are owned by the call sites that use them.
+  DevMem* work[32] = {nullptr};
+  ~Context();
 };
+
+// Workspace slot `slot` of at least `bytes` bytes (grown, never shrunk).
+int workspace(Context* ctx, int slot, size_t bytes, void** out);
 
 void retain(Context* ctx);
 void release(Context* ctx);
