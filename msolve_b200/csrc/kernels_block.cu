@@ -301,25 +301,26 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, in
       : "memory");
 }
 
-__global__ void __launch_bounds__(128, 4)
+constexpr int kOpThreads = 32 * (kWarps + 1);  // 4 consumer warps + 1 TMA producer warp
+
+__global__ void __launch_bounds__(kOpThreads, 4)
     k_op_tma(Lattice L, const __grid_constant__ KhatF K, const __grid_constant__ CUtensorMap tm_p,
-             const __grid_constant__ CUtensorMap tm_e, const float* __restrict__ p, const uint8_t* __restrict__ mask,
-             float* __restrict__ q, double* __restrict__ partial, int* __restrict__ err) {
-  extern __shared__ unsigned char smem_raw[];
-  // 128-byte aligned stage ring (TMA destinations), then the mbarriers
-  float* smem = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+             const __grid_constant__ CUtensorMap tm_e, const uint8_t* __restrict__ mask, float* __restrict__ q,
+             double* __restrict__ partial, int* __restrict__ err) {
+  extern __shared__ __align__(128) float smem_dyn[];
+  // 128-byte aligned stage ring (TMA destinations), then the mbarriers; the
+  // offset is applied to the shared-memory pointer so reads stay in the shared space
+  float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageFloats);
   uint64_t* empty = full + kStages;
-  const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+  __shared__ double red[kWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int tile = blockIdx.x;
   const int tj = tile % L.tiles_j, tk = tile / L.tiles_j;
-  const int J0 = 1 + tj * kTJ, K0 = 1 + tk * kTK;   // padded coordinates of the tile's first pencil
-  const int jy = w % kTJ, kz = w / kTJ;
-  const int J = J0 + jy, Kz = K0 + kz;
-  const bool valid = J <= L.NY && Kz <= L.NZ;
+  const int J0 = 1 + tj * kTJ, K0 = 1 + tk * kTK;  // padded coordinates of the tile's first pencil
   const int Rp = L.Rp, g32 = blockIdx.y * 32, rr = g32 + lane;
   const int NX = L.NX;
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     for (int st = 0; st < kStages; ++st) {
       mbar_init(&full[st], 1);
       mbar_init(&empty[st], kWarps);
@@ -327,93 +328,100 @@ __global__ void __launch_bounds__(128, 4)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  auto issue = [&](int P) {  // plane P into stage (P-1) % kStages
-    const int st = (P - 1) % kStages;
-    float* dst = smem + st * kStageFloats;
-    mbar_expect_tx(&full[st], kStageBytes);
-    tma_load_5d(dst, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
-    tma_load_4d(dst + kPlaneFloats, &tm_e, g32, P, J0 - 1, K0 - 1, &full[st]);
-  };
-  if (tid == 0)
-    for (int P = 1; P <= NX && P <= kStages; ++P) issue(P);
-
-  float kv[kKhatClasses];
-#pragma unroll
-  for (int i = 0; i < kKhatClasses; ++i) kv[i] = K.v[i];
-  const size_t row0 = (size_t)(J + L.NYp * Kz) * L.NXp;
-  float ym[3] = {0.f, 0.f, 0.f}, y0[3] = {0.f, 0.f, 0.f}, yp[3];
-  float Eprev[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-  float own_m[3] = {0.f, 0.f, 0.f};
-  double pq[1] = {0.0};
-  bool ok = true;
-  auto emit = [&](size_t node, const float* ownv, const float* y) {
-    const uint8_t m = mask[node];
-    float acc = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float qc = ((m >> c) & 1) ? 0.f : y[c];
-      q[(node * 3 + c) * Rp + rr] = qc;
-      acc = fmaf(ownv[c], qc, acc);
+  if (w == kWarps) {
+    // producer warp: plane P into stage (P-1) % kStages once its previous use is consumed
+    if (lane == 0) {
+      for (int P = 1; P <= NX; ++P) {
+        const int st = (P - 1) % kStages, use = (P - 1) / kStages;
+        if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+          atomicExch(err, 1);
+          break;
+        }
+        float* dst = smem + st * kStageFloats;
+        mbar_expect_tx(&full[st], kStageBytes);
+        tma_load_5d(dst, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+        tma_load_4d(dst + kPlaneFloats, &tm_e, g32, P, J0 - 1, K0 - 1, &full[st]);
+      }
     }
-    pq[0] += (double)acc;
-  };
-#pragma unroll 1
-  for (int P = 1; P <= NX; ++P) {
-    // refill the stage consumed one plane ago (the other warps have had a plane to release it)
-    if (tid == 0 && P >= 2 && P - 1 + kStages <= NX) {
-      const int prev = P - 1;
-      if (!mbar_wait(&empty[(prev - 1) % kStages], ((prev - 1) / kStages) & 1)) { atomicExch(err, 1); ok = false; }
-      else issue(prev + kStages);
-    }
-    const int st = (P - 1) % kStages;
-    if (!mbar_wait(&full[st], ((P - 1) / kStages) & 1)) { atomicExch(err, 1); ok = false; }
-    if (!ok) break;
-    const float* pt = smem + st * kStageFloats;
-    const float* et = pt + kPlaneFloats;
-    float pl[3][3][3];
+  } else {
+    const int jy = w % kTJ, kz = w / kTJ;
+    const int J = J0 + jy, Kz = K0 + kz;
+    const bool valid = J <= L.NY && Kz <= L.NZ;
+    float kv[kKhatClasses];
 #pragma unroll
-    for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-      for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) pl[dy][dz][c] = pt[(((kz + dz) * kPJ + (jy + dy)) * 3 + c) * 32 + lane];
-    float Ecur[2][2];
-#pragma unroll
-    for (int ey = 0; ey < 2; ++ey)
-#pragma unroll
-      for (int ez = 0; ez < 2; ++ez) Ecur[ey][ez] = et[((kz + ez) * kEJ + (jy + ey)) * 32 + lane];
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[st]);
-    if (valid) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) yp[c] = 0.f;
-      slab_apply<float, 1, 0>(kv, pl, Ecur, yp);
-      slab_apply<float, 0, 0>(kv, pl, Ecur, y0);
-      slab_apply<float, 1, 1>(kv, pl, Eprev, y0);
-      slab_apply<float, 0, 1>(kv, pl, Eprev, ym);
-      if (P > 1) emit(row0 + P - 1, own_m, ym);
+    for (int i = 0; i < kKhatClasses; ++i) kv[i] = K.v[i];
+    const size_t row0 = (size_t)(J + L.NYp * Kz) * L.NXp;
+    float ym[3] = {0.f, 0.f, 0.f}, y0[3] = {0.f, 0.f, 0.f}, yp[3];
+    float Eprev[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+    float own_m[3] = {0.f, 0.f, 0.f};
+    double pq = 0.0;
+    bool ok = true;
+    auto emit = [&](size_t node, const float* ownv, const float* y) {
+      const uint8_t m = mask[node];
+      float acc = 0.f;
+      float* qn = q + node * 3 * Rp + rr;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        ym[c] = y0[c];
-        y0[c] = yp[c];
-        own_m[c] = pl[1][1][c];
+        const float qc = ((m >> c) & 1) ? 0.f : y[c];
+        qn[c * Rp] = qc;
+        acc = fmaf(ownv[c], qc, acc);
       }
+      pq += (double)acc;
+    };
+#pragma unroll 1
+    for (int P = 1; P <= NX; ++P) {
+      const int st = (P - 1) % kStages;
+      if (!mbar_wait(&full[st], ((P - 1) / kStages) & 1)) {
+        atomicExch(err, 1);
+        ok = false;
+        break;
+      }
+      const float* pt = smem + st * kStageFloats;
+      const float* et = pt + kPlaneFloats;
+      float pl[3][3][3];
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) pl[dy][dz][c] = pt[(((kz + dz) * kPJ + (jy + dy)) * 3 + c) * 32 + lane];
+      float Ecur[2][2];
 #pragma unroll
       for (int ey = 0; ey < 2; ++ey)
 #pragma unroll
-        for (int ez = 0; ez < 2; ++ez) Eprev[ey][ez] = Ecur[ey][ez];
+        for (int ez = 0; ez < 2; ++ez) Ecur[ey][ez] = et[((kz + ez) * kEJ + (jy + ey)) * 32 + lane];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      if (valid) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) yp[c] = 0.f;
+        slab_apply<float, 1, 0>(kv, pl, Ecur, yp);
+        slab_apply<float, 0, 0>(kv, pl, Ecur, y0);
+        slab_apply<float, 1, 1>(kv, pl, Eprev, y0);
+        slab_apply<float, 0, 1>(kv, pl, Eprev, ym);
+        if (P > 1) emit(row0 + P - 1, own_m, ym);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ym[c] = y0[c];
+          y0[c] = yp[c];
+          own_m[c] = pl[1][1][c];
+        }
+#pragma unroll
+        for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+          for (int ez = 0; ez < 2; ++ez) Eprev[ey][ez] = Ecur[ey][ez];
+      }
     }
+    if (ok && valid) emit(row0 + NX, own_m, ym);
+    red[w][lane] = pq;
   }
-  if (ok && valid) emit(row0 + NX, own_m, ym);
-  if (!ok && tid == 0) {
-    // let copies already issued land before the CTA's shared memory goes away (bounded)
-    for (int P = 1; P <= NX; ++P) {
-      const int st = (P - 1) % kStages;
-      if (!mbar_wait(&full[st], ((P - 1) / kStages) & 1)) break;
-    }
+  __syncthreads();  // also keeps the CTA (and its shared memory) alive until every copy has landed
+  if (w == 0) {
+    double s = 0;
+#pragma unroll
+    for (int ww = 0; ww < kWarps; ++ww) s += red[ww][lane];
+    partial[(size_t)tile * Rp + rr] = s;
   }
-  (void)p;
-  cta_partial<1>(pq, partial, blockIdx.x, Rp, rr);
 }
 
 // FP64 true residual: r = b - K x (masked), r32 = (float) r; partials ||r||^2
@@ -757,6 +765,12 @@ __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __re
     b[i] = (float)a[i];
 }
 
+// A context workspace buffer seen through the DevMem-style accessor.
+struct WSlot {
+  void* ptr = nullptr;
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
 }  // namespace
 
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
@@ -794,10 +808,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   const double kdiag = K576[0];
 
   // workspace of the batch (context slots 0-11, reused by the next batch)
-  struct WS {
-    void* ptr = nullptr;
-    template <class T> T* as() const { return static_cast<T*>(ptr); }
-  } x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;
+  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;
   MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &x.ptr));
   MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &r32.ptr));
   MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &p.ptr));
@@ -923,8 +934,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
       if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-      k_op_tma<<<op_grid, op_block, kOpSmem, st>>>(L, KF, tm_p, tm_e, p.as<float>(), mask, q.as<float>(),
-                                                   part_op.as<double>(), s.err);
+      k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, KF, tm_p, tm_e, mask, q.as<float>(), part_op.as<double>(),
+                                                     s.err);
       if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
       k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
       if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
