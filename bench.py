@@ -241,7 +241,7 @@ def main():
     launches0 = ctx.stats()["launches"]
     clocks = Clocks(local)
     clocks.start()
-    lat, iters, resmax = [], [], []
+    lat, iters, resmax, phases = [], [], [], []
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     barrier()
@@ -254,6 +254,9 @@ def main():
         b.record()
         b.synchronize()
         lat.append(a.elapsed_time(b))
+        stp = ctx.stats()
+        phases.append({k: round(stp[k], 1) for k in ("t_field_ms", "t_inner_ms", "t_resid_ms", "t_total_ms")}
+                      | {"reliable_updates": stp["reliable_updates"]})
         iters.append(its_h[:R].copy())
         resmax.append(float(res_h[:R].max()))
     e1.record()
@@ -356,7 +359,9 @@ def main():
                          "update_launch_ms": st["update_launch_ms"], "samples": st["launch_samples"]},
             "cpu_baseline": cpu,
             "clocks": clk,
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "steps": [round(v, 1) for v in lat]},
+            "phases_ms": phases,
             "iterations": {"mean": float(its_all.mean()), "max": int(its_all.max()),
                            "reliable_updates_last_step": st["reliable_updates"]},
             "max_true_rel_residual": max(resmax),

@@ -887,8 +887,9 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   const double delta2 = ctx->reliable_delta * ctx->reliable_delta;
   const double tol2 = 0.25 * tol * tol;  // ask for a check once the recursive residual is at tol/2
 
-  cudaEvent_t ev[8];  // 0-3 host-side phases, 4-7 captured around the first operator / update launch
-  for (auto& e : ev) MSG_CUDA(ctx, cudaEventCreate(&e));
+  // context events: 0-3 host-side phases, 4-7 captured around the first operator / update launch
+  MSG_TRY(context_resources(ctx));
+  cudaEvent_t* ev = ctx->ev;
   float t_resid = 0.f, t_inner = 0.f;
 
   // TMA descriptors of p (5-D: realization, component, x, y, z) and of the
@@ -924,8 +925,30 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   }
 
   const int chunk = std::max(2, ctx->chunk & ~1);
-  cudaGraphExec_t gexec = nullptr;
+  // The inner-loop graph is kept in the context and captured again only when
+  // one of its kernel arguments changes (FNV-1a over the argument bytes).
+  size_t key = 1469598103934665603ull;
+  auto mix = [&key](const void* data, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) key = (key ^ b[i]) * 1099511628211ull;
+  };
   {
+    const void* ptrs[] = {interior, mask, r32.ptr, p.ptr, q.ptr, d.ptr, dinv.ptr, part_op.ptr, part_up.ptr, scal.ptr};
+    mix(ptrs, sizeof(ptrs));
+    mix(&L, sizeof(L));
+    mix(&KF, sizeof(KF));
+    mix(&tm_p, sizeof(tm_p));
+    mix(&tm_e, sizeof(tm_e));
+    const double dd[2] = {delta2, tol2};
+    mix(dd, sizeof(dd));
+    const int ii[6] = {chunk, n_dir, n_upd, n_tiles, sblocks, (int)upd_smem};
+    mix(ii, sizeof(ii));
+  }
+  if (ctx->batch_graph && ctx->batch_graph_key != key) {
+    cudaGraphExecDestroy(ctx->batch_graph);
+    ctx->batch_graph = nullptr;
+  }
+  if (!ctx->batch_graph) {
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < chunk; ++it) {
@@ -947,13 +970,17 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     }
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (e != cudaSuccess) return cuda_error(ctx, e, "capture inner chunk");
-    e = cudaGraphInstantiate(&gexec, g, 0);
+    e = cudaGraphInstantiate(&ctx->batch_graph, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "instantiate inner chunk");
+    if (e != cudaSuccess) {
+      ctx->batch_graph = nullptr;
+      return cuda_error(ctx, e, "instantiate inner chunk");
+    }
+    ctx->batch_graph_key = key;
   }
+  cudaGraphExec_t gexec = ctx->batch_graph;
 
-  int* h_flags = nullptr;  // [0] active, [4] update requests (16-byte apart as in Scal)
-  MSG_CUDA(ctx, cudaMallocHost(&h_flags, 64));
+  int* h_flags = ctx->h_flags;  // [0] active, [4] update requests, [8] wait timeout (pinned, per context)
   int status = MSG_OK;
   int total_inner = 0;
   int n_updates = 0;
@@ -984,11 +1011,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     if (total_inner >= max_it) { status = MSG_ERR_NOT_CONVERGED; break; }
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
-    if (e != cudaSuccess) {
-      cudaFreeHost(h_flags);
-      cudaGraphExecDestroy(gexec);
-      return cuda_error(ctx, e, "inner chunk");
-    }
+    if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
     count_launch(ctx, 5 * chunk);
     total_inner += chunk;
     cudaEventRecord(ev[3], st);
@@ -1011,9 +1034,6 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     }
     need_update = (h_flags[4] > 0) || (h_flags[0] == 0);
   }
-  cudaFreeHost(h_flags);
-  cudaGraphExecDestroy(gexec);
-  for (auto& e : ev) cudaEventDestroy(e);
   ctx->t_phase[1] = t_inner;
   ctx->t_phase[3] = t_resid;
   ctx->t_phase[2] = (double)n_updates;
@@ -1024,13 +1044,13 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     k_gather_solution<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, R, Rp, m->d_pad_free_rows.as<int>(), x.as<double>(), d_X);
     count_launch(ctx);
   }
-  DevMem tipbuf;
+  WSlot tipbuf;
   if (out.tip && tip_dof >= 0 && tip_dof < m->n_dofs) {
     int row = 0;
     MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_pad_free_rows.as<int>() + tip_dof, sizeof(int), cudaMemcpyDeviceToHost,
                                   st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
-    MSG_TRY(tipbuf.alloc(ctx, sizeof(double) * Rp));
+    MSG_TRY(workspace(ctx, 17, sizeof(double) * Rp, &tipbuf.ptr));
     k_gather_tip<<<(R + 127) / 128, 128, 0, st>>>(R, Rp, row, x.as<double>(), tipbuf.as<double>());
     count_launch(ctx);
     MSG_CUDA(ctx, cudaMemcpyAsync(out.tip, tipbuf.ptr, sizeof(double) * R, cudaMemcpyDeviceToHost, st));

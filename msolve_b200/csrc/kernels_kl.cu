@@ -82,18 +82,18 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
     tab[10 * k + 9] = kl->eig[k];
     if (!(kl->eig[k] >= 0)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "KL eigenvalue %d is negative", k);
   }
-  DevMem d_tab;
-  MSG_TRY(d_tab.alloc(ctx, sizeof(double) * tab.size()));
-  MSG_TRY(out->d_psi.alloc(ctx, sizeof(double) * (size_t)K * m->n_elems));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_tab.ptr, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice,
-                                ctx->stream));
+  // table and psi live in context workspace slots 16 and 15 (no per-call allocation)
+  void *d_tab = nullptr, *d_psi = nullptr;
+  MSG_TRY(workspace(ctx, 16, sizeof(double) * tab.size(), &d_tab));
+  MSG_TRY(workspace(ctx, 15, sizeof(double) * (size_t)K * m->n_elems, &d_psi));
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, ctx->stream));
   dim3 grid((m->n_elems + 127) / 128, K);
-  k_kl_psi<<<grid, 128, 0, ctx->stream>>>(m->n_elems, K, m->d_centroid.as<double>(), d_tab.as<double>(),
-                                          kl->domain[0], kl->domain[1], kl->domain[2], kl->sigma,
-                                          out->d_psi.as<double>());
+  out->psi = static_cast<double*>(d_psi);
+  k_kl_psi<<<grid, 128, 0, ctx->stream>>>(m->n_elems, K, m->d_centroid.as<double>(), static_cast<double*>(d_tab),
+                                          kl->domain[0], kl->domain[1], kl->domain[2], kl->sigma, out->psi);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
-  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // d_tab is released on return
+  // the host table is staged synchronously by the pageable copy; nothing to wait for
   out->n_terms = K;
   out->mu = std::log(kl->mean) - (kl->mean_correction ? 0.5 * kl->sigma * kl->sigma : 0.0);
   return MSG_OK;
@@ -102,7 +102,7 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
 int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int Rp, const double* d_xi,
                     double* d_E64_er, float* d_E32_er, double* d_E64_re, const int* d_elem_row) {
   dim3 grid((m->n_elems + 31) / 32, Rp / 32);
-  k_kl_field<<<grid, dim3(32, 8), 0, ctx->stream>>>(m->n_elems, kl->n_terms, R, Rp, d_xi, kl->d_psi.as<double>(),
+  k_kl_field<<<grid, dim3(32, 8), 0, ctx->stream>>>(m->n_elems, kl->n_terms, R, Rp, d_xi, kl->psi,
                                                     kl->mu, d_E64_er, d_E32_er, d_E64_re, d_elem_row);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());

@@ -67,6 +67,17 @@ Context::~Context() {
     delete w;
     w = nullptr;
   }
+  if (batch_graph) cudaGraphExecDestroy(batch_graph);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (h_flags) cudaFreeHost(h_flags);
+}
+
+int context_resources(Context* ctx) {
+  if (!ctx->h_flags) MSG_CUDA(ctx, cudaMallocHost(&ctx->h_flags, 64));
+  for (auto& e : ctx->ev)
+    if (!e) MSG_CUDA(ctx, cudaEventCreate(&e));
+  return MSG_OK;
 }
 
 int workspace(Context* ctx, int slot, size_t bytes, void** out) {
@@ -374,9 +385,8 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "MC batch: invalid arguments");
   if (tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
   const int Rp = (R + 31) / 32 * 32;
-  cudaEvent_t e0, e1;
-  MSG_CUDA(ctx, cudaEventCreate(&e0));
-  MSG_CUDA(ctx, cudaEventCreate(&e1));
+  MSG_TRY(context_resources(ctx));
+  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   cudaEventRecord(e0, ctx->stream);
   KLDevice kd;
   MSG_TRY(kl_prepare(ctx, m, kl, &kd));
@@ -428,8 +438,6 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   ctx->t_phase[4] = ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   return status;
 }
 

@@ -70,8 +70,16 @@ struct Context {
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
   DevMem* work[32] = {nullptr};
+  // per-context host/driver resources reused by every batch (created lazily)
+  int* h_flags = nullptr;           // 64 bytes of pinned host memory
+  cudaEvent_t ev[12] = {nullptr};   // timing events
+  cudaGraphExec_t batch_graph = nullptr;  // inner-loop graph of the last batch configuration
+  size_t batch_graph_key = 0;
   ~Context();
 };
+
+// Lazily created pinned flags and events of a context.
+int context_resources(Context* ctx);
 
 // Workspace slot `slot` of at least `bytes` bytes (grown, never shrunk).
 int workspace(Context* ctx, int slot, size_t bytes, void** out);
@@ -184,7 +192,7 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b_node, double* d_
 // KL field: E64/E32 [n_elems][Rp] (realization innermost) and/or E64 [R][n_elems].
 struct KLDevice {
   int n_terms = 0;
-  DevMem d_psi;   // [K][n_elems]
+  double* psi = nullptr;  // [K][n_elems], context workspace slot 15
   double mu = 0;
 };
 int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out);
