@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--reliable-delta", type=float, default=None, help="MSG_SET_OPTION reliable_delta")
     p.add_argument("--chunk", type=int, default=None, help="MSG_SET_OPTION chunk")
+    p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
+                   help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
 
 
@@ -203,6 +205,8 @@ def main():
         ctx.set_option("reliable_delta", args.reliable_delta)
     if args.chunk is not None:
         ctx.set_option("chunk", args.chunk)
+    if args.modal_operator is not None:
+        ctx.set_option("modal_operator", args.modal_operator)
     model, kl = make_problem(args)
     mesh = M.GpuMesh(ctx, model)
     R, K_terms = args.R, args.terms

@@ -195,7 +195,8 @@ int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R,
 /* Tunables of the mixed solver on this context: "reliable_delta" (the FP32
  * recursive residual may fall by this factor before it is replaced by the FP64
  * true residual, default 0.1), "chunk" (FP32 iterations per CUDA-graph launch,
- * even, default 16). */
+ * even, default 16), "modal_operator" (1: the FP32 operator works on the
+ * element's Walsh modes, default; 0: dense value-class stencil). */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 
 /* Kernel launch counter of this context (kernels launched since creation),

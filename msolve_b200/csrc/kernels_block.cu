@@ -424,6 +424,334 @@ __global__ void __launch_bounds__(kOpThreads, 4)
   }
 }
 
+// ---------------------------------------------------------------- modal FP32 operator
+// The element matrices of a cube are nearly diagonal in the element's Walsh
+// modes. With the corner coordinates a = (ax, ay, az) in {0,1}^3 and the mode
+// bits m = (mx, my, mz), s(a, m) = prod_d (2 a_d - 1)^{m_d} and T = s (x) I3
+// (T T^T = 8 I), Km = T^T Khat T has 45 non-zeros in nine blocks (the rigid
+// translations m = 0 are its null space):
+//   V  {(1,x) (2,y) (4,z)}           [[a b b] [b a b] [b b a]]  (volumetric)
+//   S  {(1,y) (2,x)} {(1,z) (4,x)} {(2,z) (4,y)}   [[a b] [b a]]  (linear shear)
+//   P  {(3,x) (6,z)} {(3,y) (5,z)} {(5,x) (6,y)}   [[a b] [b a]]
+//   T  {(3,z) (5,y) (6,x)}           [[a b b] [b a b] [b b a]]
+//   D  (7,x) (7,y) (7,z)             a
+// (mode m = mx + 2 my + 4 mz, component). The consistent mass is diagonal in
+// the same modes. So Khat u = T (Km / 64) T^T u: the +-1 transforms factor
+// per axis (sum and difference of two values), and the yz part of a plane
+// is shared by the elements on both sides of it along x.
+//
+// A CTA owns a 4 x 4 tile of node pencils for 32 realizations and runs one
+// warp per element pencil of the 5 x 5 that touch it (the tile's own
+// elements plus one halo row and column below; the 9 halo pencils are also
+// computed by the neighbouring CTA). Per x-plane P every element warp turns
+// its 4 plane nodes into 4 yz-modes per component, combines them with the
+// previous plane's modes into the element's 24 modes, applies the blocks,
+// and folds the result back onto the yz-modes of planes P-1 and P; the P-1
+// part completes that plane and goes back to its 4 corner nodes. The corner
+// contributions meet in a shared-memory exchange buffer, where the warp that
+// owns node pencil (J, K) sums the four elements around it in fixed order,
+// so results stay deterministic. About 150 FP32 operations per element and
+// plane instead of the 576 FMAs of a dense Khat row block per node.
+//
+// The kernel is persistent (one CTA per SM walks work items, a tile and a
+// realization group each), with a dedicated TMA producer warp filling the
+// same 4-stage mbarrier ring as the dense operator, and an mbarrier (bounded
+// waits, like every other wait here) in place of a CTA barrier between the
+// element and node phases of a plane.
+struct ModalC {
+  float vd, vb;  // V: a - b, b
+  float sa, sb;  // S: a, b
+  float pa, pb;  // P: a, b
+  float td, tb;  // T: a - b, b
+  float da;      // D
+  float m[8];    // mass per mode (0 when no mass term)
+};
+
+constexpr int kMJ = 4, kMK = 4;                       // node pencils per tile
+constexpr int kMEJ = kMJ + 1, kMEK = kMK + 1;         // element pencils per tile
+constexpr int kMWarps = kMEJ * kMEK;                  // 25 element warps
+constexpr int kMPJ = kMJ + 2, kMPK = kMK + 2;         // node patch per plane
+constexpr int kMPlaneFloats = 32 * 3 * kMPJ * kMPK;   // 3456
+constexpr int kMEFloats = 32 * kMEJ * kMEK;           // 800
+constexpr int kMStageFloats = kMPlaneFloats + kMEFloats;  // 17,024 bytes, a multiple of 128
+constexpr uint32_t kMStageBytes = kMStageFloats * 4;
+constexpr int kMStages = 4;
+constexpr int kMXFloats = kMWarps * 4 * 3 * 32;       // exchange buffer: element x corner x component x lane
+constexpr int kMThreads = 32 * (kMWarps + 1);         // + 1 TMA producer warp
+constexpr size_t kMSmem = 128 + sizeof(float) * ((size_t)kMStages * kMStageFloats + 2 * (size_t)kMXFloats) +
+                          sizeof(double) * 16 * 32 + sizeof(uint64_t) * (2 * kMStages + 1);
+
+// yz transform of one plane's 4 nodes u[ay][az] into the modes B[my + 2 mz]
+__device__ __forceinline__ void yz_forward(const float (&u)[2][2][3], float (&B)[3][4]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float z00 = u[0][0][c] + u[0][1][c], z01 = u[0][1][c] - u[0][0][c];
+    const float z10 = u[1][0][c] + u[1][1][c], z11 = u[1][1][c] - u[1][0][c];
+    B[c][0] = z00 + z10;
+    B[c][1] = z10 - z00;
+    B[c][2] = z01 + z11;
+    B[c][3] = z11 - z01;
+  }
+}
+
+// inverse of yz_forward up to the factor 4 (the transpose of the same signs)
+__device__ __forceinline__ void yz_inverse(const float (&B)[3][4], float (&y)[2][2][3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float a00 = B[c][0] - B[c][1], a10 = B[c][0] + B[c][1];
+    const float a01 = B[c][2] - B[c][3], a11 = B[c][2] + B[c][3];
+    y[0][0][c] = a00 - a01;
+    y[0][1][c] = a00 + a01;
+    y[1][0][c] = a10 - a11;
+    y[1][1][c] = a10 + a11;
+  }
+}
+
+// One element between planes P-1 (yz-modes Bp) and P (Bc): T0 += the part of
+// E Km/64 u (+ mass) that lands on plane P-1, C1 = the part on plane P, both
+// in yz-modes. y0 / y1 hold the element modes with mx = 0 / 1, as [c][my + 2 mz].
+template <bool kMass>
+__device__ __forceinline__ void modal_apply(const ModalC& C, float E, const float (&Bp)[3][4], const float (&Bc)[3][4],
+                                            float (&T0)[3][4], float (&C1)[3][4]) {
+  float y0[3][4], y1[3][4];
+  auto U0 = [&](int q, int c) { return Bc[c][q] + Bp[c][q]; };
+  auto U1 = [&](int q, int c) { return Bc[c][q] - Bp[c][q]; };
+  const float Evd = E * C.vd, Evb = E * C.vb, Esa = E * C.sa, Esb = E * C.sb;
+  const float Epa = E * C.pa, Epb = E * C.pb, Etd = E * C.td, Etb = E * C.tb, Eda = E * C.da;
+  {  // V
+    const float a = U1(0, 0), b = U0(1, 1), c = U0(2, 2);
+    const float t = Evb * (a + b + c);
+    y1[0][0] = fmaf(Evd, a, t);
+    y0[1][1] = fmaf(Evd, b, t);
+    y0[2][2] = fmaf(Evd, c, t);
+  }
+  {  // S
+    float a = U1(0, 1), b = U0(1, 0);
+    y1[1][0] = fmaf(Esa, a, Esb * b);
+    y0[0][1] = fmaf(Esa, b, Esb * a);
+    a = U1(0, 2), b = U0(2, 0);
+    y1[2][0] = fmaf(Esa, a, Esb * b);
+    y0[0][2] = fmaf(Esa, b, Esb * a);
+    a = U0(1, 2), b = U0(2, 1);
+    y0[2][1] = fmaf(Esa, a, Esb * b);
+    y0[1][2] = fmaf(Esa, b, Esb * a);
+  }
+  {  // P
+    float a = U1(1, 0), b = U0(3, 2);
+    y1[0][1] = fmaf(Epa, a, Epb * b);
+    y0[2][3] = fmaf(Epa, b, Epb * a);
+    a = U1(1, 1), b = U1(2, 2);
+    y1[1][1] = fmaf(Epa, a, Epb * b);
+    y1[2][2] = fmaf(Epa, b, Epb * a);
+    a = U1(2, 0), b = U0(3, 1);
+    y1[0][2] = fmaf(Epa, a, Epb * b);
+    y0[1][3] = fmaf(Epa, b, Epb * a);
+  }
+  {  // T
+    const float a = U1(1, 2), b = U1(2, 1), c = U0(3, 0);
+    const float t = Etb * (a + b + c);
+    y1[2][1] = fmaf(Etd, a, t);
+    y1[1][2] = fmaf(Etd, b, t);
+    y0[0][3] = fmaf(Etd, c, t);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {  // D and the null modes
+    y1[c][3] = Eda * U1(3, c);
+    y0[c][0] = 0.f;
+  }
+  if constexpr (kMass) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        y0[c][q] = fmaf(C.m[2 * q], U0(q, c), y0[c][q]);
+        y1[c][q] = fmaf(C.m[2 * q + 1], U1(q, c), y1[c][q]);
+      }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      T0[c][q] = (T0[c][q] + y0[c][q]) - y1[c][q];
+      C1[c][q] = y0[c][q] + y1[c][q];
+    }
+}
+
+template <bool kMass>
+__global__ void __launch_bounds__(kMThreads, 1)
+    k_op_modal(Lattice L, const __grid_constant__ ModalC C, const __grid_constant__ CUtensorMap tm_p,
+               const __grid_constant__ CUtensorMap tm_e, int tiles_j, int n_tiles, int n_items,
+               const uint8_t* __restrict__ mask, float* __restrict__ q, double* __restrict__ partial,
+               int* __restrict__ err) {
+  extern __shared__ __align__(128) float smem_dyn[];
+  float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
+  float* xbuf = smem + kMStages * kMStageFloats;                            // 2 exchange buffers
+  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);            // [16][32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + 16 * 32);
+  uint64_t* empty = full + kMStages;
+  uint64_t* cbar = empty + kMStages;                                        // consumer barrier
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int NX = L.NX, Rp = L.Rp;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kMStages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kMWarps);
+    }
+    mbar_init(cbar, kMWarps);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (w == kMWarps) {
+    // producer: plane P of every work item, in the consumers' order
+    if (lane == 0) {
+      uint32_t seq = 0;
+      for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+        const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
+        for (int P = 1; P <= NX; ++P, ++seq) {
+          const int st = seq % kMStages;
+          const uint32_t use = seq / kMStages;
+          if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+            atomicExch(err, 1);
+            return;
+          }
+          float* dst = smem + st * kMStageFloats;
+          mbar_expect_tx(&full[st], kMStageBytes);
+          tma_load_5d(dst, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_4d(dst + kMPlaneFloats, &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+        }
+      }
+    }
+    return;
+  }
+  const int ej = w % kMEJ, ek = w / kMEJ;
+  const bool node_warp = ej >= 1 && ek >= 1;
+  uint32_t seq = 0, cphase = 0;
+  int xsel = 0;
+  // consumer barrier between the element and the node phase of a plane
+  auto csync = [&]() -> bool {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(cbar);
+    const bool ok = mbar_wait(cbar, cphase & 1);
+    ++cphase;
+    return ok;
+  };
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+    const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
+    const int Je = J0 - 1 + ej, Ke = K0 - 1 + ek;  // element pencil (lower corner), padded
+    // real elements have lower corners 1..NY-1 (1..NZ-1); others are ghosts
+    auto realj = [&](int j) { return j >= 1 && j <= L.NY - 1; };
+    auto realk = [&](int k) { return k >= 1 && k <= L.NZ - 1; };
+    const bool real = realj(Je) && realk(Ke);
+    const bool node_ok = node_warp && Je <= L.NY && Ke <= L.NZ;
+    const bool r00 = realj(Je) && realk(Ke), r10 = realj(Je - 1) && realk(Ke);
+    const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
+    const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;  // padded node (0, Je, Ke)
+    const int rr = g32 + lane;
+    float Bp[3][4], T0[3][4], own[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      own[c] = 0.f;
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) T0[c][qq] = 0.f;
+    }
+    double pq = 0.0;
+    // node phase of plane X: sum the corner contributions of the 4 elements
+    auto node_phase = [&](int X) {
+      const float* xb = xbuf + xsel * kMXFloats;
+      const size_t node = nrow + X;
+      const uint8_t mk = mask[node];
+      float acc = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float y = 0.f;
+        if (r00) y += xb[((w * 4 + 0) * 3 + c) * 32 + lane];
+        if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
+        if (r01) y += xb[(((w - kMEJ) * 4 + 2) * 3 + c) * 32 + lane];
+        if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        const float qc = ((mk >> c) & 1) ? 0.f : y;
+        q[(node * 3 + c) * Rp + rr] = qc;
+        acc = fmaf(own[c], qc, acc);
+      }
+      pq += (double)acc;
+    };
+    auto emit_corners = [&](const float (&B)[3][4]) {
+      float y[2][2][3];
+      yz_inverse(B, y);
+      float* xb = xbuf + xsel * kMXFloats;
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
+    };
+    for (int P = 1; P <= NX; ++P, ++seq) {
+      const int st = seq % kMStages;
+      if (!mbar_wait(&full[st], (seq / kMStages) & 1)) {
+        atomicExch(err, 1);
+        return;
+      }
+      const float* pt = smem + st * kMStageFloats;
+      float u[2][2][3];
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) u[ay][az][c] = pt[(((ek + az) * kMPJ + (ej + ay)) * 3 + c) * 32 + lane];
+      const float E = pt[kMPlaneFloats + w * 32 + lane];  // element (P-1, Je, Ke)
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      float Bc[3][4];
+      yz_forward(u, Bc);
+      if (P >= 2) {
+        if (real) {
+          float C1[3][4];
+          modal_apply<kMass>(C, E, Bp, Bc, T0, C1);
+          emit_corners(T0);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
+        }
+        if (!csync()) {
+          atomicExch(err, 1);
+          return;
+        }
+        if (node_ok) node_phase(P - 1);
+        xsel ^= 1;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        own[c] = u[0][0][c];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) Bp[c][qq] = Bc[c][qq];
+      }
+    }
+    // plane NX: the slab above it is a ghost, so the pending part is complete
+    if (real) emit_corners(T0);
+    if (!csync()) {
+      atomicExch(err, 1);
+      return;
+    }
+    if (node_ok) node_phase(NX);
+    xsel ^= 1;
+    if (node_warp) red[((ek - 1) * kMJ + (ej - 1)) * 32 + lane] = pq;
+    if (!csync()) {
+      atomicExch(err, 1);
+      return;
+    }
+    if (w == 0) {
+      double s = 0.0;
+#pragma unroll
+      for (int i = 0; i < kMJ * kMK; ++i) s += red[i * 32 + lane];
+      partial[(size_t)tile * Rp + rr] = s;
+    }
+  }
+}
+
 // FP64 true residual: r = b - K x (masked), r32 = (float) r; partials ||r||^2
 // and (dinv r32).r32.
 __global__ void __launch_bounds__(128)
@@ -765,6 +1093,89 @@ __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __re
     b[i] = (float)a[i];
 }
 
+// Walsh-mode form of a cube's element matrices (host, FP64): Km = T^T K T with
+// T = s (x) I3. Fills the block coefficients of cK * Khat / 64 (and the
+// diagonal of cM * Mhat / 64 when M576 is given) and checks that every other
+// entry vanishes, so the modal operator reproduces the element matrices.
+int modal_coefficients(Context* ctx, const double* K576, const double* M576, double cK, double cM, ModalC* out) {
+  auto sgn = [](int a, int m) {  // s(a, m) for corner id a and mode m
+    const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
+    int s = 1;
+    if ((m & 1) && !ax) s = -s;
+    if ((m & 2) && !ay) s = -s;
+    if ((m & 4) && !az) s = -s;
+    return s;
+  };
+  auto to_modal = [&](const double* A, std::vector<double>& Am) {
+    Am.assign(576, 0.0);
+    for (int m = 0; m < 8; ++m)
+      for (int c = 0; c < 3; ++c)
+        for (int m2 = 0; m2 < 8; ++m2)
+          for (int c2 = 0; c2 < 3; ++c2) {
+            double s = 0;
+            for (int a = 0; a < 8; ++a)
+              for (int b = 0; b < 8; ++b) s += sgn(a, m) * sgn(b, m2) * A[(3 * a + c) * 24 + 3 * b + c2];
+            Am[(3 * m + c) * 24 + 3 * m2 + c2] = s;
+          }
+  };
+  std::vector<double> Km;
+  to_modal(K576, Km);
+  auto at = [&](int m, int c, int m2, int c2) { return Km[(3 * m + c) * 24 + 3 * m2 + c2]; };
+  const double va = at(1, 0, 1, 0), vb = at(1, 0, 2, 1), sa = at(1, 1, 1, 1), sb = at(1, 1, 2, 0);
+  const double pa = at(3, 0, 3, 0), pb = at(3, 0, 6, 2), ta = at(3, 2, 3, 2), tb = at(3, 2, 5, 1);
+  const double da = at(7, 0, 7, 0);
+  // rebuild Km from the nine blocks
+  std::vector<double> R(576, 0.0);
+  auto put_block = [&](std::initializer_list<std::pair<int, int>> dofs, double a, double b) {
+    for (auto i : dofs)
+      for (auto j : dofs) R[(3 * i.first + i.second) * 24 + 3 * j.first + j.second] = (i == j) ? a : b;
+  };
+  put_block({{1, 0}, {2, 1}, {4, 2}}, va, vb);
+  put_block({{1, 1}, {2, 0}}, sa, sb);
+  put_block({{1, 2}, {4, 0}}, sa, sb);
+  put_block({{2, 2}, {4, 1}}, sa, sb);
+  put_block({{3, 0}, {6, 2}}, pa, pb);
+  put_block({{3, 1}, {5, 2}}, pa, pb);
+  put_block({{5, 0}, {6, 1}}, pa, pb);
+  put_block({{3, 2}, {5, 1}, {6, 0}}, ta, tb);
+  put_block({{7, 0}}, da, 0.0);
+  put_block({{7, 1}}, da, 0.0);
+  put_block({{7, 2}}, da, 0.0);
+  double kmax = 0, dev = 0;
+  for (int i = 0; i < 576; ++i) {
+    kmax = std::max(kmax, std::fabs(Km[i]));
+    dev = std::max(dev, std::fabs(Km[i] - R[i]));
+  }
+  if (!(dev <= 1e-11 * kmax))
+    return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element stiffness lacks the cube's modal structure (%g)", dev / kmax);
+  const double f = cK / 64.0;
+  out->vd = (float)((va - vb) * f);
+  out->vb = (float)(vb * f);
+  out->sa = (float)(sa * f);
+  out->sb = (float)(sb * f);
+  out->pa = (float)(pa * f);
+  out->pb = (float)(pb * f);
+  out->td = (float)((ta - tb) * f);
+  out->tb = (float)(tb * f);
+  out->da = (float)(da * f);
+  for (int m = 0; m < 8; ++m) out->m[m] = 0.f;
+  if (M576) {
+    std::vector<double> Mm;
+    to_modal(M576, Mm);
+    double mmax = 0, mdev = 0;
+    for (int i = 0; i < 576; ++i) mmax = std::max(mmax, std::fabs(Mm[i]));
+    for (int i = 0; i < 24; ++i)
+      for (int j = 0; j < 24; ++j) {
+        const double expect = (i == j) ? Mm[(3 * (i / 3)) * 24 + 3 * (i / 3)] : 0.0;
+        mdev = std::max(mdev, std::fabs(Mm[i * 24 + j] - expect));
+      }
+    if (!(mdev <= 1e-11 * mmax))
+      return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element mass lacks the cube's modal structure (%g)", mdev / mmax);
+    for (int m = 0; m < 8; ++m) out->m[m] = (float)(Mm[(3 * m) * 24 + 3 * m] * cM / 64.0);
+  }
+  return MSG_OK;
+}
+
 // A context workspace buffer seen through the DevMem-style accessor.
 struct WSlot {
   void* ptr = nullptr;
@@ -806,6 +1217,14 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element stiffness does not have the unit-cube structure");
   }
   const double kdiag = K576[0];
+  const bool modal = ctx->modal != 0;
+  ModalC MC{};
+  if (modal) MSG_TRY(modal_coefficients(ctx, K576, nullptr, 1.0, 0.0, &MC));
+  // modal operator: 4 x 4 node tiles, persistent CTAs over (tile, realization group) items
+  const int tiles_jm = (L.NY + kMJ - 1) / kMJ, n_tiles_m = tiles_jm * ((L.NZ + kMK - 1) / kMK);
+  const int n_items_m = n_tiles_m * (Rp / 32);
+  const int grid_m = std::min(n_items_m, ctx->sm_count);
+  const int n_tiles_op = modal ? n_tiles_m : n_tiles;
 
   // workspace of the batch (context slots 0-11, reused by the next batch)
   WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;
@@ -819,7 +1238,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   MSG_TRY(workspace(ctx, 7, sizeof(float) * npad * Rp, &E32.ptr));
   MSG_TRY(workspace(ctx, 8, sizeof(double) * npad * 3, &blat.ptr));
   const int n_upd = std::min(L.n_int, ctx->sm_count * 4);
-  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)n_tiles * Rp * 2, &part_op.ptr));
+  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)std::max(n_tiles, n_tiles_m) * Rp * 2, &part_op.ptr));
   MSG_TRY(workspace(ctx, 10, sizeof(double) * (size_t)n_upd * Rp * 2, &part_up.ptr));
   const size_t scal_bytes = (sizeof(float) * 2 + sizeof(double) * 5 + sizeof(int) * 4) * (size_t)Rp + 64;
   MSG_TRY(workspace(ctx, 11, scal_bytes, &scal.ptr));
@@ -894,7 +1313,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
 
   // TMA descriptors of p (5-D: realization, component, x, y, z) and of the
   // FP32 element field (4-D: realization, x, y, z) for the staged operator
-  CUtensorMap tm_p, tm_e;
+  CUtensorMap tm_p, tm_e, tm_pm, tm_em;
   {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
@@ -920,8 +1339,25 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     CUresult e2 = encode(&tm_e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, E32.ptr, ed, es, eb, one,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (e1 != CUDA_SUCCESS || e2 != CUDA_SUCCESS)
-      return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d, %d)", (int)e1, (int)e2);
+    const cuuint32_t pbm[5] = {32, 3, 1, kMPJ, kMPK};
+    const cuuint32_t ebm[4] = {32, 1, kMEJ, kMEK};
+    CUresult e3 = encode(&tm_pm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, p.ptr, pd, ps, pbm, one,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult e4 = encode(&tm_em, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, E32.ptr, ed, es, ebm, one,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (e1 != CUDA_SUCCESS || e2 != CUDA_SUCCESS || e3 != CUDA_SUCCESS || e4 != CUDA_SUCCESS)
+      return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d, %d, %d, %d)", (int)e1, (int)e2, (int)e3,
+                       (int)e4);
+  }
+  if (modal) {
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+      attr_err = cudaFuncSetAttribute(k_op_modal<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMSmem);
+    });
+    MSG_CUDA(ctx, attr_err);
   }
 
   const int chunk = std::max(2, ctx->chunk & ~1);
@@ -939,6 +1375,11 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     mix(&KF, sizeof(KF));
     mix(&tm_p, sizeof(tm_p));
     mix(&tm_e, sizeof(tm_e));
+    mix(&tm_pm, sizeof(tm_pm));
+    mix(&tm_em, sizeof(tm_em));
+    mix(&MC, sizeof(MC));
+    const int mm[4] = {modal ? 1 : 0, n_tiles_m, n_items_m, grid_m};
+    mix(mm, sizeof(mm));
     const double dd[2] = {delta2, tol2};
     mix(dd, sizeof(dd));
     const int ii[6] = {chunk, n_dir, n_upd, n_tiles, sblocks, (int)upd_smem};
@@ -957,10 +1398,14 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
       if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-      k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, KF, tm_p, tm_e, mask, q.as<float>(), part_op.as<double>(),
-                                                     s.err);
+      if (modal)
+        k_op_modal<false><<<grid_m, kMThreads, kMSmem, st>>>(L, MC, tm_pm, tm_em, tiles_jm, n_tiles_m, n_items_m, mask,
+                                                            q.as<float>(), part_op.as<double>(), s.err);
+      else
+        k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, KF, tm_p, tm_e, mask, q.as<float>(), part_op.as<double>(),
+                                                       s.err);
       if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
-      k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
+      k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles_op, part_op.as<double>(), s);
       if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
       k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, s.alpha, q.as<float>(), r32.as<float>(),
                                              dinv.as<float>(), part_up.as<double>());

@@ -507,6 +507,7 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!key) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "null option key");
   if (!std::strcmp(key, "reliable_delta") && value > 0 && value < 1) { ctx->reliable_delta = value; return MSG_OK; }
   if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
+  if (!std::strcmp(key, "modal_operator") && (value == 0 || value == 1)) { ctx->modal = (int)value; return MSG_OK; }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 

@@ -66,6 +66,7 @@ struct Context {
   // mixed-solver tunables (MSG_SET_OPTION)
   double reliable_delta = 0.1;  // FP64 residual replacement when ||r|| drops by this factor
   int chunk = 16;               // inner iterations per captured graph launch
+  int modal = 1;                // FP32 operator: 1 = Walsh-mode (modal) kernel, 0 = dense value-class kernel
   // Workspace kept across calls (allocation and cudaFree synchronise the
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
