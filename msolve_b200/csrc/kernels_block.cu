@@ -440,9 +440,9 @@ __global__ void __launch_bounds__(kOpThreads, 4)
 // per axis (sum and difference of two values), and the yz part of a plane
 // is shared by the elements on both sides of it along x.
 //
-// A CTA owns a 4 x 4 tile of node pencils for 32 realizations and runs one
-// warp per element pencil of the 5 x 5 that touch it (the tile's own
-// elements plus one halo row and column below; the 9 halo pencils are also
+// A CTA owns a 4 x 3 tile of node pencils for 32 realizations and runs one
+// warp per element pencil of the 5 x 4 that touch it (the tile's own
+// elements plus one halo row and column below; the 8 halo pencils are also
 // computed by the neighbouring CTA). Per x-plane P every element warp turns
 // its 4 plane nodes into 4 yz-modes per component, combines them with the
 // previous plane's modes into the element's 24 modes, applies the blocks,
@@ -451,7 +451,9 @@ __global__ void __launch_bounds__(kOpThreads, 4)
 // contributions meet in a shared-memory exchange buffer, where the warp that
 // owns node pencil (J, K) sums the four elements around it in fixed order,
 // so results stay deterministic. About 150 FP32 operations per element and
-// plane instead of the 576 FMAs of a dense Khat row block per node.
+// plane instead of the 576 FMAs of a dense Khat row block per node. The
+// output is not masked here: constrained components of p are zero, so p.q
+// is unaffected, and k_update leaves the constrained components of r at zero.
 //
 // The kernel is persistent (one CTA per SM walks work items, a tile and a
 // realization group each), with a dedicated TMA producer warp filling the
@@ -467,19 +469,25 @@ struct ModalC {
   float m[8];    // mass per mode (0 when no mass term)
 };
 
-constexpr int kMJ = 4, kMK = 4;                       // node pencils per tile
+constexpr int kMJ = 4, kMK = 3;                       // node pencils per tile
 constexpr int kMEJ = kMJ + 1, kMEK = kMK + 1;         // element pencils per tile
-constexpr int kMWarps = kMEJ * kMEK;                  // 25 element warps
+constexpr int kMWarps = kMEJ * kMEK;                  // 20 element warps (+ 1 producer: 80 registers a thread)
 constexpr int kMPJ = kMJ + 2, kMPK = kMK + 2;         // node patch per plane
-constexpr int kMPlaneFloats = 32 * 3 * kMPJ * kMPK;   // 3456
-constexpr int kMEFloats = 32 * kMEJ * kMEK;           // 800
-constexpr int kMStageFloats = kMPlaneFloats + kMEFloats;  // 17,024 bytes, a multiple of 128
+constexpr int kMPlaneFloats = 32 * 3 * kMPJ * kMPK;   // r or p patch of a plane: 2880
+constexpr int kMNodeFloats = 32 * kMPJ * kMPK;        // dinv patch: 960
+constexpr int kMEFloats = 32 * kMEJ * kMEK;           // E patch: 640
+constexpr int kMDFloats = 32 * 3 * kMJ * kMK;         // d of the tile's own nodes: 1152
+// stage: r | p_{k-1} | dinv | E | d (each patch a multiple of 128 bytes)
+constexpr int kMOffR = 0, kMOffP = kMPlaneFloats, kMOffDinv = 2 * kMPlaneFloats;
+constexpr int kMOffE = kMOffDinv + kMNodeFloats, kMOffD = kMOffE + kMEFloats;
+constexpr int kMStageFloats = kMOffD + kMDFloats;     // 8512 floats, 34,048 bytes
 constexpr uint32_t kMStageBytes = kMStageFloats * 4;
 constexpr int kMStages = 4;
 constexpr int kMXFloats = kMWarps * 4 * 3 * 32;       // exchange buffer: element x corner x component x lane
 constexpr int kMThreads = 32 * (kMWarps + 1);         // + 1 TMA producer warp
 constexpr size_t kMSmem = 128 + sizeof(float) * ((size_t)kMStages * kMStageFloats + 2 * (size_t)kMXFloats) +
-                          sizeof(double) * 16 * 32 + sizeof(uint64_t) * (2 * kMStages + 1);
+                          sizeof(double) * kMJ * kMK * 32 + sizeof(uint64_t) * (2 * kMStages);
+static_assert(kMSmem <= 227 * 1024, "modal operator shared memory");
 
 // yz transform of one plane's 4 nodes u[ay][az] into the modes B[my + 2 mz]
 __device__ __forceinline__ void yz_forward(const float (&u)[2][2][3], float (&B)[3][4]) {
@@ -577,19 +585,26 @@ __device__ __forceinline__ void modal_apply(const ModalC& C, float E, const floa
     }
 }
 
+// The direction update of PCG iteration k (d += alpha_{k-1} p_{k-1},
+// p_k = dinv r_k + beta_k p_{k-1}) is fused into the operator: each stage
+// carries the plane's r, p_{k-1} and dinv patches (and the tile's d), the
+// element warps form p_k at their corners on the fly, and the warp that owns a
+// node pencil writes p_k and d back. p_k goes to the other buffer of a pair
+// (neighbouring CTAs still read p_{k-1} in their halos).
 template <bool kMass>
 __global__ void __launch_bounds__(kMThreads, 1)
-    k_op_modal(Lattice L, const __grid_constant__ ModalC C, const __grid_constant__ CUtensorMap tm_p,
-               const __grid_constant__ CUtensorMap tm_e, int tiles_j, int n_tiles, int n_items,
-               const uint8_t* __restrict__ mask, float* __restrict__ q, double* __restrict__ partial,
+    k_op_modal(Lattice L, const __grid_constant__ ModalC C, const __grid_constant__ CUtensorMap tm_r,
+               const __grid_constant__ CUtensorMap tm_p, const __grid_constant__ CUtensorMap tm_dinv,
+               const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_d, int tiles_j,
+               int n_tiles, int n_items, const float* __restrict__ alpha, const float* __restrict__ beta,
+               float* __restrict__ p_out, float* __restrict__ d, float* __restrict__ q, double* __restrict__ partial,
                int* __restrict__ err) {
   extern __shared__ __align__(128) float smem_dyn[];
   float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
   float* xbuf = smem + kMStages * kMStageFloats;                            // 2 exchange buffers
-  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);            // [16][32]
-  uint64_t* full = reinterpret_cast<uint64_t*>(red + 16 * 32);
+  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);            // [node pencils][32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + kMJ * kMK * 32);
   uint64_t* empty = full + kMStages;
-  uint64_t* cbar = empty + kMStages;                                        // consumer barrier
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int NX = L.NX, Rp = L.Rp;
   if (threadIdx.x == 0) {
@@ -597,7 +612,6 @@ __global__ void __launch_bounds__(kMThreads, 1)
       mbar_init(&full[st], 1);
       mbar_init(&empty[st], kMWarps);
     }
-    mbar_init(cbar, kMWarps);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -617,8 +631,11 @@ __global__ void __launch_bounds__(kMThreads, 1)
           }
           float* dst = smem + st * kMStageFloats;
           mbar_expect_tx(&full[st], kMStageBytes);
-          tma_load_5d(dst, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
-          tma_load_4d(dst + kMPlaneFloats, &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+          tma_load_5d(dst + kMOffR, &tm_r, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_5d(dst + kMOffP, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_4d(dst + kMOffDinv, &tm_dinv, g32, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_4d(dst + kMOffE, &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+          tma_load_5d(dst + kMOffD, &tm_d, g32, 0, P, J0, K0, &full[st]);
         }
       }
     }
@@ -626,16 +643,12 @@ __global__ void __launch_bounds__(kMThreads, 1)
   }
   const int ej = w % kMEJ, ek = w / kMEJ;
   const bool node_warp = ej >= 1 && ek >= 1;
-  uint32_t seq = 0, cphase = 0;
+  uint32_t seq = 0;
   int xsel = 0;
-  // consumer barrier between the element and the node phase of a plane
-  auto csync = [&]() -> bool {
-    __syncwarp();
-    if (lane == 0) mbar_arrive(cbar);
-    const bool ok = mbar_wait(cbar, cphase & 1);
-    ++cphase;
-    return ok;
-  };
+  bool dead = false;  // a stage never arrived: finish the walk without data (err is set)
+  // barrier of the consumer warps between the element and the node phase of a
+  // plane; every consumer warp passes the same sequence of them, error or not
+  auto csync = [&]() { asm volatile("bar.sync 1, %0;" ::"r"(kMWarps * 32) : "memory"); };
   for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
     const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
@@ -645,10 +658,11 @@ __global__ void __launch_bounds__(kMThreads, 1)
     auto realk = [&](int k) { return k >= 1 && k <= L.NZ - 1; };
     const bool real = realj(Je) && realk(Ke);
     const bool node_ok = node_warp && Je <= L.NY && Ke <= L.NZ;
-    const bool r00 = realj(Je) && realk(Ke), r10 = realj(Je - 1) && realk(Ke);
+    const bool r00 = real, r10 = realj(Je - 1) && realk(Ke);
     const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
     const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;  // padded node (0, Je, Ke)
     const int rr = g32 + lane;
+    const float al = alpha[rr], be = beta[rr];
     float Bp[3][4], T0[3][4], own[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -661,7 +675,6 @@ __global__ void __launch_bounds__(kMThreads, 1)
     auto node_phase = [&](int X) {
       const float* xb = xbuf + xsel * kMXFloats;
       const size_t node = nrow + X;
-      const uint8_t mk = mask[node];
       float acc = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -670,9 +683,8 @@ __global__ void __launch_bounds__(kMThreads, 1)
         if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
         if (r01) y += xb[(((w - kMEJ) * 4 + 2) * 3 + c) * 32 + lane];
         if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
-        const float qc = ((mk >> c) & 1) ? 0.f : y;
-        q[(node * 3 + c) * Rp + rr] = qc;
-        acc = fmaf(own[c], qc, acc);
+        q[(node * 3 + c) * Rp + rr] = y;
+        acc = fmaf(own[c], y, acc);
       }
       pq += (double)acc;
     };
@@ -689,19 +701,36 @@ __global__ void __launch_bounds__(kMThreads, 1)
     };
     for (int P = 1; P <= NX; ++P, ++seq) {
       const int st = seq % kMStages;
-      if (!mbar_wait(&full[st], (seq / kMStages) & 1)) {
+      if (!dead && !mbar_wait(&full[st], (seq / kMStages) & 1)) {
         atomicExch(err, 1);
-        return;
+        dead = true;
       }
       const float* pt = smem + st * kMStageFloats;
+      // p_k at the element's 4 plane corners: dinv r + beta p_{k-1}
       float u[2][2][3];
 #pragma unroll
       for (int ay = 0; ay < 2; ++ay)
 #pragma unroll
-        for (int az = 0; az < 2; ++az)
+        for (int az = 0; az < 2; ++az) {
+          const int o = (ek + az) * kMPJ + (ej + ay);
+          const float dv = pt[kMOffDinv + o * 32 + lane];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) u[ay][az][c] = pt[(((ek + az) * kMPJ + (ej + ay)) * 3 + c) * 32 + lane];
-      const float E = pt[kMPlaneFloats + w * 32 + lane];  // element (P-1, Je, Ke)
+          for (int c = 0; c < 3; ++c)
+            u[ay][az][c] = fmaf(dv, pt[kMOffR + (o * 3 + c) * 32 + lane], be * pt[kMOffP + (o * 3 + c) * 32 + lane]);
+        }
+      const float E = pt[kMOffE + w * 32 + lane];  // element (P-1, Je, Ke)
+      if (node_ok) {
+        // the owner writes p_k and d += alpha_{k-1} p_{k-1} of node (P, Je, Ke)
+        const int o = ek * kMPJ + ej, od = (ek - 1) * kMJ + (ej - 1);
+        const size_t node = nrow + P;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float pold = pt[kMOffP + (o * 3 + c) * 32 + lane];
+          const float dn = fmaf(al, pold, pt[kMOffD + (od * 3 + c) * 32 + lane]);
+          p_out[(node * 3 + c) * Rp + rr] = u[0][0][c];
+          d[(node * 3 + c) * Rp + rr] = dn;
+        }
+      }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);
       float Bc[3][4];
@@ -716,10 +745,7 @@ __global__ void __launch_bounds__(kMThreads, 1)
 #pragma unroll
             for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
         }
-        if (!csync()) {
-          atomicExch(err, 1);
-          return;
-        }
+        csync();
         if (node_ok) node_phase(P - 1);
         xsel ^= 1;
       }
@@ -732,17 +758,11 @@ __global__ void __launch_bounds__(kMThreads, 1)
     }
     // plane NX: the slab above it is a ghost, so the pending part is complete
     if (real) emit_corners(T0);
-    if (!csync()) {
-      atomicExch(err, 1);
-      return;
-    }
+    csync();
     if (node_ok) node_phase(NX);
     xsel ^= 1;
     if (node_warp) red[((ek - 1) * kMJ + (ej - 1)) * 32 + lane] = pq;
-    if (!csync()) {
-      atomicExch(err, 1);
-      return;
-    }
+    csync();
     if (w == 0) {
       double s = 0.0;
 #pragma unroll
@@ -850,11 +870,12 @@ __global__ void __launch_bounds__(256) k_dir(int n_int, int Rp, const int* __res
   }
 }
 
-// r -= alpha q; partials (dinv r).r and r.r per realization (interior nodes).
+// r -= alpha q on free components (constrained components of r stay zero);
+// partials (dinv r).r and r.r per realization (interior nodes).
 __global__ void __launch_bounds__(256) k_update(int n_int, int Rp, const int* __restrict__ interior,
-                                                const float* __restrict__ alpha, const float* __restrict__ q,
-                                                float* __restrict__ r, const float* __restrict__ dinv,
-                                                double* __restrict__ partial) {
+                                                const uint8_t* __restrict__ mask, const float* __restrict__ alpha,
+                                                const float* __restrict__ q, float* __restrict__ r,
+                                                const float* __restrict__ dinv, double* __restrict__ partial) {
   Quad qd(Rp);
   const int per = (n_int + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(n_int, t0 + per);
@@ -865,15 +886,18 @@ __global__ void __launch_bounds__(256) k_update(int n_int, int Rp, const int* __
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       for (int t = t0 + qd.g; t < t1; t += qd.G) {
         const size_t n = (size_t)interior[t];
+        const uint8_t mk = mask[n];
         const float4 dv = reinterpret_cast<const float4*>(dinv + n * Rp)[qb];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const size_t o = (n * 3 + c) * Rp;
-          const float4 qv = reinterpret_cast<const float4*>(q + o)[qb];
           float4 rv = reinterpret_cast<const float4*>(r + o)[qb];
-          rv.x = fmaf(-a4.x, qv.x, rv.x); rv.y = fmaf(-a4.y, qv.y, rv.y);
-          rv.z = fmaf(-a4.z, qv.z, rv.z); rv.w = fmaf(-a4.w, qv.w, rv.w);
-          reinterpret_cast<float4*>(r + o)[qb] = rv;
+          if (!((mk >> c) & 1)) {
+            const float4 qv = reinterpret_cast<const float4*>(q + o)[qb];
+            rv.x = fmaf(-a4.x, qv.x, rv.x); rv.y = fmaf(-a4.y, qv.y, rv.y);
+            rv.z = fmaf(-a4.z, qv.z, rv.z); rv.w = fmaf(-a4.w, qv.w, rv.w);
+            reinterpret_cast<float4*>(r + o)[qb] = rv;
+          }
           acc[0] += (double)(dv.x * rv.x * rv.x); acc[4] += (double)(rv.x * rv.x);
           acc[1] += (double)(dv.y * rv.y * rv.y); acc[5] += (double)(rv.y * rv.y);
           acc[2] += (double)(dv.z * rv.z * rv.z); acc[6] += (double)(rv.z * rv.z);
@@ -1227,10 +1251,11 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   const int n_tiles_op = modal ? n_tiles_m : n_tiles;
 
   // workspace of the batch (context slots 0-11, reused by the next batch)
-  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal;
+  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal, pB;
   MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &x.ptr));
   MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &r32.ptr));
   MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &p.ptr));
+  if (modal) MSG_TRY(workspace(ctx, 18, sizeof(float) * nvec, &pB.ptr));  // second direction buffer
   MSG_TRY(workspace(ctx, 3, sizeof(float) * nvec, &q.ptr));
   MSG_TRY(workspace(ctx, 4, sizeof(float) * nvec, &d.ptr));
   MSG_TRY(workspace(ctx, 5, sizeof(float) * npad * Rp, &dinv.ptr));
@@ -1265,6 +1290,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   MSG_CUDA(ctx, cudaMemsetAsync(x.ptr, 0, sizeof(double) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(r32.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(p.ptr, 0, sizeof(float) * nvec, st));
+  if (modal) MSG_CUDA(ctx, cudaMemsetAsync(pB.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(q.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(d.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(dinv.ptr, 0, sizeof(float) * npad * Rp, st));
@@ -1313,7 +1339,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
 
   // TMA descriptors of p (5-D: realization, component, x, y, z) and of the
   // FP32 element field (4-D: realization, x, y, z) for the staged operator
-  CUtensorMap tm_p, tm_e, tm_pm, tm_em;
+  CUtensorMap tm_p, tm_e, tm_rm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
   {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
@@ -1339,17 +1365,28 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     CUresult e2 = encode(&tm_e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, E32.ptr, ed, es, eb, one,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    const cuuint32_t pbm[5] = {32, 3, 1, kMPJ, kMPK};
-    const cuuint32_t ebm[4] = {32, 1, kMEJ, kMEK};
-    CUresult e3 = encode(&tm_pm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, p.ptr, pd, ps, pbm, one,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    CUresult e4 = encode(&tm_em, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, E32.ptr, ed, es, ebm, one,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (e1 != CUDA_SUCCESS || e2 != CUDA_SUCCESS || e3 != CUDA_SUCCESS || e4 != CUDA_SUCCESS)
-      return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d, %d, %d, %d)", (int)e1, (int)e2, (int)e3,
-                       (int)e4);
+    CUresult e3 = CUDA_SUCCESS;
+    if (modal) {
+      // modal operator: r, p (both buffers) and dinv patches with halo, the element patch, the tile's d
+      const cuuint32_t pbm[5] = {32, 3, 1, kMPJ, kMPK};
+      const cuuint32_t nbm[4] = {32, 1, kMPJ, kMPK};
+      const cuuint32_t ebm[4] = {32, 1, kMEJ, kMEK};
+      const cuuint32_t dbm[5] = {32, 3, 1, kMJ, kMK};
+      auto enc5 = [&](CUtensorMap* tm, void* base, const cuuint32_t* box) {
+        return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base, pd, ps, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      };
+      auto enc4 = [&](CUtensorMap* tm, void* base, const cuuint32_t* box) {
+        return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ed, es, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      };
+      const CUresult rs[6] = {enc5(&tm_rm, r32.ptr, pbm), enc5(&tm_pAm, p.ptr, pbm), enc5(&tm_pBm, pB.ptr, pbm),
+                              enc4(&tm_dinvm, dinv.ptr, nbm), enc4(&tm_em, E32.ptr, ebm), enc5(&tm_dm, d.ptr, dbm)};
+      for (CUresult r : rs)
+        if (r != CUDA_SUCCESS) e3 = r;
+    }
+    if (e1 != CUDA_SUCCESS || e2 != CUDA_SUCCESS || e3 != CUDA_SUCCESS)
+      return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d, %d, %d)", (int)e1, (int)e2, (int)e3);
   }
   if (modal) {
     static std::once_flag attr_once;
@@ -1375,8 +1412,11 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     mix(&KF, sizeof(KF));
     mix(&tm_p, sizeof(tm_p));
     mix(&tm_e, sizeof(tm_e));
-    mix(&tm_pm, sizeof(tm_pm));
-    mix(&tm_em, sizeof(tm_em));
+    if (modal) {
+      const CUtensorMap* tms[6] = {&tm_rm, &tm_pAm, &tm_pBm, &tm_dinvm, &tm_em, &tm_dm};
+      for (const CUtensorMap* t : tms) mix(t, sizeof(CUtensorMap));
+      mix(&pB.ptr, sizeof(pB.ptr));
+    }
     mix(&MC, sizeof(MC));
     const int mm[4] = {modal ? 1 : 0, n_tiles_m, n_items_m, grid_m};
     mix(mm, sizeof(mm));
@@ -1393,21 +1433,26 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int it = 0; it < chunk; ++it) {
-      k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
-                                   p.as<float>(), d.as<float>());
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
-      if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-      if (modal)
-        k_op_modal<false><<<grid_m, kMThreads, kMSmem, st>>>(L, MC, tm_pm, tm_em, tiles_jm, n_tiles_m, n_items_m, mask,
-                                                            q.as<float>(), part_op.as<double>(), s.err);
-      else
+      if (modal) {
+        // direction update fused into the operator; p alternates between the two buffers
+        const bool even = (it & 1) == 0;
+        if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
+        k_op_modal<false><<<grid_m, kMThreads, kMSmem, st>>>(
+            L, MC, tm_rm, even ? tm_pAm : tm_pBm, tm_dinvm, tm_em, tm_dm, tiles_jm, n_tiles_m, n_items_m, s.alpha,
+            s.beta, even ? pB.as<float>() : p.as<float>(), d.as<float>(), q.as<float>(), part_op.as<double>(), s.err);
+      } else {
+        k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
+                                     p.as<float>(), d.as<float>());
+        if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
         k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, KF, tm_p, tm_e, mask, q.as<float>(), part_op.as<double>(),
                                                        s.err);
+      }
       if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
       k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles_op, part_op.as<double>(), s);
       if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-      k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, s.alpha, q.as<float>(), r32.as<float>(),
+      k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, mask, s.alpha, q.as<float>(), r32.as<float>(),
                                              dinv.as<float>(), part_up.as<double>());
       if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
       cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
@@ -1457,7 +1502,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
-    count_launch(ctx, 5 * chunk);
+    count_launch(ctx, (modal ? 4 : 5) * chunk);
     total_inner += chunk;
     cudaEventRecord(ev[3], st);
     MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
