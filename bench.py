@@ -15,8 +15,9 @@ e2e    = the same through MSG_MC_SOLVE_BATCH with host (pinned) buffers: xi and
          b copied in, every realization's full displacement field copied out.
 fp64_dropin = the plain FP64 drop-in (assembled BSR + Jacobi PCG, one
          realization after another, MSG_MODE_FP64_BSR) on a sample of the batch.
-roofline = the matrix-free operator kernel (k_inner_op), live per-launch CUDA
-         event durations inside the timed region.
+roofline = the dominant kernel (k_op_modal: fused PCG direction update and
+         matrix-free FP32 operator), live per-launch CUDA event durations
+         inside the timed region.
 cpu_baseline = the oracle (C++ FP64 restatement of the reference: assembled
          CSR Jacobi-PCG per realization) on the host cores, a bounded sample.
 
@@ -40,6 +41,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p99 latency"
+# DRAM traffic of one k_op_modal launch per realization on the 32^3 lattice (ncu capture
+# at R = 512, dram__bytes_read.sum + dram__bytes_write.sum divided by 512); None until measured
+OP_DRAM_BYTES_PER_REALIZATION = None
 
 
 def parse():
@@ -285,16 +289,20 @@ def main():
     tip_mean = su / cnt
     tip_var = (su2 - cnt * tip_mean ** 2) / max(cnt - 1, 1)
 
-    # roofline of the matrix-free operator (live samples from the timed region)
+    # roofline of the dominant kernel, the fused direction + matrix-free FP32 operator
+    # (k_op_modal; live per-launch samples from the timed region)
     op_ms = st["op_launch_ms"]
     nn = model.n_nodes
     ne = model.n_elems
     Rp = (R + 31) // 32 * 32
-    # algorithmic bytes of one operator launch: read r, p_old (3 per node), dinv (1 per node), E (1 per
-    # element); write p_new, q (3 per node); FP32, realization-innermost, each once
-    op_bytes = 4.0 * Rp * (3 * nn * 4 + nn + ne)
+    # algorithmic bytes of one launch, FP32, realization-innermost, each value once:
+    # read r, p_{k-1}, d (3 per node), dinv (1 per node), E (1 per element); write p_k, d, q (3 per node)
+    op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 1 + 3 + 3 + 3) * nn + ne)
     hbm, peak_kind = load_peaks()
     achieved = op_bytes / (op_ms / 1e3) / 1e9 if op_ms > 0 else 0.0
+    # DRAM bytes per launch from one ncu capture of the same kernel at 512 realizations
+    # (dram__bytes_read.sum + dram__bytes_write.sum), scaled by the realizations processed
+    traffic = OP_DRAM_BYTES_PER_REALIZATION * Rp if OP_DRAM_BYTES_PER_REALIZATION else None
 
     line = None
     if rank == 0:
@@ -357,8 +365,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(R * K_terms * 8 + Nd * 8),
                     "d2h_bytes_per_step": int(R * Nd * 8 + R * (8 + 4 + 8))},
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "k_inner_op (matrix-free FP32 operator)", "bound": "hbm", "achieved": achieved,
-                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if hbm else None, "traffic": None,
+            "roofline": {"kernel": "k_op_modal (fused PCG direction update + matrix-free FP32 Hexa8 operator)",
+                         "bound": "hbm", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if hbm else None, "traffic": traffic,
                          "peak_kind": peak_kind, "launch_ms": op_ms, "bytes_per_launch": op_bytes,
                          "update_launch_ms": st["update_launch_ms"], "samples": st["launch_samples"]},
             "cpu_baseline": cpu,

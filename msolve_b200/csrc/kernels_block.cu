@@ -440,9 +440,9 @@ __global__ void __launch_bounds__(kOpThreads, 4)
 // per axis (sum and difference of two values), and the yz part of a plane
 // is shared by the elements on both sides of it along x.
 //
-// A CTA owns a 4 x 3 tile of node pencils for 32 realizations and runs one
-// warp per element pencil of the 5 x 4 that touch it (the tile's own
-// elements plus one halo row and column below; the 8 halo pencils are also
+// A CTA owns a 3 x 3 tile of node pencils for 32 realizations and runs one
+// warp per element pencil of the 4 x 4 that touch it (the tile's own
+// elements plus one halo row and column below; the 7 halo pencils are also
 // computed by the neighbouring CTA). Per x-plane P every element warp turns
 // its 4 plane nodes into 4 yz-modes per component, combines them with the
 // previous plane's modes into the element's 24 modes, applies the blocks,
@@ -469,24 +469,24 @@ struct ModalC {
   float m[8];    // mass per mode (0 when no mass term)
 };
 
-constexpr int kMJ = 4, kMK = 3;                       // node pencils per tile
+constexpr int kMJ = 3, kMK = 3;                       // node pencils per tile
 constexpr int kMEJ = kMJ + 1, kMEK = kMK + 1;         // element pencils per tile
-constexpr int kMWarps = kMEJ * kMEK;                  // 20 element warps (+ 1 producer: 80 registers a thread)
+constexpr int kMWarps = kMEJ * kMEK;                  // 16 element warps (+ 1 producer: 96 registers a thread)
 constexpr int kMPJ = kMJ + 2, kMPK = kMK + 2;         // node patch per plane
-constexpr int kMPlaneFloats = 32 * 3 * kMPJ * kMPK;   // r or p patch of a plane: 2880
-constexpr int kMNodeFloats = 32 * kMPJ * kMPK;        // dinv patch: 960
-constexpr int kMEFloats = 32 * kMEJ * kMEK;           // E patch: 640
-constexpr int kMDFloats = 32 * 3 * kMJ * kMK;         // d of the tile's own nodes: 1152
-// stage: r | p_{k-1} | dinv | E | d (each patch a multiple of 128 bytes)
-constexpr int kMOffR = 0, kMOffP = kMPlaneFloats, kMOffDinv = 2 * kMPlaneFloats;
+constexpr int kMPlaneFloats = 32 * 3 * kMPJ * kMPK;   // r, q or p patch of a plane: 2400
+constexpr int kMNodeFloats = 32 * kMPJ * kMPK;        // dinv patch: 800
+constexpr int kMEFloats = 32 * kMEJ * kMEK;           // E patch: 512
+constexpr int kMDFloats = 32 * 3 * kMJ * kMK;         // d of the tile's own nodes: 864
+// stage: r | q | p | dinv | E | d (each patch a multiple of 128 bytes)
+constexpr int kMOffR = 0, kMOffQ = kMPlaneFloats, kMOffP = 2 * kMPlaneFloats, kMOffDinv = 3 * kMPlaneFloats;
 constexpr int kMOffE = kMOffDinv + kMNodeFloats, kMOffD = kMOffE + kMEFloats;
-constexpr int kMStageFloats = kMOffD + kMDFloats;     // 8512 floats, 34,048 bytes
+constexpr int kMStageFloats = kMOffD + kMDFloats;     // 9,376 floats, 37,504 bytes
 constexpr uint32_t kMStageBytes = kMStageFloats * 4;
-constexpr int kMStages = 4;
+constexpr int kMStages = 3;
 constexpr int kMXFloats = kMWarps * 4 * 3 * 32;       // exchange buffer: element x corner x component x lane
 constexpr int kMThreads = 32 * (kMWarps + 1);         // + 1 TMA producer warp
 constexpr size_t kMSmem = 128 + sizeof(float) * ((size_t)kMStages * kMStageFloats + 2 * (size_t)kMXFloats) +
-                          sizeof(double) * kMJ * kMK * 32 + sizeof(uint64_t) * (2 * kMStages);
+                          sizeof(double) * 4 * kMJ * kMK * 32 + sizeof(uint64_t) * (2 * kMStages);
 static_assert(kMSmem <= 227 * 1024, "modal operator shared memory");
 
 // yz transform of one plane's 4 nodes u[ay][az] into the modes B[my + 2 mz]
@@ -585,25 +585,35 @@ __device__ __forceinline__ void modal_apply(const ModalC& C, float E, const floa
     }
 }
 
-// The direction update of PCG iteration k (d += alpha_{k-1} p_{k-1},
-// p_k = dinv r_k + beta_k p_{k-1}) is fused into the operator: each stage
-// carries the plane's r, p_{k-1} and dinv patches (and the tile's d), the
-// element warps form p_k at their corners on the fly, and the warp that owns a
-// node pencil writes p_k and d back. p_k goes to the other buffer of a pair
-// (neighbouring CTAs still read p_{k-1} in their halos).
+// One whole inner PCG iteration per launch (single-reduction form). Launch k+1
+// receives r_k, q_k = K p_k, p_k, alpha_k and beta_{k+1} and, at every node,
+//   r_{k+1} = r_k - alpha_k q_k,  p_{k+1} = dinv r_{k+1} + beta_{k+1} p_k,
+//   d += alpha_k p_k (the FP32 solution correction),
+// then q_{k+1} = K p_{k+1} (masked) with the partials p.q, (dinv r).q,
+// q.dinv.q and (dinv r).r of p_{k+1}, r_{k+1}, q_{k+1}. The scalar kernel that
+// follows forms alpha_{k+1} = gamma_{k+1} / p.q from the gamma of r_{k+1}
+// itself and the next gamma by the expansion of (dinv r_{k+2}).r_{k+2},
+//   gamma_{k+2} = gamma_{k+1} - 2 alpha (dinv r).q + alpha^2 q.dinv.q,
+// so r never needs a pass of its own (and the expansion never runs for more
+// than one step, which keeps the FP32 iteration count of the two-pass loop). Each stage carries the plane's r, q, p and dinv patches with halo (and
+// the tile's d); the element warps form p_{k+1} at their corners on the fly,
+// and the owner of a node pencil writes r, p and d back. r, q and p each have
+// a second buffer: neighbouring CTAs still read the old values in their halos.
+constexpr int kMParts = 4;  // partials per realization and tile: p.q, (dinv r).q, q.dinv.q, (dinv r).r
 template <bool kMass>
 __global__ void __launch_bounds__(kMThreads, 1)
     k_op_modal(Lattice L, const __grid_constant__ ModalC C, const __grid_constant__ CUtensorMap tm_r,
-               const __grid_constant__ CUtensorMap tm_p, const __grid_constant__ CUtensorMap tm_dinv,
-               const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_d, int tiles_j,
-               int n_tiles, int n_items, const float* __restrict__ alpha, const float* __restrict__ beta,
-               float* __restrict__ p_out, float* __restrict__ d, float* __restrict__ q, double* __restrict__ partial,
-               int* __restrict__ err) {
+               const __grid_constant__ CUtensorMap tm_q, const __grid_constant__ CUtensorMap tm_p,
+               const __grid_constant__ CUtensorMap tm_dinv, const __grid_constant__ CUtensorMap tm_e,
+               const __grid_constant__ CUtensorMap tm_d, int tiles_j, int n_tiles, int n_items,
+               const uint8_t* __restrict__ mask, const float* __restrict__ alpha, const float* __restrict__ beta,
+               float* __restrict__ r_out, float* __restrict__ p_out, float* __restrict__ q_out, float* __restrict__ d,
+               double* __restrict__ partial, int* __restrict__ err) {
   extern __shared__ __align__(128) float smem_dyn[];
   float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
   float* xbuf = smem + kMStages * kMStageFloats;                            // 2 exchange buffers
-  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);            // [node pencils][32]
-  uint64_t* full = reinterpret_cast<uint64_t*>(red + kMJ * kMK * 32);
+  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);            // [parts][node pencils][32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + kMParts * kMJ * kMK * 32);
   uint64_t* empty = full + kMStages;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int NX = L.NX, Rp = L.Rp;
@@ -632,6 +642,7 @@ __global__ void __launch_bounds__(kMThreads, 1)
           float* dst = smem + st * kMStageFloats;
           mbar_expect_tx(&full[st], kMStageBytes);
           tma_load_5d(dst + kMOffR, &tm_r, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_5d(dst + kMOffQ, &tm_q, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
           tma_load_5d(dst + kMOffP, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
           tma_load_4d(dst + kMOffDinv, &tm_dinv, g32, P, J0 - 1, K0 - 1, &full[st]);
           tma_load_4d(dst + kMOffE, &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
@@ -663,19 +674,24 @@ __global__ void __launch_bounds__(kMThreads, 1)
     const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;  // padded node (0, Je, Ke)
     const int rr = g32 + lane;
     const float al = alpha[rr], be = beta[rr];
-    float Bp[3][4], T0[3][4], own[3];
+    float Bp[3][4], T0[3][4];
+    float op[3] = {0.f, 0.f, 0.f}, orr[3] = {0.f, 0.f, 0.f}, odv = 0.f;  // p, r, dinv at the own node
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      own[c] = 0.f;
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int qq = 0; qq < 4; ++qq) T0[c][qq] = 0.f;
-    }
-    double pq = 0.0;
+    double acc_pq = 0.0, acc_zq = 0.0, acc_qq = 0.0, acc_zr = 0.0;
+    uint32_t mreg = 0;  // constraint bits of plane base + lane of the own pencil
     // node phase of plane X: sum the corner contributions of the 4 elements
     auto node_phase = [&](int X) {
+      if (((X - 1) & 31) == 0) {
+        const int pl = X + lane;
+        mreg = (pl <= NX) ? mask[nrow + pl] : 0u;
+      }
+      const uint32_t mk = __shfl_sync(0xffffffffu, mreg, (X - 1) & 31);
       const float* xb = xbuf + xsel * kMXFloats;
       const size_t node = nrow + X;
-      float acc = 0.f;
+      float spq = 0.f, szq = 0.f, sqq = 0.f, szr = 0.f;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         float y = 0.f;
@@ -683,10 +699,17 @@ __global__ void __launch_bounds__(kMThreads, 1)
         if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
         if (r01) y += xb[(((w - kMEJ) * 4 + 2) * 3 + c) * 32 + lane];
         if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
-        q[(node * 3 + c) * Rp + rr] = y;
-        acc = fmaf(own[c], y, acc);
+        y = ((mk >> c) & 1) ? 0.f : y;
+        q_out[(node * 3 + c) * Rp + rr] = y;
+        spq = fmaf(op[c], y, spq);
+        szq = fmaf(orr[c], y, szq);
+        sqq = fmaf(y, y, sqq);
+        szr = fmaf(orr[c], orr[c], szr);
       }
-      pq += (double)acc;
+      acc_pq += (double)spq;
+      acc_zq += (double)odv * (double)szq;
+      acc_qq += (double)odv * (double)sqq;
+      acc_zr += (double)odv * (double)szr;
     };
     auto emit_corners = [&](const float (&B)[3][4]) {
       float y[2][2][3];
@@ -706,8 +729,8 @@ __global__ void __launch_bounds__(kMThreads, 1)
         dead = true;
       }
       const float* pt = smem + st * kMStageFloats;
-      // p_k at the element's 4 plane corners: dinv r + beta p_{k-1}
-      float u[2][2][3];
+      // p_{k+1} at the element's 4 plane corners: dinv (r - alpha q) + beta p_k
+      float u[2][2][3], rc[3], dvc = 0.f;
 #pragma unroll
       for (int ay = 0; ay < 2; ++ay)
 #pragma unroll
@@ -715,18 +738,24 @@ __global__ void __launch_bounds__(kMThreads, 1)
           const int o = (ek + az) * kMPJ + (ej + ay);
           const float dv = pt[kMOffDinv + o * 32 + lane];
 #pragma unroll
-          for (int c = 0; c < 3; ++c)
-            u[ay][az][c] = fmaf(dv, pt[kMOffR + (o * 3 + c) * 32 + lane], be * pt[kMOffP + (o * 3 + c) * 32 + lane]);
+          for (int c = 0; c < 3; ++c) {
+            const int i = (o * 3 + c) * 32 + lane;
+            const float rn = fmaf(-al, pt[kMOffQ + i], pt[kMOffR + i]);
+            u[ay][az][c] = fmaf(dv, rn, be * pt[kMOffP + i]);
+            if (ay == 0 && az == 0) rc[c] = rn;
+          }
+          if (ay == 0 && az == 0) dvc = dv;
         }
       const float E = pt[kMOffE + w * 32 + lane];  // element (P-1, Je, Ke)
       if (node_ok) {
-        // the owner writes p_k and d += alpha_{k-1} p_{k-1} of node (P, Je, Ke)
+        // the owner writes r_{k+1}, p_{k+1} and d += alpha_k p_k of node (P, Je, Ke)
         const int o = ek * kMPJ + ej, od = (ek - 1) * kMJ + (ej - 1);
         const size_t node = nrow + P;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const float pold = pt[kMOffP + (o * 3 + c) * 32 + lane];
           const float dn = fmaf(al, pold, pt[kMOffD + (od * 3 + c) * 32 + lane]);
+          r_out[(node * 3 + c) * Rp + rr] = rc[c];
           p_out[(node * 3 + c) * Rp + rr] = u[0][0][c];
           d[(node * 3 + c) * Rp + rr] = dn;
         }
@@ -751,7 +780,9 @@ __global__ void __launch_bounds__(kMThreads, 1)
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        own[c] = u[0][0][c];
+        op[c] = u[0][0][c];
+        orr[c] = rc[c];
+        odv = dvc;
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) Bp[c][qq] = Bc[c][qq];
       }
@@ -761,13 +792,19 @@ __global__ void __launch_bounds__(kMThreads, 1)
     csync();
     if (node_ok) node_phase(NX);
     xsel ^= 1;
-    if (node_warp) red[((ek - 1) * kMJ + (ej - 1)) * 32 + lane] = pq;
+    if (node_warp) {
+      const int nw = (ek - 1) * kMJ + (ej - 1);
+      red[(0 * kMJ * kMK + nw) * 32 + lane] = acc_pq;
+      red[(1 * kMJ * kMK + nw) * 32 + lane] = acc_zq;
+      red[(2 * kMJ * kMK + nw) * 32 + lane] = acc_qq;
+      red[(3 * kMJ * kMK + nw) * 32 + lane] = acc_zr;
+    }
     csync();
-    if (w == 0) {
-      double s = 0.0;
+    if (w < kMParts) {
+      double sum = 0.0;
 #pragma unroll
-      for (int i = 0; i < kMJ * kMK; ++i) s += red[i * 32 + lane];
-      partial[(size_t)tile * Rp + rr] = s;
+      for (int i = 0; i < kMJ * kMK; ++i) sum += red[(w * kMJ * kMK + i) * 32 + lane];
+      partial[((size_t)tile * Rp + rr) * kMParts + w] = sum;
     }
   }
 }
@@ -962,9 +999,10 @@ struct Scal {
   float* beta;         // [Rp]
   double* gamma;       // [Rp] (dinv r).r
   double* gamma_prev;  // [Rp] gamma of the previous iteration
-  double* rho_ref;     // [Rp] r.r at the last reliable update
+  double* rho_ref;     // [Rp] r.r (gamma for the single-reduction loop) at the last reliable update
   double* res;         // [Rp] FP64 ||b - K x|| / ||b||
   double* bnorm;       // [Rp]
+  double* gamma0;      // [Rp] gamma of the first true residual (r = b)
   int* act;            // [Rp] iterating
   int* done;           // [Rp] converged (true residual)
   int* its;            // [Rp] operator applications
@@ -994,6 +1032,7 @@ __device__ __forceinline__ void reduce_rows(const double* __restrict__ partial, 
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     double s = 0.0;
+#pragma unroll 4
     for (int gg = 0; gg < 32; ++gg) s += sh[gg][q][lane];
     out[q] = s;
   }
@@ -1056,7 +1095,7 @@ __global__ void __launch_bounds__(1024) k_beta(int Rp, int n_blk, const double* 
 // the search-direction coefficient beta = gamma_new / gamma_prev (first call:
 // beta = 0, p starts from z).
 __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, const double* __restrict__ partial,
-                                                        Scal s, double tol, int first) {
+                                                        Scal s, double tol, int first, int gamma_ref) {
   double v[2];
   reduce_rows<2>(partial, n_tiles, Rp, v);
   const int r = blockIdx.x * 32 + threadIdx.x;
@@ -1071,12 +1110,55 @@ __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, con
     s.act[r] = a;
     s.beta[r] = (a && !first && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
     s.gamma[r] = g;
-    s.rho_ref[r] = rr;
-    s.alpha[r] = 0.f;  // the pending alpha p term was folded into x
+    s.rho_ref[r] = gamma_ref ? g : rr;
+    if (first) s.gamma0[r] = g;
+    s.alpha[r] = 0.f;  // the pending alpha p term was folded into x (and no r update is pending)
     active = a;
   }
   active = __syncthreads_count(active);
   if (threadIdx.x == 0 && active) atomicAdd(s.n_active, active);
+}
+
+// Scalars of the single-reduction loop after k_op_modal: with gamma = (dinv r).r
+// of the launch's r, alpha = gamma / p.q, gamma' = gamma - 2 alpha (dinv r).q +
+// alpha^2 q.dinv.q (the gamma of the next r), beta = gamma' / gamma;
+// a reliable update is requested once gamma has dropped by delta^2 since the
+// last one, or below tol2 * gamma0.
+__global__ void __launch_bounds__(1024) k_alpha_gamma(int Rp, int n_tiles, const double* __restrict__ partial, Scal s,
+                                                      double delta2, double tol2) {
+  double v[4];
+  reduce_rows<4>(partial, n_tiles, Rp, v);
+  const int r = blockIdx.x * 32 + threadIdx.x;
+  int active = 0, upd = 0;
+  if (threadIdx.x < 32) {
+    float a = 0.f, b = 0.f;
+    if (s.act[r]) {
+      const double pq = v[0], zq = v[1], qdq = v[2], g = v[3];
+      const double al = g / pq;
+      double gn = g - 2.0 * al * zq + al * al * qdq;
+      if (!(pq > 0.0) || !(g > 0.0) || !(gn == gn)) {
+        s.act[r] = 0;
+        s.breakdown[r] = 1;
+      } else {
+        gn = gn > 0.0 ? gn : 0.0;  // rounding at convergence; the true residual decides
+        a = (float)al;
+        b = (float)(gn / g);
+        s.its[r] += 1;
+        s.gamma_prev[r] = g;
+        s.gamma[r] = gn;
+        active = 1;
+        upd = (gn < delta2 * s.rho_ref[r] || gn < tol2 * s.gamma0[r]) ? 1 : 0;
+      }
+    }
+    s.alpha[r] = a;
+    s.beta[r] = b;
+  }
+  active = __syncthreads_count(active);
+  upd = __syncthreads_count(upd);
+  if (threadIdx.x == 0) {
+    if (active) atomicAdd(s.n_active, active);
+    if (upd) atomicAdd(s.n_update, upd);
+  }
 }
 
 __global__ void k_lattice_rhs(int n_dofs, const int* __restrict__ rows, const double* __restrict__ b_dof,
@@ -1248,14 +1330,17 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   const int tiles_jm = (L.NY + kMJ - 1) / kMJ, n_tiles_m = tiles_jm * ((L.NZ + kMK - 1) / kMK);
   const int n_items_m = n_tiles_m * (Rp / 32);
   const int grid_m = std::min(n_items_m, ctx->sm_count);
-  const int n_tiles_op = modal ? n_tiles_m : n_tiles;
 
   // workspace of the batch (context slots 0-11, reused by the next batch)
-  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal, pB;
+  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal, pB, rB, qB;
   MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &x.ptr));
   MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &r32.ptr));
   MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &p.ptr));
-  if (modal) MSG_TRY(workspace(ctx, 18, sizeof(float) * nvec, &pB.ptr));  // second direction buffer
+  if (modal) {  // second buffers of p, r and q for the single-reduction loop
+    MSG_TRY(workspace(ctx, 18, sizeof(float) * nvec, &pB.ptr));
+    MSG_TRY(workspace(ctx, 19, sizeof(float) * nvec, &rB.ptr));
+    MSG_TRY(workspace(ctx, 20, sizeof(float) * nvec, &qB.ptr));
+  }
   MSG_TRY(workspace(ctx, 3, sizeof(float) * nvec, &q.ptr));
   MSG_TRY(workspace(ctx, 4, sizeof(float) * nvec, &d.ptr));
   MSG_TRY(workspace(ctx, 5, sizeof(float) * npad * Rp, &dinv.ptr));
@@ -1263,9 +1348,9 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   MSG_TRY(workspace(ctx, 7, sizeof(float) * npad * Rp, &E32.ptr));
   MSG_TRY(workspace(ctx, 8, sizeof(double) * npad * 3, &blat.ptr));
   const int n_upd = std::min(L.n_int, ctx->sm_count * 4);
-  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)std::max(n_tiles, n_tiles_m) * Rp * 2, &part_op.ptr));
+  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)std::max(n_tiles * 2, n_tiles_m * kMParts) * Rp, &part_op.ptr));
   MSG_TRY(workspace(ctx, 10, sizeof(double) * (size_t)n_upd * Rp * 2, &part_up.ptr));
-  const size_t scal_bytes = (sizeof(float) * 2 + sizeof(double) * 5 + sizeof(int) * 4) * (size_t)Rp + 64;
+  const size_t scal_bytes = (sizeof(float) * 2 + sizeof(double) * 6 + sizeof(int) * 4) * (size_t)Rp + 64;
   MSG_TRY(workspace(ctx, 11, scal_bytes, &scal.ptr));
   MSG_CUDA(ctx, cudaMemsetAsync(scal.ptr, 0, scal_bytes, st));
   Scal s;
@@ -1278,6 +1363,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     s.rho_ref = (double*)base; base += sizeof(double) * Rp;
     s.res = (double*)base; base += sizeof(double) * Rp;
     s.bnorm = (double*)base; base += sizeof(double) * Rp;
+    s.gamma0 = (double*)base; base += sizeof(double) * Rp;
     s.act = (int*)base; base += sizeof(int) * Rp;
     s.done = (int*)base; base += sizeof(int) * Rp;
     s.its = (int*)base; base += sizeof(int) * Rp;
@@ -1290,7 +1376,11 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   MSG_CUDA(ctx, cudaMemsetAsync(x.ptr, 0, sizeof(double) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(r32.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(p.ptr, 0, sizeof(float) * nvec, st));
-  if (modal) MSG_CUDA(ctx, cudaMemsetAsync(pB.ptr, 0, sizeof(float) * nvec, st));
+  if (modal) {
+    MSG_CUDA(ctx, cudaMemsetAsync(pB.ptr, 0, sizeof(float) * nvec, st));
+    MSG_CUDA(ctx, cudaMemsetAsync(rB.ptr, 0, sizeof(float) * nvec, st));
+    MSG_CUDA(ctx, cudaMemsetAsync(qB.ptr, 0, sizeof(float) * nvec, st));
+  }
   MSG_CUDA(ctx, cudaMemsetAsync(q.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(d.ptr, 0, sizeof(float) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(dinv.ptr, 0, sizeof(float) * npad * Rp, st));
@@ -1330,7 +1420,9 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   const int n_xu = ctx->sm_count * 8;
   const int n_dir = std::min(L.n_int, ctx->sm_count * 8);
   const double delta2 = ctx->reliable_delta * ctx->reliable_delta;
-  const double tol2 = 0.25 * tol * tol;  // ask for a check once the recursive residual is at tol/2
+  // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
+  // sqrt(gamma / gamma0) is at tol/4 (single-reduction loop, dinv-weighted norm)
+  const double tol2 = (modal ? 0.0625 : 0.25) * tol * tol;
 
   // context events: 0-3 host-side phases, 4-7 captured around the first operator / update launch
   MSG_TRY(context_resources(ctx));
@@ -1339,7 +1431,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
 
   // TMA descriptors of p (5-D: realization, component, x, y, z) and of the
   // FP32 element field (4-D: realization, x, y, z) for the staged operator
-  CUtensorMap tm_p, tm_e, tm_rm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
+  CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
   {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
@@ -1380,7 +1472,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
         return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ed, es, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
       };
-      const CUresult rs[6] = {enc5(&tm_rm, r32.ptr, pbm), enc5(&tm_pAm, p.ptr, pbm), enc5(&tm_pBm, pB.ptr, pbm),
+      const CUresult rs[10] = {enc5(&tm_rAm, r32.ptr, pbm), enc5(&tm_rBm, rB.ptr, pbm), enc5(&tm_qAm, q.ptr, pbm),
+                               enc5(&tm_qBm, qB.ptr, pbm), enc5(&tm_pAm, p.ptr, pbm), enc5(&tm_pBm, pB.ptr, pbm),
                               enc4(&tm_dinvm, dinv.ptr, nbm), enc4(&tm_em, E32.ptr, ebm), enc5(&tm_dm, d.ptr, dbm)};
       for (CUresult r : rs)
         if (r != CUDA_SUCCESS) e3 = r;
@@ -1413,9 +1506,10 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     mix(&tm_p, sizeof(tm_p));
     mix(&tm_e, sizeof(tm_e));
     if (modal) {
-      const CUtensorMap* tms[6] = {&tm_rm, &tm_pAm, &tm_pBm, &tm_dinvm, &tm_em, &tm_dm};
+      const CUtensorMap* tms[9] = {&tm_rAm, &tm_rBm, &tm_qAm, &tm_qBm, &tm_pAm, &tm_pBm, &tm_dinvm, &tm_em, &tm_dm};
       for (const CUtensorMap* t : tms) mix(t, sizeof(CUtensorMap));
-      mix(&pB.ptr, sizeof(pB.ptr));
+      const void* bp[3] = {pB.ptr, rB.ptr, qB.ptr};
+      mix(bp, sizeof(bp));
     }
     mix(&MC, sizeof(MC));
     const int mm[4] = {modal ? 1 : 0, n_tiles_m, n_items_m, grid_m};
@@ -1436,27 +1530,35 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
       if (modal) {
-        // direction update fused into the operator; p alternates between the two buffers
+        // single-reduction loop: one operator launch per iteration; r, q and p
+        // alternate between their two buffers
         const bool even = (it & 1) == 0;
         if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
         k_op_modal<false><<<grid_m, kMThreads, kMSmem, st>>>(
-            L, MC, tm_rm, even ? tm_pAm : tm_pBm, tm_dinvm, tm_em, tm_dm, tiles_jm, n_tiles_m, n_items_m, s.alpha,
-            s.beta, even ? pB.as<float>() : p.as<float>(), d.as<float>(), q.as<float>(), part_op.as<double>(), s.err);
+            L, MC, even ? tm_rAm : tm_rBm, even ? tm_qAm : tm_qBm, even ? tm_pAm : tm_pBm, tm_dinvm, tm_em, tm_dm,
+            tiles_jm, n_tiles_m, n_items_m, mask, s.alpha, s.beta, even ? rB.as<float>() : r32.as<float>(),
+            even ? pB.as<float>() : p.as<float>(), even ? qB.as<float>() : q.as<float>(), d.as<float>(),
+            part_op.as<double>(), s.err);
+        if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
+        cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
+        if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
+        k_alpha_gamma<<<sblocks, 1024, 0, st>>>(Rp, n_tiles_m, part_op.as<double>(), s, delta2, tol2);
+        if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
       } else {
         k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
                                      p.as<float>(), d.as<float>());
         if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
         k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, KF, tm_p, tm_e, mask, q.as<float>(), part_op.as<double>(),
                                                        s.err);
+        if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
+        k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
+        if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
+        k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, mask, s.alpha, q.as<float>(), r32.as<float>(),
+                                               dinv.as<float>(), part_up.as<double>());
+        if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
+        cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
+        k_beta<<<sblocks, 1024, 0, st>>>(Rp, n_upd, part_up.as<double>(), s, delta2, tol2);
       }
-      if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
-      k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles_op, part_op.as<double>(), s);
-      if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-      k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, mask, s.alpha, q.as<float>(), r32.as<float>(),
-                                             dinv.as<float>(), part_up.as<double>());
-      if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
-      cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
-      k_beta<<<sblocks, 1024, 0, st>>>(Rp, n_upd, part_up.as<double>(), s, delta2, tol2);
     }
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (e != cudaSuccess) return cuda_error(ctx, e, "capture inner chunk");
@@ -1486,7 +1588,8 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       k_resid<<<op_grid, op_block, 0, st>>>(L, KD, x.as<double>(), blat.as<double>(), E64.as<double>(), mask,
                                             dinv.as<float>(), r32.as<float>(), part_op.as<double>());
       MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
-      k_resid_scalars<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol, first ? 1 : 0);
+      k_resid_scalars<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol, first ? 1 : 0,
+                                                modal ? 1 : 0);
       cudaEventRecord(ev[1], st);
       count_launch(ctx, 2);
       MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
@@ -1502,7 +1605,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
-    count_launch(ctx, (modal ? 4 : 5) * chunk);
+    count_launch(ctx, (modal ? 2 : 5) * chunk);
     total_inner += chunk;
     cudaEventRecord(ev[3], st);
     MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
