@@ -192,6 +192,42 @@ int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R,
                               const double* b_dev, int mode, int max_it, double tol, int tip_dof, double* X_dev,
                               double* tip, int* iterations, double* rel_res);
 
+/* ------------------------------------------------------------------ Newmark batch */
+/* Parameters of NewmarkDynamicAnalyzer (ISAAR.MSolve.Analyzers/NewmarkDynamicAnalyzer.cs:38-77)
+ * with the structural provider's effective matrix K + a0 M + a1 C
+ * (ProblemStructural.cs:138-157), Hexa8 consistent mass and Rayleigh damping
+ * C_e = rayleigh_alpha M_e + rayleigh_beta K_e (Hexa8.cs:403-451), and one
+ * MassAccelerationSinusoidalLoad (MassAccelerationSinusoidalLoad.cs:17-20):
+ * ground acceleration acc_amp sin(2 pi / acc_period * dt * i) in DOF acc_dof at
+ * step i, applied as the inertial load sum_e M_e a_g (Hexa8.cs:512-530). */
+typedef struct {
+  double rho;            /* density of the consistent mass */
+  double rayleigh_alpha; /* mass-proportional damping */
+  double rayleigh_beta;  /* stiffness-proportional damping */
+  double alpha;          /* Newmark alpha (>= (0.5 + delta)^2 / 4), 0.25: average acceleration */
+  double delta;          /* Newmark delta (>= 0.5) */
+  double dt;             /* time step */
+  int n_steps;           /* the reference runs (int)(totalTime / dt) steps */
+  double acc_amp;
+  double acc_period;
+  int acc_dof;           /* 0 X, 1 Y, 2 Z */
+} MSG_NEWMARK;
+
+/* Newmark integration of R realizations at once (the batched counterpart of
+ * NewmarkDynamicAnalyzer.Solve, :280-315, for a stochastic material: E field
+ * of realization r from xi[r] as in MSG_MC_SOLVE_BATCH). Every step solves the
+ * effective system of all realizations with the mixed batched PCG to the FP64
+ * true relative residual tol, warm-started from the previous displacement
+ * (the reference restarts SolverPCG from zero; both stop on the same
+ * criterion). Structured cube lattices only (MSG_ERR_NOT_STRUCTURED otherwise).
+ * xi [R][kl->n_terms]; f_static [n_dofs] static nodal loads added every step
+ * (Model.AssignLoads) or NULL. Outputs (each may be NULL): tip_hist
+ * [R][n_steps] displacement of DOF tip_dof after each step, U [R][n_dofs] final
+ * displacements, iterations [R] operator products summed over the steps. */
+int MSG_NEWMARK_BATCH(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const double* xi, const MSG_NEWMARK* nm,
+                      const double* f_static, int max_it, double tol, int tip_dof, double* tip_hist, double* U,
+                      int* iterations);
+
 /* Tunables of the mixed solver on this context: "reliable_delta" (the FP32
  * recursive residual may fall by this factor before it is replaced by the FP64
  * true residual, default 0.1), "chunk" (FP32 iterations per CUDA-graph launch,

@@ -7,14 +7,15 @@ solver and analyzer interfaces, bound through ctypes.
 from ._native import (ArgumentError, Context, InvalidOperationError, MSolveError, MSG_MODE_FP64_BSR,
                       MSG_MODE_MIXED_BATCHED, lib)
 from .analyzers import (GpuMatrix, GpuMesh, LinearAnalyzer, LognormalStochasticCoefficientsProvider,
-                        MonteCarloAnalyzerWithStochasticMaterial, ProblemStructural, SolverPCG, StaticAnalyzer,
-                        h8_mass_batch, h8_stiffness_batch)
-from .model import Hexa8MeshGenerator, Model, cantilever_model, clamped_block_model, tip_dof
+                        MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer, ProblemStructural, SolverPCG,
+                        StaticAnalyzer, h8_mass_batch, h8_stiffness_batch)
+from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, cantilever_model, clamped_block_model,
+                    tip_dof)
 
 __all__ = [
     "ArgumentError", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
     "lib", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
-    "MonteCarloAnalyzerWithStochasticMaterial", "ProblemStructural", "SolverPCG", "StaticAnalyzer",
-    "h8_mass_batch", "h8_stiffness_batch", "Hexa8MeshGenerator", "Model", "cantilever_model",
-    "clamped_block_model", "tip_dof",
+    "MonteCarloAnalyzerWithStochasticMaterial", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
+    "StaticAnalyzer", "h8_mass_batch", "h8_stiffness_batch", "Hexa8MeshGenerator", "MassAccelerationSinusoidalLoad",
+    "Model", "cantilever_model", "clamped_block_model", "tip_dof",
 ]

@@ -52,6 +52,21 @@ class MSG_KL(C.Structure):
 
 
 # name -> (restype, argtypes); the exported symbol set of include/msolve_gpu.h
+class MSG_NEWMARK(C.Structure):
+    _fields_ = [
+        ("rho", C.c_double),
+        ("rayleigh_alpha", C.c_double),
+        ("rayleigh_beta", C.c_double),
+        ("alpha", C.c_double),
+        ("delta", C.c_double),
+        ("dt", C.c_double),
+        ("n_steps", C.c_int),
+        ("acc_amp", C.c_double),
+        ("acc_period", C.c_double),
+        ("acc_dof", C.c_int),
+    ]
+
+
 SIGNATURES = {
     "MSG_CREATE": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
     "MSG_DESTROY": (C.c_int, [_vp]),
@@ -75,6 +90,8 @@ SIGNATURES = {
                                      C.c_double, C.c_int, _d, _d, _i, _d]),
     "MSG_MC_SOLVE_BATCH_DEVICE": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _vp, _vp, C.c_int,
                                             C.c_int, C.c_double, C.c_int, _vp, _d, _i, _d]),
+    "MSG_NEWMARK_BATCH": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _d, C.POINTER(MSG_NEWMARK), _d,
+                                    C.c_int, C.c_double, C.c_int, _d, _d, _i]),
     "MSG_SET_OPTION": (C.c_int, [_vp, C.c_char_p, C.c_double]),
     "MSG_STATS": (C.c_int, [_vp, _i64, _d]),
     "MSG_STATS_RESET": (C.c_int, [_vp]),

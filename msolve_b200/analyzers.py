@@ -289,3 +289,72 @@ class MonteCarloAnalyzerWithStochasticMaterial:
     def statistics(self):
         t = self.TipValues
         return dict(mean=float(np.mean(t)), variance=float(np.var(t, ddof=1)) if len(t) > 1 else 0.0)
+
+
+class NewmarkDynamicAnalyzer:
+    """Implicit Newmark integration (NewmarkDynamicAnalyzer.cs:16-315) of every
+    realization of a stochastic-material batch at once. Same parameters as the
+    reference (alpha, delta, timeStep, totalTime; the loop runs
+    int(totalTime / timeStep) steps), with the structural provider's effective
+    matrix K + a0 M + a1 C, Rayleigh damping C = rayleigh_alpha M + rayleigh_beta K
+    (Hexa8.DampingMatrix) and a MassAccelerationSinusoidalLoad as ground
+    acceleration. BuildMatrices() checks the coefficients (InitializeCoefficients),
+    Initialize() draws xi, Solve() runs MSG_NEWMARK_BATCH. Results: TipHistory
+    [R][n_steps], Solutions [R][n_dofs] (final displacements), Iterations [R]."""
+
+    def __init__(self, ctx, model, coefficients_provider, alpha, delta, time_step, total_time, load,
+                 expansion_order=50, simulations=1, seed=12345, density=1.0, rayleigh_alpha=0.0, rayleigh_beta=0.0,
+                 max_iterations=20000, tolerance=1e-8, tip_dof=None, static_loads=False):
+        self.ctx, self.model, self.kl = ctx, model, coefficients_provider
+        self.alpha, self.delta, self.time_step, self.total_time = alpha, delta, time_step, total_time
+        self.load = load
+        self.expansion_order, self.simulations, self.seed = expansion_order, simulations, seed
+        self.density, self.rayleigh_alpha, self.rayleigh_beta = density, rayleigh_alpha, rayleigh_beta
+        self.max_iterations, self.tolerance = max_iterations, tolerance
+        self.tip_dof = _tip_dof(model) if tip_dof is None else tip_dof
+        self.static_loads = static_loads
+        self.mesh = GpuMesh(ctx, model)
+        self.RandomNumbers = None
+
+    @property
+    def steps(self):
+        return int(self.total_time / self.time_step)
+
+    def BuildMatrices(self):
+        if self.delta < 0.5:
+            raise N.InvalidOperationError(N.MSG_ERR_INVALID_ARGUMENT, "Newmark delta has to be bigger than 0.5.")
+        a_limit = 0.25 * (0.5 + self.delta) ** 2
+        if self.alpha < a_limit:
+            raise N.InvalidOperationError(N.MSG_ERR_INVALID_ARGUMENT,
+                                          "Newmark alpha has to be bigger than %s." % a_limit)
+
+    def Initialize(self):
+        rng = np.random.default_rng(self.seed)
+        self.RandomNumbers = rng.standard_normal((self.simulations, self.expansion_order))
+
+    def params(self):
+        nm = N.MSG_NEWMARK()
+        nm.rho, nm.rayleigh_alpha, nm.rayleigh_beta = self.density, self.rayleigh_alpha, self.rayleigh_beta
+        nm.alpha, nm.delta, nm.dt, nm.n_steps = self.alpha, self.delta, self.time_step, self.steps
+        nm.acc_amp, nm.acc_period, nm.acc_dof = self.load.magnitude, self.load.period, self.load.dof
+        return nm
+
+    def Solve(self, keep_solutions=True):
+        self.BuildMatrices()
+        if self.RandomNumbers is None:
+            self.Initialize()
+        R, S = self.simulations, self.steps
+        xi = N.f64(self.RandomNumbers)
+        f = N.f64(self.model.subdomains[0].RHS) if self.static_loads else None
+        hist = np.zeros((R, S))
+        U = np.zeros((R, self.model.n_dofs)) if keep_solutions else None
+        its = np.zeros(R, dtype=np.int32)
+        s = self.kl.struct()
+        nm = self.params()
+        st = N.lib().MSG_NEWMARK_BATCH(self.mesh.handle, float(self.model.poisson), C.byref(s), R, N.ptr(xi),
+                                       C.byref(nm), N.ptr(f) if f is not None else None, int(self.max_iterations),
+                                       float(self.tolerance), int(self.tip_dof), N.ptr(hist),
+                                       N.ptr(U) if U is not None else None, N.ptr(its, N._i))
+        self.TipHistory, self.Solutions, self.Iterations = hist, U, its
+        N.check(st, self.ctx.handle, "MSG_NEWMARK_BATCH")
+        return hist

@@ -87,18 +87,24 @@ template <> struct KhatOf<double> { using type = KhatD; };
 template <class T>
 __device__ __forceinline__ T ldv(const T* p) { return __ldg(p); }
 
+// Consistent mass of a cube element as value classes: entry (a, c), (b, c2)
+// is delta(c, c2) * v[number of coordinates in which corners a and b differ].
+template <class T> struct MassClasses { T v[4]; };
+
 // Contribution of one input plane to one output node through the 4 elements
 // of one x-slab: y[c] += E_e * sum_{by,bz,c2} Khat[(an,c),(bn,c2)] * u[ey+by][ez+bz][c2]
 // with an = corner(AX, 1-ey, 1-ez) (output node in the element) and
-// bn = corner(BX, by, bz) (input node in the element).
-template <class T, int AX, int BX>
+// bn = corner(BX, by, bz) (input node in the element); with kMass also
+// + sum_{by,bz} Mhat[an,bn] u[ey+by][ez+bz][c] for every real element (E > 0).
+template <class T, int AX, int BX, bool kMass = false>
 __device__ __forceinline__ void slab_apply(const T (&kv)[kKhatClasses], const T (&u)[3][3][3], const T (&E)[2][2],
-                                           T (&y)[3]) {
+                                           T (&y)[3], const T* mv = nullptr) {
   static_for<2>([&](auto EY) {
     static_for<2>([&](auto EZ) {
       constexpr int ey = decltype(EY)::value, ez = decltype(EZ)::value;
       constexpr int an = corner_id(AX, 1 - ey, 1 - ez);
       T t[3] = {T(0), T(0), T(0)};
+      T tm[3] = {T(0), T(0), T(0)};
       static_for<2>([&](auto BY) {
         static_for<2>([&](auto BZ) {
           constexpr int by = decltype(BY)::value, bz = decltype(BZ)::value;
@@ -111,11 +117,21 @@ __device__ __forceinline__ void slab_apply(const T (&kv)[kKhatClasses], const T 
               const T k = code > 0 ? kv[cls] : -kv[cls];
               t[c] = fma(k, u[ey + by][ez + bz][c2], t[c]);
             });
+            if constexpr (kMass) {
+              constexpr int c = decltype(C)::value;
+              constexpr int dist = (AX != BX) + ((1 - ey) != by) + ((1 - ez) != bz);
+              tm[c] = fma(mv[dist], u[ey + by][ez + bz][c], tm[c]);
+            }
           });
         });
       });
 #pragma unroll
       for (int c = 0; c < 3; ++c) y[c] = fma(E[ey][ez], t[c], y[c]);
+      if constexpr (kMass) {
+        if (E[ey][ez] > T(0))
+#pragma unroll
+          for (int c = 0; c < 3; ++c) y[c] += tm[c];
+      }
     });
   });
 }
@@ -128,13 +144,19 @@ __device__ __forceinline__ void slab_apply(const T (&kv)[kKhatClasses], const T 
 // produces the operator input at a node, Own(node, v3) runs once per node of
 // the pencil with its input, Emit(node, own3, y3) receives the input and the
 // operator output at the node.
-template <class T, class Load, class Own, class Emit>
+template <class T, bool kMass = false, class Load, class Own, class Emit>
 __device__ __forceinline__ void pencil_sweep(const Lattice& L, const typename KhatOf<T>::type& K, int J, int Kz,
-                                             const T* __restrict__ E, Load load, Own own, Emit emit) {
+                                             const T* __restrict__ E, Load load, Own own, Emit emit,
+                                             const MassClasses<T>* M = nullptr) {
   const int Rp = L.Rp;
   T kv[kKhatClasses];  // class values in registers
 #pragma unroll
   for (int i = 0; i < kKhatClasses; ++i) kv[i] = K.v[i];
+  T mv[4] = {T(0), T(0), T(0), T(0)};
+  if constexpr (kMass) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mv[i] = M->v[i];
+  }
   const size_t sxy = (size_t)L.NXp, sxz = (size_t)L.NXp * L.NYp;
   const size_t row0 = (size_t)(J + L.NYp * Kz) * L.NXp;  // padded node index of x = 0
   T ym[3] = {T(0), T(0), T(0)}, y0[3] = {T(0), T(0), T(0)}, yp[3];  // outputs at P-1, P, P+1
@@ -158,10 +180,10 @@ __device__ __forceinline__ void pencil_sweep(const Lattice& L, const typename Kh
       for (int ez = 0; ez < 2; ++ez) Ecur[ey][ez] = ldv(E + (node + (ey - 1) * sxy + (ez - 1) * sxz) * Rp);
 #pragma unroll
     for (int c = 0; c < 3; ++c) yp[c] = T(0);
-    slab_apply<T, 1, 0>(kv, pl, Ecur, yp);   // slab P, output P+1
-    slab_apply<T, 0, 0>(kv, pl, Ecur, y0);   // slab P, output P
-    slab_apply<T, 1, 1>(kv, pl, Eprev, y0);  // slab P-1, output P
-    slab_apply<T, 0, 1>(kv, pl, Eprev, ym);  // slab P-1, output P-1
+    slab_apply<T, 1, 0, kMass>(kv, pl, Ecur, yp, mv);   // slab P, output P+1
+    slab_apply<T, 0, 0, kMass>(kv, pl, Ecur, y0, mv);   // slab P, output P
+    slab_apply<T, 1, 1, kMass>(kv, pl, Eprev, y0, mv);  // slab P-1, output P
+    slab_apply<T, 0, 1, kMass>(kv, pl, Eprev, ym, mv);  // slab P-1, output P-1
     if (P > 1) emit(node - 1, own_m, ym);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -691,7 +713,9 @@ __global__ void __launch_bounds__(kMThreads, 1)
       const uint32_t mk = __shfl_sync(0xffffffffu, mreg, (X - 1) & 31);
       const float* xb = xbuf + xsel * kMXFloats;
       const size_t node = nrow + X;
-      float spq = 0.f, szq = 0.f, sqq = 0.f, szr = 0.f;
+      // products in FP64: a fast-converging realization drives r and q towards the
+      // bottom of the FP32 range, where FP32 squares would underflow
+      double spq = 0.0, szq = 0.0, sqq = 0.0, szr = 0.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         float y = 0.f;
@@ -701,15 +725,17 @@ __global__ void __launch_bounds__(kMThreads, 1)
         if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
         y = ((mk >> c) & 1) ? 0.f : y;
         q_out[(node * 3 + c) * Rp + rr] = y;
-        spq = fmaf(op[c], y, spq);
-        szq = fmaf(orr[c], y, szq);
-        sqq = fmaf(y, y, sqq);
-        szr = fmaf(orr[c], orr[c], szr);
+        const double yd = (double)y, rd = (double)orr[c];
+        spq = fma((double)op[c], yd, spq);
+        szq = fma(rd, yd, szq);
+        sqq = fma(yd, yd, sqq);
+        szr = fma(rd, rd, szr);
       }
-      acc_pq += (double)spq;
-      acc_zq += (double)odv * (double)szq;
-      acc_qq += (double)odv * (double)sqq;
-      acc_zr += (double)odv * (double)szr;
+      const double dvd = (double)odv;
+      acc_pq += spq;
+      acc_zq += dvd * szq;
+      acc_qq += dvd * sqq;
+      acc_zr += dvd * szr;
     };
     auto emit_corners = [&](const float (&B)[3][4]) {
       float y[2][2][3];
@@ -809,12 +835,16 @@ __global__ void __launch_bounds__(kMThreads, 1)
   }
 }
 
-// FP64 true residual: r = b - K x (masked), r32 = (float) r; partials ||r||^2
-// and (dinv r32).r32.
+// FP64 true residual: r = b - A x (masked), r32 = (float) r; partials ||r||^2
+// and (dinv r32).r32. A = E Khat (+ Mhat on real elements when kMass); b is
+// one vector for the batch (b[node*3 + c]) or, with kBPerR, one per
+// realization in the batch layout.
+template <bool kMass, bool kBPerR>
 __global__ void __launch_bounds__(128)
-    k_resid(Lattice L, const __grid_constant__ KhatD K, const double* __restrict__ x, const double* __restrict__ b_lat,
-            const double* __restrict__ E, const uint8_t* __restrict__ mask, const float* __restrict__ dinv,
-            float* __restrict__ r32, double* __restrict__ partial) {
+    k_resid(Lattice L, const __grid_constant__ KhatD K, const __grid_constant__ MassClasses<double> M,
+            const double* __restrict__ x, const double* __restrict__ b_lat, const double* __restrict__ E,
+            const uint8_t* __restrict__ mask, const float* __restrict__ dinv, float* __restrict__ r32,
+            double* __restrict__ partial) {
   int J, Kz;
   bool valid;
   pencil_of(L, J, Kz, valid);
@@ -827,7 +857,8 @@ __global__ void __launch_bounds__(128)
       const double dv = (double)dinv[node * Rp + rr];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const double rc = ((m >> c) & 1) ? 0.0 : b_lat[node * 3 + c] - y[c];
+        const double bv = kBPerR ? b_lat[(node * 3 + c) * Rp + rr] : b_lat[node * 3 + c];
+        const double rc = ((m >> c) & 1) ? 0.0 : bv - y[c];
         const float rf = (float)rc;
         r32[(node * 3 + c) * Rp + rr] = rf;
         acc[0] += rc * rc;
@@ -839,24 +870,57 @@ __global__ void __launch_bounds__(128)
       for (int c = 0; c < 3; ++c) o[c] = ldv(x + (node * 3 + c) * Rp + rr);
     };
     auto own = [](size_t, const double*) {};
-    pencil_sweep<double>(L, K, J, Kz, E + rr, load, own, emit);
+    pencil_sweep<double, kMass>(L, K, J, Kz, E + rr, load, own, emit, &M);
   }
   cta_partial<2>(acc, partial, blockIdx.x, Rp, rr);
 }
 
-// Jacobi diagonal: K_nn,cc = Khat_diag * sum of E over the node's 8 elements
-// (all 24 diagonal entries of a cube's Khat are equal); 0 on ghosts.
-__global__ void k_dinv(Lattice L, double kdiag, const float* __restrict__ E, const int* __restrict__ interior,
-                       float* __restrict__ dinv) {
+// FP64 operator application y (+)= (E Khat + Mhat on real elements) x, no
+// mask, batch layout (the Newmark right-hand side).
+template <bool kAccumulate>
+__global__ void __launch_bounds__(128)
+    k_apply64(Lattice L, const __grid_constant__ KhatD K, const __grid_constant__ MassClasses<double> M,
+              const double* __restrict__ x, const double* __restrict__ E, double* __restrict__ y) {
+  int J, Kz;
+  bool valid;
+  pencil_of(L, J, Kz, valid);
+  const int Rp = L.Rp;
+  const int rr = blockIdx.y * 32 + threadIdx.x;
+  if (!valid) return;
+  auto emit = [&](size_t node, const double*, const double* v) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double* o = y + (node * 3 + c) * Rp + rr;
+      *o = kAccumulate ? *o + v[c] : v[c];
+    }
+  };
+  auto load = [&](size_t node, double* o) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[c] = ldv(x + (node * 3 + c) * Rp + rr);
+  };
+  auto own = [](size_t, const double*) {};
+  pencil_sweep<double, true>(L, K, J, Kz, E + rr, load, own, emit, &M);
+}
+
+// Jacobi diagonal: A_nn,cc = Khat_diag * sum of E over the node's 8 elements
+// (all 24 diagonal entries of a cube's Khat are equal) + Mhat_diag * the
+// number of real elements (E > 0) around the node; 0 on ghosts.
+__global__ void k_dinv(Lattice L, double kdiag, double mdiag, const float* __restrict__ E,
+                       const int* __restrict__ interior, float* __restrict__ dinv) {
   const int t = blockIdx.x;
   const size_t node = (size_t)interior[t];
   const size_t sxy = (size_t)L.NXp, sxz = (size_t)L.NXp * L.NYp;
   for (int rr = threadIdx.x; rr < L.Rp; rr += blockDim.x) {
     double s = 0;
+    int n_real = 0;
     for (int ez = -1; ez <= 0; ++ez)
       for (int ey = -1; ey <= 0; ++ey)
-        for (int ex = -1; ex <= 0; ++ex) s += (double)E[(node + ex + ey * sxy + ez * sxz) * L.Rp + rr];
-    dinv[node * L.Rp + rr] = (float)(1.0 / (kdiag * s));
+        for (int ex = -1; ex <= 0; ++ex) {
+          const float e = E[(node + ex + ey * sxy + ez * sxz) * L.Rp + rr];
+          s += (double)e;
+          n_real += e > 0.f;
+        }
+    dinv[node * L.Rp + rr] = (float)(1.0 / (kdiag * s + mdiag * n_real));
   }
 }
 
@@ -1111,7 +1175,6 @@ __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, con
     s.beta[r] = (a && !first && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
     s.gamma[r] = g;
     s.rho_ref[r] = gamma_ref ? g : rr;
-    if (first) s.gamma0[r] = g;
     s.alpha[r] = 0.f;  // the pending alpha p term was folded into x (and no r update is pending)
     active = a;
   }
@@ -1136,7 +1199,11 @@ __global__ void __launch_bounds__(1024) k_alpha_gamma(int Rp, int n_tiles, const
       const double pq = v[0], zq = v[1], qdq = v[2], g = v[3];
       const double al = g / pq;
       double gn = g - 2.0 * al * zq + al * al * qdq;
-      if (!(pq > 0.0) || !(g > 0.0) || !(gn == gn)) {
+      if (g == 0.0) {
+        // the recursive residual vanished: hold still and ask for a true-residual check
+        active = 1;
+        upd = 1;
+      } else if (!(pq > 0.0) || !(g > 0.0) || !(gn == gn)) {
         s.act[r] = 0;
         s.breakdown[r] = 1;
       } else {
@@ -1159,6 +1226,116 @@ __global__ void __launch_bounds__(1024) k_alpha_gamma(int Rp, int n_tiles, const
     if (active) atomicAdd(s.n_active, active);
     if (upd) atomicAdd(s.n_update, upd);
   }
+}
+
+// Per-realization ||b||^2 and (dinv b).b of a batch right-hand side (shared
+// vector b[node*3 + c] or, with per_r, the batch layout): CTA partials
+// [blk][Rp][2] over a slice of the interior nodes (32 realizations x 8 groups).
+__global__ void __launch_bounds__(256) k_bsq(int n_int, int Rp, const int* __restrict__ interior,
+                                             const double* __restrict__ b, int per_r, const float* __restrict__ dinv,
+                                             double* __restrict__ partial) {
+  __shared__ double sh[8][2][32];
+  const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const int rr = blockIdx.y * 32 + lane;
+  const int per = (n_int + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(n_int, t0 + per);
+  double a = 0.0, z = 0.0;
+  for (int t = t0 + g; t < t1; t += 8) {
+    const size_t n = (size_t)interior[t];
+    const double dv = (double)dinv[n * Rp + rr];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double v = per_r ? b[(n * 3 + c) * Rp + rr] : b[n * 3 + c];
+      a += v * v;
+      z += dv * v * v;
+    }
+  }
+  sh[g][0][lane] = a;
+  sh[g][1][lane] = z;
+  __syncthreads();
+  if (g == 0) {
+    double sa = 0.0, sz = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      sa += sh[k][0][lane];
+      sz += sh[k][1][lane];
+    }
+    partial[((size_t)blockIdx.x * Rp + rr) * 2] = sa;
+    partial[((size_t)blockIdx.x * Rp + rr) * 2 + 1] = sz;
+  }
+}
+
+// bnorm = ||b|| and gamma0 = (dinv b).b per realization (0 beyond R)
+__global__ void __launch_bounds__(1024) k_bnorm(int R, int Rp, int n_blk, const double* __restrict__ partial, Scal s) {
+  double v[2];
+  reduce_rows<2>(partial, n_blk, Rp, v);
+  const int r = blockIdx.x * 32 + threadIdx.x;
+  if (threadIdx.x < 32) {
+    s.bnorm[r] = r < R ? sqrt(v[0]) : 0.0;
+    s.gamma0[r] = r < R ? v[1] : 0.0;
+  }
+}
+
+// Newmark right-hand-side inputs (interior nodes, batch layout):
+// w1 = c1u u + c1v v + c1a a (mass part), w2 = c2u u + c2v v + c2a a (stiffness part)
+__global__ void k_nm_pre(int n_int, int Rp, const int* __restrict__ interior, const double* __restrict__ u,
+                         const double* __restrict__ v, const double* __restrict__ a, double c1u, double c1v,
+                         double c1a, double c2u, double c2v, double c2a, double* __restrict__ w1,
+                         double* __restrict__ w2) {
+  const size_t total = (size_t)n_int * 3 * Rp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = i / Rp;
+    const size_t o = ((size_t)interior[row / 3] * 3 + row % 3) * Rp + (i - row * Rp);
+    const double uu = c1u * u[o] + c1v * v[o] + c1a * a[o];
+    const double uc = c2u * u[o] + c2v * v[o] + c2a * a[o];
+    w1[o] = uu;
+    w2[o] = uc;
+  }
+}
+
+// y = (free rows) y + f_static + ag * fM, 0 on constrained rows
+__global__ void k_nm_rhs(int n_int, int Rp, const int* __restrict__ interior, const uint8_t* __restrict__ mask,
+                         const double* __restrict__ f_static, const double* __restrict__ fM, double ag,
+                         double* __restrict__ y) {
+  const size_t total = (size_t)n_int * 3 * Rp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = i / Rp;
+    const size_t node = (size_t)interior[row / 3];
+    const int c = (int)(row % 3);
+    const size_t o = (node * 3 + c) * Rp + (i - row * Rp);
+    const double f = (f_static ? f_static[node * 3 + c] : 0.0) + ag * fM[node * 3 + c];
+    y[o] = ((mask[node] >> c) & 1) ? 0.0 : y[o] + f;
+  }
+}
+
+// after the solve x of step i: a' = a0 (x - u) - a2 v - a3 a, v += a6 a + a7 a', u = x
+__global__ void k_nm_post(int n_int, int Rp, const int* __restrict__ interior, const double* __restrict__ x,
+                          double* __restrict__ u, double* __restrict__ v, double* __restrict__ a, double a0,
+                          double a2, double a3, double a6, double a7) {
+  const size_t total = (size_t)n_int * 3 * Rp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = i / Rp;
+    const size_t o = ((size_t)interior[row / 3] * 3 + row % 3) * Rp + (i - row * Rp);
+    const double an = a0 * (x[o] - u[o]) - a2 * v[o] - a3 * a[o];
+    v[o] += a6 * a[o] + a7 * an;
+    a[o] = an;
+    u[o] = x[o];
+  }
+}
+
+// unit vector field: component dir = 1 at every interior node (batch layout)
+__global__ void k_unit_dir(int n_int, int Rp, const int* __restrict__ interior, int dir, double* __restrict__ e) {
+  const size_t total = (size_t)n_int * Rp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t t = i / Rp;
+    e[((size_t)interior[t] * 3 + dir) * Rp + (i - t * Rp)] = 1.0;
+  }
+}
+
+// one realization's column of a batch-layout vector into a shared vector
+__global__ void k_column(size_t n, int Rp, int r, const double* __restrict__ a, double* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = a[i * Rp + r];
 }
 
 __global__ void k_lattice_rhs(int n_dofs, const int* __restrict__ rows, const double* __restrict__ b_dof,
@@ -1187,11 +1364,6 @@ __global__ void k_gather_solution(int n_dofs, int R, int Rp, const int* __restri
 __global__ void k_gather_tip(int R, int Rp, int row, const double* __restrict__ x, double* __restrict__ tip) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r < R) tip[r] = x[(size_t)row * Rp + r];
-}
-
-__global__ void k_set_bnorm(int R, int Rp, double bn, double* __restrict__ bnorm) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < Rp) bnorm[r] = r < R ? bn : 0.0;
 }
 
 __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -1288,137 +1460,258 @@ struct WSlot {
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
-}  // namespace
-
-int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
-                      const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out) {
-  if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mesh is not a structured cube lattice");
+// Everything one batch of solves on a structured lattice shares: sizes,
+// operator coefficients (A = cK E Khat + cM Mhat), workspace, tensor maps.
+struct BlockSys {
   Lattice L;
+  int R = 0, Rp = 0;
+  size_t npad = 0, nvec = 0;
+  int n_tiles = 0, tiles_jm = 0, n_tiles_m = 0, n_items_m = 0, grid_m = 0, n_upd = 0, n_bsq = 0;
+  bool modal = true, mass = false;
+  double cK = 1.0, cM = 0.0, kdiag = 0.0, mdiag = 0.0;
+  KhatF KF;
+  KhatD KD;               // cK-scaled classes
+  MassClasses<double> MD; // cM-scaled mass classes
+  ModalC MC;
+  const int* interior = nullptr;
+  const uint8_t* mask = nullptr;
+  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal, pB, rB, qB;
+  size_t scal_bytes = 0;
+  Scal s;
+  CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
+};
+
+// Coefficients and workspace of a batch: A = cK E Khat(nu) + cM Mhat(rho).
+int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double cM, int R, int Rp, BlockSys* B) {
+  if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mesh is not a structured cube lattice");
+  Lattice& L = B->L;
   L.NX = m->nx + 1; L.NY = m->ny + 1; L.NZ = m->nz + 1;
   L.NXp = m->NXp; L.NYp = m->NYp; L.NZp = m->NZp;
   L.Rp = Rp;
   L.tiles_j = (L.NY + kTJ - 1) / kTJ;
   L.n_pad = L.NXp * L.NYp * L.NZp;
   L.n_int = L.NX * L.NY * L.NZ;
-  const int tiles_k = (L.NZ + kTK - 1) / kTK;
-  const int n_tiles = L.tiles_j * tiles_k;
-  const size_t npad = (size_t)L.n_pad;
-  const size_t nvec = npad * 3 * Rp;
+  B->R = R;
+  B->Rp = Rp;
+  B->n_tiles = L.tiles_j * ((L.NZ + kTK - 1) / kTK);
+  B->npad = (size_t)L.n_pad;
+  B->nvec = B->npad * 3 * Rp;
+  B->interior = m->d_pad_interior.as<int>();
+  B->mask = m->d_pad_mask.as<uint8_t>();
+  B->cK = cK;
+  B->cM = cM;
+  B->mass = cM != 0.0;
+  B->modal = ctx->modal != 0;
+  if (B->mass && !B->modal)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "a mass term needs the modal operator (modal_operator = 1)");
   cudaStream_t st = ctx->stream;
-  const int* interior = m->d_pad_interior.as<int>();
-  const uint8_t* mask = m->d_pad_mask.as<uint8_t>();
 
   double K576[576];
   MSG_TRY(unit_cube_khat(ctx, m->h, nu, K576));
-  KhatF KF;
-  KhatD KD;
   for (int c = 0; c < kKhatClasses; ++c) {
-    KD.v[c] = K576[kKhatRep[c]];
-    KF.v[c] = (float)KD.v[c];
+    const double v = K576[kKhatRep[c]];
+    B->KD.v[c] = cK * v;
+    B->KF.v[c] = (float)(cK * v);
   }
   for (int i = 0; i < 576; ++i) {  // the element must have the cube's class structure
     const int code = kKhatClass[i];
-    const double v = code > 0 ? KD.v[code - 1] : -KD.v[-code - 1];
-    if (std::fabs(v - K576[i]) > 1e-12 * std::fabs(KD.v[0]))
+    const double v = code > 0 ? K576[kKhatRep[code - 1]] : -K576[kKhatRep[-code - 1]];
+    if (std::fabs(v - K576[i]) > 1e-12 * std::fabs(K576[kKhatRep[0]]))
       return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element stiffness does not have the unit-cube structure");
   }
-  const double kdiag = K576[0];
-  const bool modal = ctx->modal != 0;
-  ModalC MC{};
-  if (modal) MSG_TRY(modal_coefficients(ctx, K576, nullptr, 1.0, 0.0, &MC));
-  // modal operator: 4 x 4 node tiles, persistent CTAs over (tile, realization group) items
-  const int tiles_jm = (L.NY + kMJ - 1) / kMJ, n_tiles_m = tiles_jm * ((L.NZ + kMK - 1) / kMK);
-  const int n_items_m = n_tiles_m * (Rp / 32);
-  const int grid_m = std::min(n_items_m, ctx->sm_count);
-
-  // workspace of the batch (context slots 0-11, reused by the next batch)
-  WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal, pB, rB, qB;
-  MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &x.ptr));
-  MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &r32.ptr));
-  MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &p.ptr));
-  if (modal) {  // second buffers of p, r and q for the single-reduction loop
-    MSG_TRY(workspace(ctx, 18, sizeof(float) * nvec, &pB.ptr));
-    MSG_TRY(workspace(ctx, 19, sizeof(float) * nvec, &rB.ptr));
-    MSG_TRY(workspace(ctx, 20, sizeof(float) * nvec, &qB.ptr));
+  B->kdiag = cK * K576[0];
+  double M576[576];
+  for (int i = 0; i < 4; ++i) B->MD.v[i] = 0.0;
+  if (B->mass) {
+    MSG_TRY(unit_cube_mhat(ctx, m->h, rho, M576));
+    // classes by the number of differing corner coordinates; check the structure
+    auto cc = [](int a, int k) {
+      const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
+      return k == 0 ? ax : (k == 1 ? ay : az);
+    };
+    auto dist = [&](int a, int b) { return (cc(a, 0) != cc(b, 0)) + (cc(a, 1) != cc(b, 1)) + (cc(a, 2) != cc(b, 2)); };
+    double rep[4] = {0, 0, 0, 0};
+    for (int b = 0; b < 8; ++b) rep[dist(0, b)] = M576[(3 * 0) * 24 + 3 * b];
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b)
+        for (int c = 0; c < 3; ++c)
+          for (int c2 = 0; c2 < 3; ++c2) {
+            const double expect = c == c2 ? rep[dist(a, b)] : 0.0;
+            if (std::fabs(M576[(3 * a + c) * 24 + 3 * b + c2] - expect) > 1e-12 * std::fabs(rep[0]))
+              return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element mass does not have the cube structure");
+          }
+    for (int i = 0; i < 4; ++i) B->MD.v[i] = cM * rep[i];
+    B->mdiag = cM * rep[0];
   }
-  MSG_TRY(workspace(ctx, 3, sizeof(float) * nvec, &q.ptr));
-  MSG_TRY(workspace(ctx, 4, sizeof(float) * nvec, &d.ptr));
-  MSG_TRY(workspace(ctx, 5, sizeof(float) * npad * Rp, &dinv.ptr));
-  MSG_TRY(workspace(ctx, 6, sizeof(double) * npad * Rp, &E64.ptr));
-  MSG_TRY(workspace(ctx, 7, sizeof(float) * npad * Rp, &E32.ptr));
-  MSG_TRY(workspace(ctx, 8, sizeof(double) * npad * 3, &blat.ptr));
-  const int n_upd = std::min(L.n_int, ctx->sm_count * 4);
-  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)std::max(n_tiles * 2, n_tiles_m * kMParts) * Rp, &part_op.ptr));
-  MSG_TRY(workspace(ctx, 10, sizeof(double) * (size_t)n_upd * Rp * 2, &part_up.ptr));
-  const size_t scal_bytes = (sizeof(float) * 2 + sizeof(double) * 6 + sizeof(int) * 4) * (size_t)Rp + 64;
-  MSG_TRY(workspace(ctx, 11, scal_bytes, &scal.ptr));
-  MSG_CUDA(ctx, cudaMemsetAsync(scal.ptr, 0, scal_bytes, st));
-  Scal s;
+  if (B->modal) MSG_TRY(modal_coefficients(ctx, K576, B->mass ? M576 : nullptr, cK, cM, &B->MC));
+  B->tiles_jm = (L.NY + kMJ - 1) / kMJ;
+  B->n_tiles_m = B->tiles_jm * ((L.NZ + kMK - 1) / kMK);
+  B->n_items_m = B->n_tiles_m * (Rp / 32);
+  B->grid_m = std::min(B->n_items_m, ctx->sm_count);
+  B->n_upd = std::min(L.n_int, ctx->sm_count * 4);
+  B->n_bsq = std::min(L.n_int, ctx->sm_count * 2);
+
+  // workspace (context slots, reused by the next batch)
+  const size_t nvec = B->nvec, npad = B->npad;
+  MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &B->x.ptr));
+  MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &B->r32.ptr));
+  MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &B->p.ptr));
+  MSG_TRY(workspace(ctx, 3, sizeof(float) * nvec, &B->q.ptr));
+  MSG_TRY(workspace(ctx, 4, sizeof(float) * nvec, &B->d.ptr));
+  MSG_TRY(workspace(ctx, 5, sizeof(float) * npad * Rp, &B->dinv.ptr));
+  MSG_TRY(workspace(ctx, 6, sizeof(double) * npad * Rp, &B->E64.ptr));
+  MSG_TRY(workspace(ctx, 7, sizeof(float) * npad * Rp, &B->E32.ptr));
+  MSG_TRY(workspace(ctx, 8, sizeof(double) * npad * 3, &B->blat.ptr));
+  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)std::max(B->n_tiles * 2, B->n_tiles_m * kMParts) * Rp,
+                    &B->part_op.ptr));
+  MSG_TRY(workspace(ctx, 10, sizeof(double) * (size_t)std::max(B->n_upd, B->n_bsq) * Rp * 2, &B->part_up.ptr));
+  B->scal_bytes = (sizeof(float) * 2 + sizeof(double) * 6 + sizeof(int) * 4) * (size_t)Rp + 64;
+  MSG_TRY(workspace(ctx, 11, B->scal_bytes, &B->scal.ptr));
+  if (B->modal) {  // second buffers of p, r and q for the single-reduction loop
+    MSG_TRY(workspace(ctx, 18, sizeof(float) * nvec, &B->pB.ptr));
+    MSG_TRY(workspace(ctx, 19, sizeof(float) * nvec, &B->rB.ptr));
+    MSG_TRY(workspace(ctx, 20, sizeof(float) * nvec, &B->qB.ptr));
+  }
+  Scal& sc = B->s;
   {
-    char* base = scal.as<char>();
-    s.alpha = (float*)base; base += sizeof(float) * Rp;
-    s.beta = (float*)base; base += sizeof(float) * Rp;
-    s.gamma = (double*)base; base += sizeof(double) * Rp;
-    s.gamma_prev = (double*)base; base += sizeof(double) * Rp;
-    s.rho_ref = (double*)base; base += sizeof(double) * Rp;
-    s.res = (double*)base; base += sizeof(double) * Rp;
-    s.bnorm = (double*)base; base += sizeof(double) * Rp;
-    s.gamma0 = (double*)base; base += sizeof(double) * Rp;
-    s.act = (int*)base; base += sizeof(int) * Rp;
-    s.done = (int*)base; base += sizeof(int) * Rp;
-    s.its = (int*)base; base += sizeof(int) * Rp;
-    s.breakdown = (int*)base; base += sizeof(int) * Rp;
-    s.n_active = (int*)base; base += 16;
-    s.n_update = (int*)base; base += 16;
-    s.err = (int*)base;  // outside the 32 bytes the iterations clear
+    char* base = B->scal.as<char>();
+    sc.alpha = (float*)base; base += sizeof(float) * Rp;
+    sc.beta = (float*)base; base += sizeof(float) * Rp;
+    sc.gamma = (double*)base; base += sizeof(double) * Rp;
+    sc.gamma_prev = (double*)base; base += sizeof(double) * Rp;
+    sc.rho_ref = (double*)base; base += sizeof(double) * Rp;
+    sc.res = (double*)base; base += sizeof(double) * Rp;
+    sc.bnorm = (double*)base; base += sizeof(double) * Rp;
+    sc.gamma0 = (double*)base; base += sizeof(double) * Rp;
+    sc.act = (int*)base; base += sizeof(int) * Rp;
+    sc.done = (int*)base; base += sizeof(int) * Rp;
+    sc.its = (int*)base; base += sizeof(int) * Rp;
+    sc.breakdown = (int*)base; base += sizeof(int) * Rp;
+    sc.n_active = (int*)base; base += 16;
+    sc.n_update = (int*)base; base += 16;
+    sc.err = (int*)base;  // outside the 32 bytes the iterations clear
   }
   // zero every padded vector once: ghost entries must stay zero
-  MSG_CUDA(ctx, cudaMemsetAsync(x.ptr, 0, sizeof(double) * nvec, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(r32.ptr, 0, sizeof(float) * nvec, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(p.ptr, 0, sizeof(float) * nvec, st));
-  if (modal) {
-    MSG_CUDA(ctx, cudaMemsetAsync(pB.ptr, 0, sizeof(float) * nvec, st));
-    MSG_CUDA(ctx, cudaMemsetAsync(rB.ptr, 0, sizeof(float) * nvec, st));
-    MSG_CUDA(ctx, cudaMemsetAsync(qB.ptr, 0, sizeof(float) * nvec, st));
-  }
-  MSG_CUDA(ctx, cudaMemsetAsync(q.ptr, 0, sizeof(float) * nvec, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(d.ptr, 0, sizeof(float) * nvec, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(dinv.ptr, 0, sizeof(float) * npad * Rp, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(E64.ptr, 0, sizeof(double) * npad * Rp, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(blat.ptr, 0, sizeof(double) * npad * 3, st));
-  // field of every realization straight into the padded element layout
-  cudaEvent_t f0, f1;
-  MSG_CUDA(ctx, cudaEventCreate(&f0));
-  MSG_CUDA(ctx, cudaEventCreate(&f1));
-  cudaEventRecord(f0, st);
-  MSG_TRY(launch_kl_field(ctx, m, kl, R, Rp, d_xi, E64.as<double>(), nullptr, nullptr, m->d_pad_elem_row.as<int>()));
-  k_f64_to_f32<<<ctx->sm_count * 8, 256, 0, st>>>(npad * Rp, E64.as<double>(), E32.as<float>());
-  cudaEventRecord(f1, st);
-  // b in lattice layout and ||b|| (one load vector for the whole batch)
-  k_lattice_rhs<<<(m->n_dofs + 255) / 256, 256, 0, st>>>(m->n_dofs, m->d_pad_free_rows.as<int>(), d_b_dof,
-                                                         blat.as<double>());
-  std::vector<double> hb(m->n_dofs);
-  MSG_CUDA(ctx, cudaMemcpyAsync(hb.data(), d_b_dof, sizeof(double) * m->n_dofs, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaStreamSynchronize(st));
-  float fms = 0.f;
-  cudaEventElapsedTime(&fms, f0, f1);
-  ctx->t_phase[0] = fms;
-  cudaEventDestroy(f0);
-  cudaEventDestroy(f1);
-  double bb = 0;
-  for (double v : hb) bb += v * v;
-  k_set_bnorm<<<(Rp + 127) / 128, 128, 0, st>>>(R, Rp, std::sqrt(bb), s.bnorm);
-  k_dinv<<<L.n_int, 128, 0, st>>>(L, kdiag, E32.as<float>(), interior, dinv.as<float>());
-  count_launch(ctx, 5);
-  MSG_CUDA(ctx, cudaGetLastError());
+  const WSlot* v32[] = {&B->r32, &B->p, &B->q, &B->d, &B->pB, &B->rB, &B->qB};
+  for (const WSlot* w : v32)
+    if (w->ptr) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(float) * nvec, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(B->x.ptr, 0, sizeof(double) * nvec, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(B->dinv.ptr, 0, sizeof(float) * npad * Rp, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(B->E64.ptr, 0, sizeof(double) * npad * Rp, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(B->blat.ptr, 0, sizeof(double) * npad * 3, st));
 
-  const dim3 op_grid(n_tiles, Rp / 32), op_block(32, kWarps);
+  // TMA descriptors of the FP32 batch vectors (5-D: realization, component,
+  // x, y, z) and of the FP32 element field and dinv (4-D: realization, x, y, z)
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &qr) == cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  if (!encode) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t fb = sizeof(float);
+  const cuuint64_t pd[5] = {(cuuint64_t)Rp, 3, (cuuint64_t)L.NXp, (cuuint64_t)L.NYp, (cuuint64_t)L.NZp};
+  const cuuint64_t ps[4] = {Rp * fb, 3 * Rp * fb, 3 * Rp * fb * L.NXp, 3 * Rp * fb * L.NXp * L.NYp};
+  const cuuint64_t ed[4] = {(cuuint64_t)Rp, (cuuint64_t)L.NXp, (cuuint64_t)L.NYp, (cuuint64_t)L.NZp};
+  const cuuint64_t es[3] = {Rp * fb, Rp * fb * L.NXp, Rp * fb * L.NXp * L.NYp};
+  const cuuint32_t one[5] = {1, 1, 1, 1, 1};
+  auto enc5 = [&](CUtensorMap* tm, void* base, const cuuint32_t* box) {
+    return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base, pd, ps, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  auto enc4 = [&](CUtensorMap* tm, void* base, const cuuint32_t* box) {
+    return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ed, es, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  CUresult e = CUDA_SUCCESS;
+  if (B->modal) {
+    // modal loop: r, q, p (both buffers) and dinv patches with halo, the element patch, the tile's d
+    const cuuint32_t pbm[5] = {32, 3, 1, kMPJ, kMPK};
+    const cuuint32_t nbm[4] = {32, 1, kMPJ, kMPK};
+    const cuuint32_t ebm[4] = {32, 1, kMEJ, kMEK};
+    const cuuint32_t dbm[5] = {32, 3, 1, kMJ, kMK};
+    const CUresult rs[9] = {enc5(&B->tm_rAm, B->r32.ptr, pbm), enc5(&B->tm_rBm, B->rB.ptr, pbm),
+                            enc5(&B->tm_qAm, B->q.ptr, pbm),   enc5(&B->tm_qBm, B->qB.ptr, pbm),
+                            enc5(&B->tm_pAm, B->p.ptr, pbm),   enc5(&B->tm_pBm, B->pB.ptr, pbm),
+                            enc4(&B->tm_dinvm, B->dinv.ptr, nbm), enc4(&B->tm_em, B->E32.ptr, ebm),
+                            enc5(&B->tm_dm, B->d.ptr, dbm)};
+    for (CUresult r : rs)
+      if (r != CUDA_SUCCESS) e = r;
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+      attr_err = cudaFuncSetAttribute(k_op_modal<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMSmem);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_op_modal<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMSmem);
+    });
+    MSG_CUDA(ctx, attr_err);
+  } else {
+    const cuuint32_t pb[5] = {32, 3, 1, kPJ, kPK};
+    const cuuint32_t eb[4] = {32, 1, kEJ, kEK};
+    const CUresult r1 = enc5(&B->tm_p, B->p.ptr, pb), r2 = enc4(&B->tm_e, B->E32.ptr, eb);
+    e = r1 != CUDA_SUCCESS ? r1 : r2;
+  }
+  if (e != CUDA_SUCCESS) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
+  return MSG_OK;
+}
+
+// Field of every realization straight into the padded element layout (FP64
+// and FP32), and the Jacobi diagonal of A.
+int block_field(Context* ctx, Mesh* m, BlockSys* B, const KLDevice* kl, const double* d_xi) {
+  cudaStream_t st = ctx->stream;
+  MSG_TRY(context_resources(ctx));
+  cudaEvent_t* ev = ctx->ev;
+  cudaEventRecord(ev[10], st);
+  MSG_TRY(launch_kl_field(ctx, m, kl, B->R, B->Rp, d_xi, B->E64.as<double>(), nullptr, nullptr,
+                          m->d_pad_elem_row.as<int>()));
+  k_f64_to_f32<<<ctx->sm_count * 8, 256, 0, st>>>(B->npad * B->Rp, B->E64.as<double>(), B->E32.as<float>());
+  cudaEventRecord(ev[11], st);
+  k_dinv<<<B->L.n_int, 128, 0, st>>>(B->L, B->kdiag, B->mdiag, B->E32.as<float>(), B->interior,
+                                     B->dinv.as<float>());
+  count_launch(ctx, 2);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+// Solve A x = b for every realization of the batch to the FP64 true relative
+// residual tol: b is one vector (blat layout) or one per realization; x (slot 0)
+// starts from zero, or from its content when warm. Per-realization results stay
+// in B->s (its, res, done, breakdown); returns the batch status.
+int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool warm, int max_it, double tol,
+                bool record_phases, int chunk_cap = 0) {
+  const Lattice& L = B->L;
+  const int Rp = B->Rp;
+  const bool modal = B->modal;
+  cudaStream_t st = ctx->stream;
+  Scal& s = B->s;
+  const int* interior = B->interior;
+  const uint8_t* mask = B->mask;
+  WSlot &x = B->x, &r32 = B->r32, &p = B->p, &q = B->q, &d = B->d, &dinv = B->dinv, &part_op = B->part_op,
+        &part_up = B->part_up, &pB = B->pB, &rB = B->rB, &qB = B->qB;
+  const size_t nvec = B->nvec;
+  MSG_CUDA(ctx, cudaMemsetAsync(B->scal.ptr, 0, B->scal_bytes, st));
+  if (!warm) MSG_CUDA(ctx, cudaMemsetAsync(x.ptr, 0, sizeof(double) * nvec, st));
+  // directions, operator outputs and the correction start from zero
+  const WSlot* z32[] = {&p, &q, &d, &pB, &qB};
+  for (const WSlot* w : z32)
+    if (w->ptr) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(float) * nvec, st));
+  // ||b|| and (dinv b).b per realization
+  k_bsq<<<dim3(B->n_bsq, Rp / 32), 256, 0, st>>>(L.n_int, Rp, interior, b, b_per_r ? 1 : 0, dinv.as<float>(),
+                                                part_up.as<double>());
+  k_bnorm<<<Rp / 32, 1024, 0, st>>>(B->R, Rp, B->n_bsq, part_up.as<double>(), s);
+  count_launch(ctx, 2);
+
+  const dim3 op_grid(B->n_tiles, Rp / 32), op_block(32, kWarps);
   const int Q = Rp / 4;
   const int G = Q >= 256 ? 1 : 256 / Q;
   const size_t upd_smem = G > 1 ? sizeof(double) * (size_t)G * Q * 8 : 0;
   const int sblocks = Rp / 32;  // scalar kernels: 32 realizations x 32 row groups per CTA
   const int n_xu = ctx->sm_count * 8;
   const int n_dir = std::min(L.n_int, ctx->sm_count * 8);
+  const int n_upd = B->n_upd, n_tiles = B->n_tiles;
   const double delta2 = ctx->reliable_delta * ctx->reliable_delta;
   // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
   // sqrt(gamma / gamma0) is at tol/4 (single-reduction loop, dinv-weighted norm)
@@ -1429,90 +1722,30 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   cudaEvent_t* ev = ctx->ev;
   float t_resid = 0.f, t_inner = 0.f;
 
-  // TMA descriptors of p (5-D: realization, component, x, y, z) and of the
-  // FP32 element field (4-D: realization, x, y, z) for the staged operator
-  CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
-  {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-      void* f = nullptr;
-      cudaDriverEntryPointQueryResult q;
-      if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-          q == cudaDriverEntryPointSuccess)
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-    });
-    if (!encode) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-    const cuuint64_t fb = sizeof(float);
-    const cuuint64_t pd[5] = {(cuuint64_t)Rp, 3, (cuuint64_t)L.NXp, (cuuint64_t)L.NYp, (cuuint64_t)L.NZp};
-    const cuuint64_t ps[4] = {Rp * fb, 3 * Rp * fb, 3 * Rp * fb * L.NXp, 3 * Rp * fb * L.NXp * L.NYp};
-    const cuuint32_t pb[5] = {32, 3, 1, kPJ, kPK};
-    const cuuint32_t one[5] = {1, 1, 1, 1, 1};
-    CUresult e1 = encode(&tm_p, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, p.ptr, pd, ps, pb, one,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    const cuuint64_t ed[4] = {(cuuint64_t)Rp, (cuuint64_t)L.NXp, (cuuint64_t)L.NYp, (cuuint64_t)L.NZp};
-    const cuuint64_t es[3] = {Rp * fb, Rp * fb * L.NXp, Rp * fb * L.NXp * L.NYp};
-    const cuuint32_t eb[4] = {32, 1, kEJ, kEK};
-    CUresult e2 = encode(&tm_e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, E32.ptr, ed, es, eb, one,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    CUresult e3 = CUDA_SUCCESS;
-    if (modal) {
-      // modal operator: r, p (both buffers) and dinv patches with halo, the element patch, the tile's d
-      const cuuint32_t pbm[5] = {32, 3, 1, kMPJ, kMPK};
-      const cuuint32_t nbm[4] = {32, 1, kMPJ, kMPK};
-      const cuuint32_t ebm[4] = {32, 1, kMEJ, kMEK};
-      const cuuint32_t dbm[5] = {32, 3, 1, kMJ, kMK};
-      auto enc5 = [&](CUtensorMap* tm, void* base, const cuuint32_t* box) {
-        return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base, pd, ps, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      };
-      auto enc4 = [&](CUtensorMap* tm, void* base, const cuuint32_t* box) {
-        return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ed, es, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      };
-      const CUresult rs[10] = {enc5(&tm_rAm, r32.ptr, pbm), enc5(&tm_rBm, rB.ptr, pbm), enc5(&tm_qAm, q.ptr, pbm),
-                               enc5(&tm_qBm, qB.ptr, pbm), enc5(&tm_pAm, p.ptr, pbm), enc5(&tm_pBm, pB.ptr, pbm),
-                              enc4(&tm_dinvm, dinv.ptr, nbm), enc4(&tm_em, E32.ptr, ebm), enc5(&tm_dm, d.ptr, dbm)};
-      for (CUresult r : rs)
-        if (r != CUDA_SUCCESS) e3 = r;
-    }
-    if (e1 != CUDA_SUCCESS || e2 != CUDA_SUCCESS || e3 != CUDA_SUCCESS)
-      return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d, %d, %d)", (int)e1, (int)e2, (int)e3);
-  }
-  if (modal) {
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-      attr_err = cudaFuncSetAttribute(k_op_modal<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMSmem);
-    });
-    MSG_CUDA(ctx, attr_err);
-  }
-
-  const int chunk = std::max(2, ctx->chunk & ~1);
+  const int chunk = std::max(2, (chunk_cap > 0 ? std::min(ctx->chunk, chunk_cap) : ctx->chunk) & ~1);
   // The inner-loop graph is kept in the context and captured again only when
   // one of its kernel arguments changes (FNV-1a over the argument bytes).
   size_t key = 1469598103934665603ull;
   auto mix = [&key](const void* data, size_t n) {
-    const unsigned char* b = static_cast<const unsigned char*>(data);
-    for (size_t i = 0; i < n; ++i) key = (key ^ b[i]) * 1099511628211ull;
+    const unsigned char* bb = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) key = (key ^ bb[i]) * 1099511628211ull;
   };
   {
-    const void* ptrs[] = {interior, mask, r32.ptr, p.ptr, q.ptr, d.ptr, dinv.ptr, part_op.ptr, part_up.ptr, scal.ptr};
+    const void* ptrs[] = {interior, mask, r32.ptr, p.ptr, q.ptr, d.ptr, dinv.ptr, part_op.ptr, part_up.ptr,
+                          B->scal.ptr, pB.ptr, rB.ptr, qB.ptr};
     mix(ptrs, sizeof(ptrs));
     mix(&L, sizeof(L));
-    mix(&KF, sizeof(KF));
-    mix(&tm_p, sizeof(tm_p));
-    mix(&tm_e, sizeof(tm_e));
+    mix(&B->KF, sizeof(B->KF));
+    mix(&B->MC, sizeof(B->MC));
     if (modal) {
-      const CUtensorMap* tms[9] = {&tm_rAm, &tm_rBm, &tm_qAm, &tm_qBm, &tm_pAm, &tm_pBm, &tm_dinvm, &tm_em, &tm_dm};
+      const CUtensorMap* tms[9] = {&B->tm_rAm, &B->tm_rBm, &B->tm_qAm,   &B->tm_qBm, &B->tm_pAm,
+                                   &B->tm_pBm, &B->tm_dinvm, &B->tm_em, &B->tm_dm};
       for (const CUtensorMap* t : tms) mix(t, sizeof(CUtensorMap));
-      const void* bp[3] = {pB.ptr, rB.ptr, qB.ptr};
-      mix(bp, sizeof(bp));
+    } else {
+      mix(&B->tm_p, sizeof(CUtensorMap));
+      mix(&B->tm_e, sizeof(CUtensorMap));
     }
-    mix(&MC, sizeof(MC));
-    const int mm[4] = {modal ? 1 : 0, n_tiles_m, n_items_m, grid_m};
+    const int mm[6] = {modal ? 1 : 0, B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
     mix(mm, sizeof(mm));
     const double dd[2] = {delta2, tol2};
     mix(dd, sizeof(dd));
@@ -1534,22 +1767,23 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
         // alternate between their two buffers
         const bool even = (it & 1) == 0;
         if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-        k_op_modal<false><<<grid_m, kMThreads, kMSmem, st>>>(
-            L, MC, even ? tm_rAm : tm_rBm, even ? tm_qAm : tm_qBm, even ? tm_pAm : tm_pBm, tm_dinvm, tm_em, tm_dm,
-            tiles_jm, n_tiles_m, n_items_m, mask, s.alpha, s.beta, even ? rB.as<float>() : r32.as<float>(),
-            even ? pB.as<float>() : p.as<float>(), even ? qB.as<float>() : q.as<float>(), d.as<float>(),
-            part_op.as<double>(), s.err);
+        auto op = B->mass ? k_op_modal<true> : k_op_modal<false>;
+        op<<<B->grid_m, kMThreads, kMSmem, st>>>(
+            L, B->MC, even ? B->tm_rAm : B->tm_rBm, even ? B->tm_qAm : B->tm_qBm, even ? B->tm_pAm : B->tm_pBm,
+            B->tm_dinvm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m, B->n_items_m, mask, s.alpha, s.beta,
+            even ? rB.as<float>() : r32.as<float>(), even ? pB.as<float>() : p.as<float>(),
+            even ? qB.as<float>() : q.as<float>(), d.as<float>(), part_op.as<double>(), s.err);
         if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
         cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
         if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-        k_alpha_gamma<<<sblocks, 1024, 0, st>>>(Rp, n_tiles_m, part_op.as<double>(), s, delta2, tol2);
+        k_alpha_gamma<<<sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part_op.as<double>(), s, delta2, tol2);
         if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
       } else {
         k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
                                      p.as<float>(), d.as<float>());
         if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-        k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, KF, tm_p, tm_e, mask, q.as<float>(), part_op.as<double>(),
-                                                       s.err);
+        k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, B->KF, B->tm_p, B->tm_e, mask, q.as<float>(),
+                                                       part_op.as<double>(), s.err);
         if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
         k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
         if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
@@ -1579,14 +1813,31 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
   bool need_update = true, first = true;
   for (int guard = 0; guard < 1000000; ++guard) {
     if (need_update) {
-      // reliable update: x += d; d = 0; r = b - K x (FP64)
+      // reliable update: x += d; d = 0; r = b - A x (FP64)
       cudaEventRecord(ev[0], st);
       if (!first) {
         k_xupdate<<<n_xu, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, p.as<float>(), x.as<double>(), d.as<float>());
         count_launch(ctx);
       }
-      k_resid<<<op_grid, op_block, 0, st>>>(L, KD, x.as<double>(), blat.as<double>(), E64.as<double>(), mask,
-                                            dinv.as<float>(), r32.as<float>(), part_op.as<double>());
+      if (B->mass) {
+        if (b_per_r)
+          k_resid<true, true><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b, B->E64.as<double>(),
+                                                            mask, dinv.as<float>(), r32.as<float>(),
+                                                            part_op.as<double>());
+        else
+          k_resid<true, false><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b, B->E64.as<double>(),
+                                                             mask, dinv.as<float>(), r32.as<float>(),
+                                                             part_op.as<double>());
+      } else {
+        if (b_per_r)
+          k_resid<false, true><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b,
+                                                             B->E64.as<double>(), mask, dinv.as<float>(),
+                                                             r32.as<float>(), part_op.as<double>());
+        else
+          k_resid<false, false><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b,
+                                                              B->E64.as<double>(), mask, dinv.as<float>(),
+                                                              r32.as<float>(), part_op.as<double>());
+      }
       MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
       k_resid_scalars<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol, first ? 1 : 0,
                                                 modal ? 1 : 0);
@@ -1601,7 +1852,10 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
       ++n_updates;
       if (h_flags[0] == 0) break;  // every realization converged (or broke down)
     }
-    if (total_inner >= max_it) { status = MSG_ERR_NOT_CONVERGED; break; }
+    if (total_inner >= max_it) {
+      status = MSG_ERR_NOT_CONVERGED;
+      break;
+    }
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
@@ -1627,14 +1881,62 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     }
     need_update = (h_flags[4] > 0) || (h_flags[0] == 0);
   }
-  ctx->t_phase[1] = t_inner;
-  ctx->t_phase[3] = t_resid;
-  ctx->t_phase[2] = (double)n_updates;
+  if (record_phases) {
+    ctx->t_phase[1] = t_inner;
+    ctx->t_phase[3] = t_resid;
+    ctx->t_phase[2] = (double)n_updates;
+  } else {
+    ctx->t_phase[1] += t_inner;
+    ctx->t_phase[3] += t_resid;
+    ctx->t_phase[2] += (double)n_updates;
+  }
+  return status;
+}
+
+// Per-realization results of the last solve on the host; batch status.
+int block_results(Context* ctx, BlockSys* B, int status, int* its_out, double* res_out) {
+  const int Rp = B->Rp;
+  cudaStream_t st = ctx->stream;
+  std::vector<int> its(Rp), brk(Rp), done(Rp);
+  std::vector<double> res(Rp);
+  MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), B->s.its, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(brk.data(), B->s.breakdown, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(done.data(), B->s.done, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(res.data(), B->s.res, sizeof(double) * Rp, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  MSG_CUDA(ctx, cudaGetLastError());
+  for (int r = 0; r < B->R; ++r) {
+    if (its_out) its_out[r] = its[r];
+    if (res_out) res_out[r] = res[r];
+    if (!done[r] && status == MSG_OK) status = brk[r] ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
+  }
+  return status;
+}
+
+}  // namespace
+
+int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
+                      const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out) {
+  BlockSys B;
+  MSG_TRY(block_setup(ctx, m, nu, 1.0, 1.0, 0.0, R, Rp, &B));
+  cudaStream_t st = ctx->stream;
+  MSG_TRY(block_field(ctx, m, &B, kl, d_xi));
+  // b in lattice layout (one load vector for the whole batch)
+  k_lattice_rhs<<<(m->n_dofs + 255) / 256, 256, 0, st>>>(m->n_dofs, m->d_pad_free_rows.as<int>(), d_b_dof,
+                                                         B.blat.as<double>());
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  float fms = 0.f;
+  cudaEventElapsedTime(&fms, ctx->ev[10], ctx->ev[11]);
+  ctx->t_phase[0] = fms;
+  int status = block_solve(ctx, &B, B.blat.as<double>(), false, false, max_it, tol, true);
+  if (status == MSG_ERR_TIMEOUT) return status;
 
   // outputs
   if (d_X) {
     dim3 g((m->n_dofs + 31) / 32, Rp / 32);
-    k_gather_solution<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, R, Rp, m->d_pad_free_rows.as<int>(), x.as<double>(), d_X);
+    k_gather_solution<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, R, Rp, m->d_pad_free_rows.as<int>(), B.x.as<double>(),
+                                                 d_X);
     count_launch(ctx);
   }
   WSlot tipbuf;
@@ -1644,26 +1946,133 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
                                   st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     MSG_TRY(workspace(ctx, 17, sizeof(double) * Rp, &tipbuf.ptr));
-    k_gather_tip<<<(R + 127) / 128, 128, 0, st>>>(R, Rp, row, x.as<double>(), tipbuf.as<double>());
+    k_gather_tip<<<(R + 127) / 128, 128, 0, st>>>(R, Rp, row, B.x.as<double>(), tipbuf.as<double>());
     count_launch(ctx);
     MSG_CUDA(ctx, cudaMemcpyAsync(out.tip, tipbuf.ptr, sizeof(double) * R, cudaMemcpyDeviceToHost, st));
   }
-  std::vector<int> its(Rp), brk(Rp), done(Rp);
-  std::vector<double> res(Rp);
-  MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), s.its, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(brk.data(), s.breakdown, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(done.data(), s.done, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(res.data(), s.res, sizeof(double) * Rp, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaStreamSynchronize(st));
-  MSG_CUDA(ctx, cudaGetLastError());
-  for (int r = 0; r < R; ++r) {
-    if (out.iterations) out.iterations[r] = its[r];
-    if (out.rel_res) out.rel_res[r] = res[r];
-    if (!done[r] && status == MSG_OK) status = brk[r] ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
-  }
+  status = block_results(ctx, &B, status, out.iterations, out.rel_res);
   if (status != MSG_OK)
     return set_error(ctx, status, "mixed batched solve: %s",
                      status == MSG_ERR_BREAKDOWN ? "PCG breakdown" : "not converged");
+  return MSG_OK;
+}
+
+int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
+                  const NewmarkParams& nm, const double* d_f_dof, int max_it, double tol, int tip_dof,
+                  double* tip_hist, double* d_U, int* its_total) {
+  if (nm.delta < 0.5) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Newmark delta has to be bigger than 0.5");
+  const double a_limit = 0.25 * (0.5 + nm.delta) * (0.5 + nm.delta);
+  if (nm.alpha < a_limit)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Newmark alpha has to be bigger than %g", a_limit);
+  if (!(nm.dt > 0) || nm.n_steps < 0 || nm.acc_dir < 0 || nm.acc_dir > 2)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "invalid Newmark time step, step count or load direction");
+  // NewmarkDynamicAnalyzer.InitializeCoefficients
+  const double dt = nm.dt;
+  const double a0 = 1 / (nm.alpha * dt * dt), a1 = nm.delta / (nm.alpha * dt), a2 = 1 / (nm.alpha * dt);
+  const double a3 = 1 / (2 * nm.alpha) - 1, a4 = nm.delta / nm.alpha - 1, a5 = dt * 0.5 * (nm.delta / nm.alpha - 2);
+  const double a6 = dt * (1 - nm.delta), a7 = nm.delta * dt;
+  // effective matrix K + a0 M + a1 (alpha_R M + beta_R K)
+  const double cK = 1.0 + a1 * nm.ray_beta, cM = a0 + a1 * nm.ray_alpha;
+  BlockSys B;
+  MSG_TRY(block_setup(ctx, m, nu, nm.rho, cK, cM, R, Rp, &B));
+  MSG_TRY(block_field(ctx, m, &B, kl, d_xi));
+  cudaStream_t st = ctx->stream;
+  const Lattice& L = B.L;
+  const size_t nvec = B.nvec, npad = B.npad;
+  // state and right-hand-side buffers (batch layout, FP64): u, v, a, w1, w2, rhs; fM, f (shared)
+  WSlot u, v, a, w1, w2, rhs, fM, fst, hist;
+  MSG_TRY(workspace(ctx, 21, sizeof(double) * nvec, &u.ptr));
+  MSG_TRY(workspace(ctx, 22, sizeof(double) * nvec, &v.ptr));
+  MSG_TRY(workspace(ctx, 23, sizeof(double) * nvec, &a.ptr));
+  MSG_TRY(workspace(ctx, 24, sizeof(double) * nvec, &w1.ptr));
+  MSG_TRY(workspace(ctx, 25, sizeof(double) * nvec, &w2.ptr));
+  MSG_TRY(workspace(ctx, 26, sizeof(double) * nvec, &rhs.ptr));
+  MSG_TRY(workspace(ctx, 27, sizeof(double) * npad * 3, &fM.ptr));
+  MSG_TRY(workspace(ctx, 28, sizeof(double) * npad * 3, &fst.ptr));
+  MSG_TRY(workspace(ctx, 29, sizeof(double) * (size_t)std::max(1, nm.n_steps) * Rp, &hist.ptr));
+  const WSlot* zs[] = {&u, &v, &a, &w1, &w2, &rhs};
+  for (const WSlot* w : zs) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(double) * nvec, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(fst.ptr, 0, sizeof(double) * npad * 3, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(hist.ptr, 0, sizeof(double) * (size_t)std::max(1, nm.n_steps) * Rp, st));
+  if (d_f_dof)
+    k_lattice_rhs<<<(m->n_dofs + 255) / 256, 256, 0, st>>>(m->n_dofs, m->d_pad_free_rows.as<int>(), d_f_dof,
+                                                           fst.as<double>());
+  // inertial load pattern fM = Mhat-assembled unit acceleration in acc_dir at every node
+  // (Hexa8.CalculateAccelerationForces), one column of M applied to the unit field
+  KhatD kzero;
+  for (int c = 0; c < kKhatClasses; ++c) kzero.v[c] = 0.0;
+  MassClasses<double> m1;
+  for (int i = 0; i < 4; ++i) m1.v[i] = B.cM != 0.0 ? B.MD.v[i] / B.cM : 0.0;
+  const dim3 op_grid(B.n_tiles, Rp / 32), op_block(32, kWarps);
+  const int ew = ctx->sm_count * 8;
+  k_unit_dir<<<ew, 256, 0, st>>>(L.n_int, Rp, B.interior, nm.acc_dir, w1.as<double>());
+  k_apply64<false><<<op_grid, op_block, 0, st>>>(L, kzero, m1, w1.as<double>(), B.E64.as<double>(), w2.as<double>());
+  k_column<<<ew, 256, 0, st>>>(npad * 3, Rp, 0, w2.as<double>(), fM.as<double>());
+  MSG_CUDA(ctx, cudaMemsetAsync(w1.ptr, 0, sizeof(double) * nvec, st));
+  count_launch(ctx, d_f_dof ? 4 : 3);
+  // RHS operators: M (w1) and beta_R E Khat (w2)
+  KhatD kbeta;
+  for (int c = 0; c < kKhatClasses; ++c) kbeta.v[c] = (B.cK != 0.0 ? B.KD.v[c] / B.cK : 0.0) * nm.ray_beta;
+  MassClasses<double> mzero;
+  for (int i = 0; i < 4; ++i) mzero.v[i] = 0.0;
+  int row = -1;
+  if (tip_dof >= 0 && tip_dof < m->n_dofs) {
+    MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_pad_free_rows.as<int>() + tip_dof, sizeof(int), cudaMemcpyDeviceToHost,
+                                  st));
+    MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  }
+  const double two_pi = 2.0 * 3.14159265358979323846;
+  int status = MSG_OK;
+  std::vector<int> its(Rp);
+  if (its_total) std::fill(its_total, its_total + R, 0);
+  ctx->t_phase[1] = ctx->t_phase[2] = ctx->t_phase[3] = 0.0;
+  for (int i = 0; i < nm.n_steps; ++i) {
+    const double ag = nm.acc_amp * std::sin(two_pi / nm.acc_period * dt * i);
+    // uu = a0 u + a2 v + a3 a, uc = a1 u + a4 v + a5 a; M uu + C uc = M (uu + alpha_R uc) + beta_R K uc
+    k_nm_pre<<<ew, 256, 0, st>>>(L.n_int, Rp, B.interior, u.as<double>(), v.as<double>(), a.as<double>(),
+                                 a0 + nm.ray_alpha * a1, a2 + nm.ray_alpha * a4, a3 + nm.ray_alpha * a5, a1, a4, a5,
+                                 w1.as<double>(), w2.as<double>());
+    k_apply64<false><<<op_grid, op_block, 0, st>>>(L, kzero, m1, w1.as<double>(), B.E64.as<double>(),
+                                                   rhs.as<double>());
+    k_apply64<true><<<op_grid, op_block, 0, st>>>(L, kbeta, mzero, w2.as<double>(), B.E64.as<double>(),
+                                                  rhs.as<double>());
+    k_nm_rhs<<<ew, 256, 0, st>>>(L.n_int, Rp, B.interior, B.mask, d_f_dof ? fst.as<double>() : nullptr,
+                                 fM.as<double>(), ag, rhs.as<double>());
+    // warm start from the last displacement
+    MSG_CUDA(ctx, cudaMemcpyAsync(B.x.ptr, u.ptr, sizeof(double) * nvec, cudaMemcpyDeviceToDevice, st));
+    count_launch(ctx, 4);
+    // a few iterations per step: short graph chunks keep the host checks close
+    status = block_solve(ctx, &B, rhs.as<double>(), true, true, max_it, tol, false, 4);
+    if (status == MSG_ERR_TIMEOUT) return status;
+    status = block_results(ctx, &B, status, its.data(), nullptr);
+    if (status != MSG_OK)
+      return set_error(ctx, status, "Newmark step %d: %s", i,
+                       status == MSG_ERR_BREAKDOWN ? "PCG breakdown" : "not converged");
+    if (its_total)
+      for (int r = 0; r < R; ++r) its_total[r] += its[r];
+    k_nm_post<<<ew, 256, 0, st>>>(L.n_int, Rp, B.interior, B.x.as<double>(), u.as<double>(), v.as<double>(),
+                                  a.as<double>(), a0, a2, a3, a6, a7);
+    count_launch(ctx);
+    if (row >= 0) {
+      k_gather_tip<<<(R + 127) / 128, 128, 0, st>>>(R, Rp, row, u.as<double>(), hist.as<double>() + (size_t)i * Rp);
+      count_launch(ctx);
+    }
+  }
+  if (d_U) {
+    dim3 g((m->n_dofs + 31) / 32, Rp / 32);
+    k_gather_solution<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, R, Rp, m->d_pad_free_rows.as<int>(), u.as<double>(),
+                                                 d_U);
+    count_launch(ctx);
+  }
+  if (tip_hist && nm.n_steps > 0) {
+    std::vector<double> h((size_t)nm.n_steps * Rp);
+    MSG_CUDA(ctx, cudaMemcpyAsync(h.data(), hist.ptr, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+    MSG_CUDA(ctx, cudaStreamSynchronize(st));
+    for (int r = 0; r < R; ++r)
+      for (int i = 0; i < nm.n_steps; ++i) tip_hist[(size_t)r * nm.n_steps + i] = h[(size_t)i * Rp + r];
+  }
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
 }
 

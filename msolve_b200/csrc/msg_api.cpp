@@ -146,6 +146,26 @@ int unit_cube_khat(Context* ctx, double h, double nu, double* K576) {
   return MSG_OK;
 }
 
+int unit_cube_mhat(Context* ctx, double h, double rho, double* M576) {
+  double xyz[24];
+  for (int a = 0; a < 8; ++a) {
+    const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
+    xyz[3 * a] = ax * h; xyz[3 * a + 1] = ay * h; xyz[3 * a + 2] = az * h;
+  }
+  DevMem dx, dm, ds;
+  MSG_TRY(upload(ctx, dx, xyz, 24));
+  MSG_TRY(dm.alloc(ctx, sizeof(double) * 300));
+  MSG_TRY(ds.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(ds.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_me(ctx, 1, dx.as<double>(), rho, dm.as<double>(), ds.as<int>()));
+  double m300[300];
+  MSG_CUDA(ctx, cudaMemcpyAsync(m300, dm.ptr, sizeof(m300), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < 24; ++i)
+    for (int j = 0; j < 24; ++j) M576[i * 24 + j] = m300[packed_index(i, j)];
+  return MSG_OK;
+}
+
 // ------------------------------------------------------------------ mesh analysis
 static int build_pattern(Mesh* m) {
   const int nn = m->n_nodes, ne = m->n_elems;
@@ -794,6 +814,54 @@ int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const dou
     MSG_CUDA(ctx, cudaMemcpyAsync(X, dX, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  return st;
+}
+
+int MSG_NEWMARK_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const double* xi, const MSG_NEWMARK* nm,
+                      const double* f_static, int max_it, double tol, int tip_dof, double* tip_hist, double* U,
+                      int* iterations) {
+  if (!m || !kl || !xi || !nm || R <= 0 || max_it <= 0 || !(tol > 0)) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "Newmark batch needs a structured cube lattice");
+  if (tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
+  const int Rp = (R + 31) / 32 * 32;
+  MSG_TRY(context_resources(ctx));
+  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
+  cudaEventRecord(e0, ctx->stream);
+  void *dxi = nullptr, *df = nullptr, *dU = nullptr;
+  MSG_TRY(workspace(ctx, 12, sizeof(double) * (size_t)R * kl->n_terms, &dxi));
+  MSG_CUDA(ctx, cudaMemcpyAsync(dxi, xi, sizeof(double) * (size_t)R * kl->n_terms, cudaMemcpyHostToDevice, ctx->stream));
+  if (f_static) {
+    MSG_TRY(workspace(ctx, 13, sizeof(double) * (size_t)std::max(1, m->n_dofs), &df));
+    MSG_CUDA(ctx, cudaMemcpyAsync(df, f_static, sizeof(double) * (size_t)m->n_dofs, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  }
+  if (U) MSG_TRY(workspace(ctx, 14, sizeof(double) * (size_t)R * m->n_dofs, &dU));
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, m, kl, &kd));
+  NewmarkParams p;
+  p.rho = nm->rho;
+  p.ray_alpha = nm->rayleigh_alpha;
+  p.ray_beta = nm->rayleigh_beta;
+  p.alpha = nm->alpha;
+  p.delta = nm->delta;
+  p.dt = nm->dt;
+  p.n_steps = nm->n_steps;
+  p.acc_amp = nm->acc_amp;
+  p.acc_period = nm->acc_period;
+  p.acc_dir = nm->acc_dof;
+  int st = block_newmark(ctx, m, nu, &kd, static_cast<double*>(dxi), R, Rp, p, static_cast<double*>(df), max_it, tol,
+                         tip_dof, tip_hist, static_cast<double*>(dU), iterations);
+  if (U && st == MSG_OK) {
+    MSG_CUDA(ctx, cudaMemcpyAsync(U, dU, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
+    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  cudaEventRecord(e1, ctx->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  ctx->t_phase[4] = ms;
   return st;
 }
 

@@ -210,8 +210,24 @@ struct BatchOut {
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
 
+// Newmark batch (implicit integration of every realization, constant time step)
+struct NewmarkParams {
+  double rho = 1.0;                        // density of the consistent mass
+  double ray_alpha = 0.0, ray_beta = 0.0;  // Rayleigh damping C = ray_alpha M + ray_beta K
+  double alpha = 0.25, delta = 0.5;        // Newmark parameters (NewmarkDynamicAnalyzer alpha, delta)
+  double dt = 0.01;
+  int n_steps = 0;
+  double acc_amp = 0.0, acc_period = 1.0;  // ground acceleration acc_amp sin(2 pi t / acc_period)
+  int acc_dir = 0;                         // 0 x, 1 y, 2 z
+};
+int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
+                  const NewmarkParams& nm, const double* d_f_dof, int max_it, double tol, int tip_dof,
+                  double* tip_hist, double* d_U, int* its_total);
+
 // Element stiffness of one cube of side h at E=1 (host, via the K1 kernel): K[24][24] full.
 int unit_cube_khat(Context* ctx, double h, double nu, double* K576);
+// Consistent mass of one cube of side h and density rho (host, via the mass kernel): M[24][24] full.
+int unit_cube_mhat(Context* ctx, double h, double rho, double* M576);
 
 }  // namespace msg
 

@@ -156,3 +156,19 @@ def tip_dof(model):
     xyz = model.xyz
     n = int(np.argmax(xyz[:, 0] + xyz[:, 1] * 1e3 + xyz[:, 2] * 1e6))
     return model.dof_of(n, Z)
+
+
+class MassAccelerationSinusoidalLoad:
+    """Ground acceleration history (MassAccelerationSinusoidalLoad.cs:11-31):
+    load[i] = magnitude sin(2 pi / period * timeStep * i) for i < int(timeLength /
+    timeStep), else 0; dof 0/1/2 = X/Y/Z (the DOFType it acts on)."""
+
+    def __init__(self, period, time_step, time_length, magnitude, dof=0):
+        self.period, self.time_step, self.time_length, self.magnitude = period, time_step, time_length, magnitude
+        self.dof = dof
+        self.time_steps = int(time_length / time_step)
+
+    def __getitem__(self, step):
+        import math
+        return self.magnitude * math.sin(2 * math.pi / self.period * self.time_step * step) \
+            if step < self.time_steps else 0.0

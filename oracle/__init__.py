@@ -69,6 +69,10 @@ def lib():
                                     C.c_double, C.c_double, C.c_int, _d]),
             "orc_block_solve_pcg": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, _u8, _d, C.c_double,
                                               _d, _d, C.c_int, C.c_double, _i, _d]),
+            "orc_block_newmark": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, _u8, _d, C.c_double, C.c_double,
+                                            C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                            C.c_double, C.c_double, C.c_int, _d, C.c_int, C.c_double, C.c_int,
+                                            _d, _d, _i]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -324,6 +328,23 @@ def block_solve_pcg(nx, ny, nz, constrained, E_elem, nu, b, h=1.0, max_it=50000,
     st = lib().orc_block_solve_pcg(nx, ny, nz, float(h), _p(cons, _u8), _p(E_elem), float(nu), _p(b), _p(x),
                                    max_it, tol, C.byref(it), C.byref(rr))
     return x, dict(status=st, iterations=it.value, rel_res=rr.value)
+
+
+def block_newmark(nx, ny, nz, constrained, E_elem, nu, rho, ray_alpha, ray_beta, nm_alpha, nm_delta, dt, n_steps,
+                  acc_amp, acc_period, acc_dir, n_dofs, f_static=None, solver=0, tol=1e-10, tip_dof=-1, h=1.0):
+    """Newmark integration of one realization (NewmarkDynamicAnalyzer.cs:53-315); returns
+    (tip history [n_steps], final displacement [n_dofs], info)."""
+    cons = np.ascontiguousarray(constrained, dtype=np.uint8)
+    E_elem = _f64(E_elem)
+    tip = np.zeros(n_steps)
+    u = np.zeros(n_dofs)
+    its = C.c_int(0)
+    fs = _p(_f64(f_static)) if f_static is not None else None
+    st = lib().orc_block_newmark(nx, ny, nz, float(h), _p(cons, _u8), _p(E_elem), float(nu), float(rho),
+                                 float(ray_alpha), float(ray_beta), float(nm_alpha), float(nm_delta), float(dt),
+                                 int(n_steps), float(acc_amp), float(acc_period), int(acc_dir), fs, int(solver),
+                                 float(tol), int(tip_dof), _p(tip), _p(u), C.byref(its))
+    return tip, u, dict(status=st, iterations=its.value)
 
 
 def num_threads():

@@ -748,4 +748,120 @@ int orc_block_solve_pcg(int nx, int ny, int nz, double h, const uint8_t* cons, c
   return orc_pcg_csr_jacobi(N, rp.data(), ci.data(), v.data(), b, x, max_it, tol, iterations, &mv, rel_res);
 }
 
+
+/* Newmark implicit integration of a structured block, one realization.
+ * NewmarkDynamicAnalyzer.cs:53-77 (coefficients a0..a7), :189-230 (RHS:
+ * uu = a0 u + a2 v + a3 a, uc = a1 u + a4 v + a5 a, rhs = F + M uu + C uc),
+ * :280-315 (loop over (int)(T/dt) steps, then a' = a0 (u' - u) - a2 v - a3 a,
+ * v += a6 a + a7 a'); ProblemStructural.cs:138-157 (K~ = 1 K + a0 M + a1 C);
+ * Hexa8.cs:403-451 (consistent mass, C_e = alpha_R M_e + beta_R K_e);
+ * Hexa8.cs:512-530 + Model.cs:266-278 (inertial load: M_e times the ground
+ * acceleration in DOF `acc_dir` at every element node, added to the free rows);
+ * MassAccelerationSinusoidalLoad.cs:17-20 (a_g(i) = A sin(2 pi / T_p dt i)).
+ * The effective matrix is factorised once (skyline LDL^T, SolverSkyline) when
+ * solver == 0, or each step is solved by Jacobi PCG from x0 = 0 to `tol` when
+ * solver == 1 (SolverPCG). tip_hist[i] = u[tip_dof] after step i. */
+int orc_block_newmark(int nx, int ny, int nz, double h, const uint8_t* cons, const double* Ee, double nu, double rho,
+                      double ray_alpha, double ray_beta, double nm_alpha, double nm_delta, double dt, int n_steps,
+                      double acc_amp, double acc_period, int acc_dir, const double* f_static, int solver, double tol,
+                      int tip_dof, double* tip_hist, double* u_final, int* total_its) {
+  if (nm_delta < 0.5) return -1;
+  if (nm_alpha < 0.25 * (0.5 + nm_delta) * (0.5 + nm_delta)) return -1;
+  const double a0 = 1 / (nm_alpha * dt * dt), a1 = nm_delta / (nm_alpha * dt), a2 = 1 / (nm_alpha * dt);
+  const double a3 = 1 / (2 * nm_alpha) - 1, a4 = nm_delta / nm_alpha - 1, a5 = dt * 0.5 * (nm_delta / nm_alpha - 2);
+  const double a6 = dt * (1 - nm_delta), a7 = nm_delta * dt;
+  const int nn = (nx + 1) * (ny + 1) * (nz + 1), ne = nx * ny * nz;
+  std::vector<double> xyz(3 * (size_t)nn);
+  std::vector<int> conn(8 * (size_t)ne), dof(3 * (size_t)nn);
+  orc_block_nodes(nx, ny, nz, h, xyz.data());
+  orc_block_conn(nx, ny, nz, conn.data());
+  const int N = orc_enumerate_dofs(nn, cons, dof.data());
+  std::vector<double> exyz(24 * (size_t)ne), K(300 * (size_t)ne), M(300 * (size_t)ne), C(300 * (size_t)ne),
+      Kt(300 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a)
+      for (int c = 0; c < 3; ++c) exyz[24 * (size_t)e + 3 * a + c] = xyz[3 * (size_t)conn[8 * e + a] + c];
+  int st = 0;
+  orc_h8_stiffness_batch(ne, exyz.data(), Ee, nu, K.data(), &st);
+  if (st) return st;
+  for (int e = 0; e < ne; ++e) {
+    st = orc_h8_consistent_mass(&exyz[24 * (size_t)e], rho, &M[300 * (size_t)e]);
+    if (st) return st;
+    for (int i = 0; i < 300; ++i) {
+      const size_t k = 300 * (size_t)e + i;
+      C[k] = ray_alpha * M[k] + ray_beta * K[k];
+      Kt[k] = 1.0 * K[k] + a0 * M[k] + a1 * C[k];
+    }
+  }
+  // assembled M, C (products) and K~ (solve)
+  std::vector<int64_t> rp(N + 1);
+  const int64_t nnz = orc_csr_pattern(nn, ne, conn.data(), dof.data(), N, rp.data(), nullptr);
+  std::vector<int> ci(nnz);
+  orc_csr_pattern(nn, ne, conn.data(), dof.data(), N, rp.data(), ci.data());
+  std::vector<double> Mv(nnz, 0.0), Cv(nnz, 0.0), Ktv(nnz, 0.0);
+  orc_csr_assemble(ne, conn.data(), dof.data(), M.data(), rp.data(), ci.data(), Mv.data());
+  orc_csr_assemble(ne, conn.data(), dof.data(), C.data(), rp.data(), ci.data(), Cv.data());
+  std::vector<int64_t> ri;
+  std::vector<double> sky;
+  if (solver == 0) {
+    ri.resize(N + 1);
+    const int64_t len = orc_skyline_rowindex(ne, conn.data(), dof.data(), N, ri.data());
+    sky.assign(len, 0.0);
+    orc_skyline_assemble(ne, conn.data(), dof.data(), Kt.data(), ri.data(), sky.data());
+    int zems = 0;
+    st = orc_skyline_factorize(N, ri.data(), sky.data(), 1e-8, &zems);
+    if (st) return st;
+  } else {
+    orc_csr_assemble(ne, conn.data(), dof.data(), Kt.data(), rp.data(), ci.data(), Ktv.data());
+  }
+  // inertial load pattern: sum_e M_e * (unit acceleration in acc_dir at all 8 nodes), free rows only
+  std::vector<double> fM(N, 0.0);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a)
+      for (int c = 0; c < 3; ++c) {
+        const int row = dof[3 * (size_t)conn[8 * e + a] + c];
+        if (row < 0) continue;
+        double s = 0;
+        for (int b = 0; b < 8; ++b) {
+          const int i = 3 * a + c, j = 3 * b + acc_dir;
+          const int r0 = i < j ? i : j, c0 = i < j ? j : i;
+          s += M[300 * (size_t)e + r0 * (47 - r0) / 2 + c0];
+        }
+        fM[row] += s;
+      }
+  std::vector<double> u(N, 0.0), v(N, 0.0), acc(N, 0.0), uu(N), uc(N), um(N), ucm(N), rhs(N), x(N);
+  const double two_pi = 2.0 * 3.14159265358979323846;
+  int its_sum = 0;
+  for (int i = 0; i < n_steps; ++i) {
+    const double ag = acc_amp * std::sin(two_pi / acc_period * dt * i);
+    for (int k = 0; k < N; ++k) {
+      uu[k] = a0 * u[k] + a2 * v[k] + a3 * acc[k];
+      uc[k] = a1 * u[k] + a4 * v[k] + a5 * acc[k];
+    }
+    orc_csr_multiply(N, rp.data(), ci.data(), Mv.data(), uu.data(), um.data());
+    orc_csr_multiply(N, rp.data(), ci.data(), Cv.data(), uc.data(), ucm.data());
+    for (int k = 0; k < N; ++k) rhs[k] = (f_static ? f_static[k] : 0.0) + ag * fM[k] + um[k] + ucm[k];
+    if (solver == 0) {
+      orc_skyline_solve(N, ri.data(), sky.data(), rhs.data(), x.data());
+    } else {
+      int it = 0, mv = 0;
+      double rr = 0;
+      std::fill(x.begin(), x.end(), 0.0);
+      st = orc_pcg_csr_jacobi(N, rp.data(), ci.data(), Ktv.data(), rhs.data(), x.data(), 100000, tol, &it, &mv, &rr);
+      if (st) return st;
+      its_sum += it;
+    }
+    for (int k = 0; k < N; ++k) {
+      const double an = a0 * (x[k] - u[k]) - a2 * v[k] - a3 * acc[k];
+      v[k] += a6 * acc[k] + a7 * an;
+      acc[k] = an;
+      u[k] = x[k];
+    }
+    if (tip_hist) tip_hist[i] = (tip_dof >= 0 && tip_dof < N) ? u[tip_dof] : 0.0;
+  }
+  if (u_final) std::copy(u.begin(), u.end(), u_final);
+  if (total_its) *total_its = its_sum;
+  return 0;
+}
+
 }  // extern "C"

@@ -81,6 +81,11 @@ int orc_block_solve_pcg(int nx, int ny, int nz, double h, const uint8_t* constra
                         const double* E_elem, double nu, const double* b_dof,
                         double* x_dof, int max_it, double tol, int* iterations, double* rel_res);
 
+int orc_block_newmark(int nx, int ny, int nz, double h, const uint8_t* constrained3, const double* E_elem, double nu,
+                      double rho, double ray_alpha, double ray_beta, double nm_alpha, double nm_delta, double dt,
+                      int n_steps, double acc_amp, double acc_period, int acc_dir, const double* f_static, int solver,
+                      double tol, int tip_dof, double* tip_hist, double* u_final, int* total_its);
+
 int orc_num_threads(void);
 
 #ifdef __cplusplus
