@@ -61,6 +61,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--reliable-delta", type=float, default=None, help="MSG_SET_OPTION reliable_delta")
     p.add_argument("--chunk", type=int, default=None, help="MSG_SET_OPTION chunk")
+    p.add_argument("--no-newmark", action="store_true", help="skip the batched Newmark measurement")
+    p.add_argument("--newmark-R", type=int, default=256)
+    p.add_argument("--newmark-n", type=int, default=24)
+    p.add_argument("--newmark-steps", type=int, default=200)
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
@@ -154,6 +158,39 @@ def cpu_baseline(args, model, kl, xi_host):
     return {"value": args.cpu_sample / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
             "sample": f"{args.cpu_sample} realizations of the {n}^3 block, FP64 CSR Jacobi-PCG to tol {args.tol:g} "
                       f"(mean {np.mean(its):.0f} iterations), {dt:.1f} s"}
+
+
+def newmark_leg(args, ctx):
+    """Batched Newmark dynamics (R realizations x n^3 Hexa8, 200 steps of dt 0.01,
+    average acceleration beta 0.25 / gamma 0.5, Rayleigh 0.01 M + 0.001 K,
+    ground acceleration 0.1 sin(2 pi t) in x, rho 1), timed end to end through
+    MSG_NEWMARK_BATCH after one warm-up call."""
+    import msolve_b200 as M
+    n, R, S = args.newmark_n, args.newmark_R, args.newmark_steps
+    model = M.clamped_block_model(n)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, args.terms, 12)
+    dt = 0.01
+    load = M.MassAccelerationSinusoidalLoad(1.0, dt, dt * S, 0.1, dof=0)
+    corner = int(np.argmax(model.xyz.sum(1)))
+    nm = M.NewmarkDynamicAnalyzer(ctx, model, kl, 0.25, 0.5, dt, dt * S, load, expansion_order=args.terms,
+                                  simulations=R, density=1.0, rayleigh_alpha=0.01, rayleigh_beta=0.001,
+                                  tolerance=1e-8, tip_dof=int(model.dof[corner, 0]), seed=7)
+    nm.Initialize()
+    import torch
+    nm.Solve(keep_solutions=False)  # warm-up (graph capture, workspace)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    hist = nm.Solve(keep_solutions=False)
+    b.record()
+    b.synchronize()
+    sec = a.elapsed_time(b) / 1e3
+    return {"workload": f"batched Newmark, {R} realizations x {n}^3 Hexa8, {nm.steps} steps (dt 0.01, beta 0.25, "
+                        f"gamma 0.5, Rayleigh 0.01 M + 0.001 K, ground acceleration 0.1 sin(2 pi t) in x), "
+                        f"FP64 true residual < 1e-8 per step, warm start",
+            "seconds": sec, "realization_steps_per_s": R * nm.steps / sec,
+            "mean_iterations_per_step": float(np.mean(nm.Iterations)) / nm.steps,
+            "tip_ux_final_mean": float(np.mean(hist[:, -1]))}
 
 
 def run_reference(args):
@@ -351,6 +388,7 @@ def main():
         if not args.no_cpu and ws == 1:
             cpu = cpu_baseline(args, model, kl, xi_all[0].numpy())
         its_all = np.concatenate(iters)
+        newmark = None if args.no_newmark else newmark_leg(args, ctx)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -384,6 +422,7 @@ def main():
                                     "recursive residual as the reference"},
             "mixed_over_fp64": value / ws / fp64_rate,
             "tip_uz": {"mean": tip_mean, "variance": tip_var, "realizations": int(cnt)},
+            "newmark": newmark,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
