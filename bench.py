@@ -255,8 +255,11 @@ def main():
     tip = M.tip_dof(model)
     dev = torch.device("cuda", local)
     steps_total = args.warmup + args.steps
-    g = torch.Generator(device="cpu").manual_seed(1000 + rank)
-    xi_all = torch.randn(steps_total + 1, R, K_terms, generator=g, dtype=torch.float64)
+    # every step draws a global table of ws * R realizations; this rank solves its shard
+    from msolve_b200 import distributed as D
+    lo, hi = D.shard(ws * R, ws, rank)
+    xi_all = torch.from_numpy(np.stack([D.global_xi(1000 + s, ws * R, K_terms)[lo:hi]
+                                        for s in range(steps_total + 1)]))
     xi_dev = xi_all.to(dev)
     b_dev = torch.from_numpy(model.subdomains[0].RHS).to(dev)
     X_dev = torch.empty(R, Nd, dtype=torch.float64, device=dev)
@@ -317,14 +320,9 @@ def main():
     ms_max = float(ms_t.item())
     value = ws * R * args.steps / (ms_max / 1e3)
 
-    # Monte Carlo statistics of the last step: one all-reduce of (sum u, sum u^2, count)
-    stats_t = torch.tensor([tip_h[:R].sum(), (tip_h[:R] ** 2).sum(), R], dtype=torch.float64, device=dev)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.all_reduce(stats_t)
-    su, su2, cnt = stats_t.tolist()
-    tip_mean = su / cnt
-    tip_var = (su2 - cnt * tip_mean ** 2) / max(cnt - 1, 1)
+    # Monte Carlo statistics of the last step: one all-reduce of (count, sum u, sum u^2)
+    mom = D.combine_moments(tip_h[:R], device=dev)
+    tip_mean, tip_var, cnt = mom["mean"], mom["variance"], mom["count"]
 
     # roofline of the dominant kernel, the fused direction + matrix-free FP32 operator
     # (k_op_modal; live per-launch samples from the timed region)
