@@ -228,11 +228,51 @@ int MSG_NEWMARK_BATCH(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const d
                       const double* f_static, int max_it, double tol, int tip_dof, double* tip_hist, double* U,
                       int* iterations);
 
+/* ------------------------------------------------------------------ serving */
+/* Continuous-batching service on a context. No counterpart in the reference
+ * (its realization loop is sequential, MonteCarloAnalyzerWithStochasticMaterial.cs:258-276).
+ * A model is a structured mesh with its material (nu), KL table and load b
+ * [n_dofs]; a request is one realization of a model (its xi [kl->n_terms]).
+ * Requests wait in a queue, enter a free slot of their model's batch at the
+ * next chunk boundary (max_batch slots per model, rounded up to 32; the slot
+ * memory of each model is allocated once, against the context's memory
+ * budget, when the model is added) and leave as soon as their own FP64 true
+ * residual is below the model's tol. A request's arithmetic does not depend on
+ * the other requests in flight: results are bitwise identical alone or mixed.
+ * One worker thread per context runs the batches; every entry point may be
+ * called from any thread. */
+#define MSG_PENDING 1 /* MSG_SERVE_POLL: not finished yet (not an error) */
+typedef uint64_t MSG_REQ;
+int MSG_SERVE_START(MSG_CTX ctx, int max_batch);
+/* Register a model; *model_id identifies it in MSG_SERVE_SUBMIT. b is copied. */
+int MSG_SERVE_ADD_MODEL(MSG_CTX ctx, MSG_MESH mesh, double nu, const MSG_KL* kl, const double* b, double tol,
+                        int max_it, int* model_id);
+/* Queue one realization (xi is copied); *id names the request. */
+int MSG_SERVE_SUBMIT(MSG_CTX ctx, int model_id, const double* xi, MSG_REQ* id);
+/* Wait up to timeout_ms (0: do not wait, < 0: until done) for request id.
+ * Finished: copies X [n_dofs] (may be NULL), iterations (operator products),
+ * rel_res (final FP64 ||b - K x|| / ||b||) and latency_ms (submit to finish),
+ * forgets the request and returns MSG_OK, MSG_ERR_NOT_CONVERGED,
+ * MSG_ERR_BREAKDOWN or MSG_ERR_CANCELLED. Not finished: MSG_PENDING. */
+int MSG_SERVE_POLL(MSG_CTX ctx, MSG_REQ id, int timeout_ms, double* X, int* iterations, double* rel_res,
+                   double* latency_ms);
+/* Cancel a request: a queued one never runs, a running one leaves its slot at
+ * the next chunk boundary; its poll returns MSG_ERR_CANCELLED. */
+int MSG_SERVE_CANCEL(MSG_CTX ctx, MSG_REQ id);
+/* Requests waiting in the queues and occupying slots. */
+int MSG_SERVE_STATS(MSG_CTX ctx, int64_t* queued, int64_t* running);
+/* Stop the worker and free every model (pending requests are dropped). */
+int MSG_SERVE_STOP(MSG_CTX ctx);
+
 /* Tunables of the mixed solver on this context: "reliable_delta" (the FP32
  * recursive residual may fall by this factor before it is replaced by the FP64
  * true residual, default 0.1), "chunk" (FP32 iterations per CUDA-graph launch,
  * even, default 16), "modal_operator" (1: the FP32 operator works on the
- * element's Walsh modes, default; 0: dense value-class stencil). */
+ * element's Walsh modes, default; 0: dense value-class stencil),
+ * "fixed_updates" (1: the FP64 true-residual step runs after every chunk for
+ * every realization, so each realization's arithmetic no longer depends on the
+ * rest of the batch: bitwise identical alone or batched; default 0: the step
+ * runs when some realization asks for it). */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 
 /* Kernel launch counter of this context (kernels launched since creation),

@@ -23,6 +23,7 @@ MSG_ERR_NOT_CONVERGED = -2001
 MSG_ERR_BREAKDOWN = -2002
 MSG_ERR_TIMEOUT = -2003
 MSG_ERR_CANCELLED = -2004
+MSG_PENDING = 1
 MSG_ERR_INVALID_ARGUMENT = -2005
 MSG_ERR_CUDA = -2006
 MSG_ERR_NOT_STRUCTURED = -2007
@@ -92,6 +93,13 @@ SIGNATURES = {
                                             C.c_int, C.c_double, C.c_int, _vp, _d, _i, _d]),
     "MSG_NEWMARK_BATCH": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _d, C.POINTER(MSG_NEWMARK), _d,
                                     C.c_int, C.c_double, C.c_int, _d, _d, _i]),
+    "MSG_SERVE_START": (C.c_int, [_vp, C.c_int]),
+    "MSG_SERVE_ADD_MODEL": (C.c_int, [_vp, _vp, C.c_double, C.POINTER(MSG_KL), _d, C.c_double, C.c_int, _i]),
+    "MSG_SERVE_SUBMIT": (C.c_int, [_vp, C.c_int, _d, C.POINTER(C.c_uint64)]),
+    "MSG_SERVE_POLL": (C.c_int, [_vp, C.c_uint64, C.c_int, _d, _i, _d, _d]),
+    "MSG_SERVE_CANCEL": (C.c_int, [_vp, C.c_uint64]),
+    "MSG_SERVE_STATS": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "MSG_SERVE_STOP": (C.c_int, [_vp]),
     "MSG_SET_OPTION": (C.c_int, [_vp, C.c_char_p, C.c_double]),
     "MSG_STATS": (C.c_int, [_vp, _i64, _d]),
     "MSG_STATS_RESET": (C.c_int, [_vp]),

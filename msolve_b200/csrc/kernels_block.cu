@@ -1070,7 +1070,8 @@ struct Scal {
   int* act;            // [Rp] iterating
   int* done;           // [Rp] converged (true residual)
   int* its;            // [Rp] operator applications
-  int* breakdown;      // [Rp]
+  int* breakdown;      // [Rp] 1: PCG breakdown, 2: iteration limit of the slot reached
+  int* fresh;          // [Rp] 1: the slot starts a new system at the next true-residual step
   int* n_active;       // [1] active count after the last k_beta / k_resid_scalars
   int* n_update;       // [1] active realizations requesting a reliable update
   int* err;            // [1] sticky: a bounded device wait expired
@@ -1159,7 +1160,7 @@ __global__ void __launch_bounds__(1024) k_beta(int Rp, int n_blk, const double* 
 // the search-direction coefficient beta = gamma_new / gamma_prev (first call:
 // beta = 0, p starts from z).
 __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, const double* __restrict__ partial,
-                                                        Scal s, double tol, int first, int gamma_ref) {
+                                                        Scal s, double tol, int first, int gamma_ref, int max_it) {
   double v[2];
   reduce_rows<2>(partial, n_tiles, Rp, v);
   const int r = blockIdx.x * 32 + threadIdx.x;
@@ -1168,11 +1169,14 @@ __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, con
     const double rr = v[0], g = v[1];
     const double bn = s.bnorm[r];
     const double rel = bn > 0 ? sqrt(rr) / bn : 0.0;
+    const int fr = first || s.fresh[r];
+    s.fresh[r] = 0;
     s.res[r] = rel;
     if (!s.done[r] && (bn <= 1e-25 || rel < tol)) s.done[r] = 1;
+    if (!s.done[r] && !s.breakdown[r] && s.its[r] >= max_it) s.breakdown[r] = 2;
     const int a = (s.done[r] || s.breakdown[r]) ? 0 : 1;
     s.act[r] = a;
-    s.beta[r] = (a && !first && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
+    s.beta[r] = (a && !fr && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
     s.gamma[r] = g;
     s.rho_ref[r] = gamma_ref ? g : rr;
     s.alpha[r] = 0.f;  // the pending alpha p term was folded into x (and no r update is pending)
@@ -1338,6 +1342,63 @@ __global__ void k_column(size_t n, int Rp, int r, const double* __restrict__ a, 
     b[i] = a[i * Rp + r];
 }
 
+// Serving slots: zero the batch-vector columns of the listed realization
+// slots and reset their scalars (fresh: the next true-residual step starts a
+// new system there).
+__global__ void k_slot_reset(int n_slots, const int* __restrict__ slots, size_t nrows, int Rp, double* __restrict__ x,
+                             float* __restrict__ v0, float* __restrict__ v1, float* __restrict__ v2,
+                             float* __restrict__ v3, float* __restrict__ v4, float* __restrict__ v5,
+                             float* __restrict__ v6, Scal s) {
+  const size_t total = (size_t)n_slots * nrows;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = i % nrows;
+    const size_t o = row * Rp + slots[i / nrows];
+    x[o] = 0.0;
+    v0[o] = v1[o] = v2[o] = v3[o] = v4[o] = v5[o] = v6[o] = 0.f;
+  }
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t < (size_t)n_slots) {
+    const int r = slots[t];
+    s.alpha[r] = s.beta[r] = 0.f;
+    s.gamma[r] = s.gamma_prev[r] = s.rho_ref[r] = s.res[r] = 0.0;
+    s.act[r] = s.done[r] = s.its[r] = s.breakdown[r] = 0;
+    s.fresh[r] = 1;
+  }
+}
+
+// Jacobi diagonal (as k_dinv) for the listed slots only
+__global__ void k_dinv_slots(Lattice L, double kdiag, double mdiag, const float* __restrict__ E,
+                             const int* __restrict__ interior, int n_slots, const int* __restrict__ slots,
+                             float* __restrict__ dinv) {
+  const size_t node = (size_t)interior[blockIdx.x];
+  const size_t sxy = (size_t)L.NXp, sxz = (size_t)L.NXp * L.NYp;
+  for (int i = threadIdx.x; i < n_slots; i += blockDim.x) {
+    const int rr = slots[i];
+    double s = 0;
+    int n_real = 0;
+    for (int ez = -1; ez <= 0; ++ez)
+      for (int ey = -1; ey <= 0; ++ey)
+        for (int ex = -1; ex <= 0; ++ex) {
+          const float e = E[(node + ex + ey * sxy + ez * sxz) * L.Rp + rr];
+          s += (double)e;
+          n_real += e > 0.f;
+        }
+    dinv[node * L.Rp + rr] = (float)(1.0 / (kdiag * s + mdiag * n_real));
+  }
+}
+
+// out[dof] = x[row(dof)*Rp + slot]
+__global__ void k_gather_column(int n_dofs, int Rp, int slot, const int* __restrict__ rows,
+                                const double* __restrict__ x, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_dofs) out[i] = x[(size_t)rows[i] * Rp + slot];
+}
+
+__global__ void k_fill_int(int* __restrict__ a, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
 __global__ void k_lattice_rhs(int n_dofs, const int* __restrict__ rows, const double* __restrict__ b_dof,
                               double* __restrict__ b_lat) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1460,9 +1521,23 @@ struct WSlot {
   template <class T> T* as() const { return static_cast<T*>(ptr); }
 };
 
+// Where a batch runs: stream, timing events, pinned flag words and the cached
+// inner-loop graph (the context's own, or a serving lane's).
+struct BlockExec {
+  cudaStream_t st = nullptr;
+  cudaEvent_t* ev = nullptr;      // 12 events
+  int* h_flags = nullptr;         // pinned, >= 64 bytes
+  cudaGraphExec_t* graph = nullptr;
+  size_t* graph_key = nullptr;
+  bool ctx_stats = true;          // accumulate the context's phase timings and launch samples
+};
+
 // Everything one batch of solves on a structured lattice shares: sizes,
 // operator coefficients (A = cK E Khat + cM Mhat), workspace, tensor maps.
 struct BlockSys {
+  BlockExec X;
+  DevMem* own = nullptr;  // 32 buffers owned by a serving lane; nullptr: the context's workspace slots
+  bool fixed = false;     // true-residual step after every graph chunk (batch-invariant trajectories)
   Lattice L;
   int R = 0, Rp = 0;
   size_t npad = 0, nvec = 0;
@@ -1478,12 +1553,34 @@ struct BlockSys {
   WSlot x, r32, p, q, d, dinv, blat, E64, E32, part_op, part_up, scal, pB, rB, qB;
   size_t scal_bytes = 0;
   Scal s;
+  int slot_alloc(Context* ctx, int slot, size_t bytes, void** out) {
+    if (!own) return workspace(ctx, slot, bytes, out);
+    if (own[slot].bytes < bytes) {
+      own[slot].release();
+      MSG_TRY(own[slot].alloc(ctx, bytes));
+    }
+    *out = own[slot].ptr;
+    return MSG_OK;
+  }
   CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
 };
 
 // Coefficients and workspace of a batch: A = cK E Khat(nu) + cM Mhat(rho).
-int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double cM, int R, int Rp, BlockSys* B) {
+int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double cM, int R, int Rp, BlockSys* B,
+                DevMem* own = nullptr, const BlockExec* exec = nullptr) {
   if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mesh is not a structured cube lattice");
+  B->own = own;
+  if (exec) {
+    B->X = *exec;
+  } else {
+    MSG_TRY(context_resources(ctx));
+    B->X.st = ctx->stream;
+    B->X.ev = ctx->ev;
+    B->X.h_flags = ctx->h_flags;
+    B->X.graph = &ctx->batch_graph;
+    B->X.graph_key = &ctx->batch_graph_key;
+    B->X.ctx_stats = true;
+  }
   Lattice& L = B->L;
   L.NX = m->nx + 1; L.NY = m->ny + 1; L.NZ = m->nz + 1;
   L.NXp = m->NXp; L.NYp = m->NYp; L.NZp = m->NZp;
@@ -1504,7 +1601,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   B->modal = ctx->modal != 0;
   if (B->mass && !B->modal)
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "a mass term needs the modal operator (modal_operator = 1)");
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = B->X.st;
 
   double K576[576];
   MSG_TRY(unit_cube_khat(ctx, m->h, nu, K576));
@@ -1553,24 +1650,24 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
 
   // workspace (context slots, reused by the next batch)
   const size_t nvec = B->nvec, npad = B->npad;
-  MSG_TRY(workspace(ctx, 0, sizeof(double) * nvec, &B->x.ptr));
-  MSG_TRY(workspace(ctx, 1, sizeof(float) * nvec, &B->r32.ptr));
-  MSG_TRY(workspace(ctx, 2, sizeof(float) * nvec, &B->p.ptr));
-  MSG_TRY(workspace(ctx, 3, sizeof(float) * nvec, &B->q.ptr));
-  MSG_TRY(workspace(ctx, 4, sizeof(float) * nvec, &B->d.ptr));
-  MSG_TRY(workspace(ctx, 5, sizeof(float) * npad * Rp, &B->dinv.ptr));
-  MSG_TRY(workspace(ctx, 6, sizeof(double) * npad * Rp, &B->E64.ptr));
-  MSG_TRY(workspace(ctx, 7, sizeof(float) * npad * Rp, &B->E32.ptr));
-  MSG_TRY(workspace(ctx, 8, sizeof(double) * npad * 3, &B->blat.ptr));
-  MSG_TRY(workspace(ctx, 9, sizeof(double) * (size_t)std::max(B->n_tiles * 2, B->n_tiles_m * kMParts) * Rp,
+  MSG_TRY(B->slot_alloc(ctx, 0, sizeof(double) * nvec, &B->x.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 1, sizeof(float) * nvec, &B->r32.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 2, sizeof(float) * nvec, &B->p.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 3, sizeof(float) * nvec, &B->q.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 4, sizeof(float) * nvec, &B->d.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 5, sizeof(float) * npad * Rp, &B->dinv.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 6, sizeof(double) * npad * Rp, &B->E64.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 7, sizeof(float) * npad * Rp, &B->E32.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 8, sizeof(double) * npad * 3, &B->blat.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 9, sizeof(double) * (size_t)std::max(B->n_tiles * 2, B->n_tiles_m * kMParts) * Rp,
                     &B->part_op.ptr));
-  MSG_TRY(workspace(ctx, 10, sizeof(double) * (size_t)std::max(B->n_upd, B->n_bsq) * Rp * 2, &B->part_up.ptr));
-  B->scal_bytes = (sizeof(float) * 2 + sizeof(double) * 6 + sizeof(int) * 4) * (size_t)Rp + 64;
-  MSG_TRY(workspace(ctx, 11, B->scal_bytes, &B->scal.ptr));
+  MSG_TRY(B->slot_alloc(ctx, 10, sizeof(double) * (size_t)std::max(B->n_upd, B->n_bsq) * Rp * 2, &B->part_up.ptr));
+  B->scal_bytes = (sizeof(float) * 2 + sizeof(double) * 6 + sizeof(int) * 5) * (size_t)Rp + 64;
+  MSG_TRY(B->slot_alloc(ctx, 11, B->scal_bytes, &B->scal.ptr));
   if (B->modal) {  // second buffers of p, r and q for the single-reduction loop
-    MSG_TRY(workspace(ctx, 18, sizeof(float) * nvec, &B->pB.ptr));
-    MSG_TRY(workspace(ctx, 19, sizeof(float) * nvec, &B->rB.ptr));
-    MSG_TRY(workspace(ctx, 20, sizeof(float) * nvec, &B->qB.ptr));
+    MSG_TRY(B->slot_alloc(ctx, 18, sizeof(float) * nvec, &B->pB.ptr));
+    MSG_TRY(B->slot_alloc(ctx, 19, sizeof(float) * nvec, &B->rB.ptr));
+    MSG_TRY(B->slot_alloc(ctx, 20, sizeof(float) * nvec, &B->qB.ptr));
   }
   Scal& sc = B->s;
   {
@@ -1587,6 +1684,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
     sc.done = (int*)base; base += sizeof(int) * Rp;
     sc.its = (int*)base; base += sizeof(int) * Rp;
     sc.breakdown = (int*)base; base += sizeof(int) * Rp;
+    sc.fresh = (int*)base; base += sizeof(int) * Rp;
     sc.n_active = (int*)base; base += 16;
     sc.n_update = (int*)base; base += 16;
     sc.err = (int*)base;  // outside the 32 bytes the iterations clear
@@ -1676,55 +1774,48 @@ int block_field(Context* ctx, Mesh* m, BlockSys* B, const KLDevice* kl, const do
   return MSG_OK;
 }
 
-// Solve A x = b for every realization of the batch to the FP64 true relative
-// residual tol: b is one vector (blat layout) or one per realization; x (slot 0)
-// starts from zero, or from its content when warm. Per-realization results stay
-// in B->s (its, res, done, breakdown); returns the batch status.
-int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool warm, int max_it, double tol,
-                bool record_phases, int chunk_cap = 0) {
+// Launch geometry and tolerances shared by the inner-loop graph and the
+// true-residual step of a batch.
+struct LoopCfg {
+  dim3 op_grid, op_block;
+  size_t upd_smem = 0;
+  int sblocks = 0, n_xu = 0, n_dir = 0, chunk = 2;
+  double delta2 = 0.0, tol2 = 0.0;
+};
+
+LoopCfg loop_cfg(Context* ctx, const BlockSys* B, double tol, int chunk_cap) {
+  LoopCfg c;
+  const int Rp = B->Rp;
+  c.op_grid = dim3(B->n_tiles, Rp / 32);
+  c.op_block = dim3(32, kWarps);
+  const int Q = Rp / 4;
+  const int G = Q >= 256 ? 1 : 256 / Q;
+  c.upd_smem = G > 1 ? sizeof(double) * (size_t)G * Q * 8 : 0;
+  c.sblocks = Rp / 32;  // scalar kernels: 32 realizations x 32 row groups per CTA
+  c.n_xu = ctx->sm_count * 8;
+  c.n_dir = std::min(B->L.n_int, ctx->sm_count * 8);
+  c.chunk = std::max(2, (chunk_cap > 0 ? std::min(ctx->chunk, chunk_cap) : ctx->chunk) & ~1);
+  c.delta2 = ctx->reliable_delta * ctx->reliable_delta;
+  // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
+  // sqrt(gamma / gamma0) is at tol/4 (single-reduction loop, dinv-weighted norm)
+  c.tol2 = (B->modal ? 0.0625 : 0.25) * tol * tol;
+  return c;
+}
+
+// The inner-loop graph of `chunk` FP32 iterations, kept in the exec slot and
+// captured again only when one of its kernel arguments changes (FNV-1a over
+// the argument bytes).
+int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* out) {
   const Lattice& L = B->L;
   const int Rp = B->Rp;
   const bool modal = B->modal;
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = B->X.st;
   Scal& s = B->s;
+  cudaEvent_t* ev = B->X.ev;
   const int* interior = B->interior;
   const uint8_t* mask = B->mask;
-  WSlot &x = B->x, &r32 = B->r32, &p = B->p, &q = B->q, &d = B->d, &dinv = B->dinv, &part_op = B->part_op,
+  WSlot &r32 = B->r32, &p = B->p, &q = B->q, &d = B->d, &dinv = B->dinv, &part_op = B->part_op,
         &part_up = B->part_up, &pB = B->pB, &rB = B->rB, &qB = B->qB;
-  const size_t nvec = B->nvec;
-  MSG_CUDA(ctx, cudaMemsetAsync(B->scal.ptr, 0, B->scal_bytes, st));
-  if (!warm) MSG_CUDA(ctx, cudaMemsetAsync(x.ptr, 0, sizeof(double) * nvec, st));
-  // directions, operator outputs and the correction start from zero
-  const WSlot* z32[] = {&p, &q, &d, &pB, &qB};
-  for (const WSlot* w : z32)
-    if (w->ptr) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(float) * nvec, st));
-  // ||b|| and (dinv b).b per realization
-  k_bsq<<<dim3(B->n_bsq, Rp / 32), 256, 0, st>>>(L.n_int, Rp, interior, b, b_per_r ? 1 : 0, dinv.as<float>(),
-                                                part_up.as<double>());
-  k_bnorm<<<Rp / 32, 1024, 0, st>>>(B->R, Rp, B->n_bsq, part_up.as<double>(), s);
-  count_launch(ctx, 2);
-
-  const dim3 op_grid(B->n_tiles, Rp / 32), op_block(32, kWarps);
-  const int Q = Rp / 4;
-  const int G = Q >= 256 ? 1 : 256 / Q;
-  const size_t upd_smem = G > 1 ? sizeof(double) * (size_t)G * Q * 8 : 0;
-  const int sblocks = Rp / 32;  // scalar kernels: 32 realizations x 32 row groups per CTA
-  const int n_xu = ctx->sm_count * 8;
-  const int n_dir = std::min(L.n_int, ctx->sm_count * 8);
-  const int n_upd = B->n_upd, n_tiles = B->n_tiles;
-  const double delta2 = ctx->reliable_delta * ctx->reliable_delta;
-  // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
-  // sqrt(gamma / gamma0) is at tol/4 (single-reduction loop, dinv-weighted norm)
-  const double tol2 = (modal ? 0.0625 : 0.25) * tol * tol;
-
-  // context events: 0-3 host-side phases, 4-7 captured around the first operator / update launch
-  MSG_TRY(context_resources(ctx));
-  cudaEvent_t* ev = ctx->ev;
-  float t_resid = 0.f, t_inner = 0.f;
-
-  const int chunk = std::max(2, (chunk_cap > 0 ? std::min(ctx->chunk, chunk_cap) : ctx->chunk) & ~1);
-  // The inner-loop graph is kept in the context and captured again only when
-  // one of its kernel arguments changes (FNV-1a over the argument bytes).
   size_t key = 1469598103934665603ull;
   auto mix = [&key](const void* data, size_t n) {
     const unsigned char* bb = static_cast<const unsigned char*>(data);
@@ -1732,7 +1823,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
   };
   {
     const void* ptrs[] = {interior, mask, r32.ptr, p.ptr, q.ptr, d.ptr, dinv.ptr, part_op.ptr, part_up.ptr,
-                          B->scal.ptr, pB.ptr, rB.ptr, qB.ptr};
+                          B->scal.ptr, pB.ptr, rB.ptr, qB.ptr, st};
     mix(ptrs, sizeof(ptrs));
     mix(&L, sizeof(L));
     mix(&B->KF, sizeof(B->KF));
@@ -1747,19 +1838,20 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
     }
     const int mm[6] = {modal ? 1 : 0, B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
     mix(mm, sizeof(mm));
-    const double dd[2] = {delta2, tol2};
+    const double dd[2] = {c.delta2, c.tol2};
     mix(dd, sizeof(dd));
-    const int ii[6] = {chunk, n_dir, n_upd, n_tiles, sblocks, (int)upd_smem};
+    const int ii[6] = {c.chunk, c.n_dir, B->n_upd, B->n_tiles, c.sblocks, (int)c.upd_smem};
     mix(ii, sizeof(ii));
   }
-  if (ctx->batch_graph && ctx->batch_graph_key != key) {
-    cudaGraphExecDestroy(ctx->batch_graph);
-    ctx->batch_graph = nullptr;
+  cudaGraphExec_t& gx = *B->X.graph;
+  if (gx && *B->X.graph_key != key) {
+    cudaGraphExecDestroy(gx);
+    gx = nullptr;
   }
-  if (!ctx->batch_graph) {
+  if (!gx) {
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    for (int it = 0; it < chunk; ++it) {
+    for (int it = 0; it < c.chunk; ++it) {
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
       if (modal) {
@@ -1776,73 +1868,117 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
         if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
         cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
         if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-        k_alpha_gamma<<<sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part_op.as<double>(), s, delta2, tol2);
+        k_alpha_gamma<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part_op.as<double>(), s, c.delta2, c.tol2);
         if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
       } else {
-        k_dir<<<n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
-                                     p.as<float>(), d.as<float>());
+        k_dir<<<c.n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
+                                       p.as<float>(), d.as<float>());
         if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-        k_op_tma<<<op_grid, kOpThreads, kOpSmem, st>>>(L, B->KF, B->tm_p, B->tm_e, mask, q.as<float>(),
-                                                       part_op.as<double>(), s.err);
+        k_op_tma<<<c.op_grid, kOpThreads, kOpSmem, st>>>(L, B->KF, B->tm_p, B->tm_e, mask, q.as<float>(),
+                                                         part_op.as<double>(), s.err);
         if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
-        k_alpha<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s);
+        k_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles, part_op.as<double>(), s);
         if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-        k_update<<<n_upd, 256, upd_smem, st>>>(L.n_int, Rp, interior, mask, s.alpha, q.as<float>(), r32.as<float>(),
-                                               dinv.as<float>(), part_up.as<double>());
+        k_update<<<B->n_upd, 256, c.upd_smem, st>>>(L.n_int, Rp, interior, mask, s.alpha, q.as<float>(),
+                                                   r32.as<float>(), dinv.as<float>(), part_up.as<double>());
         if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
         cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
-        k_beta<<<sblocks, 1024, 0, st>>>(Rp, n_upd, part_up.as<double>(), s, delta2, tol2);
+        k_beta<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_upd, part_up.as<double>(), s, c.delta2, c.tol2);
       }
     }
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (e != cudaSuccess) return cuda_error(ctx, e, "capture inner chunk");
-    e = cudaGraphInstantiate(&ctx->batch_graph, g, 0);
+    e = cudaGraphInstantiate(&gx, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
-      ctx->batch_graph = nullptr;
+      gx = nullptr;
       return cuda_error(ctx, e, "instantiate inner chunk");
     }
-    ctx->batch_graph_key = key;
+    *B->X.graph_key = key;
   }
-  cudaGraphExec_t gexec = ctx->batch_graph;
+  *out = gx;
+  return MSG_OK;
+}
 
-  int* h_flags = ctx->h_flags;  // [0] active, [4] update requests, [8] wait timeout (pinned, per context)
+// True-residual step (enqueued, not synchronised): x += d + alpha p, d = 0
+// (unless first), r = b - A x in FP64, convergence and search-direction scalars.
+int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, bool b_per_r, double tol, bool first,
+                 int max_it) {
+  const Lattice& L = B->L;
+  const int Rp = B->Rp;
+  cudaStream_t st = B->X.st;
+  Scal& s = B->s;
+  const uint8_t* mask = B->mask;
+  if (!first) {
+    k_xupdate<<<c.n_xu, 256, 0, st>>>(L.n_int, Rp, B->interior, s.alpha, B->p.as<float>(), B->x.as<double>(),
+                                      B->d.as<float>());
+    count_launch(ctx);
+  }
+  double* x = B->x.as<double>();
+  const double* E = B->E64.as<double>();
+  const float* dinv = B->dinv.as<float>();
+  float* r32 = B->r32.as<float>();
+  double* part = B->part_op.as<double>();
+  if (B->mass) {
+    if (b_per_r)
+      k_resid<true, true><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
+    else
+      k_resid<true, false><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
+  } else {
+    if (b_per_r)
+      k_resid<false, true><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
+    else
+      k_resid<false, false><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
+  }
+  MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
+  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles, part, s, tol, first ? 1 : 0, B->modal ? 1 : 0, max_it);
+  count_launch(ctx, 2);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+// ||b|| and (dinv b).b of every realization (b shared or per realization)
+int block_bnorm(Context* ctx, BlockSys* B, const double* b, bool b_per_r) {
+  cudaStream_t st = B->X.st;
+  k_bsq<<<dim3(B->n_bsq, B->Rp / 32), 256, 0, st>>>(B->L.n_int, B->Rp, B->interior, b, b_per_r ? 1 : 0,
+                                                   B->dinv.as<float>(), B->part_up.as<double>());
+  k_bnorm<<<B->Rp / 32, 1024, 0, st>>>(B->R, B->Rp, B->n_bsq, B->part_up.as<double>(), B->s);
+  count_launch(ctx, 2);
+  return MSG_OK;
+}
+
+// Solve A x = b for every realization of the batch to the FP64 true relative
+// residual tol: b is one vector (blat layout) or one per realization; x (slot 0)
+// starts from zero, or from its content when warm. Per-realization results stay
+// in B->s (its, res, done, breakdown); returns the batch status.
+int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool warm, int max_it, double tol,
+                bool record_phases, int chunk_cap = 0) {
+  cudaStream_t st = B->X.st;
+  Scal& s = B->s;
+  const size_t nvec = B->nvec;
+  MSG_CUDA(ctx, cudaMemsetAsync(B->scal.ptr, 0, B->scal_bytes, st));
+  if (!warm) MSG_CUDA(ctx, cudaMemsetAsync(B->x.ptr, 0, sizeof(double) * nvec, st));
+  // directions, operator outputs and the correction start from zero
+  const WSlot* z32[] = {&B->p, &B->q, &B->d, &B->pB, &B->qB};
+  for (const WSlot* w : z32)
+    if (w->ptr) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(float) * nvec, st));
+  MSG_TRY(block_bnorm(ctx, B, b, b_per_r));
+  const LoopCfg c = loop_cfg(ctx, B, tol, chunk_cap);
+  cudaEvent_t* ev = B->X.ev;
+  float t_resid = 0.f, t_inner = 0.f;
+  cudaGraphExec_t gexec = nullptr;
+  MSG_TRY(block_graph(ctx, B, c, &gexec));
+
+  int* h_flags = B->X.h_flags;  // [0] active, [4] update requests, [8] wait timeout (pinned)
   int status = MSG_OK;
   int total_inner = 0;
   int n_updates = 0;
   bool need_update = true, first = true;
   for (int guard = 0; guard < 1000000; ++guard) {
     if (need_update) {
-      // reliable update: x += d; d = 0; r = b - A x (FP64)
       cudaEventRecord(ev[0], st);
-      if (!first) {
-        k_xupdate<<<n_xu, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, p.as<float>(), x.as<double>(), d.as<float>());
-        count_launch(ctx);
-      }
-      if (B->mass) {
-        if (b_per_r)
-          k_resid<true, true><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b, B->E64.as<double>(),
-                                                            mask, dinv.as<float>(), r32.as<float>(),
-                                                            part_op.as<double>());
-        else
-          k_resid<true, false><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b, B->E64.as<double>(),
-                                                             mask, dinv.as<float>(), r32.as<float>(),
-                                                             part_op.as<double>());
-      } else {
-        if (b_per_r)
-          k_resid<false, true><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b,
-                                                             B->E64.as<double>(), mask, dinv.as<float>(),
-                                                             r32.as<float>(), part_op.as<double>());
-        else
-          k_resid<false, false><<<op_grid, op_block, 0, st>>>(L, B->KD, B->MD, x.as<double>(), b,
-                                                              B->E64.as<double>(), mask, dinv.as<float>(),
-                                                              r32.as<float>(), part_op.as<double>());
-      }
-      MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
-      k_resid_scalars<<<sblocks, 1024, 0, st>>>(Rp, n_tiles, part_op.as<double>(), s, tol, first ? 1 : 0,
-                                                modal ? 1 : 0);
+      MSG_TRY(block_update(ctx, B, c, b, b_per_r, tol, first, 0x7fffffff));
       cudaEventRecord(ev[1], st);
-      count_launch(ctx, 2);
       MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
       MSG_CUDA(ctx, cudaStreamSynchronize(st));
       float ms = 0.f;
@@ -1859,15 +1995,15 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
-    count_launch(ctx, (modal ? 2 : 5) * chunk);
-    total_inner += chunk;
+    count_launch(ctx, (B->modal ? 2 : 5) * c.chunk);
+    total_inner += c.chunk;
     cudaEventRecord(ev[3], st);
     MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     float ms = 0.f, op_ms = 0.f, up_ms = 0.f;
     cudaEventElapsedTime(&ms, ev[2], ev[3]);
     t_inner += ms;
-    if (cudaEventElapsedTime(&op_ms, ev[4], ev[5]) == cudaSuccess &&
+    if (B->X.ctx_stats && cudaEventElapsedTime(&op_ms, ev[4], ev[5]) == cudaSuccess &&
         cudaEventElapsedTime(&up_ms, ev[6], ev[7]) == cudaSuccess) {
       ctx->op_ms_sum += op_ms;
       ctx->upd_ms_sum += up_ms;
@@ -1879,16 +2015,18 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
       status = set_error(ctx, MSG_ERR_TIMEOUT, "a bounded wait of the staged operator expired");
       break;
     }
-    need_update = (h_flags[4] > 0) || (h_flags[0] == 0);
+    need_update = B->fixed || (h_flags[4] > 0) || (h_flags[0] == 0);
   }
-  if (record_phases) {
-    ctx->t_phase[1] = t_inner;
-    ctx->t_phase[3] = t_resid;
-    ctx->t_phase[2] = (double)n_updates;
-  } else {
-    ctx->t_phase[1] += t_inner;
-    ctx->t_phase[3] += t_resid;
-    ctx->t_phase[2] += (double)n_updates;
+  if (B->X.ctx_stats) {
+    if (record_phases) {
+      ctx->t_phase[1] = t_inner;
+      ctx->t_phase[3] = t_resid;
+      ctx->t_phase[2] = (double)n_updates;
+    } else {
+      ctx->t_phase[1] += t_inner;
+      ctx->t_phase[3] += t_resid;
+      ctx->t_phase[2] += (double)n_updates;
+    }
   }
   return status;
 }
@@ -1896,7 +2034,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
 // Per-realization results of the last solve on the host; batch status.
 int block_results(Context* ctx, BlockSys* B, int status, int* its_out, double* res_out) {
   const int Rp = B->Rp;
-  cudaStream_t st = ctx->stream;
+  cudaStream_t st = B->X.st;
   std::vector<int> its(Rp), brk(Rp), done(Rp);
   std::vector<double> res(Rp);
   MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), B->s.its, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
@@ -1908,7 +2046,7 @@ int block_results(Context* ctx, BlockSys* B, int status, int* its_out, double* r
   for (int r = 0; r < B->R; ++r) {
     if (its_out) its_out[r] = its[r];
     if (res_out) res_out[r] = res[r];
-    if (!done[r] && status == MSG_OK) status = brk[r] ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
+    if (!done[r] && status == MSG_OK) status = brk[r] == 1 ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
   }
   return status;
 }
@@ -1919,6 +2057,7 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out) {
   BlockSys B;
   MSG_TRY(block_setup(ctx, m, nu, 1.0, 1.0, 0.0, R, Rp, &B));
+  B.fixed = ctx->fixed_updates != 0;
   cudaStream_t st = ctx->stream;
   MSG_TRY(block_field(ctx, m, &B, kl, d_xi));
   // b in lattice layout (one load vector for the whole batch)
@@ -2073,6 +2212,194 @@ int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const do
   }
   MSG_CUDA(ctx, cudaStreamSynchronize(st));
   MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+// ---------------------------------------------------------------- serving lanes
+// A lane is one model (mesh, material, KL table, load) with `capacity`
+// realization slots that requests enter and leave at chunk boundaries
+// (continuous batching). The FP64 true-residual step runs after every chunk
+// for every slot, and a slot's first step treats it as a new system, so a
+// request's arithmetic is the same whatever else shares the lane. It owns its
+// memory, stream, events, pinned flags and inner-loop graph.
+struct Lane {
+  Context* ctx = nullptr;
+  Mesh* m = nullptr;
+  BlockSys B;
+  DevMem own[32];
+  DevMem psi, d_xi, d_slots, d_col;
+  KLDevice kd;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[12] = {nullptr};
+  int* h_flags = nullptr;        // pinned 64 B
+  int* h_state = nullptr;        // pinned: act, done, its, breakdown, fresh [Rp each]
+  double* h_res = nullptr;       // pinned [Rp]
+  double* h_xi = nullptr;        // pinned [capacity][n_terms]
+  int* h_slots = nullptr;        // pinned [capacity]
+  double* h_col = nullptr;       // pinned [n_dofs]
+  cudaGraphExec_t graph = nullptr;
+  size_t graph_key = 0;
+  LoopCfg cfg;
+  int capacity = 0, n_terms = 0, max_it = 0, n_pending = 0;
+  double tol = 1e-8;
+  ~Lane() {
+    if (st) cudaStreamSynchronize(st);
+    if (graph) cudaGraphExecDestroy(graph);
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    void* pins[] = {h_flags, h_state, h_res, h_xi, h_slots, h_col};
+    for (void* p : pins)
+      if (p) cudaFreeHost(p);
+    if (st) cudaStreamDestroy(st);
+    if (m) release(m);
+  }
+};
+
+int lane_create(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, const double* b_host, int capacity, double tol,
+                int max_it, Lane** out) {
+  if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "serving needs a structured cube lattice");
+  if (capacity <= 0 || !(tol > 0) || max_it <= 0)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "serving lane: invalid capacity, tolerance or iteration limit");
+  std::unique_ptr<Lane> L(new Lane());
+  L->ctx = ctx;
+  L->m = m;
+  retain(m);
+  const int Rp = (capacity + 31) / 32 * 32;
+  L->capacity = Rp;
+  L->tol = tol;
+  L->max_it = max_it;
+  L->n_terms = kl->n_terms;
+  MSG_CUDA(ctx, cudaSetDevice(ctx->device));
+  MSG_CUDA(ctx, cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking));
+  for (auto& e : L->ev) MSG_CUDA(ctx, cudaEventCreate(&e));
+  MSG_CUDA(ctx, cudaMallocHost(&L->h_flags, 64));
+  MSG_CUDA(ctx, cudaMallocHost(&L->h_state, sizeof(int) * 5 * Rp));
+  MSG_CUDA(ctx, cudaMallocHost(&L->h_res, sizeof(double) * Rp));
+  MSG_CUDA(ctx, cudaMallocHost(&L->h_xi, sizeof(double) * (size_t)Rp * kl->n_terms));
+  MSG_CUDA(ctx, cudaMallocHost(&L->h_slots, sizeof(int) * Rp));
+  MSG_CUDA(ctx, cudaMallocHost(&L->h_col, sizeof(double) * (size_t)std::max(1, m->n_dofs)));
+  std::memset(L->h_flags, 0, 64);
+  BlockExec X;
+  X.st = L->st;
+  X.ev = L->ev;
+  X.h_flags = L->h_flags;
+  X.graph = &L->graph;
+  X.graph_key = &L->graph_key;
+  X.ctx_stats = false;
+  MSG_TRY(block_setup(ctx, m, nu, 1.0, 1.0, 0.0, Rp, Rp, &L->B, L->own, &X));
+  L->B.fixed = true;
+  // KL table -> psi (own copy: the context's KL workspace is reused by other calls)
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, m, kl, &kd));
+  MSG_TRY(L->psi.alloc(ctx, sizeof(double) * (size_t)kd.n_terms * m->n_elems));
+  MSG_CUDA(ctx, cudaMemcpyAsync(L->psi.ptr, kd.psi, sizeof(double) * (size_t)kd.n_terms * m->n_elems,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  L->kd = kd;
+  L->kd.psi = L->psi.as<double>();
+  MSG_TRY(L->d_xi.alloc(ctx, sizeof(double) * (size_t)Rp * kl->n_terms));
+  MSG_TRY(L->d_slots.alloc(ctx, sizeof(int) * Rp));
+  MSG_TRY(L->d_col.alloc(ctx, sizeof(double) * (size_t)std::max(1, m->n_dofs)));
+  // the load (one vector for every request of the model)
+  DevMem db;
+  MSG_TRY(db.alloc(ctx, sizeof(double) * (size_t)std::max(1, m->n_dofs)));
+  MSG_CUDA(ctx, cudaMemcpyAsync(db.ptr, b_host, sizeof(double) * m->n_dofs, cudaMemcpyHostToDevice, L->st));
+  k_lattice_rhs<<<(m->n_dofs + 255) / 256, 256, 0, L->st>>>(m->n_dofs, m->d_pad_free_rows.as<int>(), db.as<double>(),
+                                                            L->B.blat.as<double>());
+  // every slot starts empty: scalars zero, done = 1 (not iterating)
+  MSG_CUDA(ctx, cudaMemsetAsync(L->B.scal.ptr, 0, L->B.scal_bytes, L->st));
+  k_fill_int<<<(Rp + 255) / 256, 256, 0, L->st>>>(L->B.s.done, Rp, 1);
+  count_launch(ctx, 2);
+  L->cfg = loop_cfg(ctx, &L->B, tol, 0);
+  cudaGraphExec_t g = nullptr;
+  MSG_TRY(block_graph(ctx, &L->B, L->cfg, &g));
+  MSG_CUDA(ctx, cudaStreamSynchronize(L->st));
+  *out = L.release();
+  return MSG_OK;
+}
+
+void lane_destroy(Lane* L) { delete L; }
+int lane_capacity(const Lane* L) { return L->capacity; }
+int lane_n_dofs(const Lane* L) { return L->m->n_dofs; }
+int lane_n_terms(const Lane* L) { return L->n_terms; }
+
+// Queue request xi into `slot` (host side; initialised at the next cycle).
+void lane_stage(Lane* L, int slot, const double* xi) {
+  std::memcpy(L->h_xi + (size_t)L->n_pending * L->n_terms, xi, sizeof(double) * L->n_terms);
+  L->h_slots[L->n_pending++] = slot;
+}
+
+// Stop a slot at the next cycle (its request was cancelled).
+int lane_abort(Lane* L, int slot) {
+  k_fill_int<<<1, 1, 0, L->st>>>(L->B.s.done + slot, 1, 1);
+  return cudaGetLastError() == cudaSuccess ? MSG_OK : cuda_error(L->ctx, cudaGetLastError(), "lane abort");
+}
+
+// One boundary: start staged slots (zeroed vectors, field, Jacobi diagonal,
+// norms), one FP64 true-residual step for every slot, then the next chunk of
+// FP32 iterations (asynchronous). `state[slot]`: 0 iterating or empty, 1 converged,
+// 2 breakdown, 3 iteration limit; its/res valid for finished slots.
+int lane_cycle(Lane* L, int* state, int* its, double* res, int* n_active) {
+  Context* ctx = L->ctx;
+  BlockSys& B = L->B;
+  cudaStream_t st = L->st;
+  const int Rp = B.Rp;
+  if (L->n_pending > 0) {
+    const int n = L->n_pending;
+    MSG_CUDA(ctx, cudaMemcpyAsync(L->d_xi.ptr, L->h_xi, sizeof(double) * (size_t)n * L->n_terms,
+                                  cudaMemcpyHostToDevice, st));
+    MSG_CUDA(ctx, cudaMemcpyAsync(L->d_slots.ptr, L->h_slots, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    const size_t nrows = B.npad * 3;
+    const int blocks = (int)std::min<size_t>((nrows * n + 255) / 256, (size_t)ctx->sm_count * 16);
+    k_slot_reset<<<std::max(blocks, (n + 255) / 256), 256, 0, st>>>(
+        n, L->d_slots.as<int>(), nrows, Rp, B.x.as<double>(), B.r32.as<float>(), B.rB.as<float>(), B.p.as<float>(),
+        B.pB.as<float>(), B.q.as<float>(), B.qB.as<float>(), B.d.as<float>(), B.s);
+    MSG_TRY(launch_kl_field_slots(st, L->m, &L->kd, n, L->d_slots.as<int>(), L->d_xi.as<double>(), Rp,
+                                  B.E64.as<double>(), B.E32.as<float>()));
+    k_dinv_slots<<<B.L.n_int, 128, 0, st>>>(B.L, B.kdiag, B.mdiag, B.E32.as<float>(), B.interior, n,
+                                            L->d_slots.as<int>(), B.dinv.as<float>());
+    count_launch(ctx, 3);
+    MSG_TRY(block_bnorm(ctx, &B, B.blat.as<double>(), false));
+    // the staging buffers are reused by the next cycle: wait for the copies
+    MSG_CUDA(ctx, cudaStreamSynchronize(st));
+    L->n_pending = 0;
+  }
+  MSG_TRY(block_update(ctx, &B, L->cfg, B.blat.as<double>(), false, L->tol, false, L->max_it));
+  MSG_CUDA(ctx, cudaMemcpyAsync(L->h_flags, B.s.n_active, 36, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(L->h_state, B.s.act, sizeof(int) * 5 * Rp, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(L->h_res, B.s.res, sizeof(double) * Rp, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  if (L->h_flags[8]) return set_error(ctx, MSG_ERR_TIMEOUT, "a bounded wait of the staged operator expired");
+  const int* act = L->h_state;
+  const int* done = L->h_state + Rp;
+  const int* it = L->h_state + 2 * Rp;
+  const int* brk = L->h_state + 3 * Rp;
+  for (int r = 0; r < Rp; ++r) {
+    state[r] = act[r] ? 0 : (brk[r] == 1 ? 2 : brk[r] == 2 ? 3 : (done[r] ? 1 : 0));
+    its[r] = it[r];
+    res[r] = L->h_res[r];
+  }
+  *n_active = L->h_flags[0];
+  if (L->h_flags[0] > 0) {
+    cudaGraphExec_t g = nullptr;
+    MSG_TRY(block_graph(ctx, &B, L->cfg, &g));
+    cudaError_t e = cudaGraphLaunch(g, st);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "lane chunk");
+    count_launch(ctx, (B.modal ? 2 : 5) * L->cfg.chunk);
+  }
+  return MSG_OK;
+}
+
+// Displacements of a finished slot (DOF numbering) into the caller's host buffer.
+int lane_fetch(Lane* L, int slot, double* X) {
+  Context* ctx = L->ctx;
+  const int nd = L->m->n_dofs;
+  k_gather_column<<<(nd + 255) / 256, 256, 0, L->st>>>(nd, L->B.Rp, slot, L->m->d_pad_free_rows.as<int>(),
+                                                      L->B.x.as<double>(), L->d_col.as<double>());
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaMemcpyAsync(L->h_col, L->d_col.ptr, sizeof(double) * nd, cudaMemcpyDeviceToHost, L->st));
+  MSG_CUDA(ctx, cudaStreamSynchronize(L->st));
+  if (X) std::memcpy(X, L->h_col, sizeof(double) * nd);
   return MSG_OK;
 }
 

@@ -66,7 +66,33 @@ __global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, 
   }
 }
 
+// E of a list of realization slots (one thread per element and slot):
+// E[row(e)*Rp + slot] = exp(mu + sum_k xi[i][k] psi[k][e]) in FP64 and FP32,
+// the same expression as k_kl_field. xi [n_slots][K].
+__global__ void k_kl_field_slots(int ne, int K, int n_slots, const int* __restrict__ slots,
+                                 const double* __restrict__ xi, const double* __restrict__ psi, double mu, int Rp,
+                                 double* __restrict__ E64, float* __restrict__ E32, const int* __restrict__ elem_row) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (e >= ne || i >= n_slots) return;
+  const double* x = xi + (size_t)i * K;
+  double s = mu;
+  for (int k = 0; k < K; ++k) s += x[k] * psi[(size_t)k * ne + e];
+  const double E = exp(s);
+  const size_t o = (size_t)elem_row[e] * Rp + slots[i];
+  E64[o] = E;
+  E32[o] = (float)E;
+}
+
 }  // namespace
+
+int launch_kl_field_slots(cudaStream_t st, const Mesh* m, const KLDevice* kl, int n_slots, const int* d_slots,
+                          const double* d_xi, int Rp, double* d_E64, float* d_E32) {
+  dim3 grid((m->n_elems + 127) / 128, n_slots);
+  k_kl_field_slots<<<grid, 128, 0, st>>>(m->n_elems, kl->n_terms, n_slots, d_slots, d_xi, kl->psi, kl->mu, Rp, d_E64,
+                                         d_E32, m->d_pad_elem_row.as<int>());
+  return cudaGetLastError() == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
+}
 
 int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
   const int K = kl->n_terms;

@@ -516,6 +516,10 @@ int MSG_CREATE(int device, uint64_t mem_budget_bytes, MSG_CTX* out) {
 
 int MSG_DESTROY(MSG_CTX ctx) {
   if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    if (ctx->server) server_destroy(ctx);  // the serving lanes hold meshes of this context
+  }
   release(ctx);  // freed once the last mesh/matrix of this context is destroyed
   return MSG_OK;
 }
@@ -528,6 +532,7 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!std::strcmp(key, "reliable_delta") && value > 0 && value < 1) { ctx->reliable_delta = value; return MSG_OK; }
   if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
   if (!std::strcmp(key, "modal_operator") && (value == 0 || value == 1)) { ctx->modal = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "fixed_updates") && (value == 0 || value == 1)) { ctx->fixed_updates = (int)value; return MSG_OK; }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 

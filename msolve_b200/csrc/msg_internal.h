@@ -67,6 +67,7 @@ struct Context {
   double reliable_delta = 0.1;  // FP64 residual replacement when ||r|| drops by this factor
   int chunk = 16;               // inner iterations per captured graph launch
   int modal = 1;                // FP32 operator: 1 = Walsh-mode (modal) kernel, 0 = dense value-class kernel
+  int fixed_updates = 0;        // 1: FP64 true-residual step after every graph chunk (batch-invariant results)
   // Workspace kept across calls (allocation and cudaFree synchronise the
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
@@ -76,8 +77,12 @@ struct Context {
   cudaEvent_t ev[12] = {nullptr};   // timing events
   cudaGraphExec_t batch_graph = nullptr;  // inner-loop graph of the last batch configuration
   size_t batch_graph_key = 0;
+  void* server = nullptr;  // serving worker and lanes (serve.cpp), nullptr until MSG_SERVE_START
   ~Context();
 };
+
+// Stop the serving worker of a context and free its lanes (serve.cpp).
+void server_destroy(Context* ctx);
 
 // Lazily created pinned flags and events of a context.
 int context_resources(Context* ctx);
@@ -201,6 +206,10 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out);
 int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int Rp, const double* d_xi,
                     double* d_E64_er, float* d_E32_er, double* d_E64_re, const int* d_elem_row = nullptr);
 
+// E of a list of realization slots into the padded [row][Rp] layouts (FP64 and FP32)
+int launch_kl_field_slots(cudaStream_t st, const Mesh* m, const KLDevice* kl, int n_slots, const int* d_slots,
+                          const double* d_xi, int Rp, double* d_E64, float* d_E32);
+
 // batched mixed-precision solve on a structured lattice (kernels_block.cu)
 struct BatchOut {
   double* tip = nullptr;
@@ -223,6 +232,19 @@ struct NewmarkParams {
 int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                   const NewmarkParams& nm, const double* d_f_dof, int max_it, double tol, int tip_dof,
                   double* tip_hist, double* d_U, int* its_total);
+
+// Serving lanes (kernels_block.cu): continuous batching of one model's requests.
+struct Lane;
+int lane_create(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, const double* b_host, int capacity, double tol,
+                int max_it, Lane** out);
+void lane_destroy(Lane* L);
+int lane_capacity(const Lane* L);
+int lane_n_dofs(const Lane* L);
+int lane_n_terms(const Lane* L);
+void lane_stage(Lane* L, int slot, const double* xi);
+int lane_abort(Lane* L, int slot);
+int lane_cycle(Lane* L, int* state, int* its, double* res, int* n_active);
+int lane_fetch(Lane* L, int slot, double* X);
 
 // Element stiffness of one cube of side h at E=1 (host, via the K1 kernel): K[24][24] full.
 int unit_cube_khat(Context* ctx, double h, double nu, double* K576);

@@ -1,0 +1,69 @@
+"""Host mirror of the serving entry points (MSG_SERVE_*): continuous batching of
+independent realizations of registered models on one context.
+
+    srv = Server(ctx, max_batch=64)
+    m = srv.add_model(model, kl, tol=1e-8)        # one structured mesh + material + KL table + load
+    rid = srv.submit(m, xi)                        # one realization
+    out = srv.poll(rid, timeout_ms=-1)             # dict(X, iterations, rel_res, latency_ms)
+
+A request's result does not depend on what else is in flight (bitwise)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .analyzers import GpuMesh
+
+
+class Server:
+    def __init__(self, ctx, max_batch=64):
+        self.ctx = ctx
+        self._models = []
+        N.check(N.lib().MSG_SERVE_START(ctx.handle, int(max_batch)), ctx.handle, "MSG_SERVE_START")
+
+    def add_model(self, model, coefficients_provider, tol=1e-8, max_iterations=20000):
+        mesh = GpuMesh(self.ctx, model)
+        s = coefficients_provider.struct()
+        b = N.f64(model.subdomains[0].RHS)
+        mid = C.c_int(0)
+        st = N.lib().MSG_SERVE_ADD_MODEL(self.ctx.handle, mesh.handle, float(model.poisson), C.byref(s), N.ptr(b),
+                                         float(tol), int(max_iterations), C.byref(mid))
+        N.check(st, self.ctx.handle, "MSG_SERVE_ADD_MODEL")
+        self._models.append((mesh, model, coefficients_provider, s))
+        return mid.value
+
+    def submit(self, model_id, xi):
+        xi = N.f64(xi)
+        rid = C.c_uint64(0)
+        N.check(N.lib().MSG_SERVE_SUBMIT(self.ctx.handle, int(model_id), N.ptr(xi), C.byref(rid)), self.ctx.handle,
+                "MSG_SERVE_SUBMIT")
+        return rid.value, int(model_id)
+
+    def poll(self, request, timeout_ms=-1):
+        """None while pending; else dict(X, iterations, rel_res, latency_ms). Raises on failure."""
+        rid, model_id = request
+        n_dofs = self._models[model_id][1].n_dofs
+        X = np.zeros(n_dofs)
+        its = C.c_int(0)
+        res = C.c_double(0)
+        lat = C.c_double(0)
+        st = N.lib().MSG_SERVE_POLL(self.ctx.handle, C.c_uint64(rid), int(timeout_ms), N.ptr(X), C.byref(its),
+                                    C.byref(res), C.byref(lat))
+        if st == N.MSG_PENDING:
+            return None
+        N.check(st, self.ctx.handle, "MSG_SERVE_POLL")
+        return {"X": X, "iterations": its.value, "rel_res": res.value, "latency_ms": lat.value}
+
+    def cancel(self, request):
+        N.check(N.lib().MSG_SERVE_CANCEL(self.ctx.handle, C.c_uint64(request[0])), self.ctx.handle, "MSG_SERVE_CANCEL")
+
+    def stats(self):
+        q, r = C.c_int64(0), C.c_int64(0)
+        N.check(N.lib().MSG_SERVE_STATS(self.ctx.handle, C.byref(q), C.byref(r)), self.ctx.handle, "MSG_SERVE_STATS")
+        return {"queued": q.value, "running": r.value}
+
+    def stop(self):
+        N.lib().MSG_SERVE_STOP(self.ctx.handle)
+        self._models = []

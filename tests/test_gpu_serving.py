@@ -1,0 +1,132 @@
+"""Serving (MSG_SERVE_*): continuous batching of independent realizations.
+Results against FP64 oracle solves (1e-8 max-norm), bitwise identity of a
+request alone and inside a changing mix, bitwise identity with the batched
+Monte Carlo solve under per-chunk true-residual steps, cancellation, and two
+models served side by side."""
+import numpy as np
+import pytest
+
+import msolve_b200 as M
+from msolve_b200 import _native as N
+from msolve_b200.serving import Server
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n, n_terms=12):
+    model = M.clamped_block_model(n)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, n_terms, 6)
+    return model, kl
+
+
+def _oracle(model, kl, xi, n):
+    cen = O.centroids(model.xyz, model.conn)
+    E = O.kl_field(cen, [n, n, n], kl.table(), xi[None, :], mean=kl.mean, sigma=kl.sigma,
+                   mean_correction=kl.mean_correction)[0]
+    cons = (model.dof < 0).astype(np.uint8)
+    x, info = O.block_solve_pcg(n, n, n, cons, E, model.poisson, model.subdomains[0].RHS, tol=1e-13, max_it=100000)
+    return x
+
+
+@pytest.fixture
+def server(ctx):
+    srv = Server(ctx, max_batch=32)
+    yield srv
+    srv.stop()
+
+
+def test_requests_match_oracle(server):
+    n = 6
+    model, kl = _problem(n)
+    m = server.add_model(model, kl, tol=1e-10)
+    xis = np.random.default_rng(5).standard_normal((10, 12))
+    reqs = [server.submit(m, xi) for xi in xis]
+    for xi, rq in zip(xis, reqs):
+        out = server.poll(rq, timeout_ms=-1)
+        assert out["rel_res"] < 1e-10 and out["iterations"] > 0 and out["latency_ms"] > 0
+        xo = _oracle(model, kl, xi, n)
+        assert np.abs(out["X"] - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+def test_alone_and_mixed_are_bitwise_equal(server):
+    n = 6
+    model, kl = _problem(n)
+    m = server.add_model(model, kl, tol=1e-10)
+    rng = np.random.default_rng(9)
+    xa = rng.standard_normal(12)
+    alone = server.poll(server.submit(m, xa), timeout_ms=-1)
+    others = rng.standard_normal((45, 12))
+    first = [server.submit(m, xi) for xi in others[:20]]
+    server.poll(first[0], timeout_ms=-1)  # the batch is running when the request joins
+    ra = server.submit(m, xa)
+    rest = [server.submit(m, xi) for xi in others[20:]]
+    mixed = server.poll(ra, timeout_ms=-1)
+    for rq in first[1:] + rest:
+        server.poll(rq, timeout_ms=-1)
+    assert np.array_equal(alone["X"], mixed["X"])
+    assert alone["iterations"] == mixed["iterations"] and alone["rel_res"] == mixed["rel_res"]
+
+
+def test_matches_batched_solve_with_fixed_updates(ctx, server):
+    n, R = 6, 8
+    model, kl = _problem(n)
+    xis = np.random.default_rng(2).standard_normal((R, 12))
+    ctx.set_option("fixed_updates", 1)
+    try:
+        mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=12, simulations=R,
+                                                        mode="mixed", tolerance=1e-10)
+        mc.RandomNumbers = xis
+        mc.Solve()
+    finally:
+        ctx.set_option("fixed_updates", 0)
+    m = server.add_model(model, kl, tol=1e-10)
+    outs = [server.poll(server.submit(m, xi), timeout_ms=-1) for xi in xis]
+    for r in range(R):
+        assert np.array_equal(outs[r]["X"], mc.Solutions[r]), r
+        assert outs[r]["iterations"] == mc.Iterations[r]
+
+
+def test_cancel(server):
+    n = 8
+    model, kl = _problem(n)
+    m = server.add_model(model, kl, tol=1e-12)
+    xis = np.random.default_rng(4).standard_normal((70, 12))
+    reqs = [server.submit(m, xi) for xi in xis]  # 70 > 32 slots: the tail waits in the queue
+    server.cancel(reqs[-1])
+    server.cancel(reqs[0])
+    with pytest.raises(N.MSolveError) as e:
+        server.poll(reqs[-1], timeout_ms=-1)
+    assert e.value.code == N.MSG_ERR_CANCELLED
+    with pytest.raises(N.MSolveError):
+        server.poll(reqs[0], timeout_ms=-1)
+    for rq in reqs[1:-1]:
+        assert server.poll(rq, timeout_ms=-1)["rel_res"] < 1e-12
+    assert server.stats() == {"queued": 0, "running": 0}
+
+
+def test_two_models_side_by_side(server):
+    probs = [(4,) + _problem(4), (8,) + _problem(8)]
+    ids = [server.add_model(model, kl, tol=1e-10) for _, model, kl in probs]
+    rng = np.random.default_rng(6)
+    jobs = []
+    for k in range(12):
+        which = k % 2
+        xi = rng.standard_normal(12)
+        jobs.append((which, xi, server.submit(ids[which], xi)))
+    for which, xi, rq in jobs:
+        n, model, kl = probs[which]
+        out = server.poll(rq, timeout_ms=-1)
+        xo = _oracle(model, kl, xi, n)
+        assert np.abs(out["X"] - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+def test_poll_without_wait_and_unknown_request(server):
+    model, kl = _problem(4)
+    m = server.add_model(model, kl, tol=1e-10)
+    rq = server.submit(m, np.zeros(12))
+    out = server.poll(rq, timeout_ms=0)
+    while out is None:
+        out = server.poll(rq, timeout_ms=50)
+    with pytest.raises(N.ArgumentError):
+        server.poll(rq, timeout_ms=0)  # forgotten after the successful poll
