@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--newmark-R", type=int, default=256)
     p.add_argument("--newmark-n", type=int, default=24)
     p.add_argument("--newmark-steps", type=int, default=200)
+    p.add_argument("--no-serving", action="store_true", help="skip the serving (continuous batching) measurement")
+    p.add_argument("--serve-rates", default="100,400", help="Poisson arrival rates (requests/s) to run")
+    p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
@@ -191,6 +194,61 @@ def newmark_leg(args, ctx):
             "seconds": sec, "realization_steps_per_s": R * nm.steps / sec,
             "mean_iterations_per_step": float(np.mean(nm.Iterations)) / nm.steps,
             "tip_ux_final_mean": float(np.mean(hist[:, -1]))}
+
+
+def serving_leg(args, ctx):
+    """Serving: Poisson arrivals (seeded) of single-realization requests on cube
+    meshes of side {8, 16, 24, 32, 48} (uniform), fresh xi per request, tol 1e-8,
+    through MSG_SERVE_* (continuous batching, 64 slots per model). Latency =
+    submit to finish, measured by the server."""
+    import msolve_b200 as M
+    from msolve_b200.serving import Server
+    sides = (8, 16, 24, 32, 48)
+    srv = Server(ctx, max_batch=64)
+    models = {}
+    try:
+        for n in sides:
+            model = M.clamped_block_model(n)
+            kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, args.terms, 12)
+            models[n] = srv.add_model(model, kl, tol=1e-8)
+        out = {"workload": f"Poisson arrivals, cube side uniform in {list(sides)}, one realization per request "
+                           f"({args.terms}-term KL lognormal E, sigma 0.3), FP64 true residual < 1e-8, 64 slots per "
+                           f"model, continuous batching", "rates": []}
+        # warm-up: one request per model
+        for n in sides:
+            srv.poll(srv.submit(models[n], np.zeros(args.terms)), timeout_ms=-1)
+        for rate in [float(v) for v in args.serve_rates.split(",") if v]:
+            rng = np.random.default_rng(int(rate))
+            k = args.serve_requests
+            gaps = rng.exponential(1.0 / rate, k)
+            which = rng.choice(sides, k)
+            xis = rng.standard_normal((k, args.terms))
+            reqs = []
+            t0 = time.perf_counter()
+            t_next = t0
+            for i in range(k):
+                t_next += gaps[i]
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                reqs.append((int(which[i]), srv.submit(models[int(which[i])], xis[i])))
+            lat = {n: [] for n in sides}
+            its = []
+            for n, rq in reqs:
+                o = srv.poll(rq, timeout_ms=-1)
+                lat[n].append(o["latency_ms"])
+                its.append(o["iterations"])
+            wall = time.perf_counter() - t0
+            allv = np.concatenate([np.array(v) for v in lat.values() if v])
+            out["rates"].append({
+                "rate_per_s": rate, "requests": k, "throughput_per_s": k / wall,
+                "p50_ms": float(np.percentile(allv, 50)), "p99_ms": float(np.percentile(allv, 99)),
+                "per_side": {str(n): {"count": len(v), "p50_ms": float(np.percentile(v, 50)),
+                                      "p99_ms": float(np.percentile(v, 99))} for n, v in lat.items() if v},
+                "mean_iterations": float(np.mean(its))})
+        return out
+    finally:
+        srv.stop()
 
 
 def run_reference(args):
@@ -387,6 +445,7 @@ def main():
             cpu = cpu_baseline(args, model, kl, xi_all[0].numpy())
         its_all = np.concatenate(iters)
         newmark = None if args.no_newmark else newmark_leg(args, ctx)
+        serving = None if args.no_serving else serving_leg(args, ctx)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -421,6 +480,7 @@ def main():
             "mixed_over_fp64": value / ws / fp64_rate,
             "tip_uz": {"mean": tip_mean, "variance": tip_var, "realizations": int(cnt)},
             "newmark": newmark,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -1696,6 +1696,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   MSG_CUDA(ctx, cudaMemsetAsync(B->x.ptr, 0, sizeof(double) * nvec, st));
   MSG_CUDA(ctx, cudaMemsetAsync(B->dinv.ptr, 0, sizeof(float) * npad * Rp, st));
   MSG_CUDA(ctx, cudaMemsetAsync(B->E64.ptr, 0, sizeof(double) * npad * Rp, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(B->E32.ptr, 0, sizeof(float) * npad * Rp, st));  // ghost elements stay 0
   MSG_CUDA(ctx, cudaMemsetAsync(B->blat.ptr, 0, sizeof(double) * npad * 3, st));
 
   // TMA descriptors of the FP32 batch vectors (5-D: realization, component,

@@ -1,8 +1,9 @@
 // Serving: requests (one realization of a registered model each) are queued,
 // admitted into free slots of their model's lane at chunk boundaries, and
 // returned as soon as their own FP64 true residual is below the model's
-// tolerance (continuous batching). One worker thread per context drives the
-// lanes; the C entry points only touch the queues under the server mutex.
+// tolerance (continuous batching). One worker thread per model drives its
+// lane on the lane's own stream, so models of different sizes overlap on the
+// GPU; the C entry points only touch the queues under the server mutex.
 // No counterpart in the reference (its Monte Carlo loop is sequential,
 // ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:258-276).
 #include <chrono>
@@ -35,13 +36,13 @@ struct ServeModel {
   std::vector<int> state, its;
   std::vector<double> res;
   int running = 0;
+  std::thread worker;
 };
 
 struct Server {
   Context* ctx = nullptr;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::thread worker;
   bool stop = false;
   int capacity = 32;
   uint64_t next_id = 1;
@@ -49,107 +50,98 @@ struct Server {
   std::deque<ServeModel> models;  // deque: references stay valid while models are added
   std::unordered_map<uint64_t, ServeRequest> reqs;
 
-  void run();
+  void run(ServeModel& m);
   ~Server() {
     {
       std::lock_guard<std::mutex> g(mu);
       stop = true;
     }
     cv_work.notify_all();
-    if (worker.joinable()) worker.join();
+    for (auto& m : models)
+      if (m.worker.joinable()) m.worker.join();
     for (auto& m : models) lane_destroy(m.lane);
   }
 };
 
-void Server::run() {
+void Server::run(ServeModel& m) {
   cudaSetDevice(ctx->device);
   std::unique_lock<std::mutex> lk(mu);
   for (;;) {
-    cv_work.wait(lk, [&] {
-      if (stop) return true;
-      for (auto& m : models)
-        if (m.running > 0 || !m.queue.empty()) return true;
-      return false;
-    });
+    cv_work.wait(lk, [&] { return stop || m.running > 0 || !m.queue.empty(); });
     if (stop) return;
     // admit queued requests into free slots (host staging only)
-    for (auto& m : models) {
-      const int cap = lane_capacity(m.lane);
-      for (int s = 0; s < cap && !m.queue.empty(); ++s) {
-        if (m.slot_req[s]) continue;
-        const uint64_t id = m.queue.front();
-        m.queue.pop_front();
-        auto it = reqs.find(id);
-        if (it == reqs.end() || it->second.cancelled) continue;
-        it->second.slot = s;
-        m.slot_req[s] = id;
-        lane_stage(m.lane, s, it->second.xi.data());
-        ++m.running;
-      }
+    const int cap = lane_capacity(m.lane);
+    for (int s = 0; s < cap && !m.queue.empty(); ++s) {
+      if (m.slot_req[s]) continue;
+      const uint64_t id = m.queue.front();
+      m.queue.pop_front();
+      auto it = reqs.find(id);
+      if (it == reqs.end() || it->second.cancelled) continue;
+      it->second.slot = s;
+      m.slot_req[s] = id;
+      lane_stage(m.lane, s, it->second.xi.data());
+      ++m.running;
     }
-    // one cycle per model with work, without the lock (GPU work and syncs)
-    for (size_t mi = 0; mi < models.size(); ++mi) {
-      ServeModel& m = models[mi];
-      if (m.running == 0) continue;
-      lk.unlock();
-      int n_active = 0;
-      const int st = lane_cycle(m.lane, m.state.data(), m.its.data(), m.res.data(), &n_active);
-      lk.lock();
-      if (st != MSG_OK) {
-        // a failed cycle fails every request of the lane
-        error = st;
-        for (size_t s = 0; s < m.slot_req.size(); ++s) {
-          if (!m.slot_req[s]) continue;
-          auto it = reqs.find(m.slot_req[s]);
-          if (it != reqs.end()) {
-            it->second.finished = true;
-            it->second.status = st;
-          }
-          m.slot_req[s] = 0;
-        }
-        m.running = 0;
-        cv_done.notify_all();
-        continue;
-      }
-      for (size_t s = 0; s < m.slot_req.size(); ++s) {
-        const uint64_t id = m.slot_req[s];
-        if (!id || m.state[s] == 0) continue;
-        m.slot_req[s] = 0;
-        --m.running;
-        auto it = reqs.find(id);
-        if (it == reqs.end()) continue;
-        std::vector<double> X;
-        int fs = MSG_OK;
-        if (!it->second.cancelled) {
-          // fetch without the lock (the request map may change meanwhile)
-          X.resize(lane_n_dofs(m.lane));
-          lk.unlock();
-          fs = lane_fetch(m.lane, (int)s, X.data());
-          lk.lock();
-          it = reqs.find(id);
-          if (it == reqs.end()) continue;
-        }
-        ServeRequest& r = it->second;
-        if (!r.cancelled) {
-          r.X.swap(X);
-          r.its = m.its[s];
-          r.res = m.res[s];
-          r.status = fs != MSG_OK ? fs
-                     : m.state[s] == 1 ? MSG_OK
-                     : m.state[s] == 2 ? MSG_ERR_BREAKDOWN
-                                       : MSG_ERR_NOT_CONVERGED;
-        }
-        r.finished = true;
-        r.latency_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r.t0).count();
-      }
-      // cancelled requests still occupying slots are stopped at the next cycle
+    if (m.running == 0) continue;
+    // one cycle without the lock (GPU work and a stream sync)
+    lk.unlock();
+    int n_active = 0;
+    const int st = lane_cycle(m.lane, m.state.data(), m.its.data(), m.res.data(), &n_active);
+    lk.lock();
+    if (st != MSG_OK) {
+      // a failed cycle fails every request of the lane
+      error = st;
       for (size_t s = 0; s < m.slot_req.size(); ++s) {
         if (!m.slot_req[s]) continue;
         auto it = reqs.find(m.slot_req[s]);
-        if (it != reqs.end() && it->second.cancelled) lane_abort(m.lane, (int)s);
+        if (it != reqs.end()) {
+          it->second.finished = true;
+          it->second.status = st;
+        }
+        m.slot_req[s] = 0;
       }
+      m.running = 0;
       cv_done.notify_all();
+      continue;
     }
+    for (size_t s = 0; s < m.slot_req.size(); ++s) {
+      const uint64_t id = m.slot_req[s];
+      if (!id || m.state[s] == 0) continue;
+      m.slot_req[s] = 0;
+      --m.running;
+      auto it = reqs.find(id);
+      if (it == reqs.end()) continue;
+      std::vector<double> X;
+      int fs = MSG_OK;
+      if (!it->second.cancelled) {
+        // fetch without the lock (the request map may change meanwhile)
+        X.resize(lane_n_dofs(m.lane));
+        lk.unlock();
+        fs = lane_fetch(m.lane, (int)s, X.data());
+        lk.lock();
+        it = reqs.find(id);
+        if (it == reqs.end()) continue;
+      }
+      ServeRequest& r = it->second;
+      if (!r.cancelled) {
+        r.X.swap(X);
+        r.its = m.its[s];
+        r.res = m.res[s];
+        r.status = fs != MSG_OK ? fs
+                   : m.state[s] == 1 ? MSG_OK
+                   : m.state[s] == 2 ? MSG_ERR_BREAKDOWN
+                                     : MSG_ERR_NOT_CONVERGED;
+      }
+      r.finished = true;
+      r.latency_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r.t0).count();
+    }
+    // cancelled requests still occupying slots are stopped at the next cycle
+    for (size_t s = 0; s < m.slot_req.size(); ++s) {
+      if (!m.slot_req[s]) continue;
+      auto it = reqs.find(m.slot_req[s]);
+      if (it != reqs.end() && it->second.cancelled) lane_abort(m.lane, (int)s);
+    }
+    cv_done.notify_all();
   }
 }
 
@@ -181,7 +173,6 @@ int MSG_SERVE_START(MSG_CTX ctx, int max_batch) {
   s->ctx = ctx;
   s->capacity = max_batch;
   ctx->server = s;
-  s->worker = std::thread([s] { s->run(); });
   return MSG_OK;
 }
 
@@ -201,6 +192,8 @@ int MSG_SERVE_ADD_MODEL(MSG_CTX ctx, MSG_MESH mesh, double nu, const MSG_KL* kl,
   m.its.assign(cap, 0);
   m.res.assign(cap, 0.0);
   srv->models.push_back(std::move(m));
+  ServeModel& added = srv->models.back();
+  added.worker = std::thread([srv, &added] { srv->run(added); });
   *model_id = (int)srv->models.size() - 1;
   return MSG_OK;
 }
