@@ -123,6 +123,17 @@ int MSG_MAT_DESTROY(MSG_MAT mat);
 int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
                   double* rel_res);
 
+/* MSG_PCG_SOLVE with the matrix values in FP32 inside the loop (half the
+ * bytes of the dominant SpMV traffic) and FP64 refinement: vectors stay FP64;
+ * when the recursive residual has dropped by "reliable_delta" (or below tol)
+ * it is replaced by the FP64 true residual b - K x computed with the FP64
+ * values, the search direction is kept, and the solve stops only when
+ * ||b - K x|| / ||b|| < tol in FP64 (rel_res). iterations counts as
+ * MSG_PCG_SOLVE. The FP32 copy of the values is built on first use. No
+ * counterpart in the reference. */
+int MSG_PCG_SOLVE_MIXED(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
+                        double* rel_res);
+
 /* MSG_PCG_SOLVE without device allocation. No counterpart in the reference.
  * For callers that must not allocate device memory while solving: cudaMalloc
  * and cudaFree synchronise the whole device (a caller overlapping other GPU

@@ -84,6 +84,7 @@ SIGNATURES = {
     "MSG_MAT_DIAGONAL": (C.c_int, [_vp, _d]),
     "MSG_MAT_DESTROY": (C.c_int, [_vp]),
     "MSG_PCG_SOLVE": (C.c_int, [_vp, _d, _d, C.c_int, C.c_double, _i, _d]),
+    "MSG_PCG_SOLVE_MIXED": (C.c_int, [_vp, _d, _d, C.c_int, C.c_double, _i, _d]),
     "MSG_PCG_SOLVE_NOALLOC": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_double, _i, _d]),
     "MSG_KL_TABLE": (C.c_int, [_d, C.c_double, C.c_int, C.c_int, _d, _d, _i, _d]),
     "MSG_KL_FIELD": (C.c_int, [_vp, C.POINTER(MSG_KL), C.c_int, _d, _d]),

@@ -143,11 +143,14 @@ class ProblemStructural:
 
 class SolverPCG:
     """ISolver over the device Jacobi-PCG (SolverPCG.Solve, PCG/SolverPCG.cs:105-149).
-    Solve() uses (20000, 1e-7) as SolverPCG<T>.Solve() does (SolverPCGSkyline.cs:102-108)."""
+    Solve() uses (20000, 1e-7) as SolverPCG<T>.Solve() does (SolverPCGSkyline.cs:102-108).
+    precision="mixed": FP32 matrix values in the loop, FP64 refinement to the FP64
+    true residual (MSG_PCG_SOLVE_MIXED)."""
 
-    def __init__(self, ctx, model, max_iterations=20000, tolerance=1e-7):
+    def __init__(self, ctx, model, max_iterations=20000, tolerance=1e-7, precision="fp64"):
         self.ctx, self.model = ctx, model
         self.max_iterations, self.tolerance = max_iterations, tolerance
+        self.precision = precision
         self.matrix = None
         self.iterations = 0
         self.rel_res = None
@@ -161,8 +164,9 @@ class SolverPCG:
         b = N.f64(s.RHS)
         x = np.zeros(self.model.n_dofs)
         it, rr = C.c_int(0), C.c_double(0)
-        st = N.lib().MSG_PCG_SOLVE(self.matrix.handle, N.ptr(b), N.ptr(x), int(max_iterations or self.max_iterations),
-                                   float(tolerance or self.tolerance), C.byref(it), C.byref(rr))
+        fn = N.lib().MSG_PCG_SOLVE_MIXED if self.precision == "mixed" else N.lib().MSG_PCG_SOLVE
+        st = fn(self.matrix.handle, N.ptr(b), N.ptr(x), int(max_iterations or self.max_iterations),
+                float(tolerance or self.tolerance), C.byref(it), C.byref(rr))
         self.iterations, self.rel_res = it.value, rr.value
         s.Solution = x
         N.check(st, self.ctx.handle, "MSG_PCG_SOLVE")

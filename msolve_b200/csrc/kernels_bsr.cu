@@ -15,6 +15,8 @@
 // coalesced load; the matrix stream is the whole HBM traffic of the product.
 #include <algorithm>
 
+#include <cstddef>
+
 #include "msg_internal.h"
 
 namespace msg {
@@ -218,13 +220,15 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n_rows, const doub
     st->beta = 0; st->alpha = 0; st->err = 0;
     st->it = 0; st->iterations = 0; st->matvecs = 0; st->status = 0;
     st->done = (st->bnorm > 1e-25) ? 0 : 1;  // SolverPCG.cs:112
+    st->need = 0; st->err_ref = 1.0;
     st->counter = 0;
   }
 }
 
+template <class V>
 __global__ void __launch_bounds__(96) k_pcg_dir_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
                                                               const int* __restrict__ col,
-                                                              const double* __restrict__ val,
+                                                              const V* __restrict__ val,
                                                               const double* __restrict__ dinv,
                                                               const double* __restrict__ r, double* p0, double* p1,
                                                               double* __restrict__ q, double* __restrict__ partial,
@@ -245,11 +249,11 @@ __global__ void __launch_bounds__(96) k_pcg_dir_spmv(int n_rows, const int64_t* 
     for (int64_t s = s0; s < s1; ++s) {
       const int cc = __ldg(col + s * 32 + lane);
       if (cc < 0) break;
-      const double* v = val + (s * 9 + 3 * c) * 32 + lane;
+      const V* v = val + (s * 9 + 3 * c) * 32 + lane;
       const double x0 = dinv[3 * cc] * r[3 * cc] + beta * pold[3 * cc];
       const double x1 = dinv[3 * cc + 1] * r[3 * cc + 1] + beta * pold[3 * cc + 1];
       const double x2 = dinv[3 * cc + 2] * r[3 * cc + 2] + beta * pold[3 * cc + 2];
-      yc += __ldg(v) * x0 + __ldg(v + 32) * x1 + __ldg(v + 64) * x2;
+      yc += (double)__ldg(v) * x0 + (double)__ldg(v + 32) * x1 + (double)__ldg(v + 64) * x2;
     }
     const double pn = dinv[3 * row + c] * r[3 * row + c] + beta * pold[3 * row + c];
     pnew[3 * row + c] = pn;
@@ -299,7 +303,10 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const do
   const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
   if (threadIdx.x == 0) {
     st->err = sqrt(tr) / st->bnorm;
-    if (st->err < st->tol) {
+    if (st->mixed && (st->err < st->tol || st->err < st->delta * st->err_ref)) {
+      // pause for an FP64 true residual (zr keeps the gamma of this iteration's start)
+      st->need = 1; st->done = 1; st->rr = tz;
+    } else if (st->err < st->tol) {
       st->done = 1; st->iterations = it;
     } else if (it + 1 >= st->max_it) {
       st->done = 1; st->iterations = st->max_it; st->status = MSG_ERR_NOT_CONVERGED;
@@ -310,6 +317,53 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const do
     }
     st->counter = 0;
   }
+}
+
+// Mixed precision: r = b - y (y = K x with the FP64 values), the true
+// relative residual decides convergence; otherwise the recursive residual is
+// replaced, the search direction kept (beta = gamma_true / gamma_start) and the
+// loop resumes.
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_true_resid(int n_rows, const double* __restrict__ b,
+                                                                const double* __restrict__ y,
+                                                                const double* __restrict__ dinv,
+                                                                double* __restrict__ r, double* __restrict__ partial,
+                                                                PcgState* st) {
+  __shared__ double sh[32];
+  double rr = 0, zr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
+    const double ri = b[i] - y[i];
+    r[i] = ri;
+    rr += ri * ri;
+    zr += dinv[i] * ri * ri;
+  }
+  double s1 = block_sum(rr, sh);
+  double s2 = block_sum(zr, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
+  if (!last_block(&st->counter)) return;
+  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
+  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  if (threadIdx.x == 0) {
+    const int it = st->it;
+    st->err = sqrt(tr) / st->bnorm;
+    st->need = 0;
+    if (st->err < st->tol) {
+      st->done = 1; st->iterations = it;
+    } else if (it + 1 >= st->max_it) {
+      st->done = 1; st->iterations = st->max_it; st->status = MSG_ERR_NOT_CONVERGED;
+    } else {
+      st->beta = tz / st->zr;
+      st->zr = tz;
+      st->it = it + 1;
+      st->err_ref = st->err;
+      st->done = 0;
+    }
+    st->counter = 0;
+  }
+}
+
+__global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
 }
 
 }  // namespace
@@ -367,14 +421,17 @@ int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* 
 
 // Runs the device PCG on node-layout vectors. The loop body (2 kernels) is
 // captured once per matrix as a CUDA graph of `chunk` iterations; the host
-// launches the graph and reads back the 4-byte `done` flag after each chunk.
+// launches the graph and reads back the state flags after each chunk.
 // Kernels after convergence return immediately, so the recorded iteration
-// count is exact.
+// count is exact. Mixed precision: the loop's SpMV reads FP32 values; when it
+// pauses (need), y = K x with the FP64 values and k_pcg_true_resid replace the
+// recursive residual (or end the solve on the true residual).
 int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, int max_it, double tol, int* iterations,
-                     double* rel_res, int* status) {
+                     double* rel_res, int* status, bool mixed) {
   Mesh* m = A->mesh;
   const int nr = m->n_nodes;
   const int n = 3 * nr;
+  MSG_TRY(context_resources(ctx));
   if (!A->d_r.ptr) {
     MSG_TRY(A->d_r.alloc(ctx, sizeof(double) * n));
     MSG_TRY(A->d_p0.alloc(ctx, sizeof(double) * n));
@@ -385,6 +442,13 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     MSG_TRY(A->d_state.alloc(ctx, sizeof(PcgState)));
     MSG_CUDA(ctx, cudaMemsetAsync(A->d_state.ptr, 0, sizeof(PcgState), ctx->stream));
   }
+  if (mixed && !A->d_val32.ptr) {
+    const size_t nv = (size_t)m->pat.n_slots * 32 * 9;
+    MSG_TRY(A->d_val32.alloc(ctx, sizeof(float) * std::max<size_t>(1, nv)));
+    MSG_TRY(A->d_tmp.alloc(ctx, sizeof(double) * n));
+    k_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(nv, A->d_val.as<double>(), A->d_val32.as<float>());
+    count_launch(ctx);
+  }
   PcgState* st = A->d_state.as<PcgState>();
   const int grid_v = std::min(4096, std::max(1, std::min((n + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 8)));
   const int grid_s = m->pat.n_slices;  // 96-thread CTAs, one 32-row slice each
@@ -393,22 +457,32 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
                                                       A->d_p0.as<double>(), A->d_p1.as<double>(),
                                                       A->d_partial.as<double>(), st);
   count_launch(ctx);
-  // tol / max_it into the state (after init so the counter reset does not race)
+  // tol, max_it and the mixed-precision settings into the state (after init so the counter reset does not race)
   {
-    struct { double tol; } h{tol};
-    MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &h.tol, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const int mx = mixed ? 1 : 0;
+    const double delta = ctx->reliable_delta;
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &tol, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     MSG_CUDA(ctx, cudaMemcpyAsync(&st->max_it, &max_it, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->mixed, &mx, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->delta, &delta, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    // the pageable copies above are staged before they return
   }
   const int chunk = 8;
-  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x) {
+  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x || A->graph_mixed != (int)mixed) {
     if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
-      k_pcg_dir_spmv<<<grid_s, 96, 0, ctx->stream>>>(
-          nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val.as<double>(), A->d_dinv.as<double>(),
-          A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
-          A->d_partial.as<double>(), st);
+      if (mixed)
+        k_pcg_dir_spmv<float><<<grid_s, 96, 0, ctx->stream>>>(
+            nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val32.as<float>(), A->d_dinv.as<double>(),
+            A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
+            A->d_partial.as<double>(), st);
+      else
+        k_pcg_dir_spmv<double><<<grid_s, 96, 0, ctx->stream>>>(
+            nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val.as<double>(), A->d_dinv.as<double>(),
+            A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
+            A->d_partial.as<double>(), st);
       k_pcg_update<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
                                                             A->d_p0.as<double>(), A->d_p1.as<double>(),
                                                             A->d_q.as<double>(), A->d_partial.as<double>(), st);
@@ -419,27 +493,40 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphInstantiate");
     A->graph_chunk = chunk;
     A->graph_x = d_x;
+    A->graph_mixed = mixed ? 1 : 0;
   }
-  int* h_done = nullptr;
-  MSG_CUDA(ctx, cudaMallocHost(&h_done, sizeof(int)));
-  int done = 0;
-  const int max_chunks = max_it / chunk + 2;
-  for (int c = 0; c < max_chunks && !done; ++c) {
+  int* h = ctx->h_flags;  // pinned: done and need
+  const size_t off_done = offsetof(PcgState, done), off_need = offsetof(PcgState, need);
+  const int max_rounds = max_it / chunk + 2 * max_it + 4;  // chunks plus true-residual pauses
+  for (int round = 0; round < max_rounds; ++round) {
     cudaError_t e = cudaGraphLaunch(A->graph, ctx->stream);
-    if (e != cudaSuccess) { cudaFreeHost(h_done); return cuda_error(ctx, e, "cudaGraphLaunch"); }
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphLaunch");
     count_launch(ctx, 2 * chunk);
-    e = cudaMemcpyAsync(h_done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) { cudaFreeHost(h_done); return cuda_error(ctx, e, "pcg chunk"); }
-    done = *h_done;
+    MSG_CUDA(ctx, cudaMemcpyAsync(h, reinterpret_cast<char*>(st) + off_done, sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(h + 1, reinterpret_cast<char*>(st) + off_need, sizeof(int),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h[1]) {
+      // FP64 true residual r = b - K x (x in FP64), then resume or stop
+      k_bsr_spmv3<<<m->pat.n_slices, 96, 0, ctx->stream>>>(nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
+                                                            A->d_val.as<double>(), d_x, A->d_tmp.as<double>());
+      k_pcg_true_resid<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, d_b, A->d_tmp.as<double>(),
+                                                                 A->d_dinv.as<double>(), A->d_r.as<double>(),
+                                                                 A->d_partial.as<double>(), st);
+      count_launch(ctx, 2);
+      MSG_CUDA(ctx, cudaMemcpyAsync(h, reinterpret_cast<char*>(st) + off_done, sizeof(int), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+      MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    if (h[0]) break;
   }
-  cudaFreeHost(h_done);
   PcgState hs;
   MSG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost, ctx->stream));
   MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (iterations) *iterations = hs.iterations;
   if (rel_res) *rel_res = hs.err;
-  if (status) *status = hs.status;
+  if (status) *status = hs.done ? hs.status : MSG_ERR_NOT_CONVERGED;
   return MSG_OK;
 }
 

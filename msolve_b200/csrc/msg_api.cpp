@@ -699,32 +699,42 @@ int MSG_MAT_DESTROY(MSG_MAT A) {
   return MSG_OK;
 }
 
-int MSG_PCG_SOLVE(MSG_MAT A, const double* b, double* x, int max_it, double tol, int* iterations, double* rel_res) {
+static int pcg_host(MSG_MAT A, const double* b, double* x, int max_it, double tol, int* iterations, double* rel_res,
+                    bool mixed) {
   if (!A || !b || !x || max_it <= 0 || !(tol > 0)) return MSG_ERR_INVALID_ARGUMENT;
   Mesh* m = A->mesh;
   Context* ctx = m->ctx;
   CTX_GUARD(ctx);
   const size_t n3 = 3 * (size_t)m->n_nodes;
-  DevMem dbd, dbn, dxn, dxd;
-  MSG_TRY(upload(ctx, dbd, b, (size_t)m->n_dofs));
-  MSG_TRY(dbn.alloc(ctx, sizeof(double) * n3));
-  MSG_TRY(dxn.alloc(ctx, sizeof(double) * n3));
-  MSG_TRY(dxd.alloc(ctx, sizeof(double) * std::max(1, m->n_dofs)));
-  MSG_CUDA(ctx, cudaMemsetAsync(dbn.ptr, 0, sizeof(double) * n3, ctx->stream));
-  MSG_TRY(launch_dof_to_node(ctx, m, dbd.as<double>(), dbn.as<double>(), 1, 0, 0));
+  // node-layout b / x and DOF staging kept with the matrix (no per-call allocation, graph reuse)
+  if (!A->d_bn.ptr) {
+    MSG_TRY(A->d_bd.alloc(ctx, sizeof(double) * std::max(1, m->n_dofs)));
+    MSG_TRY(A->d_bn.alloc(ctx, sizeof(double) * n3));
+    MSG_TRY(A->d_xn.alloc(ctx, sizeof(double) * n3));
+    MSG_CUDA(ctx, cudaMemsetAsync(A->d_bn.ptr, 0, sizeof(double) * n3, ctx->stream));
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(A->d_bd.ptr, b, sizeof(double) * m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
+  MSG_TRY(launch_dof_to_node(ctx, m, A->d_bd.as<double>(), A->d_bn.as<double>(), 1, 0, 0));
   int its = 0, st = 0;
   double rr = 0;
-  MSG_TRY(pcg_solve_device(ctx, A, dbn.as<double>(), dxn.as<double>(), max_it, tol, &its, &rr, &st));
-  A->graph_x = nullptr;  // dxn is released on return; force a re-capture next time
-  if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
-  MSG_TRY(launch_node_to_dof(ctx, m, dxn.as<double>(), dxd.as<double>(), 1, 0, 0));
-  MSG_CUDA(ctx, cudaMemcpyAsync(x, dxd.ptr, sizeof(double) * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_TRY(pcg_solve_device(ctx, A, A->d_bn.as<double>(), A->d_xn.as<double>(), max_it, tol, &its, &rr, &st, mixed));
+  MSG_TRY(launch_node_to_dof(ctx, m, A->d_xn.as<double>(), A->d_bd.as<double>(), 1, 0, 0));
+  MSG_CUDA(ctx, cudaMemcpyAsync(x, A->d_bd.ptr, sizeof(double) * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
   MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (iterations) *iterations = its;
   if (rel_res) *rel_res = rr;
   if (st != MSG_OK)
     return set_error(ctx, st, st == MSG_ERR_BREAKDOWN ? "PCG breakdown (p.q <= 0 or NaN)" : "PCG did not converge");
   return MSG_OK;
+}
+
+int MSG_PCG_SOLVE(MSG_MAT A, const double* b, double* x, int max_it, double tol, int* iterations, double* rel_res) {
+  return pcg_host(A, b, x, max_it, tol, iterations, rel_res, false);
+}
+
+int MSG_PCG_SOLVE_MIXED(MSG_MAT A, const double* b, double* x, int max_it, double tol, int* iterations,
+                        double* rel_res) {
+  return pcg_host(A, b, x, max_it, tol, iterations, rel_res, true);
 }
 
 int MSG_KL_TABLE(const double* L, double l, int n_terms, int n1d, double* w3, double* amp3, int* idx3, double* eig) {

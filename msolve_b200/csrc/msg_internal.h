@@ -167,16 +167,24 @@ struct PcgState {
   double tol;
   unsigned int counter;
   int pad;
+  // mixed precision (FP32 matrix values, FP64 vectors): the loop pauses (need = 1)
+  // when the recursive residual has dropped by delta since err_ref or below tol,
+  // and the host replaces it with the FP64 true residual
+  double delta, err_ref;
+  int mixed, need;
 };
 
 struct Matrix {
   Mesh* mesh = nullptr;
   DevMem d_val;   // SELL values FP64
+  DevMem d_val32; // SELL values FP32 (mixed-precision solves; built on first use)
+  DevMem d_bn, d_xn, d_bd;  // node-layout b and x, DOF-layout staging of the host entry points
   DevMem d_dinv;  // [n_nodes*3]
   // PCG workspace (node layout, 3 per node)
   DevMem d_r, d_p0, d_p1, d_q, d_partial, d_state, d_tmp, d_tmp2;
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
+  int graph_mixed = 0;
   const void* graph_x = nullptr;  // output vector the captured graph writes (not owned)
   ~Matrix();
 };
@@ -192,8 +200,10 @@ int launch_dof_to_node(Context* ctx, const Mesh* m, const double* d_in, double* 
                        int64_t out_stride);
 int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* d_out, int n_vec, int64_t in_stride,
                        int64_t out_stride);
+// mixed: FP32 matrix values in the loop's SpMV, FP64 vectors, FP64 true-residual
+// replacement (reliable updates), stop on the FP64 true residual.
 int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b_node, double* d_x_node, int max_it, double tol,
-                     int* iterations, double* rel_res, int* status);
+                     int* iterations, double* rel_res, int* status, bool mixed = false);
 
 // KL field: E64/E32 [n_elems][Rp] (realization innermost) and/or E64 [R][n_elems].
 struct KLDevice {

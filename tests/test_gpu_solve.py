@@ -107,3 +107,30 @@ def test_pcg_zero_rhs_and_not_converged(ctx):
     with pytest.raises(M.InvalidOperationError) as e:
         solver.Solve(5, 1e-12)
     assert e.value.code == -2001 and solver.iterations == 5
+
+
+def test_mixed_assembled_solve_reaches_fp64_true_residual(ctx):
+    """FP32 values in the loop, FP64 refinement: the FP64 true residual meets the
+    tolerance and the field agrees with an FP64 oracle solve; repeated calls on
+    the same matrix reuse the captured loop and give identical answers."""
+    n = 12
+    model = M.clamped_block_model(n)
+    E = np.exp(0.3 * np.random.default_rng(8).standard_normal(model.n_elems))
+    mesh = M.GpuMesh(ctx, model)
+    A = mesh.assemble(E, model.poisson)
+    b = model.subdomains[0].RHS
+    fp64 = M.SolverPCG(ctx, model, tolerance=1e-10)
+    fp64.matrix = A
+    x64 = fp64.Solve()
+    mixed = M.SolverPCG(ctx, model, tolerance=1e-10, precision="mixed")
+    mixed.matrix = A
+    xm = mixed.Solve()
+    xm2 = mixed.Solve()
+    assert np.array_equal(xm, xm2)
+    C, _ = oracle_csr(model, E)
+    xo, _ = C.pcg_jacobi(b, tol=1e-13)
+    r = b - C.multiply(xm)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
+    assert abs(mixed.rel_res - np.linalg.norm(r) / np.linalg.norm(b)) <= 1e-3 * mixed.rel_res + 1e-16
+    assert np.abs(xm - xo).max() <= 1e-8 * np.abs(xo).max()
+    assert mixed.iterations <= 1.3 * fp64.iterations + 16
