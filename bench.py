@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--newmark-n", type=int, default=24)
     p.add_argument("--newmark-steps", type=int, default=200)
     p.add_argument("--no-serving", action="store_true", help="skip the serving (continuous batching) measurement")
+    p.add_argument("--no-single", action="store_true", help="skip the 64^3 single-solve measurement")
+    p.add_argument("--single-n", type=int, default=64)
     p.add_argument("--serve-rates", default="100,400", help="Poisson arrival rates (requests/s) to run")
     p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
@@ -194,6 +196,42 @@ def newmark_leg(args, ctx):
             "seconds": sec, "realization_steps_per_s": R * nm.steps / sec,
             "mean_iterations_per_step": float(np.mean(nm.Iterations)) / nm.steps,
             "tip_ux_final_mean": float(np.mean(hist[:, -1]))}
+
+
+def single_leg(args, ctx):
+    """One large static solve (64^3 Hexa8, E = 1, nu 0.3, z=0 clamped, unit top
+    pressure): (a) the FP64 assembled drop-in (MSG_PCG_SOLVE) and (b) FP32 matrix
+    values + FP64 refinement (MSG_PCG_SOLVE_MIXED), both to the relative
+    residual 1e-8, timed after one warm-up solve each; SpMV bytes per iteration
+    (FP64: 72 B values + 4 B column per 3x3 block + x and y vectors)."""
+    import torch
+    import msolve_b200 as M
+    n = args.single_n
+    model = M.clamped_block_model(n)
+    mesh = M.GpuMesh(ctx, model)
+    A = mesh.assemble(np.ones(model.n_elems), model.poisson)
+    info = mesh.info()
+    out = {"workload": f"{n}^3 Hexa8 static solve, {model.n_dofs} free DOFs, {info['nnzb']} 3x3 blocks, "
+                       f"Jacobi PCG to ||r||/||b|| < 1e-8", "n_dofs": model.n_dofs, "nnzb": info["nnzb"]}
+    for name, prec in (("fp64", "fp64"), ("mixed", "mixed")):
+        s = M.SolverPCG(ctx, model, max_iterations=100000, tolerance=1e-8, precision=prec)
+        s.matrix = A
+        s.Solve()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.Solve()
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b)
+        per_it = ms / max(1, s.iterations)
+        spmv_bytes = (72 if prec == "fp64" else 36) * info["nnzb"] + 4 * info["nnzb"] + 16 * 3 * model.n_nodes
+        out[name] = {"ms": ms, "iterations": s.iterations, "rel_res": s.rel_res, "ms_per_iteration": per_it,
+                     "dof_iterations_per_s": model.n_dofs * s.iterations / (ms / 1e3),
+                     "spmv_bytes_per_iteration": spmv_bytes}
+    out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    A.close()
+    return out
 
 
 def serving_leg(args, ctx):
@@ -446,6 +484,7 @@ def main():
         its_all = np.concatenate(iters)
         newmark = None if args.no_newmark else newmark_leg(args, ctx)
         serving = None if args.no_serving else serving_leg(args, ctx)
+        single = None if args.no_single else single_leg(args, ctx)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -481,6 +520,7 @@ def main():
             "tip_uz": {"mean": tip_mean, "variance": tip_var, "realizations": int(cnt)},
             "newmark": newmark,
             "serving": serving,
+            "single_solve": single,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

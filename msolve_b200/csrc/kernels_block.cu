@@ -104,7 +104,7 @@ __device__ __forceinline__ void slab_apply(const T (&kv)[kKhatClasses], const T 
       constexpr int ey = decltype(EY)::value, ez = decltype(EZ)::value;
       constexpr int an = corner_id(AX, 1 - ey, 1 - ez);
       T t[3] = {T(0), T(0), T(0)};
-      T tm[3] = {T(0), T(0), T(0)};
+      [[maybe_unused]] T tm[3] = {T(0), T(0), T(0)};
       static_for<2>([&](auto BY) {
         static_for<2>([&](auto BZ) {
           constexpr int by = decltype(BY)::value, bz = decltype(BZ)::value;
@@ -225,38 +225,6 @@ __device__ __forceinline__ void pencil_of(const Lattice& L, int& J, int& Kz, boo
   valid = j < L.NY && k < L.NZ;
   J = j + 1;
   Kz = k + 1;
-}
-
-// FP32 operator: q = K p (masked), partial p.q.
-__global__ void __launch_bounds__(128, 4)
-    k_op(Lattice L, const __grid_constant__ KhatF K, const float* __restrict__ p, const float* __restrict__ E,
-         const uint8_t* __restrict__ mask, float* __restrict__ q, double* __restrict__ partial) {
-  int J, Kz;
-  bool valid;
-  pencil_of(L, J, Kz, valid);
-  const int Rp = L.Rp;
-  const int rr = blockIdx.y * 32 + threadIdx.x;
-  double pq[1] = {0.0};
-  if (valid) {
-    auto load = [&](size_t node, float* o) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) o[c] = ldv(p + (node * 3 + c) * Rp + rr);
-    };
-    auto own = [](size_t, const float*) {};
-    auto emit = [&](size_t node, const float* ownv, const float* y) {
-      const uint8_t m = mask[node];
-      float acc = 0.f;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float qc = ((m >> c) & 1) ? 0.f : y[c];
-        q[(node * 3 + c) * Rp + rr] = qc;
-        acc = fmaf(ownv[c], qc, acc);
-      }
-      pq[0] += (double)acc;
-    };
-    pencil_sweep<float>(L, K, J, Kz, E + rr, load, own, emit);
-  }
-  cta_partial<1>(pq, partial, blockIdx.x, Rp, rr);
 }
 
 // ---------------------------------------------------------------- TMA-staged FP32 operator

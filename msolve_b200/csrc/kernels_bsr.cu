@@ -22,7 +22,6 @@
 namespace msg {
 namespace {
 
-constexpr int kSpmvThreads = 128;
 
 // One thread per (flat position, block entry k): sum the element
 // contributions (e, a, b) of this block in their fixed order, then apply the
@@ -76,33 +75,6 @@ __global__ void k_bsr_diag_inv(int n_rows, const int* __restrict__ diag_pos, con
   const int lane = (int)(pos & 31);
 #pragma unroll
   for (int c = 0; c < 3; ++c) dinv[3 * row + c] = 1.0 / val[(slot * 9 + 4 * c) * 32 + lane];
-}
-
-__device__ __forceinline__ void sell_row(int row, const int64_t* __restrict__ slice_ptr, const int* __restrict__ col,
-                                         const double* __restrict__ val, const double* __restrict__ x, double* y3) {
-  const int slice = row >> 5, lane = row & 31;
-  const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
-  double y0 = 0, y1 = 0, y2 = 0;
-  for (int64_t s = s0; s < s1; ++s) {
-    const int c = __ldg(col + s * 32 + lane);
-    if (c < 0) break;
-    const double* v = val + s * 9 * 32 + lane;
-    const double x0 = __ldg(x + 3 * c), x1 = __ldg(x + 3 * c + 1), x2 = __ldg(x + 3 * c + 2);
-    y0 += __ldg(v + 0 * 32) * x0 + __ldg(v + 1 * 32) * x1 + __ldg(v + 2 * 32) * x2;
-    y1 += __ldg(v + 3 * 32) * x0 + __ldg(v + 4 * 32) * x1 + __ldg(v + 5 * 32) * x2;
-    y2 += __ldg(v + 6 * 32) * x0 + __ldg(v + 7 * 32) * x1 + __ldg(v + 8 * 32) * x2;
-  }
-  y3[0] = y0; y3[1] = y1; y3[2] = y2;
-}
-
-__global__ void __launch_bounds__(kSpmvThreads) k_bsr_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
-                                                           const int* __restrict__ col, const double* __restrict__ val,
-                                                           const double* __restrict__ x, double* __restrict__ y) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n_rows) return;
-  double y3[3];
-  sell_row(row, slice_ptr, col, val, x, y3);
-  y[3 * row] = y3[0]; y[3 * row + 1] = y3[1]; y[3 * row + 2] = y3[2];
 }
 
 // One warp per (32-row slice, output component): 3x the threads of a
@@ -225,43 +197,98 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n_rows, const doub
   }
 }
 
-template <class V>
-__global__ void __launch_bounds__(96) k_pcg_dir_spmv(int n_rows, const int64_t* __restrict__ slice_ptr,
-                                                              const int* __restrict__ col,
-                                                              const V* __restrict__ val,
-                                                              const double* __restrict__ dinv,
-                                                              const double* __restrict__ r, double* p0, double* p1,
-                                                              double* __restrict__ q, double* __restrict__ partial,
-                                                              PcgState* st) {
-  // one CTA = one 32-row slice; warp c computes output component c
+// The loop's direction + SpMV kernel: p_new = dinv.r + beta p_old (formed for
+// gathered columns, written for own rows), q = K p_new, partial p.q -> last
+// block: alpha = z.r / p.q (breakdown check). A CTA is one 32-row slice, a
+// thread owns the 3 components of its row, so every slot streams 9 coalesced
+// 256-byte value lines per warp and the gathered p is formed once per column
+// (not once per output component). A CTA takes kS slices; a slice's slots are
+// dealt round-robin to kW warps (kW = 4 for small matrices, to keep enough
+// warps in flight; 1 for large ones) and the warp sums meet in shared memory
+// in fixed order. Slots are taken in groups
+// whose value loads are all issued before use (144 bytes in flight per
+// thread); values of matrices too large for L2 stream with evict-first loads
+// so the vectors stay in L2 (smaller ones stay in L2 across iterations);
+// padded positions (column -1) hold zero values and skip the gather.
+template <class V, int kS, int kSpmvWarps, bool kStream>
+__global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int n_rows, int n_slices,
+                                                                      const int64_t* __restrict__ slice_ptr,
+                                                                      const int* __restrict__ col,
+                                                                      const V* __restrict__ val,
+                                                                      const double* __restrict__ dinv,
+                                                                      const double* __restrict__ r, double* p0,
+                                                                      double* p1, double* __restrict__ q,
+                                                                      double* __restrict__ partial, PcgState* st) {
   __shared__ double sh[32];
+  __shared__ double ys[kS][kSpmvWarps][3][32];
   if (st->done) return;
   const int it = st->it;
   const double beta = st->beta;
   const double* __restrict__ pold = (it & 1) ? p1 : p0;
   double* __restrict__ pnew = (it & 1) ? p0 : p1;
-  const int slice = blockIdx.x, c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sl = warp / kSpmvWarps, w = warp % kSpmvWarps;
+  const int slice = blockIdx.x * kS + sl;
   const int row = slice * 32 + lane;
-  double pq = 0;
-  if (row < n_rows) {
+  const bool live = slice < n_slices && row < n_rows;
+  double y0 = 0, y1 = 0, y2 = 0;
+  auto fma9 = [&](const double (&a)[9], int cc) {
+    if (cc < 0) return;  // padding (its values are zero)
+    const double x0 = dinv[3 * cc] * r[3 * cc] + beta * pold[3 * cc];
+    const double x1 = dinv[3 * cc + 1] * r[3 * cc + 1] + beta * pold[3 * cc + 1];
+    const double x2 = dinv[3 * cc + 2] * r[3 * cc + 2] + beta * pold[3 * cc + 2];
+    y0 += a[0] * x0 + a[1] * x1 + a[2] * x2;
+    y1 += a[3] * x0 + a[4] * x1 + a[5] * x2;
+    y2 += a[6] * x0 + a[7] * x1 + a[8] * x2;
+  };
+  if (live) {
     const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
-    double yc = 0;
-    for (int64_t s = s0; s < s1; ++s) {
-      const int cc = __ldg(col + s * 32 + lane);
-      if (cc < 0) break;
-      const V* v = val + (s * 9 + 3 * c) * 32 + lane;
-      const double x0 = dinv[3 * cc] * r[3 * cc] + beta * pold[3 * cc];
-      const double x1 = dinv[3 * cc + 1] * r[3 * cc + 1] + beta * pold[3 * cc + 1];
-      const double x2 = dinv[3 * cc + 2] * r[3 * cc + 2] + beta * pold[3 * cc + 2];
-      yc += (double)__ldg(v) * x0 + (double)__ldg(v + 32) * x1 + (double)__ldg(v + 64) * x2;
+    constexpr int U = 16 / (int)sizeof(V);  // 2 FP64 / 4 FP32 slots per group
+    int64_t s = s0 + w;
+    for (; s + (U - 1) * kSpmvWarps < s1; s += U * kSpmvWarps) {
+      int cu[U];
+      double a[U][9];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t su = s + u * kSpmvWarps;
+        cu[u] = __ldg(col + su * 32 + lane);
+        const V* vu = val + su * 9 * 32 + lane;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a[u][k] = (double)(kStream ? __ldcs(vu + k * 32) : __ldg(vu + k * 32));
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) fma9(a[u], cu[u]);
     }
-    const double pn = dinv[3 * row + c] * r[3 * row + c] + beta * pold[3 * row + c];
-    pnew[3 * row + c] = pn;
-    q[3 * row + c] = yc;
-    pq = pn * yc;
+    for (; s < s1; s += kSpmvWarps) {
+      const int c0 = __ldg(col + s * 32 + lane);
+      const V* v0 = val + s * 9 * 32 + lane;
+      double a0[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a0[k] = (double)(kStream ? __ldcs(v0 + k * 32) : __ldg(v0 + k * 32));
+      fma9(a0, c0);
+    }
   }
-  const double s = block_sum(pq, sh);
-  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  ys[sl][w][0][lane] = y0;
+  ys[sl][w][1][lane] = y1;
+  ys[sl][w][2][lane] = y2;
+  __syncthreads();
+  double pq = 0;
+  if (w == 0 && live) {
+    double yc[3], pn[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double t = ys[sl][0][c][lane];
+#pragma unroll
+      for (int ww = 1; ww < kSpmvWarps; ++ww) t += ys[sl][ww][c][lane];
+      yc[c] = t;
+      pn[c] = dinv[3 * row + c] * r[3 * row + c] + beta * pold[3 * row + c];
+      pnew[3 * row + c] = pn[c];
+      q[3 * row + c] = t;
+    }
+    pq = pn[0] * yc[0] + pn[1] * yc[1] + pn[2] * yc[2];
+  }
+  const double bs = block_sum(pq, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
   if (!last_block(&st->counter)) return;
   const double t = sum_partials(partial, gridDim.x, 1, 0, sh);
   if (threadIdx.x == 0) {
@@ -419,6 +446,39 @@ int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* 
   return MSG_OK;
 }
 
+// The loop's SpMV launch (shape chosen by size and value precision).
+static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float* v32, bool mixed, double* dv,
+                                double* rv, double* p0, double* p1, double* qv, double* pa, PcgState* st,
+                                cudaStream_t stream) {
+  const int nr = m->n_nodes;
+  const int ns = m->pat.n_slices;
+  const bool small = ns < ctx->sm_count * 32;  // fewer slices than 32 warps per SM: 4 warps per slice
+  const int64_t* sp = m->d_slice_ptr.as<int64_t>();
+  const int* cl = m->d_col.as<int>();
+  const int gs = ns, gl = (ns + 7) / 8;
+  // FP64 values stream through with evict-first loads (measured faster at every
+  // size); FP32 values of matrices up to ~60 % of L2 stay there across iterations
+  const size_t vbytes = (size_t)m->pat.n_slots * 32 * 9 * (mixed ? 4 : 8);
+  const bool strm = !mixed || vbytes > (size_t)76 << 20;
+#define MSG_SPMV(V, S, W, STREAM, grid, vals)                                                                       \
+  k_pcg_dir_spmv_rows<V, S, W, STREAM><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, vals, dv, rv, p0, p1, qv, pa, \
+                                                                        st)
+  if (mixed) {
+    if (small) {
+      if (strm) MSG_SPMV(float, 1, 4, true, gs, v32); else MSG_SPMV(float, 1, 4, false, gs, v32);
+    } else {
+      if (strm) MSG_SPMV(float, 8, 1, true, gl, v32); else MSG_SPMV(float, 8, 1, false, gl, v32);
+    }
+  } else {
+    if (small) {
+      if (strm) MSG_SPMV(double, 1, 4, true, gs, v64); else MSG_SPMV(double, 1, 4, false, gs, v64);
+    } else {
+      if (strm) MSG_SPMV(double, 8, 1, true, gl, v64); else MSG_SPMV(double, 8, 1, false, gl, v64);
+    }
+  }
+#undef MSG_SPMV
+}
+
 // Runs the device PCG on node-layout vectors. The loop body (2 kernels) is
 // captured once per matrix as a CUDA graph of `chunk` iterations; the host
 // launches the graph and reads back the state flags after each chunk.
@@ -451,7 +511,6 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
   }
   PcgState* st = A->d_state.as<PcgState>();
   const int grid_v = std::min(4096, std::max(1, std::min((n + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 8)));
-  const int grid_s = m->pat.n_slices;  // 96-thread CTAs, one 32-row slice each
 
   k_pcg_init<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, d_b, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
                                                       A->d_p0.as<double>(), A->d_p1.as<double>(),
@@ -473,16 +532,9 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
-      if (mixed)
-        k_pcg_dir_spmv<float><<<grid_s, 96, 0, ctx->stream>>>(
-            nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val32.as<float>(), A->d_dinv.as<double>(),
-            A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
-            A->d_partial.as<double>(), st);
-      else
-        k_pcg_dir_spmv<double><<<grid_s, 96, 0, ctx->stream>>>(
-            nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(), A->d_val.as<double>(), A->d_dinv.as<double>(),
-            A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
-            A->d_partial.as<double>(), st);
+      launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), mixed ? A->d_val32.as<float>() : nullptr, mixed,
+                          A->d_dinv.as<double>(), A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(),
+                          A->d_q.as<double>(), A->d_partial.as<double>(), st, ctx->stream);
       k_pcg_update<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
                                                             A->d_p0.as<double>(), A->d_p1.as<double>(),
                                                             A->d_q.as<double>(), A->d_partial.as<double>(), st);
@@ -599,7 +651,6 @@ extern "C" int MSG_PCG_SOLVE_NOALLOC(MSG_MAT A, const double* b_dev, double* x_d
   MSG_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(PcgState), s));
   MSG_TRY(launch_dof_to_node(ctx, m, b_dev, bn, 1, 0, 0));
   const int grid_v = std::min(4096, std::max(1, std::min((int)((n + kPcgThreads - 1) / kPcgThreads), ctx->sm_count * 8)));
-  const int grid_s = m->pat.n_slices;
   k_pcg_init<<<grid_v, kPcgThreads, 0, s>>>(nr, bn, A->d_dinv.as<double>(), r, xn, p0, p1, partial, st);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &tol, sizeof(double), cudaMemcpyHostToDevice, s));
@@ -607,8 +658,8 @@ extern "C" int MSG_PCG_SOLVE_NOALLOC(MSG_MAT A, const double* b_dev, double* x_d
   int done = 0;
   for (int it = 0; it < max_it + 8 && !done; it += 8) {
     for (int k = 0; k < 8; ++k) {
-      k_pcg_dir_spmv<<<grid_s, 96, 0, s>>>(nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
-                                           A->d_val.as<double>(), A->d_dinv.as<double>(), r, p0, p1, q, partial, st);
+      launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), nullptr, false, A->d_dinv.as<double>(), r, p0, p1, q,
+                          partial, st, s);
       k_pcg_update<<<grid_v, kPcgThreads, 0, s>>>(nr, A->d_dinv.as<double>(), r, xn, p0, p1, q, partial, st);
     }
     count_launch(ctx, 16);

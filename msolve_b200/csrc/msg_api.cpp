@@ -63,6 +63,10 @@ Matrix::~Matrix() {
 }
 
 Context::~Context() {
+  delete static_cast<msg_matrix*>(mc_matrix);
+  delete mc_ke;
+  delete mc_st;
+  delete mc_E;
   for (auto& w : work) {
     delete w;
     w = nullptr;
@@ -109,6 +113,10 @@ void release(Mesh* m) {
       std::lock_guard<std::recursive_mutex> lk(ctx->mu);
       cudaSetDevice(ctx->device);
       cudaStreamSynchronize(ctx->stream);
+      if (ctx->mc_matrix && ctx->mc_matrix->mesh == m) {
+        delete static_cast<msg_matrix*>(ctx->mc_matrix);
+        ctx->mc_matrix = nullptr;
+      }
       delete static_cast<msg_mesh*>(m);
     }
     release(ctx);
@@ -421,32 +429,47 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
     status = block_mixed_solve(ctx, m, nu, &kd, d_xi, R, Rp, d_b, max_it, tol, tip_dof, d_X, o);
     if (tip) std::copy(htip.begin(), htip.end(), tip);
   } else if (mode == MSG_MODE_FP64_BSR) {
-    DevMem E64re, ke, st, bnode, xnode, tipd;
-    MSG_TRY(E64re.alloc(ctx, sizeof(double) * (size_t)m->n_elems * R));
-    MSG_TRY(launch_kl_field(ctx, m, &kd, R, Rp, d_xi, nullptr, nullptr, E64re.as<double>()));
-    std::unique_ptr<msg_matrix> A(new msg_matrix());
-    A->mesh = m;
-    MSG_TRY(bnode.alloc(ctx, sizeof(double) * 3 * (size_t)m->n_nodes));
-    MSG_TRY(xnode.alloc(ctx, sizeof(double) * 3 * (size_t)m->n_nodes));
-    MSG_CUDA(ctx, cudaMemsetAsync(bnode.ptr, 0, sizeof(double) * 3 * (size_t)m->n_nodes, ctx->stream));
-    MSG_TRY(launch_dof_to_node(ctx, m, d_b, bnode.as<double>(), 1, 0, 0));
-    DevMem xdof;
-    MSG_TRY(xdof.alloc(ctx, sizeof(double) * (size_t)std::max(1, m->n_dofs)));
+    // the assembled matrix and its buffers stay in the context for the next call on this mesh
+    if (ctx->mc_matrix && ctx->mc_matrix->mesh != m) {
+      delete static_cast<msg_matrix*>(ctx->mc_matrix);
+      ctx->mc_matrix = nullptr;
+    }
+    if (!ctx->mc_matrix) {
+      ctx->mc_matrix = new msg_matrix();
+      ctx->mc_matrix->mesh = m;  // weak: release(Mesh*) drops this matrix with its mesh
+    }
+    if (!ctx->mc_ke) ctx->mc_ke = new DevMem();
+    if (!ctx->mc_st) ctx->mc_st = new DevMem();
+    if (!ctx->mc_E) ctx->mc_E = new DevMem();
+    Matrix* A = ctx->mc_matrix;
+    const size_t eb = sizeof(double) * (size_t)m->n_elems * R;
+    if (ctx->mc_E->bytes < eb) {
+      ctx->mc_E->release();
+      MSG_TRY(ctx->mc_E->alloc(ctx, eb));
+    }
+    MSG_TRY(launch_kl_field(ctx, m, &kd, R, Rp, d_xi, nullptr, nullptr, ctx->mc_E->as<double>()));
+    const size_t n3 = 3 * (size_t)m->n_nodes;
+    if (!A->d_bn.ptr) {
+      MSG_TRY(A->d_bd.alloc(ctx, sizeof(double) * std::max(1, m->n_dofs)));
+      MSG_TRY(A->d_bn.alloc(ctx, sizeof(double) * n3));
+      MSG_TRY(A->d_xn.alloc(ctx, sizeof(double) * n3));
+    }
+    MSG_CUDA(ctx, cudaMemsetAsync(A->d_bn.ptr, 0, sizeof(double) * n3, ctx->stream));
+    MSG_TRY(launch_dof_to_node(ctx, m, d_b, A->d_bn.as<double>(), 1, 0, 0));
     for (int r = 0; r < R; ++r) {
-      int neg = 0;
-      MSG_TRY(assemble_from_device_E(ctx, m, E64re.as<double>() + (size_t)r * m->n_elems, nu, A.get(), ke, st, nullptr));
+      MSG_TRY(assemble_from_device_E(ctx, m, ctx->mc_E->as<double>() + (size_t)r * m->n_elems, nu, A, *ctx->mc_ke,
+                                     *ctx->mc_st, nullptr));
       int its = 0, pst = 0;
       double rr = 0;
-      MSG_TRY(pcg_solve_device(ctx, A.get(), bnode.as<double>(), xnode.as<double>(), max_it, tol, &its, &rr, &pst));
-      double* xout = d_X ? d_X + (size_t)r * m->n_dofs : xdof.as<double>();
-      MSG_TRY(launch_node_to_dof(ctx, m, xnode.as<double>(), xout, 1, 0, 0));
+      MSG_TRY(pcg_solve_device(ctx, A, A->d_bn.as<double>(), A->d_xn.as<double>(), max_it, tol, &its, &rr, &pst));
+      double* xout = d_X ? d_X + (size_t)r * m->n_dofs : A->d_bd.as<double>();
+      MSG_TRY(launch_node_to_dof(ctx, m, A->d_xn.as<double>(), xout, 1, 0, 0));
       if (tip && tip_dof >= 0) {
         MSG_CUDA(ctx, cudaMemcpyAsync(tip + r, xout + tip_dof, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
       }
       if (iterations) iterations[r] = its + (pst == MSG_OK ? 1 : 0);  // matrix products
       if (rel_res) rel_res[r] = rr;
       if (pst != MSG_OK && status == MSG_OK) status = pst;
-      (void)neg;
     }
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (status != MSG_OK) set_error(ctx, status, "FP64 batch: a realization did not converge");

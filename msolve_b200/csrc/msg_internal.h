@@ -78,6 +78,12 @@ struct Context {
   cudaGraphExec_t batch_graph = nullptr;  // inner-loop graph of the last batch configuration
   size_t batch_graph_key = 0;
   void* server = nullptr;  // serving worker and lanes (serve.cpp), nullptr until MSG_SERVE_START
+  // FP64 Monte Carlo drop-in: the assembled matrix, its element-matrix scratch and
+  // staging kept across calls for one mesh (weak: dropped when that mesh is freed)
+  struct Matrix* mc_matrix = nullptr;
+  DevMem* mc_ke = nullptr;
+  DevMem* mc_st = nullptr;
+  DevMem* mc_E = nullptr;
   ~Context();
 };
 
