@@ -41,9 +41,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p99 latency"
-# DRAM traffic of one k_op_modal launch per realization on the 32^3 lattice (ncu capture
-# at R = 512, dram__bytes_read.sum + dram__bytes_write.sum divided by 512); None until measured
-OP_DRAM_BYTES_PER_REALIZATION = None
+# DRAM traffic of one k_op_modal launch per realization on the 32^3 lattice: ncu capture
+# at R = 512 (dram__bytes_read.sum 1,165.9 MB + dram__bytes_write.sum 845.5 MB) / 512
+OP_DRAM_BYTES_PER_REALIZATION = (1165.921e6 + 845.472e6) / 512
 
 
 def parse():
@@ -68,6 +68,8 @@ def parse():
     p.add_argument("--no-serving", action="store_true", help="skip the serving (continuous batching) measurement")
     p.add_argument("--no-single", action="store_true", help="skip the 64^3 single-solve measurement")
     p.add_argument("--single-n", type=int, default=64)
+    p.add_argument("--single-only", action="store_true",
+                   help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
     p.add_argument("--serve-rates", default="100,400", help="Poisson arrival rates (requests/s) to run")
     p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
@@ -338,6 +340,9 @@ def main():
     from msolve_b200 import _native as N
 
     ctx = M.Context(local)
+    if args.single_only:
+        print(json.dumps(single_leg(args, ctx)))
+        return
     if args.reliable_delta is not None:
         ctx.set_option("reliable_delta", args.reliable_delta)
     if args.chunk is not None:
