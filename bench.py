@@ -72,6 +72,8 @@ def parse():
                    help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
     p.add_argument("--serve-rates", default="100,400", help="Poisson arrival rates (requests/s) to run")
     p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
+    p.add_argument("--multigrid", type=int, default=None, choices=[0, 1],
+                   help="MSG_SET_OPTION multigrid (1: V-cycle preconditioned batched loop)")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
@@ -349,6 +351,8 @@ def main():
         ctx.set_option("chunk", args.chunk)
     if args.modal_operator is not None:
         ctx.set_option("modal_operator", args.modal_operator)
+    if args.multigrid is not None:
+        ctx.set_option("multigrid", args.multigrid)
     model, kl = make_problem(args)
     mesh = M.GpuMesh(ctx, model)
     R, K_terms = args.R, args.terms

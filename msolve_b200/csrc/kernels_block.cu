@@ -803,6 +803,346 @@ __global__ void __launch_bounds__(kMThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------- multigrid level operator
+// The Walsh-mode operator of one lattice level (same tiling, TMA ring,
+// exchange buffer and bounded waits as k_op_modal), with the node phase of one
+// step of the multigrid-preconditioned loop:
+//   kLvlStart : level 0, first step of an iteration. Corner input
+//               x0 = omega dinv (r - alpha q) (the first Jacobi sweep from zero
+//               on the updated residual); the owner writes r' = r - alpha q
+//               (out2) and x0 (out3); out = r' - A x0; partial r'.r'.
+//   kLvlResid : out = b - A u.
+//   kLvlSmooth: out = u + omega dinv (b - A u) (damped Jacobi sweep); partial
+//               out.b when partial is given.
+//   kLvlPcgZ  : level 0, search direction. Corner input p = z + beta p_old;
+//               the owner writes p (out2) and d += alpha p_old; out = A p;
+//               partial p.(A p).
+// Every output is masked (constrained components 0). Per-realization partials
+// are summed in a fixed order (node pencil, then plane), so they do not depend
+// on the batch.
+enum { kLvlStart = 0, kLvlResid = 1, kLvlSmooth = 2, kLvlPcgZ = 3 };
+template <int kMode> struct LvlStage {
+  static constexpr bool kTwo = kMode == kLvlStart || kMode == kLvlPcgZ;  // two vector patches
+  static constexpr int kOffA = 0;              // r (start), z (direction) or u
+  static constexpr int kOffB = kMPlaneFloats;  // q (start) or p_old (direction)
+  static constexpr int kOffN = (kTwo ? 2 : 1) * kMPlaneFloats;                 // dinv patch (start)
+  static constexpr int kOffE = kOffN + (kMode == kLvlStart ? kMNodeFloats : 0);
+  static constexpr int kOffD = kOffE + kMEFloats;                              // d of the tile (direction)
+  static constexpr int kFloats = kOffD + (kMode == kLvlPcgZ ? kMDFloats : 0);
+  static constexpr uint32_t kBytes = kFloats * 4;
+  static constexpr size_t kSmem = 128 + sizeof(float) * ((size_t)kMStages * kFloats + 2 * (size_t)kMXFloats) +
+                                  sizeof(double) * kMJ * kMK * 32 + sizeof(uint64_t) * (2 * kMStages);
+};
+static_assert(LvlStage<kLvlStart>::kBytes % 128 == 0 && LvlStage<kLvlResid>::kBytes % 128 == 0 &&
+                  LvlStage<kLvlPcgZ>::kBytes % 128 == 0,
+              "stage alignment");
+static_assert(LvlStage<kLvlPcgZ>::kSmem <= 227 * 1024 && LvlStage<kLvlStart>::kSmem <= 227 * 1024, "level smem");
+
+template <int kMode, bool kMass>
+__global__ void __launch_bounds__(kMThreads, 1)
+    k_lvl_op(Lattice L, const __grid_constant__ ModalC C, const __grid_constant__ CUtensorMap tm_a,
+             const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_n,
+             const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_d, int tiles_j,
+             int n_tiles, int n_items, const uint8_t* __restrict__ mask, const float* __restrict__ b,
+             const float* __restrict__ dinv, float omega, const float* __restrict__ alpha,
+             const float* __restrict__ beta, float* __restrict__ out, float* __restrict__ out2,
+             float* __restrict__ out3, float* __restrict__ d, double* __restrict__ partial, int pstride,
+             int* __restrict__ err) {
+  using S = LvlStage<kMode>;
+  extern __shared__ __align__(128) float smem_dyn[];
+  float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
+  float* xbuf = smem + kMStages * S::kFloats;
+  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);  // [node pencils][32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + kMJ * kMK * 32);
+  uint64_t* empty = full + kMStages;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int NX = L.NX, Rp = L.Rp;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kMStages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kMWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (w == kMWarps) {
+    if (lane == 0) {
+      uint32_t seq = 0;
+      for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+        const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
+        for (int P = 1; P <= NX; ++P, ++seq) {
+          const int st = seq % kMStages;
+          const uint32_t use = seq / kMStages;
+          if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+            atomicExch(err, 1);
+            return;
+          }
+          float* dst = smem + st * S::kFloats;
+          mbar_expect_tx(&full[st], S::kBytes);
+          tma_load_5d(dst + S::kOffA, &tm_a, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          if constexpr (S::kTwo) tma_load_5d(dst + S::kOffB, &tm_b, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          if constexpr (kMode == kLvlStart) tma_load_4d(dst + S::kOffN, &tm_n, g32, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_4d(dst + S::kOffE, &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+          if constexpr (kMode == kLvlPcgZ) tma_load_5d(dst + S::kOffD, &tm_d, g32, 0, P, J0, K0, &full[st]);
+        }
+      }
+    }
+    return;
+  }
+  const int ej = w % kMEJ, ek = w / kMEJ;
+  const bool node_warp = ej >= 1 && ek >= 1;
+  uint32_t seq = 0;
+  int xsel = 0;
+  bool dead = false;
+  auto csync = [&]() { asm volatile("bar.sync 1, %0;" ::"r"(kMWarps * 32) : "memory"); };
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+    const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
+    const int Je = J0 - 1 + ej, Ke = K0 - 1 + ek;
+    auto realj = [&](int j) { return j >= 1 && j <= L.NY - 1; };
+    auto realk = [&](int k) { return k >= 1 && k <= L.NZ - 1; };
+    const bool real = realj(Je) && realk(Ke);
+    const bool node_ok = node_warp && Je <= L.NY && Ke <= L.NZ;
+    const bool r00 = real, r10 = realj(Je - 1) && realk(Ke);
+    const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
+    const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;
+    const int rr = g32 + lane;
+    float al = 0.f, be = 0.f;
+    if constexpr (kMode == kLvlStart || kMode == kLvlPcgZ) al = alpha[rr];
+    if constexpr (kMode == kLvlPcgZ) be = beta[rr];
+    float Bp[3][4], T0[3][4];
+    float ou[3] = {0.f, 0.f, 0.f}, orc[3] = {0.f, 0.f, 0.f};  // corner input and r' at the own node, last plane
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) T0[c][qq] = 0.f;
+    double acc = 0.0;
+    uint32_t mreg = 0;
+    auto node_phase = [&](int X) {
+      if (((X - 1) & 31) == 0) {
+        const int pl = X + lane;
+        mreg = (pl <= NX) ? mask[nrow + pl] : 0u;
+      }
+      const uint32_t mk = __shfl_sync(0xffffffffu, mreg, (X - 1) & 31);
+      const float* xb = xbuf + xsel * kMXFloats;
+      const size_t node = nrow + X;
+      float wdv = 0.f;
+      if constexpr (kMode == kLvlSmooth) wdv = omega * dinv[node * Rp + rr];
+      double sacc = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float y = 0.f;
+        if (r00) y += xb[((w * 4 + 0) * 3 + c) * 32 + lane];
+        if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
+        if (r01) y += xb[(((w - kMEJ) * 4 + 2) * 3 + c) * 32 + lane];
+        if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        const size_t o = (node * 3 + c) * Rp + rr;
+        const bool fixed = (mk >> c) & 1;
+        float v;
+        if constexpr (kMode == kLvlStart) {
+          v = fixed ? 0.f : orc[c] - y;
+          sacc = fma((double)orc[c], (double)orc[c], sacc);
+        } else if constexpr (kMode == kLvlResid) {
+          v = fixed ? 0.f : b[o] - y;
+        } else if constexpr (kMode == kLvlSmooth) {
+          const float bv = b[o];
+          v = fixed ? 0.f : fmaf(wdv, bv - y, ou[c]);
+          sacc = fma((double)v, (double)bv, sacc);
+        } else {
+          v = fixed ? 0.f : y;
+          sacc = fma((double)ou[c], (double)v, sacc);
+        }
+        out[o] = v;
+      }
+      acc += sacc;
+    };
+    auto emit_corners = [&](const float (&B)[3][4]) {
+      float y[2][2][3];
+      yz_inverse(B, y);
+      float* xb = xbuf + xsel * kMXFloats;
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
+    };
+    for (int P = 1; P <= NX; ++P, ++seq) {
+      const int st = seq % kMStages;
+      if (!dead && !mbar_wait(&full[st], (seq / kMStages) & 1)) {
+        atomicExch(err, 1);
+        dead = true;
+      }
+      const float* pt = smem + st * S::kFloats;
+      float u[2][2][3], rc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az) {
+          const int o = (ek + az) * kMPJ + (ej + ay);
+          float wdv = 0.f;
+          if constexpr (kMode == kLvlStart) wdv = omega * pt[S::kOffN + o * 32 + lane];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int i = (o * 3 + c) * 32 + lane;
+            if constexpr (kMode == kLvlStart) {
+              const float rn = fmaf(-al, pt[S::kOffB + i], pt[S::kOffA + i]);
+              u[ay][az][c] = wdv * rn;
+              if (ay == 0 && az == 0) rc[c] = rn;
+            } else if constexpr (kMode == kLvlPcgZ) {
+              u[ay][az][c] = fmaf(be, pt[S::kOffB + i], pt[S::kOffA + i]);
+            } else {
+              u[ay][az][c] = pt[S::kOffA + i];
+            }
+          }
+        }
+      const float E = pt[S::kOffE + w * 32 + lane];
+      if constexpr (kMode == kLvlStart || kMode == kLvlPcgZ) {
+        if (node_ok) {
+          const size_t node = nrow + P;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const size_t o = (node * 3 + c) * Rp + rr;
+            if constexpr (kMode == kLvlStart) {
+              out2[o] = rc[c];
+              out3[o] = u[0][0][c];
+            } else {
+              const int op = ek * kMPJ + ej, od = (ek - 1) * kMJ + (ej - 1);
+              const float pold = pt[S::kOffB + (op * 3 + c) * 32 + lane];
+              out2[o] = u[0][0][c];
+              d[o] = fmaf(al, pold, pt[S::kOffD + (od * 3 + c) * 32 + lane]);
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      float Bc[3][4];
+      yz_forward(u, Bc);
+      if (P >= 2) {
+        if (real) {
+          float C1[3][4];
+          modal_apply<kMass>(C, E, Bp, Bc, T0, C1);
+          emit_corners(T0);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
+        }
+        csync();
+        if (node_ok) node_phase(P - 1);
+        xsel ^= 1;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ou[c] = u[0][0][c];
+        orc[c] = rc[c];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) Bp[c][qq] = Bc[c][qq];
+      }
+    }
+    if (real) emit_corners(T0);
+    csync();
+    if (node_ok) node_phase(NX);
+    xsel ^= 1;
+    if (kMode != kLvlResid && partial != nullptr) {
+      if (node_warp) red[((ek - 1) * kMJ + (ej - 1)) * 32 + lane] = acc;
+      csync();
+      if (w == 0) {
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < kMJ * kMK; ++i) sum += red[i * 32 + lane];
+        partial[((size_t)tile * Rp + rr) * pstride] = sum;
+      }
+    }
+  }
+}
+
+// Full-weighting restriction b_c = P^T t_f (P: trilinear prolongation), masked
+// at the coarse level, and x_c = omega dinv_c b_c (the first Jacobi sweep from
+// zero). Coarse node (I, J, K) (padded) sits on fine node (2I-1, 2J-1, 2K-1);
+// the fine ghost layer is zero. One CTA per coarse interior node.
+__global__ void __launch_bounds__(128) k_restrict(Lattice Lf, Lattice Lc, const int* __restrict__ interior_c,
+                                                  const uint8_t* __restrict__ mask_c, const float* __restrict__ tf,
+                                                  const float* __restrict__ dinv_c, float omega,
+                                                  float* __restrict__ bc, float* __restrict__ xc) {
+  const size_t nc = (size_t)interior_c[blockIdx.x];
+  const int I = (int)(nc % Lc.NXp), J = (int)((nc / Lc.NXp) % Lc.NYp), K = (int)(nc / ((size_t)Lc.NXp * Lc.NYp));
+  const size_t sy = (size_t)Lf.NXp, sz = (size_t)Lf.NXp * Lf.NYp;
+  const size_t fc = (size_t)(2 * I - 1) + sy * (2 * J - 1) + sz * (2 * K - 1);
+  const uint32_t mk = mask_c[nc];
+  const int Rp = Lf.Rp;
+  for (int rr = threadIdx.x; rr < Rp; rr += blockDim.x) {
+    const float wdv = omega * dinv_c[nc * Rp + rr];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float s = 0.f;
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+          for (int dx = -1; dx <= 1; ++dx) {
+            const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+            const size_t f = fc + dx + dy * sy + dz * sz;
+            s = fmaf(wgt, tf[(f * 3 + c) * Rp + rr], s);
+          }
+      s = ((mk >> c) & 1) ? 0.f : s;
+      bc[(nc * 3 + c) * Rp + rr] = s;
+      xc[(nc * 3 + c) * Rp + rr] = wdv * s;
+    }
+  }
+}
+
+// x_f += P x_c: trilinear prolongation of the coarse correction (fine node
+// with even coordinate: the coincident coarse node; odd: the mean of the two
+// neighbours, per axis), masked at the fine level. One CTA per fine interior node.
+__global__ void __launch_bounds__(128) k_prolong_add(Lattice Lf, Lattice Lc, const int* __restrict__ interior_f,
+                                                     const uint8_t* __restrict__ mask_f,
+                                                     const float* __restrict__ xc, float* __restrict__ xf) {
+  const size_t nf = (size_t)interior_f[blockIdx.x];
+  const int gi = (int)(nf % Lf.NXp) - 1, gj = (int)((nf / Lf.NXp) % Lf.NYp) - 1;
+  const int gk = (int)(nf / ((size_t)Lf.NXp * Lf.NYp)) - 1;
+  const size_t sy = (size_t)Lc.NXp, sz = (size_t)Lc.NXp * Lc.NYp;
+  const size_t c0 = (size_t)((gi >> 1) + 1) + sy * ((gj >> 1) + 1) + sz * ((gk >> 1) + 1);
+  const int ni = (gi & 1) + 1, nj = (gj & 1) + 1, nk = (gk & 1) + 1;
+  const float wgt = ((gi & 1) ? 0.5f : 1.f) * ((gj & 1) ? 0.5f : 1.f) * ((gk & 1) ? 0.5f : 1.f);
+  const uint32_t mk = mask_f[nf];
+  const int Rp = Lf.Rp;
+  for (int rr = threadIdx.x; rr < Rp; rr += blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if ((mk >> c) & 1) continue;
+      float s = 0.f;
+      for (int a = 0; a < nk; ++a)
+        for (int bb = 0; bb < nj; ++bb)
+          for (int e = 0; e < ni; ++e) s += xc[((c0 + e + bb * sy + a * sz) * 3 + c) * Rp + rr];
+      const size_t o = (nf * 3 + c) * Rp + rr;
+      xf[o] = fmaf(wgt, s, xf[o]);
+    }
+  }
+}
+
+// Coarse element field: the mean of the 8 fine elements it covers (elements
+// are stored at their lower-corner padded node). One CTA per coarse element.
+__global__ void __launch_bounds__(128) k_coarsen_E(Lattice Lf, Lattice Lc, int nxc, int nyc,
+                                                   const float* __restrict__ Ef, float* __restrict__ Ec) {
+  const int e = blockIdx.x;
+  const int I = e % nxc + 1, J = (e / nxc) % nyc + 1, K = e / (nxc * nyc) + 1;
+  const size_t nc = (size_t)I + (size_t)Lc.NXp * (J + (size_t)Lc.NYp * K);
+  const size_t sy = (size_t)Lf.NXp, sz = (size_t)Lf.NXp * Lf.NYp;
+  const size_t f0 = (size_t)(2 * I - 1) + sy * (2 * J - 1) + sz * (2 * K - 1);
+  const int Rp = Lf.Rp;
+  for (int rr = threadIdx.x; rr < Rp; rr += blockDim.x) {
+    double s = 0.0;
+    for (int a = 0; a < 2; ++a)
+      for (int bb = 0; bb < 2; ++bb)
+        for (int c = 0; c < 2; ++c) s += (double)Ef[(f0 + c + bb * sy + a * sz) * Rp + rr];
+    Ec[nc * Rp + rr] = (float)(0.125 * s);
+  }
+}
+
 // FP64 true residual: r = b - A x (masked), r32 = (float) r; partials ||r||^2
 // and (dinv r32).r32. A = E Khat (+ Mhat on real elements when kMass); b is
 // one vector for the batch (b[node*3 + c]) or, with kBPerR, one per
@@ -1126,7 +1466,9 @@ __global__ void __launch_bounds__(1024) k_beta(int Rp, int n_blk, const double* 
 
 // After a true-residual replacement: convergence test, new reference norm and
 // the search-direction coefficient beta = gamma_new / gamma_prev (first call:
-// beta = 0, p starts from z).
+// beta = 0, p starts from z). gamma_ref: 0 two-reduction Jacobi loop (reference
+// norm r.r), 1 single-reduction loop ((dinv r).r), 2 multigrid loop (r.r; beta
+// is left to k_gmg_beta).
 __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, const double* __restrict__ partial,
                                                         Scal s, double tol, int first, int gamma_ref, int max_it) {
   double v[2];
@@ -1144,9 +1486,15 @@ __global__ void __launch_bounds__(1024) k_resid_scalars(int Rp, int n_tiles, con
     if (!s.done[r] && !s.breakdown[r] && s.its[r] >= max_it) s.breakdown[r] = 2;
     const int a = (s.done[r] || s.breakdown[r]) ? 0 : 1;
     s.act[r] = a;
-    s.beta[r] = (a && !fr && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
-    s.gamma[r] = g;
-    s.rho_ref[r] = gamma_ref ? g : rr;
+    if (gamma_ref == 2) {
+      // multigrid loop: beta follows from the next preconditioned residual
+      // (k_gmg_beta); a fresh system starts its direction from z
+      if (fr) s.gamma_prev[r] = 0.0;
+    } else {
+      s.beta[r] = (a && !fr && s.gamma_prev[r] > 0) ? (float)(g / s.gamma_prev[r]) : 0.f;
+      s.gamma[r] = g;
+    }
+    s.rho_ref[r] = gamma_ref == 1 ? g : rr;
     s.alpha[r] = 0.f;  // the pending alpha p term was folded into x (and no r update is pending)
     active = a;
   }
@@ -1198,6 +1546,70 @@ __global__ void __launch_bounds__(1024) k_alpha_gamma(int Rp, int n_tiles, const
     if (active) atomicAdd(s.n_active, active);
     if (upd) atomicAdd(s.n_update, upd);
   }
+}
+
+// Scalars of the multigrid-preconditioned loop after the level-0 post-smoothing:
+// partials [tile][Rp][2] = (r'.r', z.r') with r' the updated residual and z = M r'.
+// gamma = z.r', beta = gamma / gamma_prev (0 after a fresh start), and a
+// reliable update is requested once r'.r' has dropped by delta^2 since the last
+// one or below tol2 * ||b||^2. A vanished residual holds the realization still
+// until the true-residual check.
+__global__ void __launch_bounds__(1024) k_gmg_beta(int Rp, int n_tiles, const double* __restrict__ partial, Scal s,
+                                                   double delta2, double tol2) {
+  double v[2];
+  reduce_rows<2>(partial, n_tiles, Rp, v);
+  const int r = blockIdx.x * 32 + threadIdx.x;
+  int active = 0, upd = 0;
+  if (threadIdx.x < 32) {
+    float b = 0.f;
+    if (s.act[r]) {
+      const double rr = v[0], zr = v[1];
+      if (rr == 0.0) {
+        s.gamma[r] = 0.0;
+        active = 1;
+        upd = 1;
+      } else if (!(zr > 0.0) || !(rr == rr)) {
+        s.act[r] = 0;
+        s.breakdown[r] = 1;
+      } else {
+        const double gp = s.gamma_prev[r];
+        b = gp > 0.0 ? (float)(zr / gp) : 0.f;
+        s.gamma[r] = zr;
+        s.gamma_prev[r] = zr;
+        active = 1;
+        const double bn = s.bnorm[r];
+        upd = (rr < delta2 * s.rho_ref[r] || rr < tol2 * bn * bn) ? 1 : 0;
+      }
+    }
+    s.beta[r] = b;
+  }
+  active = __syncthreads_count(active);
+  upd = __syncthreads_count(upd);
+  if (threadIdx.x == 0) {
+    if (active) atomicAdd(s.n_active, active);
+    if (upd) atomicAdd(s.n_update, upd);
+  }
+}
+
+// alpha = gamma / p.(A p) of the multigrid loop; a held realization (gamma = 0)
+// keeps alpha = 0.
+__global__ void __launch_bounds__(1024) k_gmg_alpha(int Rp, int n_tiles, const double* __restrict__ partial, Scal s) {
+  double v[1];
+  reduce_rows<1>(partial, n_tiles, Rp, v);
+  if (threadIdx.x >= 32) return;
+  const int r = blockIdx.x * 32 + threadIdx.x;
+  const double pq = v[0];
+  float a = 0.f;
+  if (s.act[r] && s.gamma[r] > 0.0) {
+    if (!(pq > 0.0)) {
+      s.act[r] = 0;
+      s.breakdown[r] = 1;
+    } else {
+      a = (float)(s.gamma[r] / pq);
+      s.its[r] += 1;
+    }
+  }
+  s.alpha[r] = a;
 }
 
 // Per-realization ||b||^2 and (dinv b).b of a batch right-hand side (shared
@@ -1502,6 +1914,22 @@ struct BlockExec {
 
 // Everything one batch of solves on a structured lattice shares: sizes,
 // operator coefficients (A = cK E Khat + cM Mhat), workspace, tensor maps.
+// One coarse level (l >= 1) of the multigrid preconditioner: its lattice,
+// operator coefficients (Khat scales with the element size 2^l h, the mass with
+// its cube), maps, vectors b (restricted residual), x (iterate) and t (residual
+// or smoothed iterate), the coarsened element field and its Jacobi diagonal.
+struct GmgLevel {
+  Lattice L;
+  int nx = 0, ny = 0, nz = 0;  // elements per axis
+  ModalC MC;
+  double kdiag = 0.0, mdiag = 0.0;
+  const int* interior = nullptr;
+  const uint8_t* mask = nullptr;
+  float *b = nullptr, *x = nullptr, *t = nullptr, *E32 = nullptr, *dinv = nullptr;
+  int tiles_j = 0, n_tiles = 0, n_items = 0, grid = 0;
+  CUtensorMap tm_x, tm_t, tm_e;
+};
+
 struct BlockSys {
   BlockExec X;
   DevMem* own = nullptr;  // 32 buffers owned by a serving lane; nullptr: the context's workspace slots
@@ -1531,7 +1959,77 @@ struct BlockSys {
     return MSG_OK;
   }
   CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
+  // multigrid preconditioner: levels 1..n_lvl-1 (level 0 is this lattice), the
+  // level-0 pre-smoothed iterate xs, the damping and the coarsest-level sweeps
+  bool gmg = false;
+  int n_lvl = 1, sweeps = 0;
+  float omega = 0.f;
+  GmgLevel lv[kGmgMaxLevels];
+  WSlot xs, arena;
+  CUtensorMap tm_xs;
 };
+
+// Largest eigenvalue of diag(K)^-1 K for one element (power iteration on the
+// symmetric D^-1/2 K D^-1/2 from a fixed vector with no rigid-body part). It
+// bounds the spectrum of the assembled Jacobi-scaled operator for any positive
+// element field, so it fixes a safe Jacobi damping for every level.
+double element_jacobi_lambda(const double* K576) {
+  double dh[24], v[24], w[24];
+  for (int i = 0; i < 24; ++i) {
+    dh[i] = 1.0 / std::sqrt(K576[i * 24 + i]);
+    v[i] = std::sin(1.7 * i + 0.3) + 0.01 * i;
+  }
+  double lam = 0.0;
+  for (int it = 0; it < 500; ++it) {
+    double nv = 0.0;
+    for (int i = 0; i < 24; ++i) nv += v[i] * v[i];
+    nv = std::sqrt(nv);
+    for (int i = 0; i < 24; ++i) v[i] /= nv;
+    for (int i = 0; i < 24; ++i) {
+      double a = 0.0;
+      for (int j = 0; j < 24; ++j) a += dh[i] * K576[i * 24 + j] * dh[j] * v[j];
+      w[i] = a;
+    }
+    lam = 0.0;
+    for (int i = 0; i < 24; ++i) lam += v[i] * w[i];
+    for (int i = 0; i < 24; ++i) v[i] = w[i];
+  }
+  return lam;
+}
+
+// Coarse-level maps of a structured mesh for levels 1..n_lvl-1 (built once per
+// mesh, under its lock): a coarse node is constrained in component c when the
+// fine node it sits on is.
+int gmg_maps(Context* ctx, Mesh* m, int n_lvl) {
+  std::lock_guard<std::mutex> lock(m->gmg_mu);
+  if (m->gmg_levels >= n_lvl) return MSG_OK;
+  const int NXf = m->nx + 1, NYf = m->ny + 1;
+  for (int l = m->gmg_levels; l < n_lvl; ++l) {
+    const int nx = m->nx >> l, ny = m->ny >> l, nz = m->nz >> l;
+    const int NX = nx + 1, NY = ny + 1, NZ = nz + 1, NXp = NX + 2, NYp = NY + 2, NZp = NZ + 2;
+    std::vector<uint8_t> mask((size_t)NXp * NYp * NZp, 7);
+    std::vector<int> interior((size_t)NX * NY * NZ);
+    size_t t = 0;
+    for (int k = 0; k < NZ; ++k)
+      for (int j = 0; j < NY; ++j)
+        for (int i = 0; i < NX; ++i, ++t) {
+          const int p = (i + 1) + NXp * ((j + 1) + NYp * (k + 1));
+          const size_t f = ((size_t)i << l) + (size_t)NXf * (((size_t)j << l) + (size_t)NYf * ((size_t)k << l));
+          uint8_t mk = 0;
+          for (int c = 0; c < 3; ++c)
+            if (m->dof[3 * f + c] < 0) mk |= (uint8_t)(1 << c);
+          mask[p] = mk;
+          interior[t] = p;
+        }
+    MSG_TRY(m->d_gmg_mask[l].alloc(ctx, mask.size()));
+    MSG_TRY(m->d_gmg_interior[l].alloc(ctx, sizeof(int) * interior.size()));
+    MSG_CUDA(ctx, cudaMemcpy(m->d_gmg_mask[l].ptr, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+    MSG_CUDA(ctx, cudaMemcpy(m->d_gmg_interior[l].ptr, interior.data(), sizeof(int) * interior.size(),
+                             cudaMemcpyHostToDevice));
+  }
+  m->gmg_levels = n_lvl;
+  return MSG_OK;
+}
 
 // Coefficients and workspace of a batch: A = cK E Khat(nu) + cM Mhat(rho).
 int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double cM, int R, int Rp, BlockSys* B,
@@ -1722,6 +2220,113 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
     e = r1 != CUDA_SUCCESS ? r1 : r2;
   }
   if (e != CUDA_SUCCESS) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
+
+  // multigrid levels: halve the lattice while every axis is even and keeps at
+  // least 2 elements
+  B->gmg = false;
+  B->n_lvl = 1;
+  if (ctx->multigrid && B->modal && !own) {
+    int n_lvl = 1;
+    while (n_lvl < ctx->mg_levels) {
+      const int nx = m->nx >> (n_lvl - 1), ny = m->ny >> (n_lvl - 1), nz = m->nz >> (n_lvl - 1);
+      if ((nx & 1) || (ny & 1) || (nz & 1) || nx < 4 || ny < 4 || nz < 4) break;
+      ++n_lvl;
+    }
+    if (n_lvl >= 2) {
+      MSG_TRY(gmg_maps(ctx, m, n_lvl));
+      B->gmg = true;
+      B->n_lvl = n_lvl;
+      B->sweeps = ctx->mg_sweeps;
+      const double lam = element_jacobi_lambda(K576);
+      B->omega = (float)(ctx->mg_omega > 0.0 ? ctx->mg_omega : std::min(0.6, 3.19 / lam));
+      MSG_TRY(B->slot_alloc(ctx, 30, sizeof(float) * nvec, &B->xs.ptr));
+      MSG_CUDA(ctx, cudaMemsetAsync(B->xs.ptr, 0, sizeof(float) * nvec, st));
+      const cuuint32_t pbm[5] = {32, 3, 1, kMPJ, kMPK};
+      if (enc5(&B->tm_xs, B->xs.ptr, pbm) != CUDA_SUCCESS)
+        return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (multigrid)");
+      size_t arena = 0;
+      auto take = [&](size_t bytes) {
+        const size_t o = arena;
+        arena += (bytes + 255) & ~(size_t)255;
+        return o;
+      };
+      size_t off[kGmgMaxLevels][5];
+      for (int l = 1; l < n_lvl; ++l) {
+        GmgLevel& g = B->lv[l];
+        g.nx = m->nx >> l;
+        g.ny = m->ny >> l;
+        g.nz = m->nz >> l;
+        Lattice& Lc = g.L;
+        Lc.NX = g.nx + 1; Lc.NY = g.ny + 1; Lc.NZ = g.nz + 1;
+        Lc.NXp = Lc.NX + 2; Lc.NYp = Lc.NY + 2; Lc.NZp = Lc.NZ + 2;
+        Lc.Rp = Rp;
+        Lc.tiles_j = (Lc.NY + kTJ - 1) / kTJ;
+        Lc.n_pad = Lc.NXp * Lc.NYp * Lc.NZp;
+        Lc.n_int = Lc.NX * Lc.NY * Lc.NZ;
+        const double sk = (double)(1 << l), sm = sk * sk * sk;
+        MSG_TRY(modal_coefficients(ctx, K576, B->mass ? M576 : nullptr, cK * sk, cM * sm, &g.MC));
+        g.kdiag = B->kdiag * sk;
+        g.mdiag = B->mdiag * sm;
+        g.interior = m->d_gmg_interior[l].as<int>();
+        g.mask = m->d_gmg_mask[l].as<uint8_t>();
+        g.tiles_j = (Lc.NY + kMJ - 1) / kMJ;
+        g.n_tiles = g.tiles_j * ((Lc.NZ + kMK - 1) / kMK);
+        g.n_items = g.n_tiles * (Rp / 32);
+        g.grid = std::min(g.n_items, ctx->sm_count);
+        const size_t nv = (size_t)Lc.n_pad * 3 * Rp, ns = (size_t)Lc.n_pad * Rp;
+        off[l][0] = take(sizeof(float) * nv);
+        off[l][1] = take(sizeof(float) * nv);
+        off[l][2] = take(sizeof(float) * nv);
+        off[l][3] = take(sizeof(float) * ns);
+        off[l][4] = take(sizeof(float) * ns);
+      }
+      MSG_TRY(B->slot_alloc(ctx, 31, arena, &B->arena.ptr));
+      MSG_CUDA(ctx, cudaMemsetAsync(B->arena.ptr, 0, arena, st));  // ghosts stay zero
+      char* base = B->arena.as<char>();
+      for (int l = 1; l < n_lvl; ++l) {
+        GmgLevel& g = B->lv[l];
+        g.b = (float*)(base + off[l][0]);
+        g.x = (float*)(base + off[l][1]);
+        g.t = (float*)(base + off[l][2]);
+        g.E32 = (float*)(base + off[l][3]);
+        g.dinv = (float*)(base + off[l][4]);
+        const Lattice& Lc = g.L;
+        const cuuint64_t cpd[5] = {(cuuint64_t)Rp, 3, (cuuint64_t)Lc.NXp, (cuuint64_t)Lc.NYp, (cuuint64_t)Lc.NZp};
+        const cuuint64_t cps[4] = {Rp * fb, 3 * Rp * fb, 3 * Rp * fb * Lc.NXp, 3 * Rp * fb * Lc.NXp * Lc.NYp};
+        const cuuint64_t ced[4] = {(cuuint64_t)Rp, (cuuint64_t)Lc.NXp, (cuuint64_t)Lc.NYp, (cuuint64_t)Lc.NZp};
+        const cuuint64_t ces[3] = {Rp * fb, Rp * fb * Lc.NXp, Rp * fb * Lc.NXp * Lc.NYp};
+        const cuuint32_t ebm[4] = {32, 1, kMEJ, kMEK};
+        auto c5 = [&](CUtensorMap* tm, void* p) {
+          return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, p, cpd, cps, pbm, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        };
+        const CUresult r1 = c5(&g.tm_x, g.x), r2 = c5(&g.tm_t, g.t);
+        const CUresult r3 = encode(&g.tm_e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g.E32, ced, ces, ebm, one,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS || r3 != CUDA_SUCCESS)
+          return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (multigrid level %d)", l);
+      }
+      static std::once_flag lvl_once;
+      static cudaError_t lvl_err = cudaSuccess;
+      std::call_once(lvl_once, [] {
+        const std::pair<const void*, size_t> fs[] = {
+            {(const void*)k_lvl_op<kLvlStart, false>, LvlStage<kLvlStart>::kSmem},
+            {(const void*)k_lvl_op<kLvlStart, true>, LvlStage<kLvlStart>::kSmem},
+            {(const void*)k_lvl_op<kLvlResid, false>, LvlStage<kLvlResid>::kSmem},
+            {(const void*)k_lvl_op<kLvlResid, true>, LvlStage<kLvlResid>::kSmem},
+            {(const void*)k_lvl_op<kLvlSmooth, false>, LvlStage<kLvlSmooth>::kSmem},
+            {(const void*)k_lvl_op<kLvlSmooth, true>, LvlStage<kLvlSmooth>::kSmem},
+            {(const void*)k_lvl_op<kLvlPcgZ, false>, LvlStage<kLvlPcgZ>::kSmem},
+            {(const void*)k_lvl_op<kLvlPcgZ, true>, LvlStage<kLvlPcgZ>::kSmem}};
+        for (const auto& f : fs)
+          if (lvl_err == cudaSuccess)
+            lvl_err = cudaFuncSetAttribute(f.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.second);
+      });
+      MSG_CUDA(ctx, lvl_err);
+    }
+  }
   return MSG_OK;
 }
 
@@ -1739,6 +2344,15 @@ int block_field(Context* ctx, Mesh* m, BlockSys* B, const KLDevice* kl, const do
   k_dinv<<<B->L.n_int, 128, 0, st>>>(B->L, B->kdiag, B->mdiag, B->E32.as<float>(), B->interior,
                                      B->dinv.as<float>());
   count_launch(ctx, 2);
+  // multigrid: coarsened element fields and the Jacobi diagonal of every level
+  for (int l = 1; l < B->n_lvl; ++l) {
+    GmgLevel& g = B->lv[l];
+    const Lattice& Lf = l == 1 ? B->L : B->lv[l - 1].L;
+    const float* Ef = l == 1 ? B->E32.as<float>() : B->lv[l - 1].E32;
+    k_coarsen_E<<<g.nx * g.ny * g.nz, 128, 0, st>>>(Lf, g.L, g.nx, g.ny, Ef, g.E32);
+    k_dinv<<<g.L.n_int, 128, 0, st>>>(g.L, g.kdiag, g.mdiag, g.E32, g.interior, g.dinv);
+    count_launch(ctx, 2);
+  }
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
 }
@@ -1765,10 +2379,111 @@ LoopCfg loop_cfg(Context* ctx, const BlockSys* B, double tol, int chunk_cap) {
   c.n_dir = std::min(B->L.n_int, ctx->sm_count * 8);
   c.chunk = std::max(2, (chunk_cap > 0 ? std::min(ctx->chunk, chunk_cap) : ctx->chunk) & ~1);
   c.delta2 = ctx->reliable_delta * ctx->reliable_delta;
+  if (B->gmg) {
+    // a multigrid iteration cuts the residual several-fold: check every few
+    // iterations, replace the residual after a larger drop
+    c.chunk = std::min(c.chunk, 4);
+    c.delta2 = ctx->mg_delta * ctx->mg_delta;
+  }
   // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
   // sqrt(gamma / gamma0) is at tol/4 (single-reduction loop, dinv-weighted norm)
-  c.tol2 = (B->modal ? 0.0625 : 0.25) * tol * tol;
+  c.tol2 = (B->modal && !B->gmg ? 0.0625 : 0.25) * tol * tol;
   return c;
+}
+
+// One iteration of the multigrid-preconditioned loop (enqueued on st; every
+// launch is a graph node while the chunk is captured). Level 0 (the batch
+// lattice): r (r32 / rB alternating), the pre-smoothed iterate xs, the residual
+// after pre-smoothing and later z (both in qB), p (p / pB alternating), q, d.
+// V-cycle: one damped Jacobi sweep down (from zero), residual, restriction;
+// `sweeps` sweeps on the coarsest level; prolongation and one sweep up. With
+// the same sweep on both sides and a fixed sweep count on the coarsest level
+// the preconditioner is symmetric positive definite (damping below
+// 2 / lambda_max(dinv A)).
+void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
+  const int Rp = B->Rp;
+  Scal& s = B->s;
+  cudaEvent_t* ev = B->X.ev;
+  const bool even = (it & 1) == 0;
+  const int nl = B->n_lvl;
+  const float om = B->omega;
+  double* part2 = B->part_op.as<double>();
+  double* part1 = part2 + (size_t)2 * B->n_tiles_m * Rp;
+  float* r_in = even ? B->r32.as<float>() : B->rB.as<float>();
+  float* r_out = even ? B->rB.as<float>() : B->r32.as<float>();
+  float* p_out = even ? B->pB.as<float>() : B->p.as<float>();
+  const CUtensorMap& tm_rin = even ? B->tm_rAm : B->tm_rBm;
+  const CUtensorMap& tm_pin = even ? B->tm_pAm : B->tm_pBm;
+  float* qB = B->qB.as<float>();
+  const bool mass = B->mass;
+  auto lvl = [&](auto mode, const Lattice& L, const ModalC& C, const CUtensorMap& ta, const CUtensorMap& tb,
+                 const CUtensorMap& tn, const CUtensorMap& te, const CUtensorMap& td, int tiles_j, int n_tiles,
+                 int n_items, int grid, const uint8_t* mask, const float* b, const float* dinv, float* out,
+                 float* out2, float* out3, float* d, double* partial, int pstride) {
+    constexpr int kMode = decltype(mode)::value;
+    auto k = mass ? k_lvl_op<kMode, true> : k_lvl_op<kMode, false>;
+    k<<<grid, kMThreads, LvlStage<kMode>::kSmem, st>>>(L, C, ta, tb, tn, te, td, tiles_j, n_tiles, n_items, mask, b,
+                                                       dinv, om, s.alpha, s.beta, out, out2, out3, d, partial,
+                                                       pstride, s.err);
+  };
+  using Start = std::integral_constant<int, kLvlStart>;
+  using Resid = std::integral_constant<int, kLvlResid>;
+  using Smooth = std::integral_constant<int, kLvlSmooth>;
+  using PcgZ = std::integral_constant<int, kLvlPcgZ>;
+  if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
+  // level 0: r' = r - alpha q, xs = omega dinv r', qB = r' - A xs, partial r'.r'
+  lvl(Start{}, B->L, B->MC, tm_rin, B->tm_qAm, B->tm_dinvm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m,
+      B->n_items_m, B->grid_m, B->mask, nullptr, nullptr, qB, r_out, B->xs.as<float>(), nullptr, part2, 2);
+  // down: restrict the residual, residual of the first sweep on every level but the coarsest
+  for (int l = 1; l < nl; ++l) {
+    GmgLevel& g = B->lv[l];
+    const Lattice& Lf = l == 1 ? B->L : B->lv[l - 1].L;
+    const float* tf = l == 1 ? qB : B->lv[l - 1].t;
+    k_restrict<<<g.L.n_int, 128, 0, st>>>(Lf, g.L, g.interior, g.mask, tf, g.dinv, om, g.b, g.x);
+    if (l < nl - 1)
+      lvl(Resid{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
+          g.mask, g.b, nullptr, g.t, nullptr, nullptr, nullptr, nullptr, 1);
+  }
+  // coarsest level: the restriction made the first sweep; sweeps - 1 more, x and t alternating
+  const float* res_c;
+  {
+    GmgLevel& g = B->lv[nl - 1];
+    bool in_x = true;
+    for (int k = 1; k < B->sweeps; ++k) {
+      lvl(Smooth{}, g.L, g.MC, in_x ? g.tm_x : g.tm_t, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles,
+          g.n_items, g.grid, g.mask, g.b, g.dinv, in_x ? g.t : g.x, nullptr, nullptr, nullptr, nullptr, 1);
+      in_x = !in_x;
+    }
+    res_c = in_x ? g.x : g.t;
+  }
+  // up: prolongate into the level's iterate, one sweep (result in t)
+  for (int l = nl - 2; l >= 1; --l) {
+    GmgLevel& g = B->lv[l];
+    k_prolong_add<<<g.L.n_int, 128, 0, st>>>(g.L, B->lv[l + 1].L, g.interior, g.mask, res_c, g.x);
+    lvl(Smooth{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
+        g.mask, g.b, g.dinv, g.t, nullptr, nullptr, nullptr, nullptr, 1);
+    res_c = g.t;
+  }
+  k_prolong_add<<<B->L.n_int, 128, 0, st>>>(B->L, B->lv[1].L, B->interior, B->mask, res_c, B->xs.as<float>());
+  // level 0 post-sweep: z (into qB) and the partial z.r'
+  lvl(Smooth{}, B->L, B->MC, B->tm_xs, B->tm_xs, B->tm_xs, B->tm_em, B->tm_xs, B->tiles_jm, B->n_tiles_m,
+      B->n_items_m, B->grid_m, B->mask, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr, part2 + 1, 2);
+  cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
+  k_gmg_beta<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part2, s, c.delta2, c.tol2);
+  // p = z + beta p_old, d += alpha p_old, q = A p, partial p.q
+  if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
+  lvl(PcgZ{}, B->L, B->MC, B->tm_qBm, tm_pin, B->tm_qBm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m,
+      B->n_items_m, B->grid_m, B->mask, nullptr, nullptr, B->q.as<float>(), p_out, nullptr, B->d.as<float>(), part1,
+      1);
+  if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
+  k_gmg_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part1, s);
+  if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
+}
+
+// Kernels of one multigrid iteration (for the launch count).
+int gmg_launches(const BlockSys* B) {
+  const int nl = B->n_lvl;
+  return 1 + (nl - 1) + (nl - 2) + (B->sweeps - 1) + (nl - 1) + (nl - 2) + 1 + 1 + 1 + 1;
 }
 
 // The inner-loop graph of `chunk` FP32 iterations, kept in the exec slot and
@@ -1807,6 +2522,14 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
     }
     const int mm[6] = {modal ? 1 : 0, B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
     mix(mm, sizeof(mm));
+    const int gg[3] = {B->gmg ? 1 : 0, B->n_lvl, B->sweeps};
+    mix(gg, sizeof(gg));
+    if (B->gmg) {
+      mix(&B->omega, sizeof(B->omega));
+      mix(&B->xs.ptr, sizeof(void*));
+      mix(&B->tm_xs, sizeof(CUtensorMap));
+      for (int l = 1; l < B->n_lvl; ++l) mix(&B->lv[l], sizeof(GmgLevel));
+    }
     const double dd[2] = {c.delta2, c.tol2};
     mix(dd, sizeof(dd));
     const int ii[6] = {c.chunk, c.n_dir, B->n_upd, B->n_tiles, c.sblocks, (int)c.upd_smem};
@@ -1823,7 +2546,9 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
     for (int it = 0; it < c.chunk; ++it) {
       // cudaEventRecordExternal: a real event-record node in the graph (plain
       // records during capture only order streams)
-      if (modal) {
+      if (B->gmg) {
+        gmg_iteration(B, c, it, st);
+      } else if (modal) {
         // single-reduction loop: one operator launch per iteration; r, q and p
         // alternate between their two buffers
         const bool even = (it & 1) == 0;
@@ -1900,7 +2625,8 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
       k_resid<false, false><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
   }
   MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
-  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles, part, s, tol, first ? 1 : 0, B->modal ? 1 : 0, max_it);
+  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles, part, s, tol, first ? 1 : 0,
+                                               B->gmg ? 2 : (B->modal ? 1 : 0), max_it);
   count_launch(ctx, 2);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
@@ -1964,7 +2690,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
-    count_launch(ctx, (B->modal ? 2 : 5) * c.chunk);
+    count_launch(ctx, (B->gmg ? gmg_launches(B) : (B->modal ? 2 : 5)) * c.chunk);
     total_inner += c.chunk;
     cudaEventRecord(ev[3], st);
     MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));

@@ -556,6 +556,17 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
   if (!std::strcmp(key, "modal_operator") && (value == 0 || value == 1)) { ctx->modal = (int)value; return MSG_OK; }
   if (!std::strcmp(key, "fixed_updates") && (value == 0 || value == 1)) { ctx->fixed_updates = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "multigrid") && (value == 0 || value == 1)) { ctx->multigrid = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "multigrid_levels") && value >= 2 && value <= kGmgMaxLevels && value == (int)value) {
+    ctx->mg_levels = (int)value;
+    return MSG_OK;
+  }
+  if (!std::strcmp(key, "multigrid_sweeps") && value >= 1 && value <= 1000 && value == (int)value) {
+    ctx->mg_sweeps = (int)value;
+    return MSG_OK;
+  }
+  if (!std::strcmp(key, "multigrid_omega") && value >= 0 && value < 1) { ctx->mg_omega = value; return MSG_OK; }
+  if (!std::strcmp(key, "multigrid_delta") && value > 0 && value < 1) { ctx->mg_delta = value; return MSG_OK; }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 

@@ -28,6 +28,8 @@ __host__ __device__ constexpr int corner_id(int ax, int ay, int az) {
   return az * 4 + (ay ? (ax ? 2 : 3) : (ax ? 1 : 0));
 }
 
+constexpr int kGmgMaxLevels = 6;  // multigrid lattice levels at most (fine level included)
+
 struct Context;
 
 // Device allocation charged against the context's memory budget.
@@ -68,6 +70,12 @@ struct Context {
   int chunk = 16;               // inner iterations per captured graph launch
   int modal = 1;                // FP32 operator: 1 = Walsh-mode (modal) kernel, 0 = dense value-class kernel
   int fixed_updates = 0;        // 1: FP64 true-residual step after every graph chunk (batch-invariant results)
+  // multigrid preconditioner of the batched lattice solves (modal operator only)
+  int multigrid = 0;            // 1: V-cycle preconditioned loop where the lattice coarsens at least once
+  int mg_levels = 4;            // lattice levels, fine level included (2..kGmgMaxLevels)
+  int mg_sweeps = 10;           // damped Jacobi sweeps on the coarsest level
+  double mg_omega = 0.0;        // Jacobi damping; 0 = from the element stiffness
+  double mg_delta = 1e-3;       // reliable-update factor of the multigrid loop (its residual falls fast)
   // Workspace kept across calls (allocation and cudaFree synchronise the
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
@@ -165,6 +173,12 @@ struct Mesh {
   DevMem d_pad_elem_row;   // [n_elems] padded row of the element
   DevMem d_pad_mask;       // [padded nodes] constrained bits, ghosts = 7
   DevMem d_pad_interior;   // [interior nodes] padded index of interior node t (generator order)
+  // coarse lattices of the multigrid preconditioner, level l = 1..gmg_levels-1
+  // (node (i, j, k) of level l sits on fine node 2^l (i, j, k)): constrained
+  // bits of the padded nodes (ghosts 7) and the interior list; built on first use
+  std::mutex gmg_mu;
+  int gmg_levels = 1;
+  DevMem d_gmg_mask[kGmgMaxLevels], d_gmg_interior[kGmgMaxLevels];
 };
 
 struct PcgState {
