@@ -44,6 +44,8 @@ METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p
 # DRAM traffic of one k_op_modal launch per realization on the 32^3 lattice: ncu capture
 # at R = 512 (dram__bytes_read.sum 1,165.9 MB + dram__bytes_write.sum 845.5 MB) / 512
 OP_DRAM_BYTES_PER_REALIZATION = (1165.921e6 + 845.472e6) / 512
+# the same for the multigrid loop's direction + operator launch (k_lvl_op<PcgZ>), 32^3 lattice
+MG_OP_DRAM_BYTES_PER_REALIZATION = None
 
 
 def parse():
@@ -74,6 +76,10 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
     p.add_argument("--multigrid", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION multigrid (1: V-cycle preconditioned batched loop)")
+    p.add_argument("--mg-levels", type=int, default=None, help="MSG_SET_OPTION multigrid_levels")
+    p.add_argument("--mg-sweeps", type=int, default=None, help="MSG_SET_OPTION multigrid_sweeps (coarsest level)")
+    p.add_argument("--mg-delta", type=float, default=None, help="MSG_SET_OPTION multigrid_delta")
+    p.add_argument("--mg-omega", type=float, default=None, help="MSG_SET_OPTION multigrid_omega")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
@@ -353,6 +359,10 @@ def main():
         ctx.set_option("modal_operator", args.modal_operator)
     if args.multigrid is not None:
         ctx.set_option("multigrid", args.multigrid)
+    for key, val in (("multigrid_levels", args.mg_levels), ("multigrid_sweeps", args.mg_sweeps),
+                     ("multigrid_delta", args.mg_delta), ("multigrid_omega", args.mg_omega)):
+        if val is not None:
+            ctx.set_option(key, val)
     model, kl = make_problem(args)
     mesh = M.GpuMesh(ctx, model)
     R, K_terms = args.R, args.terms
@@ -430,19 +440,29 @@ def main():
     tip_mean, tip_var, cnt = mom["mean"], mom["variance"], mom["count"]
 
     # roofline of the dominant kernel, the fused direction + matrix-free FP32 operator
-    # (k_op_modal; live per-launch samples from the timed region)
+    # (live per-launch samples from the timed region): k_lvl_op<PcgZ> in the multigrid
+    # loop, k_op_modal in the Jacobi loop
+    mg = args.multigrid != 0
     op_ms = st["op_launch_ms"]
     nn = model.n_nodes
     ne = model.n_elems
     Rp = (R + 31) // 32 * 32
-    # algorithmic bytes of one launch, FP32, realization-innermost, each value once:
-    # read r, p_{k-1}, d (3 per node), dinv (1 per node), E (1 per element); write p_k, d, q (3 per node)
-    op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 1 + 3 + 3 + 3) * nn + ne)
+    # algorithmic bytes of one launch, FP32, realization-innermost, each value once.
+    # multigrid: read z, p_{k-1}, d (3 per node), E (1 per element); write p_k, d, q (3 per node).
+    # Jacobi: read r, p_{k-1}, d (3 per node), dinv (1 per node), E; write p_k, d, q (3 per node)
+    if mg:
+        op_kernel = "k_lvl_op<PcgZ> (multigrid loop: fused search direction p = z + beta p + matrix-free FP32 operator)"
+        op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 3 + 3 + 3) * nn + ne)
+        per_r = MG_OP_DRAM_BYTES_PER_REALIZATION
+    else:
+        op_kernel = "k_op_modal (fused PCG direction update + matrix-free FP32 Hexa8 operator)"
+        op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 1 + 3 + 3 + 3) * nn + ne)
+        per_r = OP_DRAM_BYTES_PER_REALIZATION
     hbm, peak_kind = load_peaks()
     achieved = op_bytes / (op_ms / 1e3) / 1e9 if op_ms > 0 else 0.0
     # DRAM bytes per launch from one ncu capture of the same kernel at 512 realizations
     # (dram__bytes_read.sum + dram__bytes_write.sum), scaled by the realizations processed
-    traffic = OP_DRAM_BYTES_PER_REALIZATION * Rp if OP_DRAM_BYTES_PER_REALIZATION else None
+    traffic = per_r * Rp if (per_r and args.n == 32) else None
 
     line = None
     if rank == 0:
@@ -500,19 +520,21 @@ def main():
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": f"batched Monte Carlo, {R} realizations x {args.n}^3 Hexa8 per GPU per step "
                                    f"(z=0 clamped, unit top pressure, 50-term KL lognormal E, sigma 0.3, l 0.2*side, "
-                                   f"nu 0.3), mixed FP32 matrix-free PCG + FP64 refinement to FP64 true residual "
-                                   f"< {args.tol:g}",
+                                   f"nu 0.3), mixed FP32 matrix-free PCG "
+                                   f"({'geometric multigrid V(1,1)' if mg else 'Jacobi'} preconditioner) + FP64 "
+                                   f"refinement to FP64 true residual < {args.tol:g}",
                        "realizations_per_gpu": R, "mesh": f"{args.n}x{args.n}x{args.n}", "free_dofs": Nd,
                        "kl_terms": K_terms, "tol_true_residual": args.tol,
                        "l2": "inputs larger than L2 (per-GPU batch state ~4.6 GB)", "parallelism": f"realizations x{ws}"},
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(R * K_terms * 8 + Nd * 8),
                     "d2h_bytes_per_step": int(R * Nd * 8 + R * (8 + 4 + 8))},
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "k_op_modal (fused PCG direction update + matrix-free FP32 Hexa8 operator)",
+            "roofline": {"kernel": op_kernel,
                          "bound": "hbm", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if hbm else None, "traffic": traffic,
                          "peak_kind": peak_kind, "launch_ms": op_ms, "bytes_per_launch": op_bytes,
-                         "update_launch_ms": st["update_launch_ms"], "samples": st["launch_samples"]},
+                         ("iteration_ms" if mg else "update_launch_ms"): st["update_launch_ms"],
+                         "samples": st["launch_samples"]},
             "cpu_baseline": cpu,
             "clocks": clk,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

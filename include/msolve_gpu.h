@@ -283,7 +283,19 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * "fixed_updates" (1: the FP64 true-residual step runs after every chunk for
  * every realization, so each realization's arithmetic no longer depends on the
  * rest of the batch: bitwise identical alone or batched; default 0: the step
- * runs when some realization asks for it). */
+ * runs when some realization asks for it), "multigrid" (preconditioner of the
+ * batched lattice loop: 1, default, a geometric multigrid V-cycle for systems
+ * without a mass term (static solves, serving), Jacobi for those with one
+ * (Newmark); 2: the V-cycle for both; 0: Jacobi for both. The V-cycle needs a
+ * lattice whose element counts are even at least once; otherwise Jacobi runs),
+ * "multigrid_levels" (lattice levels at most, fine level included, 2..6,
+ * default 6; a level halves every axis while each keeps at least 2 elements),
+ * "multigrid_sweeps" (damped Jacobi sweeps on the coarsest level, default 20),
+ * "multigrid_omega" (Jacobi damping of every level, 0 = derived from the
+ * element stiffness, default), "multigrid_delta" (reliable-update factor of the
+ * V-cycle loop, default 0.01; its inner chunk is 2 iterations).
+ * In the multigrid loop t[5] below is the duration of one search-direction +
+ * operator launch and t[6] that of one whole iteration. */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 
 /* Kernel launch counter of this context (kernels launched since creation),

@@ -1062,65 +1062,91 @@ __global__ void __launch_bounds__(kMThreads, 1)
 // Full-weighting restriction b_c = P^T t_f (P: trilinear prolongation), masked
 // at the coarse level, and x_c = omega dinv_c b_c (the first Jacobi sweep from
 // zero). Coarse node (I, J, K) (padded) sits on fine node (2I-1, 2J-1, 2K-1);
-// the fine ghost layer is zero. One CTA per coarse interior node.
-__global__ void __launch_bounds__(128) k_restrict(Lattice Lf, Lattice Lc, const int* __restrict__ interior_c,
+// the fine ghost layer is zero. One thread per coarse interior node and four
+// realizations (float4).
+__global__ void __launch_bounds__(256) k_restrict(Lattice Lf, Lattice Lc, const int* __restrict__ interior_c,
                                                   const uint8_t* __restrict__ mask_c, const float* __restrict__ tf,
                                                   const float* __restrict__ dinv_c, float omega,
                                                   float* __restrict__ bc, float* __restrict__ xc) {
-  const size_t nc = (size_t)interior_c[blockIdx.x];
+  const int Q = Lf.Rp >> 2;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)Lc.n_int * Q) return;
+  const int t = (int)(idx / Q), q = (int)(idx % Q);
+  const size_t nc = (size_t)interior_c[t];
   const int I = (int)(nc % Lc.NXp), J = (int)((nc / Lc.NXp) % Lc.NYp), K = (int)(nc / ((size_t)Lc.NXp * Lc.NYp));
   const size_t sy = (size_t)Lf.NXp, sz = (size_t)Lf.NXp * Lf.NYp;
   const size_t fc = (size_t)(2 * I - 1) + sy * (2 * J - 1) + sz * (2 * K - 1);
   const uint32_t mk = mask_c[nc];
-  const int Rp = Lf.Rp;
-  for (int rr = threadIdx.x; rr < Rp; rr += blockDim.x) {
-    const float wdv = omega * dinv_c[nc * Rp + rr];
+  const float4* t4 = reinterpret_cast<const float4*>(tf);
+  const float4 dv = reinterpret_cast<const float4*>(dinv_c)[nc * Q + q];
+  float4* b4 = reinterpret_cast<float4*>(bc);
+  float4* x4 = reinterpret_cast<float4*>(xc);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      float s = 0.f;
+  for (int c = 0; c < 3; ++c) {
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-      for (int dz = -1; dz <= 1; ++dz)
+    for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
-        for (int dy = -1; dy <= 1; ++dy)
+      for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
-          for (int dx = -1; dx <= 1; ++dx) {
-            const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
-            const size_t f = fc + dx + dy * sy + dz * sz;
-            s = fmaf(wgt, tf[(f * 3 + c) * Rp + rr], s);
-          }
-      s = ((mk >> c) & 1) ? 0.f : s;
-      bc[(nc * 3 + c) * Rp + rr] = s;
-      xc[(nc * 3 + c) * Rp + rr] = wdv * s;
-    }
+        for (int dx = -1; dx <= 1; ++dx) {
+          const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+          const float4 v = t4[((fc + dx + dy * sy + dz * sz) * 3 + c) * Q + q];
+          s.x = fmaf(wgt, v.x, s.x);
+          s.y = fmaf(wgt, v.y, s.y);
+          s.z = fmaf(wgt, v.z, s.z);
+          s.w = fmaf(wgt, v.w, s.w);
+        }
+    if ((mk >> c) & 1) s = make_float4(0.f, 0.f, 0.f, 0.f);
+    b4[(nc * 3 + c) * Q + q] = s;
+    x4[(nc * 3 + c) * Q + q] =
+        make_float4(omega * dv.x * s.x, omega * dv.y * s.y, omega * dv.z * s.z, omega * dv.w * s.w);
   }
 }
 
-// x_f += P x_c: trilinear prolongation of the coarse correction (fine node
-// with even coordinate: the coincident coarse node; odd: the mean of the two
-// neighbours, per axis), masked at the fine level. One CTA per fine interior node.
-__global__ void __launch_bounds__(128) k_prolong_add(Lattice Lf, Lattice Lc, const int* __restrict__ interior_f,
+// x_f += P x_c: trilinear prolongation of the coarse correction (per axis, a
+// fine node with even coordinate takes the coincident coarse node, an odd one
+// the mean of its two neighbours), masked at the fine level. One thread per
+// fine interior node and four realizations; the 8 corner terms are summed in a
+// fixed order (an even axis repeats its coarse node with weight 0).
+__global__ void __launch_bounds__(256) k_prolong_add(Lattice Lf, Lattice Lc, const int* __restrict__ interior_f,
                                                      const uint8_t* __restrict__ mask_f,
                                                      const float* __restrict__ xc, float* __restrict__ xf) {
-  const size_t nf = (size_t)interior_f[blockIdx.x];
+  const int Q = Lf.Rp >> 2;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)Lf.n_int * Q) return;
+  const int t = (int)(idx / Q), q = (int)(idx % Q);
+  const size_t nf = (size_t)interior_f[t];
+  const uint32_t mk = mask_f[nf];
+  if (mk == 7u) return;
   const int gi = (int)(nf % Lf.NXp) - 1, gj = (int)((nf / Lf.NXp) % Lf.NYp) - 1;
   const int gk = (int)(nf / ((size_t)Lf.NXp * Lf.NYp)) - 1;
   const size_t sy = (size_t)Lc.NXp, sz = (size_t)Lc.NXp * Lc.NYp;
   const size_t c0 = (size_t)((gi >> 1) + 1) + sy * ((gj >> 1) + 1) + sz * ((gk >> 1) + 1);
-  const int ni = (gi & 1) + 1, nj = (gj & 1) + 1, nk = (gk & 1) + 1;
-  const float wgt = ((gi & 1) ? 0.5f : 1.f) * ((gj & 1) ? 0.5f : 1.f) * ((gk & 1) ? 0.5f : 1.f);
-  const uint32_t mk = mask_f[nf];
-  const int Rp = Lf.Rp;
-  for (int rr = threadIdx.x; rr < Rp; rr += blockDim.x) {
+  const size_t oi = gi & 1, oj = (gj & 1) * sy, ok = (gk & 1) * sz;  // offset of the second neighbour (or 0)
+  const float wi[2] = {(gi & 1) ? 0.5f : 1.f, (gi & 1) ? 0.5f : 0.f};
+  const float wj[2] = {(gj & 1) ? 0.5f : 1.f, (gj & 1) ? 0.5f : 0.f};
+  const float wk[2] = {(gk & 1) ? 0.5f : 1.f, (gk & 1) ? 0.5f : 0.f};
+  const float4* c4 = reinterpret_cast<const float4*>(xc);
+  float4* f4 = reinterpret_cast<float4*>(xf);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if ((mk >> c) & 1) continue;
-      float s = 0.f;
-      for (int a = 0; a < nk; ++a)
-        for (int bb = 0; bb < nj; ++bb)
-          for (int e = 0; e < ni; ++e) s += xc[((c0 + e + bb * sy + a * sz) * 3 + c) * Rp + rr];
-      const size_t o = (nf * 3 + c) * Rp + rr;
-      xf[o] = fmaf(wgt, s, xf[o]);
-    }
+  for (int c = 0; c < 3; ++c) {
+    if ((mk >> c) & 1) continue;
+    float4 s = f4[(nf * 3 + c) * Q + q];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const float wgt = wk[a] * wj[bb] * wi[e];
+          const float4 v = c4[((c0 + (e ? oi : 0) + (bb ? oj : 0) + (a ? ok : 0)) * 3 + c) * Q + q];
+          s.x = fmaf(wgt, v.x, s.x);
+          s.y = fmaf(wgt, v.y, s.y);
+          s.z = fmaf(wgt, v.z, s.z);
+          s.w = fmaf(wgt, v.w, s.w);
+        }
+    f4[(nf * 3 + c) * Q + q] = s;
   }
 }
 
@@ -1785,6 +1811,22 @@ __global__ void k_lattice_rhs(int n_dofs, const int* __restrict__ rows, const do
   if (i < n_dofs) b_lat[rows[i]] = b_dof[i];
 }
 
+// r32 = (float) b over the interior nodes (b shared, b[node*3 + c], or per
+// realization in the batch layout); constrained entries of b are zero.
+__global__ void __launch_bounds__(256) k_b_to_r32(int n_int, int Rp, const int* __restrict__ interior,
+                                                  const double* __restrict__ b, int per_r, float* __restrict__ r32) {
+  const long total = (long)n_int * Rp;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const int t = (int)(i / Rp), rr = (int)(i % Rp);
+    const size_t node = (size_t)interior[t];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t o = (node * 3 + c) * Rp + rr;
+      r32[o] = (float)(per_r ? b[o] : b[node * 3 + c]);
+    }
+  }
+}
+
 // X[r][dof] = x[(row(dof))*Rp + r] through a 32x32 shared-memory transpose.
 __global__ void k_gather_solution(int n_dofs, int R, int Rp, const int* __restrict__ rows,
                                   const double* __restrict__ x, double* __restrict__ X) {
@@ -2225,7 +2267,9 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   // least 2 elements
   B->gmg = false;
   B->n_lvl = 1;
-  if (ctx->multigrid && B->modal && !own) {
+  // (by default only without a mass term: a mass-dominated system, as in implicit
+  // dynamics, is close to diagonal and the Jacobi loop needs few cheaper iterations)
+  if (B->modal && (ctx->multigrid == 2 || (ctx->multigrid == 1 && !B->mass))) {
     int n_lvl = 1;
     while (n_lvl < ctx->mg_levels) {
       const int nx = m->nx >> (n_lvl - 1), ny = m->ny >> (n_lvl - 1), nz = m->nz >> (n_lvl - 1);
@@ -2330,6 +2374,20 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   return MSG_OK;
 }
 
+// Multigrid: coarsened element fields and the Jacobi diagonal of every coarse
+// level, for all realizations (a realization whose fine field did not change
+// gets the same values again).
+void gmg_fields(Context* ctx, BlockSys* B, cudaStream_t st) {
+  for (int l = 1; l < B->n_lvl; ++l) {
+    GmgLevel& g = B->lv[l];
+    const Lattice& Lf = l == 1 ? B->L : B->lv[l - 1].L;
+    const float* Ef = l == 1 ? B->E32.as<float>() : B->lv[l - 1].E32;
+    k_coarsen_E<<<g.nx * g.ny * g.nz, 128, 0, st>>>(Lf, g.L, g.nx, g.ny, Ef, g.E32);
+    k_dinv<<<g.L.n_int, 128, 0, st>>>(g.L, g.kdiag, g.mdiag, g.E32, g.interior, g.dinv);
+    count_launch(ctx, 2);
+  }
+}
+
 // Field of every realization straight into the padded element layout (FP64
 // and FP32), and the Jacobi diagonal of A.
 int block_field(Context* ctx, Mesh* m, BlockSys* B, const KLDevice* kl, const double* d_xi) {
@@ -2344,15 +2402,7 @@ int block_field(Context* ctx, Mesh* m, BlockSys* B, const KLDevice* kl, const do
   k_dinv<<<B->L.n_int, 128, 0, st>>>(B->L, B->kdiag, B->mdiag, B->E32.as<float>(), B->interior,
                                      B->dinv.as<float>());
   count_launch(ctx, 2);
-  // multigrid: coarsened element fields and the Jacobi diagonal of every level
-  for (int l = 1; l < B->n_lvl; ++l) {
-    GmgLevel& g = B->lv[l];
-    const Lattice& Lf = l == 1 ? B->L : B->lv[l - 1].L;
-    const float* Ef = l == 1 ? B->E32.as<float>() : B->lv[l - 1].E32;
-    k_coarsen_E<<<g.nx * g.ny * g.nz, 128, 0, st>>>(Lf, g.L, g.nx, g.ny, Ef, g.E32);
-    k_dinv<<<g.L.n_int, 128, 0, st>>>(g.L, g.kdiag, g.mdiag, g.E32, g.interior, g.dinv);
-    count_launch(ctx, 2);
-  }
+  gmg_fields(ctx, B, st);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
 }
@@ -2382,7 +2432,7 @@ LoopCfg loop_cfg(Context* ctx, const BlockSys* B, double tol, int chunk_cap) {
   if (B->gmg) {
     // a multigrid iteration cuts the residual several-fold: check every few
     // iterations, replace the residual after a larger drop
-    c.chunk = std::min(c.chunk, 4);
+    c.chunk = 2;
     c.delta2 = ctx->mg_delta * ctx->mg_delta;
   }
   // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
@@ -2439,7 +2489,8 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
     GmgLevel& g = B->lv[l];
     const Lattice& Lf = l == 1 ? B->L : B->lv[l - 1].L;
     const float* tf = l == 1 ? qB : B->lv[l - 1].t;
-    k_restrict<<<g.L.n_int, 128, 0, st>>>(Lf, g.L, g.interior, g.mask, tf, g.dinv, om, g.b, g.x);
+    k_restrict<<<(unsigned)(((long)g.L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(Lf, g.L, g.interior, g.mask,
+                                                                                      tf, g.dinv, om, g.b, g.x);
     if (l < nl - 1)
       lvl(Resid{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
           g.mask, g.b, nullptr, g.t, nullptr, nullptr, nullptr, nullptr, 1);
@@ -2459,12 +2510,14 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   // up: prolongate into the level's iterate, one sweep (result in t)
   for (int l = nl - 2; l >= 1; --l) {
     GmgLevel& g = B->lv[l];
-    k_prolong_add<<<g.L.n_int, 128, 0, st>>>(g.L, B->lv[l + 1].L, g.interior, g.mask, res_c, g.x);
+    k_prolong_add<<<(unsigned)(((long)g.L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(
+        g.L, B->lv[l + 1].L, g.interior, g.mask, res_c, g.x);
     lvl(Smooth{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
         g.mask, g.b, g.dinv, g.t, nullptr, nullptr, nullptr, nullptr, 1);
     res_c = g.t;
   }
-  k_prolong_add<<<B->L.n_int, 128, 0, st>>>(B->L, B->lv[1].L, B->interior, B->mask, res_c, B->xs.as<float>());
+  k_prolong_add<<<(unsigned)(((long)B->L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(
+      B->L, B->lv[1].L, B->interior, B->mask, res_c, B->xs.as<float>());
   // level 0 post-sweep: z (into qB) and the partial z.r'
   lvl(Smooth{}, B->L, B->MC, B->tm_xs, B->tm_xs, B->tm_xs, B->tm_em, B->tm_xs, B->tiles_jm, B->n_tiles_m,
       B->n_items_m, B->grid_m, B->mask, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr, part2 + 1, 2);
@@ -2597,7 +2650,7 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
 // True-residual step (enqueued, not synchronised): x += d + alpha p, d = 0
 // (unless first), r = b - A x in FP64, convergence and search-direction scalars.
 int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, bool b_per_r, double tol, bool first,
-                 int max_it) {
+                 int max_it, bool zero_x = false) {
   const Lattice& L = B->L;
   const int Rp = B->Rp;
   cudaStream_t st = B->X.st;
@@ -2613,6 +2666,16 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
   const float* dinv = B->dinv.as<float>();
   float* r32 = B->r32.as<float>();
   double* part = B->part_op.as<double>();
+  if (zero_x) {
+    // x = 0: r = b, and the partials ||b||^2, (dinv b).b of block_bnorm are the residual's
+    k_b_to_r32<<<c.n_dir, 256, 0, st>>>(L.n_int, Rp, B->interior, b, b_per_r ? 1 : 0, r32);
+    MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
+    k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_bsq, B->part_up.as<double>(), s, tol, first ? 1 : 0,
+                                                 B->gmg ? 2 : (B->modal ? 1 : 0), max_it);
+    count_launch(ctx, 2);
+    MSG_CUDA(ctx, cudaGetLastError());
+    return MSG_OK;
+  }
   if (B->mass) {
     if (b_per_r)
       k_resid<true, true><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
@@ -2672,7 +2735,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
   for (int guard = 0; guard < 1000000; ++guard) {
     if (need_update) {
       cudaEventRecord(ev[0], st);
-      MSG_TRY(block_update(ctx, B, c, b, b_per_r, tol, first, 0x7fffffff));
+      MSG_TRY(block_update(ctx, B, c, b, b_per_r, tol, first, 0x7fffffff, B->gmg && first && !warm));
       cudaEventRecord(ev[1], st);
       MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
       MSG_CUDA(ctx, cudaStreamSynchronize(st));
@@ -3054,6 +3117,7 @@ int lane_cycle(Lane* L, int* state, int* its, double* res, int* n_active) {
     k_dinv_slots<<<B.L.n_int, 128, 0, st>>>(B.L, B.kdiag, B.mdiag, B.E32.as<float>(), B.interior, n,
                                             L->d_slots.as<int>(), B.dinv.as<float>());
     count_launch(ctx, 3);
+    gmg_fields(ctx, &B, st);
     MSG_TRY(block_bnorm(ctx, &B, B.blat.as<double>(), false));
     // the staging buffers are reused by the next cycle: wait for the copies
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
@@ -3080,7 +3144,7 @@ int lane_cycle(Lane* L, int* state, int* its, double* res, int* n_active) {
     MSG_TRY(block_graph(ctx, &B, L->cfg, &g));
     cudaError_t e = cudaGraphLaunch(g, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "lane chunk");
-    count_launch(ctx, (B.modal ? 2 : 5) * L->cfg.chunk);
+    count_launch(ctx, (B.gmg ? gmg_launches(&B) : (B.modal ? 2 : 5)) * L->cfg.chunk);
   }
   return MSG_OK;
 }

@@ -556,7 +556,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
   if (!std::strcmp(key, "modal_operator") && (value == 0 || value == 1)) { ctx->modal = (int)value; return MSG_OK; }
   if (!std::strcmp(key, "fixed_updates") && (value == 0 || value == 1)) { ctx->fixed_updates = (int)value; return MSG_OK; }
-  if (!std::strcmp(key, "multigrid") && (value == 0 || value == 1)) { ctx->multigrid = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "multigrid") && (value == 0 || value == 1 || value == 2)) {
+    ctx->multigrid = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "multigrid_levels") && value >= 2 && value <= kGmgMaxLevels && value == (int)value) {
     ctx->mg_levels = (int)value;
     return MSG_OK;

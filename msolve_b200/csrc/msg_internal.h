@@ -71,11 +71,13 @@ struct Context {
   int modal = 1;                // FP32 operator: 1 = Walsh-mode (modal) kernel, 0 = dense value-class kernel
   int fixed_updates = 0;        // 1: FP64 true-residual step after every graph chunk (batch-invariant results)
   // multigrid preconditioner of the batched lattice solves (modal operator only)
-  int multigrid = 0;            // 1: V-cycle preconditioned loop where the lattice coarsens at least once
-  int mg_levels = 4;            // lattice levels, fine level included (2..kGmgMaxLevels)
-  int mg_sweeps = 10;           // damped Jacobi sweeps on the coarsest level
+  // 1: V-cycle preconditioned loop for systems without a mass term, 2: also with
+  // one, 0: Jacobi loop (the V-cycle needs a lattice that coarsens at least once)
+  int multigrid = 1;
+  int mg_levels = kGmgMaxLevels; // lattice levels at most, fine level included (2..kGmgMaxLevels)
+  int mg_sweeps = 20;           // damped Jacobi sweeps on the coarsest level
   double mg_omega = 0.0;        // Jacobi damping; 0 = from the element stiffness
-  double mg_delta = 1e-3;       // reliable-update factor of the multigrid loop (its residual falls fast)
+  double mg_delta = 1e-2;       // reliable-update factor of the multigrid loop
   // Workspace kept across calls (allocation and cudaFree synchronise the
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
