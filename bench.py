@@ -45,7 +45,8 @@ METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p
 # at R = 512 (dram__bytes_read.sum 1,165.9 MB + dram__bytes_write.sum 845.5 MB) / 512
 OP_DRAM_BYTES_PER_REALIZATION = (1165.921e6 + 845.472e6) / 512
 # the same for the multigrid loop's direction + operator launch (k_lvl_op<PcgZ>), 32^3 lattice
-MG_OP_DRAM_BYTES_PER_REALIZATION = None
+# ncu capture at R = 512: dram__bytes_read.sum 814.4 MB + dram__bytes_write.sum 621.0 MB
+MG_OP_DRAM_BYTES_PER_REALIZATION = (814.429e6 + 620.990e6) / 512
 
 
 def parse():
