@@ -450,14 +450,20 @@ __global__ void __launch_bounds__(kOpThreads, 4)
 // same 4-stage mbarrier ring as the dense operator, and an mbarrier (bounded
 // waits, like every other wait here) in place of a CTA barrier between the
 // element and node phases of a plane.
-struct ModalC {
-  float vd, vb;  // V: a - b, b
-  float sa, sb;  // S: a, b
-  float pa, pb;  // P: a, b
-  float td, tb;  // T: a - b, b
-  float da;      // D
-  float m[8];    // mass per mode (0 when no mass term)
+template <class T> struct ModalCT {
+  T vd, vb;  // V: a - b, b
+  T sa, sb;  // S: a, b
+  T pa, pb;  // P: a, b
+  T td, tb;  // T: a - b, b
+  T da;      // D
+  T m[8];    // mass per mode (0 when no mass term)
 };
+using ModalC = ModalCT<float>;
+using ModalCD = ModalCT<double>;
+
+template <class T> __device__ __forceinline__ T fmx(T a, T b, T c);
+template <> __device__ __forceinline__ float fmx<float>(float a, float b, float c) { return fmaf(a, b, c); }
+template <> __device__ __forceinline__ double fmx<double>(double a, double b, double c) { return fma(a, b, c); }
 
 constexpr int kMJ = 3, kMK = 3;                       // node pencils per tile
 constexpr int kMEJ = kMJ + 1, kMEK = kMK + 1;         // element pencils per tile
@@ -480,11 +486,12 @@ constexpr size_t kMSmem = 128 + sizeof(float) * ((size_t)kMStages * kMStageFloat
 static_assert(kMSmem <= 227 * 1024, "modal operator shared memory");
 
 // yz transform of one plane's 4 nodes u[ay][az] into the modes B[my + 2 mz]
-__device__ __forceinline__ void yz_forward(const float (&u)[2][2][3], float (&B)[3][4]) {
+template <class T>
+__device__ __forceinline__ void yz_forward(const T (&u)[2][2][3], T (&B)[3][4]) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float z00 = u[0][0][c] + u[0][1][c], z01 = u[0][1][c] - u[0][0][c];
-    const float z10 = u[1][0][c] + u[1][1][c], z11 = u[1][1][c] - u[1][0][c];
+    const T z00 = u[0][0][c] + u[0][1][c], z01 = u[0][1][c] - u[0][0][c];
+    const T z10 = u[1][0][c] + u[1][1][c], z11 = u[1][1][c] - u[1][0][c];
     B[c][0] = z00 + z10;
     B[c][1] = z10 - z00;
     B[c][2] = z01 + z11;
@@ -493,11 +500,12 @@ __device__ __forceinline__ void yz_forward(const float (&u)[2][2][3], float (&B)
 }
 
 // inverse of yz_forward up to the factor 4 (the transpose of the same signs)
-__device__ __forceinline__ void yz_inverse(const float (&B)[3][4], float (&y)[2][2][3]) {
+template <class T>
+__device__ __forceinline__ void yz_inverse(const T (&B)[3][4], T (&y)[2][2][3]) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const float a00 = B[c][0] - B[c][1], a10 = B[c][0] + B[c][1];
-    const float a01 = B[c][2] - B[c][3], a11 = B[c][2] + B[c][3];
+    const T a00 = B[c][0] - B[c][1], a10 = B[c][0] + B[c][1];
+    const T a01 = B[c][2] - B[c][3], a11 = B[c][2] + B[c][3];
     y[0][0][c] = a00 - a01;
     y[0][1][c] = a00 + a01;
     y[1][0][c] = a10 - a11;
@@ -508,62 +516,62 @@ __device__ __forceinline__ void yz_inverse(const float (&B)[3][4], float (&y)[2]
 // One element between planes P-1 (yz-modes Bp) and P (Bc): T0 += the part of
 // E Km/64 u (+ mass) that lands on plane P-1, C1 = the part on plane P, both
 // in yz-modes. y0 / y1 hold the element modes with mx = 0 / 1, as [c][my + 2 mz].
-template <bool kMass>
-__device__ __forceinline__ void modal_apply(const ModalC& C, float E, const float (&Bp)[3][4], const float (&Bc)[3][4],
-                                            float (&T0)[3][4], float (&C1)[3][4]) {
-  float y0[3][4], y1[3][4];
+template <bool kMass, class T>
+__device__ __forceinline__ void modal_apply(const ModalCT<T>& C, T E, const T (&Bp)[3][4], const T (&Bc)[3][4],
+                                            T (&T0)[3][4], T (&C1)[3][4]) {
+  T y0[3][4], y1[3][4];
   auto U0 = [&](int q, int c) { return Bc[c][q] + Bp[c][q]; };
   auto U1 = [&](int q, int c) { return Bc[c][q] - Bp[c][q]; };
-  const float Evd = E * C.vd, Evb = E * C.vb, Esa = E * C.sa, Esb = E * C.sb;
-  const float Epa = E * C.pa, Epb = E * C.pb, Etd = E * C.td, Etb = E * C.tb, Eda = E * C.da;
+  const T Evd = E * C.vd, Evb = E * C.vb, Esa = E * C.sa, Esb = E * C.sb;
+  const T Epa = E * C.pa, Epb = E * C.pb, Etd = E * C.td, Etb = E * C.tb, Eda = E * C.da;
   {  // V
-    const float a = U1(0, 0), b = U0(1, 1), c = U0(2, 2);
-    const float t = Evb * (a + b + c);
-    y1[0][0] = fmaf(Evd, a, t);
-    y0[1][1] = fmaf(Evd, b, t);
-    y0[2][2] = fmaf(Evd, c, t);
+    const T a = U1(0, 0), b = U0(1, 1), c = U0(2, 2);
+    const T t = Evb * (a + b + c);
+    y1[0][0] = fmx(Evd, a, t);
+    y0[1][1] = fmx(Evd, b, t);
+    y0[2][2] = fmx(Evd, c, t);
   }
   {  // S
-    float a = U1(0, 1), b = U0(1, 0);
-    y1[1][0] = fmaf(Esa, a, Esb * b);
-    y0[0][1] = fmaf(Esa, b, Esb * a);
+    T a = U1(0, 1), b = U0(1, 0);
+    y1[1][0] = fmx(Esa, a, Esb * b);
+    y0[0][1] = fmx(Esa, b, Esb * a);
     a = U1(0, 2), b = U0(2, 0);
-    y1[2][0] = fmaf(Esa, a, Esb * b);
-    y0[0][2] = fmaf(Esa, b, Esb * a);
+    y1[2][0] = fmx(Esa, a, Esb * b);
+    y0[0][2] = fmx(Esa, b, Esb * a);
     a = U0(1, 2), b = U0(2, 1);
-    y0[2][1] = fmaf(Esa, a, Esb * b);
-    y0[1][2] = fmaf(Esa, b, Esb * a);
+    y0[2][1] = fmx(Esa, a, Esb * b);
+    y0[1][2] = fmx(Esa, b, Esb * a);
   }
   {  // P
-    float a = U1(1, 0), b = U0(3, 2);
-    y1[0][1] = fmaf(Epa, a, Epb * b);
-    y0[2][3] = fmaf(Epa, b, Epb * a);
+    T a = U1(1, 0), b = U0(3, 2);
+    y1[0][1] = fmx(Epa, a, Epb * b);
+    y0[2][3] = fmx(Epa, b, Epb * a);
     a = U1(1, 1), b = U1(2, 2);
-    y1[1][1] = fmaf(Epa, a, Epb * b);
-    y1[2][2] = fmaf(Epa, b, Epb * a);
+    y1[1][1] = fmx(Epa, a, Epb * b);
+    y1[2][2] = fmx(Epa, b, Epb * a);
     a = U1(2, 0), b = U0(3, 1);
-    y1[0][2] = fmaf(Epa, a, Epb * b);
-    y0[1][3] = fmaf(Epa, b, Epb * a);
+    y1[0][2] = fmx(Epa, a, Epb * b);
+    y0[1][3] = fmx(Epa, b, Epb * a);
   }
   {  // T
-    const float a = U1(1, 2), b = U1(2, 1), c = U0(3, 0);
-    const float t = Etb * (a + b + c);
-    y1[2][1] = fmaf(Etd, a, t);
-    y1[1][2] = fmaf(Etd, b, t);
-    y0[0][3] = fmaf(Etd, c, t);
+    const T a = U1(1, 2), b = U1(2, 1), c = U0(3, 0);
+    const T t = Etb * (a + b + c);
+    y1[2][1] = fmx(Etd, a, t);
+    y1[1][2] = fmx(Etd, b, t);
+    y0[0][3] = fmx(Etd, c, t);
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {  // D and the null modes
     y1[c][3] = Eda * U1(3, c);
-    y0[c][0] = 0.f;
+    y0[c][0] = T(0);
   }
   if constexpr (kMass) {
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        y0[c][q] = fmaf(C.m[2 * q], U0(q, c), y0[c][q]);
-        y1[c][q] = fmaf(C.m[2 * q + 1], U1(q, c), y1[c][q]);
+        y0[c][q] = fmx(C.m[2 * q], U0(q, c), y0[c][q]);
+        y1[c][q] = fmx(C.m[2 * q + 1], U1(q, c), y1[c][q]);
       }
   }
 #pragma unroll
@@ -1055,6 +1063,233 @@ __global__ void __launch_bounds__(kMThreads, 1)
         for (int i = 0; i < kMJ * kMK; ++i) sum += red[i * 32 + lane];
         partial[((size_t)tile * Rp + rr) * pstride] = sum;
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- FP64 true residual (Walsh modes)
+// The reliable-update step of the batched loops in one pass: with kUpdate the
+// corner input is x + d + alpha p (the FP32 correction folded into the FP64
+// iterate; the owner writes the new x into the other x buffer; d is cleared
+// after the launch, since neighbouring tiles read it in their halos), otherwise x; then r = b - A x in FP64 with the Walsh-mode operator (mass term
+// with kMass), masked, r32 = (float) r, and the per-realization partials
+// ||r||^2, dinv r32.r32 ([tile][Rp][2], the layout of k_resid). A CTA owns a
+// 2 x 2 tile of node pencils (9 element warps + 1 TMA producer warp: FP64
+// element state needs about twice the registers of the FP32 operator);
+// staging, exchange and bounded waits as k_op_modal.
+constexpr int kRJ = 2, kRK = 2;
+constexpr int kREJ = kRJ + 1, kREK = kRK + 1, kRWarps = kREJ * kREK;
+constexpr int kRPJ = kRJ + 2, kRPK = kRK + 2;
+constexpr int kRThreads = 32 * (kRWarps + 1);
+constexpr int kRPatch = 32 * 3 * kRPJ * kRPK;          // values of a vector patch (1536)
+constexpr int kREPatch = 32 * kREJ * kREK;             // E patch (288 doubles)
+constexpr uint32_t kROffX = 0, kROffD = 8 * kRPatch, kROffP = kROffD + 4 * kRPatch, kROffE = kROffP + 4 * kRPatch;
+constexpr uint32_t kRStageBytes = kROffE + 8 * kREPatch;  // 26,880 bytes
+constexpr int kRStages = 4;
+constexpr int kRXDoubles = kRWarps * 4 * 3 * 32;        // exchange buffer (doubles)
+constexpr size_t kRSmem = 128 + (size_t)kRStages * kRStageBytes + 2 * sizeof(double) * kRXDoubles +
+                          sizeof(double) * 2 * kRJ * kRK * 32 + sizeof(uint64_t) * (2 * kRStages);
+static_assert(kRStageBytes % 128 == 0 && kROffD % 128 == 0 && kROffP % 128 == 0 && kROffE % 128 == 0, "align");
+static_assert(kRSmem <= 227 * 1024, "FP64 residual shared memory");
+
+template <bool kMass, bool kBPerR, bool kUpdate>
+__global__ void __launch_bounds__(kRThreads, 1)
+    k_resid_modal(Lattice L, const __grid_constant__ ModalCD C, const __grid_constant__ CUtensorMap tm_x,
+                  const __grid_constant__ CUtensorMap tm_d, const __grid_constant__ CUtensorMap tm_p,
+                  const __grid_constant__ CUtensorMap tm_e, int tiles_j, int n_tiles, int n_items,
+                  const uint8_t* __restrict__ mask, const double* __restrict__ b, const float* __restrict__ dinv,
+                  const float* __restrict__ alpha, double* __restrict__ x_out, float* __restrict__ r32,
+                  double* __restrict__ partial, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  double* xbuf = reinterpret_cast<double*>(smem + (size_t)kRStages * kRStageBytes);
+  double* red = xbuf + 2 * kRXDoubles;  // [2][node pencils][32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + 2 * kRJ * kRK * 32);
+  uint64_t* empty = full + kRStages;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int NX = L.NX, Rp = L.Rp;
+  constexpr uint32_t kBytes = kUpdate ? kRStageBytes : (8 * kRPatch + 8 * kREPatch);
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kRStages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kRWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (w == kRWarps) {
+    if (lane == 0) {
+      uint32_t seq = 0;
+      for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+        const int J0 = 1 + (tile % tiles_j) * kRJ, K0 = 1 + (tile / tiles_j) * kRK;
+        for (int P = 1; P <= NX; ++P, ++seq) {
+          const int st = seq % kRStages;
+          const uint32_t use = seq / kRStages;
+          if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+            atomicExch(err, 1);
+            return;
+          }
+          unsigned char* dst = smem + (size_t)st * kRStageBytes;
+          mbar_expect_tx(&full[st], kBytes);
+          tma_load_5d(dst + kROffX, &tm_x, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          if constexpr (kUpdate) {
+            tma_load_5d(dst + kROffD, &tm_d, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+            tma_load_5d(dst + kROffP, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          }
+          tma_load_4d(dst + (kUpdate ? kROffE : 8 * kRPatch), &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+        }
+      }
+    }
+    return;
+  }
+  const int ej = w % kREJ, ek = w / kREJ;
+  const bool node_warp = ej >= 1 && ek >= 1;
+  uint32_t seq = 0;
+  int xsel = 0;
+  bool dead = false;
+  auto csync = [&]() { asm volatile("bar.sync 1, %0;" ::"r"(kRWarps * 32) : "memory"); };
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+    const int J0 = 1 + (tile % tiles_j) * kRJ, K0 = 1 + (tile / tiles_j) * kRK;
+    const int Je = J0 - 1 + ej, Ke = K0 - 1 + ek;
+    auto realj = [&](int j) { return j >= 1 && j <= L.NY - 1; };
+    auto realk = [&](int k) { return k >= 1 && k <= L.NZ - 1; };
+    const bool real = realj(Je) && realk(Ke);
+    const bool node_ok = node_warp && Je <= L.NY && Ke <= L.NZ;
+    const bool r00 = real, r10 = realj(Je - 1) && realk(Ke);
+    const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
+    const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;
+    const int rr = g32 + lane;
+    double al = 0.0;
+    if constexpr (kUpdate) al = (double)alpha[rr];
+    double Bp[3][4], T0[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) T0[c][qq] = 0.0;
+    double acc_rr = 0.0, acc_dz = 0.0;
+    uint32_t mreg = 0;
+    // b and dinv of the node the next node phase completes, loaded one plane
+    // ahead so that their latency hides behind the element work
+    double nb[3] = {0.0, 0.0, 0.0};
+    float ndv = 0.f;
+    auto prefetch = [&](int X) {
+      if (!node_ok) return;
+      const size_t node = nrow + X;
+      ndv = dinv[node * Rp + rr];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nb[c] = kBPerR ? b[(node * 3 + c) * Rp + rr] : b[node * 3 + c];
+    };
+    auto node_phase = [&](int X) {
+      if (((X - 1) & 31) == 0) {
+        const int pl = X + lane;
+        mreg = (pl <= NX) ? mask[nrow + pl] : 0u;
+      }
+      const uint32_t mk = __shfl_sync(0xffffffffu, mreg, (X - 1) & 31);
+      const double* xb = xbuf + xsel * kRXDoubles;
+      const size_t node = nrow + X;
+      const double dv = (double)ndv;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double y = 0.0;
+        if (r00) y += xb[((w * 4 + 0) * 3 + c) * 32 + lane];
+        if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
+        if (r01) y += xb[(((w - kREJ) * 4 + 2) * 3 + c) * 32 + lane];
+        if (r11) y += xb[(((w - kREJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        const size_t o = (node * 3 + c) * Rp + rr;
+        const double bv = nb[c];
+        const double rc = ((mk >> c) & 1) ? 0.0 : bv - y;
+        const float rf = (float)rc;
+        r32[o] = rf;
+        acc_rr = fma(rc, rc, acc_rr);
+        acc_dz = fma(dv * (double)rf, (double)rf, acc_dz);
+      }
+    };
+    auto emit_corners = [&](const double (&B)[3][4]) {
+      double y[2][2][3];
+      yz_inverse(B, y);
+      double* xb = xbuf + xsel * kRXDoubles;
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
+    };
+    for (int P = 1; P <= NX; ++P, ++seq) {
+      const int st = seq % kRStages;
+      if (!dead && !mbar_wait(&full[st], (seq / kRStages) & 1)) {
+        atomicExch(err, 1);
+        dead = true;
+      }
+      if (P >= 2) prefetch(P - 1);
+      const unsigned char* pt = smem + (size_t)st * kRStageBytes;
+      const double* px = reinterpret_cast<const double*>(pt + kROffX);
+      const float* pd = reinterpret_cast<const float*>(pt + kROffD);
+      const float* pp = reinterpret_cast<const float*>(pt + kROffP);
+      const double* pe = reinterpret_cast<const double*>(pt + (kUpdate ? kROffE : 8 * kRPatch));
+      double u[2][2][3];
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az) {
+          const int o = (ek + az) * kRPJ + (ej + ay);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int i = (o * 3 + c) * 32 + lane;
+            double v = px[i];
+            if constexpr (kUpdate) v += (double)pd[i] + al * (double)pp[i];
+            u[ay][az][c] = v;
+          }
+        }
+      const double E = pe[w * 32 + lane];
+      if constexpr (kUpdate) {
+        if (node_ok) {
+          const size_t node = nrow + P;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) x_out[(node * 3 + c) * Rp + rr] = u[0][0][c];
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      double Bc[3][4];
+      yz_forward(u, Bc);
+      if (P >= 2) {
+        if (real) {
+          double C1[3][4];
+          modal_apply<kMass>(C, E, Bp, Bc, T0, C1);
+          emit_corners(T0);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
+        }
+        csync();
+        if (node_ok) node_phase(P - 1);
+        xsel ^= 1;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) Bp[c][qq] = Bc[c][qq];
+    }
+    prefetch(NX);
+    if (real) emit_corners(T0);
+    csync();
+    if (node_ok) node_phase(NX);
+    xsel ^= 1;
+    if (node_warp) {
+      const int nw = (ek - 1) * kRJ + (ej - 1);
+      red[(0 * kRJ * kRK + nw) * 32 + lane] = acc_rr;
+      red[(1 * kRJ * kRK + nw) * 32 + lane] = acc_dz;
+    }
+    csync();
+    if (w < 2) {
+      double sum = 0.0;
+#pragma unroll
+      for (int i = 0; i < kRJ * kRK; ++i) sum += red[(w * kRJ * kRK + i) * 32 + lane];
+      partial[((size_t)tile * Rp + rr) * 2 + w] = sum;
     }
   }
 }
@@ -1858,7 +2093,8 @@ __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __re
 // T = s (x) I3. Fills the block coefficients of cK * Khat / 64 (and the
 // diagonal of cM * Mhat / 64 when M576 is given) and checks that every other
 // entry vanishes, so the modal operator reproduces the element matrices.
-int modal_coefficients(Context* ctx, const double* K576, const double* M576, double cK, double cM, ModalC* out) {
+int modal_coefficients(Context* ctx, const double* K576, const double* M576, double cK, double cM, ModalC* out,
+                       ModalCD* out64 = nullptr) {
   auto sgn = [](int a, int m) {  // s(a, m) for corner id a and mode m
     const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
     int s = 1;
@@ -1920,6 +2156,18 @@ int modal_coefficients(Context* ctx, const double* K576, const double* M576, dou
   out->tb = (float)(tb * f);
   out->da = (float)(da * f);
   for (int m = 0; m < 8; ++m) out->m[m] = 0.f;
+  if (out64) {
+    out64->vd = (va - vb) * f;
+    out64->vb = vb * f;
+    out64->sa = sa * f;
+    out64->sb = sb * f;
+    out64->pa = pa * f;
+    out64->pb = pb * f;
+    out64->td = (ta - tb) * f;
+    out64->tb = tb * f;
+    out64->da = da * f;
+    for (int m = 0; m < 8; ++m) out64->m[m] = 0.0;
+  }
   if (M576) {
     std::vector<double> Mm;
     to_modal(M576, Mm);
@@ -1933,6 +2181,8 @@ int modal_coefficients(Context* ctx, const double* K576, const double* M576, dou
     if (!(mdev <= 1e-11 * mmax))
       return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "element mass lacks the cube's modal structure (%g)", mdev / mmax);
     for (int m = 0; m < 8; ++m) out->m[m] = (float)(Mm[(3 * m) * 24 + 3 * m] * cM / 64.0);
+    if (out64)
+      for (int m = 0; m < 8; ++m) out64->m[m] = Mm[(3 * m) * 24 + 3 * m] * cM / 64.0;
   }
   return MSG_OK;
 }
@@ -1974,7 +2224,7 @@ struct GmgLevel {
 
 struct BlockSys {
   BlockExec X;
-  DevMem* own = nullptr;  // 32 buffers owned by a serving lane; nullptr: the context's workspace slots
+  DevMem* own = nullptr;  // kWorkSlots buffers owned by a serving lane; nullptr: the context's workspace slots
   bool fixed = false;     // true-residual step after every graph chunk (batch-invariant trajectories)
   Lattice L;
   int R = 0, Rp = 0;
@@ -2001,6 +2251,12 @@ struct BlockSys {
     return MSG_OK;
   }
   CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
+  // FP64 Walsh-mode true-residual step (modal loops): the iterate alternates
+  // between x and xB (the step writes x + d + alpha p into the other buffer)
+  WSlot xB;
+  ModalCD MCD;
+  int n_items_r = 0, grid_r = 0;
+  CUtensorMap tm_xr, tm_xBr, tm_dr, tm_pr, tm_er;
   // multigrid preconditioner: levels 1..n_lvl-1 (level 0 is this lattice), the
   // level-0 pre-smoothed iterate xs, the damping and the coarsest-level sweeps
   bool gmg = false;
@@ -2148,7 +2404,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
     for (int i = 0; i < 4; ++i) B->MD.v[i] = cM * rep[i];
     B->mdiag = cM * rep[0];
   }
-  if (B->modal) MSG_TRY(modal_coefficients(ctx, K576, B->mass ? M576 : nullptr, cK, cM, &B->MC));
+  if (B->modal) MSG_TRY(modal_coefficients(ctx, K576, B->mass ? M576 : nullptr, cK, cM, &B->MC, &B->MCD));
   B->tiles_jm = (L.NY + kMJ - 1) / kMJ;
   B->n_tiles_m = B->tiles_jm * ((L.NZ + kMK - 1) / kMK);
   B->n_items_m = B->n_tiles_m * (Rp / 32);
@@ -2172,10 +2428,12 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   MSG_TRY(B->slot_alloc(ctx, 10, sizeof(double) * (size_t)std::max(B->n_upd, B->n_bsq) * Rp * 2, &B->part_up.ptr));
   B->scal_bytes = (sizeof(float) * 2 + sizeof(double) * 6 + sizeof(int) * 5) * (size_t)Rp + 64;
   MSG_TRY(B->slot_alloc(ctx, 11, B->scal_bytes, &B->scal.ptr));
-  if (B->modal) {  // second buffers of p, r and q for the single-reduction loop
+  if (B->modal) {  // second buffers of p, r and q for the single-reduction loop, and of x
     MSG_TRY(B->slot_alloc(ctx, 18, sizeof(float) * nvec, &B->pB.ptr));
     MSG_TRY(B->slot_alloc(ctx, 19, sizeof(float) * nvec, &B->rB.ptr));
     MSG_TRY(B->slot_alloc(ctx, 20, sizeof(float) * nvec, &B->qB.ptr));
+    MSG_TRY(B->slot_alloc(ctx, 32, sizeof(double) * nvec, &B->xB.ptr));
+    MSG_CUDA(ctx, cudaMemsetAsync(B->xB.ptr, 0, sizeof(double) * nvec, st));
   }
   Scal& sc = B->s;
   {
@@ -2247,6 +2505,42 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
                             enc5(&B->tm_dm, B->d.ptr, dbm)};
     for (CUresult r : rs)
       if (r != CUDA_SUCCESS) e = r;
+    // FP64 true-residual step: x (both buffers, FP64), d and p (FP32) patches
+    // of a 2 x 2 node tile with halo, the FP64 element patch
+    {
+      const cuuint64_t db = sizeof(double);
+      const cuuint64_t ps64[4] = {Rp * db, 3 * Rp * db, 3 * Rp * db * L.NXp, 3 * Rp * db * L.NXp * L.NYp};
+      const cuuint64_t es64[3] = {Rp * db, Rp * db * L.NXp, Rp * db * L.NXp * L.NYp};
+      const cuuint32_t rbox[5] = {32, 3, 1, kRPJ, kRPK};
+      const cuuint32_t rebox[4] = {32, 1, kREJ, kREK};
+      auto enc64 = [&](CUtensorMap* tm, void* base) {
+        return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, base, pd, ps64, rbox, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      };
+      const CUresult r64[5] = {
+          enc64(&B->tm_xr, B->x.ptr), enc64(&B->tm_xBr, B->xB.ptr), enc5(&B->tm_dr, B->d.ptr, rbox),
+          enc5(&B->tm_pr, B->p.ptr, rbox),
+          encode(&B->tm_er, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, B->E64.ptr, ed, es64, rebox, one,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)};
+      for (CUresult r : r64)
+        if (r != CUDA_SUCCESS) e = r;
+      B->n_items_r = B->n_tiles * (Rp / 32);
+      B->grid_r = std::min(B->n_items_r, ctx->sm_count);
+    }
+    static std::once_flag resid_once;
+    static cudaError_t resid_err = cudaSuccess;
+    std::call_once(resid_once, [] {
+      const void* fs[] = {(const void*)k_resid_modal<false, false, false>, (const void*)k_resid_modal<false, false, true>,
+                          (const void*)k_resid_modal<false, true, false>,  (const void*)k_resid_modal<false, true, true>,
+                          (const void*)k_resid_modal<true, false, false>,  (const void*)k_resid_modal<true, false, true>,
+                          (const void*)k_resid_modal<true, true, false>,   (const void*)k_resid_modal<true, true, true>};
+      for (const void* f : fs)
+        if (resid_err == cudaSuccess)
+          resid_err = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRSmem);
+    });
+    MSG_CUDA(ctx, resid_err);
     static std::once_flag attr_once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(attr_once, [] {
@@ -2656,7 +2950,7 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
   cudaStream_t st = B->X.st;
   Scal& s = B->s;
   const uint8_t* mask = B->mask;
-  if (!first) {
+  if (!first && !B->modal) {
     k_xupdate<<<c.n_xu, 256, 0, st>>>(L.n_int, Rp, B->interior, s.alpha, B->p.as<float>(), B->x.as<double>(),
                                       B->d.as<float>());
     count_launch(ctx);
@@ -2676,7 +2970,27 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
     MSG_CUDA(ctx, cudaGetLastError());
     return MSG_OK;
   }
-  if (B->mass) {
+  if (B->modal) {
+    // x += d + alpha p (into the other x buffer) and the FP64 residual in one pass
+    auto pick = [&](auto M, auto P, auto U) {
+      return k_resid_modal<decltype(M)::value, decltype(P)::value, decltype(U)::value>;
+    };
+    using T1 = std::true_type;
+    using F0 = std::false_type;
+    const bool upd = !first;
+    auto k = B->mass ? (b_per_r ? (upd ? pick(T1{}, T1{}, T1{}) : pick(T1{}, T1{}, F0{}))
+                                : (upd ? pick(T1{}, F0{}, T1{}) : pick(T1{}, F0{}, F0{})))
+                     : (b_per_r ? (upd ? pick(F0{}, T1{}, T1{}) : pick(F0{}, T1{}, F0{}))
+                                : (upd ? pick(F0{}, F0{}, T1{}) : pick(F0{}, F0{}, F0{})));
+    k<<<B->grid_r, kRThreads, kRSmem, st>>>(L, B->MCD, B->tm_xr, B->tm_dr, B->tm_pr, B->tm_er, L.tiles_j, B->n_tiles,
+                                             B->n_items_r, mask, b, dinv, s.alpha, B->xB.as<double>(), r32, part,
+                                             s.err);
+    if (upd) {
+      MSG_CUDA(ctx, cudaMemsetAsync(B->d.ptr, 0, sizeof(float) * B->nvec, st));
+      std::swap(B->x.ptr, B->xB.ptr);
+      std::swap(B->tm_xr, B->tm_xBr);
+    }
+  } else if (B->mass) {
     if (b_per_r)
       k_resid<true, true><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
     else
@@ -2984,7 +3298,7 @@ struct Lane {
   Context* ctx = nullptr;
   Mesh* m = nullptr;
   BlockSys B;
-  DevMem own[32];
+  DevMem own[kWorkSlots];
   DevMem psi, d_xi, d_slots, d_col;
   KLDevice kd;
   cudaStream_t st = nullptr;

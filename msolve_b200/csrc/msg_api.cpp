@@ -85,7 +85,7 @@ int context_resources(Context* ctx) {
 }
 
 int workspace(Context* ctx, int slot, size_t bytes, void** out) {
-  if (slot < 0 || slot >= 32) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "workspace slot");
+  if (slot < 0 || slot >= kWorkSlots) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "workspace slot");
   DevMem*& w = ctx->work[slot];
   if (!w) w = new DevMem();
   if (w->bytes < bytes) MSG_TRY(w->alloc(ctx, bytes));

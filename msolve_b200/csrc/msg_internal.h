@@ -29,6 +29,7 @@ __host__ __device__ constexpr int corner_id(int ax, int ay, int az) {
 }
 
 constexpr int kGmgMaxLevels = 6;  // multigrid lattice levels at most (fine level included)
+constexpr int kWorkSlots = 40;    // context workspace slots (see workspace())
 
 struct Context;
 
@@ -81,7 +82,7 @@ struct Context {
   // Workspace kept across calls (allocation and cudaFree synchronise the
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
-  DevMem* work[32] = {nullptr};
+  DevMem* work[kWorkSlots] = {nullptr};
   // per-context host/driver resources reused by every batch (created lazily)
   int* h_flags = nullptr;           // 64 bytes of pinned host memory
   cudaEvent_t ev[12] = {nullptr};   // timing events
