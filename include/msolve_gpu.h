@@ -80,6 +80,27 @@ int MSG_H8_KE_BATCH(MSG_CTX ctx, int n, const double* xyz, const double* E, doub
  * (ISAAR.MSolve.PreProcessor/Elements/Hexa8.cs:403-435): xyz [n][8][3], Me [n][300]. */
 int MSG_H8_ME_BATCH(MSG_CTX ctx, int n, const double* xyz, double rho, double* Me);
 
+/* Batched stress recovery, Hexa8.CalculateStresses + Hexa8.CalculateForces
+ * (ISAAR.MSolve.PreProcessor/Elements/Hexa8.cs:453-510) over CALCH8STRAINS and
+ * CALCH8FORCES (FEMElements/FEMElements/rElHexa8.f90:636-648, 724-747) with the
+ * elastic material (ElasticMaterial3D.cs:20-44, 75-81): per element and 2x2x2
+ * Gauss point (xi outer, zeta inner) strains = B u (exx, eyy, ezz, gxy, gyz,
+ * gzx), stresses = D(E, nu) B du (the material stores the strain increment),
+ * and internal forces = sum_gp w B^T stresses (24). xyz [n][8][3], E [n],
+ * u [n][24], du [n][24] (NULL: du = u). Outputs (each may be NULL): strains,
+ * stresses [n][8][6], forces [n][24]. MSG_ERR_NEG_DET as MSG_H8_KE_BATCH. */
+int MSG_H8_STRESS_BATCH(MSG_CTX ctx, int n, const double* xyz, const double* E, double nu, const double* u,
+                        const double* du, double* strains, double* stresses, double* forces);
+/* The same for every element of the mesh and every realization of a batch, on
+ * the device: E_dev [R][n_elems] (MSG_KL_FIELD layout), X_dev [R][n_dofs] (the
+ * solutions of MSG_MC_SOLVE_BATCH_DEVICE; constrained DOFs are 0), du = u.
+ * Outputs (device, each may be NULL): strains_dev, stresses_dev
+ * [R][n_elems][8][6], forces_dev [R][n_elems][24]. The reference's stochastic
+ * material reports zero stresses (StochasticElasticMaterial3D.cs:75); this
+ * returns the elastic stresses of each realization's field. */
+int MSG_STRESS_BATCH_DEVICE(MSG_MESH mesh, int R, const double* E_dev, double nu, const double* X_dev,
+                            double* strains_dev, double* stresses_dev, double* forces_dev);
+
 /* ------------------------------------------------------------------ mesh */
 /* Upload a Hexa8 mesh: xyz [n_nodes][3], conn [n_elems][8] (0-based node
  * indices), dof [n_nodes][3] (free DOF number or -1 if constrained, the
@@ -187,9 +208,11 @@ int MSG_KL_FIELD(MSG_MESH mesh, const MSG_KL* kl, int R, const double* xi, doubl
  *   mode MSG_MODE_FP64_BSR: realizations one after another, FP64 BSR + Jacobi PCG
  *     (recursive-residual stop as MSG_PCG_SOLVE).
  *   mode MSG_MODE_MIXED_BATCHED: all realizations in one batch on a structured
- *     cube lattice: matrix-free FP32 element-by-element operator inside
- *     Jacobi-PCG, FP64 true residual r = b - K x and FP64 solution update
- *     (iterative refinement); stop when ||b - K x||/||b|| < tol in FP64.
+ *     cube lattice: matrix-free FP32 element-by-element operator inside PCG
+ *     (per-realization geometric multigrid V-cycle preconditioner by default,
+ *     Jacobi with MSG_SET_OPTION "multigrid" = 0), FP64 true residual
+ *     r = b - K x and FP64 solution update (iterative refinement); stop when
+ *     ||b - K x||/||b|| < tol in FP64.
  * xi [R][kl->n_terms], b [n_dofs]. Outputs (each may be NULL): X [R][n_dofs],
  * tip [R] = X[r][tip_dof], iterations [R] (matrix products per realization),
  * rel_res [R] (final FP64 ||b - K x||/||b||). */

@@ -121,6 +121,44 @@ def h8_mass_batch(ctx, xyz, rho):
     return M
 
 
+def h8_stress_batch(ctx, xyz, E, nu, u, du=None):
+    """MSG_H8_STRESS_BATCH: Hexa8.CalculateStresses + CalculateForces for n
+    elements: strains and stresses [n][8][6] at the Gauss points, internal forces
+    [n][24] (stresses from the increment du; du = u when omitted)."""
+    xyz = N.f64(xyz).reshape(-1, 24)
+    n = xyz.shape[0]
+    E = N.f64(np.broadcast_to(np.asarray(E, dtype=np.float64), (n,)))
+    u = N.f64(u).reshape(n, 24)
+    du = None if du is None else N.f64(du).reshape(n, 24)
+    eps, sig, f = np.zeros((n, 8, 6)), np.zeros((n, 8, 6)), np.zeros((n, 24))
+    N.check(N.lib().MSG_H8_STRESS_BATCH(ctx.handle, n, N.ptr(xyz), N.ptr(E), float(nu), N.ptr(u),
+                                        None if du is None else N.ptr(du), N.ptr(eps), N.ptr(sig), N.ptr(f)),
+            ctx.handle, "MSG_H8_STRESS_BATCH")
+    return eps, sig, f
+
+
+def realization_stresses(mesh, E, nu, X, strains=True, stresses=True, forces=True):
+    """MSG_STRESS_BATCH_DEVICE: stress recovery of every element of every
+    realization on the device. E [R][n_elems] and X [R][n_dofs] are CUDA
+    float64 tensors (the KL field and the batch solutions); returns CUDA
+    tensors strains, stresses [R][n_elems][8][6] and forces [R][n_elems][24]
+    (None where not requested)."""
+    import torch
+    R = int(X.shape[0])
+    ne = mesh.model.n_elems
+    assert E.is_cuda and X.is_cuda and E.dtype == torch.float64 and X.dtype == torch.float64
+    E = E.contiguous()
+    X = X.contiguous()
+    out = [torch.empty((R, ne, 8, 6), dtype=torch.float64, device=X.device) if strains else None,
+           torch.empty((R, ne, 8, 6), dtype=torch.float64, device=X.device) if stresses else None,
+           torch.empty((R, ne, 24), dtype=torch.float64, device=X.device) if forces else None]
+    ptrs = [C.c_void_p(t.data_ptr()) if t is not None else None for t in out]
+    N.check(N.lib().MSG_STRESS_BATCH_DEVICE(mesh.handle, R, C.c_void_p(E.data_ptr()), float(nu),
+                                            C.c_void_p(X.data_ptr()), *ptrs), mesh.ctx.handle,
+            "MSG_STRESS_BATCH_DEVICE")
+    return tuple(out)
+
+
 class ProblemStructural:
     """IStaticProvider: builds the global stiffness on the device
     (ProblemStructural.BuildKs / CalculateMatrix, ProblemStructural.cs:63-89, 217-221)."""

@@ -185,6 +185,132 @@ __global__ void __launch_bounds__(kThreads) k_h8_me(int n, const double* __restr
   }
 }
 
+// Strain / stress recovery and internal forces of a batch of element
+// instances (an instance = one element of one realization), the device twin
+// of Hexa8.CalculateStresses + CalculateForces (ISAAR.MSolve.PreProcessor/
+// Elements/Hexa8.cs:453-510) over CalcH8Strains and CalcH8Forces
+// (FEMElements/FEMElements/rElHexa8.f90:636-648, 724-747) with the elastic
+// material update (ElasticMaterial3D.cs:20-44, 75-81: the stored strain is the
+// increment, stresses = D * increment). Per Gauss point m: strains = B_m u,
+// stresses = D(E) B_m du; forces = sum_m w_m B_m^T stresses_m. Sums follow the
+// reference's order (24 columns of B; 6 columns of D; 6 rows of B^T; Gauss
+// points xi outer, zeta inner). The displacements come from an instance array
+// u [n][24] or are gathered from a realization batch X [R][n_dofs] through
+// the connectivity and the DOF map (constrained DOFs: 0).
+struct StressIn {
+  const double* xyz;   // [n_e][24]
+  const double* E;     // [n] or nullptr (E_scalar)
+  double E_scalar, nu;
+  const double* u;     // [n][24] or nullptr (gather from X)
+  const double* du;    // [n][24] or nullptr (du = u)
+  const double* X;     // [R][n_dofs]
+  const int* conn;     // [n_e][8]
+  const int* dof;      // [n_nodes][3]
+  int n_e, n_dofs;
+};
+
+struct StressShared {
+  double dx[kEPB][8][8][3];
+  double w[kEPB][8];
+  double sig[kEPB][8][6];
+};
+
+__global__ void __launch_bounds__(kThreads) k_h8_stress(int n, StressIn in, double* __restrict__ strains,
+                                                        double* __restrict__ stresses, double* __restrict__ forces,
+                                                        int* __restrict__ status) {
+  __shared__ StressShared g;
+  const int i0 = blockIdx.x * kEPB;
+  const int t = threadIdx.x;
+  if (t < kEPB * 8) {
+    const int le = t >> 3, gp = t & 7, i = i0 + le;
+    if (i < n) {
+      const int e = i % in.n_e;
+      const size_t r = (size_t)(i / in.n_e);
+      double x[24];
+#pragma unroll
+      for (int k = 0; k < 24; ++k) x[k] = in.xyz[(size_t)e * 24 + k];
+      gauss_point(x, gp, &g.dx[le][gp][0][0], &g.w[le][gp], nullptr, status);
+      double u[24], du[24];
+      if (in.u) {
+#pragma unroll
+        for (int k = 0; k < 24; ++k) u[k] = in.u[(size_t)i * 24 + k];
+      } else {
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+          const int node = in.conn[(size_t)e * 8 + a];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int d = in.dof[(size_t)node * 3 + c];
+            u[3 * a + c] = d >= 0 ? in.X[r * in.n_dofs + d] : 0.0;
+          }
+        }
+      }
+      if (in.du) {
+#pragma unroll
+        for (int k = 0; k < 24; ++k) du[k] = in.du[(size_t)i * 24 + k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 24; ++k) du[k] = u[k];
+      }
+      const double* dx = &g.dx[le][gp][0][0];
+      // CalcH8Strains: MatMul(B, u) row by row over the 24 columns
+      double eps[6], deps[6];
+#pragma unroll
+      for (int row = 0; row < 6; ++row) {
+        double s = 0.0, sd = 0.0;
+#pragma unroll
+        for (int col = 0; col < 24; ++col) {
+          double B6[6];
+          b_column(dx + 3 * (col / 3), col % 3, B6);
+          s = s + B6[row] * u[col];
+          sd = sd + B6[row] * du[col];
+        }
+        eps[row] = s;
+        deps[row] = sd;
+      }
+      // ElasticMaterial3D: stresses = D * (strain increment), row by row over 6 columns
+      const double E = in.E ? in.E[i] : in.E_scalar;
+      const double e1 = E / (1.0 + in.nu);
+      const double e2 = e1 * in.nu / (1.0 - 2.0 * in.nu);
+      const double D[6][6] = {{e1 + e2, e2, e2, 0, 0, 0}, {e2, e1 + e2, e2, 0, 0, 0}, {e2, e2, e1 + e2, 0, 0, 0},
+                              {0, 0, 0, e1 * 0.5, 0, 0},   {0, 0, 0, 0, e1 * 0.5, 0},   {0, 0, 0, 0, 0, e1 * 0.5}};
+      double sig[6];
+#pragma unroll
+      for (int row = 0; row < 6; ++row) {
+        double s = 0.0;
+#pragma unroll
+        for (int col = 0; col < 6; ++col) s = s + D[row][col] * deps[col];
+        sig[row] = s;
+        g.sig[le][gp][row] = s;
+      }
+      if (strains)
+#pragma unroll
+        for (int row = 0; row < 6; ++row) strains[((size_t)i * 8 + gp) * 6 + row] = eps[row];
+      if (stresses)
+#pragma unroll
+        for (int row = 0; row < 6; ++row) stresses[((size_t)i * 8 + gp) * 6 + row] = sig[row];
+    }
+  }
+  __syncthreads();
+  if (!forces) return;
+  // CalcH8Forces: forces = forces + w_m * MatMul(Transpose(B_m), stresses_m), m in Gauss order
+  for (int q = t; q < kEPB * 24; q += kThreads) {
+    const int le = q / 24, col = q - le * 24, i = i0 + le;
+    if (i >= n) break;
+    double f = 0.0;
+#pragma unroll 1
+    for (int gp = 0; gp < 8; ++gp) {
+      double B6[6];
+      b_column(&g.dx[le][gp][col / 3][0], col % 3, B6);
+      double s = 0.0;
+#pragma unroll
+      for (int row = 0; row < 6; ++row) s = s + B6[row] * g.sig[le][gp][row];
+      f = f + g.w[le][gp] * s;
+    }
+    forces[(size_t)i * 24 + col] = f;
+  }
+}
+
 bool g_pairs_ready[64] = {false};
 std::mutex g_pairs_mu;
 
@@ -208,6 +334,18 @@ int launch_h8_ke(Context* ctx, int n, const double* d_xyz, const double* d_E, do
   if (n <= 0) return MSG_OK;
   MSG_TRY(ensure_pairs(ctx));
   k_h8_ke<<<(n + kEPB - 1) / kEPB, kThreads, 0, ctx->stream>>>(n, d_xyz, d_E, E_scalar, nu, d_K, d_status);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+int launch_h8_stress(Context* ctx, int n, const double* d_xyz, const double* d_E, double E_scalar, double nu,
+                     const double* d_u, const double* d_du, const double* d_X, const int* d_conn, const int* d_dof,
+                     int n_e, int n_dofs, double* d_strains, double* d_stresses, double* d_forces, int* d_status) {
+  if (n <= 0) return MSG_OK;
+  StressIn in{d_xyz, d_E, E_scalar, nu, d_u, d_du, d_X, d_conn, d_dof, n_e, n_dofs};
+  k_h8_stress<<<(n + kEPB - 1) / kEPB, kThreads, 0, ctx->stream>>>(n, in, d_strains, d_stresses, d_forces,
+                                                                   d_status);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;

@@ -367,6 +367,7 @@ static int create_mesh(Context* ctx, int n_nodes, const double* xyz, int n_elems
   MSG_TRY(upload(ctx, m->d_exyz, exyz.data(), exyz.size()));
   MSG_TRY(upload(ctx, m->d_centroid, cen.data(), cen.size()));
   MSG_TRY(upload(ctx, m->d_dof, m->dof.data(), m->dof.size()));
+  MSG_TRY(upload(ctx, m->d_conn, m->conn.data(), m->conn.size()));
   MSG_TRY(upload(ctx, m->d_mask, mask.data(), mask.size()));
   MSG_TRY(upload(ctx, m->d_free_rows, free_rows.data(), free_rows.size()));
   MSG_TRY(upload(ctx, m->d_col, P.col.data(), P.col.size()));
@@ -625,6 +626,63 @@ int MSG_H8_ME_BATCH(MSG_CTX ctx, int n, const double* xyz, double rho, double* M
   MSG_TRY(launch_h8_me(ctx, n, dx.as<double>(), rho, dM.as<double>(), ds.as<int>()));
   int st = 0;
   MSG_CUDA(ctx, cudaMemcpyAsync(Me, dM.ptr, sizeof(double) * 300 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&st, ds.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (st != 0) return set_error(ctx, st, "negative or tiny Jacobian determinant (H8)");
+  return MSG_OK;
+}
+
+int MSG_H8_STRESS_BATCH(MSG_CTX ctx, int n, const double* xyz, const double* E, double nu, const double* u,
+                        const double* du, double* strains, double* stresses, double* forces) {
+  CTX_GUARD(ctx);
+  if (n < 0 || (n > 0 && (!xyz || !E || !u))) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "stress batch: bad args");
+  if (n == 0) return MSG_OK;
+  if (!(nu > -1.0 && nu < 0.5)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Poisson ratio out of (-1, 0.5)");
+  DevMem dx, dE, du_, ddu, dS, dT, dF, ds;
+  MSG_TRY(upload(ctx, dx, xyz, 24 * (size_t)n));
+  MSG_TRY(upload(ctx, dE, E, (size_t)n));
+  MSG_TRY(upload(ctx, du_, u, 24 * (size_t)n));
+  if (du) MSG_TRY(upload(ctx, ddu, du, 24 * (size_t)n));
+  if (strains) MSG_TRY(dS.alloc(ctx, sizeof(double) * 48 * (size_t)n));
+  if (stresses) MSG_TRY(dT.alloc(ctx, sizeof(double) * 48 * (size_t)n));
+  if (forces) MSG_TRY(dF.alloc(ctx, sizeof(double) * 24 * (size_t)n));
+  MSG_TRY(ds.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(ds.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_stress(ctx, n, dx.as<double>(), dE.as<double>(), 0.0, nu, du_.as<double>(),
+                           du ? ddu.as<double>() : nullptr, nullptr, nullptr, nullptr, n, 0, dS.as<double>(),
+                           dT.as<double>(), dF.as<double>(), ds.as<int>()));
+  int st = 0;
+  if (strains)
+    MSG_CUDA(ctx, cudaMemcpyAsync(strains, dS.ptr, sizeof(double) * 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (stresses)
+    MSG_CUDA(ctx, cudaMemcpyAsync(stresses, dT.ptr, sizeof(double) * 48 * (size_t)n, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  if (forces)
+    MSG_CUDA(ctx, cudaMemcpyAsync(forces, dF.ptr, sizeof(double) * 24 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&st, ds.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (st != 0) return set_error(ctx, st, "negative or tiny Jacobian determinant (H8)");
+  return MSG_OK;
+}
+
+int MSG_STRESS_BATCH_DEVICE(MSG_MESH mesh, int R, const double* E_dev, double nu, const double* X_dev,
+                            double* strains_dev, double* stresses_dev, double* forces_dev) {
+  if (!mesh) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = mesh->ctx;
+  CTX_GUARD(ctx);
+  if (R < 0 || (R > 0 && (!E_dev || !X_dev)))
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "stress batch: bad args");
+  if (R == 0) return MSG_OK;
+  if (!(nu > -1.0 && nu < 0.5)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Poisson ratio out of (-1, 0.5)");
+  const int64_t n = (int64_t)R * mesh->n_elems;
+  if (n > INT32_MAX) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "stress batch: R * n_elems too large");
+  DevMem ds;
+  MSG_TRY(ds.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(ds.ptr, 0, sizeof(int), ctx->stream));
+  MSG_TRY(launch_h8_stress(ctx, (int)n, mesh->d_exyz.as<double>(), E_dev, 0.0, nu, nullptr, nullptr, X_dev,
+                           mesh->d_conn.as<int>(), mesh->d_dof.as<int>(), mesh->n_elems, mesh->n_dofs, strains_dev,
+                           stresses_dev, forces_dev, ds.as<int>()));
+  int st = 0;
   MSG_CUDA(ctx, cudaMemcpyAsync(&st, ds.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (st != 0) return set_error(ctx, st, "negative or tiny Jacobian determinant (H8)");

@@ -164,6 +164,7 @@ struct Mesh {
   // device copies
   DevMem d_exyz;       // [n_elems][24] element coordinates
   DevMem d_dof;        // [n_nodes][3]
+  DevMem d_conn;       // [n_elems][8]
   DevMem d_col, d_slice_ptr, d_contrib_ptr, d_contrib, d_diag_pos;
   DevMem d_mask;       // [n_nodes] uint8 bit c = component c constrained
   DevMem d_centroid;   // [n_elems][3]
@@ -216,6 +217,12 @@ struct Matrix {
 int launch_h8_ke(Context* ctx, int n, const double* d_xyz, const double* d_E, double E_scalar, double nu,
                  double* d_K, int* d_status);
 int launch_h8_me(Context* ctx, int n, const double* d_xyz, double rho, double* d_M, int* d_status);
+// Strains, stresses (per Gauss point) and internal forces of n element instances
+// (instance i = element i % n_e of realization i / n_e); displacements from
+// d_u [n][24] or gathered from d_X [R][n_dofs] through d_conn/d_dof.
+int launch_h8_stress(Context* ctx, int n, const double* d_xyz, const double* d_E, double E_scalar, double nu,
+                     const double* d_u, const double* d_du, const double* d_X, const int* d_conn, const int* d_dof,
+                     int n_e, int n_dofs, double* d_strains, double* d_stresses, double* d_forces, int* d_status);
 int launch_bsr_assemble(Context* ctx, const Mesh* m, const double* d_Ke, double* d_val);
 int launch_bsr_diag_inv(Context* ctx, const Mesh* m, const double* d_val, double* d_dinv);
 int launch_bsr_spmv(Context* ctx, const Mesh* m, const double* d_val, const double* d_x, double* d_y);

@@ -50,6 +50,7 @@ def lib():
             "orc_h8_stiffness_csharp": (C.c_int, [_d, C.c_double, C.c_double, _d]),
             "orc_h8_consistent_mass": (C.c_int, [_d, C.c_double, _d]),
             "orc_h8_stiffness_batch": (None, [C.c_int, _d, _d, C.c_double, _d, _i]),
+            "orc_h8_stress_batch": (None, [C.c_int, _d, _d, C.c_double, _d, _d, _d, _d, _d, _i]),
             "orc_block_nodes": (None, [C.c_int, C.c_int, C.c_int, C.c_double, _d]),
             "orc_block_conn": (None, [C.c_int, C.c_int, C.c_int, _i]),
             "orc_enumerate_dofs": (C.c_int, [C.c_int, _u8, _i]),
@@ -128,6 +129,21 @@ def h8_stiffness_batch(xyz, E, nu):
     st = C.c_int(0)
     lib().orc_h8_stiffness_batch(n, _p(xyz), _p(E), float(nu), _p(K), C.byref(st))
     return K, st.value
+
+
+def h8_stress_batch(xyz, E, nu, u, du=None):
+    """Strains, stresses [n][8][6] and internal forces [n][24] per element
+    (Hexa8.CalculateStresses + CalculateForces over CalcH8Strains/CalcH8Forces)."""
+    xyz = _f64(xyz).reshape(-1, 24)
+    n = xyz.shape[0]
+    E = _f64(np.broadcast_to(np.asarray(E, dtype=np.float64), (n,)))
+    u = _f64(u).reshape(n, 24)
+    du = None if du is None else _f64(du).reshape(n, 24)
+    eps, sig, f = np.zeros((n, 8, 6)), np.zeros((n, 8, 6)), np.zeros((n, 24))
+    st = C.c_int(0)
+    lib().orc_h8_stress_batch(n, _p(xyz), _p(E), float(nu), _p(u), None if du is None else _p(du), _p(eps), _p(sig),
+                              _p(f), C.byref(st))
+    return eps, sig, f, st.value
 
 
 def h8_gauss_matrices(xyz):

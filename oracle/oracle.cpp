@@ -268,6 +268,64 @@ int orc_h8_consistent_mass(const double* xyz, double rho, double* M300) {
   return st;
 }
 
+// CalcH8Strains (rElHexa8.f90:636-648): strains[m] = MatMul(B_m, u), each row
+// summed over the 24 columns in order.
+void orc_h8_strains(const double* B /*[8][6][24]*/, const double* u24, double* strains /*[8][6]*/) {
+  for (int m = 0; m < 8; ++m)
+    for (int row = 0; row < 6; ++row) {
+      double s = 0.0;
+      for (int col = 0; col < 24; ++col) s = s + B[144 * m + 24 * row + col] * u24[col];
+      strains[6 * m + row] = s;
+    }
+}
+
+// Hexa8.CalculateStresses + CalculateForces (Hexa8.cs:453-510) with
+// ElasticMaterial3D (ElasticMaterial3D.cs:20-44, 75-81: UpdateMaterial stores
+// the strain increment, stresses = D * increment, Matrix2D * Vector row by row)
+// and CalcH8Forces (rElHexa8.f90:724-747: forces += w_m * B_m^T stresses_m,
+// Gauss points xi outer, zeta inner). du == NULL: du = u. Outputs may be NULL.
+int orc_h8_stress(const double* xyz, double E, double nu, const double* u, const double* du, double* strains48,
+                  double* stresses48, double* forces24) {
+  double w[8], S[64], DS[192], J[72], det[8], B[8 * 144];
+  int st = orc_h8_gauss_matrices(xyz, w, S, DS, J, det, B);
+  double eps[48], deps[48], sig[48], D[36];
+  orc_h8_strains(B, u, eps);
+  orc_h8_strains(B, du ? du : u, deps);
+  orc_elastic_D(E, nu, D);
+  for (int m = 0; m < 8; ++m)
+    for (int row = 0; row < 6; ++row) {
+      double s = 0.0;
+      for (int col = 0; col < 6; ++col) s = s + D[6 * row + col] * deps[6 * m + col];
+      sig[6 * m + row] = s;
+    }
+  if (strains48) std::memcpy(strains48, eps, sizeof(eps));
+  if (stresses48) std::memcpy(stresses48, sig, sizeof(sig));
+  if (forces24) {
+    for (int i = 0; i < 24; ++i) forces24[i] = 0.0;
+    for (int m = 0; m < 8; ++m)
+      for (int i = 0; i < 24; ++i) {
+        double s = 0.0;
+        for (int row = 0; row < 6; ++row) s = s + B[144 * m + 24 * row + i] * sig[6 * m + row];
+        forces24[i] = forces24[i] + w[m] * s;
+      }
+  }
+  return st;
+}
+
+void orc_h8_stress_batch(int n, const double* xyz, const double* E, double nu, const double* u, const double* du,
+                         double* strains, double* stresses, double* forces, int* status) {
+  int st = 0;
+#pragma omp parallel for schedule(static) reduction(min : st)
+  for (int e = 0; e < n; ++e) {
+    const int64_t k = e;
+    int s = orc_h8_stress(xyz + 24 * k, E[e], nu, u + 24 * k, du ? du + 24 * k : nullptr,
+                          strains ? strains + 48 * k : nullptr, stresses ? stresses + 48 * k : nullptr,
+                          forces ? forces + 24 * k : nullptr);
+    if (s < st) st = s;
+  }
+  if (status) *status = st;
+}
+
 void orc_h8_stiffness_batch(int n, const double* xyz, const double* E, double nu, double* K, int* status) {
   int st = 0;
 #pragma omp parallel for schedule(static) reduction(min : st)

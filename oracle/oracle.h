@@ -37,6 +37,11 @@ int orc_h8_stiffness_fortran(const double* xyz24, double E, double nu, double* K
 int orc_h8_stiffness_csharp(const double* xyz24, double E, double nu, double* K300);
 int orc_h8_consistent_mass(const double* xyz24, double rho, double* M300);
 void orc_h8_stiffness_batch(int n, const double* xyz, const double* E, double nu, double* K, int* status);
+void orc_h8_strains(const double* B1152, const double* u24, double* strains48);
+int orc_h8_stress(const double* xyz24, double E, double nu, const double* u24, const double* du24,
+                  double* strains48, double* stresses48, double* forces24);
+void orc_h8_stress_batch(int n, const double* xyz, const double* E, double nu, const double* u, const double* du,
+                         double* strains, double* stresses, double* forces, int* status);
 
 /* ---- mesh / DOFs / loads (Hexa8MeshGenerator.cs, Model.cs, Subdomain.cs) ---- */
 void orc_block_nodes(int nx, int ny, int nz, double h, double* xyz);
