@@ -190,6 +190,14 @@ typedef struct {
   double mean;
   double sigma;
   int mean_correction; /* 1: reference form ln(mean) - sigma^2/2; 0: exp(sigma g) */
+  /* 0: lognormal field (LognormalFileStochasticCoefficientsProvider); 1: Gaussian
+   * field E = mean (1 + sum_k xi_k sigma sqrt(eig_k) phi_k(x)), the coefficient of
+   * GaussianFileStochasticCoefficientsProvider.GetCoefficient
+   * (ISAAR.MSolve.PreProcessor/Stochastic/GaussianFileStochasticCoefficientsProvider.cs:72-108,
+   * sigma = its covariance 0.15), so K(E) = K_0 + sum_k xi_k K_k is the matrix
+   * MonteCarloAnalyzer composes (ISAAR.MSolve.Analyzers/MonteCarloAnalyzer.cs:88-172);
+   * mean_correction is ignored. E must stay positive for the solvers. */
+  int gaussian;
 } MSG_KL;
 
 /* Build the KL table of the separable exponential kernel exp(-sum|dx_a|/corr_len)

@@ -6,16 +6,17 @@ solver and analyzer interfaces, bound through ctypes.
 """
 from ._native import (ArgumentError, Context, InvalidOperationError, MSolveError, MSG_MODE_FP64_BSR,
                       MSG_MODE_MIXED_BATCHED, lib)
-from .analyzers import (GpuMatrix, GpuMesh, LinearAnalyzer, LognormalStochasticCoefficientsProvider,
-                        MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer, ProblemStructural, SolverPCG,
+from .analyzers import (GaussianStochasticCoefficientsProvider, GpuMatrix, GpuMesh, LinearAnalyzer,
+                        LognormalStochasticCoefficientsProvider,
+                        MonteCarloAnalyzer, MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer, ProblemStructural, SolverPCG,
                         StaticAnalyzer, h8_mass_batch, h8_stiffness_batch, h8_stress_batch, realization_stresses)
 from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, cantilever_model, clamped_block_model,
                     tip_dof)
 
 __all__ = [
     "ArgumentError", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
-    "lib", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
-    "MonteCarloAnalyzerWithStochasticMaterial", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
+    "lib", "GaussianStochasticCoefficientsProvider", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
+    "MonteCarloAnalyzer", "MonteCarloAnalyzerWithStochasticMaterial", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
     "StaticAnalyzer", "h8_mass_batch", "h8_stiffness_batch", "h8_stress_batch", "realization_stresses",
     "Hexa8MeshGenerator", "MassAccelerationSinusoidalLoad",
     "Model", "cantilever_model", "clamped_block_model", "tip_dof",

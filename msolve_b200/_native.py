@@ -49,6 +49,7 @@ class MSG_KL(C.Structure):
         ("mean", C.c_double),
         ("sigma", C.c_double),
         ("mean_correction", C.c_int),
+        ("gaussian", C.c_int),
     ]
 
 

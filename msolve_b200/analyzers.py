@@ -271,6 +271,7 @@ class LognormalStochasticCoefficientsProvider:
         for a in range(3):
             s.domain[a] = float(self.domain[a])
         s.mean, s.sigma, s.mean_correction = float(self.mean), float(self.sigma), int(bool(self.mean_correction))
+        s.gaussian = 1 if getattr(self, "gaussian", False) else 0
         return s
 
     def table(self):
@@ -283,6 +284,17 @@ class LognormalStochasticCoefficientsProvider:
         N.check(N.lib().MSG_KL_FIELD(mesh.handle, C.byref(s), xi.shape[0], N.ptr(xi), N.ptr(E)), mesh.ctx.handle,
                 "MSG_KL_FIELD")
         return E
+
+
+class GaussianStochasticCoefficientsProvider(LognormalStochasticCoefficientsProvider):
+    """KL Gaussian Young's modulus (GaussianFileStochasticCoefficientsProvider.cs:24-108):
+    E = mean (1 + sum_k xi_k covariance sqrt(eig_k) phi_k(x)), the reference's
+    covariance 0.15 by default, on the same analytic table."""
+    gaussian = True
+
+    def __init__(self, domain, corr_len, n_terms=50, n1d=16, mean=1.0, covariance=0.15):
+        super().__init__(domain, corr_len, n_terms, n1d, mean=mean, sigma=covariance)
+        self.covariance = covariance
 
 
 class MonteCarloAnalyzerWithStochasticMaterial:
@@ -331,6 +343,20 @@ class MonteCarloAnalyzerWithStochasticMaterial:
     def statistics(self):
         t = self.TipValues
         return dict(mean=float(np.mean(t)), variance=float(np.var(t, ddof=1)) if len(t) > 1 else 0.0)
+
+
+class MonteCarloAnalyzer(MonteCarloAnalyzerWithStochasticMaterial):
+    """Gaussian-field Monte Carlo (ISAAR.MSolve.Analyzers/MonteCarloAnalyzer.cs:35-198).
+    The reference builds K_0 and one matrix K_k per expansion term and solves
+    K_0 + sum_k xi_k K_k for every realization. The element stiffness is linear
+    in E, so that sum is the stiffness of the field E = mean (1 + sum_k xi_k
+    psi_k); the batch evaluates that field and runs the same batched solve as the
+    lognormal analyzer (no per-term matrices are stored)."""
+
+    def __init__(self, ctx, model, coefficients_provider, expansion_order=50, simulations=1, **kw):
+        if not getattr(coefficients_provider, "gaussian", False):
+            raise TypeError("MonteCarloAnalyzer needs a GaussianStochasticCoefficientsProvider")
+        super().__init__(ctx, model, coefficients_provider, expansion_order, simulations, **kw)
 
 
 class NewmarkDynamicAnalyzer:

@@ -1,7 +1,10 @@
 // Lognormal Young's-modulus field from a separable Karhunen-Loeve table, the
 // device twin of LognormalFileStochasticCoefficientsProvider.GetCoefficient
 // (ISAAR.MSolve.PreProcessor/Stochastic/LognormalFileStochasticCoefficientsProvider.cs:134-193)
-// evaluated at element bounding-box centres (Hexa8WithStochasticMaterial.cs:112-140).
+// evaluated at element bounding-box centres (Hexa8WithStochasticMaterial.cs:112-140),
+// or the Gaussian field of GaussianFileStochasticCoefficientsProvider.GetCoefficient
+// (GaussianFileStochasticCoefficientsProvider.cs:72-108): E = mean (1 + sum_k xi_k psi_k)
+// with the same psi (its sigma is the provider's covariance).
 //
 // psi[k][e] = sigma sqrt(eig_k) prod_a amp_ka {cos|sin}(w_ka (x_ea - L_a/2)) is
 // built once per mesh and table (FP64). The field for R realizations is then
@@ -37,7 +40,7 @@ __global__ void k_kl_psi(int ne, int K, const double* __restrict__ cen, const do
 }
 
 __global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, const double* __restrict__ xi,
-                                                  const double* __restrict__ psi, double mu,
+                                                  const double* __restrict__ psi, double mu, int gaussian, double mean,
                                                   double* __restrict__ E64_er, float* __restrict__ E32_er,
                                                   double* __restrict__ E64_re, const int* __restrict__ elem_row) {
   __shared__ double s_xi[kMaxTerms][33];
@@ -56,9 +59,9 @@ __global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, 
   for (int q = 0; q < 4; ++q) {
     const int le = ty + 8 * q, e = e0 + le;
     if (e >= ne) continue;
-    double s = mu;
+    double s = gaussian ? 0.0 : mu;
     for (int k = 0; k < K; ++k) s += s_xi[k][tx] * s_psi[k][le];
-    const double E = (r < R) ? exp(s) : 1.0;
+    const double E = (r < R) ? (gaussian ? mean * (1.0 + s) : exp(s)) : 1.0;
     const size_t row = elem_row ? (size_t)elem_row[e] : (size_t)e;
     if (E64_er) E64_er[row * Rp + r] = E;
     if (E32_er) E32_er[row * Rp + r] = (float)E;
@@ -70,15 +73,16 @@ __global__ void __launch_bounds__(256) k_kl_field(int ne, int K, int R, int Rp, 
 // E[row(e)*Rp + slot] = exp(mu + sum_k xi[i][k] psi[k][e]) in FP64 and FP32,
 // the same expression as k_kl_field. xi [n_slots][K].
 __global__ void k_kl_field_slots(int ne, int K, int n_slots, const int* __restrict__ slots,
-                                 const double* __restrict__ xi, const double* __restrict__ psi, double mu, int Rp,
-                                 double* __restrict__ E64, float* __restrict__ E32, const int* __restrict__ elem_row) {
+                                 const double* __restrict__ xi, const double* __restrict__ psi, double mu,
+                                 int gaussian, double mean, int Rp, double* __restrict__ E64, float* __restrict__ E32,
+                                 const int* __restrict__ elem_row) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (e >= ne || i >= n_slots) return;
   const double* x = xi + (size_t)i * K;
-  double s = mu;
+  double s = gaussian ? 0.0 : mu;
   for (int k = 0; k < K; ++k) s += x[k] * psi[(size_t)k * ne + e];
-  const double E = exp(s);
+  const double E = gaussian ? mean * (1.0 + s) : exp(s);
   const size_t o = (size_t)elem_row[e] * Rp + slots[i];
   E64[o] = E;
   E32[o] = (float)E;
@@ -89,8 +93,8 @@ __global__ void k_kl_field_slots(int ne, int K, int n_slots, const int* __restri
 int launch_kl_field_slots(cudaStream_t st, const Mesh* m, const KLDevice* kl, int n_slots, const int* d_slots,
                           const double* d_xi, int Rp, double* d_E64, float* d_E32) {
   dim3 grid((m->n_elems + 127) / 128, n_slots);
-  k_kl_field_slots<<<grid, 128, 0, st>>>(m->n_elems, kl->n_terms, n_slots, d_slots, d_xi, kl->psi, kl->mu, Rp, d_E64,
-                                         d_E32, m->d_pad_elem_row.as<int>());
+  k_kl_field_slots<<<grid, 128, 0, st>>>(m->n_elems, kl->n_terms, n_slots, d_slots, d_xi, kl->psi, kl->mu,
+                                         kl->gaussian, kl->mean, Rp, d_E64, d_E32, m->d_pad_elem_row.as<int>());
   return cudaGetLastError() == cudaSuccess ? MSG_OK : MSG_ERR_CUDA;
 }
 
@@ -122,6 +126,8 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
   // the host table is staged synchronously by the pageable copy; nothing to wait for
   out->n_terms = K;
   out->mu = std::log(kl->mean) - (kl->mean_correction ? 0.5 * kl->sigma * kl->sigma : 0.0);
+  out->gaussian = kl->gaussian ? 1 : 0;
+  out->mean = kl->mean;
   return MSG_OK;
 }
 
@@ -129,7 +135,8 @@ int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int 
                     double* d_E64_er, float* d_E32_er, double* d_E64_re, const int* d_elem_row) {
   dim3 grid((m->n_elems + 31) / 32, Rp / 32);
   k_kl_field<<<grid, dim3(32, 8), 0, ctx->stream>>>(m->n_elems, kl->n_terms, R, Rp, d_xi, kl->psi,
-                                                    kl->mu, d_E64_er, d_E32_er, d_E64_re, d_elem_row);
+                                                    kl->mu, kl->gaussian, kl->mean, d_E64_er, d_E32_er, d_E64_re,
+                                                    d_elem_row);
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;

@@ -240,6 +240,8 @@ struct KLDevice {
   int n_terms = 0;
   double* psi = nullptr;  // [K][n_elems], context workspace slot 15
   double mu = 0;
+  int gaussian = 0;       // 1: E = mean (1 + sum xi psi); 0: E = exp(mu + sum xi psi)
+  double mean = 1.0;
 };
 int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out);
 // d_elem_row (nullable): output row of element e in the [row][Rp] layouts.

@@ -74,6 +74,8 @@ def lib():
                                             C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                             C.c_double, C.c_double, C.c_int, _d, C.c_int, C.c_double, C.c_int,
                                             _d, _d, _i]),
+            "orc_kl_field_gaussian": (None, [C.c_int, _d, _d, C.c_int, _d, _d, _i, _d, C.c_int, _d,
+                                             C.c_double, C.c_double, _d]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -332,6 +334,18 @@ def kl_field(cen, domain, table, xi, mean=1.0, sigma=0.3, mean_correction=False)
     lib().orc_kl_field(cen.shape[0], _p(cen), _p(L), K, _p(_f64(table["w"])), _p(_f64(table["amp"])),
                        _p(_i32(table["idx"]), _i), _p(_f64(table["eig"])), R, _p(xi), float(mean), float(sigma),
                        int(bool(mean_correction)), _p(E))
+    return E
+
+
+def kl_field_gaussian(cen, domain, table, xi, mean=1.0, cov=0.15):
+    """E = mean (1 + sum_k xi_k cov sqrt(eig_k) phi_k(x)) per element centroid
+    (GaussianFileStochasticCoefficientsProvider.GetCoefficient)."""
+    cen, L, xi = _f64(cen), _f64(domain), _f64(xi)
+    R, K = xi.shape
+    E = np.zeros((R, cen.shape[0]))
+    lib().orc_kl_field_gaussian(cen.shape[0], _p(cen), _p(L), K, _p(_f64(table["w"])), _p(_f64(table["amp"])),
+                                _p(_i32(table["idx"]), _i), _p(_f64(table["eig"])), R, _p(xi), float(mean),
+                                float(cov), _p(E))
     return E
 
 

@@ -778,6 +778,32 @@ void orc_kl_field(int ne, const double* cen, const double* L, int K, const doubl
     }
 }
 
+// GaussianFileStochasticCoefficientsProvider (:72-108) as the Monte Carlo
+// analyzer's matrix composition sees it (MonteCarloAnalyzer.cs:88-172): K_0 is
+// built with coefficient 1 (order -1), K_k with GetCoefficientInternal(x, k) =
+// cov * sqrt(eig_k) * prod_ax amp*{cos|sin}(w*(x_ax - L_ax/2)), and the
+// realization's matrix is K_0 + sum_k xi_k K_k. The stiffness is linear in E, so
+// this is one element stiffness with E = mean * (1 + sum_k xi_k * coefficient_k),
+// GetCoefficient's own formula (:101-108). Output E[n_real][n_elems].
+void orc_kl_field_gaussian(int ne, const double* cen, const double* L, int K, const double* w3, const double* amp3,
+                           const int* idx3, const double* eig, int R, const double* xi, double mean, double cov,
+                           double* E) {
+  for (int r = 0; r < R; ++r)
+    for (int e = 0; e < ne; ++e) {
+      double result = 1;
+      for (int k = 0; k < K; ++k) {
+        double f = cov * std::sqrt(eig[k]);
+        for (int ax = 0; ax < 3; ++ax) {
+          double x = cen[3 * e + ax] - L[ax] / 2;
+          double ww = w3[3 * k + ax], aa = amp3[3 * k + ax];
+          f *= (idx3[3 * k + ax] % 2 == 0) ? aa * std::sin(ww * x) : aa * std::cos(ww * x);
+        }
+        result += xi[(size_t)r * K + k] * f;
+      }
+      E[(size_t)r * ne + e] = result * mean;
+    }
+}
+
 // One FP64 static solve of a structured nx*ny*nz block of h-cubes: element
 // stiffness through the Fortran restatement with each element's E, CSR
 // assembly over the free DOFs, Jacobi-PCG with SolverPCG semantics.

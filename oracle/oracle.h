@@ -43,6 +43,10 @@ int orc_h8_stress(const double* xyz24, double E, double nu, const double* u24, c
 void orc_h8_stress_batch(int n, const double* xyz, const double* E, double nu, const double* u, const double* du,
                          double* strains, double* stresses, double* forces, int* status);
 
+void orc_kl_field_gaussian(int ne, const double* cen, const double* L, int K, const double* w3, const double* amp3,
+                           const int* idx3, const double* eig, int R, const double* xi, double mean, double cov,
+                           double* E);
+
 /* ---- mesh / DOFs / loads (Hexa8MeshGenerator.cs, Model.cs, Subdomain.cs) ---- */
 void orc_block_nodes(int nx, int ny, int nz, double h, double* xyz);
 void orc_block_conn(int nx, int ny, int nz, int* conn);
