@@ -54,6 +54,7 @@ extern "C" {
 typedef struct msg_context* MSG_CTX;
 typedef struct msg_mesh* MSG_MESH;
 typedef struct msg_matrix* MSG_MAT;
+typedef struct msg_svs* MSG_SVS;
 
 /* ------------------------------------------------------------------ context */
 /* Create a context on CUDA device `device`. mem_budget_bytes = 0 means no budget
@@ -154,6 +155,31 @@ int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double to
  * counterpart in the reference. */
 int MSG_PCG_SOLVE_MIXED(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
                         double* rel_res);
+
+/* Search vectors kept across solves: SolverPCGReorthogonalizationSearchVectorCalculator
+ * (ISAAR.MSolve.Solvers/PCG/SolverPCGReorthogonalizationSearchVectorCalculator.cs:11-65)
+ * holds every direction p and K p of the solves it served; here a device store of at
+ * most `capacity` pairs for one mesh. MSG_SVS_CLEAR keeps the `keep_from_top` oldest
+ * pairs (ClearSearchVectors, :36-63; < 1 clears all). */
+int MSG_SVS_CREATE(MSG_MESH mesh, int capacity, MSG_SVS* out);
+int MSG_SVS_CLEAR(MSG_SVS store, int keep_from_top);
+int MSG_SVS_COUNT(MSG_SVS store, int* count);
+int MSG_SVS_DESTROY(MSG_SVS store);
+/* SolverPCG (ISAAR.MSolve.Solvers/PCG/SolverPCG.cs:105-149) with the
+ * re-orthogonalising search-vector calculator (SearchVectors.cs:13-166): each new
+ * direction is z - sum_c (z.q_c / p_c.q_c) p_c over every stored pair, the gradient
+ * is (p.r)/(p.q) and each (p, q) is appended to the store; Jacobi preconditioner,
+ * FP64, stop on the recursive ||r||/||b|| < tol, iteration count = loop index at
+ * the break (as MSG_PCG_SOLVE). start_from_store = 1:
+ * InitializeStartingVectorFromReorthogonalizedSearchVectors (:115-166; drops the
+ * last pair, x0 = sum_c (p_c.b / p_c.q_c) p_c), then r0 = b - K x0.
+ * start_from_store = 2: the same starting vector, then the store is emptied: the
+ * pairs are K-conjugate only for the matrix that produced them, so a changed
+ * matrix (the next Monte Carlo realization) takes them as an initial guess but
+ * must not re-orthogonalise against them. b, x [n_dofs] (host).
+ * MSG_ERR_OUT_OF_MEMORY when the store fills up during the solve. */
+int MSG_PCG_SOLVE_REORTH(MSG_MAT mat, MSG_SVS store, const double* b, double* x, int start_from_store, int max_it,
+                         double tol, int* iterations, double* rel_res);
 
 /* MSG_PCG_SOLVE without device allocation. No counterpart in the reference.
  * For callers that must not allocate device memory while solving: cudaMalloc

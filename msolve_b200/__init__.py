@@ -8,7 +8,8 @@ from ._native import (ArgumentError, Context, InvalidOperationError, MSolveError
                       MSG_MODE_MIXED_BATCHED, lib)
 from .analyzers import (GaussianStochasticCoefficientsProvider, GpuMatrix, GpuMesh, LinearAnalyzer,
                         LognormalStochasticCoefficientsProvider,
-                        MonteCarloAnalyzer, MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer, ProblemStructural, SolverPCG,
+                        MonteCarloAnalyzer, MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer,
+                        SolverPCGReorthogonalizationSearchVectorCalculator, SolverPCGReorthogonalized, ProblemStructural, SolverPCG,
                         StaticAnalyzer, h8_mass_batch, h8_stiffness_batch, h8_stress_batch, realization_stresses)
 from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, cantilever_model, clamped_block_model,
                     tip_dof)
@@ -16,7 +17,8 @@ from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, c
 __all__ = [
     "ArgumentError", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
     "lib", "GaussianStochasticCoefficientsProvider", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
-    "MonteCarloAnalyzer", "MonteCarloAnalyzerWithStochasticMaterial", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
+    "MonteCarloAnalyzer", "MonteCarloAnalyzerWithStochasticMaterial", "SolverPCGReorthogonalizationSearchVectorCalculator",
+    "SolverPCGReorthogonalized", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
     "StaticAnalyzer", "h8_mass_batch", "h8_stiffness_batch", "h8_stress_batch", "realization_stresses",
     "Hexa8MeshGenerator", "MassAccelerationSinusoidalLoad",
     "Model", "cantilever_model", "clamped_block_model", "tip_dof",

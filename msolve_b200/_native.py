@@ -76,6 +76,12 @@ SIGNATURES = {
     "MSG_VERSION": (C.c_int, []),
     "MSG_H8_KE_BATCH": (C.c_int, [_vp, C.c_int, _d, _d, C.c_double, _d]),
     "MSG_H8_ME_BATCH": (C.c_int, [_vp, C.c_int, _d, C.c_double, _d]),
+    "MSG_SVS_CREATE": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "MSG_SVS_CLEAR": (C.c_int, [_vp, C.c_int]),
+    "MSG_SVS_COUNT": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "MSG_SVS_DESTROY": (C.c_int, [_vp]),
+    "MSG_PCG_SOLVE_REORTH": (C.c_int, [_vp, _vp, _d, _d, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_double)]),
     "MSG_H8_STRESS_BATCH": (C.c_int, [_vp, C.c_int, _d, _d, C.c_double, _d, _d, _d, _d, _d]),
     "MSG_STRESS_BATCH_DEVICE": (C.c_int, [_vp, C.c_int, _vp, C.c_double, _vp, _vp, _vp, _vp]),
     "MSG_MESH_CREATE": (C.c_int, [_vp, C.c_int, _d, C.c_int, _i, _i, C.c_int, C.POINTER(_vp)]),

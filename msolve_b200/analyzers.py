@@ -211,6 +211,63 @@ class SolverPCG:
         return x
 
 
+class SolverPCGReorthogonalizationSearchVectorCalculator:
+    """The re-orthogonalising search-vector calculator
+    (SolverPCGReorthogonalizationSearchVectorCalculator.cs:11-65) as a device store of
+    (p, K p) pairs for one mesh (MSG_SVS_*), at most `capacity` pairs."""
+
+    def __init__(self, mesh, capacity):
+        h = C.c_void_p()
+        N.check(N.lib().MSG_SVS_CREATE(mesh.handle, int(capacity), C.byref(h)), mesh.ctx.handle, "MSG_SVS_CREATE")
+        self.mesh, self.handle, self.capacity = mesh, h, capacity
+
+    @property
+    def count(self):
+        c = C.c_int(0)
+        N.check(N.lib().MSG_SVS_COUNT(self.handle, C.byref(c)))
+        return c.value
+
+    def ClearSearchVectors(self, vectors_to_keep_from_top=0):
+        N.check(N.lib().MSG_SVS_CLEAR(self.handle, int(vectors_to_keep_from_top)), self.mesh.ctx.handle,
+                "MSG_SVS_CLEAR")
+
+    def close(self):
+        if self.handle:
+            N.lib().MSG_SVS_DESTROY(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolverPCGReorthogonalized(SolverPCG):
+    """SolverPCG with the re-orthogonalising search-vector calculator
+    (MSG_PCG_SOLVE_REORTH). start_from_store: 0 x0 = 0; 1 the starting vector
+    from the stored directions (InitializeStartingVectorFromSearchVectors), the
+    store kept; 2 the same starting vector, then a fresh store (for a changed matrix)."""
+
+    def __init__(self, ctx, model, search, max_iterations=20000, tolerance=1e-7, start_from_store=0):
+        super().__init__(ctx, model, max_iterations, tolerance)
+        self.search, self.start_from_store = search, start_from_store
+
+    def Solve(self, max_iterations=None, tolerance=None, start_from_store=None):
+        s = self.model.subdomains[0]
+        b = N.f64(s.RHS)
+        x = np.zeros(self.model.n_dofs)
+        it, rr = C.c_int(0), C.c_double(0)
+        start = self.start_from_store if start_from_store is None else start_from_store
+        st = N.lib().MSG_PCG_SOLVE_REORTH(self.matrix.handle, self.search.handle, N.ptr(b), N.ptr(x), int(start),
+                                          int(max_iterations or self.max_iterations),
+                                          float(tolerance or self.tolerance), C.byref(it), C.byref(rr))
+        self.iterations, self.rel_res = it.value, rr.value
+        s.Solution = x
+        N.check(st, self.ctx.handle, "MSG_PCG_SOLVE_REORTH")
+        return x
+
+
 class LinearAnalyzer:
     """IAnalyzer child: Initialize -> solver.Initialize, Solve -> solver.Solve (LinearAnalyzer.cs:57-69)."""
 

@@ -832,6 +832,68 @@ int MSG_PCG_SOLVE_MIXED(MSG_MAT A, const double* b, double* x, int max_it, doubl
   return pcg_host(A, b, x, max_it, tol, iterations, rel_res, true);
 }
 
+int MSG_SVS_CREATE(MSG_MESH mesh, int capacity, MSG_SVS* out) {
+  if (!mesh || !out) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = mesh->ctx;
+  CTX_GUARD(ctx);
+  SearchVectorStore* s = nullptr;
+  MSG_TRY(svs_create(ctx, mesh, capacity, &s));
+  *out = static_cast<MSG_SVS>(s);
+  return MSG_OK;
+}
+
+int MSG_SVS_CLEAR(MSG_SVS store, int keep_from_top) {
+  if (!store) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = store->mesh->ctx;
+  CTX_GUARD(ctx);
+  store->count = keep_from_top < 1 ? 0 : std::min(store->count, keep_from_top);
+  return MSG_OK;
+}
+
+int MSG_SVS_COUNT(MSG_SVS store, int* count) {
+  if (!store || !count) return MSG_ERR_INVALID_ARGUMENT;
+  *count = store->count;
+  return MSG_OK;
+}
+
+int MSG_SVS_DESTROY(MSG_SVS store) {
+  if (!store) return MSG_OK;
+  Context* ctx = store->mesh->ctx;
+  {
+    CTX_GUARD(ctx);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  delete static_cast<SearchVectorStore*>(store);
+  return MSG_OK;
+}
+
+int MSG_PCG_SOLVE_REORTH(MSG_MAT A, MSG_SVS store, const double* b, double* x, int start_from_store, int max_it,
+                         double tol, int* iterations, double* rel_res) {
+  if (!A || !store || !b || !x || max_it <= 0 || !(tol > 0)) return MSG_ERR_INVALID_ARGUMENT;
+  Mesh* m = A->mesh;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  if (store->mesh != m) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "search vector store belongs to another mesh");
+  const size_t n3 = 3 * (size_t)m->n_nodes;
+  if (!A->d_bn.ptr) {
+    MSG_TRY(A->d_bd.alloc(ctx, sizeof(double) * std::max(1, m->n_dofs)));
+    MSG_TRY(A->d_bn.alloc(ctx, sizeof(double) * n3));
+    MSG_TRY(A->d_xn.alloc(ctx, sizeof(double) * n3));
+    MSG_CUDA(ctx, cudaMemsetAsync(A->d_bn.ptr, 0, sizeof(double) * n3, ctx->stream));
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(A->d_bd.ptr, b, sizeof(double) * m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
+  MSG_TRY(launch_dof_to_node(ctx, m, A->d_bd.as<double>(), A->d_bn.as<double>(), 1, 0, 0));
+  if (start_from_store < 0 || start_from_store > 2)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "start_from_store must be 0, 1 or 2");
+  const int st = pcg_reorth_solve(ctx, A, store, A->d_bn.as<double>(), A->d_xn.as<double>(), start_from_store,
+                                  max_it, tol, iterations, rel_res);
+  if (st != MSG_OK && st != MSG_ERR_NOT_CONVERGED) return st;
+  MSG_TRY(launch_node_to_dof(ctx, m, A->d_xn.as<double>(), A->d_bd.as<double>(), 1, 0, 0));
+  MSG_CUDA(ctx, cudaMemcpyAsync(x, A->d_bd.ptr, sizeof(double) * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return st;
+}
+
 int MSG_KL_TABLE(const double* L, double l, int n_terms, int n1d, double* w3, double* amp3, int* idx3, double* eig) {
   if (!L || !(l > 0) || n_terms <= 0 || n1d <= 0 || !w3 || !amp3 || !idx3 || !eig) return MSG_ERR_INVALID_ARGUMENT;
   if ((int64_t)n1d * n1d * n1d < n_terms) return MSG_ERR_INVALID_ARGUMENT;

@@ -213,6 +213,21 @@ struct Matrix {
   ~Matrix();
 };
 
+// Search vectors (p, K p) kept across solves for the re-orthogonalised PCG
+// (kernels_recycle.cu): node layout, count pairs of capacity in use.
+struct SearchVectorStore {
+  Mesh* mesh = nullptr;
+  int64_t n3 = 0;
+  int capacity = 0, count = 0;
+  DevMem P, Q, pq, coef, work, scal;
+  ~SearchVectorStore() {
+    if (mesh) release(mesh);
+  }
+};
+int svs_create(Context* ctx, Mesh* m, int capacity, SearchVectorStore** out);
+int pcg_reorth_solve(Context* ctx, Matrix* A, SearchVectorStore* S, const double* d_b, double* d_x, int start_mode,
+                     int max_it, double tol, int* iterations, double* rel_res);
+
 // ---------------------------------------------------------------- kernel launchers (kernels_*.cu)
 int launch_h8_ke(Context* ctx, int n, const double* d_xyz, const double* d_E, double E_scalar, double nu,
                  double* d_K, int* d_status);
@@ -298,3 +313,4 @@ int unit_cube_mhat(Context* ctx, double h, double rho, double* M576);
 struct msg_context : msg::Context {};
 struct msg_mesh : msg::Mesh {};
 struct msg_matrix : msg::Matrix {};
+struct msg_svs : msg::SearchVectorStore {};

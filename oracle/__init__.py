@@ -76,6 +76,8 @@ def lib():
                                             _d, _d, _i]),
             "orc_kl_field_gaussian": (None, [C.c_int, _d, _d, C.c_int, _d, _d, _i, _d, C.c_int, _d,
                                              C.c_double, C.c_double, _d]),
+            "orc_pcg_reorth_csr": (C.c_int, [C.c_int, _i64, _i, _d, _d, _d, _d, _d, _d, C.c_int, _i, C.c_int,
+                                             C.c_int, C.c_double, _i, _d]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -307,6 +309,31 @@ class CSR:
         st = lib().orc_pcg_csr_jacobi(self.n, _p(self.rp, _i64), _p(self.ci, _i), _p(self.val), _p(b), _p(x),
                                       max_it, tol, C.byref(it), C.byref(mv), C.byref(rr))
         return x, dict(status=st, iterations=it.value, matvecs=mv.value, rel_res=rr.value)
+
+
+class SearchVectorStore:
+    """Host store of (p, K p) pairs for CSR.pcg_reorth (capacity pairs of length n)."""
+
+    def __init__(self, n, capacity):
+        self.P = np.zeros((capacity, n))
+        self.Q = np.zeros((capacity, n))
+        self.pq = np.zeros(capacity)
+        self.capacity, self.count = capacity, 0
+
+    def clear(self, keep_from_top=0):
+        self.count = 0 if keep_from_top < 1 else min(self.count, keep_from_top)
+
+
+def pcg_reorth(csr, store, b, start=False, max_it=20000, tol=1e-7):
+    """Re-orthogonalised PCG over the store (SolverPCG + SearchVectors)."""
+    b = _f64(b)
+    x = np.zeros(csr.n)
+    it, rr, cnt = C.c_int(0), C.c_double(0), C.c_int(store.count)
+    st = lib().orc_pcg_reorth_csr(csr.n, _p(csr.rp, _i64), _p(csr.ci, _i), _p(csr.val), _p(b), _p(x), _p(store.P),
+                                  _p(store.Q), _p(store.pq), store.capacity, C.byref(cnt), int(start), max_it,
+                                  tol, C.byref(it), C.byref(rr))
+    store.count = cnt.value
+    return x, dict(status=st, iterations=it.value, rel_res=rr.value)
 
 
 # ---------------------------------------------------------------- KL field

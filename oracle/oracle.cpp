@@ -635,6 +635,94 @@ extern "C" {
 // Jacobi-preconditioned PCG on a CSR matrix. The diagonal preconditioner
 // z_j = r_j / K_jj follows PolynomialChaosSolverPCGMatrixCalculator.PreconditionDiagonal
 // (:467-495); the loop is SolverPCG.Solve.
+// SolverPCG (SolverPCG.cs:105-149) with SolverPCGReorthogonalizationSearchVectorCalculator
+// (SearchVectors.cs:13-166): p = z - sum_c (z.q_c / p_c.q_c) p_c over every stored
+// pair, gradient (p.r)/(p.q), the pair appended to the store (P, Q [cap][n], pq
+// [cap], *count pairs in use). start: InitializeStartingVectorFromReorthogonalized-
+// SearchVectors drops the last pair and sets x0 = sum_c (p_c.b / p_c.q_c) p_c,
+// then r0 = b - K x0 (start = 2: the store is emptied after x0, for a matrix
+// other than the one the pairs came from). Jacobi preconditioner on the CSR diagonal. Returns 0,
+// -2001 (not converged) or -1 (store full).
+int orc_pcg_reorth_csr(int n, const int64_t* rp, const int* ci, const double* v, const double* b, double* x,
+                       double* P, double* Q, double* pq, int cap, int* count, int start, int max_it, double tol,
+                       int* iterations, double* rel_res) {
+  std::vector<double> dinv(n), r(n), z(n), p(n), q(n);
+  for (int i = 0; i < n; ++i) {
+    double dd = 0;
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) dd = v[k];
+    dinv[i] = 1.0 / dd;
+  }
+  int k = *count;
+  const double detf = std::sqrt(dot(n, b, b));
+  for (int i = 0; i < n; ++i) x[i] = 0.0;
+  if (start && k > 0) --k;
+  if (start && k > 0) {
+    for (int c = 0; c < k; ++c) {
+      const double* pc = P + (int64_t)c * n;
+      double a = 0, bt = 0;
+      for (int i = 0; i < n; ++i) {
+        a += pc[i] * Q[(int64_t)c * n + i];
+        bt += pc[i] * b[i];
+      }
+      const double vv = bt / a;
+      for (int i = 0; i < n; ++i) x[i] += vv * pc[i];
+    }
+    orc_csr_multiply(n, rp, ci, v, x, q.data());
+    for (int i = 0; i < n; ++i) r[i] = b[i] - q[i];
+    if (start == 2) k = 0;  // the pairs belong to another matrix: start a fresh store
+  } else {
+    for (int i = 0; i < n; ++i) r[i] = b[i];
+  }
+  int it = 0, st = 0;
+  double err = std::sqrt(dot(n, r.data(), r.data())) / detf;
+  if (std::sqrt(dot(n, r.data(), r.data())) > 1e-25) {
+    for (int i = 0; i < n; ++i) z[i] = r[i] * dinv[i];
+    st = -2001;
+    for (it = 0; it < max_it; ++it) {
+      if (k >= cap) {
+        st = -1;
+        break;
+      }
+      for (int i = 0; i < n; ++i) p[i] = z[i];
+      for (int c = 0; c < k; ++c) {
+        const double* pc = P + (int64_t)c * n;
+        const double* qc = Q + (int64_t)c * n;
+        double a = 0, bb = 0;
+        for (int i = 0; i < n; ++i) {
+          a += z[i] * qc[i];
+          bb += pc[i] * qc[i];
+        }
+        const double ab = a / bb;
+        for (int i = 0; i < n; ++i) p[i] -= ab * pc[i];
+      }
+      orc_csr_multiply(n, rp, ci, v, p.data(), q.data());
+      const double pr = dot(n, p.data(), r.data()), pqv = dot(n, p.data(), q.data());
+      std::memcpy(P + (int64_t)k * n, p.data(), sizeof(double) * n);
+      std::memcpy(Q + (int64_t)k * n, q.data(), sizeof(double) * n);
+      pq[k] = pqv;
+      ++k;
+      const double a = pr / pqv;
+      double detz = 0;
+      for (int i = 0; i < n; ++i) {
+        r[i] -= a * q[i];
+        x[i] += a * p[i];
+        detz += r[i] * r[i];
+      }
+      err = std::sqrt(detz) / detf;
+      if (err < tol) {
+        st = 0;
+        break;
+      }
+      for (int i = 0; i < n; ++i) z[i] = r[i] * dinv[i];
+    }
+  }
+  *count = k;
+  if (iterations) *iterations = it;
+  if (rel_res) *rel_res = err;
+  return st;
+}
+
 int orc_pcg_csr_jacobi(int n, const int64_t* rp, const int* ci, const double* v, const double* b,
                        double* x, int max_it, double tol, int* iterations, int* matvecs, double* rel_res) {
   std::vector<double> dinv(n);

@@ -43,6 +43,9 @@ int orc_h8_stress(const double* xyz24, double E, double nu, const double* u24, c
 void orc_h8_stress_batch(int n, const double* xyz, const double* E, double nu, const double* u, const double* du,
                          double* strains, double* stresses, double* forces, int* status);
 
+int orc_pcg_reorth_csr(int n, const int64_t* rp, const int* ci, const double* v, const double* b, double* x,
+                       double* P, double* Q, double* pq, int cap, int* count, int start, int max_it, double tol,
+                       int* iterations, double* rel_res);
 void orc_kl_field_gaussian(int ne, const double* cen, const double* L, int K, const double* w3, const double* amp3,
                            const int* idx3, const double* eig, int R, const double* xi, double mean, double cov,
                            double* E);
