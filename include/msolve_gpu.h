@@ -235,6 +235,22 @@ int MSG_KL_TABLE(const double* domain3, double corr_len, int n_terms, int n1d, d
  * MonteCarloAnalyzerWithStochasticMaterial.cs:258-261). */
 int MSG_KL_FIELD(MSG_MESH mesh, const MSG_KL* kl, int R, const double* xi, double* E);
 
+/* ------------------------------------------------------------------ polynomial chaos (Gaussian) */
+/* Basis of PolynomialChaosCoefficientsCalculator (ISAAR.MSolve.PreProcessor/Stochastic/
+ * PolynomialChaosCoefficientsCalculator.cs:30-300): the multi-indices of m Gaussian
+ * variables up to total degree p in the reference's order (P = MSG_PC_SIZE of them,
+ * basis [P][m]) and their squared norms prod_l alpha_l! (norms [P]). */
+int MSG_PC_SIZE(int m, int p, int* size);
+int MSG_PC_BASIS(int m, int p, int* basis, int* norms);
+/* The stochastic Galerkin product y = A u of PolynomialChaosSolverPCGMatrixCalculator.
+ * MultiplyWithMatrix (ISAAR.MSolve.Analyzers/PolynomialChaosSolverPCGMatrixCalculator.cs:1062-1089,
+ * Gaussian branch): y_j = <psi_j^2> K_0 u_j + sum_i sum_k <xi_i psi_j psi_k> K_i u_k,
+ * with K_0 the stiffness of the mean modulus and K_i that of the i-th KL term
+ * (kl->gaussian = 1, the first m terms; the Monte Carlo composition's matrices),
+ * applied element by element on a structured lattice in FP64. u, y: block-major
+ * [P][n_dofs] (host), the reference's vector layout. */
+int MSG_PC_GALERKIN_MATVEC(MSG_MESH mesh, double nu, const MSG_KL* kl, int m, int p, const double* u, double* y);
+
 /* ------------------------------------------------------------------ Monte Carlo batch */
 /* The realization loop of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
  * (ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:232-296):

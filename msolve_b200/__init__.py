@@ -11,6 +11,7 @@ from .analyzers import (GaussianStochasticCoefficientsProvider, GpuMatrix, GpuMe
                         MonteCarloAnalyzer, MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer,
                         SolverPCGReorthogonalizationSearchVectorCalculator, SolverPCGReorthogonalized, ProblemStructural, SolverPCG,
                         StaticAnalyzer, h8_mass_batch, h8_stiffness_batch, h8_stress_batch, realization_stresses)
+from .polynomial_chaos import PolynomialChaosSolverPCGMatrixCalculator, pc_basis
 from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, cantilever_model, clamped_block_model,
                     tip_dof)
 
@@ -21,5 +22,5 @@ __all__ = [
     "SolverPCGReorthogonalized", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
     "StaticAnalyzer", "h8_mass_batch", "h8_stiffness_batch", "h8_stress_batch", "realization_stresses",
     "Hexa8MeshGenerator", "MassAccelerationSinusoidalLoad",
-    "Model", "cantilever_model", "clamped_block_model", "tip_dof",
+    "Model", "PolynomialChaosSolverPCGMatrixCalculator", "pc_basis", "cantilever_model", "clamped_block_model", "tip_dof",
 ]

@@ -76,6 +76,9 @@ SIGNATURES = {
     "MSG_VERSION": (C.c_int, []),
     "MSG_H8_KE_BATCH": (C.c_int, [_vp, C.c_int, _d, _d, C.c_double, _d]),
     "MSG_H8_ME_BATCH": (C.c_int, [_vp, C.c_int, _d, C.c_double, _d]),
+    "MSG_PC_SIZE": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "MSG_PC_BASIS": (C.c_int, [C.c_int, C.c_int, _i, _i]),
+    "MSG_PC_GALERKIN_MATVEC": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, C.c_int, _d, _d]),
     "MSG_SVS_CREATE": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
     "MSG_SVS_CLEAR": (C.c_int, [_vp, C.c_int]),
     "MSG_SVS_COUNT": (C.c_int, [_vp, C.POINTER(C.c_int)]),

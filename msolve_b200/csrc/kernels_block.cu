@@ -227,6 +227,76 @@ __device__ __forceinline__ void pencil_of(const Lattice& L, int& J, int& Kz, boo
   Kz = k + 1;
 }
 
+// ---------------------------------------------------------------- polynomial-chaos Galerkin product
+// y_j = sum over the terms t of block j of c_t K(E_pos_t) u_k_t, FP64: the
+// stochastic Galerkin matrix-vector product of PolynomialChaosSolverPCGMatrixCalculator.
+// MultiplyWithMatrix (ISAAR.MSolve.Analyzers/PolynomialChaosSolverPCGMatrixCalculator.cs:1062-1089)
+// on a structured lattice, each K_pos applied element by element from its
+// field E_pos (value-class stencil, the pencil sweep of the FP64 residual).
+// One thread per node pencil and output block (lane = block j); terms are
+// accumulated in the reference's order (matrix, then input block) into the
+// thread's own outputs.
+__global__ void __launch_bounds__(128)
+    k_pc_matvec(Lattice L, const __grid_constant__ KhatD K, const double* __restrict__ u,
+                const double* __restrict__ Epc, int Mp, const uint8_t* __restrict__ mask,
+                const int* __restrict__ term_ptr, const int* __restrict__ term_pos, const int* __restrict__ term_k,
+                const double* __restrict__ term_c, int P, double* __restrict__ y) {
+  int J, Kz;
+  bool valid;
+  pencil_of(L, J, Kz, valid);
+  const int Pp = L.Rp;
+  const int j = blockIdx.y * 32 + threadIdx.x;
+  if (!valid || j >= P) return;
+  Lattice LE = L;
+  LE.Rp = Mp;  // the pencil sweep strides the element field by Rp
+  for (int t = term_ptr[j]; t < term_ptr[j + 1]; ++t) {
+    const int pos = term_pos[t], k = term_k[t];
+    const double c = term_c[t];
+    const bool first = t == term_ptr[j];
+    auto load = [&](size_t node, double* o) {
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) o[cc] = u[(node * 3 + cc) * Pp + k];
+    };
+    auto own = [](size_t, const double*) {};
+    auto emit = [&](size_t node, const double*, const double* yy) {
+      const uint32_t mk = mask[node];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const size_t o = (node * 3 + cc) * Pp + j;
+        const double v = ((mk >> cc) & 1) ? 0.0 : c * yy[cc];
+        y[o] = first ? v : y[o] + v;
+      }
+    };
+    pencil_sweep<double>(LE, K, J, Kz, Epc + pos, load, own, emit);
+  }
+}
+
+// E_pc[row(e)][0] = mean, E_pc[row(e)][1 + i] = mean * psi[i][e] (the field of
+// the i-th expansion term, GaussianFileStochasticCoefficientsProvider
+// GetCoefficientInternal scaled by the mean modulus)
+__global__ void k_pc_fields(int ne, int m, int Mp, double mean, const double* __restrict__ psi,
+                            const int* __restrict__ elem_row, double* __restrict__ Epc) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const size_t row = (size_t)elem_row[e];
+  Epc[row * Mp] = mean;
+  for (int i = 0; i < m; ++i) Epc[row * Mp + 1 + i] = mean * psi[(size_t)i * ne + e];
+}
+
+// block-major DOF vectors [P][n_dofs] <-> lattice layout [padded node][3][Pp]
+__global__ void k_pc_scatter(int n_dofs, int P, int Pp, const int* __restrict__ rows, const double* __restrict__ in,
+                             double* __restrict__ out) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (d < n_dofs && j < P) out[(size_t)rows[d] * Pp + j] = in[(size_t)j * n_dofs + d];
+}
+__global__ void k_pc_gather(int n_dofs, int P, int Pp, const int* __restrict__ rows, const double* __restrict__ in,
+                            double* __restrict__ out) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (d < n_dofs && j < P) out[(size_t)j * n_dofs + d] = in[(size_t)rows[d] * Pp + j];
+}
+
 // ---------------------------------------------------------------- TMA-staged FP32 operator
 // The production FP32 operator. A CTA owns a 2x2 tile of pencils (one warp
 // each) for 32 realizations. For every x-plane P one thread issues two TMA
@@ -3124,6 +3194,70 @@ int block_results(Context* ctx, BlockSys* B, int status, int* its_out, double* r
 }
 
 }  // namespace
+
+int pc_matvec(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int mo, int po, const double* u_host,
+              double* y_host) {
+  if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "the Galerkin product needs a structured lattice");
+  if (!kl->gaussian) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "the Galerkin product needs a Gaussian KL field");
+  if (mo < 1 || po < 1 || mo > kl->n_terms)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "polynomial chaos: need 1 <= m <= n_terms and p >= 1");
+  std::vector<int> tptr, tpos, tk;
+  std::vector<double> tc;
+  MSG_TRY(pc_gaussian_terms(mo, po, tptr, tpos, tk, tc));
+  const int P = (int)tptr.size() - 1;
+  const int Pp = (P + 31) / 32 * 32, Mp = mo + 1;
+  cudaStream_t st = ctx->stream;
+  double K576[576];
+  MSG_TRY(unit_cube_khat(ctx, m->h, nu, K576));
+  KhatD KD;
+  for (int c = 0; c < kKhatClasses; ++c) KD.v[c] = K576[kKhatRep[c]];
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, m, kl, &kd));
+  const size_t npad = (size_t)m->NXp * m->NYp * m->NZp;
+  DevMem dE, du, dy, dlat_u, dlat_y, dptr, dpos, dk, dc;
+  MSG_TRY(dE.alloc(ctx, sizeof(double) * npad * Mp));
+  MSG_TRY(du.alloc(ctx, sizeof(double) * (size_t)P * std::max(1, m->n_dofs)));
+  MSG_TRY(dy.alloc(ctx, sizeof(double) * (size_t)P * std::max(1, m->n_dofs)));
+  MSG_TRY(dlat_u.alloc(ctx, sizeof(double) * npad * 3 * Pp));
+  MSG_TRY(dlat_y.alloc(ctx, sizeof(double) * npad * 3 * Pp));
+  MSG_TRY(dptr.alloc(ctx, sizeof(int) * tptr.size()));
+  MSG_TRY(dpos.alloc(ctx, sizeof(int) * std::max<size_t>(1, tpos.size())));
+  MSG_TRY(dk.alloc(ctx, sizeof(int) * std::max<size_t>(1, tk.size())));
+  MSG_TRY(dc.alloc(ctx, sizeof(double) * std::max<size_t>(1, tc.size())));
+  MSG_CUDA(ctx, cudaMemcpyAsync(dptr.ptr, tptr.data(), sizeof(int) * tptr.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(dpos.ptr, tpos.data(), sizeof(int) * tpos.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(dk.ptr, tk.data(), sizeof(int) * tk.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(dc.ptr, tc.data(), sizeof(double) * tc.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(du.ptr, u_host, sizeof(double) * (size_t)P * m->n_dofs, cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(dE.ptr, 0, sizeof(double) * npad * Mp, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(dlat_u.ptr, 0, sizeof(double) * npad * 3 * Pp, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(dlat_y.ptr, 0, sizeof(double) * npad * 3 * Pp, st));
+  k_pc_fields<<<(m->n_elems + 127) / 128, 128, 0, st>>>(m->n_elems, mo, Mp, kl->mean, kd.psi,
+                                                        m->d_pad_elem_row.as<int>(), dE.as<double>());
+  const dim3 gd((m->n_dofs + 255) / 256, P);
+  if (m->n_dofs > 0)
+    k_pc_scatter<<<gd, 256, 0, st>>>(m->n_dofs, P, Pp, m->d_pad_free_rows.as<int>(), du.as<double>(),
+                                     dlat_u.as<double>());
+  Lattice L;
+  L.NX = m->nx + 1; L.NY = m->ny + 1; L.NZ = m->nz + 1;
+  L.NXp = m->NXp; L.NYp = m->NYp; L.NZp = m->NZp;
+  L.Rp = Pp;
+  L.tiles_j = (L.NY + kTJ - 1) / kTJ;
+  L.n_pad = (int)npad;
+  L.n_int = L.NX * L.NY * L.NZ;
+  const int n_tiles = L.tiles_j * ((L.NZ + kTK - 1) / kTK);
+  k_pc_matvec<<<dim3(n_tiles, Pp / 32), dim3(32, kWarps), 0, st>>>(
+      L, KD, dlat_u.as<double>(), dE.as<double>(), Mp, m->d_pad_mask.as<uint8_t>(), dptr.as<int>(), dpos.as<int>(),
+      dk.as<int>(), dc.as<double>(), P, dlat_y.as<double>());
+  if (m->n_dofs > 0)
+    k_pc_gather<<<gd, 256, 0, st>>>(m->n_dofs, P, Pp, m->d_pad_free_rows.as<int>(), dlat_y.as<double>(),
+                                    dy.as<double>());
+  count_launch(ctx, 4);
+  MSG_CUDA(ctx, cudaGetLastError());
+  MSG_CUDA(ctx, cudaMemcpyAsync(y_host, dy.ptr, sizeof(double) * (size_t)P * m->n_dofs, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  return MSG_OK;
+}
 
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out) {

@@ -832,6 +832,30 @@ int MSG_PCG_SOLVE_MIXED(MSG_MAT A, const double* b, double* x, int max_it, doubl
   return pcg_host(A, b, x, max_it, tol, iterations, rel_res, true);
 }
 
+int MSG_PC_SIZE(int m, int p, int* size) {
+  if (!size) return MSG_ERR_INVALID_ARGUMENT;
+  const int P = pc_size(m, p);
+  if (P < 0) return MSG_ERR_INVALID_ARGUMENT;
+  *size = P;
+  return MSG_OK;
+}
+
+int MSG_PC_BASIS(int m, int p, int* basis, int* norms) {
+  std::vector<int> b, n;
+  if (pc_basis(m, p, b, n) != MSG_OK) return MSG_ERR_INVALID_ARGUMENT;
+  if (basis) std::memcpy(basis, b.data(), sizeof(int) * b.size());
+  if (norms) std::memcpy(norms, n.data(), sizeof(int) * n.size());
+  return MSG_OK;
+}
+
+int MSG_PC_GALERKIN_MATVEC(MSG_MESH mesh, double nu, const MSG_KL* kl, int m, int p, const double* u, double* y) {
+  if (!mesh || !kl || !u || !y) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = mesh->ctx;
+  CTX_GUARD(ctx);
+  if (!(nu > -1.0 && nu < 0.5)) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "Poisson ratio out of (-1, 0.5)");
+  return pc_matvec(ctx, mesh, nu, kl, m, p, u, y);
+}
+
 int MSG_SVS_CREATE(MSG_MESH mesh, int capacity, MSG_SVS* out) {
   if (!mesh || !out) return MSG_ERR_INVALID_ARGUMENT;
   Context* ctx = mesh->ctx;

@@ -228,6 +228,17 @@ int svs_create(Context* ctx, Mesh* m, int capacity, SearchVectorStore** out);
 int pcg_reorth_solve(Context* ctx, Matrix* A, SearchVectorStore* S, const double* d_b, double* d_x, int start_mode,
                      int max_it, double tol, int* iterations, double* rel_res);
 
+// Polynomial chaos (pc.cpp): size of the basis of m Gaussian variables up to
+// degree p, the basis in the reference's order with its squared norms, and the
+// Galerkin terms of each output block (CSR over blocks: matrix, input block, weight).
+int pc_size(int m, int p);
+int pc_basis(int m, int p, std::vector<int>& basis, std::vector<int>& norms);
+int pc_gaussian_terms(int m, int p, std::vector<int>& term_ptr, std::vector<int>& term_pos, std::vector<int>& term_k,
+                      std::vector<double>& term_c);
+// y = Galerkin product of the block vector u [P][n_dofs] (host), kernels_block.cu
+int pc_matvec(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int mo, int po, const double* u_host,
+              double* y_host);
+
 // ---------------------------------------------------------------- kernel launchers (kernels_*.cu)
 int launch_h8_ke(Context* ctx, int n, const double* d_xyz, const double* d_E, double E_scalar, double nu,
                  double* d_K, int* d_status);

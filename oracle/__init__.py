@@ -78,6 +78,9 @@ def lib():
                                              C.c_double, C.c_double, _d]),
             "orc_pcg_reorth_csr": (C.c_int, [C.c_int, _i64, _i, _d, _d, _d, _d, _d, _d, C.c_int, _i, C.c_int,
                                              C.c_int, C.c_double, _i, _d]),
+            "orc_pc_size": (C.c_int, [C.c_int, C.c_int]),
+            "orc_pc_basis": (C.c_int, [C.c_int, C.c_int, _i, _i]),
+            "orc_pc_gaussian_matvec": (None, [C.c_int, _i64, _i, _d, C.c_int64, C.c_int, C.c_int, _d, _d]),
             "orc_num_threads": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -334,6 +337,23 @@ def pcg_reorth(csr, store, b, start=False, max_it=20000, tol=1e-7):
                                   tol, C.byref(it), C.byref(rr))
     store.count = cnt.value
     return x, dict(status=st, iterations=it.value, rel_res=rr.value)
+
+
+def pc_basis(m, p):
+    P = lib().orc_pc_size(m, p)
+    basis = np.zeros((P, m), dtype=np.int32)
+    norms = np.zeros(P, dtype=np.int32)
+    lib().orc_pc_basis(m, p, _p(basis, _i), _p(norms, _i))
+    return basis, norms
+
+
+def pc_gaussian_matvec(csr, vals, m, p, u):
+    """Galerkin product over the m + 1 matrices vals [m+1][nnz] of csr's pattern."""
+    vals = _f64(vals)
+    u = _f64(u)
+    y = np.zeros_like(u)
+    lib().orc_pc_gaussian_matvec(csr.n, _p(csr.rp, _i64), _p(csr.ci, _i), _p(vals), vals.shape[1], m, p, _p(u), _p(y))
+    return y
 
 
 # ---------------------------------------------------------------- KL field

@@ -892,6 +892,92 @@ void orc_kl_field_gaussian(int ne, const double* cen, const double* L, int K, co
     }
 }
 
+// PolynomialChaosCoefficientsCalculator (PolynomialChaosCoefficientsCalculator.cs:30-300):
+// basis size sum_k C(m+k-1, k), multi-indices in the reference's generation
+// order (bar positions t of each total degree, advanced from the right), norms
+// prod_l alpha_l!.
+static double orc_fact(int f) {
+  double r = 1;
+  for (int i = 2; i <= f; ++i) r *= i;
+  return r;
+}
+int orc_pc_size(int m, int p) {
+  double s = 0;
+  for (int k = 0; k <= p; ++k) s += orc_fact(m + k - 1) / (orc_fact(k) * orc_fact(m - 1));
+  return (int)s;
+}
+int orc_pc_basis(int m, int p, int* basis, int* norms) {
+  const int P = orc_pc_size(m, p);
+  for (int i = 0; i < P * m; ++i) basis[i] = 0;
+  if (m == 1) {
+    for (int i = 0; i < p; ++i) basis[(i + 1) * m] = i;
+  } else {
+    const int mm = m - 1;
+    std::vector<int> t(mm);
+    int n = 0;
+    for (int cur = 1; cur <= p; ++cur) {
+      bool end = false, first = false;
+      while (!end) {
+        ++n;
+        if (!first) {
+          for (int i = 0; i < mm; ++i) t[i] = i + 1;
+          first = true;
+        } else if (t[mm - 1] < mm + cur) {
+          t[mm - 1] += 1;
+        } else {
+          int j = mm;
+          while (t[j - 1] == j + cur) --j;
+          t[j - 1]++;
+          for (int k = j; k < mm; ++k) t[k] = t[j - 1] + k - j + 1;
+        }
+        basis[n * m + 0] = t[0] - 1;
+        for (int i = 1; i < mm; ++i) basis[n * m + i] = t[i] - t[i - 1] - 1;
+        basis[n * m + mm] = m + cur - t[mm - 1] - 1;
+        if (t[0] == cur + 1) end = true;
+      }
+    }
+  }
+  for (int k = 0; k < P; ++k) {
+    int nn = 1;
+    for (int j = 0; j < m; ++j) nn *= (int)orc_fact(basis[k * m + j]);
+    norms[k] = nn;
+  }
+  return P;
+}
+
+// PolynomialChaosSolverPCGMatrixCalculator.MultiplyWithMatrix (:1062-1089), Gaussian
+// branch, over m + 1 CSR matrices of one pattern (vals [m+1][nnz]): y = 0; for pos,
+// for each (i, j, c) of GaussianCoefficients[pos] (PolynomialChaosCoefficientsCalculator
+// .cs:294-326): y[block i] += c * K_pos u[block j]. u, y [P][n].
+void orc_pc_gaussian_matvec(int n, const int64_t* rp, const int* ci, const double* vals, int64_t nnz, int m, int p,
+                            const double* u, double* y) {
+  const int P = orc_pc_size(m, p);
+  std::vector<int> basis((size_t)P * m), norms(P);
+  orc_pc_basis(m, p, basis.data(), norms.data());
+  std::vector<double> tmp(n);
+  for (int64_t i = 0; i < (int64_t)P * n; ++i) y[i] = 0.0;
+  auto apply = [&](int pos, int i, int j, double c) {
+    orc_csr_multiply(n, rp, ci, vals + (int64_t)pos * nnz, u + (int64_t)j * n, tmp.data());
+    for (int r = 0; r < n; ++r) y[(int64_t)i * n + r] += c * tmp[r];
+  };
+  for (int i = 0; i < P; ++i) apply(0, i, i, (double)norms[i]);
+  for (int v = 0; v < m; ++v)
+    for (int j = 0; j < P; ++j)
+      for (int k = 0; k < P; ++k) {
+        bool almost = false;
+        for (int l = 0; l < m; ++l)
+          if (l != v && basis[j * m + l] != basis[k * m + l]) {
+            almost = true;
+            break;
+          }
+        if (almost) continue;
+        if (basis[k * m + v] == basis[j * m + v] - 1)
+          apply(v + 1, j, k, (double)norms[j]);
+        else if (basis[k * m + v] == basis[j * m + v] + 1)
+          apply(v + 1, j, k, (double)norms[j] * (basis[j * m + v] + 1));
+      }
+}
+
 // One FP64 static solve of a structured nx*ny*nz block of h-cubes: element
 // stiffness through the Fortran restatement with each element's E, CSR
 // assembly over the free DOFs, Jacobi-PCG with SolverPCG semantics.

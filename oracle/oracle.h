@@ -46,6 +46,10 @@ void orc_h8_stress_batch(int n, const double* xyz, const double* E, double nu, c
 int orc_pcg_reorth_csr(int n, const int64_t* rp, const int* ci, const double* v, const double* b, double* x,
                        double* P, double* Q, double* pq, int cap, int* count, int start, int max_it, double tol,
                        int* iterations, double* rel_res);
+int orc_pc_size(int m, int p);
+int orc_pc_basis(int m, int p, int* basis, int* norms);
+void orc_pc_gaussian_matvec(int n, const int64_t* rp, const int* ci, const double* vals, int64_t nnz, int m, int p,
+                            const double* u, double* y);
 void orc_kl_field_gaussian(int ne, const double* cen, const double* L, int K, const double* w3, const double* amp3,
                            const int* idx3, const double* eig, int R, const double* xi, double mean, double cov,
                            double* E);
