@@ -366,7 +366,10 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * "multigrid_sweeps" (damped Jacobi sweeps on the coarsest level, default 20),
  * "multigrid_omega" (Jacobi damping of every level, 0 = derived from the
  * element stiffness, default), "multigrid_delta" (reliable-update factor of the
- * V-cycle loop, default 0.01; its inner chunk is 2 iterations).
+ * V-cycle loop, default 0.01; its inner chunk is 2 iterations), "multigrid_packed"
+ * (1, default: the three level-0 operator passes of an iteration work on two
+ * realizations per thread with packed FP32 arithmetic; 0: one per thread).
+ * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);

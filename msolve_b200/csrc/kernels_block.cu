@@ -534,6 +534,14 @@ using ModalCD = ModalCT<double>;
 template <class T> __device__ __forceinline__ T fmx(T a, T b, T c);
 template <> __device__ __forceinline__ float fmx<float>(float a, float b, float c) { return fmaf(a, b, c); }
 template <> __device__ __forceinline__ double fmx<double>(double a, double b, double c) { return fma(a, b, c); }
+// Two realizations in one register pair: Blackwell's packed FP32 instructions
+// (one issue slot for both halves of a float2)
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 operator*(float2 a, float2 b) { return __fmul2_rn(a, b); }
+template <> __device__ __forceinline__ float2 fmx<float2>(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+template <class T> __device__ __forceinline__ T zero_of() { return T(0); }
+template <> __device__ __forceinline__ float2 zero_of<float2>() { return make_float2(0.f, 0.f); }
 
 constexpr int kMJ = 3, kMK = 3;                       // node pencils per tile
 constexpr int kMEJ = kMJ + 1, kMEK = kMK + 1;         // element pencils per tile
@@ -633,7 +641,7 @@ __device__ __forceinline__ void modal_apply(const ModalCT<T>& C, T E, const T (&
 #pragma unroll
   for (int c = 0; c < 3; ++c) {  // D and the null modes
     y1[c][3] = Eda * U1(3, c);
-    y0[c][0] = T(0);
+    y0[c][0] = zero_of<T>();
   }
   if constexpr (kMass) {
 #pragma unroll
@@ -1132,6 +1140,287 @@ __global__ void __launch_bounds__(kMThreads, 1)
 #pragma unroll
         for (int i = 0; i < kMJ * kMK; ++i) sum += red[i * 32 + lane];
         partial[((size_t)tile * Rp + rr) * pstride] = sum;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- packed level operator (level 0)
+// k_lvl_op with two realizations per lane in float2 registers: the element and
+// node arithmetic issues Blackwell's packed FP32 instructions (one issue slot
+// for both), halving the instructions per realization of an issue-bound
+// kernel. The doubled register state (up to 152 registers a thread) allows
+// 3 warps per SM sub-partition: a 3 x 2 tile of node pencils with its 12
+// element warps for 64 realizations, and no separate producer warp: lane 0
+// of warp 0 issues the TMA loads two planes ahead (the 3-stage ring refills
+// the stage of the plane before the current one; its readers have arrived on
+// its "empty" barrier, a bounded wait). Modes, exchange, barriers and bounded
+// waits as k_lvl_op otherwise.
+constexpr int kQJ = 3, kQK = 2;                     // node pencils per tile (y, z)
+constexpr int kQEJ = kQJ + 1, kQEK = kQK + 1;       // element pencils 4 x 3
+constexpr int kQWarps = kQEJ * kQEK;                // 12 element warps
+constexpr int kQThreads = 32 * kQWarps;
+constexpr int kQPJ = kQJ + 2, kQPK = kQK + 2;       // node patch 5 x 4
+constexpr int kQR = 64;                             // realizations per work item
+constexpr int kQPlane = kQR * 3 * kQPJ * kQPK;      // vector patch (floats)
+constexpr int kQNode = kQR * kQPJ * kQPK;           // dinv patch
+constexpr int kQE = kQR * kQEJ * kQEK;              // E patch
+constexpr int kQD = kQR * 3 * kQJ * kQK;            // d of the tile's own nodes
+constexpr int kQX = kQWarps * 4 * 3 * kQR;          // exchange buffer
+template <int kMode> struct LvlStage2 {
+  static constexpr bool kTwo = kMode == kLvlStart || kMode == kLvlPcgZ;
+  static constexpr int kOffA = 0;
+  static constexpr int kOffB = kQPlane;
+  static constexpr int kOffN = (kTwo ? 2 : 1) * kQPlane;
+  static constexpr int kOffE = kOffN + (kMode == kLvlStart ? kQNode : 0);
+  static constexpr int kOffD = kOffE + kQE;
+  static constexpr int kFloats = kOffD + (kMode == kLvlPcgZ ? kQD : 0);
+  static constexpr uint32_t kBytes = kFloats * 4;
+  static constexpr size_t kSmem = 128 + sizeof(float) * ((size_t)kMStages * kFloats + 2 * (size_t)kQX) +
+                                  sizeof(double) * kQJ * kQK * kQR + sizeof(uint64_t) * (2 * kMStages);
+};
+static_assert(LvlStage2<kLvlStart>::kBytes % 128 == 0 && LvlStage2<kLvlSmooth>::kBytes % 128 == 0 &&
+                  LvlStage2<kLvlPcgZ>::kBytes % 128 == 0,
+              "stage alignment");
+static_assert(LvlStage2<kLvlPcgZ>::kSmem <= 227 * 1024 && LvlStage2<kLvlStart>::kSmem <= 227 * 1024, "smem");
+
+template <int kMode, bool kMass>
+__global__ void __maxnreg__(152)
+    k_lvl_op2(Lattice L, const __grid_constant__ ModalCT<float2> C, const __grid_constant__ CUtensorMap tm_a,
+              const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_n,
+              const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_d, int tiles_j,
+              int n_tiles, int n_items, const uint8_t* __restrict__ mask, const float* __restrict__ b,
+              const float* __restrict__ dinv, float omega, const float* __restrict__ alpha,
+              const float* __restrict__ beta, float* __restrict__ out, float* __restrict__ out2,
+              float* __restrict__ out3, float* __restrict__ d, double* __restrict__ partial, int pstride,
+              int* __restrict__ err) {
+  using S = LvlStage2<kMode>;
+  extern __shared__ __align__(128) float smem_dyn[];
+  float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
+  float* xbuf = smem + kMStages * S::kFloats;
+  double* red = reinterpret_cast<double*>(xbuf + 2 * kQX);  // [node pencils][64]
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + kQJ * kQK * kQR);
+  uint64_t* empty = full + kMStages;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int NX = L.NX, Rp = L.Rp, Rp2 = L.Rp >> 1;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kMStages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kQWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // producer role: global step q loads (item, plane) = (blockIdx.x + (q / NX) gridDim.x, q % NX + 1)
+  // into stage q % 3
+  const bool producer = w == 0 && lane == 0;
+  auto produce = [&](uint32_t q) {
+    const int item = blockIdx.x + (int)(q / (uint32_t)NX) * gridDim.x;
+    if (item >= n_items) return;
+    const int P = (int)(q % (uint32_t)NX) + 1;
+    const int tile = item % n_tiles, g64 = (item / n_tiles) * kQR;
+    const int J0 = 1 + (tile % tiles_j) * kQJ, K0 = 1 + (tile / tiles_j) * kQK;
+    const int st = q % kMStages;
+    const uint32_t use = q / kMStages;
+    if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+      atomicExch(err, 1);
+      return;
+    }
+    float* dst = smem + st * S::kFloats;
+    mbar_expect_tx(&full[st], S::kBytes);
+    tma_load_5d(dst + S::kOffA, &tm_a, g64, 0, P, J0 - 1, K0 - 1, &full[st]);
+    if constexpr (S::kTwo) tma_load_5d(dst + S::kOffB, &tm_b, g64, 0, P, J0 - 1, K0 - 1, &full[st]);
+    if constexpr (kMode == kLvlStart) tma_load_4d(dst + S::kOffN, &tm_n, g64, P, J0 - 1, K0 - 1, &full[st]);
+    tma_load_4d(dst + S::kOffE, &tm_e, g64, P - 1, J0 - 1, K0 - 1, &full[st]);
+    if constexpr (kMode == kLvlPcgZ) tma_load_5d(dst + S::kOffD, &tm_d, g64, 0, P, J0, K0, &full[st]);
+  };
+  if (producer) {
+    produce(0);
+    produce(1);
+  }
+  const int ej = w % kQEJ, ek = w / kQEJ;
+  const bool node_warp = ej >= 1 && ek >= 1;
+  uint32_t seq = 0;
+  int xsel = 0;
+  bool dead = false;
+  auto csync = [&]() { asm volatile("bar.sync 1, %0;" ::"r"(kQWarps * 32) : "memory"); };
+  const float2 z2 = make_float2(0.f, 0.f);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int tile = item % n_tiles, g64 = (item / n_tiles) * kQR;
+    const int J0 = 1 + (tile % tiles_j) * kQJ, K0 = 1 + (tile / tiles_j) * kQK;
+    const int Je = J0 - 1 + ej, Ke = K0 - 1 + ek;
+    auto realj = [&](int j) { return j >= 1 && j <= L.NY - 1; };
+    auto realk = [&](int k) { return k >= 1 && k <= L.NZ - 1; };
+    const bool real = realj(Je) && realk(Ke);
+    const bool node_ok = node_warp && Je <= L.NY && Ke <= L.NZ;
+    const bool r00 = real, r10 = realj(Je - 1) && realk(Ke);
+    const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
+    const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;
+    const int rr2 = (g64 >> 1) + lane;  // float2 index of this lane's realization pair
+    float2 al = z2, be = z2;
+    if constexpr (kMode == kLvlStart || kMode == kLvlPcgZ) al = reinterpret_cast<const float2*>(alpha)[rr2];
+    if constexpr (kMode == kLvlPcgZ) be = reinterpret_cast<const float2*>(beta)[rr2];
+    const float2 nal = make_float2(-al.x, -al.y);
+    const float2 om2 = make_float2(omega, omega);
+    const float2* xb2 = reinterpret_cast<const float2*>(xbuf);
+    float2* out_2 = reinterpret_cast<float2*>(out);
+    float2 Bp[3][4], T0[3][4];
+    float2 ou[3] = {z2, z2, z2}, orc[3] = {z2, z2, z2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) T0[c][qq] = z2;
+    double acc0 = 0.0, acc1 = 0.0;
+    uint32_t mreg = 0;
+    auto node_phase = [&](int X) {
+      if (((X - 1) & 31) == 0) {
+        const int pl = X + lane;
+        mreg = (pl <= NX) ? mask[nrow + pl] : 0u;
+      }
+      const uint32_t mk = __shfl_sync(0xffffffffu, mreg, (X - 1) & 31);
+      const float2* xb = xb2 + xsel * (kQX / 2);
+      const size_t node = nrow + X;
+      float2 wdv = z2;
+      if constexpr (kMode == kLvlSmooth) wdv = om2 * reinterpret_cast<const float2*>(dinv)[node * Rp2 + rr2];
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float2 y = z2;
+        if (r00) y = y + xb[((w * 4 + 0) * 3 + c) * 32 + lane];
+        if (r10) y = y + xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
+        if (r01) y = y + xb[(((w - kQEJ) * 4 + 2) * 3 + c) * 32 + lane];
+        if (r11) y = y + xb[(((w - kQEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        const size_t o = (node * 3 + c) * Rp2 + rr2;
+        const bool fixed = (mk >> c) & 1;
+        float2 v;
+        if constexpr (kMode == kLvlStart) {
+          v = fixed ? z2 : orc[c] - y;
+          s0 = fma((double)orc[c].x, (double)orc[c].x, s0);
+          s1 = fma((double)orc[c].y, (double)orc[c].y, s1);
+        } else if constexpr (kMode == kLvlResid) {
+          v = fixed ? z2 : reinterpret_cast<const float2*>(b)[o] - y;
+        } else if constexpr (kMode == kLvlSmooth) {
+          const float2 bv = reinterpret_cast<const float2*>(b)[o];
+          v = fixed ? z2 : fmx(wdv, bv - y, ou[c]);
+          s0 = fma((double)v.x, (double)bv.x, s0);
+          s1 = fma((double)v.y, (double)bv.y, s1);
+        } else {
+          v = fixed ? z2 : y;
+          s0 = fma((double)ou[c].x, (double)v.x, s0);
+          s1 = fma((double)ou[c].y, (double)v.y, s1);
+        }
+        out_2[o] = v;
+      }
+      acc0 += s0;
+      acc1 += s1;
+    };
+    auto emit_corners = [&](const float2 (&B)[3][4]) {
+      float2 y[2][2][3];
+      yz_inverse(B, y);
+      float2* xb = reinterpret_cast<float2*>(xbuf) + xsel * (kQX / 2);
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
+    };
+    for (int P = 1; P <= NX; ++P, ++seq) {
+      const int st = seq % kMStages;
+      if (producer && !dead) produce(seq + 2);
+      if (!dead && !mbar_wait(&full[st], (seq / kMStages) & 1)) {
+        atomicExch(err, 1);
+        dead = true;
+      }
+      const float* pt = smem + st * S::kFloats;
+      const float2* pa = reinterpret_cast<const float2*>(pt + S::kOffA);
+      const float2* pb = reinterpret_cast<const float2*>(pt + S::kOffB);
+      float2 u[2][2][3], rc[3] = {z2, z2, z2};
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az) {
+          const int o = (ek + az) * kQPJ + (ej + ay);
+          float2 wdv = z2;
+          if constexpr (kMode == kLvlStart)
+            wdv = om2 * reinterpret_cast<const float2*>(pt + S::kOffN)[o * 32 + lane];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int i = (o * 3 + c) * 32 + lane;
+            if constexpr (kMode == kLvlStart) {
+              const float2 rn = fmx(nal, pb[i], pa[i]);
+              u[ay][az][c] = wdv * rn;
+              if (ay == 0 && az == 0) rc[c] = rn;
+            } else if constexpr (kMode == kLvlPcgZ) {
+              u[ay][az][c] = fmx(be, pb[i], pa[i]);
+            } else {
+              u[ay][az][c] = pa[i];
+            }
+          }
+        }
+      const float2 E = reinterpret_cast<const float2*>(pt + S::kOffE)[w * 32 + lane];
+      if constexpr (kMode == kLvlStart || kMode == kLvlPcgZ) {
+        if (node_ok) {
+          const size_t node = nrow + P;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const size_t o = (node * 3 + c) * Rp2 + rr2;
+            if constexpr (kMode == kLvlStart) {
+              reinterpret_cast<float2*>(out2)[o] = rc[c];
+              reinterpret_cast<float2*>(out3)[o] = u[0][0][c];
+            } else {
+              const int op = ek * kQPJ + ej, od = (ek - 1) * kQJ + (ej - 1);
+              const float2 pold = pb[(op * 3 + c) * 32 + lane];
+              const float2 dold = reinterpret_cast<const float2*>(pt + S::kOffD)[(od * 3 + c) * 32 + lane];
+              reinterpret_cast<float2*>(out2)[o] = u[0][0][c];
+              reinterpret_cast<float2*>(d)[o] = fmx(al, pold, dold);
+            }
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      float2 Bc[3][4];
+      yz_forward(u, Bc);
+      if (P >= 2) {
+        if (real) {
+          float2 C1[3][4];
+          modal_apply<kMass>(C, E, Bp, Bc, T0, C1);
+          emit_corners(T0);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
+        }
+        csync();
+        if (node_ok) node_phase(P - 1);
+        xsel ^= 1;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ou[c] = u[0][0][c];
+        orc[c] = rc[c];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) Bp[c][qq] = Bc[c][qq];
+      }
+    }
+    if (real) emit_corners(T0);
+    csync();
+    if (node_ok) node_phase(NX);
+    xsel ^= 1;
+    if (kMode != kLvlResid && partial != nullptr) {
+      if (node_warp) {
+        const int nw = (ek - 1) * kQJ + (ej - 1);
+        red[nw * kQR + 2 * lane] = acc0;
+        red[nw * kQR + 2 * lane + 1] = acc1;
+      }
+      csync();
+      if (w < 2) {
+        const int rl = w * 32 + lane;  // realization within the item
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < kQJ * kQK; ++i) sum += red[i * kQR + rl];
+        partial[((size_t)tile * Rp + g64 + rl) * pstride] = sum;
       }
     }
   }
@@ -2335,6 +2624,11 @@ struct BlockSys {
   GmgLevel lv[kGmgMaxLevels];
   WSlot xs, arena;
   CUtensorMap tm_xs;
+  // packed level-0 operator (k_lvl_op2: 64 realizations per item, 3 x 2 tiles)
+  bool pack = false;
+  ModalCT<float2> MC2;
+  int tiles_j2 = 0, n_tiles2 = 0, n_items2 = 0, grid2 = 0;
+  CUtensorMap tm2_rA, tm2_rB, tm2_qA, tm2_qB, tm2_pA, tm2_pB, tm2_xs, tm2_dinv, tm2_e, tm2_d;
 };
 
 // Largest eigenvalue of diag(K)^-1 K for one element (power iteration on the
@@ -2716,6 +3010,50 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
         if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS || r3 != CUDA_SUCCESS)
           return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (multigrid level %d)", l);
       }
+      // packed level-0 operator: realizations in multiples of 64
+      B->pack = ctx->mg_packed && (Rp % kQR) == 0;
+      if (B->pack) {
+        const ModalC& f = B->MC;
+        auto b2 = [](float v) { return make_float2(v, v); };
+        ModalCT<float2>& g2 = B->MC2;
+        g2.vd = b2(f.vd); g2.vb = b2(f.vb); g2.sa = b2(f.sa); g2.sb = b2(f.sb); g2.pa = b2(f.pa); g2.pb = b2(f.pb);
+        g2.td = b2(f.td); g2.tb = b2(f.tb); g2.da = b2(f.da);
+        for (int i = 0; i < 8; ++i) g2.m[i] = b2(f.m[i]);
+        B->tiles_j2 = (L.NY + kQJ - 1) / kQJ;
+        B->n_tiles2 = B->tiles_j2 * ((L.NZ + kQK - 1) / kQK);
+        B->n_items2 = B->n_tiles2 * (Rp / kQR);
+        B->grid2 = std::min(B->n_items2, ctx->sm_count);
+        // the loop's partials: [tile][Rp][2] and [tile][Rp] over the packed tiles
+        const size_t need = sizeof(double) * (size_t)std::max({B->n_tiles * 2, B->n_tiles_m * kMParts,
+                                                                B->n_tiles2 * 3}) * Rp;
+        MSG_TRY(B->slot_alloc(ctx, 9, need, &B->part_op.ptr));
+        const cuuint32_t pb2[5] = {kQR, 3, 1, kQPJ, kQPK};
+        const cuuint32_t nb2[4] = {kQR, 1, kQPJ, kQPK};
+        const cuuint32_t eb2[4] = {kQR, 1, kQEJ, kQEK};
+        const cuuint32_t db2[5] = {kQR, 3, 1, kQJ, kQK};
+        const CUresult r2[10] = {enc5(&B->tm2_rA, B->r32.ptr, pb2), enc5(&B->tm2_rB, B->rB.ptr, pb2),
+                                 enc5(&B->tm2_qA, B->q.ptr, pb2),   enc5(&B->tm2_qB, B->qB.ptr, pb2),
+                                 enc5(&B->tm2_pA, B->p.ptr, pb2),   enc5(&B->tm2_pB, B->pB.ptr, pb2),
+                                 enc5(&B->tm2_xs, B->xs.ptr, pb2),  enc4(&B->tm2_dinv, B->dinv.ptr, nb2),
+                                 enc4(&B->tm2_e, B->E32.ptr, eb2),  enc5(&B->tm2_d, B->d.ptr, db2)};
+        for (CUresult r : r2)
+          if (r != CUDA_SUCCESS) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (packed)");
+        static std::once_flag pack_once;
+        static cudaError_t pack_err = cudaSuccess;
+        std::call_once(pack_once, [] {
+          const std::pair<const void*, size_t> fs[] = {
+              {(const void*)k_lvl_op2<kLvlStart, false>, LvlStage2<kLvlStart>::kSmem},
+              {(const void*)k_lvl_op2<kLvlStart, true>, LvlStage2<kLvlStart>::kSmem},
+              {(const void*)k_lvl_op2<kLvlSmooth, false>, LvlStage2<kLvlSmooth>::kSmem},
+              {(const void*)k_lvl_op2<kLvlSmooth, true>, LvlStage2<kLvlSmooth>::kSmem},
+              {(const void*)k_lvl_op2<kLvlPcgZ, false>, LvlStage2<kLvlPcgZ>::kSmem},
+              {(const void*)k_lvl_op2<kLvlPcgZ, true>, LvlStage2<kLvlPcgZ>::kSmem}};
+          for (const auto& f : fs)
+            if (pack_err == cudaSuccess)
+              pack_err = cudaFuncSetAttribute(f.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.second);
+        });
+        MSG_CUDA(ctx, pack_err);
+      }
       static std::once_flag lvl_once;
       static cudaError_t lvl_err = cudaSuccess;
       std::call_once(lvl_once, [] {
@@ -2821,8 +3159,9 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   const bool even = (it & 1) == 0;
   const int nl = B->n_lvl;
   const float om = B->omega;
+  const int nt0 = B->pack ? B->n_tiles2 : B->n_tiles_m;  // tiles of the level-0 launches
   double* part2 = B->part_op.as<double>();
-  double* part1 = part2 + (size_t)2 * B->n_tiles_m * Rp;
+  double* part1 = part2 + (size_t)2 * nt0 * Rp;
   float* r_in = even ? B->r32.as<float>() : B->rB.as<float>();
   float* r_out = even ? B->rB.as<float>() : B->r32.as<float>();
   float* p_out = even ? B->pB.as<float>() : B->p.as<float>();
@@ -2840,14 +3179,29 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
                                                        dinv, om, s.alpha, s.beta, out, out2, out3, d, partial,
                                                        pstride, s.err);
   };
+  // level 0 with two realizations per lane (k_lvl_op2) where the batch allows it
+  auto lvl0 = [&](auto mode, const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& ta2,
+                  const CUtensorMap& tb2, const float* b, const float* dinv, float* out, float* out2, float* out3,
+                  float* d, double* partial, int pstride) {
+    constexpr int kMode = decltype(mode)::value;
+    if (B->pack) {
+      auto k = mass ? k_lvl_op2<kMode, true> : k_lvl_op2<kMode, false>;
+      k<<<B->grid2, kQThreads, LvlStage2<kMode>::kSmem, st>>>(
+          B->L, B->MC2, ta2, tb2, B->tm2_dinv, B->tm2_e, B->tm2_d, B->tiles_j2, B->n_tiles2, B->n_items2, B->mask, b,
+          dinv, om, s.alpha, s.beta, out, out2, out3, d, partial, pstride, s.err);
+    } else {
+      lvl(mode, B->L, B->MC, ta, tb, B->tm_dinvm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m, B->n_items_m,
+          B->grid_m, B->mask, b, dinv, out, out2, out3, d, partial, pstride);
+    }
+  };
   using Start = std::integral_constant<int, kLvlStart>;
   using Resid = std::integral_constant<int, kLvlResid>;
   using Smooth = std::integral_constant<int, kLvlSmooth>;
   using PcgZ = std::integral_constant<int, kLvlPcgZ>;
   if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
   // level 0: r' = r - alpha q, xs = omega dinv r', qB = r' - A xs, partial r'.r'
-  lvl(Start{}, B->L, B->MC, tm_rin, B->tm_qAm, B->tm_dinvm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m,
-      B->n_items_m, B->grid_m, B->mask, nullptr, nullptr, qB, r_out, B->xs.as<float>(), nullptr, part2, 2);
+  lvl0(Start{}, tm_rin, B->tm_qAm, even ? B->tm2_rA : B->tm2_rB, B->tm2_qA, nullptr, nullptr, qB, r_out,
+       B->xs.as<float>(), nullptr, part2, 2);
   // down: restrict the residual, residual of the first sweep on every level but the coarsest
   for (int l = 1; l < nl; ++l) {
     GmgLevel& g = B->lv[l];
@@ -2883,17 +3237,16 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   k_prolong_add<<<(unsigned)(((long)B->L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(
       B->L, B->lv[1].L, B->interior, B->mask, res_c, B->xs.as<float>());
   // level 0 post-sweep: z (into qB) and the partial z.r'
-  lvl(Smooth{}, B->L, B->MC, B->tm_xs, B->tm_xs, B->tm_xs, B->tm_em, B->tm_xs, B->tiles_jm, B->n_tiles_m,
-      B->n_items_m, B->grid_m, B->mask, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr, part2 + 1, 2);
+  lvl0(Smooth{}, B->tm_xs, B->tm_xs, B->tm2_xs, B->tm2_xs, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr,
+       part2 + 1, 2);
   cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
-  k_gmg_beta<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part2, s, c.delta2, c.tol2);
+  k_gmg_beta<<<c.sblocks, 1024, 0, st>>>(Rp, nt0, part2, s, c.delta2, c.tol2);
   // p = z + beta p_old, d += alpha p_old, q = A p, partial p.q
   if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-  lvl(PcgZ{}, B->L, B->MC, B->tm_qBm, tm_pin, B->tm_qBm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m,
-      B->n_items_m, B->grid_m, B->mask, nullptr, nullptr, B->q.as<float>(), p_out, nullptr, B->d.as<float>(), part1,
-      1);
+  lvl0(PcgZ{}, B->tm_qBm, tm_pin, B->tm2_qB, even ? B->tm2_pA : B->tm2_pB, nullptr, nullptr, B->q.as<float>(), p_out,
+       nullptr, B->d.as<float>(), part1, 1);
   if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
-  k_gmg_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part1, s);
+  k_gmg_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, nt0, part1, s);
   if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
 }
 
@@ -2939,13 +3292,19 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
     }
     const int mm[6] = {modal ? 1 : 0, B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
     mix(mm, sizeof(mm));
-    const int gg[3] = {B->gmg ? 1 : 0, B->n_lvl, B->sweeps};
+    const int gg[4] = {B->gmg ? 1 : 0, B->n_lvl, B->sweeps, B->pack ? 1 : 0};
     mix(gg, sizeof(gg));
     if (B->gmg) {
       mix(&B->omega, sizeof(B->omega));
       mix(&B->xs.ptr, sizeof(void*));
       mix(&B->tm_xs, sizeof(CUtensorMap));
       for (int l = 1; l < B->n_lvl; ++l) mix(&B->lv[l], sizeof(GmgLevel));
+      if (B->pack) {
+        const CUtensorMap* t2[10] = {&B->tm2_rA, &B->tm2_rB, &B->tm2_qA, &B->tm2_qB, &B->tm2_pA,
+                                     &B->tm2_pB, &B->tm2_xs, &B->tm2_dinv, &B->tm2_e, &B->tm2_d};
+        for (const CUtensorMap* t : t2) mix(t, sizeof(CUtensorMap));
+        mix(&B->MC2, sizeof(B->MC2));
+      }
     }
     const double dd[2] = {c.delta2, c.tol2};
     mix(dd, sizeof(dd));
@@ -3470,7 +3829,7 @@ int lane_create(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, const double
   L->ctx = ctx;
   L->m = m;
   retain(m);
-  const int Rp = (capacity + 31) / 32 * 32;
+  const int Rp = (capacity + 63) / 64 * 64;  // 64-wide groups: the packed level operator
   L->capacity = Rp;
   L->tol = tol;
   L->max_it = max_it;

@@ -413,7 +413,8 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
   if (R <= 0 || !kl || !d_xi || !d_b || max_it <= 0 || !(tol > 0))
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "MC batch: invalid arguments");
   if (tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
-  const int Rp = (R + 31) / 32 * 32;
+  // realizations padded to 64: the packed level operator works on pairs of 32-wide groups
+  const int Rp = (R + 63) / 64 * 64;
   MSG_TRY(context_resources(ctx));
   cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   cudaEventRecord(e0, ctx->stream);
@@ -571,6 +572,7 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   }
   if (!std::strcmp(key, "multigrid_omega") && value >= 0 && value < 1) { ctx->mg_omega = value; return MSG_OK; }
   if (!std::strcmp(key, "multigrid_delta") && value > 0 && value < 1) { ctx->mg_delta = value; return MSG_OK; }
+  if (!std::strcmp(key, "multigrid_packed") && (value == 0 || value == 1)) { ctx->mg_packed = (int)value; return MSG_OK; }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 
@@ -1021,7 +1023,8 @@ int MSG_NEWMARK_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const doub
   CTX_GUARD(ctx);
   if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "Newmark batch needs a structured cube lattice");
   if (tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
-  const int Rp = (R + 31) / 32 * 32;
+  // realizations padded to 64: the packed level operator works on pairs of 32-wide groups
+  const int Rp = (R + 63) / 64 * 64;
   MSG_TRY(context_resources(ctx));
   cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
   cudaEventRecord(e0, ctx->stream);

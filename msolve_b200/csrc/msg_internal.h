@@ -79,6 +79,7 @@ struct Context {
   int mg_sweeps = 20;           // damped Jacobi sweeps on the coarsest level
   double mg_omega = 0.0;        // Jacobi damping; 0 = from the element stiffness
   double mg_delta = 1e-2;       // reliable-update factor of the multigrid loop
+  int mg_packed = 1;            // 1: level-0 operator with two realizations per lane (packed FP32)
   // Workspace kept across calls (allocation and cudaFree synchronise the
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.

@@ -19,7 +19,7 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-DEFAULTS = {"multigrid": 1, "fixed_updates": 0, "multigrid_levels": 6, "multigrid_sweeps": 20}
+DEFAULTS = {"multigrid": 1, "fixed_updates": 0, "multigrid_levels": 6, "multigrid_sweeps": 20, "multigrid_packed": 1}
 
 
 @contextlib.contextmanager
@@ -53,12 +53,13 @@ def mixed_solve(ctx, model, kl, xi, tol):
     return mc
 
 
-@pytest.mark.parametrize("n,R,mg,levels", [(4, 5, 1, 6), (8, 40, 1, 6), (16, 64, 1, 6), (16, 64, 1, 3),
-                                           (8, 40, 0, 6)])
-def test_multigrid_matches_fp64_oracle(ctx, n, R, mg, levels):
+@pytest.mark.parametrize("n,R,mg,levels,packed", [(4, 5, 1, 6, 1), (8, 40, 1, 6, 1), (16, 64, 1, 6, 1),
+                                                  (16, 64, 1, 3, 1), (16, 70, 1, 6, 0), (8, 40, 0, 6, 1)])
+def test_multigrid_matches_fp64_oracle(ctx, n, R, mg, levels, packed):
+    """packed = 0: the level-0 operator with one realization per lane."""
     model = M.clamped_block_model(n)
     kl, xi = problem(model, (n, n, n), R, seed=n)
-    with options(ctx, multigrid=mg, multigrid_levels=levels):
+    with options(ctx, multigrid=mg, multigrid_levels=levels, multigrid_packed=packed):
         mc = mixed_solve(ctx, model, kl, xi, 1e-10)
     assert (mc.Residuals < 1e-10).all()
     E = oracle_fields(model, kl, xi, (n, n, n))
