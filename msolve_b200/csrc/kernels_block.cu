@@ -1433,17 +1433,20 @@ __global__ void __maxnreg__(152)
 // after the launch, since neighbouring tiles read it in their halos), otherwise x; then r = b - A x in FP64 with the Walsh-mode operator (mass term
 // with kMass), masked, r32 = (float) r, and the per-realization partials
 // ||r||^2, dinv r32.r32 ([tile][Rp][2], the layout of k_resid). A CTA owns a
-// 2 x 2 tile of node pencils (9 element warps + 1 TMA producer warp: FP64
-// element state needs about twice the registers of the FP32 operator);
-// staging, exchange and bounded waits as k_op_modal.
-constexpr int kRJ = 2, kRK = 2;
+// 3 x 2 tile of node pencils with its 12 element warps (FP64 element state
+// needs about twice the registers of the FP32 operator: 3 warps per SM
+// sub-partition) and no separate producer warp: lane 0 of warp 0 issues the
+// TMA loads three planes ahead into the 4-stage ring (refilling the stage of
+// the plane before the current one, a bounded wait on its "empty" barrier);
+// exchange and bounded waits as k_op_modal.
+constexpr int kRJ = 3, kRK = 2;
 constexpr int kREJ = kRJ + 1, kREK = kRK + 1, kRWarps = kREJ * kREK;
 constexpr int kRPJ = kRJ + 2, kRPK = kRK + 2;
-constexpr int kRThreads = 32 * (kRWarps + 1);
+constexpr int kRThreads = 32 * kRWarps;
 constexpr int kRPatch = 32 * 3 * kRPJ * kRPK;          // values of a vector patch (1536)
 constexpr int kREPatch = 32 * kREJ * kREK;             // E patch (288 doubles)
 constexpr uint32_t kROffX = 0, kROffD = 8 * kRPatch, kROffP = kROffD + 4 * kRPatch, kROffE = kROffP + 4 * kRPatch;
-constexpr uint32_t kRStageBytes = kROffE + 8 * kREPatch;  // 26,880 bytes
+constexpr uint32_t kRStageBytes = kROffE + 8 * kREPatch;  // 33,792 bytes
 constexpr int kRStages = 4;
 constexpr int kRXDoubles = kRWarps * 4 * 3 * 32;        // exchange buffer (doubles)
 constexpr size_t kRSmem = 128 + (size_t)kRStages * kRStageBytes + 2 * sizeof(double) * kRXDoubles +
@@ -1476,32 +1479,31 @@ __global__ void __launch_bounds__(kRThreads, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (w == kRWarps) {
-    if (lane == 0) {
-      uint32_t seq = 0;
-      for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
-        const int J0 = 1 + (tile % tiles_j) * kRJ, K0 = 1 + (tile / tiles_j) * kRK;
-        for (int P = 1; P <= NX; ++P, ++seq) {
-          const int st = seq % kRStages;
-          const uint32_t use = seq / kRStages;
-          if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
-            atomicExch(err, 1);
-            return;
-          }
-          unsigned char* dst = smem + (size_t)st * kRStageBytes;
-          mbar_expect_tx(&full[st], kBytes);
-          tma_load_5d(dst + kROffX, &tm_x, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
-          if constexpr (kUpdate) {
-            tma_load_5d(dst + kROffD, &tm_d, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
-            tma_load_5d(dst + kROffP, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
-          }
-          tma_load_4d(dst + (kUpdate ? kROffE : 8 * kRPatch), &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
-        }
-      }
+  // producer role: global step q loads (item, plane) = (blockIdx.x + (q / NX) gridDim.x, q % NX + 1)
+  const bool producer = w == 0 && lane == 0;
+  auto produce = [&](uint32_t q) {
+    const int item = blockIdx.x + (int)(q / (uint32_t)NX) * gridDim.x;
+    if (item >= n_items) return;
+    const int P = (int)(q % (uint32_t)NX) + 1;
+    const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+    const int J0 = 1 + (tile % tiles_j) * kRJ, K0 = 1 + (tile / tiles_j) * kRK;
+    const int st = q % kRStages;
+    const uint32_t use = q / kRStages;
+    if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+      atomicExch(err, 1);
+      return;
     }
-    return;
-  }
+    unsigned char* dst = smem + (size_t)st * kRStageBytes;
+    mbar_expect_tx(&full[st], kBytes);
+    tma_load_5d(dst + kROffX, &tm_x, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+    if constexpr (kUpdate) {
+      tma_load_5d(dst + kROffD, &tm_d, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+      tma_load_5d(dst + kROffP, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+    }
+    tma_load_4d(dst + (kUpdate ? kROffE : 8 * kRPatch), &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+  };
+  if (producer)
+    for (int q = 0; q < kRStages - 1; ++q) produce(q);
   const int ej = w % kREJ, ek = w / kREJ;
   const bool node_warp = ej >= 1 && ek >= 1;
   uint32_t seq = 0;
@@ -1578,6 +1580,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
     };
     for (int P = 1; P <= NX; ++P, ++seq) {
       const int st = seq % kRStages;
+      if (producer && !dead) produce(seq + kRStages - 1);
       if (!dead && !mbar_wait(&full[st], (seq / kRStages) & 1)) {
         atomicExch(err, 1);
         dead = true;
@@ -2614,7 +2617,7 @@ struct BlockSys {
   // between x and xB (the step writes x + d + alpha p into the other buffer)
   WSlot xB;
   ModalCD MCD;
-  int n_items_r = 0, grid_r = 0;
+  int tiles_jr = 0, n_tiles_r = 0, n_items_r = 0, grid_r = 0;
   CUtensorMap tm_xr, tm_xBr, tm_dr, tm_pr, tm_er;
   // multigrid preconditioner: levels 1..n_lvl-1 (level 0 is this lattice), the
   // level-0 pre-smoothed iterate xs, the damping and the coarsest-level sweeps
@@ -2870,7 +2873,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
     for (CUresult r : rs)
       if (r != CUDA_SUCCESS) e = r;
     // FP64 true-residual step: x (both buffers, FP64), d and p (FP32) patches
-    // of a 2 x 2 node tile with halo, the FP64 element patch
+    // of a 3 x 2 node tile with halo, the FP64 element patch
     {
       const cuuint64_t db = sizeof(double);
       const cuuint64_t ps64[4] = {Rp * db, 3 * Rp * db, 3 * Rp * db * L.NXp, 3 * Rp * db * L.NXp * L.NYp};
@@ -2890,7 +2893,9 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE)};
       for (CUresult r : r64)
         if (r != CUDA_SUCCESS) e = r;
-      B->n_items_r = B->n_tiles * (Rp / 32);
+      B->tiles_jr = (L.NY + kRJ - 1) / kRJ;
+      B->n_tiles_r = B->tiles_jr * ((L.NZ + kRK - 1) / kRK);
+      B->n_items_r = B->n_tiles_r * (Rp / 32);
       B->grid_r = std::min(B->n_items_r, ctx->sm_count);
     }
     static std::once_flag resid_once;
@@ -3411,9 +3416,9 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
                                 : (upd ? pick(T1{}, F0{}, T1{}) : pick(T1{}, F0{}, F0{})))
                      : (b_per_r ? (upd ? pick(F0{}, T1{}, T1{}) : pick(F0{}, T1{}, F0{}))
                                 : (upd ? pick(F0{}, F0{}, T1{}) : pick(F0{}, F0{}, F0{})));
-    k<<<B->grid_r, kRThreads, kRSmem, st>>>(L, B->MCD, B->tm_xr, B->tm_dr, B->tm_pr, B->tm_er, L.tiles_j, B->n_tiles,
-                                             B->n_items_r, mask, b, dinv, s.alpha, B->xB.as<double>(), r32, part,
-                                             s.err);
+    k<<<B->grid_r, kRThreads, kRSmem, st>>>(L, B->MCD, B->tm_xr, B->tm_dr, B->tm_pr, B->tm_er, B->tiles_jr,
+                                             B->n_tiles_r, B->n_items_r, mask, b, dinv, s.alpha, B->xB.as<double>(),
+                                             r32, part, s.err);
     if (upd) {
       MSG_CUDA(ctx, cudaMemsetAsync(B->d.ptr, 0, sizeof(float) * B->nvec, st));
       std::swap(B->x.ptr, B->xB.ptr);
@@ -3431,8 +3436,8 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
       k_resid<false, false><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
   }
   MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
-  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles, part, s, tol, first ? 1 : 0,
-                                               B->gmg ? 2 : (B->modal ? 1 : 0), max_it);
+  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->modal ? B->n_tiles_r : B->n_tiles, part, s, tol,
+                                               first ? 1 : 0, B->gmg ? 2 : (B->modal ? 1 : 0), max_it);
   count_launch(ctx, 2);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
