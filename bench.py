@@ -44,9 +44,9 @@ METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p
 # DRAM traffic of one k_op_modal launch per realization on the 32^3 lattice: ncu capture
 # at R = 512 (dram__bytes_read.sum 1,165.9 MB + dram__bytes_write.sum 845.5 MB) / 512
 OP_DRAM_BYTES_PER_REALIZATION = (1165.921e6 + 845.472e6) / 512
-# the same for the multigrid loop's direction + operator launch (k_lvl_op<PcgZ>), 32^3 lattice
-# ncu capture at R = 512: dram__bytes_read.sum 814.4 MB + dram__bytes_write.sum 621.0 MB
-MG_OP_DRAM_BYTES_PER_REALIZATION = (814.429e6 + 620.990e6) / 512
+# the same for the multigrid loop's direction + operator launch (packed k_lvl_op2<PcgZ>), 32^3
+# lattice, ncu capture at R = 512: dram__bytes_read.sum 840.9 MB + dram__bytes_write.sum 626.0 MB
+MG_OP_DRAM_BYTES_PER_REALIZATION = (840.853e6 + 626.001e6) / 512
 
 
 def parse():
@@ -452,7 +452,8 @@ def main():
     # multigrid: read z, p_{k-1}, d (3 per node), E (1 per element); write p_k, d, q (3 per node).
     # Jacobi: read r, p_{k-1}, d (3 per node), dinv (1 per node), E; write p_k, d, q (3 per node)
     if mg:
-        op_kernel = "k_lvl_op<PcgZ> (multigrid loop: fused search direction p = z + beta p + matrix-free FP32 operator)"
+        op_kernel = ("k_lvl_op2<PcgZ> (multigrid loop, level 0: fused search direction p = z + beta p + "
+                     "matrix-free FP32 operator, two realizations per lane in packed FP32)")
         op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 3 + 3 + 3) * nn + ne)
         per_r = MG_OP_DRAM_BYTES_PER_REALIZATION
     else:
