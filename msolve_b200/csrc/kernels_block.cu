@@ -1169,20 +1169,28 @@ constexpr int kQD = kQR * 3 * kQJ * kQK;            // d of the tile's own nodes
 constexpr int kQX = kQWarps * 4 * 3 * kQR;          // exchange buffer
 template <int kMode> struct LvlStage2 {
   static constexpr bool kTwo = kMode == kLvlStart || kMode == kLvlPcgZ;
+  // Smooth also stages b and dinv of the tile's own nodes, read by the node
+  // phase one plane later: its stages are released after that node phase, so
+  // the ring has 4 stages (loads still go two planes ahead)
+  static constexpr bool kOwn = kMode == kLvlSmooth;
+  static constexpr int kStages = kOwn ? 4 : kMStages;
   static constexpr int kOffA = 0;
   static constexpr int kOffB = kQPlane;
   static constexpr int kOffN = (kTwo ? 2 : 1) * kQPlane;
   static constexpr int kOffE = kOffN + (kMode == kLvlStart ? kQNode : 0);
-  static constexpr int kOffD = kOffE + kQE;
-  static constexpr int kFloats = kOffD + (kMode == kLvlPcgZ ? kQD : 0);
+  static constexpr int kOffD = kOffE + kQE;  // d (direction) or own b (smooth)
+  static constexpr int kOffO = kOffD + (kOwn ? kQD : 0);  // own dinv (smooth)
+  static constexpr int kFloats = kOffO + (kMode == kLvlPcgZ ? kQD : 0) + (kOwn ? kQR * kQJ * kQK : 0);
   static constexpr uint32_t kBytes = kFloats * 4;
-  static constexpr size_t kSmem = 128 + sizeof(float) * ((size_t)kMStages * kFloats + 2 * (size_t)kQX) +
-                                  sizeof(double) * kQJ * kQK * kQR + sizeof(uint64_t) * (2 * kMStages);
+  static constexpr size_t kSmem = 128 + sizeof(float) * ((size_t)kStages * kFloats + 2 * (size_t)kQX) +
+                                  sizeof(double) * kQJ * kQK * kQR + sizeof(uint64_t) * (2 * kStages);
 };
 static_assert(LvlStage2<kLvlStart>::kBytes % 128 == 0 && LvlStage2<kLvlSmooth>::kBytes % 128 == 0 &&
                   LvlStage2<kLvlPcgZ>::kBytes % 128 == 0,
               "stage alignment");
-static_assert(LvlStage2<kLvlPcgZ>::kSmem <= 227 * 1024 && LvlStage2<kLvlStart>::kSmem <= 227 * 1024, "smem");
+static_assert(LvlStage2<kLvlPcgZ>::kSmem <= 227 * 1024 && LvlStage2<kLvlStart>::kSmem <= 227 * 1024 &&
+                  LvlStage2<kLvlSmooth>::kSmem <= 227 * 1024 && (kQR * kQJ * kQK * 4) % 128 == 0,
+              "smem");
 
 template <int kMode, bool kMass>
 __global__ void __maxnreg__(152)
@@ -1197,14 +1205,15 @@ __global__ void __maxnreg__(152)
   using S = LvlStage2<kMode>;
   extern __shared__ __align__(128) float smem_dyn[];
   float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
-  float* xbuf = smem + kMStages * S::kFloats;
+  constexpr int kSt = S::kStages;
+  float* xbuf = smem + kSt * S::kFloats;
   double* red = reinterpret_cast<double*>(xbuf + 2 * kQX);  // [node pencils][64]
   uint64_t* full = reinterpret_cast<uint64_t*>(red + kQJ * kQK * kQR);
-  uint64_t* empty = full + kMStages;
+  uint64_t* empty = full + kSt;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int NX = L.NX, Rp = L.Rp, Rp2 = L.Rp >> 1;
   if (threadIdx.x == 0) {
-    for (int st = 0; st < kMStages; ++st) {
+    for (int st = 0; st < kSt; ++st) {
       mbar_init(&full[st], 1);
       mbar_init(&empty[st], kQWarps);
     }
@@ -1220,8 +1229,8 @@ __global__ void __maxnreg__(152)
     const int P = (int)(q % (uint32_t)NX) + 1;
     const int tile = item % n_tiles, g64 = (item / n_tiles) * kQR;
     const int J0 = 1 + (tile % tiles_j) * kQJ, K0 = 1 + (tile / tiles_j) * kQK;
-    const int st = q % kMStages;
-    const uint32_t use = q / kMStages;
+    const int st = q % kSt;
+    const uint32_t use = q / kSt;
     if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
       atomicExch(err, 1);
       return;
@@ -1233,6 +1242,10 @@ __global__ void __maxnreg__(152)
     if constexpr (kMode == kLvlStart) tma_load_4d(dst + S::kOffN, &tm_n, g64, P, J0 - 1, K0 - 1, &full[st]);
     tma_load_4d(dst + S::kOffE, &tm_e, g64, P - 1, J0 - 1, K0 - 1, &full[st]);
     if constexpr (kMode == kLvlPcgZ) tma_load_5d(dst + S::kOffD, &tm_d, g64, 0, P, J0, K0, &full[st]);
+    if constexpr (S::kOwn) {
+      tma_load_5d(dst + S::kOffD, &tm_b, g64, 0, P, J0, K0, &full[st]);
+      tma_load_4d(dst + S::kOffO, &tm_n, g64, P, J0, K0, &full[st]);
+    }
   };
   if (producer) {
     produce(0);
@@ -1272,7 +1285,9 @@ __global__ void __maxnreg__(152)
       for (int qq = 0; qq < 4; ++qq) T0[c][qq] = z2;
     double acc0 = 0.0, acc1 = 0.0;
     uint32_t mreg = 0;
-    auto node_phase = [&](int X) {
+    auto node_phase = [&](int X, uint32_t seq_x) {
+      [[maybe_unused]] const float* px = smem + (seq_x % kSt) * S::kFloats;
+      [[maybe_unused]] const int od = (ek - 1) * kQJ + (ej - 1);
       if (((X - 1) & 31) == 0) {
         const int pl = X + lane;
         mreg = (pl <= NX) ? mask[nrow + pl] : 0u;
@@ -1281,7 +1296,7 @@ __global__ void __maxnreg__(152)
       const float2* xb = xb2 + xsel * (kQX / 2);
       const size_t node = nrow + X;
       float2 wdv = z2;
-      if constexpr (kMode == kLvlSmooth) wdv = om2 * reinterpret_cast<const float2*>(dinv)[node * Rp2 + rr2];
+      if constexpr (kMode == kLvlSmooth) wdv = om2 * reinterpret_cast<const float2*>(px + S::kOffO)[od * 32 + lane];
       double s0 = 0.0, s1 = 0.0;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -1300,7 +1315,7 @@ __global__ void __maxnreg__(152)
         } else if constexpr (kMode == kLvlResid) {
           v = fixed ? z2 : reinterpret_cast<const float2*>(b)[o] - y;
         } else if constexpr (kMode == kLvlSmooth) {
-          const float2 bv = reinterpret_cast<const float2*>(b)[o];
+          const float2 bv = reinterpret_cast<const float2*>(px + S::kOffD)[(od * 3 + c) * 32 + lane];
           v = fixed ? z2 : fmx(wdv, bv - y, ou[c]);
           s0 = fma((double)v.x, (double)bv.x, s0);
           s1 = fma((double)v.y, (double)bv.y, s1);
@@ -1326,9 +1341,9 @@ __global__ void __maxnreg__(152)
           for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
     };
     for (int P = 1; P <= NX; ++P, ++seq) {
-      const int st = seq % kMStages;
+      const int st = seq % kSt;
       if (producer && !dead) produce(seq + 2);
-      if (!dead && !mbar_wait(&full[st], (seq / kMStages) & 1)) {
+      if (!dead && !mbar_wait(&full[st], (seq / kSt) & 1)) {
         atomicExch(err, 1);
         dead = true;
       }
@@ -1379,7 +1394,7 @@ __global__ void __maxnreg__(152)
         }
       }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[st]);
+      if (!S::kOwn && lane == 0) mbar_arrive(&empty[st]);
       float2 Bc[3][4];
       yz_forward(u, Bc);
       if (P >= 2) {
@@ -1393,8 +1408,12 @@ __global__ void __maxnreg__(152)
             for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
         }
         csync();
-        if (node_ok) node_phase(P - 1);
+        if (node_ok) node_phase(P - 1, seq - 1);
         xsel ^= 1;
+        if constexpr (S::kOwn) {  // the node phase of plane P - 1 is done with its stage
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&empty[(seq - 1) % kSt]);
+        }
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -1406,8 +1425,12 @@ __global__ void __maxnreg__(152)
     }
     if (real) emit_corners(T0);
     csync();
-    if (node_ok) node_phase(NX);
+    if (node_ok) node_phase(NX, seq - 1);
     xsel ^= 1;
+    if constexpr (S::kOwn) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[(seq - 1) % kSt]);
+    }
     if (kMode != kLvlResid && partial != nullptr) {
       if (node_warp) {
         const int nw = (ek - 1) * kQJ + (ej - 1);
@@ -1705,7 +1728,7 @@ __global__ void __launch_bounds__(256) k_restrict(Lattice Lf, Lattice Lc, const 
 // fine node with even coordinate takes the coincident coarse node, an odd one
 // the mean of its two neighbours), masked at the fine level. One thread per
 // fine interior node and four realizations; the 8 corner terms are summed in a
-// fixed order (an even axis repeats its coarse node with weight 0).
+// fixed order (the terms of an even axis's second neighbour, weight 0, are skipped).
 __global__ void __launch_bounds__(256) k_prolong_add(Lattice Lf, Lattice Lc, const int* __restrict__ interior_f,
                                                      const uint8_t* __restrict__ mask_f,
                                                      const float* __restrict__ xc, float* __restrict__ xf) {
@@ -1736,6 +1759,8 @@ __global__ void __launch_bounds__(256) k_prolong_add(Lattice Lf, Lattice Lc, con
       for (int bb = 0; bb < 2; ++bb)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
+          // an even coordinate has one coarse neighbour on that axis: skip the zero-weight loads
+          if ((e && !(gi & 1)) || (bb && !(gj & 1)) || (a && !(gk & 1))) continue;
           const float wgt = wk[a] * wj[bb] * wi[e];
           const float4 v = c4[((c0 + (e ? oi : 0) + (bb ? oj : 0) + (a ? ok : 0)) * 3 + c) * Q + q];
           s.x = fmaf(wgt, v.x, s.x);
@@ -2632,6 +2657,7 @@ struct BlockSys {
   ModalCT<float2> MC2;
   int tiles_j2 = 0, n_tiles2 = 0, n_items2 = 0, grid2 = 0;
   CUtensorMap tm2_rA, tm2_rB, tm2_qA, tm2_qB, tm2_pA, tm2_pB, tm2_xs, tm2_dinv, tm2_e, tm2_d;
+  CUtensorMap tm2_rAo, tm2_rBo, tm2_dinvo;  // own-tile boxes of r (both buffers) and dinv (post-sweep)
 };
 
 // Largest eigenvalue of diag(K)^-1 K for one element (power iteration on the
@@ -3036,6 +3062,10 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
         const cuuint32_t nb2[4] = {kQR, 1, kQPJ, kQPK};
         const cuuint32_t eb2[4] = {kQR, 1, kQEJ, kQEK};
         const cuuint32_t db2[5] = {kQR, 3, 1, kQJ, kQK};
+        const cuuint32_t ob2[4] = {kQR, 1, kQJ, kQK};
+        if (enc5(&B->tm2_rAo, B->r32.ptr, db2) != CUDA_SUCCESS || enc5(&B->tm2_rBo, B->rB.ptr, db2) != CUDA_SUCCESS ||
+            enc4(&B->tm2_dinvo, B->dinv.ptr, ob2) != CUDA_SUCCESS)
+          return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (packed)");
         const CUresult r2[10] = {enc5(&B->tm2_rA, B->r32.ptr, pb2), enc5(&B->tm2_rB, B->rB.ptr, pb2),
                                  enc5(&B->tm2_qA, B->q.ptr, pb2),   enc5(&B->tm2_qB, B->qB.ptr, pb2),
                                  enc5(&B->tm2_pA, B->p.ptr, pb2),   enc5(&B->tm2_pB, B->pB.ptr, pb2),
@@ -3191,9 +3221,12 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
     constexpr int kMode = decltype(mode)::value;
     if (B->pack) {
       auto k = mass ? k_lvl_op2<kMode, true> : k_lvl_op2<kMode, false>;
+      // post-sweep: b (= r') and dinv of the own nodes come through the stage
+      const CUtensorMap& tn2 = kMode == kLvlSmooth ? B->tm2_dinvo : B->tm2_dinv;
+      const CUtensorMap& tbb = kMode == kLvlSmooth ? (even ? B->tm2_rBo : B->tm2_rAo) : tb2;
       k<<<B->grid2, kQThreads, LvlStage2<kMode>::kSmem, st>>>(
-          B->L, B->MC2, ta2, tb2, B->tm2_dinv, B->tm2_e, B->tm2_d, B->tiles_j2, B->n_tiles2, B->n_items2, B->mask, b,
-          dinv, om, s.alpha, s.beta, out, out2, out3, d, partial, pstride, s.err);
+          B->L, B->MC2, ta2, tbb, tn2, B->tm2_e, B->tm2_d, B->tiles_j2, B->n_tiles2, B->n_items2, B->mask, b, dinv,
+          om, s.alpha, s.beta, out, out2, out3, d, partial, pstride, s.err);
     } else {
       lvl(mode, B->L, B->MC, ta, tb, B->tm_dinvm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m, B->n_items_m,
           B->grid_m, B->mask, b, dinv, out, out2, out3, d, partial, pstride);
@@ -3305,8 +3338,9 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
       mix(&B->tm_xs, sizeof(CUtensorMap));
       for (int l = 1; l < B->n_lvl; ++l) mix(&B->lv[l], sizeof(GmgLevel));
       if (B->pack) {
-        const CUtensorMap* t2[10] = {&B->tm2_rA, &B->tm2_rB, &B->tm2_qA, &B->tm2_qB, &B->tm2_pA,
-                                     &B->tm2_pB, &B->tm2_xs, &B->tm2_dinv, &B->tm2_e, &B->tm2_d};
+        const CUtensorMap* t2[13] = {&B->tm2_rA, &B->tm2_rB, &B->tm2_qA, &B->tm2_qB, &B->tm2_pA,
+                                     &B->tm2_pB, &B->tm2_xs, &B->tm2_dinv, &B->tm2_e, &B->tm2_d,
+                                     &B->tm2_rAo, &B->tm2_rBo, &B->tm2_dinvo};
         for (const CUtensorMap* t : t2) mix(t, sizeof(CUtensorMap));
         mix(&B->MC2, sizeof(B->MC2));
       }
