@@ -1682,26 +1682,30 @@ __global__ void __launch_bounds__(kRThreads, 1)
 // Full-weighting restriction b_c = P^T t_f (P: trilinear prolongation), masked
 // at the coarse level, and x_c = omega dinv_c b_c (the first Jacobi sweep from
 // zero). Coarse node (I, J, K) (padded) sits on fine node (2I-1, 2J-1, 2K-1);
-// the fine ghost layer is zero. One thread per coarse interior node and four
-// realizations (float4).
-__global__ void __launch_bounds__(256) k_restrict(Lattice Lf, Lattice Lc, const int* __restrict__ interior_c,
-                                                  const uint8_t* __restrict__ mask_c, const float* __restrict__ tf,
-                                                  const float* __restrict__ dinv_c, float omega,
-                                                  float* __restrict__ bc, float* __restrict__ xc) {
+// the fine ghost layer is zero. Grid: x = coarse interior node, y = chunks of
+// 128 float4 realization groups; one thread per node and four realizations.
+// Offsets are 32-bit and relative to the centre node (the 27 loads of a
+// component share one base address).
+constexpr int kXferThreads = 128;
+__global__ void __launch_bounds__(kXferThreads, 8) k_restrict(Lattice Lf, Lattice Lc, const int* __restrict__ interior_c,
+                                                              const uint8_t* __restrict__ mask_c,
+                                                              const float* __restrict__ tf,
+                                                              const float* __restrict__ dinv_c, float omega,
+                                                              float* __restrict__ bc, float* __restrict__ xc) {
   const int Q = Lf.Rp >> 2;
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)Lc.n_int * Q) return;
-  const int t = (int)(idx / Q), q = (int)(idx % Q);
-  const size_t nc = (size_t)interior_c[t];
-  const int I = (int)(nc % Lc.NXp), J = (int)((nc / Lc.NXp) % Lc.NYp), K = (int)(nc / ((size_t)Lc.NXp * Lc.NYp));
-  const size_t sy = (size_t)Lf.NXp, sz = (size_t)Lf.NXp * Lf.NYp;
-  const size_t fc = (size_t)(2 * I - 1) + sy * (2 * J - 1) + sz * (2 * K - 1);
+  const int q = blockIdx.y * kXferThreads + threadIdx.x;
+  if (q >= Q) return;
+  const int nc = interior_c[blockIdx.x];
+  const int I = nc % Lc.NXp, J = (nc / Lc.NXp) % Lc.NYp, K = nc / (Lc.NXp * Lc.NYp);
+  const int fc = (2 * I - 1) + Lf.NXp * ((2 * J - 1) + Lf.NYp * (2 * K - 1));
+  const int sx = 3 * Q, sy = Lf.NXp * sx, sz = Lf.NYp * sy;  // float4 strides between fine nodes
+  const float4* t4 = reinterpret_cast<const float4*>(tf) + (size_t)fc * sx + q;
   const uint32_t mk = mask_c[nc];
-  const float4* t4 = reinterpret_cast<const float4*>(tf);
-  const float4 dv = reinterpret_cast<const float4*>(dinv_c)[nc * Q + q];
-  float4* b4 = reinterpret_cast<float4*>(bc);
-  float4* x4 = reinterpret_cast<float4*>(xc);
-#pragma unroll
+  const size_t oc = (size_t)nc * sx + q;
+  const float4* dv4 = reinterpret_cast<const float4*>(dinv_c) + (size_t)nc * Q + q;
+  float4* b4 = reinterpret_cast<float4*>(bc) + oc;
+  float4* x4 = reinterpret_cast<float4*>(xc) + oc;
+#pragma unroll 1
   for (int c = 0; c < 3; ++c) {
     float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
@@ -1711,48 +1715,47 @@ __global__ void __launch_bounds__(256) k_restrict(Lattice Lf, Lattice Lc, const 
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
           const float wgt = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
-          const float4 v = t4[((fc + dx + dy * sy + dz * sz) * 3 + c) * Q + q];
+          const float4 v = t4[dx * sx + dy * sy + dz * sz + c * Q];
           s.x = fmaf(wgt, v.x, s.x);
           s.y = fmaf(wgt, v.y, s.y);
           s.z = fmaf(wgt, v.z, s.z);
           s.w = fmaf(wgt, v.w, s.w);
         }
     if ((mk >> c) & 1) s = make_float4(0.f, 0.f, 0.f, 0.f);
-    b4[(nc * 3 + c) * Q + q] = s;
-    x4[(nc * 3 + c) * Q + q] =
-        make_float4(omega * dv.x * s.x, omega * dv.y * s.y, omega * dv.z * s.z, omega * dv.w * s.w);
+    b4[c * Q] = s;
+    const float4 dv = *dv4;  // loaded after the sums: no register held across the 27 loads
+    x4[c * Q] = make_float4(omega * dv.x * s.x, omega * dv.y * s.y, omega * dv.z * s.z, omega * dv.w * s.w);
   }
 }
 
 // x_f += P x_c: trilinear prolongation of the coarse correction (per axis, a
 // fine node with even coordinate takes the coincident coarse node, an odd one
-// the mean of its two neighbours), masked at the fine level. One thread per
-// fine interior node and four realizations; the 8 corner terms are summed in a
+// the mean of its two neighbours), masked at the fine level. Grid as
+// k_restrict over the fine interior nodes; the 8 corner terms are summed in a
 // fixed order (the terms of an even axis's second neighbour, weight 0, are skipped).
-__global__ void __launch_bounds__(256) k_prolong_add(Lattice Lf, Lattice Lc, const int* __restrict__ interior_f,
-                                                     const uint8_t* __restrict__ mask_f,
-                                                     const float* __restrict__ xc, float* __restrict__ xf) {
+__global__ void __launch_bounds__(kXferThreads, 8) k_prolong_add(Lattice Lf, Lattice Lc,
+                                                                 const int* __restrict__ interior_f,
+                                                                 const uint8_t* __restrict__ mask_f,
+                                                                 const float* __restrict__ xc, float* __restrict__ xf) {
   const int Q = Lf.Rp >> 2;
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)Lf.n_int * Q) return;
-  const int t = (int)(idx / Q), q = (int)(idx % Q);
-  const size_t nf = (size_t)interior_f[t];
+  const int q = blockIdx.y * kXferThreads + threadIdx.x;
+  if (q >= Q) return;
+  const int nf = interior_f[blockIdx.x];
   const uint32_t mk = mask_f[nf];
   if (mk == 7u) return;
-  const int gi = (int)(nf % Lf.NXp) - 1, gj = (int)((nf / Lf.NXp) % Lf.NYp) - 1;
-  const int gk = (int)(nf / ((size_t)Lf.NXp * Lf.NYp)) - 1;
-  const size_t sy = (size_t)Lc.NXp, sz = (size_t)Lc.NXp * Lc.NYp;
-  const size_t c0 = (size_t)((gi >> 1) + 1) + sy * ((gj >> 1) + 1) + sz * ((gk >> 1) + 1);
-  const size_t oi = gi & 1, oj = (gj & 1) * sy, ok = (gk & 1) * sz;  // offset of the second neighbour (or 0)
+  const int gi = nf % Lf.NXp - 1, gj = (nf / Lf.NXp) % Lf.NYp - 1, gk = nf / (Lf.NXp * Lf.NYp) - 1;
+  const int sx = 3 * Q, sy = Lc.NXp * sx, sz = Lc.NYp * sy;  // float4 strides between coarse nodes
+  const int c0 = ((gi >> 1) + 1) + Lc.NXp * (((gj >> 1) + 1) + Lc.NYp * ((gk >> 1) + 1));
+  const int oi = (gi & 1) * sx, oj = (gj & 1) * sy, ok = (gk & 1) * sz;  // offset of the second neighbour (or 0)
   const float wi[2] = {(gi & 1) ? 0.5f : 1.f, (gi & 1) ? 0.5f : 0.f};
   const float wj[2] = {(gj & 1) ? 0.5f : 1.f, (gj & 1) ? 0.5f : 0.f};
   const float wk[2] = {(gk & 1) ? 0.5f : 1.f, (gk & 1) ? 0.5f : 0.f};
-  const float4* c4 = reinterpret_cast<const float4*>(xc);
-  float4* f4 = reinterpret_cast<float4*>(xf);
+  const float4* c4 = reinterpret_cast<const float4*>(xc) + (size_t)c0 * sx + q;
+  float4* f4 = reinterpret_cast<float4*>(xf) + (size_t)nf * sx + q;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     if ((mk >> c) & 1) continue;
-    float4 s = f4[(nf * 3 + c) * Q + q];
+    float4 s = f4[c * Q];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -1762,15 +1765,21 @@ __global__ void __launch_bounds__(256) k_prolong_add(Lattice Lf, Lattice Lc, con
           // an even coordinate has one coarse neighbour on that axis: skip the zero-weight loads
           if ((e && !(gi & 1)) || (bb && !(gj & 1)) || (a && !(gk & 1))) continue;
           const float wgt = wk[a] * wj[bb] * wi[e];
-          const float4 v = c4[((c0 + (e ? oi : 0) + (bb ? oj : 0) + (a ? ok : 0)) * 3 + c) * Q + q];
+          const float4 v = c4[(e ? oi : 0) + (bb ? oj : 0) + (a ? ok : 0) + c * Q];
           s.x = fmaf(wgt, v.x, s.x);
           s.y = fmaf(wgt, v.y, s.y);
           s.z = fmaf(wgt, v.z, s.z);
           s.w = fmaf(wgt, v.w, s.w);
         }
-    f4[(nf * 3 + c) * Q + q] = s;
+    f4[c * Q] = s;
   }
 }
+
+// grid of the transfer kernels: x = interior node, y = chunks of kXferThreads float4 groups
+inline dim3 xfer_grid(int n_int, int Rp) {
+  return dim3((unsigned)n_int, (unsigned)((Rp / 4 + kXferThreads - 1) / kXferThreads));
+}
+inline int xfer_block(int Rp) { return std::min(kXferThreads, (Rp / 4 + 31) / 32 * 32); }
 
 // Coarse element field: the mean of the 8 fine elements it covers (elements
 // are stored at their lower-corner padded node). One CTA per coarse element.
@@ -3245,8 +3254,8 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
     GmgLevel& g = B->lv[l];
     const Lattice& Lf = l == 1 ? B->L : B->lv[l - 1].L;
     const float* tf = l == 1 ? qB : B->lv[l - 1].t;
-    k_restrict<<<(unsigned)(((long)g.L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(Lf, g.L, g.interior, g.mask,
-                                                                                      tf, g.dinv, om, g.b, g.x);
+    k_restrict<<<xfer_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(Lf, g.L, g.interior, g.mask, tf, g.dinv, om, g.b,
+                                                                     g.x);
     if (l < nl - 1)
       lvl(Resid{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
           g.mask, g.b, nullptr, g.t, nullptr, nullptr, nullptr, nullptr, 1);
@@ -3266,14 +3275,14 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   // up: prolongate into the level's iterate, one sweep (result in t)
   for (int l = nl - 2; l >= 1; --l) {
     GmgLevel& g = B->lv[l];
-    k_prolong_add<<<(unsigned)(((long)g.L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(
-        g.L, B->lv[l + 1].L, g.interior, g.mask, res_c, g.x);
+    k_prolong_add<<<xfer_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(g.L, B->lv[l + 1].L, g.interior, g.mask, res_c,
+                                                                        g.x);
     lvl(Smooth{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
         g.mask, g.b, g.dinv, g.t, nullptr, nullptr, nullptr, nullptr, 1);
     res_c = g.t;
   }
-  k_prolong_add<<<(unsigned)(((long)B->L.n_int * (Rp / 4) + 255) / 256), 256, 0, st>>>(
-      B->L, B->lv[1].L, B->interior, B->mask, res_c, B->xs.as<float>());
+  k_prolong_add<<<xfer_grid(B->L.n_int, Rp), xfer_block(Rp), 0, st>>>(B->L, B->lv[1].L, B->interior, B->mask, res_c,
+                                                                        B->xs.as<float>());
   // level 0 post-sweep: z (into qB) and the partial z.r'
   lvl0(Smooth{}, B->tm_xs, B->tm_xs, B->tm2_xs, B->tm2_xs, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr,
        part2 + 1, 2);
