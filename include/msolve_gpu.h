@@ -368,7 +368,10 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * element stiffness, default), "multigrid_delta" (reliable-update factor of the
  * V-cycle loop, default 0.01; its inner chunk is 2 iterations), "multigrid_packed"
  * (1, default: the three level-0 operator passes of an iteration work on two
- * realizations per thread with packed FP32 arithmetic; 0: one per thread).
+ * realizations per thread with packed FP32 arithmetic; 0: one per thread),
+ * "multigrid_fused_coarse" (1, default: every sweep of the coarsest level in
+ * one launch when that level has at most 3 x 3 nodes across y and z; 0: one
+ * launch per sweep; the results are identical).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

@@ -1145,6 +1145,149 @@ __global__ void __launch_bounds__(kMThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------- coarsest-level sweeps
+// All damped Jacobi sweeps of the coarsest level in one launch. That level has
+// at most 3 x 3 node pencils in (y, z), one k_lvl_op tile, so a CTA holds the
+// whole level for its 32 realizations in shared memory (the iterate in two
+// buffers, b, omega dinv, E and the mask, real nodes only) and consecutive
+// sweeps are separated by CTA barriers instead of launches. Every sweep is the
+// arithmetic of k_lvl_op<kLvlSmooth> in the same order (element warps over the
+// x-planes, the same exchange and the same node sums), so the iterates are
+// identical to the launch-per-sweep loop.
+inline size_t coarse_sweep_smem(const Lattice& L) {
+  const size_t nn = (size_t)L.NX * L.NY * L.NZ, ne = (size_t)(L.NX - 1) * (L.NY - 1) * (L.NZ - 1);
+  return sizeof(float) * (nn * 32 * 10 + ne * 32 + 2 * (size_t)kMXFloats) + nn;
+}
+template <bool kMass>
+__global__ void __launch_bounds__(kMWarps * 32, 1)
+    k_coarse_sweeps(Lattice L, const __grid_constant__ ModalC C, const uint8_t* __restrict__ mask,
+                    const float* __restrict__ b, const float* __restrict__ dinv, const float* __restrict__ E,
+                    float omega, int n_sweeps, const float* __restrict__ x, float* __restrict__ out) {
+  extern __shared__ __align__(16) float smem_cs[];
+  const int NX = L.NX, NY = L.NY, NZ = L.NZ, Rp = L.Rp;
+  const int nn = NX * NY * NZ, ne = (NX - 1) * (NY - 1) * (NZ - 1);
+  float* src = smem_cs;           // iterate [node][c][32]
+  float* dst = src + nn * 96;
+  float* bs = dst + nn * 96;      // b [node][c][32]
+  float* ws = bs + nn * 96;       // omega dinv [node][32]
+  float* es = ws + nn * 32;       // E [element][32]
+  float* xbuf = es + ne * 32;     // two exchange buffers
+  uint8_t* mks = reinterpret_cast<uint8_t*>(xbuf + 2 * kMXFloats);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rr = blockIdx.x * 32 + lane;
+  auto cn = [&](int X, int J, int K) { return (X - 1) + NX * ((J - 1) + NY * (K - 1)); };
+  auto ce = [&](int X, int J, int K) { return (X - 1) + (NX - 1) * ((J - 1) + (NY - 1) * (K - 1)); };
+  auto pn = [&](int X, int J, int K) { return (size_t)X + (size_t)L.NXp * ((size_t)J + (size_t)L.NYp * K); };
+  for (int i = w; i < nn; i += kMWarps) {
+    const int X = i % NX + 1, J = (i / NX) % NY + 1, K = i / (NX * NY) + 1;
+    const size_t pi = pn(X, J, K);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      src[(i * 3 + c) * 32 + lane] = x[(pi * 3 + c) * Rp + rr];
+      bs[(i * 3 + c) * 32 + lane] = b[(pi * 3 + c) * Rp + rr];
+    }
+    ws[i * 32 + lane] = omega * dinv[pi * Rp + rr];
+    if (lane == 0) mks[i] = mask[pi];
+  }
+  for (int i = w; i < ne; i += kMWarps) {
+    const int X = i % (NX - 1) + 1, J = (i / (NX - 1)) % (NY - 1) + 1, K = i / ((NX - 1) * (NY - 1)) + 1;
+    es[i * 32 + lane] = E[pn(X, J, K) * Rp + rr];
+  }
+  __syncthreads();
+  // the tile starts at node pencil (1, 1): element pencil (Je, Ke) = (ej, ek)
+  const int Je = w % kMEJ, Ke = w / kMEJ;
+  auto realj = [&](int j) { return j >= 1 && j <= NY - 1; };
+  auto realk = [&](int k) { return k >= 1 && k <= NZ - 1; };
+  const bool real = realj(Je) && realk(Ke);
+  const bool node_ok = Je >= 1 && Ke >= 1 && Je <= NY && Ke <= NZ;
+  const bool r00 = real, r10 = realj(Je - 1) && realk(Ke);
+  const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
+  int xsel = 0;
+  for (int sw = 0; sw < n_sweeps; ++sw) {
+    float Bp[3][4], T0[3][4], ou[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int qq = 0; qq < 4; ++qq) T0[c][qq] = 0.f;
+    auto node_phase = [&](int X) {
+      const int i = cn(X, Je, Ke);
+      const uint32_t mk = mks[i];
+      const float* xb = xbuf + xsel * kMXFloats;
+      const float wdv = ws[i * 32 + lane];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float y = 0.f;
+        if (r00) y += xb[((w * 4 + 0) * 3 + c) * 32 + lane];
+        if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
+        if (r01) y += xb[(((w - kMEJ) * 4 + 2) * 3 + c) * 32 + lane];
+        if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        const float bv = bs[(i * 3 + c) * 32 + lane];
+        dst[(i * 3 + c) * 32 + lane] = ((mk >> c) & 1) ? 0.f : fmaf(wdv, bv - y, ou[c]);
+      }
+    };
+    auto emit_corners = [&](const float (&B)[3][4]) {
+      float y[2][2][3];
+      yz_inverse(B, y);
+      float* xb = xbuf + xsel * kMXFloats;
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
+    };
+    for (int P = 1; P <= NX; ++P) {
+      float u[2][2][3];
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az) {
+          const int J = Je + ay, K = Ke + az;
+          const bool in = J >= 1 && J <= NY && K >= 1 && K <= NZ;  // ghost nodes are zero
+          const int i = in ? cn(P, J, K) : 0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) u[ay][az][c] = in ? src[(i * 3 + c) * 32 + lane] : 0.f;
+        }
+      float Bc[3][4];
+      yz_forward(u, Bc);
+      if (P >= 2) {
+        if (real) {
+          float C1[3][4];
+          modal_apply<kMass>(C, es[ce(P - 1, Je, Ke) * 32 + lane], Bp, Bc, T0, C1);
+          emit_corners(T0);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) T0[c][qq] = C1[c][qq];
+        }
+        __syncthreads();
+        if (node_ok) node_phase(P - 1);
+        xsel ^= 1;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ou[c] = u[0][0][c];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) Bp[c][qq] = Bc[c][qq];
+      }
+    }
+    if (real) emit_corners(T0);
+    __syncthreads();
+    if (node_ok) node_phase(NX);
+    xsel ^= 1;
+    __syncthreads();  // the sweep's iterate is complete before the next one reads it
+    float* tmp = src;
+    src = dst;
+    dst = tmp;
+  }
+  for (int i = w; i < nn; i += kMWarps) {
+    const int X = i % NX + 1, J = (i / NX) % NY + 1, K = i / (NX * NY) + 1;
+    const size_t pi = pn(X, J, K);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[(pi * 3 + c) * Rp + rr] = src[(i * 3 + c) * 32 + lane];
+  }
+}
+
 // ---------------------------------------------------------------- packed level operator (level 0)
 // k_lvl_op with two realizations per lane in float2 registers: the element and
 // node arithmetic issues Blackwell's packed FP32 instructions (one issue slot
@@ -2616,6 +2759,7 @@ struct GmgLevel {
   float *b = nullptr, *x = nullptr, *t = nullptr, *E32 = nullptr, *dinv = nullptr;
   int tiles_j = 0, n_tiles = 0, n_items = 0, grid = 0;
   CUtensorMap tm_x, tm_t, tm_e;
+  size_t sweep_smem = 0;  // coarsest level: all sweeps in one k_coarse_sweeps launch (0: launch per sweep)
 };
 
 struct BlockSys {
@@ -3050,6 +3194,23 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
         if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS || r3 != CUDA_SUCCESS)
           return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (multigrid level %d)", l);
       }
+      {  // coarsest level: one launch for all its sweeps when it fits a CTA
+        GmgLevel& g = B->lv[n_lvl - 1];
+        const size_t sm = coarse_sweep_smem(g.L);
+        g.sweep_smem = (ctx->mg_fused_coarse && g.L.NY <= kMJ && g.L.NZ <= kMK && sm <= 200 * 1024) ? sm : 0;
+        if (g.sweep_smem) {
+          static std::once_flag cs_once;
+          static cudaError_t cs_err = cudaSuccess;
+          std::call_once(cs_once, [] {
+            cs_err = cudaFuncSetAttribute(k_coarse_sweeps<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          200 * 1024);
+            if (cs_err == cudaSuccess)
+              cs_err = cudaFuncSetAttribute(k_coarse_sweeps<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            200 * 1024);
+          });
+          MSG_CUDA(ctx, cs_err);
+        }
+      }
       // packed level-0 operator: realizations in multiples of 64
       B->pack = ctx->mg_packed && (Rp % kQR) == 0;
       if (B->pack) {
@@ -3262,7 +3423,16 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   }
   // coarsest level: the restriction made the first sweep; sweeps - 1 more, x and t alternating
   const float* res_c;
-  {
+  if (B->lv[nl - 1].sweep_smem) {
+    GmgLevel& g = B->lv[nl - 1];
+    res_c = g.x;
+    if (B->sweeps > 1) {
+      auto k = mass ? k_coarse_sweeps<true> : k_coarse_sweeps<false>;
+      k<<<Rp / 32, kMWarps * 32, g.sweep_smem, st>>>(g.L, g.MC, g.mask, g.b, g.dinv, g.E32, om, B->sweeps - 1, g.x,
+                                                      g.t);
+      res_c = g.t;
+    }
+  } else {
     GmgLevel& g = B->lv[nl - 1];
     bool in_x = true;
     for (int k = 1; k < B->sweeps; ++k) {
@@ -3300,7 +3470,8 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
 // Kernels of one multigrid iteration (for the launch count).
 int gmg_launches(const BlockSys* B) {
   const int nl = B->n_lvl;
-  return 1 + (nl - 1) + (nl - 2) + (B->sweeps - 1) + (nl - 1) + (nl - 2) + 1 + 1 + 1 + 1;
+  const int coarse = B->lv[nl - 1].sweep_smem ? (B->sweeps > 1 ? 1 : 0) : B->sweeps - 1;
+  return 1 + (nl - 1) + (nl - 2) + coarse + (nl - 1) + (nl - 2) + 1 + 1 + 1 + 1;
 }
 
 // The inner-loop graph of `chunk` FP32 iterations, kept in the exec slot and

@@ -573,6 +573,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!std::strcmp(key, "multigrid_omega") && value >= 0 && value < 1) { ctx->mg_omega = value; return MSG_OK; }
   if (!std::strcmp(key, "multigrid_delta") && value > 0 && value < 1) { ctx->mg_delta = value; return MSG_OK; }
   if (!std::strcmp(key, "multigrid_packed") && (value == 0 || value == 1)) { ctx->mg_packed = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "multigrid_fused_coarse") && (value == 0 || value == 1)) {
+    ctx->mg_fused_coarse = (int)value;
+    return MSG_OK;
+  }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 

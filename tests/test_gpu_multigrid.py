@@ -19,7 +19,8 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-DEFAULTS = {"multigrid": 1, "fixed_updates": 0, "multigrid_levels": 6, "multigrid_sweeps": 20, "multigrid_packed": 1}
+DEFAULTS = {"multigrid": 1, "fixed_updates": 0, "multigrid_levels": 6, "multigrid_sweeps": 20, "multigrid_packed": 1,
+            "multigrid_fused_coarse": 1}
 
 
 @contextlib.contextmanager
@@ -113,6 +114,41 @@ def test_multigrid_batch_invariant_with_fixed_updates(ctx):
             one = mixed_solve(ctx, model, kl, xi[r:r + 1], 1e-10)
             assert np.array_equal(one.Solutions[0], full.Solutions[r]), r
             assert one.Iterations[0] == full.Iterations[r]
+
+
+@pytest.mark.parametrize("case", ["cube16", "cantilever"])
+def test_fused_coarsest_sweeps_identical(ctx, case):
+    """All coarsest-level sweeps in one launch (multigrid_fused_coarse = 1)
+    return bit for bit what one launch per sweep returns: 2 x 2 x 2 coarsest
+    elements of a 16^3 cube and 5 x 2 x 2 of the 10 x 4 x 4 cantilever."""
+    if case == "cube16":
+        model, dims, R = M.clamped_block_model(16), (16, 16, 16), 70
+    else:
+        model, dims, R = M.cantilever_model(), (10, 4, 4), 12
+    kl, xi = problem(model, dims, R, seed=31)
+    with options(ctx, multigrid_fused_coarse=0):
+        ref = mixed_solve(ctx, model, kl, xi, 1e-10)
+    fused = mixed_solve(ctx, model, kl, xi, 1e-10)
+    assert np.array_equal(fused.Solutions, ref.Solutions)
+    assert np.array_equal(fused.Iterations, ref.Iterations)
+
+
+def test_fused_coarsest_sweeps_identical_with_mass(ctx):
+    """The same with a mass term (Newmark on the V-cycle loop)."""
+    n, R, steps, dt = 8, 33, 5, 0.01
+    model = M.clamped_block_model(n)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, 12, 6)
+    xi = np.random.default_rng(7).standard_normal((R, 12))
+    load = M.MassAccelerationSinusoidalLoad(1.0, dt, dt * steps, 0.1, dof=0)
+    out = []
+    for fused in (0, 1):
+        with options(ctx, multigrid=2, multigrid_fused_coarse=fused):
+            nm = M.NewmarkDynamicAnalyzer(ctx, model, kl, 0.25, 0.5, dt, dt * steps, load, expansion_order=12,
+                                          simulations=R, density=1.0, rayleigh_alpha=0.01, rayleigh_beta=0.001,
+                                          tolerance=1e-10)
+            nm.RandomNumbers = xi
+            out.append((nm.Solve(), nm.Solutions.copy()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
 @pytest.mark.parametrize("n,R,steps,mg", [(4, 3, 30, 2), (8, 33, 20, 2), (8, 33, 20, 1)])
