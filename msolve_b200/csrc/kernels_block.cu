@@ -1292,24 +1292,28 @@ __global__ void __launch_bounds__(kMWarps * 32, 1)
 // k_lvl_op with two realizations per lane in float2 registers: the element and
 // node arithmetic issues Blackwell's packed FP32 instructions (one issue slot
 // for both), halving the instructions per realization of an issue-bound
-// kernel. The doubled register state (up to 152 registers a thread) allows
-// 3 warps per SM sub-partition: a 3 x 2 tile of node pencils with its 12
-// element warps for 64 realizations, and no separate producer warp: lane 0
+// kernel. A 3 x 3 tile of node pencils with its 16 element warps for 64
+// realizations, at most 128 registers a thread (16 warps fill the register
+// file: 4 warps per SM sub-partition), and no separate producer warp: lane 0
 // of warp 0 issues the TMA loads two planes ahead (the 3-stage ring refills
 // the stage of the plane before the current one; its readers have arrived on
-// its "empty" barrier, a bounded wait). Modes, exchange, barriers and bounded
-// waits as k_lvl_op otherwise.
-constexpr int kQJ = 3, kQK = 2;                     // node pencils per tile (y, z)
-constexpr int kQEJ = kQJ + 1, kQEK = kQK + 1;       // element pencils 4 x 3
-constexpr int kQWarps = kQEJ * kQEK;                // 12 element warps
+// its "empty" barrier, a bounded wait). The exchange buffer holds corners 1..3
+// of each element (corner 0 stays in the registers of the warp that owns its
+// node pencil), which leaves room for the 5 x 5 node patches. Modes, barriers
+// and bounded waits as k_lvl_op otherwise.
+constexpr int kQJ = 3, kQK = 3;                     // node pencils per tile (y, z)
+constexpr int kQEJ = kQJ + 1, kQEK = kQK + 1;       // element pencils 4 x 4
+constexpr int kQWarps = kQEJ * kQEK;                // 16 element warps
 constexpr int kQThreads = 32 * kQWarps;
-constexpr int kQPJ = kQJ + 2, kQPK = kQK + 2;       // node patch 5 x 4
+constexpr int kQPJ = kQJ + 2, kQPK = kQK + 2;       // node patch 5 x 5
 constexpr int kQR = 64;                             // realizations per work item
 constexpr int kQPlane = kQR * 3 * kQPJ * kQPK;      // vector patch (floats)
 constexpr int kQNode = kQR * kQPJ * kQPK;           // dinv patch
 constexpr int kQE = kQR * kQEJ * kQEK;              // E patch
 constexpr int kQD = kQR * 3 * kQJ * kQK;            // d of the tile's own nodes
-constexpr int kQX = kQWarps * 4 * 3 * kQR;          // exchange buffer
+// exchange buffer: corners 1..3 of every element warp (corner 0 belongs to the
+// node pencil of the warp itself and stays in its registers)
+constexpr int kQX = kQWarps * 3 * 3 * kQR;
 template <int kMode> struct LvlStage2 {
   static constexpr bool kTwo = kMode == kLvlStart || kMode == kLvlPcgZ;
   // Smooth also stages b and dinv of the tile's own nodes, read by the node
@@ -1336,7 +1340,7 @@ static_assert(LvlStage2<kLvlPcgZ>::kSmem <= 227 * 1024 && LvlStage2<kLvlStart>::
               "smem");
 
 template <int kMode, bool kMass>
-__global__ void __maxnreg__(152)
+__global__ void __maxnreg__(128)
     k_lvl_op2(Lattice L, const __grid_constant__ ModalCT<float2> C, const __grid_constant__ CUtensorMap tm_a,
               const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_n,
               const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_d, int tiles_j,
@@ -1422,6 +1426,7 @@ __global__ void __maxnreg__(152)
     float2* out_2 = reinterpret_cast<float2*>(out);
     float2 Bp[3][4], T0[3][4];
     float2 ou[3] = {z2, z2, z2}, orc[3] = {z2, z2, z2};
+    float2 own[3] = {z2, z2, z2};  // corner 0 of the warp's element: its own node pencil
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -1444,10 +1449,10 @@ __global__ void __maxnreg__(152)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         float2 y = z2;
-        if (r00) y = y + xb[((w * 4 + 0) * 3 + c) * 32 + lane];
-        if (r10) y = y + xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
-        if (r01) y = y + xb[(((w - kQEJ) * 4 + 2) * 3 + c) * 32 + lane];
-        if (r11) y = y + xb[(((w - kQEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        if (r00) y = y + own[c];
+        if (r10) y = y + xb[(((w - 1) * 3 + 0) * 3 + c) * 32 + lane];
+        if (r01) y = y + xb[(((w - kQEJ) * 3 + 1) * 3 + c) * 32 + lane];
+        if (r11) y = y + xb[(((w - kQEJ - 1) * 3 + 2) * 3 + c) * 32 + lane];
         const size_t o = (node * 3 + c) * Rp2 + rr2;
         const bool fixed = (mk >> c) & 1;
         float2 v;
@@ -1477,11 +1482,12 @@ __global__ void __maxnreg__(152)
       yz_inverse(B, y);
       float2* xb = reinterpret_cast<float2*>(xbuf) + xsel * (kQX / 2);
 #pragma unroll
-      for (int ay = 0; ay < 2; ++ay)
-#pragma unroll
-        for (int az = 0; az < 2; ++az)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = y[ay][az][c];
+      for (int c = 0; c < 3; ++c) {
+        own[c] = y[0][0][c];
+        xb[((w * 3 + 0) * 3 + c) * 32 + lane] = y[1][0][c];
+        xb[((w * 3 + 1) * 3 + c) * 32 + lane] = y[0][1][c];
+        xb[((w * 3 + 2) * 3 + c) * 32 + lane] = y[1][1][c];
+      }
     };
     for (int P = 1; P <= NX; ++P, ++seq) {
       const int st = seq % kSt;
@@ -2805,7 +2811,7 @@ struct BlockSys {
   GmgLevel lv[kGmgMaxLevels];
   WSlot xs, arena;
   CUtensorMap tm_xs;
-  // packed level-0 operator (k_lvl_op2: 64 realizations per item, 3 x 2 tiles)
+  // packed level-0 operator (k_lvl_op2: 64 realizations per item, 3 x 3 tiles)
   bool pack = false;
   ModalCT<float2> MC2;
   int tiles_j2 = 0, n_tiles2 = 0, n_items2 = 0, grid2 = 0;
