@@ -2766,6 +2766,10 @@ struct GmgLevel {
   int tiles_j = 0, n_tiles = 0, n_items = 0, grid = 0;
   CUtensorMap tm_x, tm_t, tm_e;
   size_t sweep_smem = 0;  // coarsest level: all sweeps in one k_coarse_sweeps launch (0: launch per sweep)
+  // packed operator (k_lvl_op2) on this level: x patches, element patches, own b and dinv
+  ModalCT<float2> MC2;
+  int tiles_j2 = 0, n_tiles2 = 0, n_items2 = 0, grid2 = 0;
+  CUtensorMap tm2_x, tm2_e, tm2_bo, tm2_dinvo;
 };
 
 struct BlockSys {
@@ -3220,12 +3224,13 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
       // packed level-0 operator: realizations in multiples of 64
       B->pack = ctx->mg_packed && (Rp % kQR) == 0;
       if (B->pack) {
-        const ModalC& f = B->MC;
         auto b2 = [](float v) { return make_float2(v, v); };
-        ModalCT<float2>& g2 = B->MC2;
-        g2.vd = b2(f.vd); g2.vb = b2(f.vb); g2.sa = b2(f.sa); g2.sb = b2(f.sb); g2.pa = b2(f.pa); g2.pb = b2(f.pb);
-        g2.td = b2(f.td); g2.tb = b2(f.tb); g2.da = b2(f.da);
-        for (int i = 0; i < 8; ++i) g2.m[i] = b2(f.m[i]);
+        auto pack_c = [&](const ModalC& f, ModalCT<float2>& g2) {
+          g2.vd = b2(f.vd); g2.vb = b2(f.vb); g2.sa = b2(f.sa); g2.sb = b2(f.sb); g2.pa = b2(f.pa); g2.pb = b2(f.pb);
+          g2.td = b2(f.td); g2.tb = b2(f.tb); g2.da = b2(f.da);
+          for (int i = 0; i < 8; ++i) g2.m[i] = b2(f.m[i]);
+        };
+        pack_c(B->MC, B->MC2);
         B->tiles_j2 = (L.NY + kQJ - 1) / kQJ;
         B->n_tiles2 = B->tiles_j2 * ((L.NZ + kQK - 1) / kQK);
         B->n_items2 = B->n_tiles2 * (Rp / kQR);
@@ -3249,10 +3254,41 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
                                  enc4(&B->tm2_e, B->E32.ptr, eb2),  enc5(&B->tm2_d, B->d.ptr, db2)};
         for (CUresult r : r2)
           if (r != CUDA_SUCCESS) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (packed)");
+        // the coarse levels' residual and post-sweeps on the packed operator too
+        for (int l = 1; l < n_lvl; ++l) {
+          GmgLevel& g = B->lv[l];
+          const Lattice& Lc = g.L;
+          pack_c(g.MC, g.MC2);
+          g.tiles_j2 = (Lc.NY + kQJ - 1) / kQJ;
+          g.n_tiles2 = g.tiles_j2 * ((Lc.NZ + kQK - 1) / kQK);
+          g.n_items2 = g.n_tiles2 * (Rp / kQR);
+          g.grid2 = std::min(g.n_items2, ctx->sm_count);
+          const cuuint64_t cpd[5] = {(cuuint64_t)Rp, 3, (cuuint64_t)Lc.NXp, (cuuint64_t)Lc.NYp, (cuuint64_t)Lc.NZp};
+          const cuuint64_t cps[4] = {Rp * fb, 3 * Rp * fb, 3 * Rp * fb * Lc.NXp, 3 * Rp * fb * Lc.NXp * Lc.NYp};
+          const cuuint64_t ced[4] = {(cuuint64_t)Rp, (cuuint64_t)Lc.NXp, (cuuint64_t)Lc.NYp, (cuuint64_t)Lc.NZp};
+          const cuuint64_t ces[3] = {Rp * fb, Rp * fb * Lc.NXp, Rp * fb * Lc.NXp * Lc.NYp};
+          auto l5 = [&](CUtensorMap* tm, void* p, const cuuint32_t* box) {
+            return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, p, cpd, cps, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+          };
+          auto l4 = [&](CUtensorMap* tm, void* p, const cuuint32_t* box) {
+            return encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, p, ced, ces, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+          };
+          const CUresult rl[4] = {l5(&g.tm2_x, g.x, pb2), l4(&g.tm2_e, g.E32, eb2), l5(&g.tm2_bo, g.b, db2),
+                                  l4(&g.tm2_dinvo, g.dinv, ob2)};
+          for (CUresult r : rl)
+            if (r != CUDA_SUCCESS)
+              return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (packed level %d)", l);
+        }
         static std::once_flag pack_once;
         static cudaError_t pack_err = cudaSuccess;
         std::call_once(pack_once, [] {
           const std::pair<const void*, size_t> fs[] = {
+              {(const void*)k_lvl_op2<kLvlResid, false>, LvlStage2<kLvlResid>::kSmem},
+              {(const void*)k_lvl_op2<kLvlResid, true>, LvlStage2<kLvlResid>::kSmem},
               {(const void*)k_lvl_op2<kLvlStart, false>, LvlStage2<kLvlStart>::kSmem},
               {(const void*)k_lvl_op2<kLvlStart, true>, LvlStage2<kLvlStart>::kSmem},
               {(const void*)k_lvl_op2<kLvlSmooth, false>, LvlStage2<kLvlSmooth>::kSmem},
@@ -3408,6 +3444,19 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
           B->grid_m, B->mask, b, dinv, out, out2, out3, d, partial, pstride);
     }
   };
+  // coarse level l: residual (out = b - A x) or post-sweep (out = x + omega dinv (b - A x)) of x into t
+  auto lvlc = [&](auto mode, GmgLevel& g) {
+    constexpr int kMode = decltype(mode)::value;
+    if (B->pack) {
+      auto k = mass ? k_lvl_op2<kMode, true> : k_lvl_op2<kMode, false>;
+      k<<<g.grid2, kQThreads, LvlStage2<kMode>::kSmem, st>>>(
+          g.L, g.MC2, g.tm2_x, g.tm2_bo, g.tm2_dinvo, g.tm2_e, g.tm2_x, g.tiles_j2, g.n_tiles2, g.n_items2, g.mask, g.b,
+          g.dinv, om, s.alpha, s.beta, g.t, nullptr, nullptr, nullptr, nullptr, 1, s.err);
+    } else {
+      lvl(mode, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid, g.mask,
+          g.b, kMode == kLvlSmooth ? g.dinv : nullptr, g.t, nullptr, nullptr, nullptr, nullptr, 1);
+    }
+  };
   using Start = std::integral_constant<int, kLvlStart>;
   using Resid = std::integral_constant<int, kLvlResid>;
   using Smooth = std::integral_constant<int, kLvlSmooth>;
@@ -3423,9 +3472,7 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
     const float* tf = l == 1 ? qB : B->lv[l - 1].t;
     k_restrict<<<xfer_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(Lf, g.L, g.interior, g.mask, tf, g.dinv, om, g.b,
                                                                      g.x);
-    if (l < nl - 1)
-      lvl(Resid{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
-          g.mask, g.b, nullptr, g.t, nullptr, nullptr, nullptr, nullptr, 1);
+    if (l < nl - 1) lvlc(Resid{}, g);
   }
   // coarsest level: the restriction made the first sweep; sweeps - 1 more, x and t alternating
   const float* res_c;
@@ -3453,8 +3500,7 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
     GmgLevel& g = B->lv[l];
     k_prolong_add<<<xfer_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(g.L, B->lv[l + 1].L, g.interior, g.mask, res_c,
                                                                         g.x);
-    lvl(Smooth{}, g.L, g.MC, g.tm_x, g.tm_x, g.tm_x, g.tm_e, g.tm_x, g.tiles_j, g.n_tiles, g.n_items, g.grid,
-        g.mask, g.b, g.dinv, g.t, nullptr, nullptr, nullptr, nullptr, 1);
+    lvlc(Smooth{}, g);
     res_c = g.t;
   }
   k_prolong_add<<<xfer_grid(B->L.n_int, Rp), xfer_block(Rp), 0, st>>>(B->L, B->lv[1].L, B->interior, B->mask, res_c,
