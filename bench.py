@@ -44,9 +44,10 @@ METRIC = "Hexa8 PCG solves/s at 1e-8 rel err, batched mixed vs plain FP64; p50/p
 # DRAM traffic of one k_op_modal launch per realization on the 32^3 lattice: ncu capture
 # at R = 512 (dram__bytes_read.sum 1,165.9 MB + dram__bytes_write.sum 845.5 MB) / 512
 OP_DRAM_BYTES_PER_REALIZATION = (1165.921e6 + 845.472e6) / 512
-# the same for the multigrid loop's direction + operator launch (packed k_lvl_op2<PcgZ>), 32^3
-# lattice, ncu capture at R = 512: dram__bytes_read.sum 840.9 MB + dram__bytes_write.sum 626.0 MB
-MG_OP_DRAM_BYTES_PER_REALIZATION = (840.853e6 + 626.001e6) / 512
+# the same for the multigrid loop's direction + operator launch (packed k_lvl_op2<PcgZ>, 3 x 3
+# node tiles), 32^3 lattice, ncu capture at R = 512: dram__bytes_read.sum 823.2 MB +
+# dram__bytes_write.sum 626.8 MB
+MG_OP_DRAM_BYTES_PER_REALIZATION = (823.197e6 + 626.791e6) / 512
 
 
 def parse():
