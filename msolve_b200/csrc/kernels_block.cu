@@ -1092,7 +1092,7 @@ __global__ void __launch_bounds__(kMThreads, 1)
             const size_t o = (node * 3 + c) * Rp + rr;
             if constexpr (kMode == kLvlStart) {
               out2[o] = rc[c];
-              out3[o] = u[0][0][c];
+              if (out3 != nullptr) out3[o] = u[0][0][c];
             } else {
               const int op = ek * kMPJ + ej, od = (ek - 1) * kMJ + (ej - 1);
               const float pold = pt[S::kOffB + (op * 3 + c) * 32 + lane];
@@ -1316,24 +1316,26 @@ constexpr int kQD = kQR * 3 * kQJ * kQK;            // d of the tile's own nodes
 constexpr int kQX = kQWarps * 3 * 3 * kQR;
 template <int kMode> struct LvlStage2 {
   static constexpr bool kTwo = kMode == kLvlStart || kMode == kLvlPcgZ;
-  // Smooth also stages b and dinv of the tile's own nodes, read by the node
-  // phase one plane later: its stages are released after that node phase, so
-  // the ring has 4 stages (loads still go two planes ahead)
-  static constexpr bool kOwn = kMode == kLvlSmooth;
+  // Smooth and Resid also stage b of the tile's own nodes (Smooth its dinv as
+  // well), read by the node phase one plane later: their stages are released
+  // after that node phase, so the ring has 4 stages (loads still go two planes ahead)
+  static constexpr bool kOwn = kMode == kLvlSmooth || kMode == kLvlResid;
+  static constexpr bool kOwnD = kMode == kLvlSmooth;
   static constexpr int kStages = kOwn ? 4 : kMStages;
   static constexpr int kOffA = 0;
   static constexpr int kOffB = kQPlane;
   static constexpr int kOffN = (kTwo ? 2 : 1) * kQPlane;
   static constexpr int kOffE = kOffN + (kMode == kLvlStart ? kQNode : 0);
-  static constexpr int kOffD = kOffE + kQE;  // d (direction) or own b (smooth)
+  static constexpr int kOffD = kOffE + kQE;  // d (direction) or own b (smooth, resid)
   static constexpr int kOffO = kOffD + (kOwn ? kQD : 0);  // own dinv (smooth)
-  static constexpr int kFloats = kOffO + (kMode == kLvlPcgZ ? kQD : 0) + (kOwn ? kQR * kQJ * kQK : 0);
+  static constexpr int kFloats = kOffO + (kMode == kLvlPcgZ ? kQD : 0) + (kOwnD ? kQR * kQJ * kQK : 0);
   static constexpr uint32_t kBytes = kFloats * 4;
   static constexpr size_t kSmem = 128 + sizeof(float) * ((size_t)kStages * kFloats + 2 * (size_t)kQX) +
                                   sizeof(double) * kQJ * kQK * kQR + sizeof(uint64_t) * (2 * kStages);
 };
 static_assert(LvlStage2<kLvlStart>::kBytes % 128 == 0 && LvlStage2<kLvlSmooth>::kBytes % 128 == 0 &&
-                  LvlStage2<kLvlPcgZ>::kBytes % 128 == 0,
+                  LvlStage2<kLvlPcgZ>::kBytes % 128 == 0 && LvlStage2<kLvlResid>::kBytes % 128 == 0 &&
+                  LvlStage2<kLvlResid>::kSmem <= 227 * 1024,
               "stage alignment");
 static_assert(LvlStage2<kLvlPcgZ>::kSmem <= 227 * 1024 && LvlStage2<kLvlStart>::kSmem <= 227 * 1024 &&
                   LvlStage2<kLvlSmooth>::kSmem <= 227 * 1024 && (kQR * kQJ * kQK * 4) % 128 == 0,
@@ -1389,10 +1391,8 @@ __global__ void __maxnreg__(128)
     if constexpr (kMode == kLvlStart) tma_load_4d(dst + S::kOffN, &tm_n, g64, P, J0 - 1, K0 - 1, &full[st]);
     tma_load_4d(dst + S::kOffE, &tm_e, g64, P - 1, J0 - 1, K0 - 1, &full[st]);
     if constexpr (kMode == kLvlPcgZ) tma_load_5d(dst + S::kOffD, &tm_d, g64, 0, P, J0, K0, &full[st]);
-    if constexpr (S::kOwn) {
-      tma_load_5d(dst + S::kOffD, &tm_b, g64, 0, P, J0, K0, &full[st]);
-      tma_load_4d(dst + S::kOffO, &tm_n, g64, P, J0, K0, &full[st]);
-    }
+    if constexpr (S::kOwn) tma_load_5d(dst + S::kOffD, &tm_b, g64, 0, P, J0, K0, &full[st]);
+    if constexpr (S::kOwnD) tma_load_4d(dst + S::kOffO, &tm_n, g64, P, J0, K0, &full[st]);
   };
   if (producer) {
     produce(0);
@@ -1461,7 +1461,7 @@ __global__ void __maxnreg__(128)
           s0 = fma((double)orc[c].x, (double)orc[c].x, s0);
           s1 = fma((double)orc[c].y, (double)orc[c].y, s1);
         } else if constexpr (kMode == kLvlResid) {
-          v = fixed ? z2 : reinterpret_cast<const float2*>(b)[o] - y;
+          v = fixed ? z2 : reinterpret_cast<const float2*>(px + S::kOffD)[(od * 3 + c) * 32 + lane] - y;
         } else if constexpr (kMode == kLvlSmooth) {
           const float2 bv = reinterpret_cast<const float2*>(px + S::kOffD)[(od * 3 + c) * 32 + lane];
           v = fixed ? z2 : fmx(wdv, bv - y, ou[c]);
@@ -1531,7 +1531,7 @@ __global__ void __maxnreg__(128)
             const size_t o = (node * 3 + c) * Rp2 + rr2;
             if constexpr (kMode == kLvlStart) {
               reinterpret_cast<float2*>(out2)[o] = rc[c];
-              reinterpret_cast<float2*>(out3)[o] = u[0][0][c];
+              if (out3 != nullptr) reinterpret_cast<float2*>(out3)[o] = u[0][0][c];
             } else {
               const int op = ek * kQPJ + ej, od = (ek - 1) * kQJ + (ej - 1);
               const float2 pold = pb[(op * 3 + c) * 32 + lane];
@@ -1882,16 +1882,22 @@ __global__ void __launch_bounds__(kXferThreads, 8) k_restrict(Lattice Lf, Lattic
 // the mean of its two neighbours), masked at the fine level. Grid as
 // k_restrict over the fine interior nodes; the 8 corner terms are summed in a
 // fixed order (the terms of an even axis's second neighbour, weight 0, are skipped).
+// With r0 given, the iterate before the correction is not read from x_f but
+// formed as the first Jacobi sweep from zero, x0 = (omega dinv0) r0, with the
+// arithmetic of the start pass (which then need not write it), and x_f is
+// written at every component (the constrained ones without the correction).
 __global__ void __launch_bounds__(kXferThreads, 8) k_prolong_add(Lattice Lf, Lattice Lc,
                                                                  const int* __restrict__ interior_f,
                                                                  const uint8_t* __restrict__ mask_f,
-                                                                 const float* __restrict__ xc, float* __restrict__ xf) {
+                                                                 const float* __restrict__ xc, float* __restrict__ xf,
+                                                                 const float* __restrict__ r0,
+                                                                 const float* __restrict__ dinv0, float omega) {
   const int Q = Lf.Rp >> 2;
   const int q = blockIdx.y * kXferThreads + threadIdx.x;
   if (q >= Q) return;
   const int nf = interior_f[blockIdx.x];
   const uint32_t mk = mask_f[nf];
-  if (mk == 7u) return;
+  if (mk == 7u && r0 == nullptr) return;
   const int gi = nf % Lf.NXp - 1, gj = (nf / Lf.NXp) % Lf.NYp - 1, gk = nf / (Lf.NXp * Lf.NYp) - 1;
   const int sx = 3 * Q, sy = Lc.NXp * sx, sz = Lc.NYp * sy;  // float4 strides between coarse nodes
   const int c0 = ((gi >> 1) + 1) + Lc.NXp * (((gj >> 1) + 1) + Lc.NYp * ((gk >> 1) + 1));
@@ -1901,10 +1907,25 @@ __global__ void __launch_bounds__(kXferThreads, 8) k_prolong_add(Lattice Lf, Lat
   const float wk[2] = {(gk & 1) ? 0.5f : 1.f, (gk & 1) ? 0.5f : 0.f};
   const float4* c4 = reinterpret_cast<const float4*>(xc) + (size_t)c0 * sx + q;
   float4* f4 = reinterpret_cast<float4*>(xf) + (size_t)nf * sx + q;
+  float4 wdv = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (r0 != nullptr) {
+    const float4 dv = reinterpret_cast<const float4*>(dinv0)[(size_t)nf * Q + q];
+    wdv = make_float4(omega * dv.x, omega * dv.y, omega * dv.z, omega * dv.w);
+  }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    if ((mk >> c) & 1) continue;
-    float4 s = f4[c * Q];
+    float4 s;
+    if (r0 != nullptr) {
+      const float4 rv = reinterpret_cast<const float4*>(r0)[((size_t)nf * 3 + c) * Q + q];
+      s = make_float4(wdv.x * rv.x, wdv.y * rv.y, wdv.z * rv.z, wdv.w * rv.w);
+      if ((mk >> c) & 1) {
+        f4[c * Q] = s;
+        continue;
+      }
+    } else {
+      if ((mk >> c) & 1) continue;
+      s = f4[c * Q];
+    }
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -3462,9 +3483,10 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   using Smooth = std::integral_constant<int, kLvlSmooth>;
   using PcgZ = std::integral_constant<int, kLvlPcgZ>;
   if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-  // level 0: r' = r - alpha q, xs = omega dinv r', qB = r' - A xs, partial r'.r'
-  lvl0(Start{}, tm_rin, B->tm_qAm, even ? B->tm2_rA : B->tm2_rB, B->tm2_qA, nullptr, nullptr, qB, r_out,
-       B->xs.as<float>(), nullptr, part2, 2);
+  // level 0: r' = r - alpha q, qB = r' - A x0 with x0 = omega dinv r', partial r'.r'
+  // (x0 itself is formed again by the level-0 prolongation)
+  lvl0(Start{}, tm_rin, B->tm_qAm, even ? B->tm2_rA : B->tm2_rB, B->tm2_qA, nullptr, nullptr, qB, r_out, nullptr,
+       nullptr, part2, 2);
   // down: restrict the residual, residual of the first sweep on every level but the coarsest
   for (int l = 1; l < nl; ++l) {
     GmgLevel& g = B->lv[l];
@@ -3499,12 +3521,14 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   for (int l = nl - 2; l >= 1; --l) {
     GmgLevel& g = B->lv[l];
     k_prolong_add<<<xfer_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(g.L, B->lv[l + 1].L, g.interior, g.mask, res_c,
-                                                                        g.x);
+                                                                        g.x, nullptr, nullptr, 0.f);
     lvlc(Smooth{}, g);
     res_c = g.t;
   }
+  // level 0: x0 = omega dinv r' formed here (the start pass does not write it)
   k_prolong_add<<<xfer_grid(B->L.n_int, Rp), xfer_block(Rp), 0, st>>>(B->L, B->lv[1].L, B->interior, B->mask, res_c,
-                                                                        B->xs.as<float>());
+                                                                        B->xs.as<float>(), r_out, B->dinv.as<float>(),
+                                                                        om);
   // level 0 post-sweep: z (into qB) and the partial z.r'
   lvl0(Smooth{}, B->tm_xs, B->tm_xs, B->tm2_xs, B->tm2_xs, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr,
        part2 + 1, 2);
