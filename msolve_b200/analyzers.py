@@ -20,6 +20,9 @@ MonteCarloAnalyzerWithStochasticMaterial.cs:55-296.
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
+import os
+import time
 
 import numpy as np
 
@@ -354,36 +357,109 @@ class GaussianStochasticCoefficientsProvider(LognormalStochasticCoefficientsProv
         self.covariance = covariance
 
 
+def _timespan(seconds):
+    """C# TimeSpan.ToString() layout (hh:mm:ss.fffffff), as the reference's -Times.txt lines."""
+    ticks = int(round(seconds * 1e7))
+    h, rem = divmod(ticks, 36000000000)
+    m, rem = divmod(rem, 600000000)
+    sec, frac = divmod(rem, 10000000)
+    return f"{h:02d}:{m:02d}:{sec:02d}" + (f".{frac:07d}" if frac else "")
+
+
+def write_randoms(path, table):
+    """The reference's random-number file (MonteCarloAnalyzerWithStochasticMaterial.cs:197-203):
+    one value per line, expansion term outermost: for j in terms, for i in simulations."""
+    table = np.asarray(table, dtype=np.float64)
+    with open(path, "w") as f:
+        for j in range(table.shape[1]):
+            for i in range(table.shape[0]):
+                f.write(repr(float(table[i, j])) + "\n")
+
+
+def read_randoms(path, simulations, expansion_order):
+    """Read `simulations` x `expansion_order` values in the layout of write_randoms
+    (MonteCarloAnalyzerWithStochasticMaterial.cs:207-215, randomFileSimulations rows)."""
+    vals = np.loadtxt(path, dtype=np.float64, ndmin=1)
+    need = simulations * expansion_order
+    if vals.size < need:
+        raise ValueError(f"{path}: {vals.size} values, {need} needed ({simulations} x {expansion_order})")
+    return vals[:need].reshape(expansion_order, simulations).T.copy()
+
+
 class MonteCarloAnalyzerWithStochasticMaterial:
     """The realization loop (MonteCarloAnalyzerWithStochasticMaterial.cs:55-296).
     Initialize() draws xi[simulations][expansion_order] ~ N(0,1) from a seeded
     generator (the reference draws with Troschuetz.Random; the stream is not part
-    of parity, the same table feeds every implementation). Solve() runs all
-    realizations through MSG_MC_SOLVE_BATCH in `mode` ("mixed": one batched
-    mixed-precision launch sequence; "fp64": the plain FP64 drop-in, one
-    realization after another). Results: Solutions [R][n_dofs] (if keep_solutions),
-    TipValues [R], Iterations [R], Residuals [R]."""
+    of parity, the same table feeds every implementation), or reads the
+    reference's random-number file (`randoms_read_file_name`, its first
+    `random_file_simulations` rows). Solve() runs realizations
+    simulation_start_from ... simulation_start_from + simulations - 1 of that
+    table through MSG_MC_SOLVE_BATCH in `mode` ("mixed": batched mixed-precision
+    launches; "fp64": the plain FP64 drop-in, one realization after another), in
+    batches of `batch_size` (all at once by default). Results: Solutions
+    [R][n_dofs] (if keep_solutions), TipValues [R], Iterations [R], Residuals [R].
+
+    With `file_name_for_logging` the reference's text files are written:
+    randoms{order}.txt next to it when the table is drawn, and per solved
+    realization {name}-{order}-{start}.txt (tip value), -Iters.txt (operator
+    products; the reference writes a counter it never fills) and -Times.txt
+    (rewritten after every batch). With `checkpoint` (a path) the analyzer
+    resumes by realization index: after every batch it saves the finished mask
+    with the tip values, iterations and residuals next to a fingerprint of the
+    realization table; a later Solve() with the same table solves only the
+    realizations not yet finished (their Solutions rows stay NaN)."""
 
     def __init__(self, ctx, model, coefficients_provider, expansion_order=50, simulations=1, seed=12345,
-                 mode="mixed", max_iterations=20000, tolerance=1e-8, keep_solutions=True, tip_dof=None):
+                 mode="mixed", max_iterations=20000, tolerance=1e-8, keep_solutions=True, tip_dof=None,
+                 randoms_read_file_name="", simulation_start_from=0, random_file_simulations=50000,
+                 file_name_for_logging=None, batch_size=None, checkpoint=None):
         self.ctx, self.model, self.kl = ctx, model, coefficients_provider
         self.expansion_order, self.simulations, self.seed = expansion_order, simulations, seed
         self.mode = N.MSG_MODE_MIXED_BATCHED if mode == "mixed" else N.MSG_MODE_FP64_BSR
         self.max_iterations, self.tolerance = max_iterations, tolerance
         self.keep_solutions = keep_solutions
         self.tip_dof = _tip_dof(model) if tip_dof is None else tip_dof
-        self.mesh = GpuMesh(ctx, model)
+        if simulation_start_from < 0 or simulations < 1:
+            raise N.ArgumentError(N.MSG_ERR_INVALID_ARGUMENT, "simulations must be >= 1 and simulation_start_from >= 0")
+        self.randoms_read_file_name = randoms_read_file_name
+        self.simulation_start_from = simulation_start_from
+        self.random_file_simulations = random_file_simulations
+        self.file_name_for_logging = file_name_for_logging
+        self.batch_size = batch_size
+        self.checkpoint = checkpoint
+        self._mesh = None
         self.RandomNumbers = None
 
-    def Initialize(self):
-        rng = np.random.default_rng(self.seed)
-        self.RandomNumbers = rng.standard_normal((self.simulations, self.expansion_order))
+    @property
+    def mesh(self):
+        if self._mesh is None:
+            self._mesh = GpuMesh(self.ctx, self.model)
+        return self._mesh
 
-    def Solve(self):
-        if self.RandomNumbers is None:
-            self.Initialize()
-        R = self.simulations
-        xi = N.f64(self.RandomNumbers)
+    def Initialize(self):
+        order = self.expansion_order
+        if self.randoms_read_file_name:
+            self.RandomNumbers = read_randoms(self.randoms_read_file_name, self.random_file_simulations, order)
+        else:
+            rng = np.random.default_rng(self.seed)
+            self.RandomNumbers = rng.standard_normal((self.simulations, order))
+            if self.file_name_for_logging is not None:
+                folder = os.path.dirname(self.file_name_for_logging)
+                write_randoms(os.path.join(folder, f"randoms{order}.txt"), self.RandomNumbers)
+
+    def _rows(self):
+        s0, R = self.simulation_start_from, self.simulations
+        table = np.asarray(self.RandomNumbers, dtype=np.float64)
+        if table.ndim != 2 or table.shape[1] < self.expansion_order or table.shape[0] < s0 + R:
+            raise N.ArgumentError(N.MSG_ERR_INVALID_ARGUMENT,
+                                  f"random-number table {table.shape} does not hold realizations {s0}..{s0 + R - 1} "
+                                  f"of {self.expansion_order} terms")
+        return np.ascontiguousarray(table[s0:s0 + R, :self.expansion_order])
+
+    def _solve_batch(self, xi):
+        """One MSG_MC_SOLVE_BATCH call: (tip, iterations, residuals, solutions or None)."""
+        R = xi.shape[0]
+        xi = N.f64(xi)
         b = N.f64(self.model.subdomains[0].RHS)
         X = np.zeros((R, self.model.n_dofs)) if self.keep_solutions else None
         tip = np.zeros(R)
@@ -393,9 +469,76 @@ class MonteCarloAnalyzerWithStochasticMaterial:
         st = N.lib().MSG_MC_SOLVE_BATCH(self.mesh.handle, float(self.model.poisson), C.byref(s), R, N.ptr(xi), N.ptr(b),
                                         self.mode, int(self.max_iterations), float(self.tolerance), int(self.tip_dof),
                                         N.ptr(X) if X is not None else None, N.ptr(tip), N.ptr(its, N._i), N.ptr(res))
-        self.Solutions, self.TipValues, self.Iterations, self.Residuals = X, tip, its, res
-        N.check(st, self.ctx.handle, "MSG_MC_SOLVE_BATCH")
-        return tip
+        if st not in (N.MSG_OK, N.MSG_ERR_NOT_CONVERGED):
+            N.check(st, self.ctx.handle, "MSG_MC_SOLVE_BATCH")
+        return tip, its, res, X, st
+
+    def _log_names(self):
+        base = f"{self.file_name_for_logging}-{self.expansion_order}-{self.simulation_start_from}"
+        return base + ".txt", base + "-Iters.txt", base + "-Times.txt"
+
+    def _load_checkpoint(self, xi):
+        fp = np.frombuffer(hashlib.sha256(xi.tobytes()).digest(), dtype=np.uint8)
+        R = xi.shape[0]
+        state = dict(done=np.zeros(R, dtype=bool), tip=np.zeros(R), its=np.zeros(R, dtype=np.int32), res=np.zeros(R),
+                     fingerprint=fp)
+        if self.checkpoint and os.path.exists(self.checkpoint):
+            with np.load(self.checkpoint) as z:
+                if not np.array_equal(z["fingerprint"], fp) or int(z["start"]) != self.simulation_start_from:
+                    raise ValueError(f"{self.checkpoint}: checkpoint of another realization table or start index")
+                for k in ("done", "tip", "its", "res"):
+                    state[k] = z[k].copy()
+        return state
+
+    def _save_checkpoint(self, state):
+        tmp = self.checkpoint + ".tmp.npz"
+        np.savez(tmp, start=np.int64(self.simulation_start_from), **state)
+        os.replace(tmp, self.checkpoint)
+
+    def Solve(self):
+        if self.RandomNumbers is None:
+            self.Initialize()
+        xi = self._rows()
+        R = xi.shape[0]
+        state = self._load_checkpoint(xi)
+        X = np.full((R, self.model.n_dofs), np.nan) if self.keep_solutions else None
+        logging = self.file_name_for_logging is not None
+        if logging and not state["done"].any():
+            for name in self._log_names()[:2]:
+                open(name, "w").close()
+        todo = np.flatnonzero(~state["done"])
+        batch = int(self.batch_size or R)
+        status = N.MSG_OK
+        t_all = time.perf_counter()
+        t_solve = 0.0
+        for k in range(0, len(todo), batch):
+            idx = todo[k:k + batch]
+            t0 = time.perf_counter()
+            tip, its, res, Xb, st = self._solve_batch(xi[idx])
+            t_solve += time.perf_counter() - t0
+            if st != N.MSG_OK:
+                status = st
+            state["tip"][idx], state["its"][idx], state["res"][idx] = tip, its, res
+            state["done"][idx] = True
+            if X is not None and Xb is not None:
+                X[idx] = Xb
+            if logging:
+                values, iters, times = self._log_names()
+                with open(values, "a") as f:
+                    f.writelines(repr(float(v)) + "\n" for v in tip)
+                with open(iters, "a") as f:
+                    f.writelines(f"{int(v)}\n" for v in its)
+                with open(times, "w") as f:
+                    f.write(f"Elements: {_timespan(0.0)}\nFactorize: {_timespan(0.0)}\n"
+                            f"Solution: {_timespan(t_solve)}\nAll: {_timespan(time.perf_counter() - t_all)}\n"
+                            f"Total iterations: {int(state['its'][state['done']].sum())}\n")
+            if self.checkpoint:
+                self._save_checkpoint(state)
+        self.Solutions, self.TipValues = X, state["tip"]
+        self.Iterations, self.Residuals = state["its"], state["res"]
+        if status != N.MSG_OK:
+            N.check(status, self.ctx.handle, "MSG_MC_SOLVE_BATCH")
+        return self.TipValues
 
     def statistics(self):
         t = self.TipValues

@@ -126,3 +126,32 @@ def test_mixed_32cube_sample_against_oracle(ctx):
     xo, _ = oracle_solve(model, n, E[7], tol=1e-12)
     err = np.abs(mc.Solutions[7] - xo).max() / np.abs(xo).max()
     assert err <= 1e-8, err
+
+
+def test_batches_and_resume_match_one_call(ctx, tmp_path):
+    """batch_size splits and a checkpointed resume return, bit for bit, what one
+    call over all realizations returns (fixed_updates = 1: per-realization
+    arithmetic independent of the batch)."""
+    n, R = 8, 45
+    model, kl, xi = setup(n, R, seed=11)
+    ctx.set_option("fixed_updates", 1)
+    try:
+        one = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R,
+                                                         tolerance=1e-10)
+        one.RandomNumbers = xi
+        one.Solve()
+        ck = str(tmp_path / "mc.npz")
+        split = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R,
+                                                           tolerance=1e-10, batch_size=16, checkpoint=ck)
+        split.RandomNumbers = xi
+        split.Solve()
+        assert np.array_equal(split.Solutions, one.Solutions)
+        assert np.array_equal(split.TipValues, one.TipValues) and np.array_equal(split.Iterations, one.Iterations)
+        # a second analyzer on the finished checkpoint solves nothing and reports the same values
+        again = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=20, simulations=R,
+                                                           tolerance=1e-10, batch_size=16, checkpoint=ck)
+        again.RandomNumbers = xi
+        again.Solve()
+        assert np.isnan(again.Solutions).all() and np.array_equal(again.TipValues, one.TipValues)
+    finally:
+        ctx.set_option("fixed_updates", 0)
