@@ -265,7 +265,10 @@ int MSG_PC_GALERKIN_MATVEC(MSG_MESH mesh, double nu, const MSG_KL* kl, int m, in
  *     ||b - K x||/||b|| < tol in FP64.
  * xi [R][kl->n_terms], b [n_dofs]. Outputs (each may be NULL): X [R][n_dofs],
  * tip [R] = X[r][tip_dof], iterations [R] (matrix products per realization),
- * rel_res [R] (final FP64 ||b - K x||/||b||). */
+ * rel_res [R] (final FP64 ||b - K x||/||b||). A realization that does not
+ * converge or breaks down (p.q <= 0 or NaN, e.g. from a NaN modulus) makes the
+ * call return MSG_ERR_NOT_CONVERGED or MSG_ERR_BREAKDOWN; the outputs of the
+ * other realizations are still complete. */
 int MSG_MC_SOLVE_BATCH(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const double* xi, const double* b,
                        int mode, int max_it, double tol, int tip_dof, double* X, double* tip, int* iterations,
                        double* rel_res);
@@ -390,6 +393,16 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
  * MonteCarloAnalyzerWithStochasticMaterial.cs:244-292). */
 int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t8);
 int MSG_STATS_RESET(MSG_CTX ctx);
+
+/* Self-test of the failure path of the bounded device waits (no reference
+ * counterpart). Every wait of the staged operators (an mbarrier that a TMA
+ * load or the other warps complete) polls a bounded number of times and, when
+ * it gives up, records the expiry in an error word and lets its kernel return;
+ * the batch then ends with MSG_ERR_TIMEOUT and the context stays usable. This
+ * entry launches one thread that waits, with `polls` polls (1 ... 2^24), on an
+ * mbarrier that nothing completes: it returns MSG_ERR_TIMEOUT when the wait
+ * expired as designed (MSG_OK would mean it completed). */
+int MSG_WAIT_SELFTEST(MSG_CTX ctx, int64_t polls);
 
 #ifdef __cplusplus
 }

@@ -116,6 +116,7 @@ SIGNATURES = {
     "MSG_SET_OPTION": (C.c_int, [_vp, C.c_char_p, C.c_double]),
     "MSG_STATS": (C.c_int, [_vp, _i64, _d]),
     "MSG_STATS_RESET": (C.c_int, [_vp]),
+    "MSG_WAIT_SELFTEST": (C.c_int, [_vp, C.c_int64]),
 }
 
 _lib = None

@@ -469,7 +469,7 @@ class MonteCarloAnalyzerWithStochasticMaterial:
         st = N.lib().MSG_MC_SOLVE_BATCH(self.mesh.handle, float(self.model.poisson), C.byref(s), R, N.ptr(xi), N.ptr(b),
                                         self.mode, int(self.max_iterations), float(self.tolerance), int(self.tip_dof),
                                         N.ptr(X) if X is not None else None, N.ptr(tip), N.ptr(its, N._i), N.ptr(res))
-        if st not in (N.MSG_OK, N.MSG_ERR_NOT_CONVERGED):
+        if st not in (N.MSG_OK, N.MSG_ERR_NOT_CONVERGED, N.MSG_ERR_BREAKDOWN):  # per-realization outcomes
             N.check(st, self.ctx.handle, "MSG_MC_SOLVE_BATCH")
         return tip, its, res, X, st
 
@@ -537,7 +537,7 @@ class MonteCarloAnalyzerWithStochasticMaterial:
         self.Solutions, self.TipValues = X, state["tip"]
         self.Iterations, self.Residuals = state["its"], state["res"]
         if status != N.MSG_OK:
-            N.check(status, self.ctx.handle, "MSG_MC_SOLVE_BATCH")
+            N.check(status, self.ctx.handle if self.ctx is not None else None, "MSG_MC_SOLVE_BATCH")
         return self.TipValues
 
     def statistics(self):

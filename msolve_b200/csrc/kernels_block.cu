@@ -331,9 +331,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_n(uint64_t* bar, uint32_t parity, long limit) {
   const uint32_t a = smem_u32(bar);
-  for (long i = 0; i < kWaitLimit; ++i) {
+  for (long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
@@ -343,6 +343,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (done) return true;
   }
   return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return mbar_wait_n(bar, parity, kWaitLimit); }
+
+// Self-test of the bounded waits: one thread waits, with `polls` polls, on an
+// mbarrier that nothing completes and records the expiry in *err, as every
+// operator wait does; the kernel then returns normally.
+__global__ void k_wait_selftest(long polls, int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_n(&bar, 0, polls)) atomicExch(err, 1);
 }
 __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
                                             uint64_t* bar) {
@@ -3910,6 +3924,20 @@ int pc_matvec(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int mo, int po
   MSG_CUDA(ctx, cudaGetLastError());
   MSG_CUDA(ctx, cudaMemcpyAsync(y_host, dy.ptr, sizeof(double) * (size_t)P * m->n_dofs, cudaMemcpyDeviceToHost, st));
   MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  return MSG_OK;
+}
+
+int wait_selftest(Context* ctx, long polls, int* expired) {
+  DevMem flag;
+  MSG_TRY(flag.alloc(ctx, sizeof(int)));
+  MSG_CUDA(ctx, cudaMemsetAsync(flag.ptr, 0, sizeof(int), ctx->stream));
+  k_wait_selftest<<<1, 32, 0, ctx->stream>>>(polls, flag.as<int>());
+  count_launch(ctx, 1);
+  int h = 0;
+  MSG_CUDA(ctx, cudaMemcpyAsync(&h, flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  MSG_CUDA(ctx, cudaGetLastError());
+  *expired = h;
   return MSG_OK;
 }
 

@@ -600,6 +600,15 @@ int MSG_STATS_RESET(MSG_CTX ctx) {
   return MSG_OK;
 }
 
+int MSG_WAIT_SELFTEST(MSG_CTX ctx, int64_t polls) {
+  CTX_GUARD(ctx);
+  if (polls < 1 || polls > (int64_t)1 << 24)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "wait self-test: polls must be in [1, 2^24]");
+  int expired = 0;
+  MSG_TRY(wait_selftest(ctx, (long)polls, &expired));
+  return expired ? set_error(ctx, MSG_ERR_TIMEOUT, "bounded wait expired (self-test)") : MSG_OK;
+}
+
 int MSG_H8_KE_BATCH(MSG_CTX ctx, int n, const double* xyz, const double* E, double nu, double* Ke) {
   CTX_GUARD(ctx);
   if (n < 0 || (n > 0 && (!xyz || !E || !Ke))) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "KE batch: bad args");
@@ -1012,7 +1021,8 @@ int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const dou
   MSG_CUDA(ctx, cudaMemcpyAsync(db, b, sizeof(double) * (size_t)m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
   int st = mc_batch(ctx, m, nu, kl, R, static_cast<double*>(dxi), static_cast<double*>(db), mode, max_it, tol, tip_dof,
                     X ? static_cast<double*>(dX) : nullptr, tip, iterations, rel_res);
-  if (X && (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED)) {
+  // per-realization outcomes (not converged, breakdown): the other realizations' results are valid
+  if (X && (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED || st == MSG_ERR_BREAKDOWN)) {
     MSG_CUDA(ctx, cudaMemcpyAsync(X, dX, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }

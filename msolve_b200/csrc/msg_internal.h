@@ -280,6 +280,9 @@ int launch_kl_field(Context* ctx, const Mesh* m, const KLDevice* kl, int R, int 
 int launch_kl_field_slots(cudaStream_t st, const Mesh* m, const KLDevice* kl, int n_slots, const int* d_slots,
                           const double* d_xi, int Rp, double* d_E64, float* d_E32);
 
+// self-test of the bounded device waits (kernels_block.cu): *expired = 1 when the wait gave up
+int wait_selftest(Context* ctx, long polls, int* expired);
+
 // batched mixed-precision solve on a structured lattice (kernels_block.cu)
 struct BatchOut {
   double* tip = nullptr;
