@@ -3763,6 +3763,7 @@ int block_bnorm(Context* ctx, BlockSys* B, const double* b, bool b_per_r) {
 // in B->s (its, res, done, breakdown); returns the batch status.
 int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool warm, int max_it, double tol,
                 bool record_phases, int chunk_cap = 0) {
+  NvtxRange range("msg: batched solve");
   cudaStream_t st = B->X.st;
   Scal& s = B->s;
   const size_t nvec = B->nvec;
@@ -3786,6 +3787,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
   bool need_update = true, first = true;
   for (int guard = 0; guard < 1000000; ++guard) {
     if (need_update) {
+      NvtxRange upd("msg: FP64 true residual");
       cudaEventRecord(ev[0], st);
       MSG_TRY(block_update(ctx, B, c, b, b_per_r, tol, first, 0x7fffffff, B->gmg && first && !warm));
       cudaEventRecord(ev[1], st);
@@ -3802,6 +3804,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
       status = MSG_ERR_NOT_CONVERGED;
       break;
     }
+    NvtxRange chunk_range("msg: FP32 inner chunk");
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");

@@ -410,6 +410,7 @@ static int assemble_from_device_E(Context* ctx, Mesh* m, const double* d_E, doub
 static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, const double* d_xi, const double* d_b,
                     int mode, int max_it, double tol, int tip_dof, double* d_X, double* tip, int* iterations,
                     double* rel_res) {
+  NvtxRange range("msg: Monte Carlo batch");
   if (R <= 0 || !kl || !d_xi || !d_b || max_it <= 0 || !(tol > 0))
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "MC batch: invalid arguments");
   if (tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");

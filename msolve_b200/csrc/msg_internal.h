@@ -2,6 +2,7 @@
 // CUDA kernels (*.cu) of libmsolve_gpu.so.
 #pragma once
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -133,6 +134,14 @@ int cuda_error(Context* ctx, cudaError_t e, const char* where);
 // Kernels launched counter (the bench reports how many of this library's
 // kernels ran inside its timed region).
 inline void count_launch(Context* ctx, int n = 1) { ctx->launches += n; }
+
+// Host-side NVTX range (NVTX v3, header-only: a no-op unless a tool is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // 3x3-block sliced-ELL (SELL-32) pattern of the global stiffness over all
 // mesh nodes. Block row = node. Slices of 32 rows; slot s of slice z holds
