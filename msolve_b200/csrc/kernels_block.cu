@@ -933,6 +933,8 @@ template <int kMode> struct LvlStage {
   static constexpr size_t kSmem = 128 + sizeof(float) * ((size_t)kMStages * kFloats + 2 * (size_t)kMXFloats) +
                                   sizeof(double) * kMJ * kMK * 32 + sizeof(uint64_t) * (2 * kMStages);
 };
+static_assert(LvlStage<kLvlResid>::kOffB == kMPlaneFloats && LvlStage<kLvlSmooth>::kOffB == kMPlaneFloats,
+              "the second vector patch follows the first");
 static_assert(LvlStage<kLvlStart>::kBytes % 128 == 0 && LvlStage<kLvlResid>::kBytes % 128 == 0 &&
                   LvlStage<kLvlPcgZ>::kBytes % 128 == 0,
               "stage alignment");
