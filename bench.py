@@ -76,8 +76,8 @@ def parse():
                    help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
     p.add_argument("--serve-rates", default="100,400", help="Poisson arrival rates (requests/s) to run")
     p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
-    p.add_argument("--multigrid", type=int, default=None, choices=[0, 1],
-                   help="MSG_SET_OPTION multigrid (1: V-cycle preconditioned batched loop)")
+    p.add_argument("--multigrid", type=int, default=None, choices=[0, 1, 2],
+                   help="MSG_SET_OPTION multigrid (1: V-cycle for systems without a mass term, 2: for all)")
     p.add_argument("--mg-levels", type=int, default=None, help="MSG_SET_OPTION multigrid_levels")
     p.add_argument("--mg-sweeps", type=int, default=None, help="MSG_SET_OPTION multigrid_sweeps (coarsest level)")
     p.add_argument("--mg-delta", type=float, default=None, help="MSG_SET_OPTION multigrid_delta")
