@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--reliable-delta", type=float, default=None, help="MSG_SET_OPTION reliable_delta")
     p.add_argument("--chunk", type=int, default=None, help="MSG_SET_OPTION chunk")
     p.add_argument("--no-newmark", action="store_true", help="skip the batched Newmark measurement")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the library's default loop configuration instead of timing the candidates first")
+    p.add_argument("--autotune-cache", default=None, help="JSON cache of tuned configurations (read and written)")
     p.add_argument("--newmark-R", type=int, default=256)
     p.add_argument("--newmark-n", type=int, default=24)
     p.add_argument("--newmark-steps", type=int, default=200)
@@ -399,6 +402,19 @@ def main():
             import torch.distributed as dist
             dist.barrier()
 
+    # loop configuration (tile shapes, preconditioner) picked by the project's autotuner
+    # on this rank's own batch, unless an option was forced on the command line
+    tuned = None
+    forced = any(v is not None for v in (args.multigrid, args.mg_levels, args.chunk, args.modal_operator))
+    if not args.no_autotune and not forced:
+        from msolve_b200.tuning import Autotuner
+        tuner = Autotuner(ctx, args.autotune_cache)
+        opts = tuner.tune_mc(mesh, kl, xi_all[0].numpy(), tol=args.tol)
+        tuner.apply(opts)
+        rec = tuner.cache[tuner.last_key]
+        tuned = {"options": opts, "candidates": [{"options": c["options"], "seconds": round(c["seconds"], 4)}
+                                                 for c in rec["candidates"]]}
+
     for s in range(args.warmup):
         solve_device(s)
     barrier()
@@ -444,7 +460,7 @@ def main():
     # roofline of the dominant kernel, the fused direction + matrix-free FP32 operator
     # (live per-launch samples from the timed region): k_lvl_op<PcgZ> in the multigrid
     # loop, k_op_modal in the Jacobi loop
-    mg = args.multigrid != 0
+    mg = ctx.get_option("multigrid") != 0
     op_ms = st["op_launch_ms"]
     nn = model.n_nodes
     ne = model.n_elems
@@ -532,6 +548,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(R * K_terms * 8 + Nd * 8),
                     "d2h_bytes_per_step": int(R * Nd * 8 + R * (8 + 4 + 8))},
             "gpu_launches": int(launches),
+            "tuned": tuned,
             "roofline": {"kernel": op_kernel,
                          "bound": "hbm", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if hbm else None, "traffic": traffic,

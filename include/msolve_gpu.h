@@ -379,6 +379,9 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
+/* The current value of an MSG_SET_OPTION key (MSG_ERR_INVALID_ARGUMENT for an
+ * unknown key). */
+int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value);
 
 /* Kernel launch counter of this context (kernels launched since creation),
  * and device timings in ms (t8 may be NULL):

@@ -12,11 +12,12 @@ from .analyzers import (GaussianStochasticCoefficientsProvider, GpuMatrix, GpuMe
                         SolverPCGReorthogonalizationSearchVectorCalculator, SolverPCGReorthogonalized, ProblemStructural, SolverPCG,
                         StaticAnalyzer, h8_mass_batch, h8_stiffness_batch, h8_stress_batch, realization_stresses)
 from .polynomial_chaos import PolynomialChaosSolverPCGMatrixCalculator, pc_basis
+from .tuning import Autotuner
 from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, cantilever_model, clamped_block_model,
                     tip_dof)
 
 __all__ = [
-    "ArgumentError", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
+    "ArgumentError", "Autotuner", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
     "lib", "GaussianStochasticCoefficientsProvider", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
     "MonteCarloAnalyzer", "MonteCarloAnalyzerWithStochasticMaterial", "SolverPCGReorthogonalizationSearchVectorCalculator",
     "SolverPCGReorthogonalized", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",

@@ -117,6 +117,7 @@ SIGNATURES = {
     "MSG_STATS": (C.c_int, [_vp, _i64, _d]),
     "MSG_STATS_RESET": (C.c_int, [_vp]),
     "MSG_WAIT_SELFTEST": (C.c_int, [_vp, C.c_int64]),
+    "MSG_GET_OPTION": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_double)]),
 }
 
 _lib = None
@@ -206,6 +207,11 @@ class Context:
 
     def set_option(self, key, value):
         check(lib().MSG_SET_OPTION(self.handle, key.encode(), float(value)), self.handle, "MSG_SET_OPTION")
+
+    def get_option(self, key):
+        v = C.c_double(0.0)
+        check(lib().MSG_GET_OPTION(self.handle, key.encode(), C.byref(v)), self.handle, "MSG_GET_OPTION")
+        return v.value
 
     def stats(self):
         n = C.c_int64(0)

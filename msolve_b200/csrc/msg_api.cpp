@@ -581,6 +581,31 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 
+int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
+  CTX_GUARD(ctx);
+  if (!key || !value) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "null option key or value");
+  const struct {
+    const char* name;
+    double v;
+  } opts[] = {{"reliable_delta", ctx->reliable_delta},
+              {"chunk", (double)ctx->chunk},
+              {"modal_operator", (double)ctx->modal},
+              {"fixed_updates", (double)ctx->fixed_updates},
+              {"multigrid", (double)ctx->multigrid},
+              {"multigrid_levels", (double)ctx->mg_levels},
+              {"multigrid_sweeps", (double)ctx->mg_sweeps},
+              {"multigrid_omega", ctx->mg_omega},
+              {"multigrid_delta", ctx->mg_delta},
+              {"multigrid_packed", (double)ctx->mg_packed},
+              {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse}};
+  for (const auto& o : opts)
+    if (!std::strcmp(key, o.name)) {
+      *value = o.v;
+      return MSG_OK;
+    }
+  return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option: %s", key);
+}
+
 int MSG_STATS(MSG_CTX ctx, int64_t* launches, double* t8) {
   if (!ctx) return MSG_ERR_INVALID_ARGUMENT;
   if (launches) *launches = ctx->launches.load();
