@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--reliable-delta", type=float, default=None, help="MSG_SET_OPTION reliable_delta")
     p.add_argument("--chunk", type=int, default=None, help="MSG_SET_OPTION chunk")
     p.add_argument("--no-newmark", action="store_true", help="skip the batched Newmark measurement")
+    p.add_argument("--serve-persistent", type=int, default=None, choices=[0, 1],
+                   help="MSG_SET_OPTION serve_persistent (serving lanes on persistent grids)")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the library's default loop configuration instead of timing the candidates first")
     p.add_argument("--autotune-cache", default=None, help="JSON cache of tuned configurations (read and written)")
@@ -365,7 +367,8 @@ def main():
     if args.multigrid is not None:
         ctx.set_option("multigrid", args.multigrid)
     for key, val in (("multigrid_levels", args.mg_levels), ("multigrid_sweeps", args.mg_sweeps),
-                     ("multigrid_delta", args.mg_delta), ("multigrid_omega", args.mg_omega)):
+                     ("multigrid_delta", args.mg_delta), ("multigrid_omega", args.mg_omega),
+                     ("serve_persistent", args.serve_persistent)):
         if val is not None:
             ctx.set_option(key, val)
     model, kl = make_problem(args)

@@ -374,7 +374,11 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * realizations per thread with packed FP32 arithmetic; 0: one per thread),
  * "multigrid_fused_coarse" (1, default: every sweep of the coarsest level in
  * one launch when that level has at most 3 x 3 nodes across y and z; 0: one
- * launch per sweep; the results are identical).
+ * launch per sweep; the results are identical), "serve_persistent" (serving
+ * lanes created afterwards: 0, default, one CTA per work item of their level
+ * operators, on streams whose priority grows as the model shrinks, so short
+ * launches of small models run between the work items of large ones;
+ * 1: persistent grids of one CTA per SM).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

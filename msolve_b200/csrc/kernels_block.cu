@@ -2784,6 +2784,10 @@ struct BlockExec {
   cudaGraphExec_t* graph = nullptr;
   size_t* graph_key = nullptr;
   bool ctx_stats = true;          // accumulate the context's phase timings and launch samples
+  // persistent grids (one CTA per SM walking the work items) or one CTA per
+  // item, which lets the block scheduler interleave other streams' kernels
+  // (higher-priority serving lanes) between items
+  bool persistent = true;
 };
 
 // Everything one batch of solves on a structured lattice shares: sizes,
@@ -3001,7 +3005,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   B->tiles_jm = (L.NY + kMJ - 1) / kMJ;
   B->n_tiles_m = B->tiles_jm * ((L.NZ + kMK - 1) / kMK);
   B->n_items_m = B->n_tiles_m * (Rp / 32);
-  B->grid_m = std::min(B->n_items_m, ctx->sm_count);
+  B->grid_m = B->X.persistent ? std::min(B->n_items_m, ctx->sm_count) : B->n_items_m;
   B->n_upd = std::min(L.n_int, ctx->sm_count * 4);
   B->n_bsq = std::min(L.n_int, ctx->sm_count * 2);
 
@@ -3122,7 +3126,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
       B->tiles_jr = (L.NY + kRJ - 1) / kRJ;
       B->n_tiles_r = B->tiles_jr * ((L.NZ + kRK - 1) / kRK);
       B->n_items_r = B->n_tiles_r * (Rp / 32);
-      B->grid_r = std::min(B->n_items_r, ctx->sm_count);
+      B->grid_r = B->X.persistent ? std::min(B->n_items_r, ctx->sm_count) : B->n_items_r;
     }
     static std::once_flag resid_once;
     static cudaError_t resid_err = cudaSuccess;
@@ -3205,7 +3209,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
         g.tiles_j = (Lc.NY + kMJ - 1) / kMJ;
         g.n_tiles = g.tiles_j * ((Lc.NZ + kMK - 1) / kMK);
         g.n_items = g.n_tiles * (Rp / 32);
-        g.grid = std::min(g.n_items, ctx->sm_count);
+        g.grid = B->X.persistent ? std::min(g.n_items, ctx->sm_count) : g.n_items;
         const size_t nv = (size_t)Lc.n_pad * 3 * Rp, ns = (size_t)Lc.n_pad * Rp;
         off[l][0] = take(sizeof(float) * nv);
         off[l][1] = take(sizeof(float) * nv);
@@ -3271,7 +3275,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
         B->tiles_j2 = (L.NY + kQJ - 1) / kQJ;
         B->n_tiles2 = B->tiles_j2 * ((L.NZ + kQK - 1) / kQK);
         B->n_items2 = B->n_tiles2 * (Rp / kQR);
-        B->grid2 = std::min(B->n_items2, ctx->sm_count);
+        B->grid2 = B->X.persistent ? std::min(B->n_items2, ctx->sm_count) : B->n_items2;
         // the loop's partials: [tile][Rp][2] and [tile][Rp] over the packed tiles
         const size_t need = sizeof(double) * (size_t)std::max({B->n_tiles * 2, B->n_tiles_m * kMParts,
                                                                 B->n_tiles2 * 3}) * Rp;
@@ -3299,7 +3303,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
           g.tiles_j2 = (Lc.NY + kQJ - 1) / kQJ;
           g.n_tiles2 = g.tiles_j2 * ((Lc.NZ + kQK - 1) / kQK);
           g.n_items2 = g.n_tiles2 * (Rp / kQR);
-          g.grid2 = std::min(g.n_items2, ctx->sm_count);
+          g.grid2 = B->X.persistent ? std::min(g.n_items2, ctx->sm_count) : g.n_items2;
           const cuuint64_t cpd[5] = {(cuuint64_t)Rp, 3, (cuuint64_t)Lc.NXp, (cuuint64_t)Lc.NYp, (cuuint64_t)Lc.NZp};
           const cuuint64_t cps[4] = {Rp * fb, 3 * Rp * fb, 3 * Rp * fb * Lc.NXp, 3 * Rp * fb * Lc.NXp * Lc.NYp};
           const cuuint64_t ced[4] = {(cuuint64_t)Rp, (cuuint64_t)Lc.NXp, (cuuint64_t)Lc.NYp, (cuuint64_t)Lc.NZp};
@@ -4163,7 +4167,14 @@ int lane_create(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, const double
   L->max_it = max_it;
   L->n_terms = kl->n_terms;
   MSG_CUDA(ctx, cudaSetDevice(ctx->device));
-  MSG_CUDA(ctx, cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking));
+  // smaller models get higher stream priority: their short launches are
+  // scheduled between the work items of larger models' launches
+  int prio_least = 0, prio_greatest = 0;
+  MSG_CUDA(ctx, cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+  const double lg = std::log2((double)std::max(1, m->n_nodes));
+  const double f = std::min(1.0, std::max(0.0, (lg - std::log2(729.0)) / (std::log2(117649.0) - std::log2(729.0))));
+  const int prio = prio_greatest + (int)std::lround(f * (prio_least - prio_greatest));
+  MSG_CUDA(ctx, cudaStreamCreateWithPriority(&L->st, cudaStreamNonBlocking, prio));
   for (auto& e : L->ev) MSG_CUDA(ctx, cudaEventCreate(&e));
   MSG_CUDA(ctx, cudaMallocHost(&L->h_flags, 64));
   MSG_CUDA(ctx, cudaMallocHost(&L->h_state, sizeof(int) * 5 * Rp));
@@ -4179,6 +4190,7 @@ int lane_create(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, const double
   X.graph = &L->graph;
   X.graph_key = &L->graph_key;
   X.ctx_stats = false;
+  X.persistent = ctx->serve_persistent != 0;
   MSG_TRY(block_setup(ctx, m, nu, 1.0, 1.0, 0.0, Rp, Rp, &L->B, L->own, &X));
   L->B.fixed = true;
   // KL table -> psi (own copy: the context's KL workspace is reused by other calls)
