@@ -68,6 +68,8 @@ def parse():
     p.add_argument("--no-newmark", action="store_true", help="skip the batched Newmark measurement")
     p.add_argument("--serve-persistent", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION serve_persistent (serving lanes on persistent grids)")
+    p.add_argument("--serve-priority", type=int, default=None, choices=[0, 1],
+                   help="MSG_SET_OPTION serve_priority (stream priority by model size)")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the library's default loop configuration instead of timing the candidates first")
     p.add_argument("--autotune-cache", default=None, help="JSON cache of tuned configurations (read and written)")
@@ -368,7 +370,7 @@ def main():
         ctx.set_option("multigrid", args.multigrid)
     for key, val in (("multigrid_levels", args.mg_levels), ("multigrid_sweeps", args.mg_sweeps),
                      ("multigrid_delta", args.mg_delta), ("multigrid_omega", args.mg_omega),
-                     ("serve_persistent", args.serve_persistent)):
+                     ("serve_persistent", args.serve_persistent), ("serve_priority", args.serve_priority)):
         if val is not None:
             ctx.set_option(key, val)
     model, kl = make_problem(args)

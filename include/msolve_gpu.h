@@ -375,10 +375,12 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * "multigrid_fused_coarse" (1, default: every sweep of the coarsest level in
  * one launch when that level has at most 3 x 3 nodes across y and z; 0: one
  * launch per sweep; the results are identical), "serve_persistent" (serving
- * lanes created afterwards: 0, default, one CTA per work item of their level
- * operators, on streams whose priority grows as the model shrinks, so short
- * launches of small models run between the work items of large ones;
- * 1: persistent grids of one CTA per SM).
+ * lanes created afterwards: 1, default, persistent grids of one CTA per SM;
+ * 0: one CTA per work item of their level operators, so other lanes' launches
+ * can run between the work items), "serve_priority" (serving lanes created
+ * afterwards: 0, default, equal stream priorities; 1: priority grows as the
+ * model shrinks, shortest solves first: with serve_persistent = 0 small
+ * models' latency under load halves while the largest models wait longer).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

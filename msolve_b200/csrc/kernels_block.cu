@@ -4173,7 +4173,8 @@ int lane_create(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, const double
   MSG_CUDA(ctx, cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
   const double lg = std::log2((double)std::max(1, m->n_nodes));
   const double f = std::min(1.0, std::max(0.0, (lg - std::log2(729.0)) / (std::log2(117649.0) - std::log2(729.0))));
-  const int prio = prio_greatest + (int)std::lround(f * (prio_least - prio_greatest));
+  const int prio = ctx->serve_priority ? prio_greatest + (int)std::lround(f * (prio_least - prio_greatest))
+                                       : prio_least;
   MSG_CUDA(ctx, cudaStreamCreateWithPriority(&L->st, cudaStreamNonBlocking, prio));
   for (auto& e : L->ev) MSG_CUDA(ctx, cudaEventCreate(&e));
   MSG_CUDA(ctx, cudaMallocHost(&L->h_flags, 64));

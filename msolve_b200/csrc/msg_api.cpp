@@ -582,6 +582,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
     ctx->serve_persistent = (int)value;
     return MSG_OK;
   }
+  if (!std::strcmp(key, "serve_priority") && (value == 0 || value == 1)) {
+    ctx->serve_priority = (int)value;
+    return MSG_OK;
+  }
   return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown option or value out of range: %s", key);
 }
 
@@ -602,7 +606,8 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"multigrid_delta", ctx->mg_delta},
               {"multigrid_packed", (double)ctx->mg_packed},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
-              {"serve_persistent", (double)ctx->serve_persistent}};
+              {"serve_persistent", (double)ctx->serve_persistent},
+              {"serve_priority", (double)ctx->serve_priority}};
   for (const auto& o : opts)
     if (!std::strcmp(key, o.name)) {
       *value = o.v;
