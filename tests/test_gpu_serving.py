@@ -130,3 +130,29 @@ def test_poll_without_wait_and_unknown_request(server):
         out = server.poll(rq, timeout_ms=50)
     with pytest.raises(N.ArgumentError):
         server.poll(rq, timeout_ms=0)  # forgotten after the successful poll
+
+
+def test_scheduling_options_do_not_change_results(ctx):
+    """One CTA per work item and shortest-first stream priorities change only
+    when work runs, not what it computes: two models served side by side give
+    the same bits under every scheduling option."""
+    models = [_problem(n) for n in (6, 10)]
+    rng = np.random.default_rng(21)
+    xis = rng.standard_normal((2, 6, 12))
+    results = []
+    for persistent, priority in ((1, 0), (0, 0), (0, 1)):
+        ctx.set_option("serve_persistent", persistent)
+        ctx.set_option("serve_priority", priority)
+        srv = Server(ctx, max_batch=32)
+        try:
+            ms = [srv.add_model(model, kl, tol=1e-10) for model, kl in models]
+            reqs = [[srv.submit(m, xi) for xi in xis[i]] for i, m in enumerate(ms)]
+            results.append([[srv.poll(rq, timeout_ms=-1)["X"] for rq in rs] for rs in reqs])
+        finally:
+            srv.stop()
+            ctx.set_option("serve_persistent", 1)
+            ctx.set_option("serve_priority", 0)
+    for other in results[1:]:
+        for a_model, b_model in zip(results[0], other):
+            for a, b in zip(a_model, b_model):
+                assert np.array_equal(a, b)
