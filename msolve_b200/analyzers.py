@@ -407,12 +407,16 @@ class MonteCarloAnalyzerWithStochasticMaterial:
     resumes by realization index: after every batch it saves the finished mask
     with the tip values, iterations and residuals next to a fingerprint of the
     realization table; a later Solve() with the same table solves only the
-    realizations not yet finished (their Solutions rows stay NaN)."""
+    realizations not yet finished (their Solutions rows stay NaN). With
+    `autotune` (True or a tuning.Autotuner, which may carry a JSON cache) the
+    mixed mode first picks the loop configuration on the first batch and uses
+    it for this Solve() (TunedOptions; the context's options are restored
+    afterwards)."""
 
     def __init__(self, ctx, model, coefficients_provider, expansion_order=50, simulations=1, seed=12345,
                  mode="mixed", max_iterations=20000, tolerance=1e-8, keep_solutions=True, tip_dof=None,
                  randoms_read_file_name="", simulation_start_from=0, random_file_simulations=50000,
-                 file_name_for_logging=None, batch_size=None, checkpoint=None):
+                 file_name_for_logging=None, batch_size=None, checkpoint=None, autotune=None):
         self.ctx, self.model, self.kl = ctx, model, coefficients_provider
         self.expansion_order, self.simulations, self.seed = expansion_order, simulations, seed
         self.mode = N.MSG_MODE_MIXED_BATCHED if mode == "mixed" else N.MSG_MODE_FP64_BSR
@@ -427,6 +431,8 @@ class MonteCarloAnalyzerWithStochasticMaterial:
         self.file_name_for_logging = file_name_for_logging
         self.batch_size = batch_size
         self.checkpoint = checkpoint
+        self.autotune = autotune
+        self.TunedOptions = None
         self._mesh = None
         self.RandomNumbers = None
 
@@ -508,6 +514,28 @@ class MonteCarloAnalyzerWithStochasticMaterial:
                 open(name, "w").close()
         todo = np.flatnonzero(~state["done"])
         batch = int(self.batch_size or R)
+        restore = None
+        if self.autotune and self.mode == N.MSG_MODE_MIXED_BATCHED and len(todo):
+            from .tuning import Autotuner
+            tuner = self.autotune if isinstance(self.autotune, Autotuner) else Autotuner(self.ctx)
+            self.TunedOptions = tuner.tune_mc(self.mesh, self.kl, xi[todo[:batch]], tol=self.tolerance,
+                                              max_iterations=self.max_iterations)
+            restore = {k: self.ctx.get_option(k) for k in self.TunedOptions}
+            tuner.apply(self.TunedOptions)
+        try:
+            status = self._solve_todo(xi, todo, batch, state, X)
+        finally:
+            if restore:
+                for k, v in restore.items():
+                    self.ctx.set_option(k, v)
+        self.Solutions, self.TipValues = X, state["tip"]
+        self.Iterations, self.Residuals = state["its"], state["res"]
+        if status != N.MSG_OK:
+            N.check(status, self.ctx.handle if self.ctx is not None else None, "MSG_MC_SOLVE_BATCH")
+        return self.TipValues
+
+    def _solve_todo(self, xi, todo, batch, state, X):
+        logging = self.file_name_for_logging is not None
         status = N.MSG_OK
         t_all = time.perf_counter()
         t_solve = 0.0
@@ -534,11 +562,7 @@ class MonteCarloAnalyzerWithStochasticMaterial:
                             f"Total iterations: {int(state['its'][state['done']].sum())}\n")
             if self.checkpoint:
                 self._save_checkpoint(state)
-        self.Solutions, self.TipValues = X, state["tip"]
-        self.Iterations, self.Residuals = state["its"], state["res"]
-        if status != N.MSG_OK:
-            N.check(status, self.ctx.handle if self.ctx is not None else None, "MSG_MC_SOLVE_BATCH")
-        return self.TipValues
+        return status
 
     def statistics(self):
         t = self.TipValues

@@ -33,3 +33,23 @@ def test_tune_mc_small_batch(ctx, tmp_path):
     finally:
         for k, v in before.items():
             ctx.set_option(k, v)
+
+
+def test_analyzer_autotune(ctx):
+    n, R = 8, 40
+    model = M.clamped_block_model(n)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, 12, 6)
+    xi = np.random.default_rng(8).standard_normal((R, 12))
+    before = {k: ctx.get_option(k) for k in TUNABLE}
+    ref = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=12, simulations=R,
+                                                     tolerance=1e-10)
+    ref.RandomNumbers = xi
+    ref.Solve()
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=12, simulations=R,
+                                                    tolerance=1e-10, autotune=True)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    assert mc.TunedOptions in static_candidates()
+    assert {k: ctx.get_option(k) for k in TUNABLE} == before
+    assert (mc.Residuals < 1e-10).all()
+    assert np.abs(mc.Solutions - ref.Solutions).max() <= 1e-8 * np.abs(ref.Solutions).max()
