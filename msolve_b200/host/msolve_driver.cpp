@@ -1,0 +1,147 @@
+// Replays the reference's analyzer call sequences through the C++ host mirror
+// (msolve.hpp) against the C ABI, and writes the results as raw little-endian
+// binary for the tests:
+//
+//   model   cantilever|block N OUT       n_dofs (int32), DOF map [n_nodes][3] (int32), forces [n_dofs] (f64)
+//   static  cantilever|block N OUT [mixed]
+//           StaticAnalyzer(ProblemStructural, LinearAnalyzer(SolverPCG)):
+//           BuildMatrices, Initialize, Solve(1e-10) -> iterations (int32),
+//           relative residual (f64), solution [n_dofs] (f64)
+//   mc      N R TERMS XI OUT [fp64]      MonteCarloAnalyzerWithStochasticMaterial on the N^3 clamped
+//           block with xi [R][TERMS] read from XI (f64): tip [R], residuals [R] (f64),
+//           iterations [R] (int32), solutions [R][n_dofs] (f64)
+//   newmark N R TERMS XI STEPS OUT       NewmarkDynamicAnalyzer (beta 0.25, gamma 0.5, dt 0.01,
+//           Rayleigh 0.01 / 0.001, ground acceleration 0.1 sin(2 pi t) in x):
+//           tip history [R][STEPS] (f64), final displacements [R][n_dofs] (f64)
+//   guard                                 the Newmark coefficient guards (alpha too small)
+//
+// The KL provider of mc / newmark is the separable exponential kernel with
+// correlation length 0.2 N and 6 one-dimensional modes per axis, mean 1,
+// sigma 0.3. Exit codes: 0 ok, 2 usage, 3 InvalidOperationException,
+// 4 ArgumentException, 5 other status codes, 6 I/O.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "msolve.hpp"
+
+namespace {
+
+bool write_all(FILE* f, const void* p, size_t bytes) { return bytes == 0 || std::fwrite(p, 1, bytes, f) == bytes; }
+
+template <class T> bool put(FILE* f, const std::vector<T>& v) { return write_all(f, v.data(), sizeof(T) * v.size()); }
+
+msolve::Model make_model(const std::string& kind, int n) {
+  if (kind == "cantilever") return msolve::Hexa8MeshGenerator::Cantilever();
+  return msolve::Hexa8MeshGenerator::ClampedBlock(n);
+}
+
+std::vector<double> read_doubles(const char* path, size_t count) {
+  std::vector<double> v(count);
+  FILE* f = std::fopen(path, "rb");
+  if (!f || std::fread(v.data(), sizeof(double), count, f) != count) {
+    if (f) std::fclose(f);
+    throw std::runtime_error(std::string("cannot read ") + path);
+  }
+  std::fclose(f);
+  return v;
+}
+
+int run(int argc, char** argv) {
+  if (argc < 2) return 2;
+  const std::string cmd = argv[1];
+  if (cmd == "model" && argc >= 5) {
+    msolve::Model m = make_model(argv[2], std::atoi(argv[3]));
+    FILE* f = std::fopen(argv[4], "wb");
+    if (!f) return 6;
+    const int32_t nd = m.n_dofs;
+    const bool ok = write_all(f, &nd, sizeof(nd)) && put(f, m.dof) && put(f, m.subdomain.Forces);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "static" && argc >= 5) {
+    msolve::Model m = make_model(argv[2], std::atoi(argv[3]));
+    const bool mixed = argc >= 6 && std::string(argv[5]) == "mixed";
+    msolve::Context ctx(0);
+    msolve::ProblemStructural provider(ctx, m);
+    msolve::SolverPCG solver(ctx, m, 20000, 1e-10, mixed);
+    msolve::LinearAnalyzer child(solver);
+    msolve::StaticAnalyzer parent(provider, child);
+    parent.BuildMatrices();
+    parent.Initialize();
+    parent.Solve();
+    FILE* f = std::fopen(argv[4], "wb");
+    if (!f) return 6;
+    const int32_t it = solver.Iterations;
+    const double rr = solver.RelativeResidual;
+    const bool ok = write_all(f, &it, sizeof(it)) && write_all(f, &rr, sizeof(rr)) && put(f, m.subdomain.Solution);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "mc" && argc >= 7) {
+    const int n = std::atoi(argv[2]), R = std::atoi(argv[3]), terms = std::atoi(argv[4]);
+    const bool fp64 = argc >= 8 && std::string(argv[7]) == "fp64";
+    msolve::Model m = msolve::Hexa8MeshGenerator::ClampedBlock(n);
+    msolve::Context ctx(0);
+    msolve::LognormalStochasticCoefficientsProvider kl({(double)n, (double)n, (double)n}, 0.2 * n, terms, 6);
+    msolve::MonteCarloAnalyzerWithStochasticMaterial mc(ctx, m, kl, terms, R, !fp64, 1e-10);
+    mc.RandomNumbers = read_doubles(argv[5], (size_t)R * terms);
+    mc.Solve();
+    FILE* f = std::fopen(argv[6], "wb");
+    if (!f) return 6;
+    const bool ok = put(f, mc.TipValues) && put(f, mc.Residuals) && put(f, mc.Iterations) && put(f, mc.Solutions);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "newmark" && argc >= 8) {
+    const int n = std::atoi(argv[2]), R = std::atoi(argv[3]), terms = std::atoi(argv[4]), steps = std::atoi(argv[6]);
+    msolve::Model m = msolve::Hexa8MeshGenerator::ClampedBlock(n);
+    msolve::Context ctx(0);
+    msolve::LognormalStochasticCoefficientsProvider kl({(double)n, (double)n, (double)n}, 0.2 * n, terms, 6);
+    const double dt = 0.01;
+    msolve::MassAccelerationSinusoidalLoad load{1.0, dt, dt * steps, 0.1, msolve::DOFType::X};
+    msolve::NewmarkDynamicAnalyzer nm(ctx, m, kl, 0.25, 0.5, dt, dt * steps, load, R, 1.0, 0.01, 0.001, 1e-10);
+    nm.RandomNumbers = read_doubles(argv[5], (size_t)R * terms);
+    nm.BuildMatrices();
+    nm.Solve();
+    FILE* f = std::fopen(argv[7], "wb");
+    if (!f) return 6;
+    const bool ok = put(f, nm.TipHistory) && put(f, nm.Solutions);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "guard") {
+    msolve::Model m = msolve::Hexa8MeshGenerator::ClampedBlock(2);
+    msolve::Context ctx(0);
+    msolve::LognormalStochasticCoefficientsProvider kl({2.0, 2.0, 2.0}, 0.4, 4, 4);
+    msolve::MassAccelerationSinusoidalLoad load{1.0, 0.01, 0.1, 0.1, msolve::DOFType::X};
+    msolve::NewmarkDynamicAnalyzer nm(ctx, m, kl, 0.1, 0.5, 0.01, 0.1, load, 1);
+    nm.BuildMatrices();  // alpha 0.1 < 0.25: InvalidOperationException
+    return 0;
+  }
+  return 2;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  try {
+    const int rc = run(argc, argv);
+    if (rc == 2) std::fprintf(stderr, "usage: see the header of msolve_driver.cpp\n");
+    return rc;
+  } catch (const msolve::InvalidOperationException& e) {
+    std::fprintf(stderr, "InvalidOperationException: %s\n", e.what());
+    return 3;
+  } catch (const msolve::ArgumentException& e) {
+    std::fprintf(stderr, "ArgumentException: %s\n", e.what());
+    return 4;
+  } catch (const msolve::MSolveException& e) {
+    std::fprintf(stderr, "MSolveException: %s\n", e.what());
+    return 5;
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "error: %s\n", e.what());
+    return 6;
+  }
+}
