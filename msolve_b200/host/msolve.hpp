@@ -561,4 +561,63 @@ class NewmarkDynamicAnalyzer : public IAnalyzer {
   int MaxIterations;
 };
 
+// Continuous-batching service of independent realizations (MSG_SERVE_*; no
+// counterpart in the reference, whose realization loop is sequential). Models
+// are registered once; each request is one realization (its xi row), queued,
+// run in a free slot of its model's batch and polled for its displacements.
+class Server {
+ public:
+  struct Result {
+    int Status = MSG_PENDING;
+    std::vector<double> X;
+    int Iterations = 0;
+    double RelativeResidual = 0.0, LatencyMs = 0.0;
+  };
+  Server(Context& ctx, int max_batch = 64) : ctx_(ctx) {
+    Check(MSG_SERVE_START(ctx.Handle(), max_batch), ctx.Handle(), "MSG_SERVE_START");
+  }
+  ~Server() { MSG_SERVE_STOP(ctx_.Handle()); }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+  // the model's mesh stays alive with the server
+  int AddModel(Model& model, LognormalStochasticCoefficientsProvider& provider, double tolerance = 1e-8,
+               int max_iterations = 20000) {
+    meshes_.emplace_back(new GpuMesh(ctx_, model));
+    int id = -1;
+    Check(MSG_SERVE_ADD_MODEL(ctx_.Handle(), meshes_.back()->Handle(), model.Poisson, provider.Kl(),
+                              model.subdomain.Forces.data(), tolerance, max_iterations, &id),
+          ctx_.Handle(), "MSG_SERVE_ADD_MODEL");
+    dofs_.push_back(model.n_dofs);
+    return id;
+  }
+  MSG_REQ Submit(int model_id, const std::vector<double>& xi) {
+    MSG_REQ id = 0;
+    Check(MSG_SERVE_SUBMIT(ctx_.Handle(), model_id, xi.data(), &id), ctx_.Handle(), "MSG_SERVE_SUBMIT");
+    requests_.push_back({id, model_id});
+    return id;
+  }
+  // timeout_ms < 0 waits until the request is done; a finished request that
+  // did not converge or was cancelled throws as the other calls do
+  Result Poll(MSG_REQ id, int timeout_ms = -1) {
+    Result r;
+    r.X.assign(dofs_.at(ModelOf(id)), 0.0);
+    r.Status = MSG_SERVE_POLL(ctx_.Handle(), id, timeout_ms, r.X.data(), &r.Iterations, &r.RelativeResidual,
+                              &r.LatencyMs);
+    if (r.Status != MSG_PENDING) Check(r.Status, ctx_.Handle(), "MSG_SERVE_POLL");
+    return r;
+  }
+  void Cancel(MSG_REQ id) { Check(MSG_SERVE_CANCEL(ctx_.Handle(), id), ctx_.Handle(), "MSG_SERVE_CANCEL"); }
+
+ private:
+  int ModelOf(MSG_REQ id) const {
+    for (const auto& q : requests_)
+      if (q.first == id) return q.second;
+    throw ArgumentException(MSG_ERR_INVALID_ARGUMENT, "unknown request");
+  }
+  Context& ctx_;
+  std::vector<std::unique_ptr<GpuMesh>> meshes_;
+  std::vector<int> dofs_;
+  std::vector<std::pair<MSG_REQ, int>> requests_;
+};
+
 }  // namespace msolve

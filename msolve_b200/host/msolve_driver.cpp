@@ -13,6 +13,10 @@
 //   newmark N R TERMS XI STEPS OUT       NewmarkDynamicAnalyzer (beta 0.25, gamma 0.5, dt 0.01,
 //           Rayleigh 0.01 / 0.001, ground acceleration 0.1 sin(2 pi t) in x):
 //           tip history [R][STEPS] (f64), final displacements [R][n_dofs] (f64)
+//   serve   N1 N2 R TERMS XI OUT          Server with two models (N1^3 and N2^3 clamped blocks, tol
+//           1e-10): R requests to each, xi rows [2][R][TERMS] from XI, all submitted before
+//           the first poll -> for every request in submission order: iterations (int32),
+//           relative residual (f64), displacements [n_dofs] (f64)
 //   guard                                 the Newmark coefficient guards (alpha too small)
 //
 // The KL provider of mc / newmark is the separable exponential kernel with
@@ -109,6 +113,33 @@ int run(int argc, char** argv) {
     FILE* f = std::fopen(argv[7], "wb");
     if (!f) return 6;
     const bool ok = put(f, nm.TipHistory) && put(f, nm.Solutions);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "serve" && argc >= 8) {
+    const int n1 = std::atoi(argv[2]), n2 = std::atoi(argv[3]), R = std::atoi(argv[4]), terms = std::atoi(argv[5]);
+    msolve::Model m1 = msolve::Hexa8MeshGenerator::ClampedBlock(n1);
+    msolve::Model m2 = msolve::Hexa8MeshGenerator::ClampedBlock(n2);
+    msolve::Context ctx(0);
+    msolve::LognormalStochasticCoefficientsProvider kl1({(double)n1, (double)n1, (double)n1}, 0.2 * n1, terms, 6);
+    msolve::LognormalStochasticCoefficientsProvider kl2({(double)n2, (double)n2, (double)n2}, 0.2 * n2, terms, 6);
+    const std::vector<double> xi = read_doubles(argv[6], (size_t)2 * R * terms);
+    msolve::Server srv(ctx, 32);
+    const int id[2] = {srv.AddModel(m1, kl1, 1e-10), srv.AddModel(m2, kl2, 1e-10)};
+    std::vector<MSG_REQ> reqs;
+    for (int k = 0; k < 2; ++k)
+      for (int r = 0; r < R; ++r)
+        reqs.push_back(srv.Submit(id[k], std::vector<double>(xi.begin() + ((size_t)k * R + r) * terms,
+                                                             xi.begin() + ((size_t)k * R + r + 1) * terms)));
+    FILE* f = std::fopen(argv[7], "wb");
+    if (!f) return 6;
+    bool ok = true;
+    for (MSG_REQ q : reqs) {
+      const msolve::Server::Result res = srv.Poll(q, -1);
+      const int32_t it = res.Iterations;
+      ok = ok && write_all(f, &it, sizeof(it)) && write_all(f, &res.RelativeResidual, sizeof(double)) &&
+           put(f, res.X);
+    }
     std::fclose(f);
     return ok ? 0 : 6;
   }

@@ -129,3 +129,36 @@ def test_newmark_matches_python_mirror(ctx, driver, tmp_path):
 def test_newmark_guard_raises_invalid_operation(driver):
     rc, err = run(driver, "guard")
     assert rc == 3 and "Newmark alpha has to be bigger than 0.25" in err, err
+
+
+@pytest.mark.gpu
+def test_server_matches_python_mirror(ctx, driver, tmp_path):
+    """Two models served side by side through the C++ Server: every request
+    returns the bits the Python server returns for the same realization (a
+    request's arithmetic does not depend on the mix)."""
+    from msolve_b200.serving import Server
+    n1, n2, R, terms = 6, 10, 5, 12
+    xi = np.random.default_rng(29).standard_normal((2, R, terms))
+    xi_path = tmp_path / "xi.bin"
+    xi_path.write_bytes(xi.tobytes())
+    out = tmp_path / "serve.bin"
+    rc, err = run(driver, "serve", n1, n2, R, terms, xi_path, out)
+    assert rc == 0, err
+    raw = out.read_bytes()
+    srv = Server(ctx, max_batch=32)
+    try:
+        off = 0
+        for k, n in enumerate((n1, n2)):
+            model = M.clamped_block_model(n)
+            kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, terms, 6)
+            m = srv.add_model(model, kl, tol=1e-10)
+            for r in range(R):
+                its = int(np.frombuffer(raw[off:off + 4], dtype=np.int32)[0])
+                res = float(np.frombuffer(raw[off + 4:off + 12], dtype=np.float64)[0])
+                X = np.frombuffer(raw[off + 12:off + 12 + 8 * model.n_dofs], dtype=np.float64)
+                off += 12 + 8 * model.n_dofs
+                py = srv.poll(srv.submit(m, xi[k, r]), timeout_ms=-1)
+                assert its == py["iterations"] and res == py["rel_res"] and np.array_equal(X, py["X"])
+        assert off == len(raw)
+    finally:
+        srv.stop()
