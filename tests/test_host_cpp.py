@@ -3,7 +3,7 @@ replays the reference's analyzer call sequences against the C ABI. On the CPU:
 the header compiles warning-free and its model (generator order, DOF
 numbering, assigned loads) equals the Python mirror's exactly. On the GPU:
 the StaticAnalyzer -> LinearAnalyzer -> SolverPCG chain, the Monte Carlo
-analyzer and the Newmark analyzer return the same bits as the Python mirror
+analyzer, the Newmark analyzer and the serving loop return the same bits as the Python mirror
 (same ABI calls on the same inputs), the static solve matches the oracle's
 skyline LDL^T to 1e-8, and the Newmark guard raises InvalidOperationException."""
 import os
