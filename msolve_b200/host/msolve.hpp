@@ -419,6 +419,10 @@ class LognormalStochasticCoefficientsProvider {
   LognormalStochasticCoefficientsProvider& operator=(const LognormalStochasticCoefficientsProvider&) = delete;
   const MSG_KL* Kl() const { return &kl_; }
   int Terms() const { return kl_.n_terms; }
+  const std::vector<double>& W() const { return w_; }
+  const std::vector<double>& Amp() const { return amp_; }
+  const std::vector<int>& Idx() const { return idx_; }
+  const std::vector<double>& Eig() const { return eig_; }
 
  private:
   std::array<double, 3> domain_;

@@ -17,6 +17,10 @@
 //           1e-10): R requests to each, xi rows [2][R][TERMS] from XI, all submitted before
 //           the first poll -> for every request in submission order: iterations (int32),
 //           relative residual (f64), displacements [n_dofs] (f64)
+//   kl      N TERMS OUT                  the KL table of the N^3 block's provider: w [TERMS][3],
+//           amp [TERMS][3] (f64), idx [TERMS][3] (int32), eig [TERMS] (f64) (host only)
+//   errors                               the exception type each status code maps to, one per line
+//           (host only)
 //   guard                                 the Newmark coefficient guards (alpha too small)
 //
 // The KL provider of mc / newmark is the separable exponential kernel with
@@ -142,6 +146,33 @@ int run(int argc, char** argv) {
     }
     std::fclose(f);
     return ok ? 0 : 6;
+  }
+  if (cmd == "kl" && argc >= 5) {
+    const int n = std::atoi(argv[2]), terms = std::atoi(argv[3]);
+    msolve::LognormalStochasticCoefficientsProvider kl({(double)n, (double)n, (double)n}, 0.2 * n, terms, 6);
+    FILE* f = std::fopen(argv[4], "wb");
+    if (!f) return 6;
+    const bool ok = put(f, kl.W()) && put(f, kl.Amp()) && put(f, kl.Idx()) && put(f, kl.Eig());
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "errors") {
+    const int codes[] = {MSG_ERR_NOT_CONVERGED, MSG_ERR_BREAKDOWN, MSG_ERR_NEG_DET, MSG_ERR_NOT_STRUCTURED,
+                         MSG_ERR_INVALID_ARGUMENT, MSG_ERR_OUT_OF_MEMORY, MSG_ERR_TIMEOUT, MSG_ERR_CUDA};
+    for (int c : codes) {
+      const char* kind = "none";
+      try {
+        msolve::Check(c, nullptr, "status");
+      } catch (const msolve::InvalidOperationException&) {
+        kind = "InvalidOperationException";
+      } catch (const msolve::ArgumentException&) {
+        kind = "ArgumentException";
+      } catch (const msolve::MSolveException& e) {
+        kind = e.Code == c ? "MSolveException" : "wrong-code";
+      }
+      std::printf("%d %s\n", c, kind);
+    }
+    return 0;
   }
   if (cmd == "guard") {
     msolve::Model m = msolve::Hexa8MeshGenerator::ClampedBlock(2);

@@ -162,3 +162,28 @@ def test_server_matches_python_mirror(ctx, driver, tmp_path):
         assert off == len(raw)
     finally:
         srv.stop()
+
+
+def test_status_codes_map_to_reference_exceptions(driver):
+    r = subprocess.run([driver, "errors"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    kinds = dict(line.split() for line in r.stdout.splitlines())
+    inv, arg, other = "InvalidOperationException", "ArgumentException", "MSolveException"
+    assert kinds == {"-2001": inv, "-2002": inv, "-1001": inv, "-2007": inv, "-2005": arg, "-100": other,
+                     "-2003": other, "-2006": other}
+
+
+def test_kl_table_matches_python_provider(driver, tmp_path):
+    n, terms = 8, 20
+    out = tmp_path / "kl.bin"
+    rc, err = run(driver, "kl", n, terms, out)
+    assert rc == 0, err
+    raw = out.read_bytes()
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, terms, 6)
+    o = 0
+    for arr, dt in ((kl.w, np.float64), (kl.amp, np.float64), (kl.idx, np.int32), (kl.eig, np.float64)):
+        nb = arr.size * np.dtype(dt).itemsize
+        got = np.frombuffer(raw[o:o + nb], dtype=dt).reshape(arr.shape)
+        assert np.array_equal(got, arr)
+        o += nb
+    assert o == len(raw)
