@@ -347,7 +347,7 @@ class SolverPCG : public ISolver {
   int Iterations = 0;
   double RelativeResidual = 0.0;
 
- private:
+ protected:
   Context& ctx_;
   Model& model_;
 
@@ -419,6 +419,7 @@ class LognormalStochasticCoefficientsProvider {
   LognormalStochasticCoefficientsProvider& operator=(const LognormalStochasticCoefficientsProvider&) = delete;
   const MSG_KL* Kl() const { return &kl_; }
   int Terms() const { return kl_.n_terms; }
+  bool Gaussian() const { return kl_.gaussian != 0; }
   const std::vector<double>& W() const { return w_; }
   const std::vector<double>& Amp() const { return amp_; }
   const std::vector<int>& Idx() const { return idx_; }
@@ -429,7 +430,20 @@ class LognormalStochasticCoefficientsProvider {
   std::vector<double> w_, amp_;
   std::vector<int> idx_;
   std::vector<double> eig_;
+
+ protected:
   MSG_KL kl_;
+};
+
+// KL Gaussian modulus E = mean (1 + sum_k xi_k covariance sqrt(eig_k) phi_k)
+// (GaussianFileStochasticCoefficientsProvider.cs:24-108; covariance 0.15 as the reference).
+class GaussianStochasticCoefficientsProvider : public LognormalStochasticCoefficientsProvider {
+ public:
+  GaussianStochasticCoefficientsProvider(std::array<double, 3> domain, double corr_len, int n_terms = 50,
+                                         int n1d = 16, double mean = 1.0, double covariance = 0.15)
+      : LognormalStochasticCoefficientsProvider(domain, corr_len, n_terms, n1d, mean, covariance) {
+    kl_.gaussian = 1;
+  }
 };
 
 // The realization loop: Initialize() draws xi[simulations][expansionOrder] ~
@@ -563,6 +577,102 @@ class NewmarkDynamicAnalyzer : public IAnalyzer {
  public:
   double Tolerance;
   int MaxIterations;
+};
+
+// The re-orthogonalising search-vector calculator
+// (SolverPCGReorthogonalizationSearchVectorCalculator.cs:11-65) as a device
+// store of (p, K p) pairs for one mesh, at most `capacity` pairs.
+class SolverPCGReorthogonalizationSearchVectorCalculator {
+ public:
+  SolverPCGReorthogonalizationSearchVectorCalculator(GpuMesh& mesh, int capacity) : mesh_(mesh) {
+    Check(MSG_SVS_CREATE(mesh.Handle(), capacity, &h_), mesh.Ctx().Handle(), "MSG_SVS_CREATE");
+  }
+  ~SolverPCGReorthogonalizationSearchVectorCalculator() {
+    if (h_) MSG_SVS_DESTROY(h_);
+  }
+  SolverPCGReorthogonalizationSearchVectorCalculator(const SolverPCGReorthogonalizationSearchVectorCalculator&) =
+      delete;
+  SolverPCGReorthogonalizationSearchVectorCalculator& operator=(
+      const SolverPCGReorthogonalizationSearchVectorCalculator&) = delete;
+  MSG_SVS Handle() const { return h_; }
+  int Count() const {
+    int c = 0;
+    Check(MSG_SVS_COUNT(h_, &c), mesh_.Ctx().Handle(), "MSG_SVS_COUNT");
+    return c;
+  }
+  void ClearSearchVectors(int vectors_to_keep_from_top = 0) {
+    Check(MSG_SVS_CLEAR(h_, vectors_to_keep_from_top), mesh_.Ctx().Handle(), "MSG_SVS_CLEAR");
+  }
+
+ private:
+  GpuMesh& mesh_;
+  MSG_SVS h_ = nullptr;
+};
+
+// SolverPCG with the re-orthogonalising calculator. StartFromStore: 0 x0 = 0;
+// 1 the starting vector from the stored directions
+// (InitializeStartingVectorFromSearchVectors), the store kept; 2 the same
+// starting vector, then a fresh store (for a changed matrix).
+class SolverPCGReorthogonalized : public SolverPCG {
+ public:
+  SolverPCGReorthogonalized(Context& ctx, Model& model, SolverPCGReorthogonalizationSearchVectorCalculator& search,
+                            int max_iterations = 20000, double tolerance = 1e-7, int start_from_store = 0)
+      : SolverPCG(ctx, model, max_iterations, tolerance), Search(search), StartFromStore(start_from_store) {}
+  void Solve() override {
+    Subdomain& s = model_.subdomain;
+    s.Solution.assign(model_.n_dofs, 0.0);
+    int it = 0;
+    double rr = 0.0;
+    const int st = MSG_PCG_SOLVE_REORTH(Matrix->Handle(), Search.Handle(), s.Forces.data(), s.Solution.data(),
+                                        StartFromStore, MaxIterations, Tolerance, &it, &rr);
+    Iterations = it;
+    RelativeResidual = rr;
+    Check(st, ctx_.Handle(), "MSG_PCG_SOLVE_REORTH");
+  }
+  SolverPCGReorthogonalizationSearchVectorCalculator& Search;
+  int StartFromStore;
+};
+
+// Hexa8.CalculateStresses / CalculateForces for a batch of n elements:
+// xyz [n][8][3], E [n], u (and the increment du, u when empty) [n][24] ->
+// strains, stresses [n][8][6] at the Gauss points, forces [n][24].
+inline void H8StressBatch(Context& ctx, const std::vector<double>& xyz, const std::vector<double>& E, double nu,
+                          const std::vector<double>& u, const std::vector<double>& du, std::vector<double>& strains,
+                          std::vector<double>& stresses, std::vector<double>& forces) {
+  const int n = (int)E.size();
+  strains.assign((size_t)n * 48, 0.0);
+  stresses.assign((size_t)n * 48, 0.0);
+  forces.assign((size_t)n * 24, 0.0);
+  Check(MSG_H8_STRESS_BATCH(ctx.Handle(), n, xyz.data(), E.data(), nu, u.data(), du.empty() ? nullptr : du.data(),
+                            strains.data(), stresses.data(), forces.data()),
+        ctx.Handle(), "MSG_H8_STRESS_BATCH");
+}
+
+// PolynomialChaosSolverPCGMatrixCalculator.MultiplyWithMatrix: the stochastic
+// Galerkin product over a Gaussian field's chaos basis of m variables and
+// degree p, u and y block vectors [PsiSize][n_dofs].
+class PolynomialChaosSolverPCGMatrixCalculator {
+ public:
+  PolynomialChaosSolverPCGMatrixCalculator(GpuMesh& mesh, LognormalStochasticCoefficientsProvider& provider, int m,
+                                           int p)
+      : mesh_(mesh), kl_(provider), m_(m), p_(p) {
+    if (!provider.Gaussian())
+      throw ArgumentException(MSG_ERR_INVALID_ARGUMENT,
+                              "the Galerkin operator needs a GaussianStochasticCoefficientsProvider");
+    Check(MSG_PC_SIZE(m, p, &psi_), nullptr, "MSG_PC_SIZE");
+  }
+  int PsiSize() const { return psi_; }
+  std::vector<double> MultiplyWithMatrix(const std::vector<double>& u) const {
+    std::vector<double> y(u.size(), 0.0);
+    Check(MSG_PC_GALERKIN_MATVEC(mesh_.Handle(), mesh_.GetModel().Poisson, kl_.Kl(), m_, p_, u.data(), y.data()),
+          mesh_.Ctx().Handle(), "MSG_PC_GALERKIN_MATVEC");
+    return y;
+  }
+
+ private:
+  GpuMesh& mesh_;
+  LognormalStochasticCoefficientsProvider& kl_;
+  int m_, p_, psi_ = 0;
 };
 
 // Continuous-batching service of independent realizations (MSG_SERVE_*; no

@@ -17,6 +17,14 @@
 //           1e-10): R requests to each, xi rows [2][R][TERMS] from XI, all submitted before
 //           the first poll -> for every request in submission order: iterations (int32),
 //           relative residual (f64), displacements [n_dofs] (f64)
+//   reorth  B OUT                        SolverPCGReorthogonalized on the cantilever (tol 1e-10,
+//           store of 400 pairs) for the 3 loads [3][n_dofs] in B, the first from zero, the
+//           others from the store -> per load: iterations, stored pairs (int32), solution (f64)
+//   stress  U OUT                        H8StressBatch over the cantilever's elements (E 1, nu 0.3) with
+//           u [n_elems][24] from U -> strains, stresses [n][8][6], forces [n][24] (f64)
+//   pc      N M P U OUT                  PolynomialChaosSolverPCGMatrixCalculator on the N^3 block with a
+//           Gaussian field (corr 0.3 N, max(M,4) terms, 8 modes, mean 2, covariance 0.15):
+//           y = MultiplyWithMatrix(u), u [PsiSize][n_dofs] from U (f64)
 //   kl      N TERMS OUT                  the KL table of the N^3 block's provider: w [TERMS][3],
 //           amp [TERMS][3] (f64), idx [TERMS][3] (int32), eig [TERMS] (f64) (host only)
 //   errors                               the exception type each status code maps to, one per line
@@ -144,6 +152,62 @@ int run(int argc, char** argv) {
       ok = ok && write_all(f, &it, sizeof(it)) && write_all(f, &res.RelativeResidual, sizeof(double)) &&
            put(f, res.X);
     }
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "reorth" && argc >= 4) {
+    msolve::Model m = msolve::Hexa8MeshGenerator::Cantilever();
+    msolve::Context ctx(0);
+    msolve::ProblemStructural provider(ctx, m);
+    msolve::GpuMatrix& K = provider.CalculateMatrix(m.subdomain);
+    msolve::SolverPCGReorthogonalizationSearchVectorCalculator search(provider.Mesh(), 400);
+    msolve::SolverPCGReorthogonalized solver(ctx, m, search, 20000, 1e-10);
+    solver.Matrix = &K;
+    solver.Initialize();
+    const std::vector<double> b = read_doubles(argv[2], (size_t)3 * m.n_dofs);
+    FILE* f = std::fopen(argv[3], "wb");
+    if (!f) return 6;
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+      m.subdomain.Forces.assign(b.begin() + (size_t)k * m.n_dofs, b.begin() + (size_t)(k + 1) * m.n_dofs);
+      solver.StartFromStore = k == 0 ? 0 : 1;
+      solver.Solve();
+      const int32_t hdr[2] = {solver.Iterations, search.Count()};
+      ok = ok && write_all(f, hdr, sizeof(hdr)) && put(f, m.subdomain.Solution);
+    }
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "stress" && argc >= 4) {
+    msolve::Model m = msolve::Hexa8MeshGenerator::Cantilever();
+    msolve::Context ctx(0);
+    const int ne = m.NumElements();
+    std::vector<double> xyz((size_t)ne * 24);
+    for (int e = 0; e < ne; ++e)
+      for (int a = 0; a < 8; ++a)
+        for (int c = 0; c < 3; ++c) xyz[((size_t)e * 8 + a) * 3 + c] = m.xyz[(size_t)m.conn[(size_t)e * 8 + a] * 3 + c];
+    const std::vector<double> u = read_doubles(argv[2], (size_t)ne * 24);
+    std::vector<double> eps, sig, frc;
+    msolve::H8StressBatch(ctx, xyz, m.E_elem, m.Poisson, u, {}, eps, sig, frc);
+    FILE* f = std::fopen(argv[3], "wb");
+    if (!f) return 6;
+    const bool ok = put(f, eps) && put(f, sig) && put(f, frc);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "pc" && argc >= 7) {
+    const int n = std::atoi(argv[2]), mv = std::atoi(argv[3]), pd = std::atoi(argv[4]);
+    msolve::Model m = msolve::Hexa8MeshGenerator::ClampedBlock(n);
+    msolve::Context ctx(0);
+    msolve::GaussianStochasticCoefficientsProvider kl({(double)n, (double)n, (double)n}, 0.3 * n, std::max(mv, 4), 8,
+                                                      2.0, 0.15);
+    msolve::GpuMesh mesh(ctx, m);
+    msolve::PolynomialChaosSolverPCGMatrixCalculator op(mesh, kl, mv, pd);
+    const std::vector<double> u = read_doubles(argv[5], (size_t)op.PsiSize() * m.n_dofs);
+    const std::vector<double> y = op.MultiplyWithMatrix(u);
+    FILE* f = std::fopen(argv[6], "wb");
+    if (!f) return 6;
+    const bool ok = put(f, y);
     std::fclose(f);
     return ok ? 0 : 6;
   }

@@ -187,3 +187,63 @@ def test_kl_table_matches_python_provider(driver, tmp_path):
         assert np.array_equal(got, arr)
         o += nb
     assert o == len(raw)
+
+
+@pytest.mark.gpu
+def test_reorthogonalized_solver_matches_python_mirror(ctx, driver, tmp_path):
+    model = M.cantilever_model()
+    b0 = model.subdomains[0].RHS.copy()
+    rng = np.random.default_rng(31)
+    loads = np.stack([b0, 2.0 * b0, b0 + 0.01 * np.abs(b0).max() * rng.standard_normal(model.n_dofs)])
+    b_path = tmp_path / "b.bin"
+    b_path.write_bytes(loads.tobytes())
+    out = tmp_path / "reorth.bin"
+    rc, err = run(driver, "reorth", b_path, out)
+    assert rc == 0, err
+    raw = out.read_bytes()
+    provider = M.ProblemStructural(ctx, model)
+    K = provider.CalculateMatrix()
+    search = M.SolverPCGReorthogonalizationSearchVectorCalculator(provider.mesh, 400)
+    solver = M.SolverPCGReorthogonalized(ctx, model, search, tolerance=1e-10)
+    solver.matrix = K
+    off = 0
+    for k in range(3):
+        its, count = np.frombuffer(raw[off:off + 8], dtype=np.int32)
+        x = np.frombuffer(raw[off + 8:off + 8 + 8 * model.n_dofs], dtype=np.float64)
+        off += 8 + 8 * model.n_dofs
+        model.subdomains[0].Forces = loads[k]
+        xp = solver.Solve(start_from_store=0 if k == 0 else 1)
+        assert its == solver.iterations and count == search.count and np.array_equal(x, xp)
+    assert off == len(raw)
+
+
+@pytest.mark.gpu
+def test_stress_batch_matches_python_mirror(ctx, driver, tmp_path):
+    model = M.cantilever_model()
+    u = np.random.default_rng(37).standard_normal((model.n_elems, 24))
+    u_path = tmp_path / "u.bin"
+    u_path.write_bytes(u.tobytes())
+    out = tmp_path / "stress.bin"
+    rc, err = run(driver, "stress", u_path, out)
+    assert rc == 0, err
+    raw = np.frombuffer(out.read_bytes(), dtype=np.float64)
+    ne = model.n_elems
+    eps, sig, f = raw[:ne * 48], raw[ne * 48:ne * 96], raw[ne * 96:]
+    e2, s2, f2 = M.h8_stress_batch(ctx, model.xyz[model.conn], model.E_elem, model.poisson, u)
+    assert np.array_equal(eps, e2.ravel()) and np.array_equal(sig, s2.ravel()) and np.array_equal(f, f2.ravel())
+
+
+@pytest.mark.gpu
+def test_galerkin_product_matches_python_mirror(ctx, driver, tmp_path):
+    n, m, p = 4, 2, 2
+    model = M.clamped_block_model(n)
+    kl = M.GaussianStochasticCoefficientsProvider([n, n, n], 0.3 * n, max(m, 4), 8, mean=2.0, covariance=0.15)
+    op = M.PolynomialChaosSolverPCGMatrixCalculator(M.GpuMesh(ctx, model), kl, m, p)
+    u = np.random.default_rng(41).standard_normal((op.PsiSize, model.n_dofs))
+    u_path = tmp_path / "u.bin"
+    u_path.write_bytes(u.tobytes())
+    out = tmp_path / "pc.bin"
+    rc, err = run(driver, "pc", n, m, p, u_path, out)
+    assert rc == 0, err
+    y = np.frombuffer(out.read_bytes(), dtype=np.float64).reshape(op.PsiSize, -1)
+    assert np.array_equal(y, op.MultiplyWithMatrix(u))
