@@ -102,3 +102,12 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
         raise AssertionError("expected ImportError")
     except ImportError as e:
         assert "no CPU fallback" in str(e)
+
+
+def test_integration_bindings_name_header_entry_points():
+    """Every entry point the P/Invoke declarations in INTEGRATION.md bind is
+    declared by the header (the documented binding cannot drift from the ABI)."""
+    txt = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    bound = set(re.findall(r"extern\s+int\s+(MSG_[A-Z0-9_]+)\s*\(", txt))
+    assert len(bound) >= 10
+    assert bound <= header_symbols(), bound - header_symbols()
