@@ -89,6 +89,8 @@ def parse():
     p.add_argument("--mg-sweeps", type=int, default=None, help="MSG_SET_OPTION multigrid_sweeps (coarsest level)")
     p.add_argument("--mg-delta", type=float, default=None, help="MSG_SET_OPTION multigrid_delta")
     p.add_argument("--mg-omega", type=float, default=None, help="MSG_SET_OPTION multigrid_omega")
+    p.add_argument("--mg-packed", type=int, default=None, choices=[0, 1],
+                   help="MSG_SET_OPTION multigrid_packed (0: level operators on 32-realization tiles)")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
@@ -370,7 +372,8 @@ def main():
         ctx.set_option("multigrid", args.multigrid)
     for key, val in (("multigrid_levels", args.mg_levels), ("multigrid_sweeps", args.mg_sweeps),
                      ("multigrid_delta", args.mg_delta), ("multigrid_omega", args.mg_omega),
-                     ("serve_persistent", args.serve_persistent), ("serve_priority", args.serve_priority)):
+                     ("serve_persistent", args.serve_persistent), ("serve_priority", args.serve_priority),
+                     ("multigrid_packed", args.mg_packed)):
         if val is not None:
             ctx.set_option(key, val)
     model, kl = make_problem(args)
@@ -410,7 +413,8 @@ def main():
     # loop configuration (tile shapes, preconditioner) picked by the project's autotuner
     # on this rank's own batch, unless an option was forced on the command line
     tuned = None
-    forced = any(v is not None for v in (args.multigrid, args.mg_levels, args.chunk, args.modal_operator))
+    forced = any(v is not None for v in (args.multigrid, args.mg_levels, args.chunk, args.modal_operator,
+                                         args.mg_packed))
     if not args.no_autotune and not forced:
         from msolve_b200.tuning import Autotuner
         tuner = Autotuner(ctx, args.autotune_cache)
