@@ -189,11 +189,19 @@ int MSG_PCG_SOLVE_REORTH(MSG_MAT mat, MSG_SVS store, const double* b, double* x,
  * device buffers (n_dofs doubles, DOF numbering); the solve's working vectors
  * live in one fixed device array of the library (about 9.5 MB, held on every
  * GPU that loads the library until the process exits), which limits the mesh
- * to 65536 nodes (larger meshes: MSG_ERR_INVALID_ARGUMENT). The first call on
- * a device looks up that array's device address; make the first call before
- * any stream capture. All calls share the array: calls whose GPU work
- * overlaps (two host threads on two contexts of the same device) race and must
- * be serialised by the caller. Semantics, kernels and results as MSG_PCG_SOLVE. */
+ * to 65536 nodes (larger meshes: MSG_ERR_INVALID_ARGUMENT). MSG_CREATE looks up
+ * that array's device address, so the solve itself does no set-up. Stream
+ * ordering: the call runs on the context's own stream, which does not wait for
+ * other streams (not even the legacy default stream), so the caller's writes
+ * to b_dev must be complete before the call (synchronise the stream that wrote
+ * it) and x_dev must not be in use by other GPU work; the call returns after
+ * its stream has finished, so x_dev holds the solution on return. All calls
+ * share the array, which keeps the previous call's contents (the call clears
+ * what must start at zero): calls whose GPU work overlaps (two host threads on
+ * two contexts of the same device) race and must be serialised by the caller.
+ * Semantics, kernels and results as MSG_PCG_SOLVE, including the
+ * MSG_ERR_NOT_CONVERGED / MSG_ERR_BREAKDOWN returns with x_dev, iterations and
+ * rel_res written. */
 int MSG_PCG_SOLVE_NOALLOC(MSG_MAT mat, const double* b_dev, double* x_dev, int max_it, double tol, int* iterations,
                           double* rel_res);
 

@@ -596,21 +596,15 @@ constexpr size_t kNoAllocBytes = kNoAllocStateOff + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of the scratch array on the current device, looked up once per
-// device (host code cannot use the array's name as a device address).
-static int noalloc_scratch(Context* ctx, unsigned char** out) {
-  static std::mutex mu;
-  static unsigned char* addr[64] = {nullptr};
-  if (ctx->device < 0 || ctx->device >= 64) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "device index >= 64");
-  std::lock_guard<std::mutex> lk(mu);
-  if (!addr[ctx->device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-    addr[ctx->device] = static_cast<unsigned char*>(p);
-  }
-  *out = addr[ctx->device];
-  return MSG_OK;
+// Device address of the scratch array on the current device (host code cannot
+// use the array's name as a device address). MSG_CREATE looks it up once per
+// context, with the context's device current, so no solve call triggers the
+// module load that the first lookup may cause.
+cudaError_t noalloc_scratch_address(unsigned char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  *out = static_cast<unsigned char*>(p);
+  return e;
 }
 
 }  // namespace msg
@@ -628,14 +622,14 @@ extern "C" int MSG_PCG_SOLVE_NOALLOC(MSG_MAT A, const double* b_dev, double* x_d
   Mesh* m = A->mesh;
   Context* ctx = m->ctx;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
-  cudaSetDevice(ctx->device);
+  MSG_CUDA(ctx, cudaSetDevice(ctx->device));
   const int nr = m->n_nodes;
   if (nr > kNoAllocMaxNodes)
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT,
                      "MSG_PCG_SOLVE_NOALLOC: mesh has %d nodes, the fixed scratch holds at most %d", nr,
                      kNoAllocMaxNodes);
-  unsigned char* base = nullptr;
-  MSG_TRY(noalloc_scratch(ctx, &base));
+  unsigned char* base = ctx->noalloc_scratch;
+  if (!base) return set_error(ctx, MSG_ERR_CUDA, "MSG_PCG_SOLVE_NOALLOC: scratch address not resolved");
   const size_t n = 3 * (size_t)nr;
   double* bn = reinterpret_cast<double*>(base);
   double* xn = reinterpret_cast<double*>(base + kNoAllocVecBytes);

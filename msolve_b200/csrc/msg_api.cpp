@@ -536,6 +536,9 @@ int MSG_CREATE(int device, uint64_t mem_budget_bytes, MSG_CTX* out) {
   if (cudaSetDevice(device) != cudaSuccess) return MSG_ERR_CUDA;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return MSG_ERR_CUDA;
   cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  // MSG_PCG_SOLVE_NOALLOC's scratch array: its device address is resolved here,
+  // outside any solve (the lookup may load the module and create the array)
+  if (noalloc_scratch_address(&c->noalloc_scratch) != cudaSuccess) { cudaGetLastError(); return MSG_ERR_CUDA; }
   *out = c.release();
   return MSG_OK;
 }

@@ -100,8 +100,15 @@ struct Context {
   DevMem* mc_ke = nullptr;
   DevMem* mc_st = nullptr;
   DevMem* mc_E = nullptr;
+  // device address of MSG_PCG_SOLVE_NOALLOC's fixed scratch array on this
+  // context's device, looked up by MSG_CREATE (noalloc_scratch_address)
+  unsigned char* noalloc_scratch = nullptr;
   ~Context();
 };
+
+// Device address of MSG_PCG_SOLVE_NOALLOC's scratch array on the current device
+// (kernels_bsr.cu); MSG_CREATE calls it with the context's device current.
+cudaError_t noalloc_scratch_address(unsigned char** out);
 
 // Stop the serving worker of a context and free its lanes (serve.cpp).
 void server_destroy(Context* ctx);

@@ -74,6 +74,12 @@ def lib():
                                             C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                             C.c_double, C.c_double, C.c_int, _d, C.c_int, C.c_double, C.c_int,
                                             _d, _d, _i]),
+            "orc_block_solve_pcg_batch": (None, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _u8, _d,
+                                                  C.c_double, _d, _d, C.c_int, C.c_int, C.c_double, _i, _i, _d]),
+            "orc_block_newmark_batch": (None, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _u8, _d, C.c_double,
+                                                C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_int, _d, C.c_int,
+                                                C.c_double, C.c_int, C.c_int, _d, _d, _i, _i]),
             "orc_kl_field_gaussian": (None, [C.c_int, _d, _d, C.c_int, _d, _d, _i, _d, C.c_int, _d,
                                              C.c_double, C.c_double, _d]),
             "orc_pcg_reorth_csr": (C.c_int, [C.c_int, _i64, _i, _d, _d, _d, _d, _d, _d, C.c_int, _i, C.c_int,
@@ -422,6 +428,52 @@ def block_newmark(nx, ny, nz, constrained, E_elem, nu, rho, ray_alpha, ray_beta,
                                  int(n_steps), float(acc_amp), float(acc_period), int(acc_dir), fs, int(solver),
                                  float(tol), int(tip_dof), _p(tip), _p(u), C.byref(its))
     return tip, u, dict(status=st, iterations=its.value)
+
+
+def block_solve_pcg_batch(nx, ny, nz, constrained, E, nu, b, h=1.0, max_it=50000, tol=1e-10):
+    """block_solve_pcg for every row of E [R][ne], realizations in parallel (one
+    per OpenMP thread); returns x [R][n_dofs], status, iterations, rel_res."""
+    cons = np.ascontiguousarray(constrained, dtype=np.uint8)
+    E, b = _f64(np.atleast_2d(E)), _f64(b)
+    R, N = E.shape[0], b.shape[0]
+    x = np.zeros((R, N))
+    st, it, rr = np.zeros(R, dtype=np.int32), np.zeros(R, dtype=np.int32), np.zeros(R)
+    lib().orc_block_solve_pcg_batch(R, nx, ny, nz, float(h), _p(cons, _u8), _p(E), float(nu), _p(b), _p(x), N,
+                                    max_it, tol, _p(st, _i), _p(it, _i), _p(rr))
+    return x, dict(status=st, iterations=it, rel_res=rr)
+
+
+def block_newmark_batch(nx, ny, nz, constrained, E, nu, rho, ray_alpha, ray_beta, nm_alpha, nm_delta, dt, n_steps,
+                        acc_amp, acc_period, acc_dir, n_dofs, f_static=None, solver=2, tol=1e-12, tip_dof=-1, h=1.0):
+    """block_newmark for every row of E [R][ne], realizations in parallel; returns
+    (tip histories [R][n_steps], final displacements [R][n_dofs], info)."""
+    cons = np.ascontiguousarray(constrained, dtype=np.uint8)
+    E = _f64(np.atleast_2d(E))
+    R = E.shape[0]
+    tip = np.zeros((R, n_steps))
+    u = np.zeros((R, n_dofs))
+    its, st = np.zeros(R, dtype=np.int32), np.zeros(R, dtype=np.int32)
+    fs = _p(_f64(f_static)) if f_static is not None else None
+    lib().orc_block_newmark_batch(R, nx, ny, nz, float(h), _p(cons, _u8), _p(E), float(nu), float(rho),
+                                  float(ray_alpha), float(ray_beta), float(nm_alpha), float(nm_delta), float(dt),
+                                  int(n_steps), float(acc_amp), float(acc_period), int(acc_dir), fs, int(solver),
+                                  float(tol), int(tip_dof), int(n_dofs), _p(tip), _p(u), _p(its, _i), _p(st, _i))
+    return tip, u, dict(status=st, iterations=its)
+
+
+def block_problem(n, n_terms=50, n1d=16, corr_frac=0.2):
+    """The clamped cube of the Monte Carlo workloads from the oracle alone: an
+    n^3 block of unit cubes, z = 0 face clamped, unit pressure on the top face
+    (consistent weights), the KL table of the separable exponential kernel with
+    correlation length corr_frac * n. Returns a dict with xyz, conn,
+    constrained [n_nodes][3] (uint8), dof, n_dofs, b, table, centroids, domain."""
+    xyz, conn = block_mesh(n, n, n)
+    cons = clamp_face(xyz, 2, 0.0)
+    dof, nd = enumerate_dofs(cons)
+    b = load_top_pressure(xyz, dof, nd)
+    table = kl_table([n, n, n], corr_frac * n, n_terms, n1d)
+    return dict(n=n, xyz=xyz, conn=conn, constrained=cons, dof=dof, n_dofs=nd, b=b, table=table,
+                centroids=centroids(xyz, conn), domain=[float(n)] * 3)
 
 
 def num_threads():

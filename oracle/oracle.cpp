@@ -1018,7 +1018,10 @@ int orc_block_solve_pcg(int nx, int ny, int nz, double h, const uint8_t* cons, c
  * MassAccelerationSinusoidalLoad.cs:17-20 (a_g(i) = A sin(2 pi / T_p dt i)).
  * The effective matrix is factorised once (skyline LDL^T, SolverSkyline) when
  * solver == 0, or each step is solved by Jacobi PCG from x0 = 0 to `tol` when
- * solver == 1 (SolverPCG). tip_hist[i] = u[tip_dof] after step i. */
+ * solver == 1 (SolverPCG), or from the previous step's displacement when
+ * solver == 2 (a starting vector only: converged to a tight `tol` the steps
+ * agree with solver 1 to that tolerance, in fewer iterations).
+ * tip_hist[i] = u[tip_dof] after step i. */
 int orc_block_newmark(int nx, int ny, int nz, double h, const uint8_t* cons, const double* Ee, double nu, double rho,
                       double ray_alpha, double ray_beta, double nm_alpha, double nm_delta, double dt, int n_steps,
                       double acc_amp, double acc_period, int acc_dir, const double* f_static, int solver, double tol,
@@ -1104,8 +1107,28 @@ int orc_block_newmark(int nx, int ny, int nz, double h, const uint8_t* cons, con
     } else {
       int it = 0, mv = 0;
       double rr = 0;
-      std::fill(x.begin(), x.end(), 0.0);
-      st = orc_pcg_csr_jacobi(N, rp.data(), ci.data(), Ktv.data(), rhs.data(), x.data(), 100000, tol, &it, &mv, &rr);
+      if (solver == 1) {
+        std::fill(x.begin(), x.end(), 0.0);
+        st = orc_pcg_csr_jacobi(N, rp.data(), ci.data(), Ktv.data(), rhs.data(), x.data(), 100000, tol, &it, &mv,
+                                &rr);
+      } else {
+        // warm start: solve K~ dx = rhs - K~ u for the increment from zero, to the
+        // same absolute stopping point ||r|| < tol ||rhs||, then x = u + dx
+        orc_csr_multiply(N, rp.data(), ci.data(), Ktv.data(), u.data(), um.data());
+        double nb = 0, nr = 0;
+        for (int k = 0; k < N; ++k) {
+          ucm[k] = rhs[k] - um[k];
+          nb += rhs[k] * rhs[k];
+          nr += ucm[k] * ucm[k];
+        }
+        std::fill(x.begin(), x.end(), 0.0);
+        if (nr > 0) {
+          const double tol_inc = nb > 0 ? tol * std::sqrt(nb / nr) : tol;
+          st = orc_pcg_csr_jacobi(N, rp.data(), ci.data(), Ktv.data(), ucm.data(), x.data(), 100000, tol_inc, &it,
+                                  &mv, &rr);
+        }
+        for (int k = 0; k < N; ++k) x[k] += u[k];
+      }
       if (st) return st;
       its_sum += it;
     }
@@ -1120,6 +1143,36 @@ int orc_block_newmark(int nx, int ny, int nz, double h, const uint8_t* cons, con
   if (u_final) std::copy(u.begin(), u.end(), u_final);
   if (total_its) *total_its = its_sum;
   return 0;
+}
+
+
+/* Realizations in parallel: one realization per OpenMP thread, each solved as
+ * orc_block_solve_pcg does (its inner OpenMP loops run on that one thread).
+ * E [R][ne], b shared, x [R][N]; status/iterations/rel_res per realization. */
+void orc_block_solve_pcg_batch(int R, int nx, int ny, int nz, double h, const uint8_t* cons, const double* E, double nu,
+                               const double* b, double* x, int N, int max_it, double tol, int* status,
+                               int* iterations, double* rel_res) {
+  const int64_t ne = (int64_t)nx * ny * nz;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int r = 0; r < R; ++r)
+    status[r] = orc_block_solve_pcg(nx, ny, nz, h, cons, E + r * ne, nu, b, x + (int64_t)r * N, max_it, tol,
+                                    &iterations[r], &rel_res[r]);
+}
+
+/* orc_block_newmark for R realizations in parallel (one per OpenMP thread).
+ * E [R][ne]; tip_hist [R][n_steps]; u_final [R][N]; per-realization status and
+ * total iterations. */
+void orc_block_newmark_batch(int R, int nx, int ny, int nz, double h, const uint8_t* cons, const double* E, double nu,
+                             double rho, double ray_alpha, double ray_beta, double nm_alpha, double nm_delta,
+                             double dt, int n_steps, double acc_amp, double acc_period, int acc_dir,
+                             const double* f_static, int solver, double tol, int tip_dof, int N, double* tip_hist,
+                             double* u_final, int* total_its, int* status) {
+  const int64_t ne = (int64_t)nx * ny * nz;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int r = 0; r < R; ++r)
+    status[r] = orc_block_newmark(nx, ny, nz, h, cons, E + r * ne, nu, rho, ray_alpha, ray_beta, nm_alpha, nm_delta,
+                                  dt, n_steps, acc_amp, acc_period, acc_dir, f_static, solver, tol, tip_dof,
+                                  tip_hist + (int64_t)r * n_steps, u_final + (int64_t)r * N, &total_its[r]);
 }
 
 }  // extern "C"

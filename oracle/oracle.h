@@ -102,6 +102,16 @@ int orc_block_newmark(int nx, int ny, int nz, double h, const uint8_t* constrain
                       int n_steps, double acc_amp, double acc_period, int acc_dir, const double* f_static, int solver,
                       double tol, int tip_dof, double* tip_hist, double* u_final, int* total_its);
 
+/* Realizations in parallel, one per OpenMP thread (E [R][ne], x [R][N]). */
+void orc_block_solve_pcg_batch(int R, int nx, int ny, int nz, double h, const uint8_t* constrained3, const double* E,
+                               double nu, const double* b, double* x, int N, int max_it, double tol, int* status,
+                               int* iterations, double* rel_res);
+void orc_block_newmark_batch(int R, int nx, int ny, int nz, double h, const uint8_t* constrained3, const double* E,
+                             double nu, double rho, double ray_alpha, double ray_beta, double nm_alpha,
+                             double nm_delta, double dt, int n_steps, double acc_amp, double acc_period, int acc_dir,
+                             const double* f_static, int solver, double tol, int tip_dof, int N, double* tip_hist,
+                             double* u_final, int* total_its, int* status);
+
 int orc_num_threads(void);
 
 #ifdef __cplusplus

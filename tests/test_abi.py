@@ -104,10 +104,25 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
         assert "no CPU fallback" in str(e)
 
 
-def test_integration_bindings_name_header_entry_points():
-    """Every entry point the P/Invoke declarations in INTEGRATION.md bind is
-    declared by the header (the documented binding cannot drift from the ABI)."""
-    txt = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    bound = set(re.findall(r"extern\s+int\s+(MSG_[A-Z0-9_]+)\s*\(", txt))
-    assert len(bound) >= 10
-    assert bound <= header_symbols(), bound - header_symbols()
+def header_arities():
+    """Parameter count of every entry point the headers declare."""
+    out = {}
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            for name, params in re.findall(r"^\s*(?:int|const char\*|void)\s+(MSG_[A-Z0-9_]+)\s*\(([^)]*)\)",
+                                           txt, re.M | re.S):
+                p = params.strip()
+                out[name] = 0 if p in ("", "void") else p.count(",") + 1
+    return out
+
+
+def test_bindings_match_header_declarations():
+    """Every entry point the ctypes binding declares (the Python analogue of the
+    P/Invoke shim) is declared by the header with the same number of
+    parameters, so the binding cannot drift from the ABI."""
+    ar = header_arities()
+    assert len(ar) >= 20
+    assert set(N.SIGNATURES) <= set(ar), set(N.SIGNATURES) - set(ar)
+    for name, (_, argtypes) in N.SIGNATURES.items():
+        assert len(argtypes) == ar[name], (name, len(argtypes), ar[name])

@@ -110,6 +110,29 @@ def test_cantilever_skyline_ldlt_vs_jacobi_pcg():
     assert info2["matvecs"] == 1 and np.abs(xq - xs).max() <= 1e-12 * np.abs(xs).max()
 
 
+def test_monte_carlo_first_realization_factor_preconditions_the_others():
+    """The reference's Monte Carlo solver (MonteCarloSolverPCGDirectMatrixCalculator.cs:38-80):
+    the skyline LDL^T of the first realization's K preconditions PCG on every later
+    realization (matvec: that realization's skyline product). It reaches the
+    Jacobi-PCG solution of each realization in far fewer iterations."""
+    n = 6
+    P = O.block_problem(n, 20, 8)
+    xi = np.random.default_rng(4).standard_normal((3, 20))
+    E = O.kl_field(P["centroids"], P["domain"], P["table"], xi, sigma=0.3)
+    S = O.Skyline(P["conn"], P["dof"], P["n_dofs"])
+    exyz = O.element_xyz(P["xyz"], P["conn"])
+    S.assemble(O.h8_stiffness_batch(exyz, E[0], 0.3)[0])
+    F, zems = S.factorized(1e-8)
+    assert zems == 0
+    for r in (1, 2):
+        S.assemble(O.h8_stiffness_batch(exyz, E[r], 0.3)[0])
+        x, info = S.pcg(P["b"], F, tol=1e-10)
+        xj, ij = O.block_solve_pcg(n, n, n, P["constrained"], E[r], 0.3, P["b"], tol=1e-10)
+        assert info["status"] == 0 and ij["status"] == 0
+        assert info["iterations"] * 4 < ij["iterations"]
+        assert np.abs(x - xj).max() <= 1e-8 * np.abs(xj).max()
+
+
 def test_skyline_row_index_quirk():
     """rowIndex[1] = 1 is hard-coded (GlobalMatrixAssemblerSkyline.cs:40)."""
     xyz, conn, dof, N, b, Ke = cantilever()
