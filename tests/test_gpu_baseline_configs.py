@@ -11,10 +11,11 @@ ISAAR.MSolve.Analyzers/NewmarkDynamicAnalyzer.cs:280-315).
   iteration count (+-1); FP32 values + FP64 refinement to a 1e-10 relative
   residual is within 1e-8 of the oracle converged to 1e-12.
 * Newmark, 256 realizations of the 24^3 block, 200 steps: four of them, tip
-  histories within 1e-8 and final fields within 1e-7 of the oracle's FP64
-  integration (each step converged to 1e-13). Each GPU step is solved to a
-  1e-12 true relative residual: the integration carries step errors forward
-  (a0 = 1/(beta dt^2) = 4e4), so looser steps drift further from the oracle.
+  histories and final fields within 1e-8 of the oracle's FP64 integration
+  (each step converged to 1e-14). Each GPU step is solved to a 1e-13 true
+  relative residual: the integration carries step errors forward
+  (a0 = 1/(beta dt^2) = 4e4), so looser steps drift further from the oracle
+  (1e-8 steps end 6e-4 away).
 * Serving, one 48^3 request through MSG_SERVE_*: within 1e-8 of the oracle.
 """
 import numpy as np
@@ -88,7 +89,7 @@ def test_newmark_24cube_200_steps_against_oracle(ctx):
     corner = int(np.argmax(model.xyz.sum(1)))
     nm = M.NewmarkDynamicAnalyzer(ctx, model, kl, 0.25, 0.5, dt, dt * steps, load, expansion_order=K,
                                   simulations=R, density=1.0, rayleigh_alpha=0.01, rayleigh_beta=0.001,
-                                  tolerance=1e-12, tip_dof=int(model.dof[corner, 0]))
+                                  tolerance=1e-13, tip_dof=int(model.dof[corner, 0]))
     nm.RandomNumbers = xi
     hist = nm.Solve()
     assert hist.shape == (R, steps)
@@ -97,10 +98,10 @@ def test_newmark_24cube_200_steps_against_oracle(ctx):
     E = _fields(P, xi[rows])
     for i, r in enumerate(rows):
         t, u, info = O.block_newmark(n, n, n, P["constrained"], E[i], model.poisson, 1.0, 0.01, 0.001, 0.25, 0.5, dt,
-                                     steps, 0.1, 1.0, 0, model.n_dofs, solver=2, tol=1e-13, tip_dof=nm.tip_dof)
+                                     steps, 0.1, 1.0, 0, model.n_dofs, solver=2, tol=1e-14, tip_dof=nm.tip_dof)
         assert info["status"] == 0
         assert _rel(hist[r], t) <= 1e-8, (int(r), _rel(hist[r], t))
-        assert _rel(nm.Solutions[r], u) <= 1e-7, (int(r), _rel(nm.Solutions[r], u))
+        assert _rel(nm.Solutions[r], u) <= 1e-8, (int(r), _rel(nm.Solutions[r], u))
 
 
 def test_serving_48cube_request_against_oracle(ctx):
