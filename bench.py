@@ -102,6 +102,8 @@ def parse():
     p.add_argument("--mg-omega", type=float, default=None, help="MSG_SET_OPTION multigrid_omega")
     p.add_argument("--mg-packed", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION multigrid_packed (0: level operators on 32-realization tiles)")
+    p.add_argument("--tensor-op", type=int, default=None, choices=[0, 1],
+                   help="MSG_SET_OPTION tensor_operator (1: level-0 search-direction launch on the tensor cores)")
     p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
@@ -175,6 +177,19 @@ def make_problem(args):
     model = M.clamped_block_model(args.n)
     kl = M.LognormalStochasticCoefficientsProvider([args.n] * 3, 0.2 * args.n, args.terms, 16)
     return model, kl
+
+
+def tensor_roofline(args, model, R, op_ms):
+    """Tensor-pipe figures of the tensor-core level-0 launch: useful FLOP (the
+    24 x 24 element product, 1152 per element and realization) and issued MMA
+    FLOP (per x-slab of a 3 x 3 tile of node pencils and 32 realizations: 4 M
+    tiles x 4 corner pairs x (N 64 + N 32) x M 128 x K 8), per second."""
+    n = args.n
+    tiles = ((n + 1 + 2) // 3) ** 2
+    issued = 2.0 * 4 * 4 * (128 * 64 * 8 + 128 * 32 * 8) * tiles * ((R + 31) // 32) * n
+    sec = op_ms / 1e3
+    return {"useful_tflops": 1152.0 * model.n_elems * R / sec / 1e12, "issued_tflops": issued / sec / 1e12,
+            "unit": "TFLOP/s (TF32)"}
 
 
 def workload_config(args, ws):
@@ -462,6 +477,8 @@ def main():
         ctx.set_option("chunk", args.chunk)
     if args.modal_operator is not None:
         ctx.set_option("modal_operator", args.modal_operator)
+    if args.tensor_op is not None:
+        ctx.set_option("tensor_operator", args.tensor_op)
     if args.multigrid is not None:
         ctx.set_option("multigrid", args.multigrid)
     for key, val in (("multigrid_levels", args.mg_levels), ("multigrid_sweeps", args.mg_sweeps),
@@ -508,7 +525,7 @@ def main():
     # on this rank's own batch, unless an option was forced on the command line
     tuned = None
     forced = any(v is not None for v in (args.multigrid, args.mg_levels, args.chunk, args.modal_operator,
-                                         args.mg_packed))
+                                         args.mg_packed, args.tensor_op))
     if not args.no_autotune and not forced:
         from msolve_b200.tuning import Autotuner
         tuner = Autotuner(ctx, args.autotune_cache)
@@ -571,11 +588,15 @@ def main():
     # algorithmic bytes of one launch, FP32, realization-innermost, each value once.
     # multigrid: read z, p_{k-1}, d (3 per node), E (1 per element); write p_k, d, q (3 per node).
     # Jacobi: read r, p_{k-1}, d (3 per node), dinv (1 per node), E; write p_k, d, q (3 per node)
+    tensor = mg and ctx.get_option("tensor_operator") != 0
     if mg:
         op_kernel = ("k_lvl_op2<PcgZ> (multigrid loop, level 0: fused search direction p = z + beta p + "
                      "matrix-free FP32 operator, two realizations per lane in packed FP32)")
+        if tensor:
+            op_kernel = ("k_lvl_tc<PcgZ> (multigrid loop, level 0: fused search direction p = z + beta p + element "
+                         "product E Khat u on the tensor cores, tcgen05.mma kind::tf32 with a three-term split)")
         op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 3 + 3 + 3) * nn + ne)
-        per_r = MG_OP_DRAM_BYTES_PER_REALIZATION
+        per_r = None if tensor else MG_OP_DRAM_BYTES_PER_REALIZATION
     else:
         op_kernel = "k_op_modal (fused PCG direction update + matrix-free FP32 Hexa8 operator)"
         op_bytes = 4.0 * Rp * ((3 + 3 + 3 + 1 + 3 + 3 + 3) * nn + ne)
@@ -671,7 +692,8 @@ def main():
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm if hbm else None, "traffic": traffic,
                          "peak_kind": peak_kind, "launch_ms": op_ms, "bytes_per_launch": op_bytes,
                          ("iteration_ms" if mg else "update_launch_ms"): st["update_launch_ms"],
-                         "samples": st["launch_samples"]},
+                         "samples": st["launch_samples"],
+                         "tensor": tensor_roofline(args, model, R, op_ms) if tensor else None},
             "cpu_baseline": cpu,
             "clocks": clk,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

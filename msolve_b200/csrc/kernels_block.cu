@@ -1161,6 +1161,351 @@ __global__ void __launch_bounds__(kMThreads, 1)
   }
 }
 
+// ---------------------------------------------------------------- tensor-core element product (level 0)
+// k_lvl_tc<kLvlPcgZ>: the level-0 search-direction launch of the multigrid
+// loop, with k_lvl_op<kLvlPcgZ>'s inputs, outputs, tiling and node phase, but
+// the element product on the 5th-generation tensor cores (tcgen05.mma,
+// kind::tf32, accumulators in tensor memory) instead of the Walsh modes. For
+// the element pencils of an x-slab,
+//   y_e = E_e (cK Khat) u_e
+// is a product D[(element, realization)][output DOF] = sum over four corner
+// pairs of U_pair [128 x 8] B_pair^T [8 x N]: a corner pair (ax, ay) covers the
+// two corners az = 0, 1 of the element (slots 0-2 and 3-5 of an 8-slot K
+// group; slots 6-7 are zero), so one node-pair group of a plane serves the
+// element pencils on both of its sides. An M = 128 tile is the 4 element
+// pencils along y of one z row, 32 realizations each; it reads 4 consecutive
+// 1 KB groups (MN-major, 128-byte swizzle, realizations contiguous). TF32 with
+// a three-term split keeps FP32-level accuracy:
+//   U = U_hi + U_lo (U_hi: U with the low 13 mantissa bits cleared),
+//   cK Khat = B_hi + B_lo,  U Khat ~ U_hi [B_hi | B_lo] (N = 64) + U_lo B_hi (N = 32).
+// Output column n = ((ax' 2 + ay') 2 + az') 3 + c'; columns 0-11 land on plane
+// P-1, 12-23 on plane P (carried to the next slab, as the Walsh kernels carry
+// C1). Per plane: every element warp forms p = z + beta p_old at its nodes,
+// splits it and writes both halves into the plane's groups; after a CTA
+// barrier one thread issues the 32 MMAs of the slab (P-1, P) and commits them
+// to an mbarrier; each element warp reads its element's 24 outputs from its
+// tensor-memory lane quadrant (warp w: element (w % 4, w / 4), lanes
+// 32 (w % 4) .. + 31, columns 64 (w / 4) ..), scales them by E, and the corner
+// contributions meet in k_lvl_op's exchange buffer and node phase (same fixed
+// summation order). The TMA producer warp, stage ring and bounded waits are
+// k_lvl_op's. 256 tensor-memory columns, allocated and freed by warp 0.
+constexpr int kTcGroups = 5 * 4;                          // node-pair groups per plane: y 0..4, z 0..3
+constexpr int kTcAtom = 1024;                             // one group: 32 realizations x 8 slots (bytes)
+constexpr int kTcPlane = kTcGroups * kTcAtom;             // one half (hi or lo) of a plane
+constexpr int kTcABytes = 2 * 2 * kTcPlane;               // planes P-1 and P, hi and lo: 80 KB
+constexpr int kTcBFloats = 4 * 64 * 8;                    // 4 corner pairs x [B_hi | B_lo] (64) x 8 slots
+constexpr int kTcCols = 256;                              // tensor-memory columns: 4 M tiles x 64
+using TcStage = LvlStage<kLvlPcgZ>;
+constexpr size_t kTcSmem = 1024 + kTcABytes + sizeof(float) * (kTcBFloats + (size_t)kMStages * TcStage::kFloats +
+                                                                2 * (size_t)kMXFloats) +
+                           sizeof(double) * kMJ * kMK * 32 + sizeof(uint64_t) * (2 * kMStages + 1) + 16;
+static_assert(kTcSmem <= 227 * 1024, "tensor-core level operator shared memory");
+static_assert((kTcABytes + sizeof(float) * kTcBFloats) % 128 == 0, "stage ring alignment");
+
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46) | ((uint64_t)(layout & 7u) << 61);
+}
+// instruction descriptor of kind::tf32: FP32 accumulator, A MN-major, B K-major
+__device__ __forceinline__ uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void tc_ld16(uint32_t a, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(a));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_ld8(uint32_t a, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(a));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+// byte offset of (realization r, slot k) in a 1 KB group: 128-byte swizzle
+__device__ __forceinline__ uint32_t tc_slot(int r, int k) {
+  return (uint32_t)(k * 128 + (((r >> 2) ^ k) << 4) + ((r & 3) << 2));
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kMThreads, 1)
+    k_lvl_tc(Lattice L, const float* __restrict__ bops, const __grid_constant__ CUtensorMap tm_a,
+             const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_e,
+             const __grid_constant__ CUtensorMap tm_d, int tiles_j, int n_tiles, int n_items,
+             const uint8_t* __restrict__ mask, const float* __restrict__ alpha, const float* __restrict__ beta,
+             float* __restrict__ out, float* __restrict__ out2, float* __restrict__ d, double* __restrict__ partial,
+             int pstride, int* __restrict__ err) {
+  static_assert(kMode == kLvlPcgZ, "the tensor-core level operator implements the search-direction launch");
+  using S = TcStage;
+  extern __shared__ __align__(1024) unsigned char tc_dyn[];
+  unsigned char* base = tc_dyn + ((1024u - (smem_u32(tc_dyn) & 1023u)) & 1023u);
+  unsigned char* abuf = base;                                             // [plane 2][hi, lo][group 20][1 KB]
+  float* bsm = reinterpret_cast<float*>(base + kTcABytes);                // B operands
+  float* smem = bsm + kTcBFloats;                                         // TMA stage ring
+  float* xbuf = smem + kMStages * S::kFloats;
+  double* red = reinterpret_cast<double*>(xbuf + 2 * kMXFloats);
+  uint64_t* full = reinterpret_cast<uint64_t*>(red + kMJ * kMK * 32);
+  uint64_t* empty = full + kMStages;
+  uint64_t* mma_bar = empty + kMStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_bar + 1);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int NX = L.NX, Rp = L.Rp;
+  // zero both plane buffers (slots 6-7 stay zero), load the B operands
+  for (int i = threadIdx.x; i < kTcABytes / 16; i += blockDim.x)
+    reinterpret_cast<float4*>(abuf)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < kTcBFloats / 4; i += blockDim.x)
+    reinterpret_cast<float4*>(bsm)[i] = reinterpret_cast<const float4*>(bops)[i];
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kMStages; ++st) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], kMWarps);
+    }
+    mbar_init(mma_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (w == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (w == kMWarps) {  // TMA producer (k_lvl_op's)
+    if (lane == 0) {
+      uint32_t seq = 0;
+      for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+        const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
+        for (int P = 1; P <= NX; ++P, ++seq) {
+          const int st = seq % kMStages;
+          const uint32_t use = seq / kMStages;
+          if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
+            atomicExch(err, 1);
+            return;
+          }
+          float* dst = smem + st * S::kFloats;
+          mbar_expect_tx(&full[st], S::kBytes);
+          tma_load_5d(dst + S::kOffA, &tm_a, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_5d(dst + S::kOffB, &tm_b, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
+          tma_load_4d(dst + S::kOffE, &tm_e, g32, P - 1, J0 - 1, K0 - 1, &full[st]);
+          tma_load_5d(dst + S::kOffD, &tm_d, g32, 0, P, J0, K0, &full[st]);
+        }
+      }
+    }
+    return;
+  }
+  const int ej = w % kMEJ, ek = w / kMEJ;
+  const bool node_warp = ej >= 1 && ek >= 1;
+  const uint32_t abase = smem_u32(abuf), bbase = smem_u32(bsm);
+  // tensor-memory address of this warp's element: lanes 32 ej.., columns 64 ek..
+  const uint32_t my_t = tmem + ((uint32_t)(32 * ej) << 16) + (uint32_t)(64 * ek);
+  // nodes this warp forms: its own corner (ej, ek); the warps of the last element
+  // row / column also form the patch edge beyond it (f = 1: +y, 2: +z, 3: +y +z)
+  const bool edge_y = ej == kMEJ - 1, edge_z = ek == kMEK - 1;
+  uint32_t seq = 0, slab = 0;
+  int xsel = 0;
+  bool dead = false;
+  auto csync = [&]() { asm volatile("bar.sync 1, %0;" ::"r"(kMWarps * 32) : "memory"); };
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int tile = item % n_tiles, g32 = (item / n_tiles) * 32;
+    const int J0 = 1 + (tile % tiles_j) * kMJ, K0 = 1 + (tile / tiles_j) * kMK;
+    const int Je = J0 - 1 + ej, Ke = K0 - 1 + ek;
+    auto realj = [&](int j) { return j >= 1 && j <= L.NY - 1; };
+    auto realk = [&](int k) { return k >= 1 && k <= L.NZ - 1; };
+    const bool real = realj(Je) && realk(Ke);
+    const bool node_ok = node_warp && Je <= L.NY && Ke <= L.NZ;
+    const bool r00 = real, r10 = realj(Je - 1) && realk(Ke);
+    const bool r01 = realj(Je) && realk(Ke - 1), r11 = realj(Je - 1) && realk(Ke - 1);
+    const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;
+    const int rr = g32 + lane;
+    const float al = alpha[rr], be = beta[rr];
+    float T0[12];  // plane P-1 corners (ay, az, c) carried from the slab below
+#pragma unroll
+    for (int i = 0; i < 12; ++i) T0[i] = 0.f;
+    float ou[3] = {0.f, 0.f, 0.f};
+    double acc = 0.0;
+    uint32_t mreg = 0;
+    auto node_phase = [&](int X) {
+      if (((X - 1) & 31) == 0) {
+        const int pl = X + lane;
+        mreg = (pl <= NX) ? mask[nrow + pl] : 0u;
+      }
+      const uint32_t mk = __shfl_sync(0xffffffffu, mreg, (X - 1) & 31);
+      const float* xb = xbuf + xsel * kMXFloats;
+      const size_t node = nrow + X;
+      double sacc = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float y = 0.f;
+        if (r00) y += xb[((w * 4 + 0) * 3 + c) * 32 + lane];
+        if (r10) y += xb[(((w - 1) * 4 + 1) * 3 + c) * 32 + lane];
+        if (r01) y += xb[(((w - kMEJ) * 4 + 2) * 3 + c) * 32 + lane];
+        if (r11) y += xb[(((w - kMEJ - 1) * 4 + 3) * 3 + c) * 32 + lane];
+        const size_t o = (node * 3 + c) * Rp + rr;
+        const float v = ((mk >> c) & 1) ? 0.f : y;
+        sacc = fma((double)ou[c], (double)v, sacc);
+        out[o] = v;
+      }
+      acc += sacc;
+    };
+    auto emit_corners = [&]() {
+      float* xb = xbuf + xsel * kMXFloats;
+#pragma unroll
+      for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+        for (int az = 0; az < 2; ++az)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = T0[(ay * 2 + az) * 3 + c];
+    };
+    for (int P = 1; P <= NX; ++P, ++seq) {
+      const int st = seq % kMStages;
+      if (!dead && !mbar_wait(&full[st], (seq / kMStages) & 1)) {
+        atomicExch(err, 1);
+        dead = true;
+      }
+      const float* pt = smem + st * S::kFloats;
+      // form p = z + beta p_old at this warp's nodes of plane P, split into the plane's groups
+      unsigned char* ap = abuf + (P & 1) * 2 * kTcPlane;
+      float own[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        if ((f == 1 && !edge_y) || (f == 2 && !edge_z) || (f == 3 && !(edge_y && edge_z))) continue;
+        const int py = ej + (f & 1), pz = ek + (f >> 1);
+        const int o = pz * kMPJ + py;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const int i = (o * 3 + c) * 32 + lane;
+          const float u = fmaf(be, pt[S::kOffB + i], pt[S::kOffA + i]);
+          const float hi = __uint_as_float(__float_as_uint(u) & 0xffffe000u);
+          const float lo = u - hi;
+          if (f == 0) own[c] = u;
+          if (pz <= 3) {
+            const uint32_t g = (uint32_t)(pz * 5 + py) * kTcAtom + tc_slot(lane, c);
+            *reinterpret_cast<float*>(ap + g) = hi;
+            *reinterpret_cast<float*>(ap + kTcPlane + g) = lo;
+          }
+          if (pz >= 1) {
+            const uint32_t g = (uint32_t)((pz - 1) * 5 + py) * kTcAtom + tc_slot(lane, 3 + c);
+            *reinterpret_cast<float*>(ap + g) = hi;
+            *reinterpret_cast<float*>(ap + kTcPlane + g) = lo;
+          }
+        }
+      }
+      if (node_ok) {  // the owner writes p and d += alpha p_old (k_lvl_op<kLvlPcgZ>)
+        const size_t node = nrow + P;
+        const int op = ek * kMPJ + ej, od = (ek - 1) * kMJ + (ej - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const size_t o = (node * 3 + c) * Rp + rr;
+          const float pold = pt[S::kOffB + (op * 3 + c) * 32 + lane];
+          out2[o] = own[c];
+          d[o] = fmaf(al, pold, pt[S::kOffD + (od * 3 + c) * 32 + lane]);
+        }
+      }
+      const float E = pt[S::kOffE + w * 32 + lane];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      // the plane's groups (generic-proxy writes) become visible to the tensor core
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      csync();
+      if (P >= 2) {
+        if (w == 0 && lane == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+          for (int t = 0; t < 4; ++t)      // M tile: the z row of element pencils
+#pragma unroll
+            for (int pr = 0; pr < 4; ++pr) {  // corner pair (ax, ay)
+              const int ax = pr >> 1, ay = pr & 1;
+              const uint32_t pa = abase + (uint32_t)((P - 1 + ax) & 1) * 2 * kTcPlane + (uint32_t)(t * 5 + ay) * kTcAtom;
+              const uint32_t pb = bbase + (uint32_t)pr * 64 * 8 * 4;
+              const uint64_t db = tc_sdesc(pb, 128, 256, 0);
+              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa, kTcAtom, kTcAtom, 2), db, tc_idesc(128, 64), pr > 0);
+              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa + kTcPlane, kTcAtom, kTcAtom, 2), db, tc_idesc(128, 32),
+                     1u);
+            }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                           smem_u32(mma_bar))
+                       : "memory");
+        }
+        bool ok = !dead && mbar_wait(mma_bar, slab & 1);
+        ++slab;
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) {
+          if (lane == 0) atomicExch(err, 1);
+          dead = true;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        float y[24];
+        if (ok) {
+          float a16[16], a8[8], b16[16], b8[8];
+          tc_ld16(my_t, a16);
+          tc_ld8(my_t + 16, a8);
+          tc_ld16(my_t + 32, b16);
+          tc_ld8(my_t + 48, b8);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int i = 0; i < 16; ++i) y[i] = E * (a16[i] + b16[i]);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) y[16 + i] = E * (a8[i] + b8[i]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 24; ++i) y[i] = 0.f;
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        if (real) {
+#pragma unroll
+          for (int i = 0; i < 12; ++i) T0[i] += y[i];
+          emit_corners();
+        }
+#pragma unroll
+        for (int i = 0; i < 12; ++i) T0[i] = y[12 + i];
+        csync();
+        if (node_ok) node_phase(P - 1);
+        xsel ^= 1;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ou[c] = own[c];
+    }
+    if (real) emit_corners();
+    csync();
+    if (node_ok) node_phase(NX);
+    xsel ^= 1;
+    if (partial != nullptr) {
+      if (node_warp) red[((ek - 1) * kMJ + (ej - 1)) * 32 + lane] = acc;
+      csync();
+      if (w == 0) {
+        double sum = 0.0;
+#pragma unroll
+        for (int i = 0; i < kMJ * kMK; ++i) sum += red[i * 32 + lane];
+        partial[((size_t)tile * Rp + rr) * pstride] = sum;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  csync();
+  if (w == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
+  }
+}
+
 // ---------------------------------------------------------------- coarsest-level sweeps
 // All damped Jacobi sweeps of the coarsest level in one launch. That level has
 // at most 3 x 3 node pencils in (y, z), one k_lvl_op tile, so a CTA holds the
@@ -2862,7 +3207,56 @@ struct BlockSys {
   int tiles_j2 = 0, n_tiles2 = 0, n_items2 = 0, grid2 = 0;
   CUtensorMap tm2_rA, tm2_rB, tm2_qA, tm2_qB, tm2_pA, tm2_pB, tm2_xs, tm2_dinv, tm2_e, tm2_d;
   CUtensorMap tm2_rAo, tm2_rBo, tm2_dinvo;  // own-tile boxes of r (both buffers) and dinv (post-sweep)
+  // level-0 search-direction launch on the tensor cores (k_lvl_tc): the B operand
+  // image of cK Khat (4 corner pairs x [hi | lo] x 8 slots, K-major core matrices)
+  bool tc = false;
+  WSlot tc_bops;
 };
+
+// B operands of k_lvl_tc from the unit-cube element matrix: for corner pair
+// (ax, ay) = pr, row n < 32 holds the TF32 high part and row 32 + n the low
+// part of output column n = ((ax' 2 + ay') 2 + az') 3 + c' (n < 24; rows 24..31
+// zero), slot k = az 3 + c (k < 6; slots 6, 7 zero) of cK Khat; K-major core
+// matrices of 8 rows x 4 slots (LBO 128 B between the slot halves, SBO 256 B
+// between 8-row groups), 2 KB per pair. Uploaded into workspace slot 33.
+static int tc_setup(Context* ctx, BlockSys* B, const double* K576) {
+  std::vector<float> img(kTcBFloats, 0.f);
+  auto trunc_tf32 = [](float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u &= 0xffffe000u;
+    float y;
+    std::memcpy(&y, &u, 4);
+    return y;
+  };
+  for (int pr = 0; pr < 4; ++pr) {
+    const int ax = pr >> 1, ay = pr & 1;
+    for (int n = 0; n < 24; ++n) {
+      const int c2 = n % 3, az2 = (n / 3) & 1, ay2 = (n / 6) & 1, ax2 = n / 12;
+      const int row = corner_id(ax2, ay2, az2) * 3 + c2;
+      for (int k = 0; k < 6; ++k) {
+        const int az = k / 3, c = k % 3;
+        const float f = (float)(B->cK * K576[row * 24 + corner_id(ax, ay, az) * 3 + c]);
+        const float hi = trunc_tf32(f), lo = f - hi;
+        for (int h = 0; h < 2; ++h) {
+          const int nn = n + 32 * h;
+          img[pr * 512 + (nn / 8) * 64 + (k / 4) * 32 + (nn % 8) * 4 + (k % 4)] = h ? lo : hi;
+        }
+      }
+    }
+  }
+  MSG_TRY(B->slot_alloc(ctx, 33, sizeof(float) * img.size(), &B->tc_bops.ptr));
+  MSG_CUDA(ctx, cudaMemcpyAsync(B->tc_bops.ptr, img.data(), sizeof(float) * img.size(), cudaMemcpyHostToDevice,
+                                B->X.st));
+  MSG_CUDA(ctx, cudaStreamSynchronize(B->X.st));
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [] {
+    attr = cudaFuncSetAttribute(k_lvl_tc<kLvlPcgZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  });
+  MSG_CUDA(ctx, attr);
+  return MSG_OK;
+}
 
 // Largest eigenvalue of diag(K)^-1 K for one element (power iteration on the
 // symmetric D^-1/2 K D^-1/2 from a fixed vector with no rigid-body part). It
@@ -3262,6 +3656,9 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
           MSG_CUDA(ctx, cs_err);
         }
       }
+      // level-0 search direction on the tensor cores (no mass term)
+      B->tc = ctx->tensor_op != 0 && !B->mass;
+      if (B->tc) MSG_TRY(tc_setup(ctx, B, K576));
       // packed level-0 operator: realizations in multiples of 64
       B->pack = ctx->mg_packed && (Rp % kQR) == 0;
       if (B->pack) {
@@ -3556,8 +3953,14 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   k_gmg_beta<<<c.sblocks, 1024, 0, st>>>(Rp, nt0, part2, s, c.delta2, c.tol2);
   // p = z + beta p_old, d += alpha p_old, q = A p, partial p.q
   if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-  lvl0(PcgZ{}, B->tm_qBm, tm_pin, B->tm2_qB, even ? B->tm2_pA : B->tm2_pB, nullptr, nullptr, B->q.as<float>(), p_out,
-       nullptr, B->d.as<float>(), part1, 1);
+  if (B->tc) {
+    k_lvl_tc<kLvlPcgZ><<<B->grid_m, kMThreads, kTcSmem, st>>>(
+        B->L, B->tc_bops.as<float>(), B->tm_qBm, tm_pin, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m, B->n_items_m,
+        B->mask, s.alpha, s.beta, B->q.as<float>(), p_out, B->d.as<float>(), part1, 1, s.err);
+  } else {
+    lvl0(PcgZ{}, B->tm_qBm, tm_pin, B->tm2_qB, even ? B->tm2_pA : B->tm2_pB, nullptr, nullptr, B->q.as<float>(), p_out,
+         nullptr, B->d.as<float>(), part1, 1);
+  }
   if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
   k_gmg_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, nt0, part1, s);
   if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
@@ -3606,7 +4009,7 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
     }
     const int mm[6] = {modal ? 1 : 0, B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
     mix(mm, sizeof(mm));
-    const int gg[4] = {B->gmg ? 1 : 0, B->n_lvl, B->sweeps, B->pack ? 1 : 0};
+    const int gg[5] = {B->gmg ? 1 : 0, B->n_lvl, B->sweeps, B->pack ? 1 : 0, B->tc ? 1 : 0};
     mix(gg, sizeof(gg));
     if (B->gmg) {
       mix(&B->omega, sizeof(B->omega));
