@@ -104,8 +104,6 @@ def parse():
                    help="MSG_SET_OPTION multigrid_packed (0: level operators on 32-realization tiles)")
     p.add_argument("--tensor-op", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION tensor_operator (1: level-0 search-direction launch on the tensor cores)")
-    p.add_argument("--modal-operator", type=int, default=None, choices=[0, 1],
-                   help="MSG_SET_OPTION modal_operator (1: Walsh-mode FP32 operator, 0: dense value-class stencil)")
     return p.parse_args()
 
 
@@ -475,8 +473,6 @@ def main():
         ctx.set_option("reliable_delta", args.reliable_delta)
     if args.chunk is not None:
         ctx.set_option("chunk", args.chunk)
-    if args.modal_operator is not None:
-        ctx.set_option("modal_operator", args.modal_operator)
     if args.tensor_op is not None:
         ctx.set_option("tensor_operator", args.tensor_op)
     if args.multigrid is not None:
@@ -524,8 +520,8 @@ def main():
     # loop configuration (tile shapes, preconditioner) picked by the project's autotuner
     # on this rank's own batch, unless an option was forced on the command line
     tuned = None
-    forced = any(v is not None for v in (args.multigrid, args.mg_levels, args.chunk, args.modal_operator,
-                                         args.mg_packed, args.tensor_op))
+    forced = any(v is not None for v in (args.multigrid, args.mg_levels, args.chunk, args.mg_packed,
+                                         args.tensor_op))
     if not args.no_autotune and not forced:
         from msolve_b200.tuning import Autotuner
         tuner = Autotuner(ctx, args.autotune_cache)

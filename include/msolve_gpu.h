@@ -362,9 +362,7 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
 /* Tunables of the mixed solver on this context: "reliable_delta" (the FP32
  * recursive residual may fall by this factor before it is replaced by the FP64
  * true residual, default 0.1), "chunk" (FP32 iterations per CUDA-graph launch,
- * even, default 16), "modal_operator" (1: the FP32 operator works on the
- * element's Walsh modes, default; 0: dense value-class stencil),
- * "fixed_updates" (1: the FP64 true-residual step runs after every chunk for
+ * even, default 16), "fixed_updates" (1: the FP64 true-residual step runs after every chunk for
  * every realization, so each realization's arithmetic no longer depends on the
  * rest of the batch: bitwise identical alone or batched; default 0: the step
  * runs when some realization asks for it), "multigrid" (preconditioner of the
@@ -388,7 +386,11 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * can run between the work items), "serve_priority" (serving lanes created
  * afterwards: 0, default, equal stream priorities; 1: priority grows as the
  * model shrinks, shortest solves first: with serve_persistent = 0 small
- * models' latency under load halves while the largest models wait longer).
+ * models' latency under load halves while the largest models wait longer),
+ * "tensor_operator" (0, default: every element product in the element's Walsh
+ * modes on the FP32 cores; 1: the multigrid loop's level-0 search-direction
+ * launch forms E_e Khat u_e on the tensor cores, tcgen05.mma in TF32 with a
+ * three-term split; systems without a mass term).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

@@ -15,29 +15,21 @@
 // checks. A warp is 32 realizations of one node: every access is one coalesced
 // 128-byte line and per-realization dot products need no cross-lane reduction.
 //
-// Operator kernel: one warp walks a pencil of nodes along x, streaming x-planes
-// of p: each plane (3x3 nodes x 3 components, 27 coalesced loads) and the 4 new
-// elements of its slab feed the partial outputs of the three nodes P-1, P, P+1
-// through the two adjacent element slabs, 8 x (4 x 9) FMAs per plane against
-// Khat. Khat enters as its 10 value classes held in registers; the class and
-// sign of every entry are compile-time constants (khat_classes.h), so each
-// FMA takes a register operand with a free sign modifier and no constant-bank
-// traffic. Only one plane, three partial outputs and two E slabs
-// are live in registers. Each output is written once: no atomics; results are
-// deterministic and independent of the batch mix.
+// Operator kernels (k_op_modal, k_lvl_op, k_lvl_op2, k_resid_modal): a CTA owns
+// a tile of node pencils along x and walks the x-planes, staging each plane's
+// patch with TMA; the element product is applied in the element's Walsh modes
+// (below), and the four elements around a node meet in a shared-memory
+// exchange buffer in fixed order. Each output is written once: no atomics;
+// results are deterministic and independent of the batch mix. k_lvl_tc applies
+// the same product on the tensor cores (option "tensor_operator").
 //
-// Solver: FP32 Jacobi-PCG with reliable updates. Per iteration k
-//   k_dir    : d += alpha_{k-1} p_{k-1}, p_k = dinv.r + beta_k p_{k-1} (in place)
-//   k_op     : q = K p_k (FP32, masked), partial p.q
-//   k_alpha  : alpha_k = (z.r)/(p.q) per realization
-//   k_update : r -= alpha_k q, partials (dinv r).r and r.r
-//   k_beta   : beta, and a request for a reliable update when ||r|| has
-//              dropped by `reliable_delta` since the last true residual
-// captured as one CUDA graph of `chunk` iterations. Reliable update (FP64):
-//   x += d + alpha p (the pending term), d = 0, r = b - K x with the FP64
-//   operator (k_resid), true
-//   ||r||/||b|| < tol ends a realization; otherwise the search direction is
-//   kept (beta = gamma_new / gamma_prev), so the Krylov progress survives.
+// Solvers: the single-reduction FP32 Jacobi-PCG loop (k_op_modal +
+// k_alpha_gamma per iteration) and the multigrid-preconditioned loop
+// (gmg_iteration), each captured as one CUDA graph of `chunk` iterations, with
+// reliable updates in FP64: x += d + alpha p (the pending term), d = 0,
+// r = b - K x with the FP64 Walsh-mode operator (k_resid_modal); a true
+// ||r||/||b|| < tol ends a realization, otherwise the search direction is kept
+// (beta = gamma_new / gamma_prev), so the Krylov progress survives.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -297,25 +289,9 @@ __global__ void k_pc_gather(int n_dofs, int P, int Pp, const int* __restrict__ r
   if (d < n_dofs && j < P) out[(size_t)j * n_dofs + d] = in[(size_t)rows[d] * Pp + j];
 }
 
-// ---------------------------------------------------------------- TMA-staged FP32 operator
-// The production FP32 operator. A CTA owns a 2x2 tile of pencils (one warp
-// each) for 32 realizations. For every x-plane P one thread issues two TMA
-// tensor loads (no multicast) into a 4-stage shared-memory ring: the plane's
-// 4x4 node patch (32 realizations x 3 components, 6 KB: the tile plus its
-// one-node halo) and the 3x3 element patch of the slab with lower corner x = P
-// (1.1 KB). A "full" mbarrier per stage counts the bytes; an "empty" mbarrier
-// per stage collects one arrival per warp once the warp has read the stage, and
-// the producer refills a stage one plane after it was consumed. Warps read
-// their 3x3 neighbours at compile-time shared-memory offsets. Every wait is
-// bounded: on expiry the kernel raises *err and stops streaming.
-constexpr int kStages = 4;
-constexpr int kPJ = kTJ + 2, kPK = kTK + 2;              // plane patch (nodes)
-constexpr int kEJ = kTJ + 1, kEK = kTK + 1;              // element patch
-constexpr int kPlaneFloats = 32 * 3 * kPJ * kPK;         // 1536
-constexpr int kEFloats = 32 * kEJ * kEK;                 // 288
-constexpr int kStageFloats = kPlaneFloats + kEFloats;    // 7296 bytes, a multiple of 128
-constexpr uint32_t kStageBytes = kStageFloats * 4;
-constexpr size_t kOpSmem = 128 + (size_t)kStages * kStageBytes + 2 * kStages * sizeof(uint64_t);
+// ---------------------------------------------------------------- mbarrier and TMA helpers
+// Every wait on an mbarrier is bounded: on expiry the kernel raises *err and
+// stops streaming (the host reads the flag and returns MSG_ERR_TIMEOUT).
 constexpr long kWaitLimit = 1L << 24;                    // try_wait polls before giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -373,129 +349,6 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, in
       "[%6];" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
       : "memory");
-}
-
-constexpr int kOpThreads = 32 * (kWarps + 1);  // 4 consumer warps + 1 TMA producer warp
-
-__global__ void __launch_bounds__(kOpThreads, 4)
-    k_op_tma(Lattice L, const __grid_constant__ KhatF K, const __grid_constant__ CUtensorMap tm_p,
-             const __grid_constant__ CUtensorMap tm_e, const uint8_t* __restrict__ mask, float* __restrict__ q,
-             double* __restrict__ partial, int* __restrict__ err) {
-  extern __shared__ __align__(128) float smem_dyn[];
-  // 128-byte aligned stage ring (TMA destinations), then the mbarriers; the
-  // offset is applied to the shared-memory pointer so reads stay in the shared space
-  float* smem = smem_dyn + (((128u - (smem_u32(smem_dyn) & 127u)) & 127u) >> 2);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageFloats);
-  uint64_t* empty = full + kStages;
-  __shared__ double red[kWarps][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int tile = blockIdx.x;
-  const int tj = tile % L.tiles_j, tk = tile / L.tiles_j;
-  const int J0 = 1 + tj * kTJ, K0 = 1 + tk * kTK;  // padded coordinates of the tile's first pencil
-  const int Rp = L.Rp, g32 = blockIdx.y * 32, rr = g32 + lane;
-  const int NX = L.NX;
-  if (threadIdx.x == 0) {
-    for (int st = 0; st < kStages; ++st) {
-      mbar_init(&full[st], 1);
-      mbar_init(&empty[st], kWarps);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (w == kWarps) {
-    // producer warp: plane P into stage (P-1) % kStages once its previous use is consumed
-    if (lane == 0) {
-      for (int P = 1; P <= NX; ++P) {
-        const int st = (P - 1) % kStages, use = (P - 1) / kStages;
-        if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1)) {
-          atomicExch(err, 1);
-          break;
-        }
-        float* dst = smem + st * kStageFloats;
-        mbar_expect_tx(&full[st], kStageBytes);
-        tma_load_5d(dst, &tm_p, g32, 0, P, J0 - 1, K0 - 1, &full[st]);
-        tma_load_4d(dst + kPlaneFloats, &tm_e, g32, P, J0 - 1, K0 - 1, &full[st]);
-      }
-    }
-  } else {
-    const int jy = w % kTJ, kz = w / kTJ;
-    const int J = J0 + jy, Kz = K0 + kz;
-    const bool valid = J <= L.NY && Kz <= L.NZ;
-    float kv[kKhatClasses];
-#pragma unroll
-    for (int i = 0; i < kKhatClasses; ++i) kv[i] = K.v[i];
-    const size_t row0 = (size_t)(J + L.NYp * Kz) * L.NXp;
-    float ym[3] = {0.f, 0.f, 0.f}, y0[3] = {0.f, 0.f, 0.f}, yp[3];
-    float Eprev[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-    float own_m[3] = {0.f, 0.f, 0.f};
-    double pq = 0.0;
-    bool ok = true;
-    auto emit = [&](size_t node, const float* ownv, const float* y) {
-      const uint8_t m = mask[node];
-      float acc = 0.f;
-      float* qn = q + node * 3 * Rp + rr;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float qc = ((m >> c) & 1) ? 0.f : y[c];
-        qn[c * Rp] = qc;
-        acc = fmaf(ownv[c], qc, acc);
-      }
-      pq += (double)acc;
-    };
-#pragma unroll 1
-    for (int P = 1; P <= NX; ++P) {
-      const int st = (P - 1) % kStages;
-      if (!mbar_wait(&full[st], ((P - 1) / kStages) & 1)) {
-        atomicExch(err, 1);
-        ok = false;
-        break;
-      }
-      const float* pt = smem + st * kStageFloats;
-      const float* et = pt + kPlaneFloats;
-      float pl[3][3][3];
-#pragma unroll
-      for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-        for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) pl[dy][dz][c] = pt[(((kz + dz) * kPJ + (jy + dy)) * 3 + c) * 32 + lane];
-      float Ecur[2][2];
-#pragma unroll
-      for (int ey = 0; ey < 2; ++ey)
-#pragma unroll
-        for (int ez = 0; ez < 2; ++ez) Ecur[ey][ez] = et[((kz + ez) * kEJ + (jy + ey)) * 32 + lane];
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[st]);
-      if (valid) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) yp[c] = 0.f;
-        slab_apply<float, 1, 0>(kv, pl, Ecur, yp);
-        slab_apply<float, 0, 0>(kv, pl, Ecur, y0);
-        slab_apply<float, 1, 1>(kv, pl, Eprev, y0);
-        slab_apply<float, 0, 1>(kv, pl, Eprev, ym);
-        if (P > 1) emit(row0 + P - 1, own_m, ym);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          ym[c] = y0[c];
-          y0[c] = yp[c];
-          own_m[c] = pl[1][1][c];
-        }
-#pragma unroll
-        for (int ey = 0; ey < 2; ++ey)
-#pragma unroll
-          for (int ez = 0; ez < 2; ++ez) Eprev[ey][ez] = Ecur[ey][ez];
-      }
-    }
-    if (ok && valid) emit(row0 + NX, own_m, ym);
-    red[w][lane] = pq;
-  }
-  __syncthreads();  // also keeps the CTA (and its shared memory) alive until every copy has landed
-  if (w == 0) {
-    double s = 0;
-#pragma unroll
-    for (int ww = 0; ww < kWarps; ++ww) s += red[ww][lane];
-    partial[(size_t)tile * Rp + rr] = s;
-  }
 }
 
 // ---------------------------------------------------------------- modal FP32 operator
@@ -2331,46 +2184,6 @@ __global__ void __launch_bounds__(128) k_coarsen_E(Lattice Lf, Lattice Lc, int n
   }
 }
 
-// FP64 true residual: r = b - A x (masked), r32 = (float) r; partials ||r||^2
-// and (dinv r32).r32. A = E Khat (+ Mhat on real elements when kMass); b is
-// one vector for the batch (b[node*3 + c]) or, with kBPerR, one per
-// realization in the batch layout.
-template <bool kMass, bool kBPerR>
-__global__ void __launch_bounds__(128)
-    k_resid(Lattice L, const __grid_constant__ KhatD K, const __grid_constant__ MassClasses<double> M,
-            const double* __restrict__ x, const double* __restrict__ b_lat, const double* __restrict__ E,
-            const uint8_t* __restrict__ mask, const float* __restrict__ dinv, float* __restrict__ r32,
-            double* __restrict__ partial) {
-  int J, Kz;
-  bool valid;
-  pencil_of(L, J, Kz, valid);
-  const int Rp = L.Rp;
-  const int rr = blockIdx.y * 32 + threadIdx.x;
-  double acc[2] = {0.0, 0.0};
-  if (valid) {
-    auto emit = [&](size_t node, const double*, const double* y) {
-      const uint8_t m = mask[node];
-      const double dv = (double)dinv[node * Rp + rr];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double bv = kBPerR ? b_lat[(node * 3 + c) * Rp + rr] : b_lat[node * 3 + c];
-        const double rc = ((m >> c) & 1) ? 0.0 : bv - y[c];
-        const float rf = (float)rc;
-        r32[(node * 3 + c) * Rp + rr] = rf;
-        acc[0] += rc * rc;
-        acc[1] += dv * (double)rf * (double)rf;
-      }
-    };
-    auto load = [&](size_t node, double* o) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) o[c] = ldv(x + (node * 3 + c) * Rp + rr);
-    };
-    auto own = [](size_t, const double*) {};
-    pencil_sweep<double, kMass>(L, K, J, Kz, E + rr, load, own, emit, &M);
-  }
-  cta_partial<2>(acc, partial, blockIdx.x, Rp, rr);
-}
-
 // FP64 operator application y (+)= (E Khat + Mhat on real elements) x, no
 // mask, batch layout (the Newmark right-hand side).
 template <bool kAccumulate>
@@ -2420,140 +2233,6 @@ __global__ void k_dinv(Lattice L, double kdiag, double mdiag, const float* __res
   }
 }
 
-// Elementwise passes over interior nodes, one float4 of realizations per
-// thread. Partial sums per CTA: [blk][Rp][2].
-struct Quad {
-  int Q, G, g, qb0, qstep;
-  __device__ Quad(int Rp) {
-    Q = Rp >> 2;
-    G = Q >= 256 ? 1 : 256 / Q;
-    g = Q >= 256 ? 0 : threadIdx.x / Q;
-    qb0 = Q >= 256 ? threadIdx.x : threadIdx.x % Q;
-    qstep = Q >= 256 ? 256 : Q;
-  }
-  __device__ bool live() const { return Q >= 256 || (int)threadIdx.x < G * Q; }
-};
-
-// Start of PCG iteration k (interior nodes, in place): d += alpha_{k-1} p_{k-1}
-// (the previous iteration's correction) and p_k = dinv.r_k + beta_k p_{k-1}.
-__global__ void __launch_bounds__(256) k_dir(int n_int, int Rp, const int* __restrict__ interior,
-                                             const float* __restrict__ alpha, const float* __restrict__ beta,
-                                             const float* __restrict__ r, const float* __restrict__ dinv,
-                                             float* __restrict__ p, float* __restrict__ d) {
-  Quad qd(Rp);
-  if (!qd.live()) return;
-  const int per = (n_int + gridDim.x - 1) / gridDim.x;
-  const int t0 = blockIdx.x * per, t1 = min(n_int, t0 + per);
-  for (int qb = qd.qb0; qb < qd.Q; qb += qd.qstep) {
-    const float4 a4 = reinterpret_cast<const float4*>(alpha)[qb];
-    const float4 b4 = reinterpret_cast<const float4*>(beta)[qb];
-    for (int t = t0 + qd.g; t < t1; t += qd.G) {
-      const size_t n = (size_t)interior[t];
-      const float4 dv = reinterpret_cast<const float4*>(dinv + n * Rp)[qb];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const size_t o = (n * 3 + c) * Rp;
-        const float4 rv = reinterpret_cast<const float4*>(r + o)[qb];
-        float4 pv = reinterpret_cast<const float4*>(p + o)[qb];
-        float4 dd = reinterpret_cast<const float4*>(d + o)[qb];
-        dd.x = fmaf(a4.x, pv.x, dd.x); dd.y = fmaf(a4.y, pv.y, dd.y);
-        dd.z = fmaf(a4.z, pv.z, dd.z); dd.w = fmaf(a4.w, pv.w, dd.w);
-        pv.x = fmaf(dv.x, rv.x, b4.x * pv.x); pv.y = fmaf(dv.y, rv.y, b4.y * pv.y);
-        pv.z = fmaf(dv.z, rv.z, b4.z * pv.z); pv.w = fmaf(dv.w, rv.w, b4.w * pv.w);
-        reinterpret_cast<float4*>(p + o)[qb] = pv;
-        reinterpret_cast<float4*>(d + o)[qb] = dd;
-      }
-    }
-  }
-}
-
-// r -= alpha q on free components (constrained components of r stay zero);
-// partials (dinv r).r and r.r per realization (interior nodes).
-__global__ void __launch_bounds__(256) k_update(int n_int, int Rp, const int* __restrict__ interior,
-                                                const uint8_t* __restrict__ mask, const float* __restrict__ alpha,
-                                                const float* __restrict__ q, float* __restrict__ r,
-                                                const float* __restrict__ dinv, double* __restrict__ partial) {
-  Quad qd(Rp);
-  const int per = (n_int + gridDim.x - 1) / gridDim.x;
-  const int t0 = blockIdx.x * per, t1 = min(n_int, t0 + per);
-  extern __shared__ double sh[];  // [G][Q][8] when G > 1
-  if (qd.live()) {
-    for (int qb = qd.qb0; qb < qd.Q; qb += qd.qstep) {
-      const float4 a4 = reinterpret_cast<const float4*>(alpha)[qb];
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int t = t0 + qd.g; t < t1; t += qd.G) {
-        const size_t n = (size_t)interior[t];
-        const uint8_t mk = mask[n];
-        const float4 dv = reinterpret_cast<const float4*>(dinv + n * Rp)[qb];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const size_t o = (n * 3 + c) * Rp;
-          float4 rv = reinterpret_cast<const float4*>(r + o)[qb];
-          if (!((mk >> c) & 1)) {
-            const float4 qv = reinterpret_cast<const float4*>(q + o)[qb];
-            rv.x = fmaf(-a4.x, qv.x, rv.x); rv.y = fmaf(-a4.y, qv.y, rv.y);
-            rv.z = fmaf(-a4.z, qv.z, rv.z); rv.w = fmaf(-a4.w, qv.w, rv.w);
-            reinterpret_cast<float4*>(r + o)[qb] = rv;
-          }
-          acc[0] += (double)(dv.x * rv.x * rv.x); acc[4] += (double)(rv.x * rv.x);
-          acc[1] += (double)(dv.y * rv.y * rv.y); acc[5] += (double)(rv.y * rv.y);
-          acc[2] += (double)(dv.z * rv.z * rv.z); acc[6] += (double)(rv.z * rv.z);
-          acc[3] += (double)(dv.w * rv.w * rv.w); acc[7] += (double)(rv.w * rv.w);
-        }
-      }
-      if (qd.G == 1) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const size_t o = ((size_t)blockIdx.x * Rp + 4 * qb + u) * 2;
-          partial[o] = acc[u];
-          partial[o + 1] = acc[4 + u];
-        }
-      } else {
-#pragma unroll
-        for (int u = 0; u < 8; ++u) sh[((size_t)qd.g * qd.Q + qb) * 8 + u] = acc[u];
-      }
-    }
-  }
-  if (qd.G > 1) {
-    __syncthreads();
-    for (int qb = threadIdx.x; qb < qd.Q; qb += 256) {
-      double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      for (int gg = 0; gg < qd.G; ++gg)
-#pragma unroll
-        for (int u = 0; u < 8; ++u) s[u] += sh[((size_t)gg * qd.Q + qb) * 8 + u];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const size_t o = ((size_t)blockIdx.x * Rp + 4 * qb + u) * 2;
-        partial[o] = s[u];
-        partial[o + 1] = s[4 + u];
-      }
-    }
-  }
-}
-
-// x += d + alpha p (the correction, with the last iteration's term still
-// pending), d = 0 (interior nodes; FP64 solution, FP32 correction)
-__global__ void __launch_bounds__(256) k_xupdate(int n_int, int Rp, const int* __restrict__ interior,
-                                                 const float* __restrict__ alpha, const float* __restrict__ p,
-                                                 double* __restrict__ x, float* __restrict__ d) {
-  const int Q = Rp >> 1;  // float2 / double2 per thread
-  const size_t total = (size_t)n_int * 3 * Q;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const size_t row = i / Q;
-    const int qb = (int)(i - row * Q);
-    const size_t node = (size_t)interior[row / 3];
-    const size_t o = (node * 3 + row % 3) * Rp;
-    const float2 a2 = reinterpret_cast<const float2*>(alpha)[qb];
-    const float2 pv = reinterpret_cast<const float2*>(p + o)[qb];
-    const float2 dv = reinterpret_cast<const float2*>(d + o)[qb];
-    double2 xv = reinterpret_cast<double2*>(x + o)[qb];
-    xv.x += (double)fmaf(a2.x, pv.x, dv.x);
-    xv.y += (double)fmaf(a2.y, pv.y, dv.y);
-    reinterpret_cast<double2*>(x + o)[qb] = xv;
-    reinterpret_cast<float2*>(d + o)[qb] = make_float2(0.f, 0.f);
-  }
-}
-
 struct Scal {
   float* alpha;        // [Rp]
   float* beta;         // [Rp]
@@ -2596,59 +2275,6 @@ __device__ __forceinline__ void reduce_rows(const double* __restrict__ partial, 
 #pragma unroll 4
     for (int gg = 0; gg < 32; ++gg) s += sh[gg][q][lane];
     out[q] = s;
-  }
-}
-
-__global__ void __launch_bounds__(1024) k_alpha(int Rp, int n_tiles, const double* __restrict__ partial, Scal s) {
-  double v[1];
-  reduce_rows<1>(partial, n_tiles, Rp, v);
-  if (threadIdx.x >= 32) return;
-  const int r = blockIdx.x * 32 + threadIdx.x;
-  const double pq = v[0];
-  float a = 0.f;
-  if (s.act[r]) {
-    if (!(pq > 0.0)) {
-      s.act[r] = 0;
-      s.breakdown[r] = 1;
-    } else {
-      a = (float)(s.gamma[r] / pq);
-      s.its[r] += 1;
-    }
-  }
-  s.alpha[r] = a;
-}
-
-// beta = gamma_new / gamma; request a reliable update once r.r has dropped by
-// delta^2 since the last one, or below the convergence threshold.
-__global__ void __launch_bounds__(1024) k_beta(int Rp, int n_blk, const double* __restrict__ partial, Scal s,
-                                               double delta2, double tol2) {
-  double v[2];
-  reduce_rows<2>(partial, n_blk, Rp, v);
-  const int r = blockIdx.x * 32 + threadIdx.x;
-  int active = 0, upd = 0;
-  if (threadIdx.x < 32) {
-    const double g = v[0], rho = v[1];
-    float b = 0.f;
-    if (s.act[r]) {
-      if (!(rho == rho) || !(g == g)) {
-        s.act[r] = 0;
-        s.breakdown[r] = 1;
-      } else {
-        b = (float)(g / s.gamma[r]);
-        s.gamma_prev[r] = s.gamma[r];
-        s.gamma[r] = g;
-        active = 1;
-        const double bn = s.bnorm[r];
-        upd = (rho < delta2 * s.rho_ref[r] || rho < tol2 * bn * bn) ? 1 : 0;
-      }
-    }
-    s.beta[r] = b;
-  }
-  active = __syncthreads_count(active);
-  upd = __syncthreads_count(upd);
-  if (threadIdx.x == 0) {
-    if (active) atomicAdd(s.n_active, active);
-    if (upd) atomicAdd(s.n_update, upd);
   }
 }
 
@@ -3168,7 +2794,6 @@ struct BlockSys {
   int n_tiles = 0, tiles_jm = 0, n_tiles_m = 0, n_items_m = 0, grid_m = 0, n_upd = 0, n_bsq = 0;
   bool modal = true, mass = false;
   double cK = 1.0, cM = 0.0, kdiag = 0.0, mdiag = 0.0;
-  KhatF KF;
   KhatD KD;               // cK-scaled classes
   MassClasses<double> MD; // cM-scaled mass classes
   ModalC MC;
@@ -3186,7 +2811,7 @@ struct BlockSys {
     *out = own[slot].ptr;
     return MSG_OK;
   }
-  CUtensorMap tm_p, tm_e, tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
+  CUtensorMap tm_rAm, tm_rBm, tm_qAm, tm_qBm, tm_pAm, tm_pBm, tm_dinvm, tm_em, tm_dm;
   // FP64 Walsh-mode true-residual step (modal loops): the iterate alternates
   // between x and xB (the step writes x + d + alpha p into the other buffer)
   WSlot xB;
@@ -3353,9 +2978,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   B->cK = cK;
   B->cM = cM;
   B->mass = cM != 0.0;
-  B->modal = ctx->modal != 0;
-  if (B->mass && !B->modal)
-    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "a mass term needs the modal operator (modal_operator = 1)");
+  B->modal = true;  // the Walsh-mode operator (every batched loop)
   cudaStream_t st = B->X.st;
 
   double K576[576];
@@ -3363,7 +2986,6 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
   for (int c = 0; c < kKhatClasses; ++c) {
     const double v = K576[kKhatRep[c]];
     B->KD.v[c] = cK * v;
-    B->KF.v[c] = (float)(cK * v);
   }
   for (int i = 0; i < 576; ++i) {  // the element must have the cube's class structure
     const int code = kKhatClass[i];
@@ -3542,11 +3164,6 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
         attr_err = cudaFuncSetAttribute(k_op_modal<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMSmem);
     });
     MSG_CUDA(ctx, attr_err);
-  } else {
-    const cuuint32_t pb[5] = {32, 3, 1, kPJ, kPK};
-    const cuuint32_t eb[4] = {32, 1, kEJ, kEK};
-    const CUresult r1 = enc5(&B->tm_p, B->p.ptr, pb), r2 = enc4(&B->tm_e, B->E32.ptr, eb);
-    e = r1 != CUDA_SUCCESS ? r1 : r2;
   }
   if (e != CUDA_SUCCESS) return set_error(ctx, MSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
 
@@ -3797,22 +3414,14 @@ int block_field(Context* ctx, Mesh* m, BlockSys* B, const KLDevice* kl, const do
 // Launch geometry and tolerances shared by the inner-loop graph and the
 // true-residual step of a batch.
 struct LoopCfg {
-  dim3 op_grid, op_block;
-  size_t upd_smem = 0;
-  int sblocks = 0, n_xu = 0, n_dir = 0, chunk = 2;
+  int sblocks = 0, n_dir = 0, chunk = 2;
   double delta2 = 0.0, tol2 = 0.0;
 };
 
 LoopCfg loop_cfg(Context* ctx, const BlockSys* B, double tol, int chunk_cap) {
   LoopCfg c;
   const int Rp = B->Rp;
-  c.op_grid = dim3(B->n_tiles, Rp / 32);
-  c.op_block = dim3(32, kWarps);
-  const int Q = Rp / 4;
-  const int G = Q >= 256 ? 1 : 256 / Q;
-  c.upd_smem = G > 1 ? sizeof(double) * (size_t)G * Q * 8 : 0;
   c.sblocks = Rp / 32;  // scalar kernels: 32 realizations x 32 row groups per CTA
-  c.n_xu = ctx->sm_count * 8;
   c.n_dir = std::min(B->L.n_int, ctx->sm_count * 8);
   c.chunk = std::max(2, (chunk_cap > 0 ? std::min(ctx->chunk, chunk_cap) : ctx->chunk) & ~1);
   c.delta2 = ctx->reliable_delta * ctx->reliable_delta;
@@ -3822,9 +3431,9 @@ LoopCfg loop_cfg(Context* ctx, const BlockSys* B, double tol, int chunk_cap) {
     c.chunk = 2;
     c.delta2 = ctx->mg_delta * ctx->mg_delta;
   }
-  // ask for a check once the recursive residual is at tol/2 (dense loop, r.r), or once
-  // sqrt(gamma / gamma0) is at tol/4 (single-reduction loop, dinv-weighted norm)
-  c.tol2 = (B->modal && !B->gmg ? 0.0625 : 0.25) * tol * tol;
+  // ask for a check once sqrt(gamma / gamma0) is at tol/4 (single-reduction loop,
+  // dinv-weighted norm), or once the recursive residual is at tol/2 (multigrid loop)
+  c.tol2 = (!B->gmg ? 0.0625 : 0.25) * tol * tol;
   return c;
 }
 
@@ -3979,7 +3588,6 @@ int gmg_launches(const BlockSys* B) {
 int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* out) {
   const Lattice& L = B->L;
   const int Rp = B->Rp;
-  const bool modal = B->modal;
   cudaStream_t st = B->X.st;
   Scal& s = B->s;
   cudaEvent_t* ev = B->X.ev;
@@ -3997,17 +3605,13 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
                           B->scal.ptr, pB.ptr, rB.ptr, qB.ptr, st};
     mix(ptrs, sizeof(ptrs));
     mix(&L, sizeof(L));
-    mix(&B->KF, sizeof(B->KF));
     mix(&B->MC, sizeof(B->MC));
-    if (modal) {
+    {
       const CUtensorMap* tms[9] = {&B->tm_rAm, &B->tm_rBm, &B->tm_qAm,   &B->tm_qBm, &B->tm_pAm,
                                    &B->tm_pBm, &B->tm_dinvm, &B->tm_em, &B->tm_dm};
       for (const CUtensorMap* t : tms) mix(t, sizeof(CUtensorMap));
-    } else {
-      mix(&B->tm_p, sizeof(CUtensorMap));
-      mix(&B->tm_e, sizeof(CUtensorMap));
     }
-    const int mm[6] = {modal ? 1 : 0, B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
+    const int mm[5] = {B->mass ? 1 : 0, B->n_tiles_m, B->n_items_m, B->grid_m, B->tiles_jm};
     mix(mm, sizeof(mm));
     const int gg[5] = {B->gmg ? 1 : 0, B->n_lvl, B->sweeps, B->pack ? 1 : 0, B->tc ? 1 : 0};
     mix(gg, sizeof(gg));
@@ -4026,7 +3630,7 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
     }
     const double dd[2] = {c.delta2, c.tol2};
     mix(dd, sizeof(dd));
-    const int ii[6] = {c.chunk, c.n_dir, B->n_upd, B->n_tiles, c.sblocks, (int)c.upd_smem};
+    const int ii[5] = {c.chunk, c.n_dir, B->n_upd, B->n_tiles, c.sblocks};
     mix(ii, sizeof(ii));
   }
   cudaGraphExec_t& gx = *B->X.graph;
@@ -4042,7 +3646,7 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
       // records during capture only order streams)
       if (B->gmg) {
         gmg_iteration(B, c, it, st);
-      } else if (modal) {
+      } else {
         // single-reduction loop: one operator launch per iteration; r, q and p
         // alternate between their two buffers
         const bool even = (it & 1) == 0;
@@ -4058,20 +3662,6 @@ int block_graph(Context* ctx, BlockSys* B, const LoopCfg& c, cudaGraphExec_t* ou
         if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
         k_alpha_gamma<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_m, part_op.as<double>(), s, c.delta2, c.tol2);
         if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
-      } else {
-        k_dir<<<c.n_dir, 256, 0, st>>>(L.n_int, Rp, interior, s.alpha, s.beta, r32.as<float>(), dinv.as<float>(),
-                                       p.as<float>(), d.as<float>());
-        if (it == 0) cudaEventRecordWithFlags(ev[4], st, cudaEventRecordExternal);
-        k_op_tma<<<c.op_grid, kOpThreads, kOpSmem, st>>>(L, B->KF, B->tm_p, B->tm_e, mask, q.as<float>(),
-                                                         part_op.as<double>(), s.err);
-        if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
-        k_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles, part_op.as<double>(), s);
-        if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
-        k_update<<<B->n_upd, 256, c.upd_smem, st>>>(L.n_int, Rp, interior, mask, s.alpha, q.as<float>(),
-                                                   r32.as<float>(), dinv.as<float>(), part_up.as<double>());
-        if (it == 0) cudaEventRecordWithFlags(ev[7], st, cudaEventRecordExternal);
-        cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
-        k_beta<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_upd, part_up.as<double>(), s, c.delta2, c.tol2);
       }
     }
     cudaError_t e = cudaStreamEndCapture(st, &g);
@@ -4097,13 +3687,6 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
   cudaStream_t st = B->X.st;
   Scal& s = B->s;
   const uint8_t* mask = B->mask;
-  if (!first && !B->modal) {
-    k_xupdate<<<c.n_xu, 256, 0, st>>>(L.n_int, Rp, B->interior, s.alpha, B->p.as<float>(), B->x.as<double>(),
-                                      B->d.as<float>());
-    count_launch(ctx);
-  }
-  double* x = B->x.as<double>();
-  const double* E = B->E64.as<double>();
   const float* dinv = B->dinv.as<float>();
   float* r32 = B->r32.as<float>();
   double* part = B->part_op.as<double>();
@@ -4112,12 +3695,12 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
     k_b_to_r32<<<c.n_dir, 256, 0, st>>>(L.n_int, Rp, B->interior, b, b_per_r ? 1 : 0, r32);
     MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
     k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_bsq, B->part_up.as<double>(), s, tol, first ? 1 : 0,
-                                                 B->gmg ? 2 : (B->modal ? 1 : 0), max_it);
+                                                 B->gmg ? 2 : 1, max_it);
     count_launch(ctx, 2);
     MSG_CUDA(ctx, cudaGetLastError());
     return MSG_OK;
   }
-  if (B->modal) {
+  {
     // x += d + alpha p (into the other x buffer) and the FP64 residual in one pass
     auto pick = [&](auto M, auto P, auto U) {
       return k_resid_modal<decltype(M)::value, decltype(P)::value, decltype(U)::value>;
@@ -4137,20 +3720,10 @@ int block_update(Context* ctx, BlockSys* B, const LoopCfg& c, const double* b, b
       std::swap(B->x.ptr, B->xB.ptr);
       std::swap(B->tm_xr, B->tm_xBr);
     }
-  } else if (B->mass) {
-    if (b_per_r)
-      k_resid<true, true><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
-    else
-      k_resid<true, false><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
-  } else {
-    if (b_per_r)
-      k_resid<false, true><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
-    else
-      k_resid<false, false><<<c.op_grid, c.op_block, 0, st>>>(L, B->KD, B->MD, x, b, E, mask, dinv, r32, part);
   }
   MSG_CUDA(ctx, cudaMemsetAsync(s.n_active, 0, 32, st));
-  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->modal ? B->n_tiles_r : B->n_tiles, part, s, tol,
-                                               first ? 1 : 0, B->gmg ? 2 : (B->modal ? 1 : 0), max_it);
+  k_resid_scalars<<<c.sblocks, 1024, 0, st>>>(Rp, B->n_tiles_r, part, s, tol, first ? 1 : 0, B->gmg ? 2 : 1,
+                                               max_it);
   count_launch(ctx, 2);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
@@ -4217,7 +3790,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
     cudaEventRecord(ev[2], st);
     cudaError_t e = cudaGraphLaunch(gexec, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
-    count_launch(ctx, (B->gmg ? gmg_launches(B) : (B->modal ? 2 : 5)) * c.chunk);
+    count_launch(ctx, (B->gmg ? gmg_launches(B) : 2) * c.chunk);
     total_inner += c.chunk;
     cudaEventRecord(ev[3], st);
     MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
@@ -4695,7 +4268,7 @@ int lane_cycle(Lane* L, int* state, int* its, double* res, int* n_active) {
     MSG_TRY(block_graph(ctx, &B, L->cfg, &g));
     cudaError_t e = cudaGraphLaunch(g, st);
     if (e != cudaSuccess) return cuda_error(ctx, e, "lane chunk");
-    count_launch(ctx, (B.gmg ? gmg_launches(&B) : (B.modal ? 2 : 5)) * L->cfg.chunk);
+    count_launch(ctx, (B.gmg ? gmg_launches(&B) : 2) * L->cfg.chunk);
   }
   return MSG_OK;
 }

@@ -560,7 +560,6 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!key) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "null option key");
   if (!std::strcmp(key, "reliable_delta") && value > 0 && value < 1) { ctx->reliable_delta = value; return MSG_OK; }
   if (!std::strcmp(key, "chunk") && value >= 2 && value <= 256) { ctx->chunk = ((int)value) & ~1; return MSG_OK; }
-  if (!std::strcmp(key, "modal_operator") && (value == 0 || value == 1)) { ctx->modal = (int)value; return MSG_OK; }
   if (!std::strcmp(key, "fixed_updates") && (value == 0 || value == 1)) { ctx->fixed_updates = (int)value; return MSG_OK; }
   if (!std::strcmp(key, "multigrid") && (value == 0 || value == 1 || value == 2)) {
     ctx->multigrid = (int)value;
@@ -601,7 +600,6 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
     double v;
   } opts[] = {{"reliable_delta", ctx->reliable_delta},
               {"chunk", (double)ctx->chunk},
-              {"modal_operator", (double)ctx->modal},
               {"fixed_updates", (double)ctx->fixed_updates},
               {"multigrid", (double)ctx->multigrid},
               {"multigrid_levels", (double)ctx->mg_levels},

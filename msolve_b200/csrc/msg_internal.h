@@ -70,9 +70,8 @@ struct Context {
   // mixed-solver tunables (MSG_SET_OPTION)
   double reliable_delta = 0.1;  // FP64 residual replacement when ||r|| drops by this factor
   int chunk = 16;               // inner iterations per captured graph launch
-  int modal = 1;                // FP32 operator: 1 = Walsh-mode (modal) kernel, 0 = dense value-class kernel
   int fixed_updates = 0;        // 1: FP64 true-residual step after every graph chunk (batch-invariant results)
-  // multigrid preconditioner of the batched lattice solves (modal operator only)
+  // multigrid preconditioner of the batched lattice solves
   // 1: V-cycle preconditioned loop for systems without a mass term, 2: also with
   // one, 0: Jacobi loop (the V-cycle needs a lattice that coarsens at least once)
   int multigrid = 1;
