@@ -1027,14 +1027,18 @@ __global__ void __launch_bounds__(kMThreads, 1)
 // group; slots 6-7 are zero), so one node-pair group of a plane serves the
 // element pencils on both of its sides. An M = 128 tile is the 4 element
 // pencils along y of one z row, 32 realizations each; it reads 4 consecutive
-// 1 KB groups (MN-major, 128-byte swizzle, realizations contiguous). TF32 with
-// a three-term split keeps FP32-level accuracy:
+// 1 KB groups (K-major core matrices of 8 realizations x 4 slots, no swizzle:
+// a realization's 8 slots are two 16-byte rows, LBO 128 B between the slot
+// halves, SBO 256 B between 8-realization groups). TF32 with a three-term
+// split keeps FP32-level accuracy:
 //   U = U_hi + U_lo (U_hi: U with the low 13 mantissa bits cleared),
 //   cK Khat = B_hi + B_lo,  U Khat ~ U_hi [B_hi | B_lo] (N = 64) + U_lo B_hi (N = 32).
 // Output column n = ((ax' 2 + ay') 2 + az') 3 + c'; columns 0-11 land on plane
 // P-1, 12-23 on plane P (carried to the next slab, as the Walsh kernels carry
-// C1). Per plane: every element warp forms p = z + beta p_old at its nodes,
-// splits it and writes both halves into the plane's groups; after a CTA
+// C1). Per plane: every element warp forms p = z + beta p_old at the two
+// nodes of its node-pair group (y = ej, z = ek; the last element column also
+// the group at y = 4), splits it and writes both halves with 16-byte stores
+// (conflict-free) into the plane's groups; after a CTA
 // barrier one thread issues the 32 MMAs of the slab (P-1, P) and commits them
 // to an mbarrier; each element warp reads its element's 24 outputs from its
 // tensor-memory lane quadrant (warp w: element (w % 4, w / 4), lanes
@@ -1059,9 +1063,9 @@ __device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46) | ((uint64_t)(layout & 7u) << 61);
 }
-// instruction descriptor of kind::tf32: FP32 accumulator, A MN-major, B K-major
+// instruction descriptor of kind::tf32: FP32 accumulator, A and B K-major
 __device__ __forceinline__ uint32_t tc_idesc(int M, int N) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   const uint32_t z = 0;
@@ -1088,10 +1092,8 @@ __device__ __forceinline__ void tc_ld8(uint32_t a, float (&v)[8]) {
 #pragma unroll
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
-// byte offset of (realization r, slot k) in a 1 KB group: 128-byte swizzle
-__device__ __forceinline__ uint32_t tc_slot(int r, int k) {
-  return (uint32_t)(k * 128 + (((r >> 2) ^ k) << 4) + ((r & 3) << 2));
-}
+// byte offset of realization r's slots 0-3 in a 1 KB group (slots 4-7: + 128)
+__device__ __forceinline__ uint32_t tc_row(int r) { return (uint32_t)((r >> 3) * 256 + (r & 7) * 16); }
 
 template <int kMode>
 __global__ void __launch_bounds__(kMThreads, 1)
@@ -1168,9 +1170,9 @@ __global__ void __launch_bounds__(kMThreads, 1)
   const uint32_t abase = smem_u32(abuf), bbase = smem_u32(bsm);
   // tensor-memory address of this warp's element: lanes 32 ej.., columns 64 ek..
   const uint32_t my_t = tmem + ((uint32_t)(32 * ej) << 16) + (uint32_t)(64 * ek);
-  // nodes this warp forms: its own corner (ej, ek); the warps of the last element
-  // row / column also form the patch edge beyond it (f = 1: +y, 2: +z, 3: +y +z)
-  const bool edge_y = ej == kMEJ - 1, edge_z = ek == kMEK - 1;
+  // node-pair groups this warp forms: (y = ej, z = ek), and the last element
+  // column also (y = ej + 1, z = ek)
+  const bool edge_y = ej == kMEJ - 1;
   uint32_t seq = 0, slab = 0;
   int xsel = 0;
   bool dead = false;
@@ -1233,32 +1235,38 @@ __global__ void __launch_bounds__(kMThreads, 1)
         dead = true;
       }
       const float* pt = smem + st * S::kFloats;
-      // form p = z + beta p_old at this warp's nodes of plane P, split into the plane's groups
+      // form p = z + beta p_old at the nodes of this warp's node-pair groups of plane P
+      // (slots 0-2: node (y, z), 3-5: node (y, z + 1), 6-7: zero), split into hi and lo
       unsigned char* ap = abuf + (P & 1) * 2 * kTcPlane;
       float own[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        if ((f == 1 && !edge_y) || (f == 2 && !edge_z) || (f == 3 && !(edge_y && edge_z))) continue;
-        const int py = ej + (f & 1), pz = ek + (f >> 1);
-        const int o = pz * kMPJ + py;
+      for (int f = 0; f < 2; ++f) {
+        if (f == 1 && !edge_y) continue;
+        const int py = ej + f, pz = ek;
+        float u[6];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const int i = (o * 3 + c) * 32 + lane;
-          const float u = fmaf(be, pt[S::kOffB + i], pt[S::kOffA + i]);
-          const float hi = __uint_as_float(__float_as_uint(u) & 0xffffe000u);
-          const float lo = u - hi;
-          if (f == 0) own[c] = u;
-          if (pz <= 3) {
-            const uint32_t g = (uint32_t)(pz * 5 + py) * kTcAtom + tc_slot(lane, c);
-            *reinterpret_cast<float*>(ap + g) = hi;
-            *reinterpret_cast<float*>(ap + kTcPlane + g) = lo;
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const int i = (((pz + h) * kMPJ + py) * 3 + c) * 32 + lane;
+            u[h * 3 + c] = fmaf(be, pt[S::kOffB + i], pt[S::kOffA + i]);
           }
-          if (pz >= 1) {
-            const uint32_t g = (uint32_t)((pz - 1) * 5 + py) * kTcAtom + tc_slot(lane, 3 + c);
-            *reinterpret_cast<float*>(ap + g) = hi;
-            *reinterpret_cast<float*>(ap + kTcPlane + g) = lo;
-          }
+        if (f == 0) {
+          own[0] = u[0];
+          own[1] = u[1];
+          own[2] = u[2];
         }
+        float hi[6], lo[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          hi[k] = __uint_as_float(__float_as_uint(u[k]) & 0xffffe000u);
+          lo[k] = u[k] - hi[k];
+        }
+        unsigned char* g = ap + (uint32_t)(pz * 5 + py) * kTcAtom + tc_row(lane);
+        *reinterpret_cast<float4*>(g) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<float4*>(g + 128) = make_float4(hi[4], hi[5], 0.f, 0.f);
+        *reinterpret_cast<float4*>(g + kTcPlane) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        *reinterpret_cast<float4*>(g + kTcPlane + 128) = make_float4(lo[4], lo[5], 0.f, 0.f);
       }
       if (node_ok) {  // the owner writes p and d += alpha p_old (k_lvl_op<kLvlPcgZ>)
         const size_t node = nrow + P;
@@ -1289,9 +1297,8 @@ __global__ void __launch_bounds__(kMThreads, 1)
               const uint32_t pa = abase + (uint32_t)((P - 1 + ax) & 1) * 2 * kTcPlane + (uint32_t)(t * 5 + ay) * kTcAtom;
               const uint32_t pb = bbase + (uint32_t)pr * 64 * 8 * 4;
               const uint64_t db = tc_sdesc(pb, 128, 256, 0);
-              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa, kTcAtom, kTcAtom, 2), db, tc_idesc(128, 64), pr > 0);
-              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa + kTcPlane, kTcAtom, kTcAtom, 2), db, tc_idesc(128, 32),
-                     1u);
+              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa, 128, 256, 0), db, tc_idesc(128, 64), pr > 0);
+              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa + kTcPlane, 128, 256, 0), db, tc_idesc(128, 32), 1u);
             }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                            smem_u32(mma_bar))
