@@ -1190,10 +1190,12 @@ __global__ void __launch_bounds__(kMThreads, 1)
     const size_t nrow = ((size_t)Je + (size_t)L.NYp * Ke) * L.NXp;
     const int rr = g32 + lane;
     const float al = alpha[rr], be = beta[rr];
-    float T0[12];  // plane P-1 corners (ay, az, c) carried from the slab below
+    float T0[12];  // corners (ay, az, c) of the plane below the slab being read, carried from the slab below it
 #pragma unroll
     for (int i = 0; i < 12; ++i) T0[i] = 0.f;
-    float ou[3] = {0.f, 0.f, 0.f};
+    float ou[3] = {0.f, 0.f, 0.f};   // own node's p at the plane whose node phase runs next
+    float ou1[3] = {0.f, 0.f, 0.f};  // ... and at the plane after it
+    float E1 = 0.f;                  // E of the slab whose products are in flight
     double acc = 0.0;
     uint32_t mreg = 0;
     auto node_phase = [&](int X) {
@@ -1228,6 +1230,50 @@ __global__ void __launch_bounds__(kMThreads, 1)
 #pragma unroll
           for (int c = 0; c < 3; ++c) xb[((w * 4 + ay + 2 * az) * 3 + c) * 32 + lane] = T0[(ay * 2 + az) * 3 + c];
     };
+    // products of the slab committed last: wait, read this warp's element from
+    // tensor memory, scale by its E (y: plane-below corners 0..11, plane-above 12..23)
+    auto read_slab = [&](float (&y)[24]) {
+      bool ok = !dead && mbar_wait(mma_bar, slab & 1);
+      ++slab;
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) {
+        if (lane == 0) atomicExch(err, 1);
+        dead = true;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (ok) {
+        float a16[16], a8[8], b16[16], b8[8];
+        tc_ld16(my_t, a16);
+        tc_ld8(my_t + 16, a8);
+        tc_ld16(my_t + 32, b16);
+        tc_ld8(my_t + 48, b8);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int i = 0; i < 16; ++i) y[i] = E1 * (a16[i] + b16[i]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) y[16 + i] = E1 * (a8[i] + b8[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 24; ++i) y[i] = 0.f;
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    };
+    // corners of the slab's lower plane complete that plane: into the exchange
+    // buffer (the node phase reads them after the next barrier)
+    auto emit_slab = [&](const float (&y)[24]) {
+      if (real) {
+#pragma unroll
+        for (int i = 0; i < 12; ++i) T0[i] += y[i];
+        emit_corners();
+      }
+#pragma unroll
+      for (int i = 0; i < 12; ++i) T0[i] = y[12 + i];
+    };
+    // Plane P: read the products of slab (P-2, P-1) (issued one plane earlier, so
+    // they ran during the previous node phase) and emit plane P-2's corners, form
+    // plane P into the buffer of plane P-2 (no longer read), and after one barrier
+    // issue slab (P-1, P) into the same tensor memory (read above by every warp)
+    // and run plane P-2's node phase.
     for (int P = 1; P <= NX; ++P, ++seq) {
       const int st = seq % kMStages;
       if (!dead && !mbar_wait(&full[st], (seq / kMStages) & 1)) {
@@ -1235,6 +1281,11 @@ __global__ void __launch_bounds__(kMThreads, 1)
         dead = true;
       }
       const float* pt = smem + st * S::kFloats;
+      if (P >= 3) {
+        float y[24];
+        read_slab(y);
+        emit_slab(y);
+      }
       // form p = z + beta p_old at the nodes of this warp's node-pair groups of plane P
       // (slots 0-2: node (y, z), 3-5: node (y, z + 1), 6-7: zero), split into hi and lo
       unsigned char* ap = abuf + (P & 1) * 2 * kTcPlane;
@@ -1286,63 +1337,45 @@ __global__ void __launch_bounds__(kMThreads, 1)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       csync();
-      if (P >= 2) {
-        if (w == 0 && lane == 0) {
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-          for (int t = 0; t < 4; ++t)      // M tile: the z row of element pencils
-#pragma unroll
-            for (int pr = 0; pr < 4; ++pr) {  // corner pair (ax, ay)
-              const int ax = pr >> 1, ay = pr & 1;
-              const uint32_t pa = abase + (uint32_t)((P - 1 + ax) & 1) * 2 * kTcPlane + (uint32_t)(t * 5 + ay) * kTcAtom;
-              const uint32_t pb = bbase + (uint32_t)pr * 64 * 8 * 4;
-              const uint64_t db = tc_sdesc(pb, 128, 256, 0);
-              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa, 128, 256, 0), db, tc_idesc(128, 64), pr > 0);
-              tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa + kTcPlane, 128, 256, 0), db, tc_idesc(128, 32), 1u);
-            }
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                           smem_u32(mma_bar))
-                       : "memory");
-        }
-        bool ok = !dead && mbar_wait(mma_bar, slab & 1);
-        ++slab;
-        ok = __all_sync(0xffffffffu, ok);
-        if (!ok) {
-          if (lane == 0) atomicExch(err, 1);
-          dead = true;
-        }
+      if (P >= 2 && w == 0 && lane == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        float y[24];
-        if (ok) {
-          float a16[16], a8[8], b16[16], b8[8];
-          tc_ld16(my_t, a16);
-          tc_ld8(my_t + 16, a8);
-          tc_ld16(my_t + 32, b16);
-          tc_ld8(my_t + 48, b8);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int i = 0; i < 16; ++i) y[i] = E * (a16[i] + b16[i]);
+        for (int t = 0; t < 4; ++t)      // M tile: the z row of element pencils
 #pragma unroll
-          for (int i = 0; i < 8; ++i) y[16 + i] = E * (a8[i] + b8[i]);
-        } else {
-#pragma unroll
-          for (int i = 0; i < 24; ++i) y[i] = 0.f;
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (real) {
-#pragma unroll
-          for (int i = 0; i < 12; ++i) T0[i] += y[i];
-          emit_corners();
-        }
-#pragma unroll
-        for (int i = 0; i < 12; ++i) T0[i] = y[12 + i];
-        csync();
-        if (node_ok) node_phase(P - 1);
+          for (int pr = 0; pr < 4; ++pr) {  // corner pair (ax, ay)
+            const int ax = pr >> 1, ay = pr & 1;
+            const uint32_t pa = abase + (uint32_t)((P - 1 + ax) & 1) * 2 * kTcPlane + (uint32_t)(t * 5 + ay) * kTcAtom;
+            const uint32_t pb = bbase + (uint32_t)pr * 64 * 8 * 4;
+            const uint64_t db = tc_sdesc(pb, 128, 256, 0);
+            tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa, 128, 256, 0), db, tc_idesc(128, 64), pr > 0);
+            tc_mma(tmem + (uint32_t)(64 * t), tc_sdesc(pa + kTcPlane, 128, 256, 0), db, tc_idesc(128, 32), 1u);
+          }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(mma_bar))
+                     : "memory");
+      }
+      if (P >= 3) {
+        if (node_ok) node_phase(P - 2);
         xsel ^= 1;
       }
+      E1 = E;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) ou[c] = own[c];
+      for (int c = 0; c < 3; ++c) {
+        ou[c] = ou1[c];
+        ou1[c] = own[c];
+      }
     }
+    // the last slab (NX-1, NX): plane NX-1, then plane NX from the carried corners
+    {
+      float y[24];
+      read_slab(y);
+      emit_slab(y);
+    }
+    csync();
+    if (node_ok) node_phase(NX - 1);
+    xsel ^= 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) ou[c] = ou1[c];
     if (real) emit_corners();
     csync();
     if (node_ok) node_phase(NX);
