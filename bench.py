@@ -92,8 +92,8 @@ def parse():
     p.add_argument("--single-n", type=int, default=64)
     p.add_argument("--single-only", action="store_true",
                    help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
-    p.add_argument("--serve-rates", default="100,400", help="Poisson arrival rates (requests/s) to run")
-    p.add_argument("--serve-requests", type=int, default=200, help="requests per rate")
+    p.add_argument("--serve-rates", default="100,400,1000,2000,5000", help="Poisson arrival rates (requests/s) to run")
+    p.add_argument("--serve-requests", type=int, default=300, help="requests per rate")
     p.add_argument("--multigrid", type=int, default=None, choices=[0, 1, 2],
                    help="MSG_SET_OPTION multigrid (1: V-cycle for systems without a mass term, 2: for all)")
     p.add_argument("--mg-levels", type=int, default=None, help="MSG_SET_OPTION multigrid_levels")
@@ -394,6 +394,8 @@ def serving_leg(args, ctx):
                 "per_side": {str(n): {"count": len(v), "p50_ms": float(np.percentile(v, 50)),
                                       "p99_ms": float(np.percentile(v, 99))} for n, v in lat.items() if v},
                 "mean_iterations": float(np.mean(its))})
+        out["fp64_one_at_a_time"] = fp64_serving_baseline(args, ctx, sides,
+                                                           [float(v) for v in args.serve_rates.split(",") if v])
         if not args.no_parity and largest is not None:
             import oracle as O
             n = max(sides)
@@ -405,6 +407,57 @@ def serving_leg(args, ctx):
         return out
     finally:
         srv.stop()
+
+
+def fp64_serving_baseline(args, ctx, sides, rates):
+    """The plain FP64 path serving the same kind of stream one request at a
+    time: per request its KL field, the assembled FP64 BSR matrix and the FP64
+    Jacobi-PCG drop-in (MSG_PCG_SOLVE, the reference's stopping rule at 1e-8),
+    each request's service time measured on the GPU box. A single FIFO server
+    gives each arrival process's latencies exactly: finish_i =
+    max(arrival_i, finish_{i-1}) + service_i."""
+    import msolve_b200 as M
+    rng = np.random.default_rng(7)
+    k = args.serve_requests
+    which = rng.choice(sides, k)
+    xis = rng.standard_normal((k, args.terms))
+    meshes = {}
+    for n in sides:
+        model = M.clamped_block_model(n)
+        kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, args.terms, 12)
+        solver = M.SolverPCG(ctx, model, max_iterations=100000, tolerance=1e-8, precision="fp64")
+        meshes[n] = (model, M.GpuMesh(ctx, model), kl, solver)
+
+    def serve(n, xi):
+        model, mesh, kl, solver = meshes[n]
+        A = mesh.assemble(kl.field(mesh, xi)[0], model.poisson)
+        solver.matrix = A
+        solver.Solve()
+        A.close()
+        return solver.iterations
+
+    for n in sides:  # warm-up
+        serve(n, np.zeros(args.terms))
+    service, its = np.zeros(k), np.zeros(k)
+    for i in range(k):
+        t0 = time.perf_counter()
+        its[i] = serve(int(which[i]), xis[i])
+        service[i] = time.perf_counter() - t0
+    out = {"workload": f"the same kind of stream ({k} requests, sides uniform in {list(sides)}), one request at a "
+                       f"time: KL field + FP64 BSR assembly + FP64 Jacobi-PCG (MSG_PCG_SOLVE, tol 1e-8)",
+           "service_ms_mean": 1e3 * float(service.mean()), "mean_iterations": float(its.mean()),
+           "max_throughput_per_s": k / float(service.sum()), "rates": []}
+    for rate in rates:
+        arrive = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, k))
+        finish = np.zeros(k)
+        prev = 0.0
+        for i in range(k):
+            prev = max(arrive[i], prev) + service[i]
+            finish[i] = prev
+        lat = 1e3 * (finish - arrive)
+        out["rates"].append({"rate_per_s": rate, "throughput_per_s": k / float(finish[-1] - arrive[0]),
+                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+    return out
 
 
 def run_reference(args):

@@ -328,14 +328,18 @@ int MSG_NEWMARK_BATCH(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const d
  * (its realization loop is sequential, MonteCarloAnalyzerWithStochasticMaterial.cs:258-276).
  * A model is a structured mesh with its material (nu), KL table and load b
  * [n_dofs]; a request is one realization of a model (its xi [kl->n_terms]).
- * Requests wait in a queue, enter a free slot of their model's batch at the
- * next chunk boundary (max_batch slots per model, rounded up to 32; the slot
- * memory of each model is allocated once, against the context's memory
- * budget, when the model is added) and leave as soon as their own FP64 true
- * residual is below the model's tol. A request's arithmetic does not depend on
- * the other requests in flight: results are bitwise identical alone or mixed.
- * One worker thread per context runs the batches; every entry point may be
- * called from any thread. */
+ * Requests wait in their model's queue, enter a free slot of one of the
+ * model's lanes at the next chunk boundary and leave as soon as their own FP64
+ * true residual is below the model's tol. A lane is a batch of max_batch slots
+ * (rounded up to 64) with its device state; admission is by device memory: a
+ * model's first lane is allocated when the model is added (against the
+ * context's memory budget, MSG_CREATE), a manager thread adds lanes (at most 8
+ * a model) while a model's queue outgrows its free slots and the budget has
+ * room, and retires idle extra lanes when another model's requests need the
+ * memory or after a second without work. A request's arithmetic does not
+ * depend on the other requests in flight or on its lane: results are bitwise
+ * identical alone or mixed. One worker thread per lane runs its batch on the
+ * lane's own stream; every entry point may be called from any thread. */
 #define MSG_PENDING 1 /* MSG_SERVE_POLL: not finished yet (not an error) */
 typedef uint64_t MSG_REQ;
 int MSG_SERVE_START(MSG_CTX ctx, int max_batch);
@@ -356,6 +360,9 @@ int MSG_SERVE_POLL(MSG_CTX ctx, MSG_REQ id, int timeout_ms, double* X, int* iter
 int MSG_SERVE_CANCEL(MSG_CTX ctx, MSG_REQ id);
 /* Requests waiting in the queues and occupying slots. */
 int MSG_SERVE_STATS(MSG_CTX ctx, int64_t* queued, int64_t* running);
+/* Lanes of model model_id (-1: all models) that currently admit requests, and
+ * the lanes added and retired since MSG_SERVE_START. No reference counterpart. */
+int MSG_SERVE_LANES(MSG_CTX ctx, int model_id, int* lanes, int64_t* added, int64_t* retired);
 /* Stop the worker and free every model (pending requests are dropped). */
 int MSG_SERVE_STOP(MSG_CTX ctx);
 
@@ -396,7 +403,8 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * operator launch and t[6] that of one whole iteration. */
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 /* The current value of an MSG_SET_OPTION key (MSG_ERR_INVALID_ARGUMENT for an
- * unknown key). */
+ * unknown key), or of the read-only keys "memory_used" (device bytes charged
+ * to the context) and "memory_budget" (its budget, 0 = none). */
 int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value);
 
 /* Kernel launch counter of this context (kernels launched since creation),

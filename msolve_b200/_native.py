@@ -112,6 +112,7 @@ SIGNATURES = {
     "MSG_SERVE_POLL": (C.c_int, [_vp, C.c_uint64, C.c_int, _d, _i, _d, _d]),
     "MSG_SERVE_CANCEL": (C.c_int, [_vp, C.c_uint64]),
     "MSG_SERVE_STATS": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "MSG_SERVE_LANES": (C.c_int, [_vp, C.c_int, _i, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "MSG_SERVE_STOP": (C.c_int, [_vp]),
     "MSG_SET_OPTION": (C.c_int, [_vp, C.c_char_p, C.c_double]),
     "MSG_STATS": (C.c_int, [_vp, _i64, _d]),

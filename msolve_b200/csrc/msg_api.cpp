@@ -51,6 +51,9 @@ int DevMem::alloc(Context* c, size_t n) {
   if (e != cudaSuccess) {
     ptr = nullptr;
     cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation)
+      return set_error(c, MSG_ERR_OUT_OF_MEMORY, "device memory exhausted (cudaMalloc of %llu bytes)",
+                       (unsigned long long)n);
     return cuda_error(c, e, "cudaMalloc");
   }
   bytes = n;
@@ -610,7 +613,10 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"tensor_operator", (double)ctx->tensor_op},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
-              {"serve_priority", (double)ctx->serve_priority}};
+              {"serve_priority", (double)ctx->serve_priority},
+              // read-only: device memory charged to the context and its budget (bytes)
+              {"memory_used", (double)ctx->used.load()},
+              {"memory_budget", (double)ctx->budget}};
   for (const auto& o : opts)
     if (!std::strcmp(key, o.name)) {
       *value = o.v;

@@ -1,5 +1,6 @@
 """Host mirror of the serving entry points (MSG_SERVE_*): continuous batching of
-independent realizations of registered models on one context.
+independent realizations of registered models on one context, lanes of
+max_batch slots added and retired by device memory (the context's budget).
 
     srv = Server(ctx, max_batch=64)
     m = srv.add_model(model, kl, tol=1e-8)        # one structured mesh + material + KL table + load
@@ -63,6 +64,13 @@ class Server:
         q, r = C.c_int64(0), C.c_int64(0)
         N.check(N.lib().MSG_SERVE_STATS(self.ctx.handle, C.byref(q), C.byref(r)), self.ctx.handle, "MSG_SERVE_STATS")
         return {"queued": q.value, "running": r.value}
+
+    def lanes(self, model_id=-1):
+        """Lanes admitting requests (of one model, or all), lanes added and retired so far."""
+        n, a, r = C.c_int(0), C.c_int64(0), C.c_int64(0)
+        N.check(N.lib().MSG_SERVE_LANES(self.ctx.handle, int(model_id), C.byref(n), C.byref(a), C.byref(r)),
+                self.ctx.handle, "MSG_SERVE_LANES")
+        return {"lanes": n.value, "added": a.value, "retired": r.value}
 
     def stop(self):
         N.lib().MSG_SERVE_STOP(self.ctx.handle)

@@ -156,3 +156,78 @@ def test_scheduling_options_do_not_change_results(ctx):
         for a_model, b_model in zip(results[0], other):
             for a, b in zip(a_model, b_model):
                 assert np.array_equal(a, b)
+
+
+def test_lanes_grow_with_the_backlog_and_retire_when_idle(ctx):
+    """A burst larger than one lane's slots makes the manager add lanes of the
+    same model; the results do not depend on the lane a request landed in
+    (bitwise equal to the same requests served one at a time), and the extra
+    lanes are retired once idle."""
+    import time
+    n = 6
+    model, kl = _problem(n)
+    rng = np.random.default_rng(31)
+    xis = rng.standard_normal((200, 12))
+    srv = Server(ctx, max_batch=32)
+    try:
+        m = srv.add_model(model, kl, tol=1e-10)
+        assert srv.lanes(m)["lanes"] == 1
+        alone = [srv.poll(srv.submit(m, xi), timeout_ms=-1)["X"] for xi in xis[:4]]
+        reqs = [srv.submit(m, xi) for xi in xis]
+        outs = [srv.poll(rq, timeout_ms=-1) for rq in reqs]
+        assert srv.lanes()["added"] >= 2
+        for a, o in zip(alone, outs[:4]):
+            assert np.array_equal(a, o["X"])
+        assert all(o["rel_res"] < 1e-10 for o in outs)
+        t0 = time.time()
+        while srv.lanes(m)["lanes"] > 1 and time.time() - t0 < 10:
+            time.sleep(0.2)
+        assert srv.lanes(m)["lanes"] == 1
+        assert srv.lanes()["retired"] >= 1
+    finally:
+        srv.stop()
+
+
+def test_admission_waits_for_device_memory(ctx):
+    """A context whose memory budget holds the two models' first lanes and
+    room for one more: bursts on both models queue until a lane frees memory,
+    and every request completes with the bits of an unconstrained server."""
+    models = [_problem(n) for n in (6, 8)]
+    rng = np.random.default_rng(41)
+    xis = rng.standard_normal((2, 150, 12))
+    ref = []
+    srv = Server(ctx, max_batch=32)
+    try:
+        ms = [srv.add_model(model, kl, tol=1e-10) for model, kl in models]
+        for i, m in enumerate(ms):
+            ref.append([srv.poll(rq, timeout_ms=-1)["X"] for rq in [srv.submit(m, xi) for xi in xis[i][:20]]])
+    finally:
+        srv.stop()
+    probe = M.Context(0)
+    s0 = Server(probe, max_batch=32)
+    meshes = []
+    try:
+        used0 = probe.get_option("memory_used")
+        s0.add_model(*models[0], tol=1e-10)
+        lane6 = probe.get_option("memory_used") - used0
+        s0.add_model(*models[1], tol=1e-10)
+        base = probe.get_option("memory_used")
+        lane8 = base - used0 - lane6
+    finally:
+        s0.stop()
+        probe.close()
+    tight = M.Context(0, int(base + 1.2 * max(lane6, lane8)))
+    srv = Server(tight, max_batch=32)
+    try:
+        ms = [srv.add_model(model, kl, tol=1e-10) for model, kl in models]
+        reqs = [[srv.submit(m, xi) for xi in xis[i]] for i, m in enumerate(ms)]
+        outs = [[srv.poll(rq, timeout_ms=-1) for rq in rs] for rs in reqs]
+        assert tight.get_option("memory_used") <= tight.get_option("memory_budget")
+        for i in range(2):
+            assert all(o["rel_res"] < 1e-10 for o in outs[i])
+            for a, o in zip(ref[i], outs[i][:20]):
+                assert np.array_equal(a, o["X"])
+        assert srv.lanes()["lanes"] <= 3
+    finally:
+        srv.stop()
+        tight.close()
