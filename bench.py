@@ -519,11 +519,11 @@ def main():
     from msolve_b200 import _native as N
 
     ctx = M.Context(local)
+    if args.reliable_delta is not None:
+        ctx.set_option("reliable_delta", args.reliable_delta)
     if args.single_only:
         print(json.dumps(single_leg(args, ctx)))
         return
-    if args.reliable_delta is not None:
-        ctx.set_option("reliable_delta", args.reliable_delta)
     if args.chunk is not None:
         ctx.set_option("chunk", args.chunk)
     if args.tensor_op is not None:

@@ -303,6 +303,113 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int 
   }
 }
 
+// Mixed precision (FP32 matrix values): the search direction first, once per
+// row component, p_new = dinv r + beta p_old in FP64 and its FP32 copy p32,
+// so the SpMV gathers 4 bytes per column component instead of forming p from
+// three FP64 gathers.
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_dir32(int n_rows, const double* __restrict__ dinv,
+                                                           const double* __restrict__ r, double* p0, double* p1,
+                                                           float* __restrict__ p32, const PcgState* st) {
+  if (st->done) return;
+  const int it = st->it;
+  const double beta = st->beta;
+  const double* __restrict__ pold = (it & 1) ? p1 : p0;
+  double* __restrict__ pnew = (it & 1) ? p0 : p1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
+    const double pn = dinv[i] * r[i] + beta * pold[i];
+    pnew[i] = pn;
+    p32[i] = (float)pn;
+  }
+}
+
+// q = K32 p32 for the mixed loop (FP32 values and gathered direction, each
+// 3 x 3 block product in FP32, block sums in FP64), partial p.q with the FP64
+// p of the own rows, then alpha as k_pcg_dir_spmv_rows. Same slice / warp
+// layout and streaming loads as k_pcg_dir_spmv_rows.
+template <int kS, int kSpmvWarps, bool kStream>
+__global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_spmv32(int n_rows, int n_slices,
+                                                               const int64_t* __restrict__ slice_ptr,
+                                                               const int* __restrict__ col,
+                                                               const float* __restrict__ val,
+                                                               const float* __restrict__ p32, const double* p0,
+                                                               const double* p1, double* __restrict__ q,
+                                                               double* __restrict__ partial, PcgState* st) {
+  __shared__ double sh[32];
+  __shared__ double ys[kS][kSpmvWarps][3][32];
+  if (st->done) return;
+  const int it = st->it;
+  const double* __restrict__ pnew = (it & 1) ? p0 : p1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sl = warp / kSpmvWarps, w = warp % kSpmvWarps;
+  const int slice = blockIdx.x * kS + sl;
+  const int row = slice * 32 + lane;
+  const bool live = slice < n_slices && row < n_rows;
+  double y0 = 0, y1 = 0, y2 = 0;
+  auto fma9 = [&](const float (&a)[9], int cc) {
+    if (cc < 0) return;  // padding (its values are zero)
+    const float x0 = __ldg(p32 + 3 * cc), x1 = __ldg(p32 + 3 * cc + 1), x2 = __ldg(p32 + 3 * cc + 2);
+    y0 += (double)fmaf(a[2], x2, fmaf(a[1], x1, a[0] * x0));
+    y1 += (double)fmaf(a[5], x2, fmaf(a[4], x1, a[3] * x0));
+    y2 += (double)fmaf(a[8], x2, fmaf(a[7], x1, a[6] * x0));
+  };
+  if (live) {
+    const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
+    constexpr int U = 4;  // slots per group: 144 bytes of values in flight per thread
+    int64_t s = s0 + w;
+    for (; s + (U - 1) * kSpmvWarps < s1; s += U * kSpmvWarps) {
+      int cu[U];
+      float a[U][9];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t su = s + u * kSpmvWarps;
+        cu[u] = __ldg(col + su * 32 + lane);
+        const float* vu = val + su * 9 * 32 + lane;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a[u][k] = kStream ? __ldcs(vu + k * 32) : __ldg(vu + k * 32);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) fma9(a[u], cu[u]);
+    }
+    for (; s < s1; s += kSpmvWarps) {
+      const int c0 = __ldg(col + s * 32 + lane);
+      const float* v0 = val + s * 9 * 32 + lane;
+      float a0[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a0[k] = kStream ? __ldcs(v0 + k * 32) : __ldg(v0 + k * 32);
+      fma9(a0, c0);
+    }
+  }
+  ys[sl][w][0][lane] = y0;
+  ys[sl][w][1][lane] = y1;
+  ys[sl][w][2][lane] = y2;
+  __syncthreads();
+  double pq = 0;
+  if (w == 0 && live) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double t = ys[sl][0][c][lane];
+#pragma unroll
+      for (int ww = 1; ww < kSpmvWarps; ++ww) t += ys[sl][ww][c][lane];
+      q[3 * row + c] = t;
+      pq += pnew[3 * row + c] * t;
+    }
+  }
+  const double bs = block_sum(pq, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
+  if (!last_block(&st->counter)) return;
+  const double t = sum_partials(partial, gridDim.x, 1, 0, sh);
+  if (threadIdx.x == 0) {
+    st->pq = t;
+    st->matvecs += 1;
+    if (!(t > 0) || isnan(t)) {  // breakdown: p.q <= 0 or NaN
+      st->status = MSG_ERR_BREAKDOWN; st->done = 1; st->iterations = it;
+    } else {
+      st->alpha = st->zr / t;
+    }
+    st->counter = 0;
+  }
+}
+
 __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const double* __restrict__ dinv,
                                                             double* __restrict__ r, double* __restrict__ x,
                                                             const double* __restrict__ p0,
@@ -446,10 +553,11 @@ int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* 
   return MSG_OK;
 }
 
-// The loop's SpMV launch (shape chosen by size and value precision).
+// The loop's SpMV launch (shape chosen by size and value precision). Mixed:
+// the direction pass (FP64 p and its FP32 copy p32) and the FP32 product.
 static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float* v32, bool mixed, double* dv,
                                 double* rv, double* p0, double* p1, double* qv, double* pa, PcgState* st,
-                                cudaStream_t stream) {
+                                cudaStream_t stream, float* p32 = nullptr, int grid_v = 0) {
   const int nr = m->n_nodes;
   const int ns = m->pat.n_slices;
   const bool small = ns < ctx->sm_count * 32;  // fewer slices than 32 warps per SM: 4 warps per slice
@@ -463,11 +571,14 @@ static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float*
 #define MSG_SPMV(V, S, W, STREAM, grid, vals)                                                                       \
   k_pcg_dir_spmv_rows<V, S, W, STREAM><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, vals, dv, rv, p0, p1, qv, pa, \
                                                                         st)
+#define MSG_SPMV32(S, W, STREAM, grid)                                                                           \
+  k_pcg_spmv32<S, W, STREAM><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, p0, p1, qv, pa, st)
   if (mixed) {
+    k_pcg_dir32<<<grid_v, kPcgThreads, 0, stream>>>(nr, dv, rv, p0, p1, p32, st);
     if (small) {
-      if (strm) MSG_SPMV(float, 1, 4, true, gs, v32); else MSG_SPMV(float, 1, 4, false, gs, v32);
+      if (strm) MSG_SPMV32(1, 4, true, gs); else MSG_SPMV32(1, 4, false, gs);
     } else {
-      if (strm) MSG_SPMV(float, 8, 1, true, gl, v32); else MSG_SPMV(float, 8, 1, false, gl, v32);
+      if (strm) MSG_SPMV32(8, 1, true, gl); else MSG_SPMV32(8, 1, false, gl);
     }
   } else {
     if (small) {
@@ -477,6 +588,7 @@ static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float*
     }
   }
 #undef MSG_SPMV
+#undef MSG_SPMV32
 }
 
 // Runs the device PCG on node-layout vectors. The loop body (2 kernels) is
@@ -506,6 +618,7 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     const size_t nv = (size_t)m->pat.n_slots * 32 * 9;
     MSG_TRY(A->d_val32.alloc(ctx, sizeof(float) * std::max<size_t>(1, nv)));
     MSG_TRY(A->d_tmp.alloc(ctx, sizeof(double) * n));
+    MSG_TRY(A->d_tmp2.alloc(ctx, sizeof(float) * n));  // FP32 copy of the search direction
     k_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(nv, A->d_val.as<double>(), A->d_val32.as<float>());
     count_launch(ctx);
   }
@@ -534,7 +647,8 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     for (int k = 0; k < chunk; ++k) {
       launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), mixed ? A->d_val32.as<float>() : nullptr, mixed,
                           A->d_dinv.as<double>(), A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(),
-                          A->d_q.as<double>(), A->d_partial.as<double>(), st, ctx->stream);
+                          A->d_q.as<double>(), A->d_partial.as<double>(), st, ctx->stream,
+                          mixed ? A->d_tmp2.as<float>() : nullptr, grid_v);
       k_pcg_update<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
                                                             A->d_p0.as<double>(), A->d_p1.as<double>(),
                                                             A->d_q.as<double>(), A->d_partial.as<double>(), st);
@@ -553,7 +667,7 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
   for (int round = 0; round < max_rounds; ++round) {
     cudaError_t e = cudaGraphLaunch(A->graph, ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphLaunch");
-    count_launch(ctx, 2 * chunk);
+    count_launch(ctx, (mixed ? 3 : 2) * chunk);
     MSG_CUDA(ctx, cudaMemcpyAsync(h, reinterpret_cast<char*>(st) + off_done, sizeof(int), cudaMemcpyDeviceToHost,
                                   ctx->stream));
     MSG_CUDA(ctx, cudaMemcpyAsync(h + 1, reinterpret_cast<char*>(st) + off_need, sizeof(int),
