@@ -1568,11 +1568,6 @@ constexpr int kQD = kQR * 3 * kQJ * kQK;            // d of the tile's own nodes
 // exchange buffer: corners 1..3 of every element warp (corner 0 belongs to the
 // node pencil of the warp itself and stays in its registers)
 constexpr int kQX = kQWarps * 3 * 3 * kQR;
-// Warp -> element pencil (e = ej + 4 ek) of the packed operator. Warp w runs on
-// SM sub-partition w % 4; the nine node-owning pencils (ej, ek >= 1) carry the
-// node phase, so they are dealt round-robin over the sub-partitions (3, 2, 2,
-// 2) instead of landing on the three sub-partitions of ej = 1, 2, 3.
-__device__ constexpr int kQElemOfWarp[kQWarps] = {5, 6, 7, 13, 10, 11, 9, 14, 15, 1, 3, 8, 0, 2, 4, 12};
 template <int kMode> struct LvlStage2 {
   static constexpr bool kTwo = kMode == kLvlStart || kMode == kLvlPcgZ;
   // Smooth and Resid also stage b of the tile's own nodes (Smooth its dinv as
@@ -1657,10 +1652,7 @@ __global__ void __maxnreg__(128)
     produce(0);
     produce(1);
   }
-  // element pencil of this warp (kQElemOfWarp spreads the node-owning warps
-  // over the four SM sub-partitions, warp w running on w % 4)
-  const int e = kQElemOfWarp[w];
-  const int ej = e % kQEJ, ek = e / kQEJ;
+  const int ej = w % kQEJ, ek = w / kQEJ;
   const bool node_warp = ej >= 1 && ek >= 1;
   uint32_t seq = 0;
   int xsel = 0;
@@ -1712,9 +1704,9 @@ __global__ void __maxnreg__(128)
       for (int c = 0; c < 3; ++c) {
         float2 y = z2;
         if (r00) y = y + own[c];
-        if (r10) y = y + xb[(((e - 1) * 3 + 0) * 3 + c) * 32 + lane];
-        if (r01) y = y + xb[(((e - kQEJ) * 3 + 1) * 3 + c) * 32 + lane];
-        if (r11) y = y + xb[(((e - kQEJ - 1) * 3 + 2) * 3 + c) * 32 + lane];
+        if (r10) y = y + xb[(((w - 1) * 3 + 0) * 3 + c) * 32 + lane];
+        if (r01) y = y + xb[(((w - kQEJ) * 3 + 1) * 3 + c) * 32 + lane];
+        if (r11) y = y + xb[(((w - kQEJ - 1) * 3 + 2) * 3 + c) * 32 + lane];
         const size_t o = (node * 3 + c) * Rp2 + rr2;
         const bool fixed = (mk >> c) & 1;
         float2 v;
@@ -1746,9 +1738,9 @@ __global__ void __maxnreg__(128)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         own[c] = y[0][0][c];
-        xb[((e * 3 + 0) * 3 + c) * 32 + lane] = y[1][0][c];
-        xb[((e * 3 + 1) * 3 + c) * 32 + lane] = y[0][1][c];
-        xb[((e * 3 + 2) * 3 + c) * 32 + lane] = y[1][1][c];
+        xb[((w * 3 + 0) * 3 + c) * 32 + lane] = y[1][0][c];
+        xb[((w * 3 + 1) * 3 + c) * 32 + lane] = y[0][1][c];
+        xb[((w * 3 + 2) * 3 + c) * 32 + lane] = y[1][1][c];
       }
     };
     for (int P = 1; P <= NX; ++P, ++seq) {
@@ -1784,7 +1776,7 @@ __global__ void __maxnreg__(128)
             }
           }
         }
-      const float2 E = reinterpret_cast<const float2*>(pt + S::kOffE)[e * 32 + lane];
+      const float2 E = reinterpret_cast<const float2*>(pt + S::kOffE)[w * 32 + lane];
       if constexpr (kMode == kLvlStart || kMode == kLvlPcgZ) {
         if (node_ok) {
           const size_t node = nrow + P;
