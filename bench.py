@@ -102,6 +102,8 @@ def parse():
     p.add_argument("--mg-omega", type=float, default=None, help="MSG_SET_OPTION multigrid_omega")
     p.add_argument("--mg-packed", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION multigrid_packed (0: level operators on 32-realization tiles)")
+    p.add_argument("--option", action="append", default=[], metavar="KEY=VALUE",
+                   help="MSG_SET_OPTION before anything runs (repeatable)")
     p.add_argument("--tensor-op", type=int, default=None, choices=[0, 1],
                    help="MSG_SET_OPTION tensor_operator (1: level-0 search-direction launch on the tensor cores)")
     return p.parse_args()
@@ -519,6 +521,9 @@ def main():
     from msolve_b200 import _native as N
 
     ctx = M.Context(local)
+    for kv in args.option:
+        k, v = kv.split("=", 1)
+        ctx.set_option(k, float(v))
     if args.reliable_delta is not None:
         ctx.set_option("reliable_delta", args.reliable_delta)
     if args.single_only:

@@ -394,6 +394,9 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * afterwards: 0, default, equal stream priorities; 1: priority grows as the
  * model shrinks, shortest solves first: with serve_persistent = 0 small
  * models' latency under load halves while the largest models wait longer),
+ * "spmv32_shape" (launch shape of the FP32 SpMV of MSG_PCG_SOLVE_MIXED on
+ * large matrices: 0, default, 4 slots per load group and 8 slices per CTA;
+ * 1: 8 and 8; 2: 4 and 4; 3: 8 and 4; results are identical),
  * "tensor_operator" (0, default: every element product in the element's Walsh
  * modes on the FP32 cores; 1: the multigrid loop's level-0 search-direction
  * launch forms E_e Khat u_e on the tensor cores, tcgen05.mma in TF32 with a

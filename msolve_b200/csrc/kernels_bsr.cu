@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_dir32(int n_rows, const dou
 // 3 x 3 block product in FP32, block sums in FP64), partial p.q with the FP64
 // p of the own rows, then alpha as k_pcg_dir_spmv_rows. Same slice / warp
 // layout and streaming loads as k_pcg_dir_spmv_rows.
-template <int kS, int kSpmvWarps, bool kStream>
+template <int kS, int kSpmvWarps, bool kStream, int U = 4>
 __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_spmv32(int n_rows, int n_slices,
                                                                const int64_t* __restrict__ slice_ptr,
                                                                const int* __restrict__ col,
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_spmv32(int n_rows,
   };
   if (live) {
     const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
-    constexpr int U = 4;  // slots per group: 144 bytes of values in flight per thread
+    // U slots per group: 36 U bytes of values in flight per thread
     int64_t s = s0 + w;
     for (; s + (U - 1) * kSpmvWarps < s1; s += U * kSpmvWarps) {
       int cu[U];
@@ -571,14 +571,24 @@ static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float*
 #define MSG_SPMV(V, S, W, STREAM, grid, vals)                                                                       \
   k_pcg_dir_spmv_rows<V, S, W, STREAM><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, vals, dv, rv, p0, p1, qv, pa, \
                                                                         st)
-#define MSG_SPMV32(S, W, STREAM, grid)                                                                           \
-  k_pcg_spmv32<S, W, STREAM><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, p0, p1, qv, pa, st)
+#define MSG_SPMV32(S, W, STREAM, U, grid)                                                                        \
+  k_pcg_spmv32<S, W, STREAM, U><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, p0, p1, qv, pa, st)
   if (mixed) {
     k_pcg_dir32<<<grid_v, kPcgThreads, 0, stream>>>(nr, dv, rv, p0, p1, p32, st);
+    // large matrices: slots per group (4 or 8) and slices per CTA (8 or 4) by the
+    // "spmv32_shape" option (0: 4 / 8, 1: 8 / 8, 2: 4 / 4, 3: 8 / 4)
+    const int shape = ctx->spmv32_shape;
+    const int g4 = (ns + 3) / 4;
     if (small) {
-      if (strm) MSG_SPMV32(1, 4, true, gs); else MSG_SPMV32(1, 4, false, gs);
+      if (strm) MSG_SPMV32(1, 4, true, 4, gs); else MSG_SPMV32(1, 4, false, 4, gs);
+    } else if (shape == 1) {
+      if (strm) MSG_SPMV32(8, 1, true, 8, gl); else MSG_SPMV32(8, 1, false, 8, gl);
+    } else if (shape == 2) {
+      if (strm) MSG_SPMV32(4, 1, true, 4, g4); else MSG_SPMV32(4, 1, false, 4, g4);
+    } else if (shape == 3) {
+      if (strm) MSG_SPMV32(4, 1, true, 8, g4); else MSG_SPMV32(4, 1, false, 8, g4);
     } else {
-      if (strm) MSG_SPMV32(8, 1, true, gl); else MSG_SPMV32(8, 1, false, gl);
+      if (strm) MSG_SPMV32(8, 1, true, 4, gl); else MSG_SPMV32(8, 1, false, 4, gl);
     }
   } else {
     if (small) {
@@ -640,7 +650,8 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     // the pageable copies above are staged before they return
   }
   const int chunk = 8;
-  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x || A->graph_mixed != (int)mixed) {
+  const int graph_kind = mixed ? 1 + ctx->spmv32_shape : 0;  // the captured loop's kernels and shapes
+  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x || A->graph_mixed != graph_kind) {
     if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
     cudaGraph_t g;
     MSG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -659,7 +670,7 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphInstantiate");
     A->graph_chunk = chunk;
     A->graph_x = d_x;
-    A->graph_mixed = mixed ? 1 : 0;
+    A->graph_mixed = graph_kind;
   }
   int* h = ctx->h_flags;  // pinned: done and need
   const size_t off_done = offsetof(PcgState, done), off_need = offsetof(PcgState, need);

@@ -580,6 +580,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
   if (!std::strcmp(key, "multigrid_delta") && value > 0 && value < 1) { ctx->mg_delta = value; return MSG_OK; }
   if (!std::strcmp(key, "multigrid_packed") && (value == 0 || value == 1)) { ctx->mg_packed = (int)value; return MSG_OK; }
   if (!std::strcmp(key, "tensor_operator") && (value == 0 || value == 1)) { ctx->tensor_op = (int)value; return MSG_OK; }
+  if (!std::strcmp(key, "spmv32_shape") && value >= 0 && value <= 3 && value == (int)value) {
+    ctx->spmv32_shape = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "multigrid_fused_coarse") && (value == 0 || value == 1)) {
     ctx->mg_fused_coarse = (int)value;
     return MSG_OK;
@@ -611,6 +615,7 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"multigrid_delta", ctx->mg_delta},
               {"multigrid_packed", (double)ctx->mg_packed},
               {"tensor_operator", (double)ctx->tensor_op},
+              {"spmv32_shape", (double)ctx->spmv32_shape},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
               {"serve_priority", (double)ctx->serve_priority},

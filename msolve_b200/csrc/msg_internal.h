@@ -82,6 +82,7 @@ struct Context {
   int mg_packed = 1;            // 1: level-0 operator with two realizations per lane (packed FP32)
   int mg_fused_coarse = 1;      // 1: all coarsest-level sweeps in one launch (when the level fits a CTA)
   int tensor_op = 0;            // 1: the multigrid loop's level-0 search-direction launch on the tensor cores
+  int spmv32_shape = 0;         // launch shape of the mixed assembled loop's FP32 SpMV (slots per group, slices per CTA)
   int serve_persistent = 1;     // serving lanes: 1 persistent grids, 0 one CTA per work item
   int serve_priority = 0;       // serving lanes: 1 stream priority grows as the model shrinks, 0 all equal
   // Workspace kept across calls (allocation and cudaFree synchronise the
