@@ -407,7 +407,8 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
 int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value);
 /* The current value of an MSG_SET_OPTION key (MSG_ERR_INVALID_ARGUMENT for an
  * unknown key), or of the read-only keys "memory_used" (device bytes charged
- * to the context) and "memory_budget" (its budget, 0 = none). */
+ * to the context), "memory_budget" (its budget, 0 = none) and
+ * "device_free_memory" (free bytes on the context's device). */
 int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value);
 
 /* Kernel launch counter of this context (kernels launched since creation),

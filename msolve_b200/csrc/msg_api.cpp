@@ -602,6 +602,13 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
 int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
   CTX_GUARD(ctx);
   if (!key || !value) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "null option key or value");
+  if (!std::strcmp(key, "device_free_memory")) {  // read-only: free bytes on the context's device
+    size_t free_b = 0, total_b = 0;
+    MSG_CUDA(ctx, cudaSetDevice(ctx->device));
+    MSG_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b));
+    *value = (double)free_b;
+    return MSG_OK;
+  }
   const struct {
     const char* name;
     double v;

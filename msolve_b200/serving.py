@@ -18,6 +18,55 @@ from . import _native as N
 from .analyzers import GpuMesh
 
 
+class Router:
+    """Requests over several servers (one per GPU, or several budgeted contexts
+    of one GPU): each submit goes to the server with the most free device
+    memory for new lanes (budget - used when its context has a budget, else
+    its device's free memory), ties to the one with the fewest requests
+    queued and running. Models are registered on every server; requests are
+    independent, so there is no collective.
+
+        r = Router([Server(Context(d), 64) for d in range(n_gpus)])
+        m = r.add_model(model, kl, tol=1e-8)
+        req = r.submit(m, xi)
+        out = r.poll(req)"""
+
+    def __init__(self, servers):
+        if not servers:
+            raise ValueError("a router needs at least one server")
+        self.servers = list(servers)
+
+    def add_model(self, model, coefficients_provider, tol=1e-8, max_iterations=20000):
+        return [s.add_model(model, coefficients_provider, tol=tol, max_iterations=max_iterations)
+                for s in self.servers]
+
+    def free_memory(self, i):
+        ctx = self.servers[i].ctx
+        budget = ctx.get_option("memory_budget")
+        if budget > 0:
+            return budget - ctx.get_option("memory_used")
+        return ctx.get_option("device_free_memory")
+
+    def choose(self):
+        """Index of the server the next request goes to."""
+        def key(i):
+            st = self.servers[i].stats()
+            return (-self.free_memory(i), st["queued"] + st["running"], i)
+        return min(range(len(self.servers)), key=key)
+
+    def submit(self, model, xi):
+        i = self.choose()
+        return i, self.servers[i].submit(model[i], xi)
+
+    def poll(self, request, timeout_ms=-1):
+        i, rq = request
+        return self.servers[i].poll(rq, timeout_ms=timeout_ms)
+
+    def stop(self):
+        for s in self.servers:
+            s.stop()
+
+
 class Server:
     def __init__(self, ctx, max_batch=64):
         self.ctx = ctx

@@ -231,3 +231,32 @@ def test_admission_waits_for_device_memory(ctx):
     finally:
         srv.stop()
         tight.close()
+
+
+def test_router_over_two_budgeted_contexts():
+    """Two contexts of one GPU with different memory budgets behind a router:
+    requests land where the most budget is free, and every result equals, bit
+    for bit, the same request on a single unconstrained server."""
+    from msolve_b200.serving import Router
+    model, kl = _problem(6)
+    xis = np.random.default_rng(51).standard_normal((24, 12))
+    single = Server(M.Context(0), max_batch=32)
+    try:
+        m = single.add_model(model, kl, tol=1e-10)
+        ref = [single.poll(single.submit(m, xi), timeout_ms=-1)["X"] for xi in xis]
+    finally:
+        single.stop()
+    ctxs = [M.Context(0, 6 << 30), M.Context(0, 2 << 30)]
+    r = Router([Server(c, max_batch=32) for c in ctxs])
+    try:
+        mm = r.add_model(model, kl, tol=1e-10)
+        assert r.choose() == 0  # 6 GB budget, the larger free share
+        reqs = [r.submit(mm, xi) for xi in xis]
+        assert {i for i, _ in reqs} == {0}
+        outs = [r.poll(rq) for rq in reqs]
+        for a, o in zip(ref, outs):
+            assert np.array_equal(a, o["X"])
+    finally:
+        r.stop()
+        for c in ctxs:
+            c.close()
