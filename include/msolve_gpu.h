@@ -270,7 +270,10 @@ int MSG_PC_GALERKIN_MATVEC(MSG_MESH mesh, double nu, const MSG_KL* kl, int m, in
  *     (per-realization geometric multigrid V-cycle preconditioner by default,
  *     Jacobi with MSG_SET_OPTION "multigrid" = 0), FP64 true residual
  *     r = b - K x and FP64 solution update (iterative refinement); stop when
- *     ||b - K x||/||b|| < tol in FP64.
+ *     ||b - K x||/||b|| < tol in FP64. On a mesh that is not a cube lattice
+ *     (distorted or unstructured Hexa8) the realizations are solved one after
+ *     another with the assembled FP32-value PCG and FP64 refinement of
+ *     MSG_PCG_SOLVE_MIXED, to the same FP64 stopping rule.
  * xi [R][kl->n_terms], b [n_dofs]. Outputs (each may be NULL): X [R][n_dofs],
  * tip [R] = X[r][tip_dof], iterations [R] (matrix products per realization),
  * rel_res [R] (final FP64 ||b - K x||/||b||). A realization that does not

@@ -502,6 +502,13 @@ __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restri
 
 }  // namespace
 
+int launch_to_f32(Context* ctx, size_t n, const double* a, float* b) {
+  k_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(n, a, b);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
 int launch_bsr_assemble(Context* ctx, const Mesh* m, const double* d_Ke, double* d_val) {
   const int64_t n_pos = m->pat.n_slots * 32;
   if (n_pos == 0) return MSG_OK;

@@ -425,8 +425,11 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
   KLDevice kd;
   MSG_TRY(kl_prepare(ctx, m, kl, &kd));
   int status = MSG_OK;
-  if (mode == MSG_MODE_MIXED_BATCHED) {
-    if (!m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mixed batched mode needs a structured cube lattice");
+  // meshes that are not cube lattices (distorted or unstructured): the mixed mode
+  // solves realization by realization with the assembled FP32-value PCG and FP64
+  // refinement (MSG_PCG_SOLVE_MIXED's loop) to the same FP64 true residual
+  const bool per_realization = mode == MSG_MODE_FP64_BSR || (mode == MSG_MODE_MIXED_BATCHED && !m->structured);
+  if (mode == MSG_MODE_MIXED_BATCHED && m->structured) {
     BatchOut o;
     std::vector<double> htip(R);
     o.tip = tip ? htip.data() : nullptr;
@@ -434,7 +437,8 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
     o.rel_res = rel_res;
     status = block_mixed_solve(ctx, m, nu, &kd, d_xi, R, Rp, d_b, max_it, tol, tip_dof, d_X, o);
     if (tip) std::copy(htip.begin(), htip.end(), tip);
-  } else if (mode == MSG_MODE_FP64_BSR) {
+  } else if (per_realization) {
+    const bool mixed = mode == MSG_MODE_MIXED_BATCHED;
     // the assembled matrix and its buffers stay in the context for the next call on this mesh
     if (ctx->mc_matrix && ctx->mc_matrix->mesh != m) {
       delete static_cast<msg_matrix*>(ctx->mc_matrix);
@@ -467,7 +471,12 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
                                      *ctx->mc_st, nullptr));
       int its = 0, pst = 0;
       double rr = 0;
-      MSG_TRY(pcg_solve_device(ctx, A, A->d_bn.as<double>(), A->d_xn.as<double>(), max_it, tol, &its, &rr, &pst));
+      if (mixed && A->d_val32.ptr) {  // the FP32 copy of this realization's values
+        const size_t nv = (size_t)m->pat.n_slots * 32 * 9;
+        MSG_TRY(launch_to_f32(ctx, nv, A->d_val.as<double>(), A->d_val32.as<float>()));
+      }
+      MSG_TRY(pcg_solve_device(ctx, A, A->d_bn.as<double>(), A->d_xn.as<double>(), max_it, tol, &its, &rr, &pst,
+                               mixed));
       double* xout = d_X ? d_X + (size_t)r * m->n_dofs : A->d_bd.as<double>();
       MSG_TRY(launch_node_to_dof(ctx, m, A->d_xn.as<double>(), xout, 1, 0, 0));
       if (tip && tip_dof >= 0) {
@@ -478,7 +487,8 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
       if (pst != MSG_OK && status == MSG_OK) status = pst;
     }
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (status != MSG_OK) set_error(ctx, status, "FP64 batch: a realization did not converge");
+    if (status != MSG_OK)
+      set_error(ctx, status, mixed ? "mixed batch: a realization did not converge" : "FP64 batch: a realization did not converge");
   } else {
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "unknown mode %d", mode);
   }

@@ -102,14 +102,30 @@ def test_mixed_result_is_independent_of_the_batch(ctx):
     assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
 
 
-def test_mixed_needs_structured_mesh(ctx):
-    model = M.clamped_block_model(3)
-    model.xyz[5] += 0.01  # break the lattice
-    kl = M.LognormalStochasticCoefficientsProvider([3, 3, 3], 0.6, 5, 4)
-    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=5, simulations=2, mode="mixed")
-    with pytest.raises(M.InvalidOperationError) as e:
-        mc.Solve()
-    assert e.value.code == -2007
+def test_mixed_on_a_distorted_mesh_matches_oracle(ctx):
+    """A mesh that is not a cube lattice (interior nodes moved) takes the mixed
+    mode realization by realization through the assembled FP32-value PCG with
+    FP64 refinement: within 1e-8 of FP64 oracle solves of the same geometry."""
+    n, R, K = 4, 3, 5
+    model = M.clamped_block_model(n)
+    rng = np.random.default_rng(12)
+    inner = (model.xyz > 0.5).all(axis=1) & (model.xyz < n - 0.5).all(axis=1)
+    model.xyz[inner] += 0.15 * rng.uniform(-1, 1, (int(inner.sum()), 3))
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 4)
+    xi = rng.standard_normal((R, K))
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=R, mode="mixed",
+                                                    tolerance=1e-10)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    assert (mc.Residuals < 1e-10).all()
+    cen = O.centroids(model.xyz, model.conn)
+    E = O.kl_field(cen, [n, n, n], kl.table(), xi, sigma=kl.sigma)
+    for r in range(R):
+        Cs = O.CSR(model.n_nodes, model.conn, model.dof, model.n_dofs)
+        Cs.assemble(O.h8_stiffness_batch(model.element_xyz(), E[r], model.poisson)[0])
+        xo, info = Cs.pcg_jacobi(model.subdomains[0].RHS, tol=1e-13)
+        assert info["status"] == 0
+        assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max()
 
 
 def test_mixed_32cube_sample_against_oracle(ctx):
