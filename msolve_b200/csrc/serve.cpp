@@ -228,8 +228,11 @@ void Server::manage() {
   for (;;) {
     cv_manage.wait_for(lk, std::chrono::milliseconds(200));
     if (stop) return;
-    // join and free the lanes whose workers have exited
-    for (auto& m : models)
+    // join and free the lanes whose workers have exited (models by index: a model
+    // added while the lock is released appends to the deque, which moves no
+    // element but invalidates iterators)
+    for (size_t mi = 0; mi < models.size(); ++mi) {
+      ServeModel& m = models[mi];
       for (auto it = m.lanes.begin(); it != m.lanes.end();) {
         if (!it->exited) {
           ++it;
@@ -250,13 +253,16 @@ void Server::manage() {
         lk.lock();
         ++lanes_retired;
       }
+    }
     const auto now = Clock::now();
-    for (auto& m : models)
+    for (size_t mi = 0; mi < models.size(); ++mi) {
+      ServeModel& m = models[mi];
       for (auto& l : m.lanes)
         if (!l.first && !l.retire && l.running == 0 && m.queue.empty() && now - l.idle_since > std::chrono::seconds(1)) {
           l.retire = true;
           cv_work.notify_all();
         }
+    }
     // models with more queued requests than free slots
     for (size_t mi = 0; mi < models.size(); ++mi) {
       ServeModel& m = models[mi];
