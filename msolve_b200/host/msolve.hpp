@@ -710,6 +710,17 @@ class Server {
     requests_.push_back({id, model_id});
     return id;
   }
+  // lanes of a model (-1: all) admitting requests; lanes added and retired so far
+  struct Lanes {
+    int Active = 0;
+    int64_t Added = 0, Retired = 0;
+  };
+  Lanes LaneCount(int model_id = -1) {
+    Lanes l;
+    Check(MSG_SERVE_LANES(ctx_.Handle(), model_id, &l.Active, &l.Added, &l.Retired), ctx_.Handle(),
+          "MSG_SERVE_LANES");
+    return l;
+  }
   // timeout_ms < 0 waits until the request is done; a finished request that
   // did not converge or was cancelled throws as the other calls do
   Result Poll(MSG_REQ id, int timeout_ms = -1) {
