@@ -271,9 +271,12 @@ int MSG_PC_GALERKIN_MATVEC(MSG_MESH mesh, double nu, const MSG_KL* kl, int m, in
  *     Jacobi with MSG_SET_OPTION "multigrid" = 0), FP64 true residual
  *     r = b - K x and FP64 solution update (iterative refinement); stop when
  *     ||b - K x||/||b|| < tol in FP64. On a mesh that is not a cube lattice
- *     (distorted or unstructured Hexa8) the realizations are solved one after
- *     another with the assembled FP32-value PCG and FP64 refinement of
- *     MSG_PCG_SOLVE_MIXED, to the same FP64 stopping rule.
+ *     (distorted or unstructured Hexa8) all realizations are solved at once
+ *     by Jacobi-PCG over an element-by-element operator (each element's
+ *     stiffness at E = 1 computed once, scaled by E per realization; FP32
+ *     loop, FP64 iterate and true residuals) to the same FP64 stopping rule;
+ *     with MSG_SET_OPTION "element_batch" = 0 one after another with the
+ *     assembled FP32-value PCG and FP64 refinement of MSG_PCG_SOLVE_MIXED.
  * xi [R][kl->n_terms], b [n_dofs]. Outputs (each may be NULL): X [R][n_dofs],
  * tip [R] = X[r][tip_dof], iterations [R] (matrix products per realization),
  * rel_res [R] (final FP64 ||b - K x||/||b||). A realization that does not
@@ -403,7 +406,12 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * "tensor_operator" (0, default: every element product in the element's Walsh
  * modes on the FP32 cores; 1: the multigrid loop's level-0 search-direction
  * launch forms E_e Khat u_e on the tensor cores, tcgen05.mma in TF32 with a
- * three-term split; systems without a mass term).
+ * three-term split; systems without a mass term), "element_batch" (mixed
+ * Monte Carlo batches on meshes that are not cube lattices: 1, default, every
+ * realization at once through an element-by-element operator over each
+ * element's stiffness at E = 1 (FP32 Jacobi-PCG, FP64 iterate and true
+ * residuals); 0: realization by realization through the assembled FP32-value
+ * PCG of MSG_PCG_SOLVE_MIXED).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

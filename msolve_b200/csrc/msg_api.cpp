@@ -426,10 +426,21 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
   MSG_TRY(kl_prepare(ctx, m, kl, &kd));
   int status = MSG_OK;
   // meshes that are not cube lattices (distorted or unstructured): the mixed mode
-  // solves realization by realization with the assembled FP32-value PCG and FP64
-  // refinement (MSG_PCG_SOLVE_MIXED's loop) to the same FP64 true residual
-  const bool per_realization = mode == MSG_MODE_FP64_BSR || (mode == MSG_MODE_MIXED_BATCHED && !m->structured);
-  if (mode == MSG_MODE_MIXED_BATCHED && m->structured) {
+  // solves every realization at once element by element (element_batch = 1), or
+  // realization by realization with the assembled FP32-value PCG and FP64
+  // refinement (MSG_PCG_SOLVE_MIXED's loop, element_batch = 0), to the same FP64
+  // true residual
+  const bool mixed_general = mode == MSG_MODE_MIXED_BATCHED && !m->structured;
+  const bool per_realization = mode == MSG_MODE_FP64_BSR || (mixed_general && !ctx->element_batch);
+  if (mixed_general && ctx->element_batch) {
+    BatchOut o;
+    std::vector<double> htip(R);
+    o.tip = tip ? htip.data() : nullptr;
+    o.iterations = iterations;
+    o.rel_res = rel_res;
+    status = ebe_mixed_solve(ctx, m, nu, &kd, d_xi, R, d_b, max_it, tol, tip_dof, d_X, o);
+    if (tip) std::copy(htip.begin(), htip.end(), tip);
+  } else if (mode == MSG_MODE_MIXED_BATCHED && m->structured) {
     BatchOut o;
     std::vector<double> htip(R);
     o.tip = tip ? htip.data() : nullptr;
@@ -594,6 +605,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
     ctx->spmv32_shape = (int)value;
     return MSG_OK;
   }
+  if (!std::strcmp(key, "element_batch") && (value == 0 || value == 1)) {
+    ctx->element_batch = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "multigrid_fused_coarse") && (value == 0 || value == 1)) {
     ctx->mg_fused_coarse = (int)value;
     return MSG_OK;
@@ -633,6 +648,7 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"multigrid_packed", (double)ctx->mg_packed},
               {"tensor_operator", (double)ctx->tensor_op},
               {"spmv32_shape", (double)ctx->spmv32_shape},
+              {"element_batch", (double)ctx->element_batch},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
               {"serve_priority", (double)ctx->serve_priority},

@@ -83,6 +83,7 @@ struct Context {
   int mg_fused_coarse = 1;      // 1: all coarsest-level sweeps in one launch (when the level fits a CTA)
   int tensor_op = 0;            // 1: the multigrid loop's level-0 search-direction launch on the tensor cores
   int spmv32_shape = 0;         // launch shape of the mixed assembled loop's FP32 SpMV (slots per group, slices per CTA)
+  int element_batch = 1;        // mixed mode on non-lattice meshes: 1 batched element-by-element loop, 0 per realization
   int serve_persistent = 1;     // serving lanes: 1 persistent grids, 0 one CTA per work item
   int serve_priority = 0;       // serving lanes: 1 stream priority grows as the model shrinks, 0 all equal
   // Workspace kept across calls (allocation and cudaFree synchronise the
@@ -277,10 +278,10 @@ int launch_dof_to_node(Context* ctx, const Mesh* m, const double* d_in, double* 
                        int64_t out_stride);
 int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* d_out, int n_vec, int64_t in_stride,
                        int64_t out_stride);
-// mixed: FP32 matrix values in the loop's SpMV, FP64 vectors, FP64 true-residual
-// replacement (reliable updates), stop on the FP64 true residual.
 // FP32 copy b[0..n) of FP64 a on the context's stream.
 int launch_to_f32(Context* ctx, size_t n, const double* a, float* b);
+// mixed: FP32 matrix values in the loop's SpMV, FP64 vectors, FP64 true-residual
+// replacement (reliable updates), stop on the FP64 true residual.
 int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b_node, double* d_x_node, int max_it, double tol,
                      int* iterations, double* rel_res, int* status, bool mixed = false);
 
@@ -312,6 +313,11 @@ struct BatchOut {
 };
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
+
+// batched mixed-precision solve on any mesh, element by element (kernels_ebe.cu);
+// realizations padded to 32 inside
+int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R,
+                    const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
 
 // Newmark batch (implicit integration of every realization, constant time step)
 struct NewmarkParams {

@@ -102,30 +102,116 @@ def test_mixed_result_is_independent_of_the_batch(ctx):
     assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
 
 
-def test_mixed_on_a_distorted_mesh_matches_oracle(ctx):
-    """A mesh that is not a cube lattice (interior nodes moved) takes the mixed
-    mode realization by realization through the assembled FP32-value PCG with
-    FP64 refinement: within 1e-8 of FP64 oracle solves of the same geometry."""
-    n, R, K = 4, 3, 5
+def distorted_model(n, seed=12, amp=0.15):
+    """n^3 clamped block whose interior nodes are moved by up to amp in each axis."""
     model = M.clamped_block_model(n)
-    rng = np.random.default_rng(12)
+    rng = np.random.default_rng(seed)
     inner = (model.xyz > 0.5).all(axis=1) & (model.xyz < n - 0.5).all(axis=1)
-    model.xyz[inner] += 0.15 * rng.uniform(-1, 1, (int(inner.sum()), 3))
+    model.xyz[inner] += amp * rng.uniform(-1, 1, (int(inner.sum()), 3))
+    return model
+
+
+def oracle_csr_solve(model, E_r):
+    Cs = O.CSR(model.n_nodes, model.conn, model.dof, model.n_dofs)
+    Cs.assemble(O.h8_stiffness_batch(model.element_xyz(), E_r, model.poisson)[0])
+    xo, info = Cs.pcg_jacobi(model.subdomains[0].RHS, tol=1e-13)
+    assert info["status"] == 0
+    return xo, Cs
+
+
+@pytest.mark.parametrize("element_batch", [1, 0])
+def test_mixed_on_a_distorted_mesh_matches_oracle(ctx, element_batch):
+    """A mesh that is not a cube lattice (interior nodes moved) takes the mixed
+    mode through the batched element-by-element loop (element_batch = 1) or
+    realization by realization through the assembled FP32-value PCG with FP64
+    refinement (0): within 1e-8 of FP64 oracle solves of the same geometry."""
+    n, R, K = 4, 3, 5
+    model = distorted_model(n)
+    rng = np.random.default_rng(12)
     kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 4)
     xi = rng.standard_normal((R, K))
+    ctx.set_option("element_batch", element_batch)
+    try:
+        mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=R,
+                                                        mode="mixed", tolerance=1e-10)
+        mc.RandomNumbers = xi
+        mc.Solve()
+    finally:
+        ctx.set_option("element_batch", 1)
+    assert (mc.Residuals < 1e-10).all()
+    cen = O.centroids(model.xyz, model.conn)
+    E = O.kl_field(cen, [n, n, n], kl.table(), xi, sigma=kl.sigma)
+    for r in range(R):
+        xo, _ = oracle_csr_solve(model, E[r])
+        assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max()
+        assert mc.TipValues[r] == mc.Solutions[r][mc.tip_dof]
+
+
+def test_element_batch_on_a_distorted_mesh_sample(ctx):
+    """Batched element-by-element loop on a distorted 10^3 mesh, 70 realizations
+    (three 32-wide groups, the last one partly padding): sampled realizations
+    within 1e-8 of FP64 oracle solves; the reported residual is the FP64 true
+    residual of the returned displacements; a realization solved alone agrees
+    with its batched solve to 1e-9."""
+    n, R, K = 10, 70, 12
+    model = distorted_model(n, seed=5, amp=0.2)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 8)
+    xi = np.random.default_rng(8).standard_normal((R, K))
     mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=R, mode="mixed",
                                                     tolerance=1e-10)
     mc.RandomNumbers = xi
     mc.Solve()
     assert (mc.Residuals < 1e-10).all()
+    assert (mc.Iterations > 0).all()
     cen = O.centroids(model.xyz, model.conn)
     E = O.kl_field(cen, [n, n, n], kl.table(), xi, sigma=kl.sigma)
+    b = model.subdomains[0].RHS
+    for r in (0, 37, R - 1):
+        xo, Cs = oracle_csr_solve(model, E[r])
+        assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max(), r
+        rr = np.linalg.norm(b - Cs.multiply(mc.Solutions[r])) / np.linalg.norm(b)
+        assert abs(rr - mc.Residuals[r]) <= 1e-3 * mc.Residuals[r] + 1e-15
+    one = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=1, mode="mixed",
+                                                     tolerance=1e-10)
+    one.RandomNumbers = xi[37:38]
+    one.Solve()
+    a = mc.Solutions[37]
+    assert np.abs(one.Solutions[0] - a).max() <= 1e-9 * np.abs(a).max()
+
+
+def test_element_batch_on_a_renumbered_lattice_matches_the_lattice_path(ctx):
+    """The cube lattice with its nodes and elements renumbered at random is not
+    recognised as a lattice and goes through the element-by-element loop; its
+    displacements, mapped back, agree with the lattice path's to 1e-8."""
+    n, R, K = 6, 9, 10
+    base = M.clamped_block_model(n)
+    rng = np.random.default_rng(4)
+    perm = rng.permutation(base.n_nodes)          # new id of old node i: perm[i]
+    eperm = rng.permutation(base.n_elems)
+    xyz = np.empty_like(base.xyz)
+    xyz[perm] = base.xyz
+    conn = perm[base.conn][eperm]
+    ren = M.Model(xyz, conn, base.young, base.poisson)
+    ren.constrain(np.nonzero(np.isclose(xyz[:, 2], 0.0))[0])
+    for node, d, amount in base.loads:
+        ren.add_load(perm[node], d, amount)
+    ren.ConnectDataStructures()
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 8)
+    xi = rng.standard_normal((R, K))
+    runs = []
+    for model in (base, ren):
+        mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=R,
+                                                        mode="mixed", tolerance=1e-11)
+        mc.RandomNumbers = xi
+        mc.Solve()
+        assert (mc.Residuals < 1e-11).all()
+        runs.append(mc)
+    assert M.GpuMesh(ctx, base).info()["structured"] and not M.GpuMesh(ctx, ren).info()["structured"]
     for r in range(R):
-        Cs = O.CSR(model.n_nodes, model.conn, model.dof, model.n_dofs)
-        Cs.assemble(O.h8_stiffness_batch(model.element_xyz(), E[r], model.poisson)[0])
-        xo, info = Cs.pcg_jacobi(model.subdomains[0].RHS, tol=1e-13)
-        assert info["status"] == 0
-        assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max()
+        xb, xr = runs[0].Solutions[r], runs[1].Solutions[r]
+        # DOF (node i, component c) of the base model is DOF (perm[i], c) of the renumbered one
+        nodes, comps = np.nonzero(base.dof >= 0)
+        assert np.abs(xr[ren.dof[perm[nodes], comps]] - xb[base.dof[nodes, comps]]).max() <= 1e-8 * np.abs(xb).max()
 
 
 def test_mixed_32cube_sample_against_oracle(ctx):
