@@ -411,7 +411,10 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * realization at once through an element-by-element operator over each
  * element's stiffness at E = 1 (FP32 Jacobi-PCG, FP64 iterate and true
  * residuals); 0: realization by realization through the assembled FP32-value
- * PCG of MSG_PCG_SOLVE_MIXED).
+ * PCG of MSG_PCG_SOLVE_MIXED), "element_groups" (launch shape of that
+ * element-by-element operator: realization groups of 32 per CTA, each element
+ * row block loaded once for all of them; 0, default: the largest of 8, 4, 2, 1
+ * dividing the padded group count; results are identical).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

@@ -17,10 +17,11 @@
 // the batch.
 //
 // Loop: Jacobi-preconditioned CG per realization with FP32 vectors and the
-// FP32 operator, the iterate x in FP64, and reliable updates: when a
-// realization's recursive ||r|| has dropped by `reliable_delta` since its last
-// true residual, or below tol ||b|| / 2, or it reached the iteration limit,
-// r = b - K x is formed with the FP64 operator for every running realization;
+// FP32 operator, the iterate x in FP64 through an FP32 correction d (x += d at
+// every true residual), and reliable updates: when a realization's recursive
+// ||r|| has dropped by `reliable_delta` since its last true residual, or below
+// tol ||b|| / 2, or it reached the iteration limit, r = b - K x is formed with
+// the FP64 operator for every running realization;
 // a realization whose FP64 true relative residual is below tol stops, the
 // others continue from the true residual with their search directions kept
 // (residual replacement). Per-realization sums go through [block][Rp] partial
@@ -52,26 +53,34 @@ __global__ void k_ebe_unpack(int ne, const double* __restrict__ K300, double* __
 }
 
 // CTA sum (fixed warp order) of the lanes' values into partial[blockIdx.x][Rp]
-// at this CTA's realization group.
-__device__ __forceinline__ void ebe_block_partial(double v, double* sh, double* __restrict__ partial, int Rp) {
+// at realizations col0 .. col0 + 31 (default: this CTA's realization group).
+__device__ __forceinline__ void ebe_block_partial(double v, double* sh, double* __restrict__ partial, int Rp,
+                                                  int col0 = -1) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   sh[w * 32 + lane] = v;
   __syncthreads();
   if (w == 0) {
     double s = 0.0;
     for (int i = 0; i < kEbeWarps; ++i) s += sh[i * 32 + lane];
-    partial[(size_t)blockIdx.x * Rp + blockIdx.y * 32 + lane] = s;
+    partial[(size_t)blockIdx.x * Rp + (col0 < 0 ? blockIdx.y * 32 : col0) + lane] = s;
   }
   __syncthreads();
 }
 
-// Node rows of K u in FP32 for realization rr: the corner's 72 values as 18
-// float4 broadcast loads (each per-corner block starts on a 288-byte boundary).
-__device__ __forceinline__ void ebe_rows32(int n, int Rp, int rr, const int* __restrict__ inc_ptr,
+// Node rows of K u in FP32 for G realization groups of 32 (realizations
+// rb + 32 g + lane): the corner's 72 values as 18 float4 broadcast loads (each
+// per-corner block starts on a 288-byte boundary), used by all G groups. A
+// broadcast load fills 32 lanes' registers, so its cost in the load
+// writeback path is shared by the G groups; every realization's arithmetic
+// (order of the products and sums) is the same for every G.
+template <int G>
+__device__ __forceinline__ void ebe_rows32(int n, int Rp, int rb, const int* __restrict__ inc_ptr,
                                            const int* __restrict__ inc, const int* __restrict__ conn,
                                            const float* __restrict__ Kh, const float* __restrict__ E,
-                                           const float* __restrict__ u, float (&y)[3]) {
-  y[0] = y[1] = y[2] = 0.f;
+                                           const float* __restrict__ u, float (&y)[G][3]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int g = 0; g < G; ++g) y[g][0] = y[g][1] = y[g][2] = 0.f;
   const int k1 = __ldg(inc_ptr + n + 1);
   for (int k = __ldg(inc_ptr + n); k < k1; ++k) {
     const int ea = __ldg(inc + k);
@@ -80,7 +89,9 @@ __device__ __forceinline__ void ebe_rows32(int n, int Rp, int rr, const int* __r
     const int4 c0 = __ldg(reinterpret_cast<const int4*>(conn) + 2 * (size_t)e);
     const int4 c1 = __ldg(reinterpret_cast<const int4*>(conn) + 2 * (size_t)e + 1);
     const int nb[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    float t[G][3];
+#pragma unroll
+    for (int g = 0; g < G; ++g) t[g][0] = t[g][1] = t[g][2] = 0.f;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {  // 4 columns (3 float4, 12 values) per step
       float kv[12];
@@ -90,16 +101,23 @@ __device__ __forceinline__ void ebe_rows32(int n, int Rp, int rr, const int* __r
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         const int j = 4 * q + s;  // column 3b + c2
-        const float ub = u[((size_t)nb[j / 3] * 3 + j % 3) * Rp + rr];
-        t0 = fmaf(kv[3 * s], ub, t0);
-        t1 = fmaf(kv[3 * s + 1], ub, t1);
-        t2 = fmaf(kv[3 * s + 2], ub, t2);
+        const float* __restrict__ ub = u + ((size_t)nb[j / 3] * 3 + j % 3) * Rp + rb + lane;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          const float uv = ub[32 * g];
+          t[g][0] = fmaf(kv[3 * s], uv, t[g][0]);
+          t[g][1] = fmaf(kv[3 * s + 1], uv, t[g][1]);
+          t[g][2] = fmaf(kv[3 * s + 2], uv, t[g][2]);
+        }
       }
     }
-    const float Ee = E[(size_t)e * Rp + rr];
-    y[0] = fmaf(Ee, t0, y[0]);
-    y[1] = fmaf(Ee, t1, y[1]);
-    y[2] = fmaf(Ee, t2, y[2]);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const float Ee = E[(size_t)e * Rp + rb + 32 * g + lane];
+      y[g][0] = fmaf(Ee, t[g][0], y[g][0]);
+      y[g][1] = fmaf(Ee, t[g][1], y[g][1]);
+      y[g][2] = fmaf(Ee, t[g][2], y[g][2]);
+    }
   }
 }
 
@@ -138,7 +156,9 @@ __device__ __forceinline__ void ebe_rows64(int n, int Rp, int rr, const int* __r
   }
 }
 
-// q = K p (FP32, constrained components 0) and the partial p.q per realization.
+// q = K p (FP32, constrained components 0) and the partial p.q per realization;
+// each CTA covers 32 G realizations (grid.y = Rp / (32 G)).
+template <int G>
 __global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_apply32(int n_nodes, int Rp, const int* __restrict__ inc_ptr,
                                                                const int* __restrict__ inc,
                                                                const int* __restrict__ conn,
@@ -149,21 +169,26 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_apply32(int n_nodes, int
                                                                double* __restrict__ partial) {
   __shared__ double sh[kEbeWarps * 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rr = blockIdx.y * 32 + lane;
-  double pq = 0.0;
+  const int rb = blockIdx.y * 32 * G;
+  double pq[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) pq[g] = 0.0;
   for (int n = blockIdx.x * kEbeWarps + w; n < n_nodes; n += gridDim.x * kEbeWarps) {
-    float y[3];
-    ebe_rows32(n, Rp, rr, inc_ptr, inc, conn, Kh, E, p, y);
+    float y[G][3];
+    ebe_rows32<G>(n, Rp, rb, inc_ptr, inc, conn, Kh, E, p, y);
     const unsigned mk = __ldg(mask + n);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const size_t o = ((size_t)n * 3 + c) * Rp + rr;
-      const float v = ((mk >> c) & 1u) ? 0.f : y[c];
-      q[o] = v;
-      pq += (double)p[o] * (double)v;
-    }
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const size_t o = ((size_t)n * 3 + c) * Rp + rb + 32 * g + lane;
+        const float v = ((mk >> c) & 1u) ? 0.f : y[g][c];
+        q[o] = v;
+        pq[g] += (double)p[o] * (double)v;
+      }
   }
-  ebe_block_partial(pq, sh, partial, Rp);
+#pragma unroll
+  for (int g = 0; g < G; ++g) ebe_block_partial(pq[g], sh, partial, Rp, rb + 32 * g);
 }
 
 // FP64 true residual r = b - K x (b one node-layout vector shared by every
@@ -239,14 +264,25 @@ struct EbeScal {
   int* flags;      // [2] realizations asking for a true residual, realizations still running
 };
 
-// x = 0, r = b, p = dinv b (every realization the same b)
+// x = 0, d = 0, r = b, p = dinv b (every realization the same b)
 __global__ void k_ebe_init(size_t n3, int Rp, const double* __restrict__ b, const float* __restrict__ dinv,
-                           double* __restrict__ x, float* __restrict__ r, float* __restrict__ p) {
+                           double* __restrict__ x, float* __restrict__ d, float* __restrict__ r,
+                           float* __restrict__ p) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3 * Rp; i += (size_t)gridDim.x * blockDim.x) {
     const float bv = (float)b[i / Rp];
     x[i] = 0.0;
+    d[i] = 0.f;
     r[i] = bv;
     p[i] = dinv[i] * bv;
+  }
+}
+
+// x += d, d = 0: the FP32 correction accumulated since the last true residual
+// folded into the FP64 iterate
+__global__ void k_ebe_fold(size_t nv, double* __restrict__ x, float* __restrict__ d) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nv; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += (double)d[i];
+    d[i] = 0.f;
   }
 }
 
@@ -271,18 +307,28 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_bnorm(int n_nodes, int R
   ebe_block_partial(s_zr, sh, part_zr, Rp);
 }
 
+// Sum over the block partials of realization r by one warp: lane l adds blocks
+// l, l + 32, ... in order, then a butterfly over the lanes (every lane gets the
+// same bits: each step adds the same two values on both lanes of a pair).
 __device__ __forceinline__ double ebe_sum(const double* __restrict__ part, int n_blocks, int Rp, int r) {
+  const int lane = threadIdx.x & 31;
   double s = 0.0;
-  for (int i = 0; i < n_blocks; ++i) s += part[(size_t)i * Rp + r];
+  for (int i = lane; i < n_blocks; i += 32) s += part[(size_t)i * Rp + r];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
 }
+
+// realization of this warp in the scalar kernels (one warp per realization)
+__device__ __forceinline__ int ebe_warp_realization() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
 
 // Starting scalars; a zero right-hand side (and padding) is done at once with x = 0.
 __global__ void k_ebe_start(int R, int Rp, int n_blocks, const double* __restrict__ part_rr,
                             const double* __restrict__ part_zr, EbeScal s) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = ebe_warp_realization();
   if (r >= Rp) return;
   const double bb = ebe_sum(part_rr, n_blocks, Rp, r), zr = ebe_sum(part_zr, n_blocks, Rp, r);
+  if ((threadIdx.x & 31) != 0) return;
   s.bnorm[r] = sqrt(bb);
   s.rr_ref[r] = bb;
   s.gamma[r] = zr;
@@ -295,13 +341,14 @@ __global__ void k_ebe_start(int R, int Rp, int n_blocks, const double* __restric
 
 // alpha = gamma / p.q (breakdown when p.q <= 0 or not finite)
 __global__ void k_ebe_alpha(int Rp, int n_blocks, const double* __restrict__ part_pq, EbeScal s) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = ebe_warp_realization();
   if (r >= Rp) return;
   if (s.done[r]) {
-    s.alpha[r] = 0.f;
+    if ((threadIdx.x & 31) == 0) s.alpha[r] = 0.f;
     return;
   }
   const double pq = ebe_sum(part_pq, n_blocks, Rp, r);
+  if ((threadIdx.x & 31) != 0) return;
   s.its[r] += 1;
   if (!(pq > 0.0) || !isfinite(pq)) {
     s.done[r] = 2;
@@ -311,12 +358,13 @@ __global__ void k_ebe_alpha(int Rp, int n_blocks, const double* __restrict__ par
   s.alpha[r] = (float)(s.gamma[r] / pq);
 }
 
-// x += alpha p (FP64), r -= alpha q, partials (dinv r).r and r.r
+// d += alpha p (the FP32 correction of the FP64 iterate), r -= alpha q,
+// partials (dinv r).r and r.r
 __global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_update(int n_nodes, int Rp, const float* __restrict__ alpha,
                                                               const float* __restrict__ p,
                                                               const float* __restrict__ q,
                                                               const float* __restrict__ dinv,
-                                                              double* __restrict__ x, float* __restrict__ r,
+                                                              float* __restrict__ d, float* __restrict__ r,
                                                               double* __restrict__ part_zr,
                                                               double* __restrict__ part_rr) {
   __shared__ double sh[kEbeWarps * 32];
@@ -328,7 +376,7 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_update(int n_nodes, int 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const size_t o = ((size_t)n * 3 + c) * Rp + rr;
-      x[o] += (double)al * (double)p[o];
+      d[o] = fmaf(al, p[o], d[o]);
       const float rv = fmaf(-al, q[o], r[o]);
       r[o] = rv;
       s_zr += (double)(dinv[o] * rv) * (double)rv;
@@ -343,13 +391,14 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_update(int n_nodes, int 
 // it reached the iteration limit.
 __global__ void k_ebe_beta(int Rp, int n_blocks, const double* __restrict__ part_zr,
                            const double* __restrict__ part_rr, EbeScal s, double tol2, double delta2, int max_it) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = ebe_warp_realization();
   if (r >= Rp) return;
   if (s.done[r]) {
-    s.beta[r] = 0.f;
+    if ((threadIdx.x & 31) == 0) s.beta[r] = 0.f;
     return;
   }
   const double zr = ebe_sum(part_zr, n_blocks, Rp, r), rr = ebe_sum(part_rr, n_blocks, Rp, r);
+  if ((threadIdx.x & 31) != 0) return;
   s.beta[r] = s.gamma[r] > 0.0 ? (float)(zr / s.gamma[r]) : 0.f;
   s.gamma[r] = zr;
   const double b2 = s.bnorm[r] * s.bnorm[r];
@@ -361,10 +410,11 @@ __global__ void k_ebe_beta(int Rp, int n_blocks, const double* __restrict__ part
 // realizations still running.
 __global__ void k_ebe_true(int Rp, int n_blocks, const double* __restrict__ part_rr,
                            const double* __restrict__ part_zr, EbeScal s, double tol, int max_it) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = ebe_warp_realization();
   if (r >= Rp) return;
   if (s.done[r]) return;
   const double rr = ebe_sum(part_rr, n_blocks, Rp, r), zr = ebe_sum(part_zr, n_blocks, Rp, r);
+  if ((threadIdx.x & 31) != 0) return;
   const double err = s.bnorm[r] > 0.0 ? sqrt(rr) / s.bnorm[r] : 0.0;
   s.res[r] = err;
   s.rr_ref[r] = rr;
@@ -458,8 +508,9 @@ int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kd, const 
   MSG_TRY(d_E32.alloc(ctx, sizeof(float) * (size_t)ne * Rp));
   MSG_TRY(launch_kl_field(ctx, m, kd, R, Rp, d_xi, d_E64.as<double>(), d_E32.as<float>(), nullptr));
   // vectors [node*3 + c][Rp] and scalars
-  DevMem d_x, d_r, d_p, d_q, d_dinv, d_bn, d_scal, d_part;
+  DevMem d_x, d_d, d_r, d_p, d_q, d_dinv, d_bn, d_scal, d_part;
   MSG_TRY(d_x.alloc(ctx, sizeof(double) * nv));
+  MSG_TRY(d_d.alloc(ctx, sizeof(float) * nv));
   MSG_TRY(d_r.alloc(ctx, sizeof(float) * nv));
   MSG_TRY(d_p.alloc(ctx, sizeof(float) * nv));
   MSG_TRY(d_q.alloc(ctx, sizeof(float) * nv));
@@ -487,12 +538,39 @@ int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kd, const 
   const int* dinc = d_inc.as<int>();
   const int* conn = m->d_conn.as<int>();
   const uint8_t* mask = m->d_mask.as<uint8_t>();
-  const int sb = (Rp + 255) / 256;
+  const int sb = Rp / 8;  // scalar kernels: one warp per realization, 8 per CTA
+  // realization groups of 32 per CTA of the FP32 operator: the largest of 8, 4,
+  // 2, 1 that divides the group count (or the element_groups option when it does)
+  const int ng = Rp / 32;
+  int G = ng % 8 == 0 ? 8 : ng % 4 == 0 ? 4 : ng % 2 == 0 ? 2 : 1;
+  if (ctx->element_groups > 0 && ng % ctx->element_groups == 0) G = ctx->element_groups;
+  const dim3 grid_op(gx, ng / G);
+  auto apply32 = [&]() {
+    const float* K32 = d_K32.as<float>();
+    const float* E32 = d_E32.as<float>();
+    switch (G) {
+      case 8:
+        k_ebe_apply32<8><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
+                                                              d_p.as<float>(), d_q.as<float>(), part_a);
+        break;
+      case 4:
+        k_ebe_apply32<4><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
+                                                              d_p.as<float>(), d_q.as<float>(), part_a);
+        break;
+      case 2:
+        k_ebe_apply32<2><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
+                                                              d_p.as<float>(), d_q.as<float>(), part_a);
+        break;
+      default:
+        k_ebe_apply32<1><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
+                                                              d_p.as<float>(), d_q.as<float>(), part_a);
+    }
+  };
   const int gv = (int)std::min<size_t>((nv + 255) / 256, (size_t)ctx->sm_count * 16);
   k_ebe_dinv<<<nn, 128, 0, st>>>(nn, Rp, dptr, dinc, d_K64.as<double>(), d_E64.as<double>(), mask,
                                  d_dinv.as<float>());
-  k_ebe_init<<<gv, 256, 0, st>>>(n3, Rp, d_bn.as<double>(), d_dinv.as<float>(), d_x.as<double>(), d_r.as<float>(),
-                                 d_p.as<float>());
+  k_ebe_init<<<gv, 256, 0, st>>>(n3, Rp, d_bn.as<double>(), d_dinv.as<float>(), d_x.as<double>(), d_d.as<float>(),
+                                 d_r.as<float>(), d_p.as<float>());
   k_ebe_bnorm<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, d_bn.as<double>(), d_dinv.as<float>(), part_a, part_b);
   k_ebe_start<<<sb, 256, 0, st>>>(R, Rp, gx, part_a, part_b, s);
   count_launch(ctx, 4);
@@ -506,11 +584,10 @@ int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kd, const 
   for (int chunk = 0; chunk < max_chunks; ++chunk) {
     MSG_CUDA(ctx, cudaMemsetAsync(s.flags, 0, 2 * sizeof(int), st));
     for (int k = 0; k < kEbeCheck; ++k) {
-      k_ebe_apply32<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, d_K32.as<float>(), d_E32.as<float>(),
-                                                      mask, d_p.as<float>(), d_q.as<float>(), part_a);
+      apply32();
       k_ebe_alpha<<<sb, 256, 0, st>>>(Rp, gx, part_a, s);
       k_ebe_update<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, s.alpha, d_p.as<float>(), d_q.as<float>(),
-                                                     d_dinv.as<float>(), d_x.as<double>(), d_r.as<float>(), part_a,
+                                                     d_dinv.as<float>(), d_d.as<float>(), d_r.as<float>(), part_a,
                                                      part_b);
       k_ebe_beta<<<sb, 256, 0, st>>>(Rp, gx, part_a, part_b, s, tol2, delta2, max_it);
       k_ebe_dir<<<gv, 256, 0, st>>>(n3, Rp, s.beta, d_dinv.as<float>(), d_r.as<float>(), d_p.as<float>());
@@ -521,17 +598,21 @@ int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kd, const 
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[0] == 0) continue;
     // FP64 true residual of the running realizations, then stop or continue each
+    k_ebe_fold<<<gv, 256, 0, st>>>(nv, d_x.as<double>(), d_d.as<float>());
     k_ebe_resid64<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, d_K64.as<double>(), d_E64.as<double>(),
                                                     mask, d_bn.as<double>(), d_x.as<double>(), d_dinv.as<float>(),
                                                     s.done, d_r.as<float>(), part_a, part_b);
     k_ebe_true<<<sb, 256, 0, st>>>(Rp, gx, part_a, part_b, s, tol, max_it);
-    count_launch(ctx, 2);
+    count_launch(ctx, 3);
     MSG_CUDA(ctx, cudaGetLastError());
     MSG_CUDA(ctx, cudaMemcpyAsync(h + 1, s.flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[1] == 0) break;
   }
-  // results
+  // results (a realization stops right after a fold, so d holds no correction
+  // here unless the chunk bound ended the loop)
+  k_ebe_fold<<<gv, 256, 0, st>>>(nv, d_x.as<double>(), d_d.as<float>());
+  count_launch(ctx);
   if (d_X && m->n_dofs > 0) {
     const dim3 g((m->n_dofs + 31) / 32, Rp / 32);
     k_ebe_gather<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, R, Rp, m->d_free_rows.as<int>(), d_x.as<double>(), d_X);

@@ -397,7 +397,9 @@ static int assemble_from_device_ke(Context* ctx, Mesh* m, const double* d_Ke, Ma
 // Element matrices for per-element E (device), then assembly into A.
 static int assemble_from_device_E(Context* ctx, Mesh* m, const double* d_E, double nu, Matrix* A, DevMem& ke,
                                   DevMem& st, int* neg_det) {
-  if (!ke.ptr) MSG_TRY(ke.alloc(ctx, sizeof(double) * 300 * (size_t)m->n_elems));
+  // ke may be a buffer kept from a call on another mesh: grow it to this mesh
+  const size_t ke_bytes = sizeof(double) * 300 * (size_t)m->n_elems;
+  if (!ke.ptr || ke.bytes < ke_bytes) MSG_TRY(ke.alloc(ctx, ke_bytes));
   if (!st.ptr) MSG_TRY(st.alloc(ctx, sizeof(int)));
   MSG_CUDA(ctx, cudaMemsetAsync(st.ptr, 0, sizeof(int), ctx->stream));
   MSG_TRY(launch_h8_ke(ctx, m->n_elems, m->d_exyz.as<double>(), d_E, 0.0, nu, ke.as<double>(), st.as<int>()));
@@ -609,6 +611,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
     ctx->element_batch = (int)value;
     return MSG_OK;
   }
+  if (!std::strcmp(key, "element_groups") && (value == 0 || value == 1 || value == 2 || value == 4 || value == 8)) {
+    ctx->element_groups = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "multigrid_fused_coarse") && (value == 0 || value == 1)) {
     ctx->mg_fused_coarse = (int)value;
     return MSG_OK;
@@ -649,6 +655,7 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"tensor_operator", (double)ctx->tensor_op},
               {"spmv32_shape", (double)ctx->spmv32_shape},
               {"element_batch", (double)ctx->element_batch},
+              {"element_groups", (double)ctx->element_groups},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
               {"serve_priority", (double)ctx->serve_priority},

@@ -84,6 +84,7 @@ struct Context {
   int tensor_op = 0;            // 1: the multigrid loop's level-0 search-direction launch on the tensor cores
   int spmv32_shape = 0;         // launch shape of the mixed assembled loop's FP32 SpMV (slots per group, slices per CTA)
   int element_batch = 1;        // mixed mode on non-lattice meshes: 1 batched element-by-element loop, 0 per realization
+  int element_groups = 0;       // realization groups of 32 per CTA of the element-by-element FP32 operator (0 auto)
   int serve_persistent = 1;     // serving lanes: 1 persistent grids, 0 one CTA per work item
   int serve_priority = 0;       // serving lanes: 1 stream priority grows as the model shrinks, 0 all equal
   // Workspace kept across calls (allocation and cudaFree synchronise the

@@ -147,6 +147,29 @@ def test_mixed_on_a_distorted_mesh_matches_oracle(ctx, element_batch):
         assert mc.TipValues[r] == mc.Solutions[r][mc.tip_dof]
 
 
+@pytest.mark.parametrize("mode,element_batch", [("fp64", 1), ("mixed", 0)])
+def test_per_realization_path_on_a_larger_second_mesh(mode, element_batch):
+    """The per-realization path keeps its element-matrix buffer in the context
+    across calls; a call on a mesh with more elements than the previous one
+    grows it (fresh context: 3^3, then 5^3 distorted meshes, oracle parity on
+    both)."""
+    c = M.Context(0)
+    c.set_option("element_batch", element_batch)
+    K, R = 4, 2
+    for n in (3, 5):
+        model = distorted_model(n, seed=n)
+        kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 4)
+        xi = np.random.default_rng(n).standard_normal((R, K))
+        mc = M.MonteCarloAnalyzerWithStochasticMaterial(c, model, kl, expansion_order=K, simulations=R, mode=mode,
+                                                        tolerance=1e-12 if mode == "fp64" else 1e-10)
+        mc.RandomNumbers = xi
+        mc.Solve()
+        E = O.kl_field(O.centroids(model.xyz, model.conn), [n, n, n], kl.table(), xi, sigma=kl.sigma)
+        for r in range(R):
+            xo, _ = oracle_csr_solve(model, E[r])
+            assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max(), (n, r)
+
+
 def test_element_batch_on_a_distorted_mesh_sample(ctx):
     """Batched element-by-element loop on a distorted 10^3 mesh, 70 realizations
     (three 32-wide groups, the last one partly padding): sampled realizations
