@@ -293,6 +293,40 @@ int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R,
                               const double* b_dev, int mode, int max_it, double tol, int tip_dof, double* X_dev,
                               double* tip, int* iterations, double* rel_res);
 
+/* One system of a ragged batch: a Hexa8 mesh of any shape and size (of the
+ * context the batch runs on), its material and KL field, R realizations and
+ * the load. Host buffers: xi [R][kl->n_terms], b [n_dofs]; outputs (each may
+ * be NULL) X [R][n_dofs], tip [R] = X[r][tip_dof], iterations [R] (operator
+ * products), rel_res [R] (final FP64 ||b - K x||/||b||). */
+typedef struct {
+  MSG_MESH mesh;
+  double nu;
+  const MSG_KL* kl;
+  int R;
+  const double* xi;
+  const double* b;
+  int tip_dof;
+  double* X;
+  double* tip;
+  int* iterations;
+  double* rel_res;
+} MSG_RAGGED_SYSTEM;
+/* The realization loop of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
+ * (ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:232-296)
+ * for several systems of uneven mesh size at once: every iteration of every
+ * realization of every system runs in the same three persistent launches
+ * (element-by-element FP32 operator over each element's stiffness at E = 1
+ * scaled by E per realization, per-realization scalars, fused vector update),
+ * eight iterations to a CUDA graph launch, Jacobi-preconditioned CG (the
+ * reference's SolverPCG with the diagonal preconditioner) with the iterate in
+ * FP64 and FP64 true residuals, to ||b - K x||/||b|| < tol in FP64 for each
+ * realization. A system's results do not depend on the other systems in the
+ * batch (the same bits alone and in any mix of systems). No
+ * reference counterpart as an entry point (the reference solves one
+ * realization after another). Returns MSG_ERR_NOT_CONVERGED or
+ * MSG_ERR_BREAKDOWN as MSG_MC_SOLVE_BATCH, with every other output complete. */
+int MSG_MC_SOLVE_RAGGED(MSG_CTX ctx, int n_systems, const MSG_RAGGED_SYSTEM* systems, int max_it, double tol);
+
 /* ------------------------------------------------------------------ Newmark batch */
 /* Parameters of NewmarkDynamicAnalyzer (ISAAR.MSolve.Analyzers/NewmarkDynamicAnalyzer.cs:38-77)
  * with the structural provider's effective matrix K + a0 M + a1 C

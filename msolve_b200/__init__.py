@@ -9,6 +9,7 @@ from ._native import (ArgumentError, Context, InvalidOperationError, MSolveError
 from .analyzers import (GaussianStochasticCoefficientsProvider, GpuMatrix, GpuMesh, LinearAnalyzer,
                         LognormalStochasticCoefficientsProvider,
                         MonteCarloAnalyzer, MonteCarloAnalyzerWithStochasticMaterial, NewmarkDynamicAnalyzer,
+                        RaggedMonteCarloBatch,
                         SolverPCGReorthogonalizationSearchVectorCalculator, SolverPCGReorthogonalized, ProblemStructural, SolverPCG,
                         StaticAnalyzer, h8_mass_batch, h8_stiffness_batch, h8_stress_batch, realization_stresses)
 from .polynomial_chaos import PolynomialChaosSolverPCGMatrixCalculator, pc_basis
@@ -19,7 +20,8 @@ from .model import (Hexa8MeshGenerator, MassAccelerationSinusoidalLoad, Model, c
 __all__ = [
     "ArgumentError", "Autotuner", "Context", "InvalidOperationError", "MSolveError", "MSG_MODE_FP64_BSR", "MSG_MODE_MIXED_BATCHED",
     "lib", "GaussianStochasticCoefficientsProvider", "GpuMatrix", "GpuMesh", "LinearAnalyzer", "LognormalStochasticCoefficientsProvider",
-    "MonteCarloAnalyzer", "MonteCarloAnalyzerWithStochasticMaterial", "SolverPCGReorthogonalizationSearchVectorCalculator",
+    "MonteCarloAnalyzer", "MonteCarloAnalyzerWithStochasticMaterial", "RaggedMonteCarloBatch",
+    "SolverPCGReorthogonalizationSearchVectorCalculator",
     "SolverPCGReorthogonalized", "NewmarkDynamicAnalyzer", "ProblemStructural", "SolverPCG",
     "StaticAnalyzer", "h8_mass_batch", "h8_stiffness_batch", "h8_stress_batch", "realization_stresses",
     "Hexa8MeshGenerator", "MassAccelerationSinusoidalLoad",

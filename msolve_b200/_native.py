@@ -69,6 +69,22 @@ class MSG_NEWMARK(C.Structure):
     ]
 
 
+class MSG_RAGGED_SYSTEM(C.Structure):
+    _fields_ = [
+        ("mesh", _vp),
+        ("nu", C.c_double),
+        ("kl", C.POINTER(MSG_KL)),
+        ("R", C.c_int),
+        ("xi", _d),
+        ("b", _d),
+        ("tip_dof", C.c_int),
+        ("X", _d),
+        ("tip", _d),
+        ("iterations", _i),
+        ("rel_res", _d),
+    ]
+
+
 SIGNATURES = {
     "MSG_CREATE": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_vp)]),
     "MSG_DESTROY": (C.c_int, [_vp]),
@@ -104,6 +120,7 @@ SIGNATURES = {
                                      C.c_double, C.c_int, _d, _d, _i, _d]),
     "MSG_MC_SOLVE_BATCH_DEVICE": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _vp, _vp, C.c_int,
                                             C.c_int, C.c_double, C.c_int, _vp, _d, _i, _d]),
+    "MSG_MC_SOLVE_RAGGED": (C.c_int, [_vp, C.c_int, C.POINTER(MSG_RAGGED_SYSTEM), C.c_int, C.c_double]),
     "MSG_NEWMARK_BATCH": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _d, C.POINTER(MSG_NEWMARK), _d,
                                     C.c_int, C.c_double, C.c_int, _d, _d, _i]),
     "MSG_SERVE_START": (C.c_int, [_vp, C.c_int]),

@@ -583,6 +583,55 @@ class MonteCarloAnalyzer(MonteCarloAnalyzerWithStochasticMaterial):
         super().__init__(ctx, model, coefficients_provider, expansion_order, simulations, **kw)
 
 
+class RaggedMonteCarloBatch:
+    """Monte Carlo realizations of several models of uneven size in one batch
+    (MSG_MC_SOLVE_RAGGED): each added system is a model (any Hexa8 mesh), its
+    coefficient provider and its random-number rows; Solve() runs the
+    realization loop of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
+    (MonteCarloAnalyzerWithStochasticMaterial.cs:232-296) for all of them in the
+    same launches (mixed-precision Jacobi-PCG, FP64 true residual below
+    `tolerance`). Results per system, in the order added: Solutions [R][n_dofs]
+    (if keep_solutions), TipValues [R], Iterations [R], Residuals [R]. A
+    system's results do not depend on the other systems in the batch."""
+
+    def __init__(self, ctx, max_iterations=20000, tolerance=1e-8):
+        self.ctx, self.max_iterations, self.tolerance = ctx, max_iterations, tolerance
+        self.systems = []
+        self.Results = []
+
+    def add(self, model, coefficients_provider, random_numbers, tip_dof=None, keep_solutions=True):
+        xi = np.ascontiguousarray(np.atleast_2d(random_numbers)[:, :coefficients_provider.n_terms], dtype=np.float64)
+        if xi.shape[1] != coefficients_provider.n_terms or xi.shape[0] < 1:
+            raise N.ArgumentError(N.MSG_ERR_INVALID_ARGUMENT,
+                                  f"random numbers {xi.shape} for {coefficients_provider.n_terms} KL terms")
+        self.systems.append(dict(model=model, kl=coefficients_provider, xi=xi,
+                                 tip_dof=_tip_dof(model) if tip_dof is None else tip_dof,
+                                 keep=keep_solutions, mesh=GpuMesh(self.ctx, model)))
+        return len(self.systems) - 1
+
+    def Solve(self):
+        n = len(self.systems)
+        arr = (N.MSG_RAGGED_SYSTEM * max(1, n))()
+        keep = []  # ctypes structs and arrays alive for the call
+        self.Results = []
+        for i, y in enumerate(self.systems):
+            m, R = y["model"], y["xi"].shape[0]
+            res = dict(Solutions=np.zeros((R, m.n_dofs)) if y["keep"] else None, TipValues=np.zeros(R),
+                       Iterations=np.zeros(R, dtype=np.int32), Residuals=np.zeros(R))
+            kl = y["kl"].struct()
+            b = N.f64(m.subdomains[0].RHS)
+            keep += [kl, b]
+            a = arr[i]
+            a.mesh, a.nu, a.kl, a.R = y["mesh"].handle, float(m.poisson), C.pointer(kl), R
+            a.xi, a.b, a.tip_dof = N.ptr(y["xi"]), N.ptr(b), int(y["tip_dof"])
+            a.X = N.ptr(res["Solutions"]) if y["keep"] else None
+            a.tip, a.iterations, a.rel_res = N.ptr(res["TipValues"]), N.ptr(res["Iterations"], N._i), N.ptr(res["Residuals"])
+            self.Results.append(res)
+        st = N.lib().MSG_MC_SOLVE_RAGGED(self.ctx.handle, n, arr, int(self.max_iterations), float(self.tolerance))
+        N.check(st, self.ctx.handle, "MSG_MC_SOLVE_RAGGED")
+        return self.Results
+
+
 class NewmarkDynamicAnalyzer:
     """Implicit Newmark integration (NewmarkDynamicAnalyzer.cs:16-315) of every
     realization of a stochastic-material batch at once. Same parameters as the

@@ -1,32 +1,52 @@
-// Batched mixed-precision Monte Carlo solve on any Hexa8 mesh (distorted or
-// unstructured): the path of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
+// Batched mixed-precision Monte Carlo solves on any Hexa8 meshes (distorted,
+// unstructured, and of different sizes in one batch): the path of
+// MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
 // (ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:232-296)
-// for all realizations at once, where the cube-lattice operators do not apply.
+// for all realizations of several systems at once, where the cube-lattice
+// operators do not apply.
 //
-// The stiffness of element e in realization r is K_e = E_{e,r} Khat_e with
-// Khat_e the element's stiffness at E = 1 (the constitutive matrix is linear in
-// E; Hexa8WithStochasticMaterial.cs:61-110 evaluates E once per element), so
-// Khat_e is computed once per mesh and shared by every realization. The
-// operator is applied node by node: the rows of node n are
+// Operator. The stiffness of element e in realization r is K_e = E_{e,r} Khat_e
+// with Khat_e the element's stiffness at E = 1 (the constitutive matrix is
+// linear in E; Hexa8WithStochasticMaterial.cs:61-110 evaluates E once per
+// element), so Khat_e is computed once per mesh and shared by every
+// realization. The operator is applied node by node: the rows of node n are
 //   y_n = sum over the elements e around n (corner a of e) of
 //         E_{e,r} Khat_e[3a .. 3a+2][0 .. 23] u_e,
-// one warp per node and 32 realizations (realization innermost, every vector
-// access one 128-byte line), the 72 values of the corner's rows read as
-// broadcast loads. Each output is written once and the sum over the elements
-// runs in a fixed order: no atomics, results deterministic and independent of
-// the batch.
+// one warp per node and up to 8 groups of 32 realizations (realization
+// innermost, every vector access one 128-byte line). The 72 values of the
+// corner's rows are broadcast loads shared by the groups. Each output is
+// written once and the sums over the elements run in a fixed order: no
+// atomics, deterministic results.
 //
-// Loop: Jacobi-preconditioned CG per realization with FP32 vectors and the
-// FP32 operator, the iterate x in FP64 through an FP32 correction d (x += d at
-// every true residual), and reliable updates: when a realization's recursive
-// ||r|| has dropped by `reliable_delta` since its last true residual, or below
-// tol ||b|| / 2, or it reached the iteration limit, r = b - K x is formed with
-// the FP64 operator for every running realization;
-// a realization whose FP64 true relative residual is below tol stops, the
-// others continue from the true residual with their search directions kept
-// (residual replacement). Per-realization sums go through [block][Rp] partial
-// arrays added in block order.
+// Batch. A batch is a list of systems (mesh, E field, realizations, load);
+// every node-level launch walks one list of work items (system, block of 64
+// nodes, range of realizations) with persistent CTAs, so systems of uneven
+// size share every launch. Per-realization sums go through [block][Rp]
+// partial arrays of their system, added in block order by one warp per
+// realization.
+//
+// Loop (Jacobi-preconditioned CG per realization, SolverPCG.cs:105-149 with
+// the reference's diagonal preconditioner), three launches an iteration:
+//   operator:  q = K p (FP32) and the partials p.q (FP64), (D r).q, q.D.q (FP32
+//              within a warp);
+//   scalars:   alpha = gamma / p.q and the next gamma by the expansion
+//              (D r').r' = gamma - 2 alpha (D r).q + alpha^2 q.D.q, so that
+//              beta is known before the update pass;
+//   update:    d += alpha p, r -= alpha q, p = D r + beta p with the exact
+//              partials (D r).r and r.r of the new residual (the next
+//              iteration's gamma and the convergence checks).
+// The iterate is x (FP64) plus an FP32 correction d. A realization asks for a
+// true residual when its recursive ||r|| has dropped by `reliable_delta` since
+// its last one, or below tol ||b|| / 2, or at the iteration limit; at the end
+// of the 8-iteration chunk (one CUDA graph launch) every running realization
+// of a system where one asked folds d into x and replaces r by the FP64
+// r = b - K x (the FP64 operator); those below tol stop, the others continue
+// from the true residual with their directions kept. Only those systems take
+// part, so a system's arithmetic is independent of the rest of the batch: it
+// gives the same bits alone and in any mix.
 #include <algorithm>
+#include <chrono>
+#include <memory>
 #include <vector>
 
 #include "msg_internal.h"
@@ -34,8 +54,52 @@
 namespace msg {
 namespace {
 
-constexpr int kEbeWarps = 8;  // warps (nodes in flight) per CTA
-constexpr int kEbeCheck = 8;  // iterations between host reads of the loop flags
+constexpr int kEbeWarps = 8;   // warps per CTA
+constexpr int kEbeCheck = 8;   // iterations per chunk (graph launch) between host reads of the flags
+constexpr int kRgBlk = 64;     // nodes per work item of the operator passes: 8 warps x 8 nodes
+constexpr int kRgBlkU = 512;   // nodes per work item of the update pass: 8 warps x 64 nodes
+constexpr int kRgParts = 5;    // partial arrays per system over kRgBlk blocks
+enum { kPq = 0, kDrq = 1, kDqd = 2, kZr = 3, kRr = 4 };
+
+// One system of a batch (device table).
+struct RgSys {
+  int n_nodes, Rp, n_blk, goff;  // goff: index of realization 0 in the batch-wide scalar arrays
+  int n_blk_u;                   // blocks of the update pass
+  const int* inc_ptr;            // [n_nodes + 1] node -> (element, corner) incidence
+  const int* inc;                // (e << 3) | a, ascending e per node
+  const int* conn;               // [n_elems][8]
+  const uint8_t* mask;           // [n_nodes] constrained components
+  const float* K32;              // [n_elems][8][72] Khat_e per corner (FP32)
+  const double* K64;             // the same in FP64
+  const float* E32;              // [n_elems][Rp]
+  const double* E64;
+  const double* b;               // [n_nodes * 3] load (node layout)
+  double* x;                     // [n_nodes * 3][Rp]
+  float *d, *r, *p, *q, *dinv;   // [n_nodes * 3][Rp]
+  double* part;                  // [kRgParts][n_blk][Rp]
+  double* part_u;                // [2][n_blk_u][Rp]: (D r).r and r.r of the update pass
+};
+struct RgItem {
+  int sys, blk, rb, G;  // nodes blk * 64 .., realizations rb .. rb + 32 G - 1
+};
+// Batch-wide per-realization state, index = system goff + realization.
+struct RgScal {
+  double *gamma, *rr_ref, *bnorm, *res;
+  float *alpha, *beta;
+  int *done;   // 0 running, 1 converged (or padding), 2 breakdown, 3 iteration limit
+  int *its;    // FP32 operator products
+  int *rsys;   // system of the realization
+  int *sreq;   // per system: 1 when one of its realizations asked for a true residual
+  int *gact;   // per group of 32 realizations: 1 while one of them runs
+  int* flags;  // [0] requests in this chunk, [1] realizations still running
+};
+
+// Whether the work item has a running realization (the same for the whole CTA).
+__device__ __forceinline__ bool rg_item_active(const int* __restrict__ gact, int goff, int rb, int G) {
+  bool a = false;
+  for (int g = 0; g < G; ++g) a |= gact[(goff + rb) / 32 + g] != 0;
+  return a;
+}
 
 // Khat_e in the per-corner layout (FP64 and FP32): entry [e][a][b][c2][r] =
 // Khat_e[3a + r][3b + c2], i.e. the 72 values the rows of corner a need, with
@@ -52,19 +116,39 @@ __global__ void k_ebe_unpack(int ne, const double* __restrict__ K300, double* __
   }
 }
 
-// CTA sum (fixed warp order) of the lanes' values into partial[blockIdx.x][Rp]
-// at realizations col0 .. col0 + 31 (default: this CTA's realization group).
-__device__ __forceinline__ void ebe_block_partial(double v, double* sh, double* __restrict__ partial, int Rp,
-                                                  int col0 = -1) {
+// CTA sum (fixed warp order) of the lanes' values into dst[lane].
+__device__ __forceinline__ void rg_block_partial(double v, double* sh, double* __restrict__ dst) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   sh[w * 32 + lane] = v;
   __syncthreads();
   if (w == 0) {
     double s = 0.0;
     for (int i = 0; i < kEbeWarps; ++i) s += sh[i * 32 + lane];
-    partial[(size_t)blockIdx.x * Rp + (col0 < 0 ? blockIdx.y * 32 : col0) + lane] = s;
+    dst[lane] = s;
   }
   __syncthreads();
+}
+
+// The same for N values per lane with one barrier pair: value i of every lane
+// into dst(i)[lane], warps added in the same fixed order.
+template <int N, class T, int M, class Dst>
+__device__ __forceinline__ void rg_block_partials(const T (&v)[N], double (&sh)[M], Dst dst) {
+  static_assert(M >= N * kEbeWarps * 32, "shared buffer of rg_block_partials");
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < N; ++i) sh[(i * kEbeWarps + w) * 32 + lane] = (double)v[i];
+  __syncthreads();
+  for (int j = threadIdx.x; j < N * 32; j += blockDim.x) {
+    const int i = j >> 5, l = j & 31;
+    double t = 0.0;
+    for (int k = 0; k < kEbeWarps; ++k) t += sh[(i * kEbeWarps + k) * 32 + l];
+    dst(i)[l] = t;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double* rg_part(const RgSys& S, int k, int blk, int col) {
+  return S.part + ((size_t)k * S.n_blk + blk) * S.Rp + col;
 }
 
 // Node rows of K u in FP32 for G realization groups of 32 (realizations
@@ -121,12 +205,16 @@ __device__ __forceinline__ void ebe_rows32(int n, int Rp, int rb, const int* __r
   }
 }
 
-// The same rows in FP64 (true residuals).
-__device__ __forceinline__ void ebe_rows64(int n, int Rp, int rr, const int* __restrict__ inc_ptr,
+// The node rows in FP64 for G realization groups (true residuals), the
+// corner's values loaded once for the G groups.
+template <int G>
+__device__ __forceinline__ void ebe_rows64(int n, int Rp, int rb, const int* __restrict__ inc_ptr,
                                            const int* __restrict__ inc, const int* __restrict__ conn,
                                            const double* __restrict__ Kh, const double* __restrict__ E,
-                                           const double* __restrict__ u, double (&y)[3]) {
-  y[0] = y[1] = y[2] = 0.0;
+                                           const double* __restrict__ u, double (&y)[G][3]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int g = 0; g < G; ++g) y[g][0] = y[g][1] = y[g][2] = 0.0;
   const int k1 = __ldg(inc_ptr + n + 1);
   for (int k = __ldg(inc_ptr + n); k < k1; ++k) {
     const int ea = __ldg(inc + k);
@@ -135,99 +223,332 @@ __device__ __forceinline__ void ebe_rows64(int n, int Rp, int rr, const int* __r
     const int4 c0 = __ldg(reinterpret_cast<const int4*>(conn) + 2 * (size_t)e);
     const int4 c1 = __ldg(reinterpret_cast<const int4*>(conn) + 2 * (size_t)e + 1);
     const int nb[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    double t[G][3];
+#pragma unroll
+    for (int g = 0; g < G; ++g) t[g][0] = t[g][1] = t[g][2] = 0.0;
 #pragma unroll
     for (int q = 0; q < 12; ++q) {  // 2 columns (3 double2, 6 values) per step
       const double2 ka = __ldg(K2 + 3 * q), kb = __ldg(K2 + 3 * q + 1), kc = __ldg(K2 + 3 * q + 2);
       const int j0 = 2 * q, j1 = 2 * q + 1;
-      const double u0 = u[((size_t)nb[j0 / 3] * 3 + j0 % 3) * Rp + rr];
-      const double u1 = u[((size_t)nb[j1 / 3] * 3 + j1 % 3) * Rp + rr];
-      t0 = fma(ka.x, u0, t0);
-      t1 = fma(ka.y, u0, t1);
-      t2 = fma(kb.x, u0, t2);
-      t0 = fma(kb.y, u1, t0);
-      t1 = fma(kc.x, u1, t1);
-      t2 = fma(kc.y, u1, t2);
+      const double* __restrict__ u0p = u + ((size_t)nb[j0 / 3] * 3 + j0 % 3) * Rp + rb + lane;
+      const double* __restrict__ u1p = u + ((size_t)nb[j1 / 3] * 3 + j1 % 3) * Rp + rb + lane;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const double u0 = u0p[32 * g], u1 = u1p[32 * g];
+        t[g][0] = fma(ka.x, u0, t[g][0]);
+        t[g][1] = fma(ka.y, u0, t[g][1]);
+        t[g][2] = fma(kb.x, u0, t[g][2]);
+        t[g][0] = fma(kb.y, u1, t[g][0]);
+        t[g][1] = fma(kc.x, u1, t[g][1]);
+        t[g][2] = fma(kc.y, u1, t[g][2]);
+      }
     }
-    const double Ee = E[(size_t)e * Rp + rr];
-    y[0] = fma(Ee, t0, y[0]);
-    y[1] = fma(Ee, t1, y[1]);
-    y[2] = fma(Ee, t2, y[2]);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const double Ee = E[(size_t)e * Rp + rb + 32 * g + lane];
+      y[g][0] = fma(Ee, t[g][0], y[g][0]);
+      y[g][1] = fma(Ee, t[g][1], y[g][1]);
+      y[g][2] = fma(Ee, t[g][2], y[g][2]);
+    }
   }
 }
 
-// q = K p (FP32, constrained components 0) and the partial p.q per realization;
-// each CTA covers 32 G realizations (grid.y = Rp / (32 G)).
+// ---------------------------------------------------------------- loop kernels (work items)
+
+// q = K p (FP32, constrained components 0) and the partials p.q, (D r).q, q.D.q.
 template <int G>
-__global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_apply32(int n_nodes, int Rp, const int* __restrict__ inc_ptr,
-                                                               const int* __restrict__ inc,
-                                                               const int* __restrict__ conn,
-                                                               const float* __restrict__ Kh,
-                                                               const float* __restrict__ E,
-                                                               const uint8_t* __restrict__ mask,
-                                                               const float* __restrict__ p, float* __restrict__ q,
-                                                               double* __restrict__ partial) {
-  __shared__ double sh[kEbeWarps * 32];
+__device__ __forceinline__ void rg_apply_item(const RgSys& S, int blk, int rb, double* sh) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rb = blockIdx.y * 32 * G;
+  const int Rp = S.Rp;
+  // p.q (alpha) in FP64; (D r).q and q.D.q, which only enter beta's estimate, in
+  // FP32 within a warp (FP64 across the warps and blocks)
   double pq[G];
+  float drq[G], dqd[G];
 #pragma unroll
-  for (int g = 0; g < G; ++g) pq[g] = 0.0;
-  for (int n = blockIdx.x * kEbeWarps + w; n < n_nodes; n += gridDim.x * kEbeWarps) {
+  for (int g = 0; g < G; ++g) {
+    pq[g] = 0.0;
+    drq[g] = dqd[g] = 0.f;
+  }
+  const int n1 = min(S.n_nodes, (blk + 1) * kRgBlk);
+  for (int n = blk * kRgBlk + w; n < n1; n += kEbeWarps) {
     float y[G][3];
-    ebe_rows32<G>(n, Rp, rb, inc_ptr, inc, conn, Kh, E, p, y);
-    const unsigned mk = __ldg(mask + n);
+    ebe_rows32<G>(n, Rp, rb, S.inc_ptr, S.inc, S.conn, S.K32, S.E32, S.p, y);
+    const unsigned mk = __ldg(S.mask + n);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int g = 0; g < G; ++g) {
         const size_t o = ((size_t)n * 3 + c) * Rp + rb + 32 * g + lane;
         const float v = ((mk >> c) & 1u) ? 0.f : y[g][c];
-        q[o] = v;
-        pq[g] += (double)p[o] * (double)v;
+        S.q[o] = v;
+        const float dv = S.dinv[o];
+        pq[g] += (double)S.p[o] * (double)v;
+        drq[g] = fmaf(dv * S.r[o], v, drq[g]);
+        dqd[g] = fmaf(dv * v, v, dqd[g]);
+      }
+  }
+  // one value at a time: three arrays of G live across one barrier spill under
+  // the 128-register cap
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    rg_block_partial(pq[g], sh, rg_part(S, kPq, blk, rb + 32 * g));
+    rg_block_partial((double)drq[g], sh, rg_part(S, kDrq, blk, rb + 32 * g));
+    rg_block_partial((double)dqd[g], sh, rg_part(S, kDqd, blk, rb + 32 * g));
+  }
+}
+
+__global__ void __launch_bounds__(32 * kEbeWarps, 2) k_rg_apply(const RgSys* __restrict__ Sys,
+                                                            const RgItem* __restrict__ items, int n_items,
+                                                            const int* __restrict__ gact) {
+  __shared__ double sh[kEbeWarps * 32];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    const RgSys S = Sys[I.sys];
+    if (!rg_item_active(gact, S.goff, I.rb, I.G)) continue;
+    switch (I.G) {
+      case 8: rg_apply_item<8>(S, I.blk, I.rb, sh); break;
+      case 4: rg_apply_item<4>(S, I.blk, I.rb, sh); break;
+      case 2: rg_apply_item<2>(S, I.blk, I.rb, sh); break;
+      default: rg_apply_item<1>(S, I.blk, I.rb, sh);
+    }
+  }
+}
+
+// d += alpha p, r -= alpha q, p = D r + beta p; partials (D r).r and r.r. A
+// memory-bound pass with nothing to share between realization groups: work
+// items of 512 nodes and one group (few registers, long streams per warp);
+// items of groups without a running realization skipped.
+__global__ void __launch_bounds__(32 * kEbeWarps) k_rg_update(const RgSys* __restrict__ Sys,
+                                                             const RgItem* __restrict__ items, int n_items,
+                                                             RgScal s) {
+  __shared__ double sh[2 * kEbeWarps * 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    const RgSys S = Sys[I.sys];
+    if (!s.gact[(S.goff + I.rb) / 32]) continue;  // the same for the whole CTA
+    const int Rp = S.Rp, col = I.rb;
+    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
+    const float al = s.alpha[S.goff + col + lane], be = s.beta[S.goff + col + lane];
+    double zr = 0.0, rr = 0.0;
+    for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
+        const float pv = S.p[o];
+        const float rv = fmaf(-al, S.q[o], S.r[o]);
+        S.d[o] = fmaf(al, pv, S.d[o]);
+        const float zv = S.dinv[o] * rv;
+        S.p[o] = fmaf(be, pv, zv);
+        S.r[o] = rv;
+        zr += (double)zv * (double)rv;
+        rr += (double)rv * (double)rv;
+      }
+    const double v[2] = {zr, rr};
+    rg_block_partials(v, sh, [&](int i) { return S.part_u + ((size_t)i * S.n_blk_u + I.blk) * Rp + col; });
+  }
+}
+
+// x += d, d = 0 for the systems with a true residual pending (all = 1: every
+// system; a realization's d is 0 after its last true residual).
+__global__ void k_rg_fold(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items, int n_items, RgScal s,
+                          int all) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    if (!all && !s.sreq[I.sys]) continue;
+    const RgSys S = Sys[I.sys];
+    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlk);
+    for (int g = 0; g < I.G; ++g) {
+      const int col = I.rb + 32 * g + lane;
+      for (int n = I.blk * kRgBlk + w; n < n1; n += kEbeWarps)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const size_t o = ((size_t)n * 3 + c) * S.Rp + col;
+          S.x[o] += (double)S.d[o];
+          S.d[o] = 0.f;
+        }
+    }
+  }
+}
+
+// FP64 true residual r = b - K x (constrained components 0) of every
+// realization of the systems with a true residual pending, into r (FP32);
+// partials r.r and (D r).r. The item's groups two at a time.
+template <int G>
+__device__ __forceinline__ void rg_resid_groups(const RgSys& S, int blk, int rb, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double s_rr[G], s_zr[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) s_rr[g] = s_zr[g] = 0.0;
+  const int n1 = min(S.n_nodes, (blk + 1) * kRgBlk);
+  for (int n = blk * kRgBlk + w; n < n1; n += kEbeWarps) {
+    double y[G][3];
+    ebe_rows64<G>(n, S.Rp, rb, S.inc_ptr, S.inc, S.conn, S.K64, S.E64, S.x, y);
+    const unsigned mk = __ldg(S.mask + n);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const size_t o = ((size_t)n * 3 + c) * S.Rp + rb + 32 * g + lane;
+        const double v = ((mk >> c) & 1u) ? 0.0 : S.b[(size_t)n * 3 + c] - y[g][c];
+        const float v32 = (float)v;
+        S.r[o] = v32;
+        s_rr[g] += v * v;
+        s_zr[g] += (double)(S.dinv[o] * v32) * (double)v32;
       }
   }
 #pragma unroll
-  for (int g = 0; g < G; ++g) ebe_block_partial(pq[g], sh, partial, Rp, rb + 32 * g);
+  for (int g = 0; g < G; ++g) {
+    rg_block_partial(s_rr[g], sh, rg_part(S, kRr, blk, rb + 32 * g));
+    rg_block_partial(s_zr[g], sh, rg_part(S, kZr, blk, rb + 32 * g));
+  }
 }
 
-// FP64 true residual r = b - K x (b one node-layout vector shared by every
-// realization; constrained components 0) of the running realizations into the
-// FP32 residual; partials ||r||^2 and (dinv r).r.
-__global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_resid64(int n_nodes, int Rp, const int* __restrict__ inc_ptr,
-                                                               const int* __restrict__ inc,
-                                                               const int* __restrict__ conn,
-                                                               const double* __restrict__ Kh,
-                                                               const double* __restrict__ E,
-                                                               const uint8_t* __restrict__ mask,
-                                                               const double* __restrict__ b,
-                                                               const double* __restrict__ x,
-                                                               const float* __restrict__ dinv,
-                                                               const int* __restrict__ done,
-                                                               float* __restrict__ r32, double* __restrict__ part_rr,
-                                                               double* __restrict__ part_zr) {
+__global__ void __launch_bounds__(32 * kEbeWarps) k_rg_resid64(const RgSys* __restrict__ Sys,
+                                                              const RgItem* __restrict__ items, int n_items,
+                                                              RgScal s) {
   __shared__ double sh[kEbeWarps * 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rr = blockIdx.y * 32 + lane;
-  const bool run = done[rr] == 0;
-  double s_rr = 0.0, s_zr = 0.0;
-  for (int n = blockIdx.x * kEbeWarps + w; n < n_nodes; n += gridDim.x * kEbeWarps) {
-    double y[3];
-    ebe_rows64(n, Rp, rr, inc_ptr, inc, conn, Kh, E, x, y);
-    const unsigned mk = __ldg(mask + n);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const size_t o = ((size_t)n * 3 + c) * Rp + rr;
-      const double v = ((mk >> c) & 1u) ? 0.0 : b[(size_t)n * 3 + c] - y[c];
-      const float v32 = (float)v;
-      if (run) r32[o] = v32;
-      s_rr += v * v;
-      s_zr += (double)(dinv[o] * v32) * (double)v32;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    if (!s.sreq[I.sys]) continue;  // the same for the whole CTA
+    const RgSys S = Sys[I.sys];
+    for (int g = 0; g < I.G; g += 2) {
+      const int grp = (S.goff + I.rb) / 32 + g;
+      const bool a0 = s.gact[grp] != 0, a1 = g + 1 < I.G && s.gact[grp + 1] != 0;
+      if (a0 && a1)
+        rg_resid_groups<2>(S, I.blk, I.rb + 32 * g, sh);
+      else if (a0)
+        rg_resid_groups<1>(S, I.blk, I.rb + 32 * g, sh);
+      else if (a1)
+        rg_resid_groups<1>(S, I.blk, I.rb + 32 * (g + 1), sh);
     }
   }
-  ebe_block_partial(s_rr, sh, part_rr, Rp);
-  ebe_block_partial(s_zr, sh, part_zr, Rp);
 }
+
+// ---------------------------------------------------------------- per-realization scalars (one warp each)
+
+// Sum over the block partials of realization r by one warp: lane l adds blocks
+// l, l + 32, ... in order, then a butterfly over the lanes (every lane gets the
+// same bits: each step adds the same two values on both lanes of a pair).
+__device__ __forceinline__ double rg_sum(const double* __restrict__ part, int n_blk, int Rp, int r) {
+  const int lane = threadIdx.x & 31;
+  double v = 0.0;
+  for (int i = lane; i < n_blk; i += 32) v += part[(size_t)i * Rp + r];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int rg_warp_index() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
+
+// A realization asks for a true residual of its system.
+__device__ __forceinline__ void rg_check(const RgScal& s, int g, double rr, double tol2, double delta2, int max_it) {
+  const double b2 = s.bnorm[g] * s.bnorm[g];
+  if (rr < tol2 * b2 || rr < delta2 * s.rr_ref[g] || s.its[g] >= max_it || !isfinite(rr)) {
+    const int sys = s.rsys[g];
+    if (!s.sreq[sys]) atomicAdd(s.flags, 1);
+    s.sreq[sys] = 1;
+  }
+}
+
+// alpha = gamma / p.q and beta = gamma' / gamma with gamma' by the expansion;
+// consume = 1: gamma and the check from the previous update's exact partials.
+__global__ void k_rg_scalar(const RgSys* __restrict__ Sys, int Rtot, RgScal s, int consume, double tol2,
+                            double delta2, int max_it) {
+  const int g = rg_warp_index();
+  if (g >= Rtot) return;
+  const int lane = threadIdx.x & 31;
+  if (s.done[g]) {
+    if (lane == 0) s.alpha[g] = s.beta[g] = 0.f;
+    return;
+  }
+  const RgSys& S = Sys[s.rsys[g]];
+  const int Rp = S.Rp, nb = S.n_blk, r = g - S.goff;
+  const size_t P = (size_t)nb * Rp;
+  double gam = s.gamma[g];
+  if (consume) {
+    const size_t Pu = (size_t)S.n_blk_u * Rp;
+    const double zr = rg_sum(S.part_u, S.n_blk_u, Rp, r), rr = rg_sum(S.part_u + Pu, S.n_blk_u, Rp, r);
+    gam = zr;
+    if (lane == 0) rg_check(s, g, rr, tol2, delta2, max_it);
+  }
+  const double pq = rg_sum(S.part + kPq * P, nb, Rp, r);
+  const double drq = rg_sum(S.part + kDrq * P, nb, Rp, r);
+  const double dqd = rg_sum(S.part + kDqd * P, nb, Rp, r);
+  if (lane != 0) return;
+  s.its[g] += 1;
+  s.gamma[g] = gam;
+  if (!(gam > 0.0)) {  // r = 0: nothing to do until the true residual
+    s.alpha[g] = s.beta[g] = 0.f;
+    return;
+  }
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    s.done[g] = 2;
+    s.alpha[g] = s.beta[g] = 0.f;
+    return;
+  }
+  const float af = (float)(gam / pq);
+  const double a = (double)af;
+  const double est = gam - 2.0 * a * drq + a * a * dqd;
+  s.alpha[g] = af;
+  s.beta[g] = est > 0.0 ? (float)(est / gam) : 0.f;
+}
+
+// End of a chunk: gamma and the check from the last update's partials;
+// flags[1] counts the realizations still running.
+__global__ void k_rg_chunk_end(const RgSys* __restrict__ Sys, int Rtot, RgScal s, double tol2, double delta2,
+                               int max_it) {
+  const int g = rg_warp_index();
+  if (g >= Rtot || s.done[g]) return;
+  const RgSys& S = Sys[s.rsys[g]];
+  const int Rp = S.Rp, r = g - S.goff;
+  const size_t Pu = (size_t)S.n_blk_u * Rp;
+  const double zr = rg_sum(S.part_u, S.n_blk_u, Rp, r), rr = rg_sum(S.part_u + Pu, S.n_blk_u, Rp, r);
+  if ((threadIdx.x & 31) != 0) return;
+  s.gamma[g] = zr;
+  rg_check(s, g, rr, tol2, delta2, max_it);
+  atomicAdd(s.flags + 1, 1);
+}
+
+// After the FP64 true residual: a realization of a system with a true
+// residual stops below tol (or at the iteration limit) or continues from the
+// true residual; flags[1] counts the realizations still running.
+__global__ void k_rg_true(const RgSys* __restrict__ Sys, int Rtot, RgScal s, double tol, int max_it) {
+  const int g = rg_warp_index();
+  if (g >= Rtot || s.done[g]) return;
+  const int lane = threadIdx.x & 31;
+  if (!s.sreq[s.rsys[g]]) {
+    if (lane == 0) atomicAdd(s.flags + 1, 1);
+    return;
+  }
+  const RgSys& S = Sys[s.rsys[g]];
+  const int Rp = S.Rp, nb = S.n_blk, r = g - S.goff;
+  const size_t P = (size_t)nb * Rp;
+  const double rr = rg_sum(S.part + kRr * P, nb, Rp, r), zr = rg_sum(S.part + kZr * P, nb, Rp, r);
+  if (lane != 0) return;
+  const double err = s.bnorm[g] > 0.0 ? sqrt(rr) / s.bnorm[g] : 0.0;
+  s.res[g] = err;
+  s.rr_ref[g] = rr;
+  s.gamma[g] = zr;
+  if (err < tol) {
+    s.done[g] = 1;
+  } else if (s.its[g] >= max_it || !isfinite(err)) {
+    s.done[g] = 3;
+  } else {
+    atomicAdd(s.flags + 1, 1);
+  }
+}
+
+// gact[group] = 1 while one of the group's 32 realizations runs (one warp per group).
+__global__ void k_rg_active(int n_groups, RgScal s) {
+  const int grp = rg_warp_index();
+  if (grp >= n_groups) return;
+  const unsigned run = __ballot_sync(0xffffffffu, s.done[grp * 32 + (threadIdx.x & 31)] == 0);
+  if ((threadIdx.x & 31) == 0) s.gact[grp] = run != 0u;
+}
+
+// ---------------------------------------------------------------- per-system setup and results
 
 // Jacobi diagonal of every realization: dinv = 1 / sum_e E_{e,r} Khat_e[3a+c][3a+c]
 // (1 on constrained components).
@@ -251,188 +572,47 @@ __global__ void k_ebe_dinv(int n_nodes, int Rp, const int* __restrict__ inc_ptr,
   }
 }
 
-// Per-realization loop state.
-struct EbeScal {
-  double* gamma;   // [Rp] (dinv r).r of the current residual
-  double* rr_ref;  // [Rp] ||r||^2 at the last true residual
-  double* bnorm;   // [Rp]
-  double* res;     // [Rp] last FP64 true relative residual
-  float* alpha;    // [Rp]
-  float* beta;     // [Rp]
-  int* done;       // [Rp] 0 running, 1 converged (or padding), 2 breakdown, 3 iteration limit
-  int* its;        // [Rp] FP32 operator products
-  int* flags;      // [2] realizations asking for a true residual, realizations still running
-};
-
-// x = 0, d = 0, r = b, p = dinv b (every realization the same b)
-__global__ void k_ebe_init(size_t n3, int Rp, const double* __restrict__ b, const float* __restrict__ dinv,
-                           double* __restrict__ x, float* __restrict__ d, float* __restrict__ r,
-                           float* __restrict__ p) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3 * Rp; i += (size_t)gridDim.x * blockDim.x) {
-    const float bv = (float)b[i / Rp];
-    x[i] = 0.0;
-    d[i] = 0.f;
-    r[i] = bv;
-    p[i] = dinv[i] * bv;
-  }
-}
-
-// x += d, d = 0: the FP32 correction accumulated since the last true residual
-// folded into the FP64 iterate
-__global__ void k_ebe_fold(size_t nv, double* __restrict__ x, float* __restrict__ d) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nv; i += (size_t)gridDim.x * blockDim.x) {
-    x[i] += (double)d[i];
-    d[i] = 0.f;
-  }
-}
-
-// Partials of ||b||^2 and (dinv b).b per realization (the residual at x = 0).
-__global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_bnorm(int n_nodes, int Rp, const double* __restrict__ b,
-                                                             const float* __restrict__ dinv,
-                                                             double* __restrict__ part_rr,
-                                                             double* __restrict__ part_zr) {
+// x = 0, d = 0, r = b, p = D b; partials (D b).b and b.b. Grid (n_blk, Rp / 32).
+__global__ void __launch_bounds__(32 * kEbeWarps) k_rg_init(RgSys S) {
   __shared__ double sh[kEbeWarps * 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rr = blockIdx.y * 32 + lane;
-  double s_rr = 0.0, s_zr = 0.0;
-  for (int n = blockIdx.x * kEbeWarps + w; n < n_nodes; n += gridDim.x * kEbeWarps)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double v = b[(size_t)n * 3 + c];
-      const float v32 = (float)v;
-      s_rr += v * v;
-      s_zr += (double)(dinv[((size_t)n * 3 + c) * Rp + rr] * v32) * (double)v32;
-    }
-  ebe_block_partial(s_rr, sh, part_rr, Rp);
-  ebe_block_partial(s_zr, sh, part_zr, Rp);
-}
-
-// Sum over the block partials of realization r by one warp: lane l adds blocks
-// l, l + 32, ... in order, then a butterfly over the lanes (every lane gets the
-// same bits: each step adds the same two values on both lanes of a pair).
-__device__ __forceinline__ double ebe_sum(const double* __restrict__ part, int n_blocks, int Rp, int r) {
-  const int lane = threadIdx.x & 31;
-  double s = 0.0;
-  for (int i = lane; i < n_blocks; i += 32) s += part[(size_t)i * Rp + r];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
-}
-
-// realization of this warp in the scalar kernels (one warp per realization)
-__device__ __forceinline__ int ebe_warp_realization() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
-
-// Starting scalars; a zero right-hand side (and padding) is done at once with x = 0.
-__global__ void k_ebe_start(int R, int Rp, int n_blocks, const double* __restrict__ part_rr,
-                            const double* __restrict__ part_zr, EbeScal s) {
-  const int r = ebe_warp_realization();
-  if (r >= Rp) return;
-  const double bb = ebe_sum(part_rr, n_blocks, Rp, r), zr = ebe_sum(part_zr, n_blocks, Rp, r);
-  if ((threadIdx.x & 31) != 0) return;
-  s.bnorm[r] = sqrt(bb);
-  s.rr_ref[r] = bb;
-  s.gamma[r] = zr;
-  s.alpha[r] = 0.f;
-  s.beta[r] = 0.f;
-  s.its[r] = 0;
-  s.res[r] = bb > 0.0 ? 1.0 : 0.0;
-  s.done[r] = (r >= R || !(bb > 0.0)) ? 1 : 0;
-}
-
-// alpha = gamma / p.q (breakdown when p.q <= 0 or not finite)
-__global__ void k_ebe_alpha(int Rp, int n_blocks, const double* __restrict__ part_pq, EbeScal s) {
-  const int r = ebe_warp_realization();
-  if (r >= Rp) return;
-  if (s.done[r]) {
-    if ((threadIdx.x & 31) == 0) s.alpha[r] = 0.f;
-    return;
-  }
-  const double pq = ebe_sum(part_pq, n_blocks, Rp, r);
-  if ((threadIdx.x & 31) != 0) return;
-  s.its[r] += 1;
-  if (!(pq > 0.0) || !isfinite(pq)) {
-    s.done[r] = 2;
-    s.alpha[r] = 0.f;
-    return;
-  }
-  s.alpha[r] = (float)(s.gamma[r] / pq);
-}
-
-// d += alpha p (the FP32 correction of the FP64 iterate), r -= alpha q,
-// partials (dinv r).r and r.r
-__global__ void __launch_bounds__(32 * kEbeWarps) k_ebe_update(int n_nodes, int Rp, const float* __restrict__ alpha,
-                                                              const float* __restrict__ p,
-                                                              const float* __restrict__ q,
-                                                              const float* __restrict__ dinv,
-                                                              float* __restrict__ d, float* __restrict__ r,
-                                                              double* __restrict__ part_zr,
-                                                              double* __restrict__ part_rr) {
-  __shared__ double sh[kEbeWarps * 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int rr = blockIdx.y * 32 + lane;
-  const float al = alpha[rr];
+  const int blk = blockIdx.x, col = blockIdx.y * 32 + lane;
+  const int n1 = min(S.n_nodes, (blk + 1) * kRgBlk);
   double s_zr = 0.0, s_rr = 0.0;
-  for (int n = blockIdx.x * kEbeWarps + w; n < n_nodes; n += gridDim.x * kEbeWarps)
+  for (int n = blk * kRgBlk + w; n < n1; n += kEbeWarps)
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const size_t o = ((size_t)n * 3 + c) * Rp + rr;
-      d[o] = fmaf(al, p[o], d[o]);
-      const float rv = fmaf(-al, q[o], r[o]);
-      r[o] = rv;
-      s_zr += (double)(dinv[o] * rv) * (double)rv;
-      s_rr += (double)rv * (double)rv;
+      const size_t o = ((size_t)n * 3 + c) * S.Rp + col;
+      const double bd = S.b[(size_t)n * 3 + c];
+      const float bv = (float)bd;
+      const float zv = S.dinv[o] * bv;
+      S.x[o] = 0.0;
+      S.d[o] = 0.f;
+      S.r[o] = bv;
+      S.p[o] = zv;
+      s_zr += (double)zv * (double)bv;
+      s_rr += bd * bd;
     }
-  ebe_block_partial(s_zr, sh, part_zr, Rp);
-  ebe_block_partial(s_rr, sh, part_rr, Rp);
+  rg_block_partial(s_zr, sh, rg_part(S, kZr, blk, blockIdx.y * 32));
+  rg_block_partial(s_rr, sh, rg_part(S, kRr, blk, blockIdx.y * 32));
 }
 
-// beta = gamma_new / gamma; a realization asks for a true residual when its
-// recursive ||r||^2 is below tol2 ||b||^2 or delta2 times the last true one, or
-// it reached the iteration limit.
-__global__ void k_ebe_beta(int Rp, int n_blocks, const double* __restrict__ part_zr,
-                           const double* __restrict__ part_rr, EbeScal s, double tol2, double delta2, int max_it) {
-  const int r = ebe_warp_realization();
-  if (r >= Rp) return;
-  if (s.done[r]) {
-    if ((threadIdx.x & 31) == 0) s.beta[r] = 0.f;
-    return;
-  }
-  const double zr = ebe_sum(part_zr, n_blocks, Rp, r), rr = ebe_sum(part_rr, n_blocks, Rp, r);
+// Starting scalars of one system's realizations (one warp each); a zero load
+// (and padding) is done at once with x = 0.
+__global__ void k_rg_start(RgSys S, int R, RgScal s) {
+  const int r = rg_warp_index();
+  if (r >= S.Rp) return;
+  const size_t P = (size_t)S.n_blk * S.Rp;
+  const double bb = rg_sum(S.part + kRr * P, S.n_blk, S.Rp, r), zr = rg_sum(S.part + kZr * P, S.n_blk, S.Rp, r);
   if ((threadIdx.x & 31) != 0) return;
-  s.beta[r] = s.gamma[r] > 0.0 ? (float)(zr / s.gamma[r]) : 0.f;
-  s.gamma[r] = zr;
-  const double b2 = s.bnorm[r] * s.bnorm[r];
-  if (rr < tol2 * b2 || rr < delta2 * s.rr_ref[r] || s.its[r] >= max_it) atomicAdd(s.flags, 1);
-}
-
-// After the FP64 true residual: converged realizations stop; the others keep
-// their direction and continue from the true residual. flags[1] counts the
-// realizations still running.
-__global__ void k_ebe_true(int Rp, int n_blocks, const double* __restrict__ part_rr,
-                           const double* __restrict__ part_zr, EbeScal s, double tol, int max_it) {
-  const int r = ebe_warp_realization();
-  if (r >= Rp) return;
-  if (s.done[r]) return;
-  const double rr = ebe_sum(part_rr, n_blocks, Rp, r), zr = ebe_sum(part_zr, n_blocks, Rp, r);
-  if ((threadIdx.x & 31) != 0) return;
-  const double err = s.bnorm[r] > 0.0 ? sqrt(rr) / s.bnorm[r] : 0.0;
-  s.res[r] = err;
-  s.rr_ref[r] = rr;
-  s.gamma[r] = zr;
-  if (err < tol) {
-    s.done[r] = 1;
-  } else if (s.its[r] >= max_it || !isfinite(err)) {
-    s.done[r] = 3;
-  } else {
-    atomicAdd(s.flags + 1, 1);
-  }
-}
-
-// p = dinv r + beta p
-__global__ void k_ebe_dir(size_t n3, int Rp, const float* __restrict__ beta, const float* __restrict__ dinv,
-                          const float* __restrict__ r, float* __restrict__ p) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3 * Rp; i += (size_t)gridDim.x * blockDim.x)
-    p[i] = fmaf(beta[i % Rp], p[i], dinv[i] * r[i]);
+  const int g = S.goff + r;
+  s.bnorm[g] = sqrt(bb);
+  s.rr_ref[g] = bb;
+  s.gamma[g] = zr;
+  s.alpha[g] = s.beta[g] = 0.f;
+  s.its[g] = 0;
+  s.res[g] = bb > 0.0 ? 1.0 : 0.0;
+  s.done[g] = (r >= R || !(bb > 0.0)) ? 1 : 0;
 }
 
 // X[r][dof] = x[free_rows[dof] * Rp + r] for the first R realizations
@@ -457,6 +637,27 @@ __global__ void k_ebe_tip(int R, int Rp, int row, const double* __restrict__ x, 
   if (r < R) tip[r] = x[(size_t)row * Rp + r];
 }
 
+// Device buffers of one system (carved from the batch's arena).
+struct RgBuf {
+  int R = 0, Rp = 0, G = 1, n_blk = 0, n_blk_u = 0;
+  std::vector<int> h_ptr, h_inc;  // incidence (host)
+  int *ptr = nullptr, *inc = nullptr;
+  double *K64 = nullptr, *E64 = nullptr, *bn = nullptr, *x = nullptr, *part = nullptr, *part_u = nullptr;
+  float *K32 = nullptr, *E32 = nullptr, *d = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *dinv = nullptr;
+};
+
+// Sequential carving of one device allocation at 256-byte boundaries; a first
+// pass with base == nullptr only adds up the bytes.
+struct Carver {
+  unsigned char* base = nullptr;
+  size_t off = 0;
+  template <class T> T* take(size_t n) {
+    const size_t at = off;
+    off += (sizeof(T) * std::max<size_t>(n, 1) + 255) / 256 * 256;
+    return base ? reinterpret_cast<T*>(base + at) : nullptr;
+  }
+};
+
 }  // namespace
 
 // Node -> (element, corner) incidence of a mesh: CSR over nodes, entries
@@ -472,173 +673,294 @@ static void ebe_incidence(const Mesh* m, std::vector<int>& ptr, std::vector<int>
     for (int a = 0; a < 8; ++a) inc[fill[m->conn[8 * (size_t)e + a]]++] = (e << 3) | a;
 }
 
-int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kd, const double* d_xi, int R,
-                    const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out) {
-  NvtxRange range("msg: batched element-by-element solve");
-  if ((int64_t)m->n_elems * 8 >= ((int64_t)1 << 31) || m->n_nodes <= 0 || m->n_elems <= 0)
-    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: mesh size out of range");
-  const int Rp = (R + 31) / 32 * 32;
+// Per-system sizes and incidence (host).
+static int rg_plan(Context* ctx, const RgInput& in, RgBuf& B) {
+  Mesh* m = in.m;
   const int nn = m->n_nodes, ne = m->n_elems;
-  const size_t n3 = 3 * (size_t)nn, nv = n3 * Rp;
+  if ((int64_t)ne * 8 >= ((int64_t)1 << 31) || nn <= 0 || ne <= 0 || in.R <= 0 || !in.kl || !in.d_xi || !in.d_b)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid system");
+  if (in.tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
+  B.R = in.R;
+  B.Rp = (in.R + 31) / 32 * 32;
+  const int ng = B.Rp / 32;
+  B.G = ng % 8 == 0 ? 8 : ng % 4 == 0 ? 4 : ng % 2 == 0 ? 2 : 1;
+  if (ctx->element_groups > 0 && ng % ctx->element_groups == 0) B.G = ctx->element_groups;
+  B.n_blk = (nn + kRgBlk - 1) / kRgBlk;
+  B.n_blk_u = (nn + kRgBlkU - 1) / kRgBlkU;
+  ebe_incidence(m, B.h_ptr, B.h_inc);
+  return MSG_OK;
+}
+
+// The system's buffers in the arena.
+static void rg_carve(const RgInput& in, RgBuf& B, Carver& c) {
+  const int nn = in.m->n_nodes, ne = in.m->n_elems;
+  const size_t n3 = 3 * (size_t)nn, nv = n3 * B.Rp;
+  B.ptr = c.take<int>(B.h_ptr.size());
+  B.inc = c.take<int>(B.h_inc.size());
+  B.K64 = c.take<double>(576 * (size_t)ne);
+  B.K32 = c.take<float>(576 * (size_t)ne);
+  B.E64 = c.take<double>((size_t)ne * B.Rp);
+  B.E32 = c.take<float>((size_t)ne * B.Rp);
+  B.bn = c.take<double>(n3);
+  B.x = c.take<double>(nv);
+  B.d = c.take<float>(nv);
+  B.r = c.take<float>(nv);
+  B.p = c.take<float>(nv);
+  B.q = c.take<float>(nv);
+  B.dinv = c.take<float>(nv);
+  B.part = c.take<double>(kRgParts * (size_t)B.n_blk * B.Rp);
+  B.part_u = c.take<double>(2 * (size_t)B.n_blk_u * B.Rp);
+}
+
+// Per-system device setup: element matrices at E = 1 (through the packed
+// scratch K300, at least 300 n_elems doubles), E field, load, Jacobi diagonal.
+static int rg_setup(Context* ctx, const RgInput& in, RgBuf& B, double* K300, int* d_status) {
+  Mesh* m = in.m;
+  const int nn = m->n_nodes, ne = m->n_elems;
+  const size_t n3 = 3 * (size_t)nn;
   cudaStream_t st = ctx->stream;
-  // per-mesh data: Khat_e in the per-corner layout (FP64, FP32), incidence
-  std::vector<int> ptr, inc;
-  ebe_incidence(m, ptr, inc);
-  DevMem d_ptr, d_inc, d_K300, d_K64, d_K32, d_st;
-  MSG_TRY(d_ptr.alloc(ctx, sizeof(int) * ptr.size()));
-  MSG_TRY(d_inc.alloc(ctx, sizeof(int) * inc.size()));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_ptr.ptr, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_inc.ptr, inc.data(), sizeof(int) * inc.size(), cudaMemcpyHostToDevice, st));
-  MSG_TRY(d_K300.alloc(ctx, sizeof(double) * 300 * (size_t)ne));
-  MSG_TRY(d_K64.alloc(ctx, sizeof(double) * 576 * (size_t)ne));
-  MSG_TRY(d_K32.alloc(ctx, sizeof(float) * 576 * (size_t)ne));
-  MSG_TRY(d_st.alloc(ctx, sizeof(int)));
-  MSG_CUDA(ctx, cudaMemsetAsync(d_st.ptr, 0, sizeof(int), st));
-  MSG_TRY(launch_h8_ke(ctx, ne, m->d_exyz.as<double>(), nullptr, 1.0, nu, d_K300.as<double>(), d_st.as<int>()));
-  k_ebe_unpack<<<ne, 128, 0, st>>>(ne, d_K300.as<double>(), d_K64.as<double>(), d_K32.as<float>());
+  MSG_CUDA(ctx, cudaMemcpyAsync(B.ptr, B.h_ptr.data(), sizeof(int) * B.h_ptr.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(B.inc, B.h_inc.data(), sizeof(int) * B.h_inc.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(d_status, 0, sizeof(int), st));
+  MSG_TRY(launch_h8_ke(ctx, ne, m->d_exyz.as<double>(), nullptr, 1.0, in.nu, K300, d_status));
+  k_ebe_unpack<<<ne, 128, 0, st>>>(ne, K300, B.K64, B.K32);
   count_launch(ctx);
   int neg = 0;
-  MSG_CUDA(ctx, cudaMemcpyAsync(&neg, d_st.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&neg, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
   MSG_CUDA(ctx, cudaStreamSynchronize(st));
   if (neg) return set_error(ctx, MSG_ERR_NEG_DET, "element with a non-positive Jacobian determinant");
-  d_K300.release();
-  // E of every element and realization [e][Rp]
-  DevMem d_E64, d_E32;
-  MSG_TRY(d_E64.alloc(ctx, sizeof(double) * (size_t)ne * Rp));
-  MSG_TRY(d_E32.alloc(ctx, sizeof(float) * (size_t)ne * Rp));
-  MSG_TRY(launch_kl_field(ctx, m, kd, R, Rp, d_xi, d_E64.as<double>(), d_E32.as<float>(), nullptr));
-  // vectors [node*3 + c][Rp] and scalars
-  DevMem d_x, d_d, d_r, d_p, d_q, d_dinv, d_bn, d_scal, d_part;
-  MSG_TRY(d_x.alloc(ctx, sizeof(double) * nv));
-  MSG_TRY(d_d.alloc(ctx, sizeof(float) * nv));
-  MSG_TRY(d_r.alloc(ctx, sizeof(float) * nv));
-  MSG_TRY(d_p.alloc(ctx, sizeof(float) * nv));
-  MSG_TRY(d_q.alloc(ctx, sizeof(float) * nv));
-  MSG_TRY(d_dinv.alloc(ctx, sizeof(float) * nv));
-  MSG_TRY(d_bn.alloc(ctx, sizeof(double) * n3));
-  MSG_CUDA(ctx, cudaMemsetAsync(d_bn.ptr, 0, sizeof(double) * n3, st));
-  MSG_TRY(launch_dof_to_node(ctx, m, d_b_dof, d_bn.as<double>(), 1, 0, 0));
-  const int gx = std::max(1, std::min((nn + kEbeWarps - 1) / kEbeWarps, ctx->sm_count * 4));
-  const dim3 grid(gx, Rp / 32);
-  MSG_TRY(d_scal.alloc(ctx, (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 2) * (size_t)Rp + 64));
-  EbeScal s;
-  s.gamma = d_scal.as<double>();
-  s.rr_ref = s.gamma + Rp;
-  s.bnorm = s.rr_ref + Rp;
-  s.res = s.bnorm + Rp;
-  s.alpha = reinterpret_cast<float*>(s.res + Rp);
-  s.beta = s.alpha + Rp;
-  s.done = reinterpret_cast<int*>(s.beta + Rp);
-  s.its = s.done + Rp;
-  s.flags = s.its + Rp;
-  MSG_TRY(d_part.alloc(ctx, sizeof(double) * 2 * (size_t)gx * Rp));  // two [gx][Rp] partial arrays
-  double* part_a = d_part.as<double>();
-  double* part_b = part_a + (size_t)gx * Rp;
-  const int* dptr = d_ptr.as<int>();
-  const int* dinc = d_inc.as<int>();
-  const int* conn = m->d_conn.as<int>();
-  const uint8_t* mask = m->d_mask.as<uint8_t>();
-  const int sb = Rp / 8;  // scalar kernels: one warp per realization, 8 per CTA
-  // realization groups of 32 per CTA of the FP32 operator: the largest of 8, 4,
-  // 2, 1 that divides the group count (or the element_groups option when it does)
-  const int ng = Rp / 32;
-  int G = ng % 8 == 0 ? 8 : ng % 4 == 0 ? 4 : ng % 2 == 0 ? 2 : 1;
-  if (ctx->element_groups > 0 && ng % ctx->element_groups == 0) G = ctx->element_groups;
-  const dim3 grid_op(gx, ng / G);
-  auto apply32 = [&]() {
-    const float* K32 = d_K32.as<float>();
-    const float* E32 = d_E32.as<float>();
-    switch (G) {
-      case 8:
-        k_ebe_apply32<8><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
-                                                              d_p.as<float>(), d_q.as<float>(), part_a);
-        break;
-      case 4:
-        k_ebe_apply32<4><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
-                                                              d_p.as<float>(), d_q.as<float>(), part_a);
-        break;
-      case 2:
-        k_ebe_apply32<2><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
-                                                              d_p.as<float>(), d_q.as<float>(), part_a);
-        break;
-      default:
-        k_ebe_apply32<1><<<grid_op, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, K32, E32, mask,
-                                                              d_p.as<float>(), d_q.as<float>(), part_a);
-    }
-  };
-  const int gv = (int)std::min<size_t>((nv + 255) / 256, (size_t)ctx->sm_count * 16);
-  k_ebe_dinv<<<nn, 128, 0, st>>>(nn, Rp, dptr, dinc, d_K64.as<double>(), d_E64.as<double>(), mask,
-                                 d_dinv.as<float>());
-  k_ebe_init<<<gv, 256, 0, st>>>(n3, Rp, d_bn.as<double>(), d_dinv.as<float>(), d_x.as<double>(), d_d.as<float>(),
-                                 d_r.as<float>(), d_p.as<float>());
-  k_ebe_bnorm<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, d_bn.as<double>(), d_dinv.as<float>(), part_a, part_b);
-  k_ebe_start<<<sb, 256, 0, st>>>(R, Rp, gx, part_a, part_b, s);
-  count_launch(ctx, 4);
+  // E of every element and realization [e][Rp] (the KL workspace is reused by the next system)
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, m, in.kl, &kd));
+  MSG_TRY(launch_kl_field(ctx, m, &kd, in.R, B.Rp, in.d_xi, B.E64, B.E32, nullptr));
+  MSG_CUDA(ctx, cudaMemsetAsync(B.bn, 0, sizeof(double) * n3, st));
+  MSG_TRY(launch_dof_to_node(ctx, m, in.d_b, B.bn, 1, 0, 0));
+  k_ebe_dinv<<<nn, 128, 0, st>>>(nn, B.Rp, B.ptr, B.inc, B.K64, B.E64, m->d_mask.as<uint8_t>(), B.dinv);
+  count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
+  return MSG_OK;
+}
+
+int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol) {
+  NvtxRange range("msg: batched element-by-element solve");
+  if (in.empty() || max_it <= 0 || !(tol > 0))
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid arguments");
+  cudaStream_t st = ctx->stream;
+  const auto t_setup = std::chrono::steady_clock::now();
+  const int S = (int)in.size();
+  std::vector<RgBuf> bufs(S);
+  std::vector<RgSys> sys(S);
+  int Rtot = 0, max_ne = 0;
+  for (int i = 0; i < S; ++i) {
+    if (!in[i].m || in[i].m->ctx != ctx)
+      return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: system %d has no mesh of this context", i);
+    MSG_TRY(rg_plan(ctx, in[i], bufs[i]));
+    sys[i].goff = Rtot;
+    Rtot += bufs[i].Rp;
+    max_ne = std::max(max_ne, in[i].m->n_elems);
+  }
+  // work items: per system and realization range, consecutive node blocks
+  // (operator passes: 64 nodes and G groups; update: 512 nodes and one group)
+  std::vector<RgItem> items, items_u;
+  std::vector<int> rsys(Rtot);
+  for (int i = 0; i < S; ++i) {
+    const RgBuf& B = bufs[i];
+    for (int rb = 0; rb < B.Rp; rb += 32 * B.G)
+      for (int blk = 0; blk < B.n_blk; ++blk) items.push_back(RgItem{i, blk, rb, B.G});
+    for (int rb = 0; rb < B.Rp; rb += 32)
+      for (int blk = 0; blk < B.n_blk_u; ++blk) items_u.push_back(RgItem{i, blk, rb, 1});
+    for (int r = 0; r < B.Rp; ++r) rsys[sys[i].goff + r] = i;
+  }
+  const int n_items = (int)items.size(), n_items_u = (int)items_u.size();
+  // one arena for the batch, kept by the context between calls (workspace slot
+  // 34; slot 35: the packed element matrices of one system at a time)
+  const size_t scal_bytes = (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 3) * (size_t)Rtot +
+                            sizeof(int) * (S + Rtot / 32 + 2);
+  RgSys* d_sys = nullptr;
+  RgItem *d_items = nullptr, *d_items_u = nullptr;
+  unsigned char* scal_base = nullptr;
+  int* d_status = nullptr;
+  auto carve_all = [&](Carver& c) {
+    for (int i = 0; i < S; ++i) rg_carve(in[i], bufs[i], c);
+    d_sys = c.take<RgSys>(S);
+    d_items = c.take<RgItem>(items.size());
+    d_items_u = c.take<RgItem>(items_u.size());
+    scal_base = c.take<unsigned char>(scal_bytes);
+    d_status = c.take<int>(1);
+  };
+  Carver count;
+  carve_all(count);
+  void *arena = nullptr, *k300 = nullptr;
+  MSG_TRY(workspace(ctx, 34, count.off, &arena));
+  MSG_TRY(workspace(ctx, 35, sizeof(double) * 300 * (size_t)max_ne, &k300));
+  Carver c;
+  c.base = static_cast<unsigned char*>(arena);
+  carve_all(c);
+  for (int i = 0; i < S; ++i) {
+    RgBuf& B = bufs[i];
+    MSG_TRY(rg_setup(ctx, in[i], B, static_cast<double*>(k300), d_status));
+    Mesh* m = in[i].m;
+    RgSys& Y = sys[i];
+    Y.n_nodes = m->n_nodes;
+    Y.Rp = B.Rp;
+    Y.n_blk = B.n_blk;
+    Y.n_blk_u = B.n_blk_u;
+    Y.inc_ptr = B.ptr;
+    Y.inc = B.inc;
+    Y.conn = m->d_conn.as<int>();
+    Y.mask = m->d_mask.as<uint8_t>();
+    Y.K32 = B.K32;
+    Y.K64 = B.K64;
+    Y.E32 = B.E32;
+    Y.E64 = B.E64;
+    Y.b = B.bn;
+    Y.x = B.x;
+    Y.d = B.d;
+    Y.r = B.r;
+    Y.p = B.p;
+    Y.q = B.q;
+    Y.dinv = B.dinv;
+    Y.part = B.part;
+    Y.part_u = B.part_u;
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys) * S, cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(RgItem) * items.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_items_u, items_u.data(), sizeof(RgItem) * items_u.size(), cudaMemcpyHostToDevice,
+                                st));
+  RgScal s;
+  s.gamma = reinterpret_cast<double*>(scal_base);
+  s.rr_ref = s.gamma + Rtot;
+  s.bnorm = s.rr_ref + Rtot;
+  s.res = s.bnorm + Rtot;
+  s.alpha = reinterpret_cast<float*>(s.res + Rtot);
+  s.beta = s.alpha + Rtot;
+  s.done = reinterpret_cast<int*>(s.beta + Rtot);
+  s.its = s.done + Rtot;
+  s.rsys = s.its + Rtot;
+  s.sreq = s.rsys + Rtot;
+  s.gact = s.sreq + S;
+  s.flags = s.gact + Rtot / 32;
+  MSG_CUDA(ctx, cudaMemcpyAsync(s.rsys, rsys.data(), sizeof(int) * Rtot, cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
+  for (int i = 0; i < S; ++i) {
+    const dim3 g(bufs[i].n_blk, bufs[i].Rp / 32);
+    k_rg_init<<<g, 32 * kEbeWarps, 0, st>>>(sys[i]);
+    k_rg_start<<<bufs[i].Rp / kEbeWarps, 32 * kEbeWarps, 0, st>>>(sys[i], in[i].R, s);
+    count_launch(ctx, 2);
+  }
+  const int n_groups = Rtot / 32, g_groups = (n_groups + kEbeWarps - 1) / kEbeWarps;
+  k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
+  count_launch(ctx);
+  MSG_CUDA(ctx, cudaGetLastError());
+  // persistent grids: the CTAs that fit on the device at once, at most one per item
+  int occ_apply = 1, occ_update = 1, occ_resid = 1;
+  MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_apply, k_rg_apply, 32 * kEbeWarps, 0));
+  MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_update, k_rg_update, 32 * kEbeWarps, 0));
+  MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_resid, k_rg_resid64, 32 * kEbeWarps, 0));
+  auto grid_of = [&](int occ, int n) { return std::max(1, std::min(n, ctx->sm_count * std::max(1, occ))); };
+  const int g_apply = grid_of(occ_apply, n_items), g_update = grid_of(occ_update, n_items_u);
+  const int g_resid = grid_of(occ_resid, n_items), g_fold = grid_of(occ_update, n_items);
+  const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
+  const RgSys* dS = d_sys;
+  const RgItem* dI = d_items;
+  const RgItem* dIu = d_items_u;
   const double delta2 = ctx->reliable_delta * ctx->reliable_delta, tol2 = 0.25 * tol * tol;
+  // one chunk of kEbeCheck iterations, captured once as a CUDA graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(s.flags, 0, 2 * sizeof(int), st);
+  for (int k = 0; k < kEbeCheck; ++k) {
+    k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s.gact);
+    k_rg_scalar<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, k > 0, tol2, delta2, max_it);
+    k_rg_update<<<g_update, 32 * kEbeWarps, 0, st>>>(dS, dIu, n_items_u, s);
+  }
+  k_rg_chunk_end<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol2, delta2, max_it);
+  const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaStreamEndCapture");
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return cuda_error(ctx, ie, "cudaGraphInstantiate");
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() { cudaGraphExecDestroy(e); }
+  } guard{exec};
   int* h = ctx->h_flags;
-  // every chunk adds kEbeCheck products to each running realization and a
-  // realization at the limit forces a true residual, which stops it: the loop
-  // ends after at most max_it / kEbeCheck + 1 chunks
+  int n_true = 0;
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->t_phase[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
+  cudaEventRecord(ctx->ev[10], st);
+  // a chunk adds kEbeCheck products to every running realization and one at
+  // the limit asks for a true residual, which stops it: the loop ends after at
+  // most max_it / kEbeCheck + 1 chunks
   const int max_chunks = max_it / kEbeCheck + 2;
   for (int chunk = 0; chunk < max_chunks; ++chunk) {
-    MSG_CUDA(ctx, cudaMemsetAsync(s.flags, 0, 2 * sizeof(int), st));
-    for (int k = 0; k < kEbeCheck; ++k) {
-      apply32();
-      k_ebe_alpha<<<sb, 256, 0, st>>>(Rp, gx, part_a, s);
-      k_ebe_update<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, s.alpha, d_p.as<float>(), d_q.as<float>(),
-                                                     d_dinv.as<float>(), d_d.as<float>(), d_r.as<float>(), part_a,
-                                                     part_b);
-      k_ebe_beta<<<sb, 256, 0, st>>>(Rp, gx, part_a, part_b, s, tol2, delta2, max_it);
-      k_ebe_dir<<<gv, 256, 0, st>>>(n3, Rp, s.beta, d_dinv.as<float>(), d_r.as<float>(), d_p.as<float>());
-      count_launch(ctx, 5);
-    }
-    MSG_CUDA(ctx, cudaGetLastError());
-    MSG_CUDA(ctx, cudaMemcpyAsync(h, s.flags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSG_CUDA(ctx, cudaGraphLaunch(exec, st));
+    count_launch(ctx, 3 * kEbeCheck + 1);
+    MSG_CUDA(ctx, cudaMemcpyAsync(h, s.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
+    if (h[1] == 0) break;
     if (h[0] == 0) continue;
-    // FP64 true residual of the running realizations, then stop or continue each
-    k_ebe_fold<<<gv, 256, 0, st>>>(nv, d_x.as<double>(), d_d.as<float>());
-    k_ebe_resid64<<<grid, 32 * kEbeWarps, 0, st>>>(nn, Rp, dptr, dinc, conn, d_K64.as<double>(), d_E64.as<double>(),
-                                                    mask, d_bn.as<double>(), d_x.as<double>(), d_dinv.as<float>(),
-                                                    s.done, d_r.as<float>(), part_a, part_b);
-    k_ebe_true<<<sb, 256, 0, st>>>(Rp, gx, part_a, part_b, s, tol, max_it);
-    count_launch(ctx, 3);
+    ++n_true;
+    MSG_CUDA(ctx, cudaMemsetAsync(s.flags + 1, 0, sizeof(int), st));
+    k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s, 0);
+    k_rg_resid64<<<g_resid, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s);
+    k_rg_true<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol, max_it);
+    k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
+    MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
+    count_launch(ctx, 4);
     MSG_CUDA(ctx, cudaGetLastError());
     MSG_CUDA(ctx, cudaMemcpyAsync(h + 1, s.flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[1] == 0) break;
   }
-  // results (a realization stops right after a fold, so d holds no correction
-  // here unless the chunk bound ended the loop)
-  k_ebe_fold<<<gv, 256, 0, st>>>(nv, d_x.as<double>(), d_d.as<float>());
+  cudaEventRecord(ctx->ev[11], st);
+  MSG_CUDA(ctx, cudaEventSynchronize(ctx->ev[11]));
+  float loop_ms = 0.f;
+  cudaEventElapsedTime(&loop_ms, ctx->ev[10], ctx->ev[11]);
+  ctx->t_phase[1] = loop_ms;
+  ctx->t_phase[2] = n_true;
+  ctx->t_phase[3] = 0.0;
+  // results (a realization stops right after its fold, so this adds 0 to it
+  // unless it broke down or the chunk bound ended the loop)
+  k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s, 1);
   count_launch(ctx);
-  if (d_X && m->n_dofs > 0) {
-    const dim3 g((m->n_dofs + 31) / 32, Rp / 32);
-    k_ebe_gather<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, R, Rp, m->d_free_rows.as<int>(), d_x.as<double>(), d_X);
-    count_launch(ctx);
+  std::vector<int> its(Rtot), done(Rtot);
+  std::vector<double> res(Rtot);
+  MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), s.its, sizeof(int) * Rtot, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(done.data(), s.done, sizeof(int) * Rtot, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(res.data(), s.res, sizeof(double) * Rtot, cudaMemcpyDeviceToHost, st));
+  int status = MSG_OK;
+  for (int i = 0; i < S; ++i) {
+    const RgInput& I = in[i];
+    const RgBuf& B = bufs[i];
+    Mesh* m = I.m;
+    if (I.d_X && m->n_dofs > 0) {
+      const dim3 g((m->n_dofs + 31) / 32, B.Rp / 32);
+      k_ebe_gather<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, I.R, B.Rp, m->d_free_rows.as<int>(), B.x, I.d_X);
+      count_launch(ctx);
+    }
+    if (I.h_tip && I.tip_dof >= 0) {
+      int row = 0;
+      MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_free_rows.as<int>() + I.tip_dof, sizeof(int), cudaMemcpyDeviceToHost, st));
+      MSG_CUDA(ctx, cudaStreamSynchronize(st));
+      // q (n3 * Rp floats >= R doubles) is free after the loop
+      double* tipbuf = reinterpret_cast<double*>(B.q);
+      k_ebe_tip<<<(I.R + 127) / 128, 128, 0, st>>>(I.R, B.Rp, row, B.x, tipbuf);
+      count_launch(ctx);
+      MSG_CUDA(ctx, cudaMemcpyAsync(I.h_tip, tipbuf, sizeof(double) * I.R, cudaMemcpyDeviceToHost, st));
+    }
   }
-  if (out.tip && tip_dof >= 0 && tip_dof < m->n_dofs) {
-    int row = 0;
-    MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_free_rows.as<int>() + tip_dof, sizeof(int), cudaMemcpyDeviceToHost, st));
-    MSG_CUDA(ctx, cudaStreamSynchronize(st));
-    // d_q (n3 * Rp floats >= R doubles) is free after the loop
-    k_ebe_tip<<<(R + 127) / 128, 128, 0, st>>>(R, Rp, row, d_x.as<double>(), d_q.as<double>());
-    count_launch(ctx);
-    MSG_CUDA(ctx, cudaMemcpyAsync(out.tip, d_q.ptr, sizeof(double) * R, cudaMemcpyDeviceToHost, st));
-  }
-  std::vector<int> its(Rp), done(Rp);
-  std::vector<double> res(Rp);
-  MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), s.its, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(done.data(), s.done, sizeof(int) * Rp, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(res.data(), s.res, sizeof(double) * Rp, cudaMemcpyDeviceToHost, st));
   MSG_CUDA(ctx, cudaStreamSynchronize(st));
   MSG_CUDA(ctx, cudaGetLastError());
-  int status = MSG_OK;
-  for (int r = 0; r < R; ++r) {
-    if (out.iterations) out.iterations[r] = its[r];
-    if (out.rel_res) out.rel_res[r] = res[r];
-    if (done[r] != 1 && status == MSG_OK) status = done[r] == 2 ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
+  for (int i = 0; i < S; ++i) {
+    const int g0 = sys[i].goff;
+    for (int r = 0; r < in[i].R; ++r) {
+      if (in[i].h_its) in[i].h_its[r] = its[g0 + r];
+      if (in[i].h_res) in[i].h_res[r] = res[g0 + r];
+      if (done[g0 + r] != 1 && status == MSG_OK)
+        status = done[g0 + r] == 2 ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
+    }
   }
   if (status != MSG_OK) set_error(ctx, status, "element-by-element batch: a realization did not converge");
   return status;

@@ -435,13 +435,19 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
   const bool mixed_general = mode == MSG_MODE_MIXED_BATCHED && !m->structured;
   const bool per_realization = mode == MSG_MODE_FP64_BSR || (mixed_general && !ctx->element_batch);
   if (mixed_general && ctx->element_batch) {
-    BatchOut o;
-    std::vector<double> htip(R);
-    o.tip = tip ? htip.data() : nullptr;
-    o.iterations = iterations;
-    o.rel_res = rel_res;
-    status = ebe_mixed_solve(ctx, m, nu, &kd, d_xi, R, d_b, max_it, tol, tip_dof, d_X, o);
-    if (tip) std::copy(htip.begin(), htip.end(), tip);
+    std::vector<RgInput> in(1);
+    in[0].m = m;
+    in[0].nu = nu;
+    in[0].kl = kl;
+    in[0].R = R;
+    in[0].d_xi = d_xi;
+    in[0].d_b = d_b;
+    in[0].d_X = d_X;
+    in[0].h_tip = tip;
+    in[0].tip_dof = tip_dof;
+    in[0].h_its = iterations;
+    in[0].h_res = rel_res;
+    status = ebe_ragged_solve(ctx, in, max_it, tol);
   } else if (mode == MSG_MODE_MIXED_BATCHED && m->structured) {
     BatchOut o;
     std::vector<double> htip(R);
@@ -1116,6 +1122,61 @@ int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const dou
     MSG_CUDA(ctx, cudaMemcpyAsync(X, dX, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost, ctx->stream));
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  return st;
+}
+
+int MSG_MC_SOLVE_RAGGED(MSG_CTX ctx, int n_systems, const MSG_RAGGED_SYSTEM* systems, int max_it, double tol) {
+  CTX_GUARD(ctx);
+  if (n_systems <= 0 || !systems || max_it <= 0 || !(tol > 0))
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "ragged batch: invalid arguments");
+  MSG_TRY(context_resources(ctx));
+  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
+  cudaEventRecord(e0, ctx->stream);
+  std::vector<RgInput> in(n_systems);
+  std::vector<std::unique_ptr<DevMem>> staging;
+  auto stage = [&](size_t bytes, double** out) -> int {
+    staging.emplace_back(new DevMem());
+    MSG_TRY(staging.back()->alloc(ctx, bytes));
+    *out = staging.back()->as<double>();
+    return MSG_OK;
+  };
+  for (int i = 0; i < n_systems; ++i) {
+    const MSG_RAGGED_SYSTEM& y = systems[i];
+    Mesh* m = y.mesh;
+    if (!m || m->ctx != ctx || !y.kl || !y.xi || !y.b || y.R <= 0 || y.kl->n_terms <= 0)
+      return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "ragged batch: invalid system %d", i);
+    const size_t xb = sizeof(double) * (size_t)y.R * y.kl->n_terms, bb = sizeof(double) * std::max(1, m->n_dofs);
+    double *dxi = nullptr, *db = nullptr;
+    MSG_TRY(stage(xb, &dxi));
+    MSG_TRY(stage(bb, &db));
+    MSG_CUDA(ctx, cudaMemcpyAsync(dxi, y.xi, xb, cudaMemcpyHostToDevice, ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(db, y.b, sizeof(double) * (size_t)m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
+    RgInput& I = in[i];
+    I.m = m;
+    I.nu = y.nu;
+    I.kl = y.kl;
+    I.R = y.R;
+    I.d_xi = dxi;
+    I.d_b = db;
+    if (y.X) MSG_TRY(stage(sizeof(double) * (size_t)y.R * std::max(1, m->n_dofs), &I.d_X));
+    I.h_tip = y.tip;
+    I.tip_dof = y.tip ? y.tip_dof : -1;
+    I.h_its = y.iterations;
+    I.h_res = y.rel_res;
+  }
+  const int st = ebe_ragged_solve(ctx, in, max_it, tol);
+  if (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED || st == MSG_ERR_BREAKDOWN) {
+    for (int i = 0; i < n_systems; ++i)
+      if (systems[i].X && in[i].d_X)
+        MSG_CUDA(ctx, cudaMemcpyAsync(systems[i].X, in[i].d_X,
+                                      sizeof(double) * (size_t)systems[i].R * systems[i].mesh->n_dofs,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  cudaEventRecord(e1, ctx->stream);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  ctx->t_phase[4] = ms;
   return st;
 }
 

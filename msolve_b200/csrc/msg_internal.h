@@ -315,10 +315,26 @@ struct BatchOut {
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
 
-// batched mixed-precision solve on any mesh, element by element (kernels_ebe.cu);
-// realizations padded to 32 inside
-int ebe_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R,
-                    const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
+// One system of a batched element-by-element solve (kernels_ebe.cu): a mesh
+// of any shape with its material, KL field and realizations; xi [R][n_terms],
+// b [n_dofs] and X [R][n_dofs] on the device (X may be null), tip, iterations
+// and residuals [R] on the host (each may be null).
+struct RgInput {
+  Mesh* m = nullptr;
+  double nu = 0.3;
+  const MSG_KL* kl = nullptr;
+  int R = 0;
+  const double* d_xi = nullptr;
+  const double* d_b = nullptr;
+  double* d_X = nullptr;
+  double* h_tip = nullptr;
+  int tip_dof = -1;
+  int* h_its = nullptr;
+  double* h_res = nullptr;
+};
+// All realizations of all systems in one loop (each system's realizations
+// padded to 32 inside); a system's results independent of the other systems.
+int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol);
 
 // Newmark batch (implicit integration of every realization, constant time step)
 struct NewmarkParams {

@@ -1,0 +1,105 @@
+"""GPU parity of the ragged batch (MSG_MC_SOLVE_RAGGED): systems of uneven mesh
+size and shape solved in the same launches, each realization against an FP64
+oracle solve of its own geometry and field (1e-8 relative, max-norm), and the
+same bits for a system alone and in the mix."""
+import numpy as np
+import pytest
+
+import msolve_b200 as M
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def distorted_model(n, seed, amp=0.15):
+    model = M.clamped_block_model(n)
+    rng = np.random.default_rng(seed)
+    inner = (model.xyz > 0.5).all(axis=1) & (model.xyz < n - 0.5).all(axis=1)
+    model.xyz[inner] += amp * rng.uniform(-1, 1, (int(inner.sum()), 3))
+    return model
+
+
+def systems():
+    """(model, kl, xi) of three systems: a distorted 4^3 with 3 realizations, the
+    6^3 lattice with 40 (two 32-wide groups, the second mostly padding) and a
+    distorted 5^3 with one."""
+    out = []
+    for n, R, K, distort, seed in ((4, 3, 5, True, 1), (6, 40, 8, False, 2), (5, 1, 6, True, 3)):
+        model = distorted_model(n, seed) if distort else M.clamped_block_model(n)
+        kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 4)
+        xi = np.random.default_rng(10 + seed).standard_normal((R, K))
+        out.append((model, kl, xi))
+    return out
+
+
+def solve(ctx, syss, tol=1e-10):
+    batch = M.RaggedMonteCarloBatch(ctx, tolerance=tol)
+    for model, kl, xi in syss:
+        batch.add(model, kl, xi)
+    return batch.Solve()
+
+
+def oracle_solution(model, kl, xi_r, n):
+    E = O.kl_field(O.centroids(model.xyz, model.conn), [n, n, n], kl.table(), xi_r[None, :], sigma=kl.sigma)[0]
+    Cs = O.CSR(model.n_nodes, model.conn, model.dof, model.n_dofs)
+    Cs.assemble(O.h8_stiffness_batch(model.element_xyz(), E, model.poisson)[0])
+    xo, info = Cs.pcg_jacobi(model.subdomains[0].RHS, tol=1e-13)
+    assert info["status"] == 0
+    return xo, Cs
+
+
+def test_ragged_batch_matches_oracle(ctx):
+    syss = systems()
+    res = solve(ctx, syss)
+    for (model, kl, xi), r in zip(syss, res):
+        n = round(model.xyz[:, 0].max())
+        assert (r["Residuals"] < 1e-10).all()
+        assert (r["Iterations"] > 0).all()
+        b = model.subdomains[0].RHS
+        for k in sorted({0, xi.shape[0] - 1}):
+            xo, Cs = oracle_solution(model, kl, xi[k], n)
+            x = r["Solutions"][k]
+            assert np.abs(x - xo).max() <= 1e-8 * np.abs(xo).max(), (n, k)
+            rr = np.linalg.norm(b - Cs.multiply(x)) / np.linalg.norm(b)
+            assert abs(rr - r["Residuals"][k]) <= 1e-3 * r["Residuals"][k] + 1e-15
+            assert r["TipValues"][k] == x[M.tip_dof(model)]
+
+
+def test_system_alone_equals_the_mix(ctx):
+    """A system's arithmetic is independent of the other systems: each system
+    solved alone gives the same bits as in the ragged mix. One realization
+    solved alone agrees with its batched solve to 1e-9 (the true-residual
+    steps of a system are shared by its realizations)."""
+    syss = systems()
+    mix = solve(ctx, syss)
+    for i, s in enumerate(syss):
+        alone = solve(ctx, [s])[0]
+        for key in ("Solutions", "TipValues", "Iterations", "Residuals"):
+            assert np.array_equal(alone[key], mix[i][key]), (i, key)
+    model, kl, xi = syss[1]
+    one = solve(ctx, [(model, kl, xi[17:18])])[0]
+    a = mix[1]["Solutions"][17]
+    assert np.abs(one["Solutions"][0] - a).max() <= 1e-9 * np.abs(a).max()
+
+
+def test_analyzer_on_a_distorted_mesh_is_the_one_system_batch(ctx):
+    """MSG_MC_SOLVE_BATCH in mixed mode on a mesh that is not a cube lattice runs
+    the same loop: bit-identical to the ragged batch of that one system."""
+    model, kl, xi = systems()[0]
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=kl.n_terms,
+                                                    simulations=xi.shape[0], mode="mixed", tolerance=1e-10)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    r = solve(ctx, [(model, kl, xi)])[0]
+    assert np.array_equal(mc.Solutions, r["Solutions"]) and np.array_equal(mc.Iterations, r["Iterations"])
+
+
+def test_ragged_batch_rejects_invalid_systems(ctx):
+    model, kl, xi = systems()[0]
+    other = M.Context(0)
+    batch = M.RaggedMonteCarloBatch(other, tolerance=1e-10)
+    batch.systems.append(dict(model=model, kl=kl, xi=xi, tip_dof=0, keep=False, mesh=M.GpuMesh(ctx, model)))
+    with pytest.raises(M.ArgumentError):
+        batch.Solve()  # mesh of another context
+    with pytest.raises(M.ArgumentError):
+        M.RaggedMonteCarloBatch(ctx).Solve()  # no systems
