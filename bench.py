@@ -90,6 +90,8 @@ def parse():
     p.add_argument("--no-serving", action="store_true", help="skip the serving (continuous batching) measurement")
     p.add_argument("--no-single", action="store_true", help="skip the 64^3 single-solve measurement")
     p.add_argument("--single-n", type=int, default=64)
+    p.add_argument("--no-ragged", action="store_true", help="skip the ragged (uneven mesh sizes) batch measurement")
+    p.add_argument("--ragged-R", type=int, default=64, help="realizations per system of the ragged batch")
     p.add_argument("--single-only", action="store_true",
                    help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
     p.add_argument("--serve-rates", default="100,400,1000,2000,5000", help="Poisson arrival rates (requests/s) to run")
@@ -340,6 +342,72 @@ def single_leg(args, ctx):
                          "iterations": info["iterations"], "seconds": time.perf_counter() - t0}
         for name in ("fp64", "mixed"):
             out[name]["rel_err_vs_oracle"] = float(np.abs(sols[name] - xo).max() / np.abs(xo).max())
+    return out
+
+
+def ragged_leg(args, ctx):
+    """Monte Carlo systems of uneven size in one batch (MSG_MC_SOLVE_RAGGED): the
+    serving sides {8, 16, 24, 32, 48} (cube lattices) and a 24^3 block with its
+    interior nodes moved (not a lattice), args.ragged_R realizations each with
+    its own 50-term KL field (sigma 0.3, l 0.2 * side), Jacobi-PCG with the FP32
+    element-by-element operator and the FP64 true residual < 1e-8. Timed
+    (device time of the call) as one ragged batch after a warm-up, and as the
+    same systems one call each; the oracle solves one realization of the 48^3
+    lattice and of the distorted 24^3 (FP64 CSR Jacobi-PCG to 1e-12)."""
+    import msolve_b200 as M
+    R, tol = args.ragged_R, 1e-8
+    specs = [(8, False), (16, False), (24, False), (32, False), (48, False), (24, True)]
+    systems = []
+    for i, (n, dist) in enumerate(specs):
+        model = M.clamped_block_model(n)
+        if dist:
+            rng = np.random.default_rng(100 + n)
+            inner = (model.xyz > 0.5).all(axis=1) & (model.xyz < n - 0.5).all(axis=1)
+            model.xyz[inner] += 0.2 * rng.uniform(-1, 1, (int(inner.sum()), 3))
+        kl = M.LognormalStochasticCoefficientsProvider([n] * 3, 0.2 * n, args.terms, 16)
+        xi = np.random.default_rng(1000 + i).standard_normal((R, args.terms))
+        systems.append((n, dist, model, kl, xi))
+    keep = {4, 5}
+
+    def solve(sel):
+        b = M.RaggedMonteCarloBatch(ctx, tolerance=tol)
+        for j in sel:
+            _, _, model, kl, xi = systems[j]
+            b.add(model, kl, xi, keep_solutions=j in keep)
+        res = b.Solve()
+        return res, ctx.stats()["t_total_ms"]
+
+    idx = list(range(len(systems)))
+    solve(idx)
+    res, ms = solve(idx)
+    seq_ms = sum(solve([j])[1] for j in idx)
+    dof_its = sum(systems[j][2].n_dofs * float(res[j]["Iterations"].sum()) for j in idx)
+    out = {"workload": f"{len(specs)} Monte Carlo systems in one batch: cube lattices of side 8, 16, 24, 32, 48 and "
+                       f"a 24^3 block with interior nodes moved by up to 0.2, {R} realizations each, "
+                       f"{args.terms}-term KL lognormal E, Jacobi-PCG (FP32 element-by-element operator, FP64 "
+                       f"iterate) to the FP64 true relative residual < {tol:g}",
+           "systems": [{"mesh": f"{n}^3" + (" distorted" if dist else ""), "free_dofs": model.n_dofs,
+                        "mean_iterations": float(res[j]["Iterations"].mean())}
+                       for j, (n, dist, model, _, _) in enumerate(systems)],
+           "ragged_ms": ms, "one_call_per_system_ms": seq_ms, "ragged_over_one_call_per_system": seq_ms / ms,
+           "solves_per_s": len(idx) * R / (ms / 1e3), "dof_iterations_per_s": dof_its / (ms / 1e3),
+           "max_true_rel_residual": float(max(r["Residuals"].max() for r in res))}
+    if not args.no_parity:
+        import oracle as O
+        errs = {}
+        for j in sorted(keep):
+            n, dist, model, kl, xi = systems[j]
+            P = O.block_problem(n, args.terms, 16)
+            E = O.kl_field(O.centroids(model.xyz, model.conn), P["domain"], P["table"], xi[:1], sigma=0.3)[0]
+            if dist:
+                C = O.CSR(model.n_nodes, model.conn, model.dof, model.n_dofs)
+                C.assemble(O.h8_stiffness_batch(model.element_xyz(), E, model.poisson)[0])
+                xo, _ = C.pcg_jacobi(model.subdomains[0].RHS, tol=1e-12)
+            else:
+                xo, _ = O.block_solve_pcg(n, n, n, P["constrained"], E, 0.3, P["b"], tol=1e-12, max_it=100000)
+            x = res[j]["Solutions"][0]
+            errs[out["systems"][j]["mesh"]] = float(np.abs(x - xo).max() / np.abs(xo).max())
+        out["rel_err_vs_oracle"] = errs
     return out
 
 
@@ -730,6 +798,7 @@ def main():
         newmark = None if args.no_newmark else newmark_leg(args, ctx)
         serving = None if args.no_serving else serving_leg(args, ctx)
         single = None if args.no_single else single_leg(args, ctx)
+        ragged = None if args.no_ragged else ragged_leg(args, ctx)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -769,6 +838,7 @@ def main():
             "newmark": newmark,
             "serving": serving,
             "single_solve": single,
+            "ragged": ragged,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
