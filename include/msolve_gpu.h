@@ -447,8 +447,8 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * residuals); 0: realization by realization through the assembled FP32-value
  * PCG of MSG_PCG_SOLVE_MIXED), "element_groups" (launch shape of that
  * element-by-element operator: realization groups of 32 per CTA, each element
- * row block loaded once for all of them; 0, default: the largest of 8, 4, 2, 1
- * dividing the padded group count; results are identical).
+ * row block loaded once for all of them; 0, default: the largest of 4, 2, 1
+ * dividing the padded group count; 8 is allowed; results are identical).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

@@ -57,7 +57,7 @@ namespace {
 constexpr int kEbeWarps = 8;   // warps per CTA
 constexpr int kEbeCheck = 8;   // iterations per chunk (graph launch) between host reads of the flags
 constexpr int kRgBlk = 64;     // nodes per work item of the operator passes: 8 warps x 8 nodes
-constexpr int kRgBlkU = 512;   // nodes per work item of the update pass: 8 warps x 64 nodes
+constexpr int kRgBlkU = 256;   // nodes per work item of the update pass: 8 warps x 32 nodes
 constexpr int kRgParts = 5;    // partial arrays per system over kRgBlk blocks
 enum { kPq = 0, kDrq = 1, kDqd = 2, kZr = 3, kRr = 4 };
 
@@ -155,8 +155,11 @@ __device__ __forceinline__ double* rg_part(const RgSys& S, int k, int blk, int c
 // rb + 32 g + lane): the corner's 72 values as 18 float4 broadcast loads (each
 // per-corner block starts on a 288-byte boundary), used by all G groups. A
 // broadcast load fills 32 lanes' registers, so its cost in the load
-// writeback path is shared by the G groups; every realization's arithmetic
-// (order of the products and sums) is the same for every G.
+// writeback path is shared by the G groups. Each gathered u value is scaled
+// by the element's E first (E_e Khat_e u_e = Khat_e (E_e u_e)), so the sum
+// over the element runs straight into y and no per-element partial sums are
+// held. Every realization's arithmetic (order of the products and sums) is
+// the same for every G.
 template <int G>
 __device__ __forceinline__ void ebe_rows32(int n, int Rp, int rb, const int* __restrict__ inc_ptr,
                                            const int* __restrict__ inc, const int* __restrict__ conn,
@@ -173,9 +176,9 @@ __device__ __forceinline__ void ebe_rows32(int n, int Rp, int rb, const int* __r
     const int4 c0 = __ldg(reinterpret_cast<const int4*>(conn) + 2 * (size_t)e);
     const int4 c1 = __ldg(reinterpret_cast<const int4*>(conn) + 2 * (size_t)e + 1);
     const int nb[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-    float t[G][3];
+    float Ee[G];
 #pragma unroll
-    for (int g = 0; g < G; ++g) t[g][0] = t[g][1] = t[g][2] = 0.f;
+    for (int g = 0; g < G; ++g) Ee[g] = E[(size_t)e * Rp + rb + 32 * g + lane];
 #pragma unroll
     for (int q = 0; q < 6; ++q) {  // 4 columns (3 float4, 12 values) per step
       float kv[12];
@@ -188,19 +191,12 @@ __device__ __forceinline__ void ebe_rows32(int n, int Rp, int rb, const int* __r
         const float* __restrict__ ub = u + ((size_t)nb[j / 3] * 3 + j % 3) * Rp + rb + lane;
 #pragma unroll
         for (int g = 0; g < G; ++g) {
-          const float uv = ub[32 * g];
-          t[g][0] = fmaf(kv[3 * s], uv, t[g][0]);
-          t[g][1] = fmaf(kv[3 * s + 1], uv, t[g][1]);
-          t[g][2] = fmaf(kv[3 * s + 2], uv, t[g][2]);
+          const float uv = Ee[g] * ub[32 * g];
+          y[g][0] = fmaf(kv[3 * s], uv, y[g][0]);
+          y[g][1] = fmaf(kv[3 * s + 1], uv, y[g][1]);
+          y[g][2] = fmaf(kv[3 * s + 2], uv, y[g][2]);
         }
       }
-    }
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      const float Ee = E[(size_t)e * Rp + rb + 32 * g + lane];
-      y[g][0] = fmaf(Ee, t[g][0], y[g][0]);
-      y[g][1] = fmaf(Ee, t[g][1], y[g][1]);
-      y[g][2] = fmaf(Ee, t[g][2], y[g][2]);
     }
   }
 }
@@ -297,6 +293,9 @@ __device__ __forceinline__ void rg_apply_item(const RgSys& S, int blk, int rb, d
   }
 }
 
+// Every G in one kernel at 128 registers a thread (2 CTAs an SM): each
+// variant gets registers for many gathers in flight. Compiled alone, G = 4
+// takes 80 registers (3 CTAs an SM) and runs 24 % slower at 32^3 x 512.
 __global__ void __launch_bounds__(32 * kEbeWarps, 2) k_rg_apply(const RgSys* __restrict__ Sys,
                                                             const RgItem* __restrict__ items, int n_items,
                                                             const int* __restrict__ gact) {
@@ -316,8 +315,9 @@ __global__ void __launch_bounds__(32 * kEbeWarps, 2) k_rg_apply(const RgSys* __r
 
 // d += alpha p, r -= alpha q, p = D r + beta p; partials (D r).r and r.r. A
 // memory-bound pass with nothing to share between realization groups: work
-// items of 512 nodes and one group (few registers, long streams per warp);
-// items of groups without a running realization skipped.
+// items of 256 nodes and one group, one CTA each (few registers, long streams
+// per warp, two nodes in flight); items of groups without a running
+// realization skipped.
 __global__ void __launch_bounds__(32 * kEbeWarps) k_rg_update(const RgSys* __restrict__ Sys,
                                                              const RgItem* __restrict__ items, int n_items,
                                                              RgScal s) {
@@ -331,6 +331,7 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_rg_update(const RgSys* __res
     const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
     const float al = s.alpha[S.goff + col + lane], be = s.beta[S.goff + col + lane];
     double zr = 0.0, rr = 0.0;
+#pragma unroll 2
     for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -683,7 +684,10 @@ static int rg_plan(Context* ctx, const RgInput& in, RgBuf& B) {
   B.R = in.R;
   B.Rp = (in.R + 31) / 32 * 32;
   const int ng = B.Rp / 32;
-  B.G = ng % 8 == 0 ? 8 : ng % 4 == 0 ? 4 : ng % 2 == 0 ? 2 : 1;
+  // groups per operator work item (the batch takes the smallest over its
+  // systems): 4 by default (8 amortises the element rows further but needs 128
+  // registers a thread: slower at 32^3 x 512)
+  B.G = ng % 4 == 0 ? 4 : ng % 2 == 0 ? 2 : 1;
   if (ctx->element_groups > 0 && ng % ctx->element_groups == 0) B.G = ctx->element_groups;
   B.n_blk = (nn + kRgBlk - 1) / kRgBlk;
   B.n_blk_u = (nn + kRgBlkU - 1) / kRgBlkU;
@@ -759,16 +763,21 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
     Rtot += bufs[i].Rp;
     max_ne = std::max(max_ne, in[i].m->n_elems);
   }
-  // work items: per system and realization range, consecutive node blocks
-  // (operator passes: 64 nodes and G groups; update: 512 nodes and one group)
+  int G = 8;  // one G for the batch: the smallest of the systems' (each divides the next)
+  for (int i = 0; i < S; ++i) G = std::min(G, bufs[i].G);
+  for (int i = 0; i < S; ++i) bufs[i].G = G;
+  // work items: per system and node block, the realization ranges one after
+  // another (operator passes: 64 nodes and G groups; update: 256 nodes and one
+  // group), so that CTAs running at the same time cover whole rows
+  // [node * 3 + c][0 .. Rp) of the vectors
   std::vector<RgItem> items, items_u;
   std::vector<int> rsys(Rtot);
   for (int i = 0; i < S; ++i) {
     const RgBuf& B = bufs[i];
-    for (int rb = 0; rb < B.Rp; rb += 32 * B.G)
-      for (int blk = 0; blk < B.n_blk; ++blk) items.push_back(RgItem{i, blk, rb, B.G});
-    for (int rb = 0; rb < B.Rp; rb += 32)
-      for (int blk = 0; blk < B.n_blk_u; ++blk) items_u.push_back(RgItem{i, blk, rb, 1});
+    for (int blk = 0; blk < B.n_blk; ++blk)
+      for (int rb = 0; rb < B.Rp; rb += 32 * B.G) items.push_back(RgItem{i, blk, rb, B.G});
+    for (int blk = 0; blk < B.n_blk_u; ++blk)
+      for (int rb = 0; rb < B.Rp; rb += 32) items_u.push_back(RgItem{i, blk, rb, 1});
     for (int r = 0; r < B.Rp; ++r) rsys[sys[i].goff + r] = i;
   }
   const int n_items = (int)items.size(), n_items_u = (int)items_u.size();
@@ -858,7 +867,7 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_update, k_rg_update, 32 * kEbeWarps, 0));
   MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_resid, k_rg_resid64, 32 * kEbeWarps, 0));
   auto grid_of = [&](int occ, int n) { return std::max(1, std::min(n, ctx->sm_count * std::max(1, occ))); };
-  const int g_apply = grid_of(occ_apply, n_items), g_update = grid_of(occ_update, n_items_u);
+  const int g_apply = grid_of(occ_apply, n_items), g_update = n_items_u;
   const int g_resid = grid_of(occ_resid, n_items), g_fold = grid_of(occ_update, n_items);
   const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
   const RgSys* dS = d_sys;
