@@ -91,6 +91,9 @@ def parse():
     p.add_argument("--no-single", action="store_true", help="skip the 64^3 single-solve measurement")
     p.add_argument("--single-n", type=int, default=64)
     p.add_argument("--no-ragged", action="store_true", help="skip the ragged (uneven mesh sizes) batch measurement")
+    p.add_argument("--distorted-only", action="store_true",
+                   help="only the batched solve of --R realizations on an --n cube with its interior nodes moved "
+                        "(the element-by-element path), one JSON line")
     p.add_argument("--ragged-R", type=int, default=64, help="realizations per system of the ragged batch")
     p.add_argument("--single-only", action="store_true",
                    help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
@@ -411,6 +414,39 @@ def ragged_leg(args, ctx):
     return out
 
 
+def distorted_leg(args, ctx):
+    """The Monte Carlo batch of args.R realizations on the args.n cube with its
+    interior nodes moved by up to 0.2 in each axis (not a lattice: the
+    element-by-element loop of MSG_MC_SOLVE_BATCH in mixed mode), 50-term KL
+    field, FP64 true residual < args.tol; one warm-up call, then args.steps
+    timed calls (device time of the call and of its loop)."""
+    import msolve_b200 as M
+    n, R = args.n, args.R
+    model = M.clamped_block_model(n)
+    rng = np.random.default_rng(5)
+    inner = (model.xyz > 0.5).all(axis=1) & (model.xyz < n - 0.5).all(axis=1)
+    model.xyz[inner] += 0.2 * rng.uniform(-1, 1, (int(inner.sum()), 3))
+    kl = M.LognormalStochasticCoefficientsProvider([n] * 3, 0.2 * n, args.terms, 16)
+    xi = np.random.default_rng(1).standard_normal((R, args.terms))
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=args.terms, simulations=R,
+                                                    mode="mixed", tolerance=args.tol, keep_solutions=False)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    calls, loops = [], []
+    for _ in range(max(1, args.steps)):
+        mc.Solve()
+        st = ctx.stats()
+        calls.append(st["t_total_ms"])
+        loops.append(st["t_inner_ms"])
+    best = min(calls)
+    return {"workload": f"{R} realizations x {n}^3 Hexa8 with interior nodes moved by up to 0.2 (not a cube "
+                        f"lattice), {args.terms}-term KL lognormal E, Jacobi-PCG with the FP32 element-by-element "
+                        f"operator and FP64 true residual < {args.tol:g}",
+            "solves_per_s": R / (best / 1e3), "call_ms": calls, "loop_ms": loops,
+            "true_residual_steps": st["reliable_updates"], "mean_iterations": float(np.mean(mc.Iterations)),
+            "max_true_rel_residual": float(mc.Residuals.max())}
+
+
 def serving_leg(args, ctx):
     """Serving: Poisson arrivals (seeded) of single-realization requests on cube
     meshes of side {8, 16, 24, 32, 48} (uniform), fresh xi per request, tol 1e-8,
@@ -596,6 +632,9 @@ def main():
         ctx.set_option("reliable_delta", args.reliable_delta)
     if args.single_only:
         print(json.dumps(single_leg(args, ctx)))
+        return
+    if args.distorted_only:
+        print(json.dumps(distorted_leg(args, ctx)))
         return
     if args.chunk is not None:
         ctx.set_option("chunk", args.chunk)
