@@ -488,6 +488,7 @@ class MonteCarloAnalyzerWithStochasticMaterial : public IAnalyzer {
   int TipDof = 0;
 
  private:
+  friend class RaggedMonteCarloBatch;
   Context& ctx_;
   Model& model_;
   LognormalStochasticCoefficientsProvider& kl_;
@@ -501,6 +502,53 @@ class MonteCarloAnalyzerWithStochasticMaterial : public IAnalyzer {
 
  private:
   uint64_t seed_;
+};
+
+// Several Monte Carlo analyses (models of any size or shape) in one
+// MSG_MC_SOLVE_RAGGED call: each added analyzer's RandomNumbers are solved in
+// the batched mixed mode to the batch's tolerance, and its Solutions,
+// TipValues, Iterations and Residuals are filled as by its own Solve() on the
+// same loop (the same bits alone and in the batch). No reference counterpart:
+// the reference runs one analysis, one realization after another.
+class RaggedMonteCarloBatch {
+ public:
+  explicit RaggedMonteCarloBatch(Context& ctx, double tolerance = 1e-8, int max_iterations = 20000)
+      : ctx_(ctx), Tolerance(tolerance), MaxIterations(max_iterations) {}
+  void Add(MonteCarloAnalyzerWithStochasticMaterial& analyzer) { items_.push_back(&analyzer); }
+  void Solve() {
+    std::vector<MSG_RAGGED_SYSTEM> sys(items_.size());
+    for (size_t i = 0; i < items_.size(); ++i) {
+      MonteCarloAnalyzerWithStochasticMaterial& a = *items_[i];
+      if (a.RandomNumbers.size() != (size_t)a.simulations_ * a.expansionOrder_) a.Initialize();
+      const int R = a.simulations_;
+      a.Solutions.assign((size_t)R * a.model_.n_dofs, 0.0);
+      a.TipValues.assign(R, 0.0);
+      a.Iterations.assign(R, 0);
+      a.Residuals.assign(R, 0.0);
+      MSG_RAGGED_SYSTEM& y = sys[i];
+      y.mesh = a.mesh_.Handle();
+      y.nu = a.model_.Poisson;
+      y.kl = a.kl_.Kl();
+      y.R = R;
+      y.xi = a.RandomNumbers.data();
+      y.b = a.model_.subdomain.Forces.data();
+      y.tip_dof = a.TipDof;
+      y.X = a.Solutions.data();
+      y.tip = a.TipValues.data();
+      y.iterations = a.Iterations.data();
+      y.rel_res = a.Residuals.data();
+    }
+    const int st = MSG_MC_SOLVE_RAGGED(ctx_.Handle(), (int)sys.size(), sys.data(), MaxIterations, Tolerance);
+    Check(st, ctx_.Handle(), "MSG_MC_SOLVE_RAGGED");
+  }
+
+ private:
+  Context& ctx_;
+  std::vector<MonteCarloAnalyzerWithStochasticMaterial*> items_;
+
+ public:
+  double Tolerance;
+  int MaxIterations;
 };
 
 // MassAccelerationSinusoidalLoad: magnitude sin(2 pi / period * dt * i) for i

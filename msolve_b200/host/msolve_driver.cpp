@@ -10,6 +10,10 @@
 //   mc      N R TERMS XI OUT [fp64]      MonteCarloAnalyzerWithStochasticMaterial on the N^3 clamped
 //           block with xi [R][TERMS] read from XI (f64): tip [R], residuals [R] (f64),
 //           iterations [R] (int32), solutions [R][n_dofs] (f64)
+//   ragged  N1 N2 R TERMS XI OUT         RaggedMonteCarloBatch of two analyzers (the N1^3 clamped block
+//           and the N2^3 one with move_interior, R realizations each, xi [2][R][TERMS] from
+//           XI, tol 1e-10) -> per analyzer: tip [R], residuals [R] (f64), iterations [R]
+//           (int32), solutions [R][n_dofs] (f64)
 //   newmark N R TERMS XI STEPS OUT       NewmarkDynamicAnalyzer (beta 0.25, gamma 0.5, dt 0.01,
 //           Rayleigh 0.01 / 0.001, ground acceleration 0.1 sin(2 pi t) in x):
 //           tip history [R][STEPS] (f64), final displacements [R][n_dofs] (f64)
@@ -52,6 +56,19 @@ template <class T> bool put(FILE* f, const std::vector<T>& v) { return write_all
 msolve::Model make_model(const std::string& kind, int n) {
   if (kind == "cantilever") return msolve::Hexa8MeshGenerator::Cantilever();
   return msolve::Hexa8MeshGenerator::ClampedBlock(n);
+}
+
+// Interior nodes of a block moved by exact binary fractions (the same bits in
+// every language): node i, axis a by 0.0625 * (((7 i + 3 a) mod 5) - 2).
+void move_interior(msolve::Model& m) {
+  double hi = 0.0;
+  for (double v : m.xyz) hi = std::max(hi, v);
+  for (int i = 0; i < m.NumNodes(); ++i) {
+    bool inner = true;
+    for (int a = 0; a < 3; ++a) inner = inner && m.xyz[3 * i + a] > 0.5 && m.xyz[3 * i + a] < hi - 0.5;
+    if (inner)
+      for (int a = 0; a < 3; ++a) m.xyz[3 * i + a] += 0.0625 * (((7 * i + 3 * a) % 5) - 2);
+  }
 }
 
 std::vector<double> read_doubles(const char* path, size_t count) {
@@ -108,6 +125,29 @@ int run(int argc, char** argv) {
     FILE* f = std::fopen(argv[6], "wb");
     if (!f) return 6;
     const bool ok = put(f, mc.TipValues) && put(f, mc.Residuals) && put(f, mc.Iterations) && put(f, mc.Solutions);
+    std::fclose(f);
+    return ok ? 0 : 6;
+  }
+  if (cmd == "ragged" && argc >= 8) {
+    const int n1 = std::atoi(argv[2]), n2 = std::atoi(argv[3]), R = std::atoi(argv[4]), terms = std::atoi(argv[5]);
+    const std::vector<double> xi = read_doubles(argv[6], (size_t)2 * R * terms);
+    msolve::Context ctx(0);
+    msolve::Model m1 = msolve::Hexa8MeshGenerator::ClampedBlock(n1), m2 = msolve::Hexa8MeshGenerator::ClampedBlock(n2);
+    move_interior(m2);
+    msolve::LognormalStochasticCoefficientsProvider k1({(double)n1, (double)n1, (double)n1}, 0.2 * n1, terms, 6);
+    msolve::LognormalStochasticCoefficientsProvider k2({(double)n2, (double)n2, (double)n2}, 0.2 * n2, terms, 6);
+    msolve::MonteCarloAnalyzerWithStochasticMaterial a1(ctx, m1, k1, terms, R), a2(ctx, m2, k2, terms, R);
+    a1.RandomNumbers.assign(xi.begin(), xi.begin() + (size_t)R * terms);
+    a2.RandomNumbers.assign(xi.begin() + (size_t)R * terms, xi.end());
+    msolve::RaggedMonteCarloBatch batch(ctx, 1e-10);
+    batch.Add(a1);
+    batch.Add(a2);
+    batch.Solve();
+    FILE* f = std::fopen(argv[7], "wb");
+    if (!f) return 6;
+    bool ok = true;
+    for (const auto* a : {&a1, &a2})
+      ok = ok && put(f, a->TipValues) && put(f, a->Residuals) && put(f, a->Iterations) && put(f, a->Solutions);
     std::fclose(f);
     return ok ? 0 : 6;
   }

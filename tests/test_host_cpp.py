@@ -103,6 +103,38 @@ def test_monte_carlo_matches_python_mirror(ctx, driver, tmp_path, mode):
 
 
 @pytest.mark.gpu
+def test_ragged_batch_matches_python_mirror(ctx, driver, tmp_path):
+    """C++ RaggedMonteCarloBatch (a lattice and a block with moved interior
+    nodes) returns the same bits as the Python mirror's batch."""
+    n1, n2, R, terms = 5, 4, 3, 6
+    xi = np.random.default_rng(31).standard_normal((2, R, terms))
+    xi_path = tmp_path / "xi.bin"
+    xi_path.write_bytes(xi.tobytes())
+    out = tmp_path / "rg.bin"
+    rc, err = run(driver, "ragged", n1, n2, R, terms, xi_path, out)
+    assert rc == 0, err
+    m1, m2 = M.clamped_block_model(n1), M.clamped_block_model(n2)
+    hi = m2.xyz.max()
+    inner = np.flatnonzero(((m2.xyz > 0.5) & (m2.xyz < hi - 0.5)).all(axis=1))
+    for i in inner:  # the driver's move_interior: exact binary fractions
+        m2.xyz[i] += 0.0625 * (((7 * i + 3 * np.arange(3)) % 5) - 2)
+    batch = M.RaggedMonteCarloBatch(ctx, tolerance=1e-10)
+    for m, n, x in ((m1, n1, xi[0]), (m2, n2, xi[1])):
+        batch.add(m, M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, terms, 6), x)
+    res = batch.Solve()
+    raw = out.read_bytes()
+    off = 0
+    for m, r in zip((m1, m2), res):
+        tip = np.frombuffer(raw, np.float64, R, off); off += 8 * R
+        rel = np.frombuffer(raw, np.float64, R, off); off += 8 * R
+        its = np.frombuffer(raw, np.int32, R, off); off += 4 * R
+        X = np.frombuffer(raw, np.float64, R * m.n_dofs, off).reshape(R, -1); off += 8 * R * m.n_dofs
+        assert np.array_equal(tip, r["TipValues"]) and np.array_equal(rel, r["Residuals"])
+        assert np.array_equal(its, r["Iterations"]) and np.array_equal(X, r["Solutions"])
+    assert off == len(raw)
+
+
+@pytest.mark.gpu
 def test_newmark_matches_python_mirror(ctx, driver, tmp_path):
     n, R, terms, steps = 4, 3, 12, 10
     xi = np.random.default_rng(23).standard_normal((R, terms))
