@@ -293,6 +293,22 @@ int MSG_MC_SOLVE_BATCH_DEVICE(MSG_MESH mesh, double nu, const MSG_KL* kl, int R,
                               const double* b_dev, int mode, int max_it, double tol, int tip_dof, double* X_dev,
                               double* tip, int* iterations, double* rel_res);
 
+/* MSG_MC_SOLVE_BATCH with the copy of X to the host left in flight: the copy
+ * runs on a copy stream of the context (from one of two device output buffers)
+ * while the caller prepares and submits the next batch. tip, iterations and
+ * rel_res are complete on return; X is complete when the next
+ * MSG_MC_SOLVE_BATCH_PIPELINED on the context returns, or after
+ * MSG_MC_FLUSH. So consecutive pipelined calls need different X buffers, and
+ * X should be page-locked host memory (a pageable X makes the copy
+ * synchronous). MSG_MC_SOLVE_BATCH and MSG_DESTROY flush first. No reference
+ * counterpart (the reference returns each realization's solution before the
+ * next starts). */
+int MSG_MC_SOLVE_BATCH_PIPELINED(MSG_MESH mesh, double nu, const MSG_KL* kl, int R, const double* xi,
+                                 const double* b, int mode, int max_it, double tol, int tip_dof, double* X,
+                                 double* tip, int* iterations, double* rel_res);
+/* Waits until the X of every pipelined call on the context is on the host. */
+int MSG_MC_FLUSH(MSG_CTX ctx);
+
 /* One system of a ragged batch: a Hexa8 mesh of any shape and size (of the
  * context the batch runs on), its material and KL field, R realizations and
  * the load. Host buffers: xi [R][kl->n_terms], b [n_dofs]; outputs (each may

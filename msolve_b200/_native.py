@@ -120,6 +120,9 @@ SIGNATURES = {
                                      C.c_double, C.c_int, _d, _d, _i, _d]),
     "MSG_MC_SOLVE_BATCH_DEVICE": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _vp, _vp, C.c_int,
                                             C.c_int, C.c_double, C.c_int, _vp, _d, _i, _d]),
+    "MSG_MC_SOLVE_BATCH_PIPELINED": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _d, _d, C.c_int,
+                                               C.c_int, C.c_double, C.c_int, _d, _d, _i, _d]),
+    "MSG_MC_FLUSH": (C.c_int, [_vp]),
     "MSG_MC_SOLVE_RAGGED": (C.c_int, [_vp, C.c_int, C.POINTER(MSG_RAGGED_SYSTEM), C.c_int, C.c_double]),
     "MSG_NEWMARK_BATCH": (C.c_int, [_vp, C.c_double, C.POINTER(MSG_KL), C.c_int, _d, C.POINTER(MSG_NEWMARK), _d,
                                     C.c_int, C.c_double, C.c_int, _d, _d, _i]),

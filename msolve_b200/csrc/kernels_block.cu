@@ -2792,6 +2792,7 @@ struct BlockExec {
   cudaStream_t st = nullptr;
   cudaEvent_t* ev = nullptr;      // 12 events
   int* h_flags = nullptr;         // pinned, >= 64 bytes
+  int* d_hflags = nullptr;        // device address of h_flags when it is mapped (else null)
   cudaGraphExec_t* graph = nullptr;
   size_t* graph_key = nullptr;
   bool ctx_stats = true;          // accumulate the context's phase timings and launch samples
@@ -2997,6 +2998,7 @@ int block_setup(Context* ctx, Mesh* m, double nu, double rho, double cK, double 
     B->X.st = ctx->stream;
     B->X.ev = ctx->ev;
     B->X.h_flags = ctx->h_flags;
+    B->X.d_hflags = ctx->d_hflags;
     B->X.graph = &ctx->batch_graph;
     B->X.graph_key = &ctx->batch_graph_key;
     B->X.ctx_stats = true;
@@ -3813,7 +3815,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
       cudaEventRecord(ev[0], st);
       MSG_TRY(block_update(ctx, B, c, b, b_per_r, tol, first, 0x7fffffff, B->gmg && first && !warm));
       cudaEventRecord(ev[1], st);
-      MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
+      MSG_TRY(publish_flags(ctx, s.n_active, 9, h_flags, B->X.d_hflags, st));
       MSG_CUDA(ctx, cudaStreamSynchronize(st));
       float ms = 0.f;
       cudaEventElapsedTime(&ms, ev[0], ev[1]);
@@ -3833,7 +3835,7 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
     count_launch(ctx, (B->gmg ? gmg_launches(B) : 2) * c.chunk);
     total_inner += c.chunk;
     cudaEventRecord(ev[3], st);
-    MSG_CUDA(ctx, cudaMemcpyAsync(h_flags, s.n_active, 36, cudaMemcpyDeviceToHost, st));
+    MSG_TRY(publish_flags(ctx, s.n_active, 9, h_flags, B->X.d_hflags, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     float ms = 0.f, op_ms = 0.f, up_ms = 0.f;
     cudaEventElapsedTime(&ms, ev[2], ev[3]);

@@ -729,10 +729,11 @@ static int rg_setup(Context* ctx, const RgInput& in, RgBuf& B, double* K300, int
   MSG_TRY(launch_h8_ke(ctx, ne, m->d_exyz.as<double>(), nullptr, 1.0, in.nu, K300, d_status));
   k_ebe_unpack<<<ne, 128, 0, st>>>(ne, K300, B.K64, B.K32);
   count_launch(ctx);
-  int neg = 0;
-  MSG_CUDA(ctx, cudaMemcpyAsync(&neg, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  // through the mapped flag words (word 8): no wait behind copies in flight
+  int* hneg = ctx->h_flags + 8;
+  MSG_TRY(publish_flags(ctx, d_status, 1, hneg, ctx->d_hflags ? ctx->d_hflags + 8 : nullptr, st));
   MSG_CUDA(ctx, cudaStreamSynchronize(st));
-  if (neg) return set_error(ctx, MSG_ERR_NEG_DET, "element with a non-positive Jacobian determinant");
+  if (*hneg) return set_error(ctx, MSG_ERR_NEG_DET, "element with a non-positive Jacobian determinant");
   // E of every element and realization [e][Rp] (the KL workspace is reused by the next system)
   KLDevice kd;
   MSG_TRY(kl_prepare(ctx, m, in.kl, &kd));
@@ -906,7 +907,7 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   for (int chunk = 0; chunk < max_chunks; ++chunk) {
     MSG_CUDA(ctx, cudaGraphLaunch(exec, st));
     count_launch(ctx, 3 * kEbeCheck + 1);
-    MSG_CUDA(ctx, cudaMemcpyAsync(h, s.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSG_TRY(publish_flags(ctx, s.flags, 2, h, ctx->d_hflags, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[1] == 0) break;
     if (h[0] == 0) continue;
@@ -919,7 +920,7 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
     MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
     count_launch(ctx, 4);
     MSG_CUDA(ctx, cudaGetLastError());
-    MSG_CUDA(ctx, cudaMemcpyAsync(h + 1, s.flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MSG_TRY(publish_flags(ctx, s.flags + 1, 1, h + 1, ctx->d_hflags ? ctx->d_hflags + 1 : nullptr, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[1] == 0) break;
   }

@@ -14,6 +14,8 @@
 // memory; each thread produces four (element, realization) values, written
 // realization-innermost (coalesced) in FP64 and FP32, and optionally in the
 // per-realization layout [r][e] used by the assembled FP64 path.
+#include <cstring>
+
 #include "msg_internal.h"
 
 namespace msg {
@@ -116,7 +118,17 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
   void *d_tab = nullptr, *d_psi = nullptr;
   MSG_TRY(workspace(ctx, 16, sizeof(double) * tab.size(), &d_tab));
   MSG_TRY(workspace(ctx, 15, sizeof(double) * (size_t)K * m->n_elems, &d_psi));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, ctx->stream));
+  // through the context's pinned staging buffer when there is one: a pageable
+  // upload can wait behind device-to-host copies still in flight
+  // (MSG_MC_SOLVE_BATCH_PIPELINED), a pinned one is a plain async copy. The
+  // buffer is free again: every earlier use was followed by a stream sync.
+  const double* src = tab.data();
+  if (ctx->h_stage && tab.size() * sizeof(double) <= 8192) {
+    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(ctx->h_stage, tab.data(), sizeof(double) * tab.size());
+    src = ctx->h_stage;
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_tab, src, sizeof(double) * tab.size(), cudaMemcpyHostToDevice, ctx->stream));
   dim3 grid((m->n_elems + 127) / 128, K);
   out->psi = static_cast<double*>(d_psi);
   k_kl_psi<<<grid, 128, 0, ctx->stream>>>(m->n_elems, K, m->d_centroid.as<double>(), static_cast<double*>(d_tab),
@@ -128,6 +140,24 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
   out->mu = std::log(kl->mean) - (kl->mean_correction ? 0.5 * kl->sigma * kl->sigma : 0.0);
   out->gaussian = kl->gaussian ? 1 : 0;
   out->mean = kl->mean;
+  return MSG_OK;
+}
+
+namespace {
+__global__ void k_publish_flags(const int* __restrict__ src, int* dst, int n) {
+  const int i = threadIdx.x;
+  if (i < n) dst[i] = src[i];
+}
+}  // namespace
+
+int publish_flags(Context* ctx, const int* d_src, int n, int* h_host, int* d_hmapped, cudaStream_t st) {
+  if (d_hmapped && n <= 32) {
+    k_publish_flags<<<1, 32, 0, st>>>(d_src, d_hmapped, n);
+    count_launch(ctx);
+    MSG_CUDA(ctx, cudaGetLastError());
+    return MSG_OK;
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(h_host, d_src, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
   return MSG_OK;
 }
 

@@ -77,13 +77,34 @@ Context::~Context() {
   if (batch_graph) cudaGraphExecDestroy(batch_graph);
   for (auto& e : ev)
     if (e) cudaEventDestroy(e);
+  if (copy_stream) {
+    cudaStreamSynchronize(copy_stream);
+    cudaStreamDestroy(copy_stream);
+  }
+  for (auto& e : pipe_ev)
+    if (e) cudaEventDestroy(e);
+  if (pipe_ready) cudaEventDestroy(pipe_ready);
   if (h_flags) cudaFreeHost(h_flags);
+  if (h_stage) cudaFreeHost(h_stage);
 }
 
 int context_resources(Context* ctx) {
-  if (!ctx->h_flags) MSG_CUDA(ctx, cudaMallocHost(&ctx->h_flags, 64));
+  if (!ctx->h_flags) {
+    MSG_CUDA(ctx, cudaHostAlloc(&ctx->h_flags, 64, cudaHostAllocMapped));
+    MSG_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_hflags), ctx->h_flags, 0));
+  }
+  if (!ctx->h_stage) MSG_CUDA(ctx, cudaMallocHost(&ctx->h_stage, 8192));
   for (auto& e : ctx->ev)
     if (!e) MSG_CUDA(ctx, cudaEventCreate(&e));
+  return MSG_OK;
+}
+
+int pipe_flush(Context* ctx) {
+  for (int i = 0; i < 2; ++i)
+    if (ctx->pipe_pending[i]) {
+      ctx->pipe_pending[i] = false;
+      MSG_CUDA(ctx, cudaEventSynchronize(ctx->pipe_ev[i]));
+    }
   return MSG_OK;
 }
 
@@ -133,8 +154,31 @@ static int upload(Context* ctx, DevMem& dst, const T* src, size_t n) {
   return MSG_OK;
 }
 
-// Element stiffness of one cube of side h, E = 1, through the K1 kernel; full 24x24.
+static bool cube_cached(Context* ctx, int kind, double h, double param, double* out) {
+  std::lock_guard<std::mutex> g(ctx->cube_mu);
+  for (const auto& c : ctx->cube_cache)
+    if (c.kind == kind && c.h == h && c.param == param) {
+      std::memcpy(out, c.v, sizeof(c.v));
+      return true;
+    }
+  return false;
+}
+
+static void cube_store(Context* ctx, int kind, double h, double param, const double* v) {
+  std::lock_guard<std::mutex> g(ctx->cube_mu);
+  if (ctx->cube_cache.size() >= 32) ctx->cube_cache.erase(ctx->cube_cache.begin());
+  Context::CubeMatrix c;
+  c.kind = kind;
+  c.h = h;
+  c.param = param;
+  std::memcpy(c.v, v, sizeof(c.v));
+  ctx->cube_cache.push_back(c);
+}
+
+// Element stiffness of one cube of side h, E = 1, through the K1 kernel; full
+// 24x24 (computed once per (h, nu) and context).
 int unit_cube_khat(Context* ctx, double h, double nu, double* K576) {
+  if (cube_cached(ctx, 0, h, nu, K576)) return MSG_OK;
   double xyz[24];
   for (int a = 0; a < 8; ++a) {
     const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
@@ -154,10 +198,12 @@ int unit_cube_khat(Context* ctx, double h, double nu, double* K576) {
   for (int i = 1; i < 24; ++i)
     if (std::fabs(K576[i * 25] - K576[0]) > 1e-12 * std::fabs(K576[0]))
       return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "cube stiffness has unequal diagonal entries");
+  cube_store(ctx, 0, h, nu, K576);
   return MSG_OK;
 }
 
 int unit_cube_mhat(Context* ctx, double h, double rho, double* M576) {
+  if (cube_cached(ctx, 1, h, rho, M576)) return MSG_OK;
   double xyz[24];
   for (int a = 0; a < 8; ++a) {
     const int ax = (a == 1 || a == 2 || a == 5 || a == 6), ay = (a == 2 || a == 3 || a == 6 || a == 7), az = a >= 4;
@@ -174,6 +220,7 @@ int unit_cube_mhat(Context* ctx, double h, double rho, double* M576) {
   MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (int i = 0; i < 24; ++i)
     for (int j = 0; j < 24; ++j) M576[i * 24 + j] = m300[packed_index(i, j)];
+  cube_store(ctx, 1, h, rho, M576);
   return MSG_OK;
 }
 
@@ -580,6 +627,7 @@ int MSG_DESTROY(MSG_CTX ctx) {
   {
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
     if (ctx->server) server_destroy(ctx);  // the serving lanes hold meshes of this context
+    pipe_flush(ctx);                       // pipelined copies to the caller's X
   }
   release(ctx);  // freed once the last mesh/matrix of this context is destroyed
   return MSG_OK;
@@ -1108,6 +1156,7 @@ int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const dou
   if (!m || !kl || !xi || !b || R <= 0) return MSG_ERR_INVALID_ARGUMENT;
   Context* ctx = m->ctx;
   CTX_GUARD(ctx);
+  MSG_TRY(pipe_flush(ctx));  // a pipelined call's copy may still read slot 14
   // staging buffers kept in the context (slots 12-14) across calls
   void *dxi = nullptr, *db = nullptr, *dX = nullptr;
   MSG_TRY(workspace(ctx, 12, sizeof(double) * (size_t)R * kl->n_terms, &dxi));
@@ -1123,6 +1172,54 @@ int MSG_MC_SOLVE_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const dou
     MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return st;
+}
+
+int MSG_MC_SOLVE_BATCH_PIPELINED(MSG_MESH m, double nu, const MSG_KL* kl, int R, const double* xi, const double* b,
+                                 int mode, int max_it, double tol, int tip_dof, double* X, double* tip,
+                                 int* iterations, double* rel_res) {
+  if (!m || !kl || !xi || !b || R <= 0) return MSG_ERR_INVALID_ARGUMENT;
+  Context* ctx = m->ctx;
+  CTX_GUARD(ctx);
+  MSG_TRY(context_resources(ctx));
+  if (!ctx->copy_stream) MSG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  for (auto& e : ctx->pipe_ev)
+    if (!e) MSG_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  if (!ctx->pipe_ready) MSG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->pipe_ready, cudaEventDisableTiming));
+  const int buf = ctx->pipe_next, other = buf ^ 1;
+  void *dxi = nullptr, *db = nullptr, *dX = nullptr;
+  MSG_TRY(workspace(ctx, 12, sizeof(double) * (size_t)R * kl->n_terms, &dxi));
+  MSG_TRY(workspace(ctx, 13, sizeof(double) * (size_t)std::max(1, m->n_dofs), &db));
+  if (X) {
+    // output buffer `buf` (slot 14 or 36): its copy from two calls ago must have
+    // left for the host before this batch writes it (a device-side wait)
+    if (ctx->pipe_pending[buf]) MSG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->pipe_ev[buf], 0));
+    MSG_TRY(workspace(ctx, buf ? 36 : 14, sizeof(double) * (size_t)R * std::max(1, m->n_dofs), &dX));
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(dxi, xi, sizeof(double) * (size_t)R * kl->n_terms, cudaMemcpyHostToDevice, ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(db, b, sizeof(double) * (size_t)m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
+  int st = mc_batch(ctx, m, nu, kl, R, static_cast<double*>(dxi), static_cast<double*>(db), mode, max_it, tol,
+                    tip_dof, X ? static_cast<double*>(dX) : nullptr, tip, iterations, rel_res);
+  if (X && (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED || st == MSG_ERR_BREAKDOWN)) {
+    // the copy to the host follows the batch on the copy stream and is left in flight
+    MSG_CUDA(ctx, cudaEventRecord(ctx->pipe_ready, ctx->stream));
+    MSG_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->pipe_ready, 0));
+    MSG_CUDA(ctx, cudaMemcpyAsync(X, dX, sizeof(double) * (size_t)R * m->n_dofs, cudaMemcpyDeviceToHost,
+                                  ctx->copy_stream));
+    MSG_CUDA(ctx, cudaEventRecord(ctx->pipe_ev[buf], ctx->copy_stream));
+    ctx->pipe_pending[buf] = true;
+  }
+  // the previous call's copy (overlapped with this batch) is complete on return
+  if (ctx->pipe_pending[other]) {
+    ctx->pipe_pending[other] = false;
+    MSG_CUDA(ctx, cudaEventSynchronize(ctx->pipe_ev[other]));
+  }
+  ctx->pipe_next = other;
+  return st;
+}
+
+int MSG_MC_FLUSH(MSG_CTX ctx) {
+  CTX_GUARD(ctx);
+  return pipe_flush(ctx);
 }
 
 int MSG_MC_SOLVE_RAGGED(MSG_CTX ctx, int n_systems, const MSG_RAGGED_SYSTEM* systems, int max_it, double tol) {

@@ -92,8 +92,28 @@ struct Context {
   // enough). Slots are owned by the call sites that use them.
   DevMem* work[kWorkSlots] = {nullptr};
   // per-context host/driver resources reused by every batch (created lazily)
-  int* h_flags = nullptr;           // 64 bytes of pinned host memory
+  int* h_flags = nullptr;           // 64 bytes of pinned host memory, mapped into the device
+  int* d_hflags = nullptr;          // the device's address of h_flags
+  double* h_stage = nullptr;        // 8 KB of pinned host memory: small uploads issued as true async copies
+  // unit-cube element matrices already computed (kind 0: stiffness at E = 1
+  // for (h, nu); 1: consistent mass for (h, rho)): later batches read no
+  // device data and free no device memory while setting up
+  struct CubeMatrix {
+    int kind;
+    double h, param;
+    double v[576];
+  };
+  std::vector<CubeMatrix> cube_cache;
+  std::mutex cube_mu;
   cudaEvent_t ev[12] = {nullptr};   // timing events
+  // pipelined Monte Carlo batches: the displacement copy to the host of one
+  // call runs on copy_stream from output buffer pipe_next ^ 1 while the next
+  // call computes into the other buffer
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t pipe_ev[2] = {nullptr, nullptr};  // copy of buffer i done
+  cudaEvent_t pipe_ready = nullptr;             // batch done, its copy may start
+  bool pipe_pending[2] = {false, false};
+  int pipe_next = 0;
   cudaGraphExec_t batch_graph = nullptr;  // inner-loop graph of the last batch configuration
   size_t batch_graph_key = 0;
   void* server = nullptr;  // serving worker and lanes (serve.cpp), nullptr until MSG_SERVE_START
@@ -121,6 +141,13 @@ int context_resources(Context* ctx);
 
 // Workspace slot `slot` of at least `bytes` bytes (grown, never shrunk).
 int workspace(Context* ctx, int slot, size_t bytes, void** out);
+// Waits for every displacement copy of the pipelined batches still in flight.
+int pipe_flush(Context* ctx);
+// h_host[0 .. n) = d_src[0 .. n) on stream st, written by a one-warp kernel
+// when d_hmapped (the device address of h_host) is given, so that the read
+// never waits behind copies in flight on the device's copy engines; a copy
+// otherwise. Read h_host after synchronizing st.
+int publish_flags(Context* ctx, const int* d_src, int n, int* h_host, int* d_hmapped, cudaStream_t st);
 
 void retain(Context* ctx);
 void release(Context* ctx);
