@@ -855,6 +855,11 @@ def main():
         serving = None if args.no_serving else serving_leg(args, ctx)
         single = None if args.no_single else single_leg(args, ctx)
         ragged = None if args.no_ragged else ragged_leg(args, ctx)
+        distorted = None
+        if not args.no_ragged:  # the same element-by-element loop on one mesh that is not a lattice
+            dargs = argparse.Namespace(**vars(args))
+            dargs.R, dargs.steps = 512, 2
+            distorted = distorted_leg(dargs, ctx)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -898,6 +903,7 @@ def main():
             "serving": serving,
             "single_solve": single,
             "ragged": ragged,
+            "distorted_mesh": distorted,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
