@@ -419,10 +419,12 @@ def ragged_leg(args, ctx):
 
 def distorted_leg(args, ctx):
     """The Monte Carlo batch of args.R realizations on the args.n cube with its
-    interior nodes moved by up to 0.2 in each axis (not a lattice: the
-    element-by-element loop of MSG_MC_SOLVE_BATCH in mixed mode), 50-term KL
-    field, FP64 true residual < args.tol; one warm-up call, then args.steps
-    timed calls (device time of the call and of its loop)."""
+    interior nodes moved by up to 0.2 in each axis (not a cube lattice: the
+    element-by-element loop of MSG_MC_SOLVE_BATCH in mixed mode, preconditioned
+    by the V-cycle of the cube lattice of the same numbering, or by the
+    diagonal with the multigrid option 0), 50-term KL field, FP64 true
+    residual < args.tol; one warm-up call, then args.steps timed calls (device
+    time of the call and of its loop)."""
     import msolve_b200 as M
     n, R = args.n, args.R
     model = M.clamped_block_model(n)
@@ -442,9 +444,10 @@ def distorted_leg(args, ctx):
         calls.append(st["t_total_ms"])
         loops.append(st["t_inner_ms"])
     best = min(calls)
+    prec = "diagonal" if ctx.get_option("multigrid") == 0 else "V-cycle of the cube lattice of the same numbering"
     return {"workload": f"{R} realizations x {n}^3 Hexa8 with interior nodes moved by up to 0.2 (not a cube "
-                        f"lattice), {args.terms}-term KL lognormal E, Jacobi-PCG with the FP32 element-by-element "
-                        f"operator and FP64 true residual < {args.tol:g}",
+                        f"lattice), {args.terms}-term KL lognormal E, PCG with the FP32 element-by-element "
+                        f"operator ({prec} preconditioner) and FP64 true residual < {args.tol:g}",
             "solves_per_s": R / (best / 1e3), "call_ms": calls, "loop_ms": loops,
             "true_residual_steps": st["reliable_updates"], "mean_iterations": float(np.mean(mc.Iterations)),
             "max_true_rel_residual": float(mc.Residuals.max())}
@@ -637,6 +640,8 @@ def main():
         print(json.dumps(single_leg(args, ctx)))
         return
     if args.distorted_only:
+        if args.multigrid is not None:
+            ctx.set_option("multigrid", args.multigrid)
         print(json.dumps(distorted_leg(args, ctx)))
         return
     if args.chunk is not None:

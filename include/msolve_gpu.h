@@ -272,9 +272,13 @@ int MSG_PC_GALERKIN_MATVEC(MSG_MESH mesh, double nu, const MSG_KL* kl, int m, in
  *     r = b - K x and FP64 solution update (iterative refinement); stop when
  *     ||b - K x||/||b|| < tol in FP64. On a mesh that is not a cube lattice
  *     (distorted or unstructured Hexa8) all realizations are solved at once
- *     by Jacobi-PCG over an element-by-element operator (each element's
- *     stiffness at E = 1 computed once, scaled by E per realization; FP32
- *     loop, FP64 iterate and true residuals) to the same FP64 stopping rule;
+ *     by PCG over an element-by-element operator (each element's stiffness
+ *     at E = 1 computed once, scaled by E per realization; FP32 loop, FP64
+ *     iterate and true residuals) to the same FP64 stopping rule; the
+ *     preconditioner is the multigrid V-cycle of the cube lattice with the
+ *     same numbering when the mesh has the generator's numbering and element
+ *     order (nodes moved) and that lattice coarsens (MSG_SET_OPTION
+ *     "multigrid" != 0), Jacobi otherwise;
  *     with MSG_SET_OPTION "element_batch" = 0 one after another with the
  *     assembled FP32-value PCG and FP64 refinement of MSG_PCG_SOLVE_MIXED.
  * xi [R][kl->n_terms], b [n_dofs]. Outputs (each may be NULL): X [R][n_dofs],

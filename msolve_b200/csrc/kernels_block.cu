@@ -3488,21 +3488,17 @@ LoopCfg loop_cfg(Context* ctx, const BlockSys* B, double tol, int chunk_cap) {
 // the same sweep on both sides and a fixed sweep count on the coarsest level
 // the preconditioner is symmetric positive definite (damping below
 // 2 / lambda_max(dinv A)).
-void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
+// The V-cycle of one iteration, from the level-0 start pass (r' = r - alpha q
+// from r_in into r_out, pre-smoothing, residual) to the level-0 post-sweep
+// (z into qB, partial z.r'), with the scalars of s.
+void gmg_vcycle(BlockSys* B, Scal& s, bool even, cudaStream_t st) {
   const int Rp = B->Rp;
-  Scal& s = B->s;
-  cudaEvent_t* ev = B->X.ev;
-  const bool even = (it & 1) == 0;
   const int nl = B->n_lvl;
   const float om = B->omega;
-  const int nt0 = B->pack ? B->n_tiles2 : B->n_tiles_m;  // tiles of the level-0 launches
   double* part2 = B->part_op.as<double>();
-  double* part1 = part2 + (size_t)2 * nt0 * Rp;
   float* r_in = even ? B->r32.as<float>() : B->rB.as<float>();
   float* r_out = even ? B->rB.as<float>() : B->r32.as<float>();
-  float* p_out = even ? B->pB.as<float>() : B->p.as<float>();
   const CUtensorMap& tm_rin = even ? B->tm_rAm : B->tm_rBm;
-  const CUtensorMap& tm_pin = even ? B->tm_pAm : B->tm_pBm;
   float* qB = B->qB.as<float>();
   const bool mass = B->mass;
   auto lvl = [&](auto mode, const Lattice& L, const ModalC& C, const CUtensorMap& ta, const CUtensorMap& tb,
@@ -3549,8 +3545,6 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   using Start = std::integral_constant<int, kLvlStart>;
   using Resid = std::integral_constant<int, kLvlResid>;
   using Smooth = std::integral_constant<int, kLvlSmooth>;
-  using PcgZ = std::integral_constant<int, kLvlPcgZ>;
-  if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
   // level 0: r' = r - alpha q, qB = r' - A x0 with x0 = omega dinv r', partial r'.r'
   // (x0 itself is formed again by the level-0 prolongation)
   lvl0(Start{}, tm_rin, B->tm_qAm, even ? B->tm2_rA : B->tm2_rB, B->tm2_qA, nullptr, nullptr, qB, r_out, nullptr,
@@ -3600,6 +3594,37 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
   // level 0 post-sweep: z (into qB) and the partial z.r'
   lvl0(Smooth{}, B->tm_xs, B->tm_xs, B->tm2_xs, B->tm2_xs, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr,
        part2 + 1, 2);
+}
+
+void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
+  const int Rp = B->Rp;
+  Scal& s = B->s;
+  cudaEvent_t* ev = B->X.ev;
+  const bool even = (it & 1) == 0;
+  const int nt0 = B->pack ? B->n_tiles2 : B->n_tiles_m;
+  double* part2 = B->part_op.as<double>();
+  double* part1 = part2 + (size_t)2 * nt0 * Rp;
+  float* p_out = even ? B->pB.as<float>() : B->p.as<float>();
+  const CUtensorMap& tm_pin = even ? B->tm_pAm : B->tm_pBm;
+  const bool mass = B->mass;
+  if (it == 0) cudaEventRecordWithFlags(ev[6], st, cudaEventRecordExternal);
+  gmg_vcycle(B, s, even, st);
+  using PcgZ = std::integral_constant<int, kLvlPcgZ>;
+  auto lvl0 = [&](auto mode, const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& ta2,
+                  const CUtensorMap& tb2, float* out, float* out2, float* d, double* partial, int pstride) {
+    constexpr int kMode = decltype(mode)::value;
+    if (B->pack) {
+      auto k = mass ? k_lvl_op2<kMode, true> : k_lvl_op2<kMode, false>;
+      k<<<B->grid2, kQThreads, LvlStage2<kMode>::kSmem, st>>>(
+          B->L, B->MC2, ta2, tb2, B->tm2_dinv, B->tm2_e, B->tm2_d, B->tiles_j2, B->n_tiles2, B->n_items2, B->mask,
+          nullptr, nullptr, B->omega, s.alpha, s.beta, out, out2, nullptr, d, partial, pstride, s.err);
+    } else {
+      auto k = mass ? k_lvl_op<kMode, true> : k_lvl_op<kMode, false>;
+      k<<<B->grid_m, kMThreads, LvlStage<kMode>::kSmem, st>>>(
+          B->L, B->MC, ta, tb, B->tm_dinvm, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m, B->n_items_m, B->mask,
+          nullptr, nullptr, B->omega, s.alpha, s.beta, out, out2, nullptr, d, partial, pstride, s.err);
+    }
+  };
   cudaMemsetAsync(s.n_active, 0, 32, st);  // n_active and n_update
   k_gmg_beta<<<c.sblocks, 1024, 0, st>>>(Rp, nt0, part2, s, c.delta2, c.tol2);
   // p = z + beta p_old, d += alpha p_old, q = A p, partial p.q
@@ -3609,8 +3634,8 @@ void gmg_iteration(BlockSys* B, const LoopCfg& c, int it, cudaStream_t st) {
         B->L, B->tc_bops.as<float>(), B->tm_qBm, tm_pin, B->tm_em, B->tm_dm, B->tiles_jm, B->n_tiles_m, B->n_items_m,
         B->mask, s.alpha, s.beta, B->q.as<float>(), p_out, B->d.as<float>(), part1, 1, s.err);
   } else {
-    lvl0(PcgZ{}, B->tm_qBm, tm_pin, B->tm2_qB, even ? B->tm2_pA : B->tm2_pB, nullptr, nullptr, B->q.as<float>(), p_out,
-         nullptr, B->d.as<float>(), part1, 1);
+    lvl0(PcgZ{}, B->tm_qBm, tm_pin, B->tm2_qB, even ? B->tm2_pA : B->tm2_pB, B->q.as<float>(), p_out,
+         B->d.as<float>(), part1, 1);
   }
   if (it == 0) cudaEventRecordWithFlags(ev[5], st, cudaEventRecordExternal);
   k_gmg_alpha<<<c.sblocks, 1024, 0, st>>>(Rp, nt0, part1, s);
@@ -4327,5 +4352,66 @@ int lane_fetch(Lane* L, int slot, double* X) {
   if (X) std::memcpy(X, L->h_col, sizeof(double) * nd);
   return MSG_OK;
 }
+
+namespace {
+
+// Node layout [(t * 3 + c) * Rp + r] (t: the node in generator order) to the
+// padded lattice layout [(interior[t] * 3 + c) * Rp + r] and back; one CTA per
+// node. Ghost nodes of the lattice are never written (they stay zero).
+__global__ void k_node_to_lattice(int n_int, int Rp, const int* __restrict__ interior, const float* __restrict__ in,
+                                  float* __restrict__ out) {
+  const int t = blockIdx.x;
+  if (t >= n_int) return;
+  const size_t po = (size_t)interior[t] * 3 * Rp, no = (size_t)t * 3 * Rp;
+  for (int i = threadIdx.x; i < 3 * Rp; i += blockDim.x) out[po + i] = in[no + i];
+}
+
+__global__ void k_lattice_to_node(int n_int, int Rp, const int* __restrict__ interior, const float* __restrict__ in,
+                                  float* __restrict__ out) {
+  const int t = blockIdx.x;
+  if (t >= n_int) return;
+  const size_t po = (size_t)interior[t] * 3 * Rp, no = (size_t)t * 3 * Rp;
+  for (int i = threadIdx.x; i < 3 * Rp; i += blockDim.x) out[no + i] = in[po + i];
+}
+
+// The lattice batch of the preconditioner and the scalars its start pass
+// reads: alpha = 0, so the start pass takes r' = r.
+struct GmgPrecondImpl {
+  BlockSys B;
+  Scal s0;
+  DevMem zero;
+};
+
+}  // namespace
+
+int gmg_precond_create(Context* ctx, Mesh* lat, double nu, const MSG_KL* kl, const double* d_xi, int R, int Rp,
+                       void** out) {
+  std::unique_ptr<GmgPrecondImpl> P(new GmgPrecondImpl());
+  MSG_TRY(block_setup(ctx, lat, nu, 1.0, 1.0, 0.0, R, Rp, &P->B));
+  if (!P->B.gmg)
+    return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "the lattice does not coarsen (or multigrid is off)");
+  KLDevice kd;
+  MSG_TRY(kl_prepare(ctx, lat, kl, &kd));
+  MSG_TRY(block_field(ctx, lat, &P->B, &kd, d_xi));
+  MSG_TRY(P->zero.alloc(ctx, sizeof(float) * Rp));
+  MSG_CUDA(ctx, cudaMemsetAsync(P->zero.ptr, 0, sizeof(float) * Rp, ctx->stream));
+  P->s0 = P->B.s;
+  P->s0.alpha = P->zero.as<float>();
+  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *out = P.release();
+  return MSG_OK;
+}
+
+int gmg_precond_apply(Context* ctx, void* handle, const float* r_node, float* z_node, cudaStream_t st) {
+  GmgPrecondImpl* P = static_cast<GmgPrecondImpl*>(handle);
+  BlockSys& B = P->B;
+  k_node_to_lattice<<<B.L.n_int, 256, 0, st>>>(B.L.n_int, B.Rp, B.interior, r_node, B.r32.as<float>());
+  gmg_vcycle(&B, P->s0, true, st);
+  k_lattice_to_node<<<B.L.n_int, 256, 0, st>>>(B.L.n_int, B.Rp, B.interior, B.qB.as<float>(), z_node);
+  count_launch(ctx, 2 + gmg_launches(&B) - 3);  // the iteration's launches but beta, the direction pass and alpha
+  return MSG_OK;
+}
+
+void gmg_precond_destroy(void* handle) { delete static_cast<GmgPrecondImpl*>(handle); }
 
 }  // namespace msg

@@ -541,6 +541,12 @@ __global__ void k_rg_true(const RgSys* __restrict__ Sys, int Rtot, RgScal s, dou
   }
 }
 
+// flags[1] = realizations still running (the multigrid-preconditioned loop's chunk end).
+__global__ void k_rg_chunk_end_count(int Rtot, RgScal s) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < Rtot && !s.done[g]) atomicAdd(s.flags + 1, 1);
+}
+
 // gact[group] = 1 while one of the group's 32 realizations runs (one warp per group).
 __global__ void k_rg_active(int n_groups, RgScal s) {
   const int grp = rg_warp_index();
@@ -638,6 +644,166 @@ __global__ void k_ebe_tip(int R, int Rp, int row, const double* __restrict__ x, 
   if (r < R) tip[r] = x[(size_t)row * Rp + r];
 }
 
+// ---------------------------------------------------------------- multigrid-preconditioned loop (one system)
+// Standard PCG with z = V(r) (the cube lattice's V-cycle, gmg_precond_apply):
+// operator (k_rg_apply: q = K p, partial p.q), alpha, update (r, d and r.r),
+// preconditioner, z.r, beta, direction. Work items of the update pass; the
+// partials of the update pass are part_u [0] z.r and [1] r.r.
+
+// r -= alpha q, d += alpha p, partial r.r (into part_u[1])
+__global__ void __launch_bounds__(32 * kEbeWarps) k_vc_update(const RgSys* __restrict__ Sys,
+                                                             const RgItem* __restrict__ items, int n_items,
+                                                             RgScal s) {
+  __shared__ double sh[kEbeWarps * 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    const RgSys S = Sys[I.sys];
+    if (!s.gact[(S.goff + I.rb) / 32]) continue;  // the same for the whole CTA
+    const int Rp = S.Rp, col = I.rb;
+    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
+    const float al = s.alpha[S.goff + col + lane];
+    double rr = 0.0;
+#pragma unroll 2
+    for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
+        const float rv = fmaf(-al, S.q[o], S.r[o]);
+        S.d[o] = fmaf(al, S.p[o], S.d[o]);
+        S.r[o] = rv;
+        rr += (double)rv * (double)rv;
+      }
+    rg_block_partial(rr, sh, S.part_u + ((size_t)1 * S.n_blk_u + I.blk) * Rp + col);
+  }
+}
+
+// partial z.r (into part_u[0])
+__global__ void __launch_bounds__(32 * kEbeWarps) k_vc_zr(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items,
+                                                         int n_items, RgScal s, const float* __restrict__ z) {
+  __shared__ double sh[kEbeWarps * 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    const RgSys S = Sys[I.sys];
+    if (!s.gact[(S.goff + I.rb) / 32]) continue;
+    const int Rp = S.Rp, col = I.rb;
+    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
+    double zr = 0.0;
+#pragma unroll 2
+    for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
+        zr += (double)z[o] * (double)S.r[o];
+      }
+    rg_block_partial(zr, sh, S.part_u + (size_t)I.blk * Rp + col);
+  }
+}
+
+// p = z + beta p
+__global__ void __launch_bounds__(32 * kEbeWarps) k_vc_dir(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items,
+                                                          int n_items, RgScal s, const float* __restrict__ z) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    const RgSys S = Sys[I.sys];
+    if (!s.gact[(S.goff + I.rb) / 32]) continue;
+    const int Rp = S.Rp, col = I.rb;
+    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
+    const float be = s.beta[S.goff + col + lane];
+#pragma unroll 2
+    for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
+        S.p[o] = fmaf(be, S.p[o], z[o]);
+      }
+  }
+}
+
+// alpha = gamma / p.q (one warp per realization)
+__global__ void k_vc_alpha(const RgSys* __restrict__ Sys, int Rtot, RgScal s) {
+  const int g = rg_warp_index();
+  if (g >= Rtot) return;
+  const int lane = threadIdx.x & 31;
+  if (s.done[g]) {
+    if (lane == 0) s.alpha[g] = 0.f;
+    return;
+  }
+  const RgSys& S = Sys[s.rsys[g]];
+  const int r = g - S.goff;
+  const double pq = rg_sum(S.part + (size_t)kPq * S.n_blk * S.Rp, S.n_blk, S.Rp, r);
+  if (lane != 0) return;
+  s.its[g] += 1;
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    s.done[g] = 2;
+    s.alpha[g] = 0.f;
+    return;
+  }
+  s.alpha[g] = (float)(s.gamma[g] / pq);
+}
+
+// beta = gamma_new / gamma with gamma_new = z.r, and the true-residual check on r.r
+__global__ void k_vc_beta(const RgSys* __restrict__ Sys, int Rtot, RgScal s, double tol2, double delta2,
+                          int max_it) {
+  const int g = rg_warp_index();
+  if (g >= Rtot) return;
+  const int lane = threadIdx.x & 31;
+  if (s.done[g]) {
+    if (lane == 0) s.beta[g] = 0.f;
+    return;
+  }
+  const RgSys& S = Sys[s.rsys[g]];
+  const int r = g - S.goff;
+  const size_t Pu = (size_t)S.n_blk_u * S.Rp;
+  const double zr = rg_sum(S.part_u, S.n_blk_u, S.Rp, r), rr = rg_sum(S.part_u + Pu, S.n_blk_u, S.Rp, r);
+  if (lane != 0) return;
+  s.beta[g] = s.gamma[g] > 0.0 ? (float)(zr / s.gamma[g]) : 0.f;
+  s.gamma[g] = zr;
+  rg_check(s, g, rr, tol2, delta2, max_it);
+}
+
+// Starting scalars: ||b|| from the init partials, gamma = z.b, beta = 0 (p = z)
+__global__ void k_vc_start(RgSys S, int R, RgScal s) {
+  const int r = rg_warp_index();
+  if (r >= S.Rp) return;
+  const double bb = rg_sum(S.part + (size_t)kRr * S.n_blk * S.Rp, S.n_blk, S.Rp, r);
+  const double zr = rg_sum(S.part_u, S.n_blk_u, S.Rp, r);
+  if ((threadIdx.x & 31) != 0) return;
+  const int g = S.goff + r;
+  s.bnorm[g] = sqrt(bb);
+  s.rr_ref[g] = bb;
+  s.gamma[g] = zr;
+  s.alpha[g] = s.beta[g] = 0.f;
+  s.its[g] = 0;
+  s.res[g] = bb > 0.0 ? 1.0 : 0.0;
+  s.done[g] = (r >= R || !(bb > 0.0)) ? 1 : 0;
+}
+
+// After the FP64 true residual (r.r in part kRr) and z = V(r) (z.r in part_u[0])
+__global__ void k_vc_true(const RgSys* __restrict__ Sys, int Rtot, RgScal s, double tol, int max_it) {
+  const int g = rg_warp_index();
+  if (g >= Rtot || s.done[g]) return;
+  const int lane = threadIdx.x & 31;
+  const RgSys& S = Sys[s.rsys[g]];
+  const int r = g - S.goff;
+  const double rr = rg_sum(S.part + (size_t)kRr * S.n_blk * S.Rp, S.n_blk, S.Rp, r);
+  const double zr = rg_sum(S.part_u, S.n_blk_u, S.Rp, r);
+  if (lane != 0) return;
+  const double err = s.bnorm[g] > 0.0 ? sqrt(rr) / s.bnorm[g] : 0.0;
+  s.res[g] = err;
+  s.rr_ref[g] = rr;
+  s.gamma[g] = zr;
+  if (err < tol) {
+    s.done[g] = 1;
+  } else if (s.its[g] >= max_it || !isfinite(err)) {
+    s.done[g] = 3;
+  } else {
+    atomicAdd(s.flags + 1, 1);
+  }
+}
+
 // Device buffers of one system (carved from the batch's arena).
 struct RgBuf {
   int R = 0, Rp = 0, G = 1, n_blk = 0, n_blk_u = 0;
@@ -675,14 +841,14 @@ static void ebe_incidence(const Mesh* m, std::vector<int>& ptr, std::vector<int>
 }
 
 // Per-system sizes and incidence (host).
-static int rg_plan(Context* ctx, const RgInput& in, RgBuf& B) {
+static int rg_plan(Context* ctx, const RgInput& in, RgBuf& B, int rp_multiple = 32) {
   Mesh* m = in.m;
   const int nn = m->n_nodes, ne = m->n_elems;
   if ((int64_t)ne * 8 >= ((int64_t)1 << 31) || nn <= 0 || ne <= 0 || in.R <= 0 || !in.kl || !in.d_xi || !in.d_b)
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid system");
   if (in.tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
   B.R = in.R;
-  B.Rp = (in.R + 31) / 32 * 32;
+  B.Rp = (in.R + rp_multiple - 1) / rp_multiple * rp_multiple;
   const int ng = B.Rp / 32;
   // groups per operator work item (the batch takes the smallest over its
   // systems): 4 by default (8 amortises the element rows further but needs 128
@@ -744,6 +910,53 @@ static int rg_setup(Context* ctx, const RgInput& in, RgBuf& B, double* K300, int
   count_launch(ctx);
   MSG_CUDA(ctx, cudaGetLastError());
   return MSG_OK;
+}
+
+// Results of a batch: displacements gathered into each system's X, tip values,
+// iterations and residuals; the worst status.
+static int rg_results(Context* ctx, const std::vector<RgInput>& in, const std::vector<RgBuf>& bufs,
+                      const std::vector<RgSys>& sys, const RgScal& s, int Rtot) {
+  cudaStream_t st = ctx->stream;
+  const int S = (int)in.size();
+  std::vector<int> its(Rtot), done(Rtot);
+  std::vector<double> res(Rtot);
+  MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), s.its, sizeof(int) * Rtot, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(done.data(), s.done, sizeof(int) * Rtot, cudaMemcpyDeviceToHost, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(res.data(), s.res, sizeof(double) * Rtot, cudaMemcpyDeviceToHost, st));
+  int status = MSG_OK;
+  for (int i = 0; i < S; ++i) {
+    const RgInput& I = in[i];
+    const RgBuf& B = bufs[i];
+    Mesh* m = I.m;
+    if (I.d_X && m->n_dofs > 0) {
+      const dim3 g((m->n_dofs + 31) / 32, B.Rp / 32);
+      k_ebe_gather<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, I.R, B.Rp, m->d_free_rows.as<int>(), B.x, I.d_X);
+      count_launch(ctx);
+    }
+    if (I.h_tip && I.tip_dof >= 0) {
+      int row = 0;
+      MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_free_rows.as<int>() + I.tip_dof, sizeof(int), cudaMemcpyDeviceToHost, st));
+      MSG_CUDA(ctx, cudaStreamSynchronize(st));
+      // q (n3 * Rp floats >= R doubles) is free after the loop
+      double* tipbuf = reinterpret_cast<double*>(B.q);
+      k_ebe_tip<<<(I.R + 127) / 128, 128, 0, st>>>(I.R, B.Rp, row, B.x, tipbuf);
+      count_launch(ctx);
+      MSG_CUDA(ctx, cudaMemcpyAsync(I.h_tip, tipbuf, sizeof(double) * I.R, cudaMemcpyDeviceToHost, st));
+    }
+  }
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  MSG_CUDA(ctx, cudaGetLastError());
+  for (int i = 0; i < S; ++i) {
+    const int g0 = sys[i].goff;
+    for (int r = 0; r < in[i].R; ++r) {
+      if (in[i].h_its) in[i].h_its[r] = its[g0 + r];
+      if (in[i].h_res) in[i].h_res[r] = res[g0 + r];
+      if (done[g0 + r] != 1 && status == MSG_OK)
+        status = done[g0 + r] == 2 ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
+    }
+  }
+  if (status != MSG_OK) set_error(ctx, status, "element-by-element batch: a realization did not converge");
+  return status;
 }
 
 int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol) {
@@ -935,45 +1148,190 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   // unless it broke down or the chunk bound ended the loop)
   k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s, 1);
   count_launch(ctx);
-  std::vector<int> its(Rtot), done(Rtot);
-  std::vector<double> res(Rtot);
-  MSG_CUDA(ctx, cudaMemcpyAsync(its.data(), s.its, sizeof(int) * Rtot, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(done.data(), s.done, sizeof(int) * Rtot, cudaMemcpyDeviceToHost, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(res.data(), s.res, sizeof(double) * Rtot, cudaMemcpyDeviceToHost, st));
-  int status = MSG_OK;
-  for (int i = 0; i < S; ++i) {
-    const RgInput& I = in[i];
-    const RgBuf& B = bufs[i];
-    Mesh* m = I.m;
-    if (I.d_X && m->n_dofs > 0) {
-      const dim3 g((m->n_dofs + 31) / 32, B.Rp / 32);
-      k_ebe_gather<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, I.R, B.Rp, m->d_free_rows.as<int>(), B.x, I.d_X);
-      count_launch(ctx);
-    }
-    if (I.h_tip && I.tip_dof >= 0) {
-      int row = 0;
-      MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_free_rows.as<int>() + I.tip_dof, sizeof(int), cudaMemcpyDeviceToHost, st));
-      MSG_CUDA(ctx, cudaStreamSynchronize(st));
-      // q (n3 * Rp floats >= R doubles) is free after the loop
-      double* tipbuf = reinterpret_cast<double*>(B.q);
-      k_ebe_tip<<<(I.R + 127) / 128, 128, 0, st>>>(I.R, B.Rp, row, B.x, tipbuf);
-      count_launch(ctx);
-      MSG_CUDA(ctx, cudaMemcpyAsync(I.h_tip, tipbuf, sizeof(double) * I.R, cudaMemcpyDeviceToHost, st));
-    }
-  }
-  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  return rg_results(ctx, in, bufs, sys, s, Rtot);
+}
+
+int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
+  NvtxRange range("msg: multigrid-preconditioned element-by-element solve");
+  if (!inp.m || inp.m->ctx != ctx || max_it <= 0 || !(tol > 0))
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid arguments");
+  cudaStream_t st = ctx->stream;
+  const auto t_setup = std::chrono::steady_clock::now();
+  Mesh* lat = nullptr;
+  MSG_TRY(lattice_shadow(ctx, inp.m, &lat));
+  const std::vector<RgInput> in(1, inp);
+  std::vector<RgBuf> bufs(1);
+  std::vector<RgSys> sys(1);
+  MSG_TRY(rg_plan(ctx, inp, bufs[0], 64));  // the packed level-0 operator of the V-cycle takes pairs of groups
+  RgBuf& B = bufs[0];
+  const int Rp = B.Rp, Rtot = Rp;
+  sys[0].goff = 0;
+  std::vector<RgItem> items, items_u;
+  for (int blk = 0; blk < B.n_blk; ++blk)
+    for (int rb = 0; rb < Rp; rb += 32 * B.G) items.push_back(RgItem{0, blk, rb, B.G});
+  for (int blk = 0; blk < B.n_blk_u; ++blk)
+    for (int rb = 0; rb < Rp; rb += 32) items_u.push_back(RgItem{0, blk, rb, 1});
+  const int n_items = (int)items.size(), n_items_u = (int)items_u.size();
+  const size_t nv = 3 * (size_t)inp.m->n_nodes * Rp;
+  const size_t scal_bytes = (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 3) * (size_t)Rtot +
+                            sizeof(int) * (1 + Rtot / 32 + 2);
+  RgSys* d_sys = nullptr;
+  RgItem *d_items = nullptr, *d_items_u = nullptr;
+  unsigned char* scal_base = nullptr;
+  int* d_status = nullptr;
+  float* z = nullptr;
+  auto carve_all = [&](Carver& c) {
+    rg_carve(inp, B, c);
+    z = c.take<float>(nv);
+    d_sys = c.take<RgSys>(1);
+    d_items = c.take<RgItem>(items.size());
+    d_items_u = c.take<RgItem>(items_u.size());
+    scal_base = c.take<unsigned char>(scal_bytes);
+    d_status = c.take<int>(1);
+  };
+  Carver count;
+  carve_all(count);
+  void *arena = nullptr, *k300 = nullptr;
+  MSG_TRY(workspace(ctx, 34, count.off, &arena));
+  MSG_TRY(workspace(ctx, 35, sizeof(double) * 300 * (size_t)inp.m->n_elems, &k300));
+  Carver c;
+  c.base = static_cast<unsigned char*>(arena);
+  carve_all(c);
+  MSG_TRY(rg_setup(ctx, inp, B, static_cast<double*>(k300), d_status));
+  RgSys& Y = sys[0];
+  Mesh* m = inp.m;
+  Y.n_nodes = m->n_nodes;
+  Y.Rp = Rp;
+  Y.n_blk = B.n_blk;
+  Y.n_blk_u = B.n_blk_u;
+  Y.inc_ptr = B.ptr;
+  Y.inc = B.inc;
+  Y.conn = m->d_conn.as<int>();
+  Y.mask = m->d_mask.as<uint8_t>();
+  Y.K32 = B.K32;
+  Y.K64 = B.K64;
+  Y.E32 = B.E32;
+  Y.E64 = B.E64;
+  Y.b = B.bn;
+  Y.x = B.x;
+  Y.d = B.d;
+  Y.r = B.r;
+  Y.p = B.p;
+  Y.q = B.q;
+  Y.dinv = B.dinv;
+  Y.part = B.part;
+  Y.part_u = B.part_u;
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(RgItem) * items.size(), cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_items_u, items_u.data(), sizeof(RgItem) * items_u.size(), cudaMemcpyHostToDevice,
+                                st));
+  RgScal s;
+  s.gamma = reinterpret_cast<double*>(scal_base);
+  s.rr_ref = s.gamma + Rtot;
+  s.bnorm = s.rr_ref + Rtot;
+  s.res = s.bnorm + Rtot;
+  s.alpha = reinterpret_cast<float*>(s.res + Rtot);
+  s.beta = s.alpha + Rtot;
+  s.done = reinterpret_cast<int*>(s.beta + Rtot);
+  s.its = s.done + Rtot;
+  s.rsys = s.its + Rtot;
+  s.sreq = s.rsys + Rtot;
+  s.gact = s.sreq + 1;
+  s.flags = s.gact + Rtot / 32;
+  MSG_CUDA(ctx, cudaMemsetAsync(s.rsys, 0, sizeof(int) * (Rtot + 1), st));  // rsys (all 0) and sreq
+  // the preconditioner: the V-cycle of the cube lattice of the same numbering
+  // (its own workspace slots), E of every realization on the lattice's elements
+  void* P = nullptr;
+  MSG_TRY(gmg_precond_create(ctx, lat, inp.nu, inp.kl, inp.d_xi, inp.R, Rp, &P));
+  struct PGuard {
+    void* p;
+    ~PGuard() { gmg_precond_destroy(p); }
+  } pguard{P};
+  const RgSys* dS = d_sys;
+  const int n_groups = Rtot / 32, g_groups = (n_groups + kEbeWarps - 1) / kEbeWarps;
+  const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
+  int occ_apply = 1, occ_resid = 1, occ_u = 1;
+  MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_apply, k_rg_apply, 32 * kEbeWarps, 0));
+  MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_resid, k_rg_resid64, 32 * kEbeWarps, 0));
+  MSG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k_rg_fold, 32 * kEbeWarps, 0));
+  auto grid_of = [&](int occ, int n) { return std::max(1, std::min(n, ctx->sm_count * std::max(1, occ))); };
+  const int g_apply = grid_of(occ_apply, n_items), g_resid = grid_of(occ_resid, n_items);
+  const int g_fold = grid_of(occ_u, n_items), g_u = n_items_u;
+  // start: x = 0, d = 0, r = b, ||b||; z = V(b), gamma = z.b, p = z
+  k_rg_init<<<dim3(B.n_blk, Rp / 32), 32 * kEbeWarps, 0, st>>>(Y);
+  MSG_CUDA(ctx, cudaMemsetAsync(s.gact, 0xff, sizeof(int) * n_groups, st));  // every group until k_vc_start
+  MSG_TRY(gmg_precond_apply(ctx, P, B.r, z, st));
+  k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+  k_vc_start<<<Rp / kEbeWarps, 32 * kEbeWarps, 0, st>>>(Y, inp.R, s);
+  k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
+  k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+  count_launch(ctx, 5);
   MSG_CUDA(ctx, cudaGetLastError());
-  for (int i = 0; i < S; ++i) {
-    const int g0 = sys[i].goff;
-    for (int r = 0; r < in[i].R; ++r) {
-      if (in[i].h_its) in[i].h_its[r] = its[g0 + r];
-      if (in[i].h_res) in[i].h_res[r] = res[g0 + r];
-      if (done[g0 + r] != 1 && status == MSG_OK)
-        status = done[g0 + r] == 2 ? MSG_ERR_BREAKDOWN : MSG_ERR_NOT_CONVERGED;
-    }
+  // two iterations to a graph launch (the multigrid loop's chunk), its reliable-update factor
+  constexpr int kChunk = 2;
+  const double delta2 = ctx->mg_delta * ctx->mg_delta, tol2 = 0.25 * tol * tol;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(s.flags, 0, 2 * sizeof(int), st);
+  for (int k = 0; k < kChunk; ++k) {
+    k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s.gact);
+    k_vc_alpha<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s);
+    k_vc_update<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
+    gmg_precond_apply(ctx, P, B.r, z, st);
+    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+    k_vc_beta<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol2, delta2, max_it);
+    k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
   }
-  if (status != MSG_OK) set_error(ctx, status, "element-by-element batch: a realization did not converge");
-  return status;
+  k_rg_chunk_end_count<<<g_scal, 32 * kEbeWarps, 0, st>>>(Rtot, s);
+  const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+  if (ce != cudaSuccess) return cuda_error(ctx, ce, "cudaStreamEndCapture");
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) return cuda_error(ctx, ie, "cudaGraphInstantiate");
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() { cudaGraphExecDestroy(e); }
+  } guard{exec};
+  int* h = ctx->h_flags;
+  int n_true = 0;
+  MSG_CUDA(ctx, cudaStreamSynchronize(st));
+  ctx->t_phase[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
+  cudaEventRecord(ctx->ev[10], st);
+  const int max_chunks = max_it / kChunk + 2;
+  for (int chunk = 0; chunk < max_chunks; ++chunk) {
+    MSG_CUDA(ctx, cudaGraphLaunch(exec, st));
+    count_launch(ctx, kChunk * 6 + 1);
+    MSG_TRY(publish_flags(ctx, s.flags, 2, h, ctx->d_hflags, st));
+    MSG_CUDA(ctx, cudaStreamSynchronize(st));
+    if (h[1] == 0) break;
+    if (h[0] == 0) continue;
+    // FP64 true residual, z = V(r), gamma = z.r: every running realization stops or continues
+    ++n_true;
+    MSG_CUDA(ctx, cudaMemsetAsync(s.flags + 1, 0, sizeof(int), st));
+    k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s, 0);
+    k_rg_resid64<<<g_resid, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s);
+    MSG_TRY(gmg_precond_apply(ctx, P, B.r, z, st));
+    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+    k_vc_true<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol, max_it);
+    k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
+    MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int), st));
+    count_launch(ctx, 6);
+    MSG_CUDA(ctx, cudaGetLastError());
+    MSG_TRY(publish_flags(ctx, s.flags + 1, 1, h + 1, ctx->d_hflags ? ctx->d_hflags + 1 : nullptr, st));
+    MSG_CUDA(ctx, cudaStreamSynchronize(st));
+    if (h[1] == 0) break;
+  }
+  cudaEventRecord(ctx->ev[11], st);
+  MSG_CUDA(ctx, cudaEventSynchronize(ctx->ev[11]));
+  float loop_ms = 0.f;
+  cudaEventElapsedTime(&loop_ms, ctx->ev[10], ctx->ev[11]);
+  ctx->t_phase[1] = loop_ms;
+  ctx->t_phase[2] = n_true;
+  ctx->t_phase[3] = 0.0;
+  k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s, 1);
+  count_launch(ctx);
+  return rg_results(ctx, in, bufs, sys, s, Rtot);
 }
 
 }  // namespace msg

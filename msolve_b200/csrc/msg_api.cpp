@@ -141,6 +141,7 @@ void release(Mesh* m) {
         delete static_cast<msg_matrix*>(ctx->mc_matrix);
         ctx->mc_matrix = nullptr;
       }
+      if (m->shadow) release(m->shadow);
       delete static_cast<msg_mesh*>(m);
     }
     release(ctx);
@@ -341,6 +342,30 @@ static void detect_structured(Mesh* m) {
 }
 
 // Index maps of the padded lattice used by the batched matrix-free path.
+// The generator's numbering and element order with any node coordinates
+// (element 0 on node 0, x fastest; the cube test of detect_structured left out).
+static void detect_lattice_topology(Mesh* m) {
+  m->topo_lattice = false;
+  const int nn = m->n_nodes, ne = m->n_elems;
+  if (nn < 8 || ne < 1 || m->conn[0] != 0) return;
+  const int NX = m->conn[3], NXY = m->conn[4];
+  if (NX < 2 || NXY < 2 * NX || NXY % NX != 0 || nn % NXY != 0) return;
+  const int nx = NX - 1, ny = NXY / NX - 1, nz = nn / NXY - 1;
+  if (nz < 1 || (int64_t)nx * ny * nz != ne) return;
+  for (int k = 0, e = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i, ++e) {
+        const int b = i + NX * j + NXY * k;
+        const int ref[8] = {b, b + 1, b + NX + 1, b + NX, b + NXY, b + NXY + 1, b + NXY + NX + 1, b + NXY + NX};
+        for (int a = 0; a < 8; ++a)
+          if (m->conn[8 * (size_t)e + a] != ref[a]) return;
+      }
+  m->topo_lattice = true;
+  m->tnx = nx;
+  m->tny = ny;
+  m->tnz = nz;
+}
+
 static int build_padded_maps(Context* ctx, Mesh* m) {
   const int NX = m->nx + 1, NY = m->ny + 1, NZ = m->nz + 1;
   m->NXp = NX + 2; m->NYp = NY + 2; m->NZp = NZ + 2;
@@ -400,6 +425,7 @@ static int create_mesh(Context* ctx, int n_nodes, const double* xyz, int n_elems
   MSG_TRY(build_pattern(m.get()));
   detect_structured(m.get());
   if (m->structured) MSG_TRY(build_padded_maps(ctx, m.get()));
+  else detect_lattice_topology(m.get());
   std::vector<double> exyz(24 * (size_t)n_elems), cen(3 * (size_t)n_elems);
   for (int e = 0; e < n_elems; ++e) {
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -494,7 +520,14 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
     in[0].tip_dof = tip_dof;
     in[0].h_its = iterations;
     in[0].h_res = rel_res;
-    status = ebe_ragged_solve(ctx, in, max_it, tol);
+    // lattice topology with moved nodes: Jacobi replaced by the V-cycle of the
+    // cube lattice of the same numbering when that lattice coarsens
+    const bool coarsens = m->topo_lattice && m->tnx % 2 == 0 && m->tny % 2 == 0 && m->tnz % 2 == 0 &&
+                          m->tnx >= 4 && m->tny >= 4 && m->tnz >= 4;
+    if (coarsens && ctx->multigrid != 0)
+      status = ebe_vcycle_solve(ctx, in[0], max_it, tol);
+    else
+      status = ebe_ragged_solve(ctx, in, max_it, tol);
   } else if (mode == MSG_MODE_MIXED_BATCHED && m->structured) {
     BatchOut o;
     std::vector<double> htip(R);
@@ -588,6 +621,41 @@ static double kl_root(double A, double c, bool is_sin, double lo, double hi) {
     w = wn;
   }
   return w;
+}
+
+int lattice_shadow(Context* ctx, Mesh* m, Mesh** out) {
+  std::lock_guard<std::mutex> lock(m->shadow_mu);
+  if (!m->topo_lattice) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mesh has no lattice topology");
+  if (!m->shadow) {
+    // cubes of the mean spacing of the mesh's bounding box, from its lower corner
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < m->n_nodes; ++i)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], m->xyz[3 * (size_t)i + a]);
+        hi[a] = std::max(hi[a], m->xyz[3 * (size_t)i + a]);
+      }
+    const int n[3] = {m->tnx, m->tny, m->tnz};
+    double h = 0.0;
+    for (int a = 0; a < 3; ++a) h += (hi[a] - lo[a]) / n[a] / 3.0;
+    if (!(h > 0)) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "degenerate lattice extent");
+    std::vector<double> xyz(3 * (size_t)m->n_nodes);
+    for (int k = 0, t = 0; k <= n[2]; ++k)
+      for (int j = 0; j <= n[1]; ++j)
+        for (int i = 0; i <= n[0]; ++i, ++t) {
+          xyz[3 * (size_t)t] = lo[0] + i * h;
+          xyz[3 * (size_t)t + 1] = lo[1] + j * h;
+          xyz[3 * (size_t)t + 2] = lo[2] + k * h;
+        }
+    Mesh* sh = nullptr;
+    MSG_TRY(create_mesh(ctx, m->n_nodes, xyz.data(), m->n_elems, m->conn.data(), m->dof.data(), m->n_dofs, &sh));
+    if (!sh->structured) {
+      release(sh);
+      return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "lattice shadow was not recognised as a cube lattice");
+    }
+    m->shadow = sh;
+  }
+  *out = m->shadow;
+  return MSG_OK;
 }
 
 }  // namespace msg

@@ -233,6 +233,14 @@ struct Mesh {
   std::mutex gmg_mu;
   int gmg_levels = 1;
   DevMem d_gmg_mask[kGmgMaxLevels], d_gmg_interior[kGmgMaxLevels];
+  // lattice topology with moved nodes (the generator's numbering and element
+  // order, any coordinates; not `structured`): the element-by-element loop
+  // takes the multigrid V-cycle of the cube lattice of the same numbering
+  // (`shadow`, built on first use, owned) as its preconditioner
+  bool topo_lattice = false;
+  int tnx = 0, tny = 0, tnz = 0;
+  Mesh* shadow = nullptr;
+  std::mutex shadow_mu;
 };
 
 struct PcgState {
@@ -342,6 +350,18 @@ struct BatchOut {
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
 
+// The cube lattice with the numbering of a lattice-topology mesh (built once).
+int lattice_shadow(Context* ctx, Mesh* m, Mesh** out);
+// Multigrid V-cycle of a cube lattice mesh as a preconditioner of another
+// operator with the same node numbering (kernels_block.cu): R realizations of
+// the KL field xi [R][n_terms] (on the lattice's element centroids), Rp a
+// multiple of 32. apply enqueues z = V(r) on st for node-layout FP32 vectors
+// [n_nodes * 3][Rp] (constrained components of r zero); graph-capturable.
+int gmg_precond_create(Context* ctx, Mesh* lattice, double nu, const MSG_KL* kl, const double* d_xi, int R, int Rp,
+                       void** out);
+int gmg_precond_apply(Context* ctx, void* P, const float* r_node, float* z_node, cudaStream_t st);
+void gmg_precond_destroy(void* P);
+
 // One system of a batched element-by-element solve (kernels_ebe.cu): a mesh
 // of any shape with its material, KL field and realizations; xi [R][n_terms],
 // b [n_dofs] and X [R][n_dofs] on the device (X may be null), tip, iterations
@@ -362,6 +382,9 @@ struct RgInput {
 // All realizations of all systems in one loop (each system's realizations
 // padded to 32 inside); a system's results independent of the other systems.
 int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol);
+// One system on a mesh with lattice topology: PCG over the element-by-element
+// operator preconditioned by the cube lattice's multigrid V-cycle.
+int ebe_vcycle_solve(Context* ctx, const RgInput& in, int max_it, double tol);
 
 // Newmark batch (implicit integration of every realization, constant time step)
 struct NewmarkParams {

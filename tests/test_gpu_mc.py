@@ -170,6 +170,37 @@ def test_per_realization_path_on_a_larger_second_mesh(mode, element_batch):
             assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max(), (n, r)
 
 
+def test_multigrid_on_a_distorted_lattice(ctx):
+    """A mesh with the lattice's topology and moved interior nodes (8^3, 40
+    realizations) takes PCG over the element-by-element operator with the cube
+    lattice's V-cycle as preconditioner: within 1e-8 of FP64 oracle solves of
+    the distorted geometry, with at least 3x fewer operator products than the
+    same loop with the diagonal preconditioner (multigrid 0)."""
+    n, R, K = 8, 40, 10
+    model = distorted_model(n, seed=21, amp=0.2)
+    kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 8)
+    xi = np.random.default_rng(22).standard_normal((R, K))
+    runs = {}
+    for mg in (1, 0):
+        ctx.set_option("multigrid", mg)
+        try:
+            mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=R,
+                                                            mode="mixed", tolerance=1e-10)
+            mc.RandomNumbers = xi
+            mc.Solve()
+        finally:
+            ctx.set_option("multigrid", 1)
+        assert (mc.Residuals < 1e-10).all()
+        runs[mg] = mc
+    assert 3 * runs[1].Iterations.mean() < runs[0].Iterations.mean(), (runs[1].Iterations.mean(),
+                                                                         runs[0].Iterations.mean())
+    E = O.kl_field(O.centroids(model.xyz, model.conn), [n, n, n], kl.table(), xi, sigma=kl.sigma)
+    for r in (0, R - 1):
+        xo, _ = oracle_csr_solve(model, E[r])
+        for mc in runs.values():
+            assert np.abs(mc.Solutions[r] - xo).max() <= 1e-8 * np.abs(xo).max(), r
+
+
 def test_element_batch_on_a_distorted_mesh_sample(ctx):
     """Batched element-by-element loop on a distorted 10^3 mesh, 70 realizations
     (three 32-wide groups, the last one partly padding): sampled realizations
