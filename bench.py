@@ -98,6 +98,8 @@ def parse():
                    help="only the batched solve of --R realizations on an --n cube with its interior nodes moved "
                         "(the element-by-element path), one JSON line")
     p.add_argument("--ragged-R", type=int, default=64, help="realizations per system of the ragged batch")
+    p.add_argument("--ragged-only", action="store_true",
+                   help="only the ragged batch of uneven mesh sizes (MSG_MC_SOLVE_RAGGED), one JSON line")
     p.add_argument("--single-only", action="store_true",
                    help="run only the single-solve measurement (FP64 and mixed) and print its JSON object")
     p.add_argument("--serve-rates", default="100,400,1000,2000,5000", help="Poisson arrival rates (requests/s) to run")
@@ -355,8 +357,10 @@ def ragged_leg(args, ctx):
     """Monte Carlo systems of uneven size in one batch (MSG_MC_SOLVE_RAGGED): the
     serving sides {8, 16, 24, 32, 48} (cube lattices) and a 24^3 block with its
     interior nodes moved (not a lattice), args.ragged_R realizations each with
-    its own 50-term KL field (sigma 0.3, l 0.2 * side), Jacobi-PCG with the FP32
-    element-by-element operator and the FP64 true residual < 1e-8. Timed
+    its own 50-term KL field (sigma 0.3, l 0.2 * side), PCG with the FP32
+    element-by-element operator and the FP64 true residual < 1e-8, each system
+    preconditioned by the V-cycle of its cube lattice (the diagonal with the
+    multigrid option 0). Timed
     (device time of the call) as one ragged batch after a warm-up, and as the
     same systems one call each; the oracle solves one realization of the 48^3
     lattice and of the distorted 24^3 (FP64 CSR Jacobi-PCG to 1e-12)."""
@@ -388,9 +392,10 @@ def ragged_leg(args, ctx):
     res, ms = solve(idx)
     seq_ms = sum(solve([j])[1] for j in idx)
     dof_its = sum(systems[j][2].n_dofs * float(res[j]["Iterations"].sum()) for j in idx)
+    prec = "Jacobi-PCG" if ctx.get_option("multigrid") == 0 else "PCG preconditioned by each system's V-cycle"
     out = {"workload": f"{len(specs)} Monte Carlo systems in one batch: cube lattices of side 8, 16, 24, 32, 48 and "
                        f"a 24^3 block with interior nodes moved by up to 0.2, {R} realizations each, "
-                       f"{args.terms}-term KL lognormal E, Jacobi-PCG (FP32 element-by-element operator, FP64 "
+                       f"{args.terms}-term KL lognormal E, {prec} (FP32 element-by-element operator, FP64 "
                        f"iterate) to the FP64 true relative residual < {tol:g}",
            "systems": [{"mesh": f"{n}^3" + (" distorted" if dist else ""), "free_dofs": model.n_dofs,
                         "mean_iterations": float(res[j]["Iterations"].mean())}
@@ -639,10 +644,10 @@ def main():
     if args.single_only:
         print(json.dumps(single_leg(args, ctx)))
         return
-    if args.distorted_only:
+    if args.distorted_only or args.ragged_only:
         if args.multigrid is not None:
             ctx.set_option("multigrid", args.multigrid)
-        print(json.dumps(distorted_leg(args, ctx)))
+        print(json.dumps(distorted_leg(args, ctx) if args.distorted_only else ragged_leg(args, ctx)))
         return
     if args.chunk is not None:
         ctx.set_option("chunk", args.chunk)

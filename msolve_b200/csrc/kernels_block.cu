@@ -4380,14 +4380,15 @@ struct GmgPrecondImpl {
   BlockSys B;
   Scal s0;
   DevMem zero;
+  DevMem own[kWorkSlots];
 };
 
 }  // namespace
 
 int gmg_precond_create(Context* ctx, Mesh* lat, double nu, const MSG_KL* kl, const double* d_xi, int R, int Rp,
-                       void** out) {
+                       bool own_buffers, void** out) {
   std::unique_ptr<GmgPrecondImpl> P(new GmgPrecondImpl());
-  MSG_TRY(block_setup(ctx, lat, nu, 1.0, 1.0, 0.0, R, Rp, &P->B));
+  MSG_TRY(block_setup(ctx, lat, nu, 1.0, 1.0, 0.0, R, Rp, &P->B, own_buffers ? P->own : nullptr));
   if (!P->B.gmg)
     return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "the lattice does not coarsen (or multigrid is off)");
   KLDevice kd;

@@ -77,7 +77,9 @@ struct RgSys {
   double* x;                     // [n_nodes * 3][Rp]
   float *d, *r, *p, *q, *dinv;   // [n_nodes * 3][Rp]
   double* part;                  // [kRgParts][n_blk][Rp]
-  double* part_u;                // [2][n_blk_u][Rp]: (D r).r and r.r of the update pass
+  double* part_u;                // [2][n_blk_u][Rp]: (D r).r and r.r of the update pass (z.r, r.r: ebe_mg_solve)
+  int kind;                      // ebe_mg_solve: 1 multigrid V-cycle, 0 diagonal preconditioner
+  float* z;                      // ebe_mg_solve: [n_nodes * 3][Rp] preconditioned residual
 };
 struct RgItem {
   int sys, blk, rb, G;  // nodes blk * 64 .., realizations rb .. rb + 32 G - 1
@@ -645,7 +647,8 @@ __global__ void k_ebe_tip(int R, int Rp, int row, const double* __restrict__ x, 
 }
 
 // ---------------------------------------------------------------- multigrid-preconditioned loop (one system)
-// Standard PCG with z = V(r) (the cube lattice's V-cycle, gmg_precond_apply):
+// Standard PCG with z = M^-1 r: M^-1 the V-cycle of the system's cube lattice
+// (gmg_precond_apply) or the diagonal (k_vc_jacobi_z):
 // operator (k_rg_apply: q = K p, partial p.q), alpha, update (r, d and r.r),
 // preconditioner, z.r, beta, direction. Work items of the update pass; the
 // partials of the update pass are part_u [0] z.r and [1] r.r.
@@ -680,7 +683,7 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_update(const RgSys* __res
 
 // partial z.r (into part_u[0])
 __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_zr(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items,
-                                                         int n_items, RgScal s, const float* __restrict__ z) {
+                                                         int n_items, RgScal s) {
   __shared__ double sh[kEbeWarps * 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
@@ -695,7 +698,7 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_zr(const RgSys* __restric
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
-        zr += (double)z[o] * (double)S.r[o];
+        zr += (double)S.z[o] * (double)S.r[o];
       }
     rg_block_partial(zr, sh, S.part_u + (size_t)I.blk * Rp + col);
   }
@@ -703,7 +706,7 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_zr(const RgSys* __restric
 
 // p = z + beta p
 __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_dir(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items,
-                                                          int n_items, RgScal s, const float* __restrict__ z) {
+                                                          int n_items, RgScal s) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const RgItem I = items[it];
@@ -717,7 +720,28 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_dir(const RgSys* __restri
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
-        S.p[o] = fmaf(be, S.p[o], z[o]);
+        S.p[o] = fmaf(be, S.p[o], S.z[o]);
+      }
+  }
+}
+
+// z = D^-1 r for the systems with the diagonal preconditioner
+__global__ void __launch_bounds__(32 * kEbeWarps) k_vc_jacobi_z(const RgSys* __restrict__ Sys,
+                                                               const RgItem* __restrict__ items, int n_items,
+                                                               RgScal s) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const RgItem I = items[it];
+    const RgSys S = Sys[I.sys];
+    if (S.kind != 0 || !s.gact[(S.goff + I.rb) / 32]) continue;
+    const int Rp = S.Rp, col = I.rb;
+    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
+#pragma unroll 2
+    for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
+        S.z[o] = S.dinv[o] * S.r[o];
       }
   }
 }
@@ -781,11 +805,16 @@ __global__ void k_vc_start(RgSys S, int R, RgScal s) {
   s.done[g] = (r >= R || !(bb > 0.0)) ? 1 : 0;
 }
 
-// After the FP64 true residual (r.r in part kRr) and z = V(r) (z.r in part_u[0])
+// After the FP64 true residual (r.r in part kRr) and z = M^-1 r (z.r in part_u[0])
+// of the systems that asked; flags[1] counts the realizations still running
 __global__ void k_vc_true(const RgSys* __restrict__ Sys, int Rtot, RgScal s, double tol, int max_it) {
   const int g = rg_warp_index();
   if (g >= Rtot || s.done[g]) return;
   const int lane = threadIdx.x & 31;
+  if (!s.sreq[s.rsys[g]]) {  // its system took no true residual
+    if (lane == 0) atomicAdd(s.flags + 1, 1);
+    return;
+  }
   const RgSys& S = Sys[s.rsys[g]];
   const int r = g - S.goff;
   const double rr = rg_sum(S.part + (size_t)kRr * S.n_blk * S.Rp, S.n_blk, S.Rp, r);
@@ -1151,39 +1180,57 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   return rg_results(ctx, in, bufs, sys, s, Rtot);
 }
 
-int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
-  NvtxRange range("msg: multigrid-preconditioned element-by-element solve");
-  if (!inp.m || inp.m->ctx != ctx || max_it <= 0 || !(tol > 0))
+int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector<int>& use_vcycle, int max_it,
+                 double tol) {
+  NvtxRange range("msg: preconditioned element-by-element solve");
+  if (in.empty() || in.size() != use_vcycle.size() || max_it <= 0 || !(tol > 0))
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid arguments");
   cudaStream_t st = ctx->stream;
   const auto t_setup = std::chrono::steady_clock::now();
-  Mesh* lat = nullptr;
-  MSG_TRY(lattice_shadow(ctx, inp.m, &lat));
-  const std::vector<RgInput> in(1, inp);
-  std::vector<RgBuf> bufs(1);
-  std::vector<RgSys> sys(1);
-  MSG_TRY(rg_plan(ctx, inp, bufs[0], 64));  // the packed level-0 operator of the V-cycle takes pairs of groups
-  RgBuf& B = bufs[0];
-  const int Rp = B.Rp, Rtot = Rp;
-  sys[0].goff = 0;
+  const int S = (int)in.size();
+  if (S > 1000) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: more than 1000 systems");
+  std::vector<RgBuf> bufs(S);
+  std::vector<RgSys> sys(S);
+  std::vector<Mesh*> lats(S, nullptr);
+  int Rtot = 0;
+  for (int i = 0; i < S; ++i) {
+    if (!in[i].m || in[i].m->ctx != ctx)
+      return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: system %d has no mesh of this context", i);
+    if (use_vcycle[i]) MSG_TRY(lattice_shadow(ctx, in[i].m, &lats[i]));
+    // the packed level-0 operator of a V-cycle takes pairs of realization groups
+    MSG_TRY(rg_plan(ctx, in[i], bufs[i], use_vcycle[i] ? 64 : 32));
+    sys[i].goff = Rtot;
+    Rtot += bufs[i].Rp;
+  }
+  int G = 8;
+  for (int i = 0; i < S; ++i) G = std::min(G, bufs[i].G);
+  for (int i = 0; i < S; ++i) bufs[i].G = G;
   std::vector<RgItem> items, items_u;
-  for (int blk = 0; blk < B.n_blk; ++blk)
-    for (int rb = 0; rb < Rp; rb += 32 * B.G) items.push_back(RgItem{0, blk, rb, B.G});
-  for (int blk = 0; blk < B.n_blk_u; ++blk)
-    for (int rb = 0; rb < Rp; rb += 32) items_u.push_back(RgItem{0, blk, rb, 1});
+  std::vector<int> rsys(Rtot);
+  for (int i = 0; i < S; ++i) {
+    const RgBuf& B = bufs[i];
+    for (int blk = 0; blk < B.n_blk; ++blk)
+      for (int rb = 0; rb < B.Rp; rb += 32 * B.G) items.push_back(RgItem{i, blk, rb, B.G});
+    for (int blk = 0; blk < B.n_blk_u; ++blk)
+      for (int rb = 0; rb < B.Rp; rb += 32) items_u.push_back(RgItem{i, blk, rb, 1});
+    for (int r = 0; r < B.Rp; ++r) rsys[sys[i].goff + r] = i;
+  }
   const int n_items = (int)items.size(), n_items_u = (int)items_u.size();
-  const size_t nv = 3 * (size_t)inp.m->n_nodes * Rp;
   const size_t scal_bytes = (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 3) * (size_t)Rtot +
-                            sizeof(int) * (1 + Rtot / 32 + 2);
+                            sizeof(int) * (S + Rtot / 32 + 2);
   RgSys* d_sys = nullptr;
   RgItem *d_items = nullptr, *d_items_u = nullptr;
   unsigned char* scal_base = nullptr;
   int* d_status = nullptr;
-  float* z = nullptr;
+  std::vector<float*> zs(S, nullptr);
+  int max_ne = 0;
+  for (int i = 0; i < S; ++i) max_ne = std::max(max_ne, in[i].m->n_elems);
   auto carve_all = [&](Carver& c) {
-    rg_carve(inp, B, c);
-    z = c.take<float>(nv);
-    d_sys = c.take<RgSys>(1);
+    for (int i = 0; i < S; ++i) {
+      rg_carve(in[i], bufs[i], c);
+      zs[i] = c.take<float>(3 * (size_t)in[i].m->n_nodes * bufs[i].Rp);
+    }
+    d_sys = c.take<RgSys>(S);
     d_items = c.take<RgItem>(items.size());
     d_items_u = c.take<RgItem>(items_u.size());
     scal_base = c.take<unsigned char>(scal_bytes);
@@ -1193,35 +1240,40 @@ int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
   carve_all(count);
   void *arena = nullptr, *k300 = nullptr;
   MSG_TRY(workspace(ctx, 34, count.off, &arena));
-  MSG_TRY(workspace(ctx, 35, sizeof(double) * 300 * (size_t)inp.m->n_elems, &k300));
+  MSG_TRY(workspace(ctx, 35, sizeof(double) * 300 * (size_t)max_ne, &k300));
   Carver c;
   c.base = static_cast<unsigned char*>(arena);
   carve_all(c);
-  MSG_TRY(rg_setup(ctx, inp, B, static_cast<double*>(k300), d_status));
-  RgSys& Y = sys[0];
-  Mesh* m = inp.m;
-  Y.n_nodes = m->n_nodes;
-  Y.Rp = Rp;
-  Y.n_blk = B.n_blk;
-  Y.n_blk_u = B.n_blk_u;
-  Y.inc_ptr = B.ptr;
-  Y.inc = B.inc;
-  Y.conn = m->d_conn.as<int>();
-  Y.mask = m->d_mask.as<uint8_t>();
-  Y.K32 = B.K32;
-  Y.K64 = B.K64;
-  Y.E32 = B.E32;
-  Y.E64 = B.E64;
-  Y.b = B.bn;
-  Y.x = B.x;
-  Y.d = B.d;
-  Y.r = B.r;
-  Y.p = B.p;
-  Y.q = B.q;
-  Y.dinv = B.dinv;
-  Y.part = B.part;
-  Y.part_u = B.part_u;
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys), cudaMemcpyHostToDevice, st));
+  for (int i = 0; i < S; ++i) {
+    RgBuf& B = bufs[i];
+    MSG_TRY(rg_setup(ctx, in[i], B, static_cast<double*>(k300), d_status));
+    Mesh* m = in[i].m;
+    RgSys& Y = sys[i];
+    Y.n_nodes = m->n_nodes;
+    Y.Rp = B.Rp;
+    Y.n_blk = B.n_blk;
+    Y.n_blk_u = B.n_blk_u;
+    Y.inc_ptr = B.ptr;
+    Y.inc = B.inc;
+    Y.conn = m->d_conn.as<int>();
+    Y.mask = m->d_mask.as<uint8_t>();
+    Y.K32 = B.K32;
+    Y.K64 = B.K64;
+    Y.E32 = B.E32;
+    Y.E64 = B.E64;
+    Y.b = B.bn;
+    Y.x = B.x;
+    Y.d = B.d;
+    Y.r = B.r;
+    Y.p = B.p;
+    Y.q = B.q;
+    Y.dinv = B.dinv;
+    Y.part = B.part;
+    Y.part_u = B.part_u;
+    Y.kind = use_vcycle[i] ? 1 : 0;
+    Y.z = zs[i];
+  }
+  MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys) * S, cudaMemcpyHostToDevice, st));
   MSG_CUDA(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(RgItem) * items.size(), cudaMemcpyHostToDevice, st));
   MSG_CUDA(ctx, cudaMemcpyAsync(d_items_u, items_u.data(), sizeof(RgItem) * items_u.size(), cudaMemcpyHostToDevice,
                                 st));
@@ -1236,17 +1288,26 @@ int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
   s.its = s.done + Rtot;
   s.rsys = s.its + Rtot;
   s.sreq = s.rsys + Rtot;
-  s.gact = s.sreq + 1;
+  s.gact = s.sreq + S;
   s.flags = s.gact + Rtot / 32;
-  MSG_CUDA(ctx, cudaMemsetAsync(s.rsys, 0, sizeof(int) * (Rtot + 1), st));  // rsys (all 0) and sreq
-  // the preconditioner: the V-cycle of the cube lattice of the same numbering
-  // (its own workspace slots), E of every realization on the lattice's elements
-  void* P = nullptr;
-  MSG_TRY(gmg_precond_create(ctx, lat, inp.nu, inp.kl, inp.d_xi, inp.R, Rp, &P));
+  MSG_CUDA(ctx, cudaMemcpyAsync(s.rsys, rsys.data(), sizeof(int) * Rtot, cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
+  // preconditioners: the V-cycle of each system's cube lattice (lattice buffers
+  // of their own when several systems hold one), E of every realization on the
+  // lattice's elements
+  int n_vc = 0;
+  for (int i = 0; i < S; ++i) n_vc += use_vcycle[i] ? 1 : 0;
+  std::vector<void*> P(S, nullptr);
   struct PGuard {
-    void* p;
-    ~PGuard() { gmg_precond_destroy(p); }
+    std::vector<void*>& p;
+    ~PGuard() {
+      for (void* q : p)
+        if (q) gmg_precond_destroy(q);
+    }
   } pguard{P};
+  for (int i = 0; i < S; ++i)
+    if (use_vcycle[i])
+      MSG_TRY(gmg_precond_create(ctx, lats[i], in[i].nu, in[i].kl, in[i].d_xi, in[i].R, bufs[i].Rp, n_vc > 1, &P[i]));
   const RgSys* dS = d_sys;
   const int n_groups = Rtot / 32, g_groups = (n_groups + kEbeWarps - 1) / kEbeWarps;
   const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
@@ -1257,15 +1318,29 @@ int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
   auto grid_of = [&](int occ, int n) { return std::max(1, std::min(n, ctx->sm_count * std::max(1, occ))); };
   const int g_apply = grid_of(occ_apply, n_items), g_resid = grid_of(occ_resid, n_items);
   const int g_fold = grid_of(occ_u, n_items), g_u = n_items_u;
-  // start: x = 0, d = 0, r = b, ||b||; z = V(b), gamma = z.b, p = z
-  k_rg_init<<<dim3(B.n_blk, Rp / 32), 32 * kEbeWarps, 0, st>>>(Y);
-  MSG_CUDA(ctx, cudaMemsetAsync(s.gact, 0xff, sizeof(int) * n_groups, st));  // every group until k_vc_start
-  MSG_TRY(gmg_precond_apply(ctx, P, B.r, z, st));
-  k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
-  k_vc_start<<<Rp / kEbeWarps, 32 * kEbeWarps, 0, st>>>(Y, inp.R, s);
+  // z = M^-1 r of the systems in `which` (nullptr: all): V-cycles one system
+  // after another, the diagonal for all the others in one launch
+  auto precondition = [&](const std::vector<int>* which) -> int {
+    for (int i = 0; i < S; ++i)
+      if (P[i] && (!which || (*which)[i])) MSG_TRY(gmg_precond_apply(ctx, P[i], bufs[i].r, zs[i], st));
+    if (n_vc < S) {
+      k_vc_jacobi_z<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
+      count_launch(ctx);
+    }
+    return MSG_OK;
+  };
+  // start: x = 0, d = 0, r = b, ||b||; z = M^-1 b, gamma = z.b, p = z
+  for (int i = 0; i < S; ++i) {
+    k_rg_init<<<dim3(bufs[i].n_blk, bufs[i].Rp / 32), 32 * kEbeWarps, 0, st>>>(sys[i]);
+    count_launch(ctx);
+  }
+  MSG_CUDA(ctx, cudaMemsetAsync(s.gact, 0xff, sizeof(int) * n_groups, st));  // every group until the start
+  MSG_TRY(precondition(nullptr));
+  k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
+  for (int i = 0; i < S; ++i) k_vc_start<<<bufs[i].Rp / kEbeWarps, 32 * kEbeWarps, 0, st>>>(sys[i], in[i].R, s);
   k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
-  k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
-  count_launch(ctx, 5);
+  k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
+  count_launch(ctx, 3 + S);
   MSG_CUDA(ctx, cudaGetLastError());
   // two iterations to a graph launch (the multigrid loop's chunk), its reliable-update factor
   constexpr int kChunk = 2;
@@ -1278,10 +1353,10 @@ int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
     k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s.gact);
     k_vc_alpha<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s);
     k_vc_update<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
-    gmg_precond_apply(ctx, P, B.r, z, st);
-    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+    precondition(nullptr);
+    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     k_vc_beta<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol2, delta2, max_it);
-    k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+    k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
   }
   k_rg_chunk_end_count<<<g_scal, 32 * kEbeWarps, 0, st>>>(Rtot, s);
   const cudaError_t ce = cudaStreamEndCapture(st, &graph);
@@ -1294,29 +1369,35 @@ int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
     ~ExecGuard() { cudaGraphExecDestroy(e); }
   } guard{exec};
   int* h = ctx->h_flags;
+  int* hreq = ctx->h_flags + 16;  // per-system requests (mapped words 16 .. 16 + S)
   int n_true = 0;
+  std::vector<int> req(S, 0);
   MSG_CUDA(ctx, cudaStreamSynchronize(st));
   ctx->t_phase[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
   cudaEventRecord(ctx->ev[10], st);
   const int max_chunks = max_it / kChunk + 2;
   for (int chunk = 0; chunk < max_chunks; ++chunk) {
     MSG_CUDA(ctx, cudaGraphLaunch(exec, st));
-    count_launch(ctx, kChunk * 6 + 1);
+    count_launch(ctx, kChunk * (6 + n_vc + (n_vc < S ? 1 : 0)) + 1);
     MSG_TRY(publish_flags(ctx, s.flags, 2, h, ctx->d_hflags, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[1] == 0) break;
     if (h[0] == 0) continue;
-    // FP64 true residual, z = V(r), gamma = z.r: every running realization stops or continues
+    // the systems that asked: FP64 true residual, z = M^-1 r, gamma = z.r; each
+    // of their running realizations stops or continues
     ++n_true;
+    MSG_TRY(publish_flags(ctx, s.sreq, S, hreq, ctx->d_hflags ? ctx->d_hflags + 16 : nullptr, st));
+    MSG_CUDA(ctx, cudaStreamSynchronize(st));
+    for (int i = 0; i < S; ++i) req[i] = hreq[i];
     MSG_CUDA(ctx, cudaMemsetAsync(s.flags + 1, 0, sizeof(int), st));
     k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s, 0);
     k_rg_resid64<<<g_resid, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s);
-    MSG_TRY(gmg_precond_apply(ctx, P, B.r, z, st));
-    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s, z);
+    MSG_TRY(precondition(&req));
+    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     k_vc_true<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol, max_it);
     k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
-    MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int), st));
-    count_launch(ctx, 6);
+    MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
+    count_launch(ctx, 5);
     MSG_CUDA(ctx, cudaGetLastError());
     MSG_TRY(publish_flags(ctx, s.flags + 1, 1, h + 1, ctx->d_hflags ? ctx->d_hflags + 1 : nullptr, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
@@ -1332,6 +1413,22 @@ int ebe_vcycle_solve(Context* ctx, const RgInput& inp, int max_it, double tol) {
   k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s, 1);
   count_launch(ctx);
   return rg_results(ctx, in, bufs, sys, s, Rtot);
+}
+
+int ebe_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol) {
+  std::vector<int> vc(in.size(), 0);
+  bool any = false;
+  for (size_t i = 0; i < in.size(); ++i) {
+    const Mesh* m = in[i].m;
+    if (!m || ctx->multigrid == 0 || ctx->mg_levels < 2) continue;
+    const int nx = m->structured ? m->nx : m->tnx, ny = m->structured ? m->ny : m->tny,
+              nz = m->structured ? m->nz : m->tnz;
+    const bool lattice = m->structured || m->topo_lattice;
+    vc[i] = lattice && nx % 2 == 0 && ny % 2 == 0 && nz % 2 == 0 && nx >= 4 && ny >= 4 && nz >= 4;
+    any = any || vc[i];
+  }
+  // the loop publishes one request word a system into the mapped flag page
+  return any && in.size() <= 1000 ? ebe_mg_solve(ctx, in, vc, max_it, tol) : ebe_ragged_solve(ctx, in, max_it, tol);
 }
 
 }  // namespace msg

@@ -145,14 +145,13 @@ int kl_prepare(Context* ctx, const Mesh* m, const MSG_KL* kl, KLDevice* out) {
 
 namespace {
 __global__ void k_publish_flags(const int* __restrict__ src, int* dst, int n) {
-  const int i = threadIdx.x;
-  if (i < n) dst[i] = src[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 }  // namespace
 
 int publish_flags(Context* ctx, const int* d_src, int n, int* h_host, int* d_hmapped, cudaStream_t st) {
-  if (d_hmapped && n <= 32) {
-    k_publish_flags<<<1, 32, 0, st>>>(d_src, d_hmapped, n);
+  if (d_hmapped && n <= 1024) {
+    k_publish_flags<<<1, n <= 32 ? 32 : 256, 0, st>>>(d_src, d_hmapped, n);
     count_launch(ctx);
     MSG_CUDA(ctx, cudaGetLastError());
     return MSG_OK;

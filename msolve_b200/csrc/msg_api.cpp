@@ -90,7 +90,7 @@ Context::~Context() {
 
 int context_resources(Context* ctx) {
   if (!ctx->h_flags) {
-    MSG_CUDA(ctx, cudaHostAlloc(&ctx->h_flags, 64, cudaHostAllocMapped));
+    MSG_CUDA(ctx, cudaHostAlloc(&ctx->h_flags, 4096, cudaHostAllocMapped));
     MSG_CUDA(ctx, cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_hflags), ctx->h_flags, 0));
   }
   if (!ctx->h_stage) MSG_CUDA(ctx, cudaMallocHost(&ctx->h_stage, 8192));
@@ -520,14 +520,7 @@ static int mc_batch(Context* ctx, Mesh* m, double nu, const MSG_KL* kl, int R, c
     in[0].tip_dof = tip_dof;
     in[0].h_its = iterations;
     in[0].h_res = rel_res;
-    // lattice topology with moved nodes: Jacobi replaced by the V-cycle of the
-    // cube lattice of the same numbering when that lattice coarsens
-    const bool coarsens = m->topo_lattice && m->tnx % 2 == 0 && m->tny % 2 == 0 && m->tnz % 2 == 0 &&
-                          m->tnx >= 4 && m->tny >= 4 && m->tnz >= 4;
-    if (coarsens && ctx->multigrid != 0)
-      status = ebe_vcycle_solve(ctx, in[0], max_it, tol);
-    else
-      status = ebe_ragged_solve(ctx, in, max_it, tol);
+    status = ebe_solve(ctx, in, max_it, tol);
   } else if (mode == MSG_MODE_MIXED_BATCHED && m->structured) {
     BatchOut o;
     std::vector<double> htip(R);
@@ -624,6 +617,10 @@ static double kl_root(double A, double c, bool is_sin, double lo, double hi) {
 }
 
 int lattice_shadow(Context* ctx, Mesh* m, Mesh** out) {
+  if (m->structured) {  // a cube lattice is its own
+    *out = m;
+    return MSG_OK;
+  }
   std::lock_guard<std::mutex> lock(m->shadow_mu);
   if (!m->topo_lattice) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mesh has no lattice topology");
   if (!m->shadow) {
@@ -1329,7 +1326,7 @@ int MSG_MC_SOLVE_RAGGED(MSG_CTX ctx, int n_systems, const MSG_RAGGED_SYSTEM* sys
     I.h_its = y.iterations;
     I.h_res = y.rel_res;
   }
-  const int st = ebe_ragged_solve(ctx, in, max_it, tol);
+  const int st = ebe_solve(ctx, in, max_it, tol);
   if (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED || st == MSG_ERR_BREAKDOWN) {
     for (int i = 0; i < n_systems; ++i)
       if (systems[i].X && in[i].d_X)

@@ -92,7 +92,7 @@ struct Context {
   // enough). Slots are owned by the call sites that use them.
   DevMem* work[kWorkSlots] = {nullptr};
   // per-context host/driver resources reused by every batch (created lazily)
-  int* h_flags = nullptr;           // 64 bytes of pinned host memory, mapped into the device
+  int* h_flags = nullptr;           // 4 KB of pinned host memory, mapped into the device
   int* d_hflags = nullptr;          // the device's address of h_flags
   double* h_stage = nullptr;        // 8 KB of pinned host memory: small uploads issued as true async copies
   // unit-cube element matrices already computed (kind 0: stiffness at E = 1
@@ -143,8 +143,8 @@ int context_resources(Context* ctx);
 int workspace(Context* ctx, int slot, size_t bytes, void** out);
 // Waits for every displacement copy of the pipelined batches still in flight.
 int pipe_flush(Context* ctx);
-// h_host[0 .. n) = d_src[0 .. n) on stream st, written by a one-warp kernel
-// when d_hmapped (the device address of h_host) is given, so that the read
+// h_host[0 .. n) = d_src[0 .. n) on stream st, written by a one-block kernel
+// when d_hmapped (the device address of h_host) is given and n <= 1024, so that the read
 // never waits behind copies in flight on the device's copy engines; a copy
 // otherwise. Read h_host after synchronizing st.
 int publish_flags(Context* ctx, const int* d_src, int n, int* h_host, int* d_hmapped, cudaStream_t st);
@@ -350,15 +350,18 @@ struct BatchOut {
 int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                       const double* d_b_dof, int max_it, double tol, int tip_dof, double* d_X, BatchOut out);
 
-// The cube lattice with the numbering of a lattice-topology mesh (built once).
+// The cube lattice with the numbering of a lattice-topology mesh (built once;
+// a cube lattice is its own).
 int lattice_shadow(Context* ctx, Mesh* m, Mesh** out);
 // Multigrid V-cycle of a cube lattice mesh as a preconditioner of another
 // operator with the same node numbering (kernels_block.cu): R realizations of
 // the KL field xi [R][n_terms] (on the lattice's element centroids), Rp a
 // multiple of 32. apply enqueues z = V(r) on st for node-layout FP32 vectors
 // [n_nodes * 3][Rp] (constrained components of r zero); graph-capturable.
+// own_buffers: lattice buffers of its own (several preconditioners at once)
+// instead of the context's workspace.
 int gmg_precond_create(Context* ctx, Mesh* lattice, double nu, const MSG_KL* kl, const double* d_xi, int R, int Rp,
-                       void** out);
+                       bool own_buffers, void** out);
 int gmg_precond_apply(Context* ctx, void* P, const float* r_node, float* z_node, cudaStream_t st);
 void gmg_precond_destroy(void* P);
 
@@ -382,9 +385,15 @@ struct RgInput {
 // All realizations of all systems in one loop (each system's realizations
 // padded to 32 inside); a system's results independent of the other systems.
 int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol);
-// One system on a mesh with lattice topology: PCG over the element-by-element
-// operator preconditioned by the cube lattice's multigrid V-cycle.
-int ebe_vcycle_solve(Context* ctx, const RgInput& in, int max_it, double tol);
+// PCG over the element-by-element operator for every system of a batch, each
+// preconditioned by the multigrid V-cycle of its cube lattice (use_vcycle[i])
+// or by the diagonal; standard PCG, two iterations to a graph launch.
+int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector<int>& use_vcycle, int max_it,
+                 double tol);
+// The element-by-element batch: systems whose mesh has the lattice's numbering
+// and coarsens take the V-cycle (multigrid option != 0; then ebe_mg_solve for
+// the whole batch), a batch without one the fused Jacobi loop (ebe_ragged_solve).
+int ebe_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol);
 
 // Newmark batch (implicit integration of every realization, constant time step)
 struct NewmarkParams {
