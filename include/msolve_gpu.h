@@ -340,8 +340,15 @@ typedef struct {
  * eight iterations to a CUDA graph launch, Jacobi-preconditioned CG (the
  * reference's SolverPCG with the diagonal preconditioner) with the iterate in
  * FP64 and FP64 true residuals, to ||b - K x||/||b|| < tol in FP64 for each
- * realization. A system's results do not depend on the other systems in the
- * batch (the same bits alone and in any mix of systems). No
+ * realization. With the multigrid option on (the default), a system whose mesh
+ * has the numbering of an nx x ny x nz lattice with every side even and >= 4
+ * (moved nodes allowed) is preconditioned instead by the V-cycle of its cube
+ * lattice, and then the whole batch runs standard PCG (the operator, scalar
+ * and vector launches shared, one V-cycle per such system, the diagonal for
+ * the others; two iterations to a graph launch). A system's results do not
+ * depend on the other systems in the batch: the same bits alone and in any mix
+ * of systems, except that a system without a V-cycle takes the fused Jacobi
+ * loop when no system of its batch has one (the same solution to rounding). No
  * reference counterpart as an entry point (the reference solves one
  * realization after another). Returns MSG_ERR_NOT_CONVERGED or
  * MSG_ERR_BREAKDOWN as MSG_MC_SOLVE_BATCH, with every other output complete. */
