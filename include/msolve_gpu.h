@@ -145,11 +145,14 @@ int MSG_MAT_DESTROY(MSG_MAT mat);
 int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
                   double* rel_res);
 
-/* MSG_PCG_SOLVE with the matrix values in FP32 inside the loop (half the
- * bytes of the dominant SpMV traffic) and FP64 refinement: vectors stay FP64;
- * when the recursive residual has dropped by "reliable_delta" (or below tol)
- * it is replaced by the FP64 true residual b - K x computed with the FP64
- * values, the search direction is kept, and the solve stops only when
+/* MSG_PCG_SOLVE with the matrix values and the loop's vectors in FP32 (half
+ * the bytes of the dominant SpMV traffic) and FP64 refinement: the iterate x is
+ * FP64, accumulated from an FP32 correction, and every dot product is summed in
+ * FP64; two kernels an iteration (the FP32 SpMV with alpha and beta from its
+ * partials, then one update pass that also forms the next direction). When the
+ * recursive residual has dropped by "reliable_delta" (or below tol) it is
+ * replaced by the FP64 true residual b - K x computed with the FP64 values,
+ * the search direction is kept, and the solve stops only when
  * ||b - K x|| / ||b|| < tol in FP64 (rel_res). iterations counts as
  * MSG_PCG_SOLVE. The FP32 copy of the values is built on first use. No
  * counterpart in the reference. */

@@ -303,42 +303,37 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int 
   }
 }
 
-// Mixed precision (FP32 matrix values): the search direction first, once per
-// row component, p_new = dinv r + beta p_old in FP64 and its FP32 copy p32,
-// so the SpMV gathers 4 bytes per column component instead of forming p from
-// three FP64 gathers.
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_dir32(int n_rows, const double* __restrict__ dinv,
-                                                           const double* __restrict__ r, double* p0, double* p1,
-                                                           float* __restrict__ p32, const PcgState* st) {
-  if (st->done) return;
-  const int it = st->it;
-  const double beta = st->beta;
-  const double* __restrict__ pold = (it & 1) ? p1 : p0;
-  double* __restrict__ pnew = (it & 1) ? p0 : p1;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
-    const double pn = dinv[i] * r[i] + beta * pold[i];
-    pnew[i] = pn;
-    p32[i] = (float)pn;
-  }
-}
-
-// q = K32 p32 for the mixed loop (FP32 values and gathered direction, each
-// 3 x 3 block product in FP32, block sums in FP64), partial p.q with the FP64
-// p of the own rows, then alpha as k_pcg_dir_spmv_rows. Same slice / warp
-// layout and streaming loads as k_pcg_dir_spmv_rows.
+// ------------------------------------------------------------------ mixed-precision PCG
+// MSG_PCG_SOLVE_MIXED's loop: FP32 matrix values and FP32 vectors (r, p, q, the
+// correction d and D^-1) inside the loop, the iterate x in FP64 (x += d at each
+// FP64 true residual) and FP64 sums for every dot product. Two kernels an
+// iteration:
+//   k_pcgm_spmv:   q = K32 p (p gathered in FP32), partials p.q, (D r).q and
+//     q.D q -> last block: alpha = gamma / p.q (breakdown check) and, since
+//     r' = r - alpha q, gamma' = (D r').r' = gamma - 2 alpha (D r).q +
+//     alpha^2 q.D q, hence beta = gamma' / gamma before the update;
+//   k_pcgm_update: r -= alpha q, d += alpha p, z = D r, p = z + beta p (the
+//     next direction, formed in the same pass) and the exact z.r, r.r ->
+//     last block: gamma = z.r, ||r||/||b||, pause for an FP64 true residual
+//     when it has dropped by delta since the last one or below tol.
+// On a pause the host runs k_pcgm_fold (x += d, d = 0), y = K64 x with the FP64
+// values and k_pcgm_true (r = b - y into the FP32 r, gamma = (D r).r; stop
+// when ||r||/||b|| < tol in FP64). The direction is kept across the
+// replacement. Per iteration the vectors cost 36 bytes a DOF besides the
+// matrix (FP64 vectors and a separate direction pass: 100).
 template <int kS, int kSpmvWarps, bool kStream, int U = 4>
-__global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_spmv32(int n_rows, int n_slices,
-                                                               const int64_t* __restrict__ slice_ptr,
-                                                               const int* __restrict__ col,
-                                                               const float* __restrict__ val,
-                                                               const float* __restrict__ p32, const double* p0,
-                                                               const double* p1, double* __restrict__ q,
-                                                               double* __restrict__ partial, PcgState* st) {
+__global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcgm_spmv(int n_rows, int n_slices,
+                                                              const int64_t* __restrict__ slice_ptr,
+                                                              const int* __restrict__ col,
+                                                              const float* __restrict__ val,
+                                                              const float* __restrict__ p32,
+                                                              const float* __restrict__ r32,
+                                                              const float* __restrict__ dinv32,
+                                                              float* __restrict__ q32, double* __restrict__ partial,
+                                                              PcgState* st) {
   __shared__ double sh[32];
   __shared__ double ys[kS][kSpmvWarps][3][32];
   if (st->done) return;
-  const int it = st->it;
-  const double* __restrict__ pnew = (it & 1) ? p0 : p1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sl = warp / kSpmvWarps, w = warp % kSpmvWarps;
   const int slice = blockIdx.x * kS + sl;
@@ -383,28 +378,163 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_spmv32(int n_rows,
   ys[sl][w][1][lane] = y1;
   ys[sl][w][2][lane] = y2;
   __syncthreads();
-  double pq = 0;
+  double pq = 0, dq = 0, qdq = 0;
   if (w == 0 && live) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       double t = ys[sl][0][c][lane];
 #pragma unroll
       for (int ww = 1; ww < kSpmvWarps; ++ww) t += ys[sl][ww][c][lane];
-      q[3 * row + c] = t;
-      pq += pnew[3 * row + c] * t;
+      const int i = 3 * row + c;
+      const float qf = (float)t, dv = dinv32[i];
+      q32[i] = qf;
+      pq += (double)p32[i] * (double)qf;
+      dq += (double)(dv * r32[i]) * (double)qf;
+      qdq += (double)(dv * qf) * (double)qf;
     }
   }
-  const double bs = block_sum(pq, sh);
-  if (threadIdx.x == 0) partial[blockIdx.x] = bs;
+  const double b0 = block_sum(pq, sh), b1 = block_sum(dq, sh), b2 = block_sum(qdq, sh);
+  if (threadIdx.x == 0) {
+    partial[3 * blockIdx.x] = b0;
+    partial[3 * blockIdx.x + 1] = b1;
+    partial[3 * blockIdx.x + 2] = b2;
+  }
   if (!last_block(&st->counter)) return;
-  const double t = sum_partials(partial, gridDim.x, 1, 0, sh);
+  const double t = sum_partials(partial, gridDim.x, 3, 0, sh);
+  const double tdq = sum_partials(partial, gridDim.x, 3, 1, sh);
+  const double tqdq = sum_partials(partial, gridDim.x, 3, 2, sh);
   if (threadIdx.x == 0) {
     st->pq = t;
     st->matvecs += 1;
     if (!(t > 0) || isnan(t)) {  // breakdown: p.q <= 0 or NaN
-      st->status = MSG_ERR_BREAKDOWN; st->done = 1; st->iterations = it;
+      st->status = MSG_ERR_BREAKDOWN; st->done = 1; st->iterations = st->it;
     } else {
-      st->alpha = st->zr / t;
+      const double al = st->zr / t;
+      const double g1 = st->zr - 2.0 * al * tdq + al * al * tqdq;
+      st->alpha = al;
+      st->beta = g1 > 0.0 ? g1 / st->zr : 0.0;  // a non-positive estimate restarts from z
+    }
+    st->counter = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcgm_update(int n3, const float* __restrict__ dinv32,
+                                                             float* __restrict__ r32, float* __restrict__ p32,
+                                                             const float* __restrict__ q32, float* __restrict__ d32,
+                                                             double* __restrict__ partial, PcgState* st) {
+  __shared__ double sh[32];
+  if (st->done) return;
+  const float al = (float)st->alpha, be = (float)st->beta;
+  double zr = 0, rr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    const float pv = p32[i];
+    const float rv = fmaf(-al, q32[i], r32[i]);
+    const float zv = dinv32[i] * rv;
+    d32[i] = fmaf(al, pv, d32[i]);
+    p32[i] = fmaf(be, pv, zv);
+    r32[i] = rv;
+    zr += (double)zv * (double)rv;
+    rr += (double)rv * (double)rv;
+  }
+  const double s1 = block_sum(rr, sh), s2 = block_sum(zr, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
+  if (!last_block(&st->counter)) return;
+  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
+  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  if (threadIdx.x == 0) {
+    const int it = st->it;
+    st->err = sqrt(tr) / st->bnorm;
+    st->rr = tr;
+    st->zr = tz;
+    if (st->err < st->tol || st->err < st->delta * st->err_ref) {
+      st->need = 1; st->done = 1;  // pause for an FP64 true residual
+    } else if (it + 1 >= st->max_it) {
+      st->done = 1; st->iterations = st->max_it; st->status = MSG_ERR_NOT_CONVERGED;
+    } else {
+      st->it = it + 1;
+    }
+    st->counter = 0;
+  }
+}
+
+// Start of the mixed loop: x = 0, d = 0, r = (float) b, D^-1 in FP32, p = z =
+// D^-1 r, gamma = z.r, ||b|| in FP64.
+__global__ void __launch_bounds__(kPcgThreads) k_pcgm_init(int n3, const double* __restrict__ b,
+                                                           const double* __restrict__ dinv, double* __restrict__ x,
+                                                           float* __restrict__ r32, float* __restrict__ p32,
+                                                           float* __restrict__ d32, float* __restrict__ dinv32,
+                                                           double* __restrict__ partial, PcgState* st) {
+  __shared__ double sh[32];
+  double bb = 0, zr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    const double bi = b[i];
+    const float rv = (float)bi, dv = (float)dinv[i], zv = dv * rv;
+    x[i] = 0;
+    r32[i] = rv;
+    dinv32[i] = dv;
+    p32[i] = zv;
+    d32[i] = 0.f;
+    bb += bi * bi;
+    zr += (double)zv * (double)rv;
+  }
+  const double s1 = block_sum(bb, sh), s2 = block_sum(zr, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
+  if (!last_block(&st->counter)) return;
+  const double tb = sum_partials(partial, gridDim.x, 2, 0, sh);
+  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  if (threadIdx.x == 0) {
+    st->bnorm = sqrt(tb);
+    st->zr = tz;
+    st->beta = 0; st->alpha = 0; st->err = 0;
+    st->it = 0; st->iterations = 0; st->matvecs = 0; st->status = 0;
+    st->done = (st->bnorm > 1e-25) ? 0 : 1;  // SolverPCG.cs:112
+    st->need = 0; st->err_ref = 1.0;
+    st->counter = 0;
+  }
+}
+
+// x += d, d = 0 (the FP32 correction into the FP64 iterate)
+__global__ void k_pcgm_fold(int n3, double* __restrict__ x, float* __restrict__ d32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    x[i] += (double)d32[i];
+    d32[i] = 0.f;
+  }
+}
+
+// FP64 true residual r = b - y (y = K x with the FP64 values) into the FP32 r:
+// stop when ||r||/||b|| < tol, else gamma = (D r).r and the loop resumes with
+// its direction.
+__global__ void __launch_bounds__(kPcgThreads) k_pcgm_true(int n3, const double* __restrict__ b,
+                                                           const double* __restrict__ y,
+                                                           const float* __restrict__ dinv32, float* __restrict__ r32,
+                                                           double* __restrict__ partial, PcgState* st) {
+  __shared__ double sh[32];
+  double rr = 0, zr = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    const double ri = b[i] - y[i];
+    const float rv = (float)ri;
+    r32[i] = rv;
+    rr += ri * ri;
+    zr += (double)(dinv32[i] * rv) * (double)rv;
+  }
+  const double s1 = block_sum(rr, sh), s2 = block_sum(zr, sh);
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
+  if (!last_block(&st->counter)) return;
+  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
+  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  if (threadIdx.x == 0) {
+    const int it = st->it;
+    st->err = sqrt(tr) / st->bnorm;
+    st->need = 0;
+    if (st->err < st->tol) {
+      st->done = 1; st->iterations = it;
+    } else if (it + 1 >= st->max_it) {
+      st->done = 1; st->iterations = st->max_it; st->status = MSG_ERR_NOT_CONVERGED;
+    } else {
+      st->zr = tz;
+      st->it = it + 1;
+      st->err_ref = st->err;
+      st->done = 0;
     }
     st->counter = 0;
   }
@@ -437,49 +567,6 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const do
   const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
   if (threadIdx.x == 0) {
     st->err = sqrt(tr) / st->bnorm;
-    if (st->mixed && (st->err < st->tol || st->err < st->delta * st->err_ref)) {
-      // pause for an FP64 true residual (zr keeps the gamma of this iteration's start)
-      st->need = 1; st->done = 1; st->rr = tz;
-    } else if (st->err < st->tol) {
-      st->done = 1; st->iterations = it;
-    } else if (it + 1 >= st->max_it) {
-      st->done = 1; st->iterations = st->max_it; st->status = MSG_ERR_NOT_CONVERGED;
-    } else {
-      st->beta = tz / st->zr;
-      st->zr = tz;
-      st->it = it + 1;
-    }
-    st->counter = 0;
-  }
-}
-
-// Mixed precision: r = b - y (y = K x with the FP64 values), the true
-// relative residual decides convergence; otherwise the recursive residual is
-// replaced, the search direction kept (beta = gamma_true / gamma_start) and the
-// loop resumes.
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_true_resid(int n_rows, const double* __restrict__ b,
-                                                                const double* __restrict__ y,
-                                                                const double* __restrict__ dinv,
-                                                                double* __restrict__ r, double* __restrict__ partial,
-                                                                PcgState* st) {
-  __shared__ double sh[32];
-  double rr = 0, zr = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
-    const double ri = b[i] - y[i];
-    r[i] = ri;
-    rr += ri * ri;
-    zr += dinv[i] * ri * ri;
-  }
-  double s1 = block_sum(rr, sh);
-  double s2 = block_sum(zr, sh);
-  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
-  if (!last_block(&st->counter)) return;
-  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
-  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
-  if (threadIdx.x == 0) {
-    const int it = st->it;
-    st->err = sqrt(tr) / st->bnorm;
-    st->need = 0;
     if (st->err < st->tol) {
       st->done = 1; st->iterations = it;
     } else if (it + 1 >= st->max_it) {
@@ -488,8 +575,6 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_true_resid(int n_rows, cons
       st->beta = tz / st->zr;
       st->zr = tz;
       st->it = it + 1;
-      st->err_ref = st->err;
-      st->done = 0;
     }
     st->counter = 0;
   }
@@ -560,51 +645,50 @@ int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* 
   return MSG_OK;
 }
 
-// The loop's SpMV launch (shape chosen by size and value precision). Mixed:
-// the direction pass (FP64 p and its FP32 copy p32) and the FP32 product.
-static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float* v32, bool mixed, double* dv,
-                                double* rv, double* p0, double* p1, double* qv, double* pa, PcgState* st,
-                                cudaStream_t stream, float* p32 = nullptr, int grid_v = 0) {
+// The FP64 loop's direction + SpMV launch (shape chosen by size).
+static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, double* dv, double* rv, double* p0,
+                                double* p1, double* qv, double* pa, PcgState* st, cudaStream_t stream) {
   const int nr = m->n_nodes;
   const int ns = m->pat.n_slices;
   const bool small = ns < ctx->sm_count * 32;  // fewer slices than 32 warps per SM: 4 warps per slice
   const int64_t* sp = m->d_slice_ptr.as<int64_t>();
   const int* cl = m->d_col.as<int>();
-  const int gs = ns, gl = (ns + 7) / 8;
-  // FP64 values stream through with evict-first loads (measured faster at every
-  // size); FP32 values of matrices up to ~60 % of L2 stay there across iterations
-  const size_t vbytes = (size_t)m->pat.n_slots * 32 * 9 * (mixed ? 4 : 8);
-  const bool strm = !mixed || vbytes > (size_t)76 << 20;
-#define MSG_SPMV(V, S, W, STREAM, grid, vals)                                                                       \
-  k_pcg_dir_spmv_rows<V, S, W, STREAM><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, vals, dv, rv, p0, p1, qv, pa, \
-                                                                        st)
-#define MSG_SPMV32(S, W, STREAM, U, grid)                                                                        \
-  k_pcg_spmv32<S, W, STREAM, U><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, p0, p1, qv, pa, st)
-  if (mixed) {
-    k_pcg_dir32<<<grid_v, kPcgThreads, 0, stream>>>(nr, dv, rv, p0, p1, p32, st);
-    // large matrices: slots per group (4 or 8) and slices per CTA (8 or 4) by the
-    // "spmv32_shape" option (0: 4 / 8, 1: 8 / 8, 2: 4 / 4, 3: 8 / 4)
-    const int shape = ctx->spmv32_shape;
-    const int g4 = (ns + 3) / 4;
-    if (small) {
-      if (strm) MSG_SPMV32(1, 4, true, 4, gs); else MSG_SPMV32(1, 4, false, 4, gs);
-    } else if (shape == 1) {
-      if (strm) MSG_SPMV32(8, 1, true, 8, gl); else MSG_SPMV32(8, 1, false, 8, gl);
-    } else if (shape == 2) {
-      if (strm) MSG_SPMV32(4, 1, true, 4, g4); else MSG_SPMV32(4, 1, false, 4, g4);
-    } else if (shape == 3) {
-      if (strm) MSG_SPMV32(4, 1, true, 8, g4); else MSG_SPMV32(4, 1, false, 8, g4);
-    } else {
-      if (strm) MSG_SPMV32(8, 1, true, 4, gl); else MSG_SPMV32(8, 1, false, 4, gl);
-    }
-  } else {
-    if (small) {
-      if (strm) MSG_SPMV(double, 1, 4, true, gs, v64); else MSG_SPMV(double, 1, 4, false, gs, v64);
-    } else {
-      if (strm) MSG_SPMV(double, 8, 1, true, gl, v64); else MSG_SPMV(double, 8, 1, false, gl, v64);
-    }
-  }
-#undef MSG_SPMV
+  // FP64 values stream through with evict-first loads (measured faster at every size)
+  if (small)
+    k_pcg_dir_spmv_rows<double, 1, 4, true><<<ns, 128, 0, stream>>>(nr, ns, sp, cl, v64, dv, rv, p0, p1, qv, pa, st);
+  else
+    k_pcg_dir_spmv_rows<double, 8, 1, true><<<(ns + 7) / 8, 256, 0, stream>>>(nr, ns, sp, cl, v64, dv, rv, p0, p1, qv,
+                                                                              pa, st);
+}
+
+// The mixed loop's FP32 SpMV launch: small matrices one slice per CTA with 4
+// warps; large ones by the "spmv32_shape" option (slots per group / slices per
+// CTA: 0: 4 / 8, 1: 8 / 8, 2: 4 / 4, 3: 8 / 4). FP32 values of matrices up to
+// ~60 % of L2 stay there across iterations, larger ones stream (evict-first).
+static void launch_pcgm_spmv(Context* ctx, const Mesh* m, const float* v32, const float* p32, const float* r32,
+                             const float* dinv32, float* q32, double* pa, PcgState* st, cudaStream_t stream) {
+  const int nr = m->n_nodes;
+  const int ns = m->pat.n_slices;
+  const bool small = ns < ctx->sm_count * 32;
+  const int64_t* sp = m->d_slice_ptr.as<int64_t>();
+  const int* cl = m->d_col.as<int>();
+  const bool strm = (size_t)m->pat.n_slots * 32 * 9 * 4 > (size_t)76 << 20;
+  const int shape = ctx->spmv32_shape;
+#define MSG_SPMV32(S, W, U)                                                                                       \
+  do {                                                                                                           \
+    const int grid = (ns + S - 1) / S;                                                                           \
+    if (strm)                                                                                                    \
+      k_pcgm_spmv<S, W, true, U><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, r32, dinv32, q32, pa, \
+                                                                  st);                                           \
+    else                                                                                                         \
+      k_pcgm_spmv<S, W, false, U><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, r32, dinv32, q32,    \
+                                                                   pa, st);                                      \
+  } while (0)
+  if (small) MSG_SPMV32(1, 4, 4);
+  else if (shape == 1) MSG_SPMV32(8, 1, 8);
+  else if (shape == 2) MSG_SPMV32(4, 1, 4);
+  else if (shape == 3) MSG_SPMV32(4, 1, 8);
+  else MSG_SPMV32(8, 1, 4);
 #undef MSG_SPMV32
 }
 
@@ -612,48 +696,59 @@ static void launch_pcg_dir_spmv(Context* ctx, const Mesh* m, double* v64, float*
 // captured once per matrix as a CUDA graph of `chunk` iterations; the host
 // launches the graph and reads back the state flags after each chunk.
 // Kernels after convergence return immediately, so the recorded iteration
-// count is exact. Mixed precision: the loop's SpMV reads FP32 values; when it
-// pauses (need), y = K x with the FP64 values and k_pcg_true_resid replace the
+// count is exact. Mixed precision: the FP32 loop (k_pcgm_*); when it pauses
+// (need), x += d, y = K x with the FP64 values and k_pcgm_true replace the
 // recursive residual (or end the solve on the true residual).
 int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, int max_it, double tol, int* iterations,
                      double* rel_res, int* status, bool mixed) {
   Mesh* m = A->mesh;
   const int nr = m->n_nodes;
   const int n = 3 * nr;
+  cudaStream_t s = ctx->stream;
   MSG_TRY(context_resources(ctx));
   if (!A->d_r.ptr) {
     MSG_TRY(A->d_r.alloc(ctx, sizeof(double) * n));
     MSG_TRY(A->d_p0.alloc(ctx, sizeof(double) * n));
     MSG_TRY(A->d_p1.alloc(ctx, sizeof(double) * n));
     MSG_TRY(A->d_q.alloc(ctx, sizeof(double) * n));
-    // partials: one per SpMV CTA (slice) or two per update CTA
-    MSG_TRY(A->d_partial.alloc(ctx, sizeof(double) * std::max<size_t>(2 * 4096, m->pat.n_slices)));
+    // partials: one per FP64 SpMV CTA (slice), three per FP32 SpMV CTA or two per update CTA
+    MSG_TRY(A->d_partial.alloc(ctx, sizeof(double) * std::max<size_t>(2 * 4096, 3 * (size_t)m->pat.n_slices)));
     MSG_TRY(A->d_state.alloc(ctx, sizeof(PcgState)));
-    MSG_CUDA(ctx, cudaMemsetAsync(A->d_state.ptr, 0, sizeof(PcgState), ctx->stream));
+    MSG_CUDA(ctx, cudaMemsetAsync(A->d_state.ptr, 0, sizeof(PcgState), s));
   }
   if (mixed && !A->d_val32.ptr) {
     const size_t nv = (size_t)m->pat.n_slots * 32 * 9;
     MSG_TRY(A->d_val32.alloc(ctx, sizeof(float) * std::max<size_t>(1, nv)));
-    MSG_TRY(A->d_tmp.alloc(ctx, sizeof(double) * n));
-    MSG_TRY(A->d_tmp2.alloc(ctx, sizeof(float) * n));  // FP32 copy of the search direction
-    k_to_f32<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(nv, A->d_val.as<double>(), A->d_val32.as<float>());
+    MSG_TRY(A->d_tmp.alloc(ctx, sizeof(double) * n));   // y = K x of the true residual
+    MSG_TRY(A->d_tmp2.alloc(ctx, sizeof(float) * n));   // p (FP32)
+    MSG_TRY(A->d_m32.alloc(ctx, sizeof(float) * 4 * (size_t)n));
+    k_to_f32<<<ctx->sm_count * 8, 256, 0, s>>>(nv, A->d_val.as<double>(), A->d_val32.as<float>());
     count_launch(ctx);
   }
   PcgState* st = A->d_state.as<PcgState>();
   const int grid_v = std::min(4096, std::max(1, std::min((n + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 8)));
-
-  k_pcg_init<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, d_b, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
-                                                      A->d_p0.as<double>(), A->d_p1.as<double>(),
-                                                      A->d_partial.as<double>(), st);
+  double* pa = A->d_partial.as<double>();
+  float *p32 = nullptr, *r32 = nullptr, *q32 = nullptr, *d32 = nullptr, *dinv32 = nullptr;
+  if (mixed) {
+    p32 = A->d_tmp2.as<float>();
+    r32 = A->d_m32.as<float>();
+    q32 = r32 + n;
+    d32 = q32 + n;
+    dinv32 = d32 + n;
+    k_pcgm_init<<<grid_v, kPcgThreads, 0, s>>>(n, d_b, A->d_dinv.as<double>(), d_x, r32, p32, d32, dinv32, pa, st);
+  } else {
+    k_pcg_init<<<grid_v, kPcgThreads, 0, s>>>(nr, d_b, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
+                                              A->d_p0.as<double>(), A->d_p1.as<double>(), pa, st);
+  }
   count_launch(ctx);
   // tol, max_it and the mixed-precision settings into the state (after init so the counter reset does not race)
   {
     const int mx = mixed ? 1 : 0;
     const double delta = ctx->reliable_delta;
-    MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &tol, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    MSG_CUDA(ctx, cudaMemcpyAsync(&st->max_it, &max_it, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    MSG_CUDA(ctx, cudaMemcpyAsync(&st->mixed, &mx, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    MSG_CUDA(ctx, cudaMemcpyAsync(&st->delta, &delta, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->tol, &tol, sizeof(double), cudaMemcpyHostToDevice, s));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->max_it, &max_it, sizeof(int), cudaMemcpyHostToDevice, s));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->mixed, &mx, sizeof(int), cudaMemcpyHostToDevice, s));
+    MSG_CUDA(ctx, cudaMemcpyAsync(&st->delta, &delta, sizeof(double), cudaMemcpyHostToDevice, s));
     // the pageable copies above are staged before they return
   }
   const int chunk = 8;
@@ -661,17 +756,20 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
   if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x || A->graph_mixed != graph_kind) {
     if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
     cudaGraph_t g;
-    MSG_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    MSG_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
-      launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), mixed ? A->d_val32.as<float>() : nullptr, mixed,
-                          A->d_dinv.as<double>(), A->d_r.as<double>(), A->d_p0.as<double>(), A->d_p1.as<double>(),
-                          A->d_q.as<double>(), A->d_partial.as<double>(), st, ctx->stream,
-                          mixed ? A->d_tmp2.as<float>() : nullptr, grid_v);
-      k_pcg_update<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
-                                                            A->d_p0.as<double>(), A->d_p1.as<double>(),
-                                                            A->d_q.as<double>(), A->d_partial.as<double>(), st);
+      if (mixed) {
+        launch_pcgm_spmv(ctx, m, A->d_val32.as<float>(), p32, r32, dinv32, q32, pa, st, s);
+        k_pcgm_update<<<grid_v, kPcgThreads, 0, s>>>(n, dinv32, r32, p32, q32, d32, pa, st);
+      } else {
+        launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), A->d_dinv.as<double>(), A->d_r.as<double>(),
+                            A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(), pa, st, s);
+        k_pcg_update<<<grid_v, kPcgThreads, 0, s>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
+                                                    A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
+                                                    pa, st);
+      }
     }
-    MSG_CUDA(ctx, cudaStreamEndCapture(ctx->stream, &g));
+    MSG_CUDA(ctx, cudaStreamEndCapture(s, &g));
     cudaError_t e = cudaGraphInstantiate(&A->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphInstantiate");
@@ -679,35 +777,35 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     A->graph_x = d_x;
     A->graph_mixed = graph_kind;
   }
-  int* h = ctx->h_flags;  // pinned: done and need
-  const size_t off_done = offsetof(PcgState, done), off_need = offsetof(PcgState, need);
+  int* h = ctx->h_flags;  // pinned, mapped: done and need
+  int* dh = ctx->d_hflags;
   const int max_rounds = max_it / chunk + 2 * max_it + 4;  // chunks plus true-residual pauses
   for (int round = 0; round < max_rounds; ++round) {
-    cudaError_t e = cudaGraphLaunch(A->graph, ctx->stream);
+    cudaError_t e = cudaGraphLaunch(A->graph, s);
     if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphLaunch");
-    count_launch(ctx, (mixed ? 3 : 2) * chunk);
-    MSG_CUDA(ctx, cudaMemcpyAsync(h, reinterpret_cast<char*>(st) + off_done, sizeof(int), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-    MSG_CUDA(ctx, cudaMemcpyAsync(h + 1, reinterpret_cast<char*>(st) + off_need, sizeof(int),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (h[1]) {
-      // FP64 true residual r = b - K x (x in FP64), then resume or stop
-      k_bsr_spmv3<<<m->pat.n_slices, 96, 0, ctx->stream>>>(nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
-                                                            A->d_val.as<double>(), d_x, A->d_tmp.as<double>());
-      k_pcg_true_resid<<<grid_v, kPcgThreads, 0, ctx->stream>>>(nr, d_b, A->d_tmp.as<double>(),
-                                                                 A->d_dinv.as<double>(), A->d_r.as<double>(),
-                                                                 A->d_partial.as<double>(), st);
-      count_launch(ctx, 2);
-      MSG_CUDA(ctx, cudaMemcpyAsync(h, reinterpret_cast<char*>(st) + off_done, sizeof(int), cudaMemcpyDeviceToHost,
-                                    ctx->stream));
-      MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    count_launch(ctx, 2 * chunk);
+    MSG_TRY(publish_flags(ctx, &st->done, 2, h, dh, s));  // done, need
+    MSG_CUDA(ctx, cudaStreamSynchronize(s));
+    if (mixed && h[1]) {
+      // FP64 true residual r = b - K x (x += d in FP64 first), then resume or stop
+      k_pcgm_fold<<<grid_v, kPcgThreads, 0, s>>>(n, d_x, d32);
+      k_bsr_spmv3<<<m->pat.n_slices, 96, 0, s>>>(nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
+                                                  A->d_val.as<double>(), d_x, A->d_tmp.as<double>());
+      k_pcgm_true<<<grid_v, kPcgThreads, 0, s>>>(n, d_b, A->d_tmp.as<double>(), dinv32, r32, pa, st);
+      count_launch(ctx, 3);
+      MSG_TRY(publish_flags(ctx, &st->done, 1, h, dh, s));
+      MSG_CUDA(ctx, cudaStreamSynchronize(s));
     }
     if (h[0]) break;
   }
+  if (mixed) {  // a correction left by a solve that ended without a true residual
+    k_pcgm_fold<<<grid_v, kPcgThreads, 0, s>>>(n, d_x, d32);
+    count_launch(ctx);
+  }
+  MSG_CUDA(ctx, cudaGetLastError());
   PcgState hs;
-  MSG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost, ctx->stream));
-  MSG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  MSG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+  MSG_CUDA(ctx, cudaStreamSynchronize(s));
   if (iterations) *iterations = hs.iterations;
   if (rel_res) *rel_res = hs.err;
   if (status) *status = hs.done ? hs.status : MSG_ERR_NOT_CONVERGED;
@@ -784,8 +882,7 @@ extern "C" int MSG_PCG_SOLVE_NOALLOC(MSG_MAT A, const double* b_dev, double* x_d
   int done = 0;
   for (int it = 0; it < max_it + 8 && !done; it += 8) {
     for (int k = 0; k < 8; ++k) {
-      launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), nullptr, false, A->d_dinv.as<double>(), r, p0, p1, q,
-                          partial, st, s);
+      launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), A->d_dinv.as<double>(), r, p0, p1, q, partial, st, s);
       k_pcg_update<<<grid_v, kPcgThreads, 0, s>>>(nr, A->d_dinv.as<double>(), r, xn, p0, p1, q, partial, st);
     }
     count_launch(ctx, 16);

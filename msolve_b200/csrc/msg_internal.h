@@ -245,15 +245,15 @@ struct Mesh {
 
 struct PcgState {
   double zr, pq, rr, bnorm, alpha, beta, err;
-  int it, done, status, iterations, matvecs, max_it;
+  // need (mixed precision) follows done: the host reads both as one pair
+  int it, done, need, status, iterations, matvecs, max_it;
   double tol;
   unsigned int counter;
-  int pad;
-  // mixed precision (FP32 matrix values, FP64 vectors): the loop pauses (need = 1)
-  // when the recursive residual has dropped by delta since err_ref or below tol,
-  // and the host replaces it with the FP64 true residual
+  // mixed precision (FP32 matrix values and vectors, FP64 iterate): the loop
+  // pauses (need = 1) when the recursive residual has dropped by delta since
+  // err_ref or below tol, and the host replaces it with the FP64 true residual
   double delta, err_ref;
-  int mixed, need;
+  int mixed, pad;
 };
 
 struct Matrix {
@@ -264,6 +264,7 @@ struct Matrix {
   DevMem d_dinv;  // [n_nodes*3]
   // PCG workspace (node layout, 3 per node)
   DevMem d_r, d_p0, d_p1, d_q, d_partial, d_state, d_tmp, d_tmp2;
+  DevMem d_m32;  // mixed loop: FP32 r, q, d and D^-1 ([4][n_nodes*3]; p32 in d_tmp2)
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   int graph_mixed = 0;
