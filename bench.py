@@ -310,8 +310,12 @@ def single_leg(args, ctx):
     """One large static solve (64^3 Hexa8, E = 1, nu 0.3, z=0 clamped, unit top
     pressure): (a) the FP64 assembled drop-in (MSG_PCG_SOLVE) and (b) FP32 matrix
     values + FP64 refinement (MSG_PCG_SOLVE_MIXED), both to the relative
-    residual 1e-8, timed after one warm-up solve each; SpMV bytes per iteration
-    (FP64: 72 B values + 4 B column per 3x3 block + x and y vectors)."""
+    residual 1e-8, timed after one warm-up solve each. Algorithmic bytes per
+    iteration: the SpMV (72 B FP64 / 36 B FP32 values + 4 B column per 3x3
+    block, each vector read or written once) and the update pass (FP64: r, q, x,
+    p, D^-1 read, r, x written; mixed: p, q, r, d, D^-1 read, p, r, d written, in
+    FP32); hbm_frac = those bytes per iteration / time per iteration / the
+    measured copy bandwidth."""
     import torch
     import msolve_b200 as M
     n = args.single_n
@@ -334,10 +338,17 @@ def single_leg(args, ctx):
         b.synchronize()
         ms = a.elapsed_time(b)
         per_it = ms / max(1, s.iterations)
-        spmv_bytes = (72 if prec == "fp64" else 36) * info["nnzb"] + 4 * info["nnzb"] + 16 * 3 * model.n_nodes
+        # vectors of the SpMV pass: FP64 D^-1, r, p_old read and p_new, q written (the direction is formed in
+        # that pass); mixed p (gathered), r, D^-1 read and q written in FP32
+        spmv_bytes = ((72 if prec == "fp64" else 36) * info["nnzb"] + 4 * info["nnzb"]
+                      + (5 * 8 if prec == "fp64" else 4 * 4) * 3 * model.n_nodes)
+        update_bytes = (7 * 8 if prec == "fp64" else 8 * 4) * 3 * model.n_nodes
+        peak, peak_src = load_peaks()
         out[name] = {"ms": ms, "iterations": s.iterations, "rel_res": s.rel_res, "ms_per_iteration": per_it,
                      "dof_iterations_per_s": model.n_dofs * s.iterations / (ms / 1e3),
-                     "spmv_bytes_per_iteration": spmv_bytes}
+                     "spmv_bytes_per_iteration": spmv_bytes, "update_bytes_per_iteration": update_bytes,
+                     "hbm_frac": (spmv_bytes + update_bytes) / (per_it * 1e-3) / (peak * 1e9),
+                     "hbm_peak": f"{peak:g} GB/s ({peak_src})"}
     out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
     A.close()
     if not args.no_parity:

@@ -146,13 +146,34 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;  // valid in thread 0
 }
 
-// Whole-block sum of partial[i*stride + off], i < n, in a fixed order (thread
-// t takes i = t, t + blockDim, ...; then the block tree): called by every
-// thread of the last block, result valid in thread 0.
-__device__ __forceinline__ double sum_partials(const double* partial, int n, int stride, int off, double* sh) {
-  double s = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += __ldcg(partial + (size_t)i * stride + off);
-  return block_sum(s, sh);
+// Whole-block sums of the K interleaved partials partial[i*K + k], i < n, in a
+// fixed order (thread t adds i = t, t + blockDim, ... in turn; then the block
+// tree): called by every thread of the last block, results valid in thread 0.
+// The loads of four rounds are issued before their adds (the order of the adds
+// is unchanged), so the last block waits for one L2 round trip, not n / blockDim.
+template <int K>
+__device__ __forceinline__ void sum_partials(const double* partial, int n, double (&out)[K], double* sh) {
+  double s[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) s[k] = 0;
+  const int B = blockDim.x;
+  int i = threadIdx.x;
+  for (; i + 3 * B < n; i += 4 * B) {
+    double v[4][K];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[u][k] = __ldcg(partial + (size_t)(i + u * B) * K + k);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int k = 0; k < K; ++k) s[k] += v[u][k];
+  }
+  for (; i < n; i += B)
+#pragma unroll
+    for (int k = 0; k < K; ++k) s[k] += __ldcg(partial + (size_t)i * K + k);
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = block_sum(s[k], sh);
 }
 
 // Returns true in every thread of the last block to finish.
@@ -184,8 +205,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_init(int n_rows, const doub
   double s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
   if (!last_block(&st->counter)) return;
-  const double tb = sum_partials(partial, gridDim.x, 2, 0, sh);
-  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  double tt[2];
+  sum_partials<2>(partial, gridDim.x, tt, sh);
+  const double tb = tt[0], tz = tt[1];
   if (threadIdx.x == 0) {
     st->bnorm = sqrt(tb);
     st->zr = tz;
@@ -290,7 +312,9 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int 
   const double bs = block_sum(pq, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = bs;
   if (!last_block(&st->counter)) return;
-  const double t = sum_partials(partial, gridDim.x, 1, 0, sh);
+  double tt[1];
+  sum_partials<1>(partial, gridDim.x, tt, sh);
+  const double t = tt[0];
   if (threadIdx.x == 0) {
     st->pq = t;
     st->matvecs += 1;
@@ -321,6 +345,10 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int 
 // when ||r||/||b|| < tol in FP64). The direction is kept across the
 // replacement. Per iteration the vectors cost 36 bytes a DOF besides the
 // matrix (FP64 vectors and a separate direction pass: 100).
+// A warp owns one slice at a time; with kSpmvWarps = 1 the CTAs are persistent
+// (the grid fills the SMs once) and a warp strides over the slices, summing its
+// partials across them; with kSpmvWarps > 1 (small matrices) a CTA takes one
+// slice whose slots are dealt to its warps, whose sums meet in shared memory.
 template <int kS, int kSpmvWarps, bool kStream, int U = 4>
 __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcgm_spmv(int n_rows, int n_slices,
                                                               const int64_t* __restrict__ slice_ptr,
@@ -332,66 +360,77 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcgm_spmv(int n_rows, 
                                                               float* __restrict__ q32, double* __restrict__ partial,
                                                               PcgState* st) {
   __shared__ double sh[32];
-  __shared__ double ys[kS][kSpmvWarps][3][32];
+  __shared__ double ys[kSpmvWarps > 1 ? kS : 1][kSpmvWarps][3][32];
   if (st->done) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sl = warp / kSpmvWarps, w = warp % kSpmvWarps;
-  const int slice = blockIdx.x * kS + sl;
-  const int row = slice * 32 + lane;
-  const bool live = slice < n_slices && row < n_rows;
-  double y0 = 0, y1 = 0, y2 = 0;
-  auto fma9 = [&](const float (&a)[9], int cc) {
-    if (cc < 0) return;  // padding (its values are zero)
-    const float x0 = __ldg(p32 + 3 * cc), x1 = __ldg(p32 + 3 * cc + 1), x2 = __ldg(p32 + 3 * cc + 2);
-    y0 += (double)fmaf(a[2], x2, fmaf(a[1], x1, a[0] * x0));
-    y1 += (double)fmaf(a[5], x2, fmaf(a[4], x1, a[3] * x0));
-    y2 += (double)fmaf(a[8], x2, fmaf(a[7], x1, a[6] * x0));
-  };
-  if (live) {
-    const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
-    // U slots per group: 36 U bytes of values in flight per thread
-    int64_t s = s0 + w;
-    for (; s + (U - 1) * kSpmvWarps < s1; s += U * kSpmvWarps) {
-      int cu[U];
-      float a[U][9];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int64_t su = s + u * kSpmvWarps;
-        cu[u] = __ldg(col + su * 32 + lane);
-        const float* vu = val + su * 9 * 32 + lane;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) a[u][k] = kStream ? __ldcs(vu + k * 32) : __ldg(vu + k * 32);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) fma9(a[u], cu[u]);
-    }
-    for (; s < s1; s += kSpmvWarps) {
-      const int c0 = __ldg(col + s * 32 + lane);
-      const float* v0 = val + s * 9 * 32 + lane;
-      float a0[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) a0[k] = kStream ? __ldcs(v0 + k * 32) : __ldg(v0 + k * 32);
-      fma9(a0, c0);
-    }
-  }
-  ys[sl][w][0][lane] = y0;
-  ys[sl][w][1][lane] = y1;
-  ys[sl][w][2][lane] = y2;
-  __syncthreads();
   double pq = 0, dq = 0, qdq = 0;
-  if (w == 0 && live) {
+  const int stride = kSpmvWarps > 1 ? n_slices : gridDim.x * kS;
+  for (int slice = blockIdx.x * kS + sl; slice < n_slices || (kSpmvWarps > 1 && slice == blockIdx.x * kS + sl);
+       slice += stride) {
+    const int row = slice * 32 + lane;
+    const bool live = slice < n_slices && row < n_rows;
+    double y0 = 0, y1 = 0, y2 = 0;
+    auto fma9 = [&](const float (&a)[9], int cc) {
+      if (cc < 0) return;  // padding (its values are zero)
+      const float x0 = __ldg(p32 + 3 * cc), x1 = __ldg(p32 + 3 * cc + 1), x2 = __ldg(p32 + 3 * cc + 2);
+      y0 += (double)fmaf(a[2], x2, fmaf(a[1], x1, a[0] * x0));
+      y1 += (double)fmaf(a[5], x2, fmaf(a[4], x1, a[3] * x0));
+      y2 += (double)fmaf(a[8], x2, fmaf(a[7], x1, a[6] * x0));
+    };
+    if (live) {
+      const int64_t s0 = slice_ptr[slice], s1 = slice_ptr[slice + 1];
+      // U slots per group: 36 U bytes of values in flight per thread
+      int64_t s = s0 + w;
+      for (; s + (U - 1) * kSpmvWarps < s1; s += U * kSpmvWarps) {
+        int cu[U];
+        float a[U][9];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double t = ys[sl][0][c][lane];
+        for (int u = 0; u < U; ++u) {
+          const int64_t su = s + u * kSpmvWarps;
+          cu[u] = __ldg(col + su * 32 + lane);
+          const float* vu = val + su * 9 * 32 + lane;
 #pragma unroll
-      for (int ww = 1; ww < kSpmvWarps; ++ww) t += ys[sl][ww][c][lane];
-      const int i = 3 * row + c;
-      const float qf = (float)t, dv = dinv32[i];
-      q32[i] = qf;
-      pq += (double)p32[i] * (double)qf;
-      dq += (double)(dv * r32[i]) * (double)qf;
-      qdq += (double)(dv * qf) * (double)qf;
+          for (int k = 0; k < 9; ++k) a[u][k] = kStream ? __ldcs(vu + k * 32) : __ldg(vu + k * 32);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) fma9(a[u], cu[u]);
+      }
+      for (; s < s1; s += kSpmvWarps) {
+        const int c0 = __ldg(col + s * 32 + lane);
+        const float* v0 = val + s * 9 * 32 + lane;
+        float a0[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) a0[k] = kStream ? __ldcs(v0 + k * 32) : __ldg(v0 + k * 32);
+        fma9(a0, c0);
+      }
     }
+    double yc[3] = {y0, y1, y2};
+    if constexpr (kSpmvWarps > 1) {
+      ys[sl][w][0][lane] = y0;
+      ys[sl][w][1][lane] = y1;
+      ys[sl][w][2][lane] = y2;
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double t = ys[sl][0][c][lane];
+#pragma unroll
+        for (int ww = 1; ww < kSpmvWarps; ++ww) t += ys[sl][ww][c][lane];
+        yc[c] = t;
+      }
+    }
+    if (w == 0 && live) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int i = 3 * row + c;
+        const float qf = (float)yc[c], dv = dinv32[i];
+        q32[i] = qf;
+        pq += (double)p32[i] * (double)qf;
+        dq += (double)(dv * r32[i]) * (double)qf;
+        qdq += (double)(dv * qf) * (double)qf;
+      }
+    }
+    if constexpr (kSpmvWarps > 1) break;
   }
   const double b0 = block_sum(pq, sh), b1 = block_sum(dq, sh), b2 = block_sum(qdq, sh);
   if (threadIdx.x == 0) {
@@ -400,9 +439,9 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcgm_spmv(int n_rows, 
     partial[3 * blockIdx.x + 2] = b2;
   }
   if (!last_block(&st->counter)) return;
-  const double t = sum_partials(partial, gridDim.x, 3, 0, sh);
-  const double tdq = sum_partials(partial, gridDim.x, 3, 1, sh);
-  const double tqdq = sum_partials(partial, gridDim.x, 3, 2, sh);
+  double tt[3];
+  sum_partials<3>(partial, gridDim.x, tt, sh);
+  const double t = tt[0], tdq = tt[1], tqdq = tt[2];
   if (threadIdx.x == 0) {
     st->pq = t;
     st->matvecs += 1;
@@ -418,6 +457,8 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcgm_spmv(int n_rows, 
   }
 }
 
+// The vectors start at 16-byte boundaries: four components a thread at a
+// time (float4), the n3 % 4 tail one at a time.
 __global__ void __launch_bounds__(kPcgThreads) k_pcgm_update(int n3, const float* __restrict__ dinv32,
                                                              float* __restrict__ r32, float* __restrict__ p32,
                                                              const float* __restrict__ q32, float* __restrict__ d32,
@@ -426,21 +467,36 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcgm_update(int n3, const float
   if (st->done) return;
   const float al = (float)st->alpha, be = (float)st->beta;
   double zr = 0, rr = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
-    const float pv = p32[i];
-    const float rv = fmaf(-al, q32[i], r32[i]);
-    const float zv = dinv32[i] * rv;
-    d32[i] = fmaf(al, pv, d32[i]);
-    p32[i] = fmaf(be, pv, zv);
-    r32[i] = rv;
-    zr += (double)zv * (double)rv;
-    rr += (double)rv * (double)rv;
+  auto step = [&](float pv, float qv, float rv, float dv, float dd, float& pn, float& rn, float& dn) {
+    rn = fmaf(-al, qv, rv);
+    const float zv = dv * rn;
+    dn = fmaf(al, pv, dd);
+    pn = fmaf(be, pv, zv);
+    zr += (double)zv * (double)rn;
+    rr += (double)rn * (double)rn;
+  };
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  const int n4 = n3 >> 2;
+  for (int i = tid; i < n4; i += nt) {
+    const float4 p = reinterpret_cast<const float4*>(p32)[i], q = reinterpret_cast<const float4*>(q32)[i];
+    const float4 r = reinterpret_cast<const float4*>(r32)[i], dv = reinterpret_cast<const float4*>(dinv32)[i];
+    const float4 d = reinterpret_cast<const float4*>(d32)[i];
+    float4 pn, rn, dn;
+    step(p.x, q.x, r.x, dv.x, d.x, pn.x, rn.x, dn.x);
+    step(p.y, q.y, r.y, dv.y, d.y, pn.y, rn.y, dn.y);
+    step(p.z, q.z, r.z, dv.z, d.z, pn.z, rn.z, dn.z);
+    step(p.w, q.w, r.w, dv.w, d.w, pn.w, rn.w, dn.w);
+    reinterpret_cast<float4*>(p32)[i] = pn;
+    reinterpret_cast<float4*>(r32)[i] = rn;
+    reinterpret_cast<float4*>(d32)[i] = dn;
   }
+  for (int i = 4 * n4 + tid; i < n3; i += nt) step(p32[i], q32[i], r32[i], dinv32[i], d32[i], p32[i], r32[i], d32[i]);
   const double s1 = block_sum(rr, sh), s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
   if (!last_block(&st->counter)) return;
-  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
-  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  double tt[2];
+  sum_partials<2>(partial, gridDim.x, tt, sh);
+  const double tr = tt[0], tz = tt[1];
   if (threadIdx.x == 0) {
     const int it = st->it;
     st->err = sqrt(tr) / st->bnorm;
@@ -480,8 +536,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcgm_init(int n3, const double*
   const double s1 = block_sum(bb, sh), s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
   if (!last_block(&st->counter)) return;
-  const double tb = sum_partials(partial, gridDim.x, 2, 0, sh);
-  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  double tt[2];
+  sum_partials<2>(partial, gridDim.x, tt, sh);
+  const double tb = tt[0], tz = tt[1];
   if (threadIdx.x == 0) {
     st->bnorm = sqrt(tb);
     st->zr = tz;
@@ -520,8 +577,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcgm_true(int n3, const double*
   const double s1 = block_sum(rr, sh), s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
   if (!last_block(&st->counter)) return;
-  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
-  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  double tt[2];
+  sum_partials<2>(partial, gridDim.x, tt, sh);
+  const double tr = tt[0], tz = tt[1];
   if (threadIdx.x == 0) {
     const int it = st->it;
     st->err = sqrt(tr) / st->bnorm;
@@ -552,7 +610,22 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const do
   const double alpha = st->alpha;
   const double* __restrict__ pnew = (it & 1) ? p0 : p1;
   double rr = 0, zr = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n_rows; i += gridDim.x * blockDim.x) {
+  // two components a thread at a time (double2; the vectors start at 16-byte boundaries)
+  const int n3 = 3 * n_rows, n2 = n3 >> 1;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  for (int i = tid; i < n2; i += nt) {
+    const double2 rv = reinterpret_cast<const double2*>(r)[i], qv = reinterpret_cast<const double2*>(q)[i];
+    const double2 xv = reinterpret_cast<const double2*>(x)[i], pv = reinterpret_cast<const double2*>(pnew)[i];
+    const double2 dv = reinterpret_cast<const double2*>(dinv)[i];
+    const double r0 = rv.x - alpha * qv.x, r1 = rv.y - alpha * qv.y;
+    reinterpret_cast<double2*>(r)[i] = make_double2(r0, r1);
+    reinterpret_cast<double2*>(x)[i] = make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y);
+    rr += r0 * r0;
+    zr += dv.x * r0 * r0;
+    rr += r1 * r1;
+    zr += dv.y * r1 * r1;
+  }
+  for (int i = 2 * n2 + tid; i < n3; i += nt) {
     const double ri = r[i] - alpha * q[i];
     r[i] = ri;
     x[i] = x[i] + alpha * pnew[i];
@@ -563,8 +636,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n_rows, const do
   double s2 = block_sum(zr, sh);
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1; partial[2 * blockIdx.x + 1] = s2; }
   if (!last_block(&st->counter)) return;
-  const double tr = sum_partials(partial, gridDim.x, 2, 0, sh);
-  const double tz = sum_partials(partial, gridDim.x, 2, 1, sh);
+  double tt[2];
+  sum_partials<2>(partial, gridDim.x, tt, sh);
+  const double tr = tt[0], tz = tt[1];
   if (threadIdx.x == 0) {
     st->err = sqrt(tr) / st->bnorm;
     if (st->err < st->tol) {
@@ -674,9 +748,16 @@ static void launch_pcgm_spmv(Context* ctx, const Mesh* m, const float* v32, cons
   const int* cl = m->d_col.as<int>();
   const bool strm = (size_t)m->pat.n_slots * 32 * 9 * 4 > (size_t)76 << 20;
   const int shape = ctx->spmv32_shape;
+  // persistent grid (W = 1): the resident CTAs of every SM once
+  auto fill = [&](const void* k, int threads, int n_ctas) {
+    int occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, 0) != cudaSuccess || occ < 1) occ = 1;
+    return std::max(1, std::min(n_ctas, ctx->sm_count * occ));
+  };
 #define MSG_SPMV32(S, W, U)                                                                                       \
   do {                                                                                                           \
-    const int grid = (ns + S - 1) / S;                                                                           \
+    const int grid = W > 1 ? (ns + S - 1) / S                                                                    \
+                           : fill((const void*)k_pcgm_spmv<S, W, true, U>, 32 * S * W, (ns + S - 1) / S);        \
     if (strm)                                                                                                    \
       k_pcgm_spmv<S, W, true, U><<<grid, 32 * S * W, 0, stream>>>(nr, ns, sp, cl, v32, p32, r32, dinv32, q32, pa, \
                                                                   st);                                           \
@@ -721,20 +802,23 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     MSG_TRY(A->d_val32.alloc(ctx, sizeof(float) * std::max<size_t>(1, nv)));
     MSG_TRY(A->d_tmp.alloc(ctx, sizeof(double) * n));   // y = K x of the true residual
     MSG_TRY(A->d_tmp2.alloc(ctx, sizeof(float) * n));   // p (FP32)
-    MSG_TRY(A->d_m32.alloc(ctx, sizeof(float) * 4 * (size_t)n));
+    MSG_TRY(A->d_m32.alloc(ctx, sizeof(float) * 4 * (((size_t)n + 31) / 32 * 32)));
     k_to_f32<<<ctx->sm_count * 8, 256, 0, s>>>(nv, A->d_val.as<double>(), A->d_val32.as<float>());
     count_launch(ctx);
   }
   PcgState* st = A->d_state.as<PcgState>();
   const int grid_v = std::min(4096, std::max(1, std::min((n + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 8)));
+  // the update passes: float4 (mixed) or double2 (FP64) a thread, at most 4 CTAs an SM
+  const int grid_u = std::max(1, std::min((n / (mixed ? 4 : 2) + kPcgThreads - 1) / kPcgThreads, ctx->sm_count * 4));
   double* pa = A->d_partial.as<double>();
   float *p32 = nullptr, *r32 = nullptr, *q32 = nullptr, *d32 = nullptr, *dinv32 = nullptr;
   if (mixed) {
+    const size_t n32 = ((size_t)n + 31) / 32 * 32;  // 128-byte aligned vectors
     p32 = A->d_tmp2.as<float>();
     r32 = A->d_m32.as<float>();
-    q32 = r32 + n;
-    d32 = q32 + n;
-    dinv32 = d32 + n;
+    q32 = r32 + n32;
+    d32 = q32 + n32;
+    dinv32 = d32 + n32;
     k_pcgm_init<<<grid_v, kPcgThreads, 0, s>>>(n, d_b, A->d_dinv.as<double>(), d_x, r32, p32, d32, dinv32, pa, st);
   } else {
     k_pcg_init<<<grid_v, kPcgThreads, 0, s>>>(nr, d_b, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
@@ -760,11 +844,11 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
     for (int k = 0; k < chunk; ++k) {
       if (mixed) {
         launch_pcgm_spmv(ctx, m, A->d_val32.as<float>(), p32, r32, dinv32, q32, pa, st, s);
-        k_pcgm_update<<<grid_v, kPcgThreads, 0, s>>>(n, dinv32, r32, p32, q32, d32, pa, st);
+        k_pcgm_update<<<grid_u, kPcgThreads, 0, s>>>(n, dinv32, r32, p32, q32, d32, pa, st);
       } else {
         launch_pcg_dir_spmv(ctx, m, A->d_val.as<double>(), A->d_dinv.as<double>(), A->d_r.as<double>(),
                             A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(), pa, st, s);
-        k_pcg_update<<<grid_v, kPcgThreads, 0, s>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
+        k_pcg_update<<<grid_u, kPcgThreads, 0, s>>>(nr, A->d_dinv.as<double>(), A->d_r.as<double>(), d_x,
                                                     A->d_p0.as<double>(), A->d_p1.as<double>(), A->d_q.as<double>(),
                                                     pa, st);
       }
