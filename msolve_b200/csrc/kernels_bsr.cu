@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int 
 // partials across them; with kSpmvWarps > 1 (small matrices) a CTA takes one
 // slice whose slots are dealt to its warps, whose sums meet in shared memory.
 template <int kS, int kSpmvWarps, bool kStream, int U = 4>
-__global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcgm_spmv(int n_rows, int n_slices,
+__global__ void __launch_bounds__(32 * kS * kSpmvWarps, kSpmvWarps > 1 ? 1 : (U > 4 ? 3 : 4)) k_pcgm_spmv(int n_rows, int n_slices,
                                                               const int64_t* __restrict__ slice_ptr,
                                                               const int* __restrict__ col,
                                                               const float* __restrict__ val,
