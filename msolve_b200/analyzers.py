@@ -589,10 +589,13 @@ class RaggedMonteCarloBatch:
     coefficient provider and its random-number rows; Solve() runs the
     realization loop of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
     (MonteCarloAnalyzerWithStochasticMaterial.cs:232-296) for all of them in the
-    same launches (mixed-precision Jacobi-PCG, FP64 true residual below
-    `tolerance`). Results per system, in the order added: Solutions [R][n_dofs]
-    (if keep_solutions), TipValues [R], Iterations [R], Residuals [R]. A
-    system's results do not depend on the other systems in the batch."""
+    same launches (mixed-precision PCG, FP64 true residual below `tolerance`;
+    with the context's multigrid option on, each system whose mesh has lattice
+    numbering is preconditioned by the V-cycle of its cube lattice, the others
+    by the diagonal). Results per system, in the order added: Solutions
+    [R][n_dofs] (if keep_solutions), TipValues [R], Iterations [R], Residuals
+    [R]. A system's results do not depend on the other systems in the batch.
+    The meshes are uploaded once, in add(); Solve() may be called again."""
 
     def __init__(self, ctx, max_iterations=20000, tolerance=1e-8):
         self.ctx, self.max_iterations, self.tolerance = ctx, max_iterations, tolerance

@@ -4380,15 +4380,14 @@ struct GmgPrecondImpl {
   BlockSys B;
   Scal s0;
   DevMem zero;
-  DevMem own[kWorkSlots];
 };
 
 }  // namespace
 
 int gmg_precond_create(Context* ctx, Mesh* lat, double nu, const MSG_KL* kl, const double* d_xi, int R, int Rp,
-                       bool own_buffers, void** out) {
+                       DevMem* own, void** out) {
   std::unique_ptr<GmgPrecondImpl> P(new GmgPrecondImpl());
-  MSG_TRY(block_setup(ctx, lat, nu, 1.0, 1.0, 0.0, R, Rp, &P->B, own_buffers ? P->own : nullptr));
+  MSG_TRY(block_setup(ctx, lat, nu, 1.0, 1.0, 0.0, R, Rp, &P->B, own));
   if (!P->B.gmg)
     return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "the lattice does not coarsen (or multigrid is off)");
   KLDevice kd;
@@ -4406,11 +4405,20 @@ int gmg_precond_create(Context* ctx, Mesh* lat, double nu, const MSG_KL* kl, con
 int gmg_precond_apply(Context* ctx, void* handle, const float* r_node, float* z_node, cudaStream_t st) {
   GmgPrecondImpl* P = static_cast<GmgPrecondImpl*>(handle);
   BlockSys& B = P->B;
-  k_node_to_lattice<<<B.L.n_int, 256, 0, st>>>(B.L.n_int, B.Rp, B.interior, r_node, B.r32.as<float>());
+  if (r_node) k_node_to_lattice<<<B.L.n_int, 256, 0, st>>>(B.L.n_int, B.Rp, B.interior, r_node, B.r32.as<float>());
   gmg_vcycle(&B, P->s0, true, st);
-  k_lattice_to_node<<<B.L.n_int, 256, 0, st>>>(B.L.n_int, B.Rp, B.interior, B.qB.as<float>(), z_node);
-  count_launch(ctx, 2 + gmg_launches(&B) - 3);  // the iteration's launches but beta, the direction pass and alpha
+  if (z_node) k_lattice_to_node<<<B.L.n_int, 256, 0, st>>>(B.L.n_int, B.Rp, B.interior, B.qB.as<float>(), z_node);
+  // the iteration's launches but beta, the direction pass and alpha
+  count_launch(ctx, (r_node ? 1 : 0) + (z_node ? 1 : 0) + gmg_launches(&B) - 3);
   return MSG_OK;
+}
+
+void gmg_precond_buffers(void* handle, float** r_lat, float** z_lat, const int** node_to_lattice, int* Rp) {
+  GmgPrecondImpl* P = static_cast<GmgPrecondImpl*>(handle);
+  *r_lat = P->B.r32.as<float>();
+  *z_lat = P->B.qB.as<float>();
+  *node_to_lattice = P->B.interior;
+  *Rp = P->B.Rp;
 }
 
 void gmg_precond_destroy(void* handle) { delete static_cast<GmgPrecondImpl*>(handle); }

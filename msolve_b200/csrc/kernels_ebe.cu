@@ -79,7 +79,11 @@ struct RgSys {
   double* part;                  // [kRgParts][n_blk][Rp]
   double* part_u;                // [2][n_blk_u][Rp]: (D r).r and r.r of the update pass (z.r, r.r: ebe_mg_solve)
   int kind;                      // ebe_mg_solve: 1 multigrid V-cycle, 0 diagonal preconditioner
-  float* z;                      // ebe_mg_solve: [n_nodes * 3][Rp] preconditioned residual
+  float* z;                      // ebe_mg_solve: preconditioned residual ([n_nodes * 3][Rp], or lattice layout)
+  // V-cycle systems: the lattice's r buffer and the padded lattice index of
+  // each node; z then is the lattice's z buffer, indexed the same way
+  float* rl;
+  const int* lmap;
 };
 struct RgItem {
   int sys, blk, rb, G;  // nodes blk * 64 .., realizations rb .. rb + 32 G - 1
@@ -255,7 +259,7 @@ __device__ __forceinline__ void ebe_rows64(int n, int Rp, int rb, const int* __r
 
 // q = K p (FP32, constrained components 0) and the partials p.q, (D r).q, q.D.q.
 template <int G>
-__device__ __forceinline__ void rg_apply_item(const RgSys& S, int blk, int rb, double* sh) {
+__device__ __forceinline__ void rg_apply_item(const RgSys& S, int blk, int rb, double* sh, bool pq_only) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int Rp = S.Rp;
   // p.q (alpha) in FP64; (D r).q and q.D.q, which only enter beta's estimate, in
@@ -279,10 +283,12 @@ __device__ __forceinline__ void rg_apply_item(const RgSys& S, int blk, int rb, d
         const size_t o = ((size_t)n * 3 + c) * Rp + rb + 32 * g + lane;
         const float v = ((mk >> c) & 1u) ? 0.f : y[g][c];
         S.q[o] = v;
-        const float dv = S.dinv[o];
         pq[g] += (double)S.p[o] * (double)v;
-        drq[g] = fmaf(dv * S.r[o], v, drq[g]);
-        dqd[g] = fmaf(dv * v, v, dqd[g]);
+        if (!pq_only) {
+          const float dv = S.dinv[o];
+          drq[g] = fmaf(dv * S.r[o], v, drq[g]);
+          dqd[g] = fmaf(dv * v, v, dqd[g]);
+        }
       }
   }
   // one value at a time: three arrays of G live across one barrier spill under
@@ -290,27 +296,31 @@ __device__ __forceinline__ void rg_apply_item(const RgSys& S, int blk, int rb, d
 #pragma unroll
   for (int g = 0; g < G; ++g) {
     rg_block_partial(pq[g], sh, rg_part(S, kPq, blk, rb + 32 * g));
-    rg_block_partial((double)drq[g], sh, rg_part(S, kDrq, blk, rb + 32 * g));
-    rg_block_partial((double)dqd[g], sh, rg_part(S, kDqd, blk, rb + 32 * g));
+    if (!pq_only) {
+      rg_block_partial((double)drq[g], sh, rg_part(S, kDrq, blk, rb + 32 * g));
+      rg_block_partial((double)dqd[g], sh, rg_part(S, kDqd, blk, rb + 32 * g));
+    }
   }
 }
 
 // Every G in one kernel at 128 registers a thread (2 CTAs an SM): each
 // variant gets registers for many gathers in flight. Compiled alone, G = 4
 // takes 80 registers (3 CTAs an SM) and runs 24 % slower at 32^3 x 512.
+// pq_only (the standard PCG of ebe_mg_solve): p.q alone, without the partials
+// of beta's expansion and their reads of r and D^-1.
 __global__ void __launch_bounds__(32 * kEbeWarps, 2) k_rg_apply(const RgSys* __restrict__ Sys,
                                                             const RgItem* __restrict__ items, int n_items,
-                                                            const int* __restrict__ gact) {
+                                                            const int* __restrict__ gact, int pq_only) {
   __shared__ double sh[kEbeWarps * 32];
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const RgItem I = items[it];
     const RgSys S = Sys[I.sys];
     if (!rg_item_active(gact, S.goff, I.rb, I.G)) continue;
     switch (I.G) {
-      case 8: rg_apply_item<8>(S, I.blk, I.rb, sh); break;
-      case 4: rg_apply_item<4>(S, I.blk, I.rb, sh); break;
-      case 2: rg_apply_item<2>(S, I.blk, I.rb, sh); break;
-      default: rg_apply_item<1>(S, I.blk, I.rb, sh);
+      case 8: rg_apply_item<8>(S, I.blk, I.rb, sh, pq_only != 0); break;
+      case 4: rg_apply_item<4>(S, I.blk, I.rb, sh, pq_only != 0); break;
+      case 2: rg_apply_item<2>(S, I.blk, I.rb, sh, pq_only != 0); break;
+      default: rg_apply_item<1>(S, I.blk, I.rb, sh, pq_only != 0);
     }
   }
 }
@@ -675,6 +685,7 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_update(const RgSys* __res
         const float rv = fmaf(-al, S.q[o], S.r[o]);
         S.d[o] = fmaf(al, S.p[o], S.d[o]);
         S.r[o] = rv;
+        if (S.lmap) S.rl[((size_t)__ldg(S.lmap + n) * 3 + c) * Rp + col + lane] = rv;  // the V-cycle's input
         rr += (double)rv * (double)rv;
       }
     rg_block_partial(rr, sh, S.part_u + ((size_t)1 * S.n_blk_u + I.blk) * Rp + col);
@@ -698,7 +709,8 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_zr(const RgSys* __restric
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
-        zr += (double)S.z[o] * (double)S.r[o];
+        const size_t oz = S.lmap ? ((size_t)__ldg(S.lmap + n) * 3 + c) * Rp + col + lane : o;
+        zr += (double)S.z[oz] * (double)S.r[o];
       }
     rg_block_partial(zr, sh, S.part_u + (size_t)I.blk * Rp + col);
   }
@@ -720,7 +732,8 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_dir(const RgSys* __restri
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
-        S.p[o] = fmaf(be, S.p[o], S.z[o]);
+        const size_t oz = S.lmap ? ((size_t)__ldg(S.lmap + n) * 3 + c) * Rp + col + lane : o;
+        S.p[o] = fmaf(be, S.p[o], S.z[oz]);
       }
   }
 }
@@ -1123,7 +1136,7 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaMemsetAsync(s.flags, 0, 2 * sizeof(int), st);
   for (int k = 0; k < kEbeCheck; ++k) {
-    k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s.gact);
+    k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, dI, n_items, s.gact, 0);
     k_rg_scalar<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, k > 0, tol2, delta2, max_it);
     k_rg_update<<<g_update, 32 * kEbeWarps, 0, st>>>(dS, dIu, n_items_u, s);
   }
@@ -1228,7 +1241,8 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   auto carve_all = [&](Carver& c) {
     for (int i = 0; i < S; ++i) {
       rg_carve(in[i], bufs[i], c);
-      zs[i] = c.take<float>(3 * (size_t)in[i].m->n_nodes * bufs[i].Rp);
+      // z of a V-cycle system is the lattice's own buffer
+      zs[i] = c.take<float>(use_vcycle[i] ? 1 : 3 * (size_t)in[i].m->n_nodes * bufs[i].Rp);
     }
     d_sys = c.take<RgSys>(S);
     d_items = c.take<RgItem>(items.size());
@@ -1244,6 +1258,36 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   Carver c;
   c.base = static_cast<unsigned char*>(arena);
   carve_all(c);
+  // preconditioners: the V-cycle of each system's cube lattice (lattice buffers
+  // of their own when several systems hold one), E of every realization on the
+  // lattice's elements; r and z of such a system live in the lattice's buffers
+  int n_vc = 0;
+  for (int i = 0; i < S; ++i) n_vc += use_vcycle[i] ? 1 : 0;
+  std::vector<void*> P(S, nullptr);
+  struct PGuard {
+    std::vector<void*>& p;
+    ~PGuard() {
+      for (void* q : p)
+        if (q) gmg_precond_destroy(q);
+    }
+  } pguard{P};
+  if (n_vc > 1)
+    while ((int)ctx->vc_pool.size() < n_vc) ctx->vc_pool.push_back(new DevMem[kWorkSlots]);
+  for (int i = 0, k = 0; i < S; ++i)
+    if (use_vcycle[i]) {
+      DevMem* own = n_vc > 1 ? ctx->vc_pool[k++] : nullptr;
+      MSG_TRY(gmg_precond_create(ctx, lats[i], in[i].nu, in[i].kl, in[i].d_xi, in[i].R, bufs[i].Rp, own, &P[i]));
+      float *rl = nullptr, *zl = nullptr;
+      const int* lmap = nullptr;
+      int lrp = 0;
+      gmg_precond_buffers(P[i], &rl, &zl, &lmap, &lrp);
+      if (lrp != bufs[i].Rp)
+        return set_error(ctx, MSG_ERR_UNKNOWN, "element-by-element batch: lattice layout of %d realizations, not %d",
+                         lrp, bufs[i].Rp);
+      sys[i].rl = rl;
+      sys[i].z = zl;
+      sys[i].lmap = lmap;
+    }
   for (int i = 0; i < S; ++i) {
     RgBuf& B = bufs[i];
     MSG_TRY(rg_setup(ctx, in[i], B, static_cast<double*>(k300), d_status));
@@ -1271,7 +1315,7 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
     Y.part = B.part;
     Y.part_u = B.part_u;
     Y.kind = use_vcycle[i] ? 1 : 0;
-    Y.z = zs[i];
+    if (!use_vcycle[i]) Y.z = zs[i];
   }
   MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys) * S, cudaMemcpyHostToDevice, st));
   MSG_CUDA(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(RgItem) * items.size(), cudaMemcpyHostToDevice, st));
@@ -1292,22 +1336,6 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   s.flags = s.gact + Rtot / 32;
   MSG_CUDA(ctx, cudaMemcpyAsync(s.rsys, rsys.data(), sizeof(int) * Rtot, cudaMemcpyHostToDevice, st));
   MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
-  // preconditioners: the V-cycle of each system's cube lattice (lattice buffers
-  // of their own when several systems hold one), E of every realization on the
-  // lattice's elements
-  int n_vc = 0;
-  for (int i = 0; i < S; ++i) n_vc += use_vcycle[i] ? 1 : 0;
-  std::vector<void*> P(S, nullptr);
-  struct PGuard {
-    std::vector<void*>& p;
-    ~PGuard() {
-      for (void* q : p)
-        if (q) gmg_precond_destroy(q);
-    }
-  } pguard{P};
-  for (int i = 0; i < S; ++i)
-    if (use_vcycle[i])
-      MSG_TRY(gmg_precond_create(ctx, lats[i], in[i].nu, in[i].kl, in[i].d_xi, in[i].R, bufs[i].Rp, n_vc > 1, &P[i]));
   const RgSys* dS = d_sys;
   const int n_groups = Rtot / 32, g_groups = (n_groups + kEbeWarps - 1) / kEbeWarps;
   const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
@@ -1319,10 +1347,13 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   const int g_apply = grid_of(occ_apply, n_items), g_resid = grid_of(occ_resid, n_items);
   const int g_fold = grid_of(occ_u, n_items), g_u = n_items_u;
   // z = M^-1 r of the systems in `which` (nullptr: all): V-cycles one system
-  // after another, the diagonal for all the others in one launch
-  auto precondition = [&](const std::vector<int>* which) -> int {
+  // after another, the diagonal for all the others in one launch. from_node:
+  // r of the V-cycle systems in node layout (the start and the true
+  // residuals); in the loop the update pass has written it to the lattice
+  auto precondition = [&](const std::vector<int>* which, bool from_node) -> int {
     for (int i = 0; i < S; ++i)
-      if (P[i] && (!which || (*which)[i])) MSG_TRY(gmg_precond_apply(ctx, P[i], bufs[i].r, zs[i], st));
+      if (P[i] && (!which || (*which)[i]))
+        MSG_TRY(gmg_precond_apply(ctx, P[i], from_node ? bufs[i].r : nullptr, nullptr, st));
     if (n_vc < S) {
       k_vc_jacobi_z<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
       count_launch(ctx);
@@ -1335,7 +1366,7 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
     count_launch(ctx);
   }
   MSG_CUDA(ctx, cudaMemsetAsync(s.gact, 0xff, sizeof(int) * n_groups, st));  // every group until the start
-  MSG_TRY(precondition(nullptr));
+  MSG_TRY(precondition(nullptr, true));
   k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
   for (int i = 0; i < S; ++i) k_vc_start<<<bufs[i].Rp / kEbeWarps, 32 * kEbeWarps, 0, st>>>(sys[i], in[i].R, s);
   k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
@@ -1350,10 +1381,10 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   MSG_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaMemsetAsync(s.flags, 0, 2 * sizeof(int), st);
   for (int k = 0; k < kChunk; ++k) {
-    k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s.gact);
+    k_rg_apply<<<g_apply, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s.gact, 1);
     k_vc_alpha<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s);
     k_vc_update<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
-    precondition(nullptr);
+    precondition(nullptr, false);
     k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     k_vc_beta<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol2, delta2, max_it);
     k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
@@ -1392,7 +1423,7 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
     MSG_CUDA(ctx, cudaMemsetAsync(s.flags + 1, 0, sizeof(int), st));
     k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s, 0);
     k_rg_resid64<<<g_resid, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s);
-    MSG_TRY(precondition(&req));
+    MSG_TRY(precondition(&req, true));
     k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     k_vc_true<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol, max_it);
     k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);

@@ -74,6 +74,8 @@ Context::~Context() {
     delete w;
     w = nullptr;
   }
+  for (DevMem* set : vc_pool) delete[] set;
+  vc_pool.clear();
   if (batch_graph) cudaGraphExecDestroy(batch_graph);
   for (auto& e : ev)
     if (e) cudaEventDestroy(e);

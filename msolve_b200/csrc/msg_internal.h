@@ -91,6 +91,10 @@ struct Context {
   // device; a batch reuses the previous batch's buffers when they are large
   // enough). Slots are owned by the call sites that use them.
   DevMem* work[kWorkSlots] = {nullptr};
+  // lattice buffer sets (kWorkSlots each) of the V-cycle preconditioners of an
+  // element-by-element batch with several of them: set k for the k-th such
+  // system, kept (and grown) across calls like the workspace slots
+  std::vector<DevMem*> vc_pool;
   // per-context host/driver resources reused by every batch (created lazily)
   int* h_flags = nullptr;           // 4 KB of pinned host memory, mapped into the device
   int* d_hflags = nullptr;          // the device's address of h_flags
@@ -359,11 +363,16 @@ int lattice_shadow(Context* ctx, Mesh* m, Mesh** out);
 // the KL field xi [R][n_terms] (on the lattice's element centroids), Rp a
 // multiple of 32. apply enqueues z = V(r) on st for node-layout FP32 vectors
 // [n_nodes * 3][Rp] (constrained components of r zero); graph-capturable.
-// own_buffers: lattice buffers of its own (several preconditioners at once)
-// instead of the context's workspace.
+// own: kWorkSlots lattice buffers for this preconditioner (several
+// preconditioners at once; not owned, kept by the caller across calls), or
+// nullptr for the context's workspace. r_node nullptr: r is already in the
+// lattice's r buffer; z_node nullptr: z stays in the lattice's z buffer.
 int gmg_precond_create(Context* ctx, Mesh* lattice, double nu, const MSG_KL* kl, const double* d_xi, int R, int Rp,
-                       bool own_buffers, void** out);
+                       DevMem* own, void** out);
 int gmg_precond_apply(Context* ctx, void* P, const float* r_node, float* z_node, cudaStream_t st);
+// The lattice's r and z buffers ((padded node * 3 + c) * Rp + realization), the
+// padded index of each mesh node and the buffers' Rp.
+void gmg_precond_buffers(void* P, float** r_lat, float** z_lat, const int** node_to_lattice, int* Rp);
 void gmg_precond_destroy(void* P);
 
 // One system of a batched element-by-element solve (kernels_ebe.cu): a mesh

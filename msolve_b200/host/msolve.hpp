@@ -508,8 +508,10 @@ class MonteCarloAnalyzerWithStochasticMaterial : public IAnalyzer {
 // MSG_MC_SOLVE_RAGGED call: each added analyzer's RandomNumbers are solved in
 // the batched mixed mode to the batch's tolerance, and its Solutions,
 // TipValues, Iterations and Residuals are filled as by its own Solve() on the
-// same loop (the same bits alone and in the batch). No reference counterpart:
-// the reference runs one analysis, one realization after another.
+// same loop (the same bits alone and in the batch; a system without lattice
+// numbering batched with systems that have one runs the V-cycle batch's
+// standard PCG with the diagonal, the same solution to rounding). No reference
+// counterpart: the reference runs one analysis, one realization after another.
 class RaggedMonteCarloBatch {
  public:
   explicit RaggedMonteCarloBatch(Context& ctx, double tolerance = 1e-8, int max_iterations = 20000)
