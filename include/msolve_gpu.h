@@ -336,8 +336,10 @@ typedef struct {
 } MSG_RAGGED_SYSTEM;
 /* The realization loop of MonteCarloAnalyzerWithStochasticMaterial.SolveNormal
  * (ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:232-296)
- * for several systems of uneven mesh size at once: every iteration of every
- * realization of every system runs in the same three persistent launches
+ * for several systems of uneven mesh size at once. Structured cube lattices go
+ * through the lattice loop of MSG_MC_SOLVE_BATCH (mixed mode, the same results
+ * as that call) unless the "ragged_lattice_loop" option is 0; for the other
+ * systems every iteration of every realization runs in the same three persistent launches
  * (element-by-element FP32 operator over each element's stiffness at E = 1
  * scaled by E per realization, per-realization scalars, fused vector update),
  * eight iterations to a CUDA graph launch, Jacobi-preconditioned CG (the
@@ -473,12 +475,16 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * three-term split; systems without a mass term), "element_batch" (mixed
  * Monte Carlo batches on meshes that are not cube lattices: 1, default, every
  * realization at once through an element-by-element operator over each
- * element's stiffness at E = 1 (FP32 Jacobi-PCG, FP64 iterate and true
+ * element's stiffness at E = 1 (FP32 PCG, FP64 iterate and true
  * residuals); 0: realization by realization through the assembled FP32-value
  * PCG of MSG_PCG_SOLVE_MIXED), "element_groups" (launch shape of that
  * element-by-element operator: realization groups of 32 per CTA, each element
  * row block loaded once for all of them; 0, default: the largest of 4, 2, 1
- * dividing the padded group count; 8 is allowed; results are identical).
+ * dividing the padded group count; 8 is allowed; results are identical),
+ * "ragged_lattice_loop" (MSG_MC_SOLVE_RAGGED: 1, default, structured cube
+ * lattices of the batch are solved by the lattice loop of
+ * MSG_MC_SOLVE_BATCH, one after another, the other systems together in the
+ * element-by-element batch; 0: every system in the element-by-element batch).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

@@ -736,6 +736,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
     ctx->element_groups = (int)value;
     return MSG_OK;
   }
+  if (!std::strcmp(key, "ragged_lattice_loop") && (value == 0 || value == 1)) {
+    ctx->ragged_lattice_loop = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "multigrid_fused_coarse") && (value == 0 || value == 1)) {
     ctx->mg_fused_coarse = (int)value;
     return MSG_OK;
@@ -777,6 +781,7 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"spmv32_shape", (double)ctx->spmv32_shape},
               {"element_batch", (double)ctx->element_batch},
               {"element_groups", (double)ctx->element_groups},
+              {"ragged_lattice_loop", (double)ctx->ragged_lattice_loop},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
               {"serve_priority", (double)ctx->serve_priority},
@@ -1294,54 +1299,91 @@ int MSG_MC_SOLVE_RAGGED(MSG_CTX ctx, int n_systems, const MSG_RAGGED_SYSTEM* sys
   if (n_systems <= 0 || !systems || max_it <= 0 || !(tol > 0))
     return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "ragged batch: invalid arguments");
   MSG_TRY(context_resources(ctx));
-  cudaEvent_t e0 = ctx->ev[8], e1 = ctx->ev[9];
+  MSG_TRY(pipe_flush(ctx));
+  cudaEvent_t e0 = ctx->ev[12], e1 = ctx->ev[13];
   cudaEventRecord(e0, ctx->stream);
-  std::vector<RgInput> in(n_systems);
-  std::vector<std::unique_ptr<DevMem>> staging;
-  auto stage = [&](size_t bytes, double** out) -> int {
-    staging.emplace_back(new DevMem());
-    MSG_TRY(staging.back()->alloc(ctx, bytes));
-    *out = staging.back()->as<double>();
-    return MSG_OK;
-  };
   for (int i = 0; i < n_systems; ++i) {
     const MSG_RAGGED_SYSTEM& y = systems[i];
     Mesh* m = y.mesh;
     if (!m || m->ctx != ctx || !y.kl || !y.xi || !y.b || y.R <= 0 || y.kl->n_terms <= 0)
       return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "ragged batch: invalid system %d", i);
-    const size_t xb = sizeof(double) * (size_t)y.R * y.kl->n_terms, bb = sizeof(double) * std::max(1, m->n_dofs);
-    double *dxi = nullptr, *db = nullptr;
-    MSG_TRY(stage(xb, &dxi));
-    MSG_TRY(stage(bb, &db));
-    MSG_CUDA(ctx, cudaMemcpyAsync(dxi, y.xi, xb, cudaMemcpyHostToDevice, ctx->stream));
+    if (y.tip && y.tip_dof >= m->n_dofs) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "tip_dof out of range");
+  }
+  // every system's xi, b and X staged in one workspace slot (kept across calls)
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  std::vector<size_t> off(3 * (size_t)n_systems);
+  size_t total = 0;
+  for (int i = 0; i < n_systems; ++i) {
+    const MSG_RAGGED_SYSTEM& y = systems[i];
+    const size_t nd = (size_t)std::max(1, y.mesh->n_dofs);
+    off[3 * i] = total;
+    total += up(sizeof(double) * (size_t)y.R * y.kl->n_terms);
+    off[3 * i + 1] = total;
+    total += up(sizeof(double) * nd);
+    off[3 * i + 2] = total;
+    if (y.X) total += up(sizeof(double) * (size_t)y.R * nd);
+  }
+  void* stage = nullptr;
+  MSG_TRY(workspace(ctx, 37, total, &stage));
+  unsigned char* base = static_cast<unsigned char*>(stage);
+  std::vector<RgInput> in;  // the systems of the shared element-by-element batch
+  std::vector<int> lattice;  // cube lattices solved by the lattice loop
+  for (int i = 0; i < n_systems; ++i) {
+    const MSG_RAGGED_SYSTEM& y = systems[i];
+    Mesh* m = y.mesh;
+    double* dxi = reinterpret_cast<double*>(base + off[3 * i]);
+    double* db = reinterpret_cast<double*>(base + off[3 * i + 1]);
+    MSG_CUDA(ctx, cudaMemcpyAsync(dxi, y.xi, sizeof(double) * (size_t)y.R * y.kl->n_terms, cudaMemcpyHostToDevice,
+                                  ctx->stream));
     MSG_CUDA(ctx, cudaMemcpyAsync(db, y.b, sizeof(double) * (size_t)m->n_dofs, cudaMemcpyHostToDevice, ctx->stream));
-    RgInput& I = in[i];
+    if (ctx->ragged_lattice_loop && m->structured) {
+      lattice.push_back(i);
+      continue;
+    }
+    RgInput I;
     I.m = m;
     I.nu = y.nu;
     I.kl = y.kl;
     I.R = y.R;
     I.d_xi = dxi;
     I.d_b = db;
-    if (y.X) MSG_TRY(stage(sizeof(double) * (size_t)y.R * std::max(1, m->n_dofs), &I.d_X));
+    I.d_X = y.X ? reinterpret_cast<double*>(base + off[3 * i + 2]) : nullptr;
     I.h_tip = y.tip;
     I.tip_dof = y.tip ? y.tip_dof : -1;
     I.h_its = y.iterations;
     I.h_res = y.rel_res;
+    in.push_back(I);
   }
-  const int st = ebe_solve(ctx, in, max_it, tol);
-  if (st == MSG_OK || st == MSG_ERR_NOT_CONVERGED || st == MSG_ERR_BREAKDOWN) {
-    for (int i = 0; i < n_systems; ++i)
-      if (systems[i].X && in[i].d_X)
-        MSG_CUDA(ctx, cudaMemcpyAsync(systems[i].X, in[i].d_X,
-                                      sizeof(double) * (size_t)systems[i].R * systems[i].mesh->n_dofs,
-                                      cudaMemcpyDeviceToHost, ctx->stream));
+  // per-realization outcomes (not converged, breakdown) leave every other output complete
+  int worst = MSG_OK;
+  auto outcome = [&](int st) {
+    if (st != MSG_OK && st != MSG_ERR_NOT_CONVERGED && st != MSG_ERR_BREAKDOWN) return false;
+    if (worst == MSG_OK) worst = st;
+    return true;
+  };
+  for (int i : lattice) {
+    const MSG_RAGGED_SYSTEM& y = systems[i];
+    const int st = mc_batch(ctx, y.mesh, y.nu, y.kl, y.R, reinterpret_cast<double*>(base + off[3 * i]),
+                            reinterpret_cast<double*>(base + off[3 * i + 1]), MSG_MODE_MIXED_BATCHED, max_it, tol,
+                            y.tip ? y.tip_dof : -1, y.X ? reinterpret_cast<double*>(base + off[3 * i + 2]) : nullptr,
+                            y.tip, y.iterations, y.rel_res);
+    if (!outcome(st)) return st;
   }
+  if (!in.empty()) {
+    const int st = ebe_solve(ctx, in, max_it, tol);
+    if (!outcome(st)) return st;
+  }
+  for (int i = 0; i < n_systems; ++i)
+    if (systems[i].X)
+      MSG_CUDA(ctx, cudaMemcpyAsync(systems[i].X, base + off[3 * i + 2],
+                                    sizeof(double) * (size_t)systems[i].R * systems[i].mesh->n_dofs,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
   cudaEventRecord(e1, ctx->stream);
   cudaEventSynchronize(e1);
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   ctx->t_phase[4] = ms;
-  return st;
+  return worst;
 }
 
 int MSG_NEWMARK_BATCH(MSG_MESH m, double nu, const MSG_KL* kl, int R, const double* xi, const MSG_NEWMARK* nm,

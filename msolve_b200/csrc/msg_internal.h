@@ -85,6 +85,7 @@ struct Context {
   int spmv32_shape = 0;         // launch shape of the mixed assembled loop's FP32 SpMV (slots per group, slices per CTA)
   int element_batch = 1;        // mixed mode on non-lattice meshes: 1 batched element-by-element loop, 0 per realization
   int element_groups = 0;       // realization groups of 32 per CTA of the element-by-element FP32 operator (0 auto)
+  int ragged_lattice_loop = 1;  // ragged batches: cube lattices through the lattice loop (1) or the shared loop (0)
   int serve_persistent = 1;     // serving lanes: 1 persistent grids, 0 one CTA per work item
   int serve_priority = 0;       // serving lanes: 1 stream priority grows as the model shrinks, 0 all equal
   // Workspace kept across calls (allocation and cudaFree synchronise the
@@ -109,7 +110,7 @@ struct Context {
   };
   std::vector<CubeMatrix> cube_cache;
   std::mutex cube_mu;
-  cudaEvent_t ev[12] = {nullptr};   // timing events
+  cudaEvent_t ev[14] = {nullptr};   // timing events
   // pipelined Monte Carlo batches: the displacement copy to the host of one
   // call runs on copy_stream from output buffer pipe_next ^ 1 while the next
   // call computes into the other buffer

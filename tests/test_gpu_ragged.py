@@ -48,7 +48,17 @@ def oracle_solution(model, kl, xi_r, n):
     return xo, Cs
 
 
-def test_ragged_batch_matches_oracle(ctx):
+@pytest.fixture
+def lattice_loop(ctx, request):
+    """ragged_lattice_loop option: cube lattices through the lattice loop (1) or
+    the shared element-by-element batch (0)."""
+    ctx.set_option("ragged_lattice_loop", request.param)
+    yield request.param
+    ctx.set_option("ragged_lattice_loop", 1)
+
+
+@pytest.mark.parametrize("lattice_loop", [0, 1], indirect=True)
+def test_ragged_batch_matches_oracle(ctx, lattice_loop):
     syss = systems()
     res = solve(ctx, syss)
     for (model, kl, xi), r in zip(syss, res):
@@ -72,8 +82,9 @@ def multigrid(ctx, request):
     ctx.set_option("multigrid", 1)
 
 
+@pytest.mark.parametrize("lattice_loop", [0, 1], indirect=True)
 @pytest.mark.parametrize("multigrid", [0, 1], indirect=True)
-def test_system_alone_equals_the_mix(ctx, multigrid):
+def test_system_alone_equals_the_mix(ctx, multigrid, lattice_loop):
     """A system's arithmetic is independent of the other systems: each system
     solved alone gives the same bits as in the ragged mix. With the multigrid
     option on, the two even lattices (the distorted 4^3 and the 6^3) take the
@@ -99,7 +110,23 @@ def test_system_alone_equals_the_mix(ctx, multigrid):
     assert np.abs(one["Solutions"][0] - a).max() <= 1e-9 * np.abs(a).max()
 
 
-def test_lattice_systems_take_the_vcycle(ctx):
+def test_lattice_system_equals_its_own_batch_call(ctx):
+    """With the ragged_lattice_loop option on (default), a structured cube
+    lattice of a ragged batch is solved by the lattice loop of
+    MSG_MC_SOLVE_BATCH: the same bits as the analyzer's own mixed-mode call."""
+    model, kl, xi = systems()[1]
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=kl.n_terms,
+                                                    simulations=xi.shape[0], mode="mixed", tolerance=1e-10)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    r = solve(ctx, systems())[1]
+    for key, ref in (("Solutions", mc.Solutions), ("TipValues", mc.TipValues), ("Iterations", mc.Iterations),
+                     ("Residuals", mc.Residuals)):
+        assert np.array_equal(r[key], ref), key
+
+
+@pytest.mark.parametrize("lattice_loop", [0], indirect=True)
+def test_lattice_systems_take_the_vcycle(ctx, lattice_loop):
     """Two 8^3 systems, one a cube lattice and one with moved interior nodes:
     with the multigrid option each converges in a fraction of the Jacobi
     iterations, to the same 1e-10 residual and within 1e-8 of the Jacobi
