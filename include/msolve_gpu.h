@@ -384,9 +384,9 @@ typedef struct {
  * NewmarkDynamicAnalyzer.Solve, :280-315, for a stochastic material: E field
  * of realization r from xi[r] as in MSG_MC_SOLVE_BATCH). Every step solves the
  * effective system of all realizations with the mixed batched PCG to the FP64
- * true relative residual tol, warm-started from the previous displacement
- * (the reference restarts SolverPCG from zero; both stop on the same
- * criterion). Structured cube lattices only (MSG_ERR_NOT_STRUCTURED otherwise).
+ * true relative residual tol, started from the Newmark predictor of the new
+ * displacement (option "newmark_predictor"; 0: from the previous displacement;
+ * the reference restarts SolverPCG from zero; all stop on the same criterion). Structured cube lattices only (MSG_ERR_NOT_STRUCTURED otherwise).
  * xi [R][kl->n_terms]; f_static [n_dofs] static nodal loads added every step
  * (Model.AssignLoads) or NULL. Outputs (each may be NULL): tip_hist
  * [R][n_steps] displacement of DOF tip_dof after each step, U [R][n_dofs] final
@@ -481,7 +481,9 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * element-by-element operator: realization groups of 32 per CTA, each element
  * row block loaded once for all of them; 0, default: the largest of 4, 2, 1
  * dividing the padded group count; 8 is allowed; results are identical),
- * "ragged_lattice_loop" (MSG_MC_SOLVE_RAGGED: 1, default, structured cube
+ * "newmark_predictor" (MSG_NEWMARK_BATCH: 1, default, each step's solve
+ * starts from the Newmark predictor u + dt v + (1/2 - alpha) dt^2 a; 0: from
+ * the last displacement), "ragged_lattice_loop" (MSG_MC_SOLVE_RAGGED: 1, default, structured cube
  * lattices of the batch are solved by the lattice loop of
  * MSG_MC_SOLVE_BATCH, one after another, the other systems together in the
  * element-by-element batch; 0: every system in the element-by-element batch).

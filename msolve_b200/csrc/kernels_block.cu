@@ -2561,6 +2561,14 @@ __global__ void k_nm_post(int n_int, int Rp, const int* __restrict__ interior, c
   }
 }
 
+// start of a Newmark step's solve: the Newmark predictor x = u + dt v + (1/2 - alpha) dt^2 a
+// (elementwise over the whole batch layout; padding and constrained entries stay 0)
+__global__ void k_nm_predict(size_t n, const double* __restrict__ u, const double* __restrict__ v,
+                             const double* __restrict__ a, double cv, double ca, double* __restrict__ x) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = u[i] + cv * v[i] + ca * a[i];
+}
+
 // unit vector field: component dir = 1 at every interior node (batch layout)
 __global__ void k_unit_dir(int n_int, int Rp, const int* __restrict__ interior, int dir, double* __restrict__ e) {
   const size_t total = (size_t)n_int * Rp;
@@ -4117,8 +4125,15 @@ int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const do
                                                   rhs.as<double>());
     k_nm_rhs<<<ew, 256, 0, st>>>(L.n_int, Rp, B.interior, B.mask, d_f_dof ? fst.as<double>() : nullptr,
                                  fM.as<double>(), ag, rhs.as<double>());
-    // warm start from the last displacement
-    MSG_CUDA(ctx, cudaMemcpyAsync(B.x.ptr, u.ptr, sizeof(double) * nvec, cudaMemcpyDeviceToDevice, st));
+    // start from the Newmark predictor of the new displacement (newmark_predictor = 1),
+    // or from the last displacement
+    if (ctx->nm_predictor) {
+      k_nm_predict<<<ew, 256, 0, st>>>(nvec, u.as<double>(), v.as<double>(), a.as<double>(), dt,
+                                       (0.5 - nm.alpha) * dt * dt, B.x.as<double>());
+      count_launch(ctx);
+    } else {
+      MSG_CUDA(ctx, cudaMemcpyAsync(B.x.ptr, u.ptr, sizeof(double) * nvec, cudaMemcpyDeviceToDevice, st));
+    }
     count_launch(ctx, 4);
     // a few iterations per step: short graph chunks keep the host checks close
     status = block_solve(ctx, &B, rhs.as<double>(), true, true, max_it, tol, false, 4);

@@ -740,6 +740,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
     ctx->ragged_lattice_loop = (int)value;
     return MSG_OK;
   }
+  if (!std::strcmp(key, "newmark_predictor") && (value == 0 || value == 1)) {
+    ctx->nm_predictor = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "multigrid_fused_coarse") && (value == 0 || value == 1)) {
     ctx->mg_fused_coarse = (int)value;
     return MSG_OK;
@@ -782,6 +786,7 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"element_batch", (double)ctx->element_batch},
               {"element_groups", (double)ctx->element_groups},
               {"ragged_lattice_loop", (double)ctx->ragged_lattice_loop},
+              {"newmark_predictor", (double)ctx->nm_predictor},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
               {"serve_priority", (double)ctx->serve_priority},

@@ -86,6 +86,7 @@ struct Context {
   int element_batch = 1;        // mixed mode on non-lattice meshes: 1 batched element-by-element loop, 0 per realization
   int element_groups = 0;       // realization groups of 32 per CTA of the element-by-element FP32 operator (0 auto)
   int ragged_lattice_loop = 1;  // ragged batches: cube lattices through the lattice loop (1) or the shared loop (0)
+  int nm_predictor = 1;         // Newmark steps start from the Newmark predictor (1) or the last displacement (0)
   int serve_persistent = 1;     // serving lanes: 1 persistent grids, 0 one CTA per work item
   int serve_priority = 0;       // serving lanes: 1 stream priority grows as the model shrinks, 0 all equal
   // Workspace kept across calls (allocation and cudaFree synchronise the
