@@ -5,8 +5,10 @@ block of unit cubes (35,937 nodes, 104,544 free DOFs), z=0 face clamped,
 unit pressure on the top face (consistent weights), E_e = exp(sigma g(x_e))
 with a 50-term separable-exponential KL field (l = 0.2 * 32, sigma = 0.3),
 nu = 0.3, every realization solved to an FP64 true relative residual < tol
-(default 1e-10: the measured displacement error against an FP64 solve is then
-below 1e-8) with the matrix-free FP32 PCG + FP64 refinement path. Each step
+(default 1e-9, a decade inside the metric's 1e-8; the displacement error
+against FP64 oracle solves of a sample of the batch is measured every run and
+reported as rel_err_vs_oracle: about 3e-11) with the matrix-free FP32 PCG +
+FP64 refinement path. Each step
 draws a fresh xi table (seeded); state is ~4.6 GB per GPU, larger than L2.
 
 value  = realizations solved per second with xi / b / X resident in HBM
@@ -62,7 +64,7 @@ def parse():
     p.add_argument("--n", type=int, default=32)
     p.add_argument("--R", type=int, default=1024)
     p.add_argument("--terms", type=int, default=50)
-    p.add_argument("--tol", type=float, default=1e-10)
+    p.add_argument("--tol", type=float, default=1e-9)
     p.add_argument("--fp64-sample", type=int, default=8)
     p.add_argument("--cpu-sample", type=int, default=16,
                    help="realizations the in-arm CPU baseline (the oracle) solves")
@@ -326,8 +328,11 @@ def single_leg(args, ctx):
     out = {"workload": f"{n}^3 Hexa8 static solve, {model.n_dofs} free DOFs, {info['nnzb']} 3x3 blocks, "
                        f"Jacobi PCG to ||r||/||b|| < 1e-8", "n_dofs": model.n_dofs, "nnzb": info["nnzb"]}
     sols = {}
-    for name, prec in (("fp64", "fp64"), ("mixed", "mixed")):
-        s = M.SolverPCG(ctx, model, max_iterations=100000, tolerance=1e-8, precision=prec)
+    # the mixed variant stops on the FP64 true residual; run to 1e-8 (the
+    # configuration) it ends 1.1e-8 from the oracle on this block, so it is also
+    # run to 5e-9 (mixed_tol_5e-9), which ends inside 1e-8
+    for name, prec, tol in (("fp64", "fp64", 1e-8), ("mixed", "mixed", 1e-8), ("mixed_tol_5e-9", "mixed", 5e-9)):
+        s = M.SolverPCG(ctx, model, max_iterations=100000, tolerance=tol, precision=prec)
         s.matrix = A
         sols[name] = s.Solve().copy()
         a = torch.cuda.Event(enable_timing=True)
@@ -350,6 +355,7 @@ def single_leg(args, ctx):
                      "hbm_frac": (spmv_bytes + update_bytes) / (per_it * 1e-3) / (peak * 1e9),
                      "hbm_peak": f"{peak:g} GB/s ({peak_src})"}
     out["mixed_over_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    out["mixed_tol_5e-9_over_fp64"] = out["fp64"]["ms"] / out["mixed_tol_5e-9"]["ms"]
     A.close()
     if not args.no_parity:
         import oracle as O
@@ -359,7 +365,7 @@ def single_leg(args, ctx):
                                      max_it=100000)
         out["oracle"] = {"oracle": "FP64 CSR Jacobi-PCG restatement of SolverPCG to 1e-11",
                          "iterations": info["iterations"], "seconds": time.perf_counter() - t0}
-        for name in ("fp64", "mixed"):
+        for name in sols:
             out[name]["rel_err_vs_oracle"] = float(np.abs(sols[name] - xo).max() / np.abs(xo).max())
     return out
 
