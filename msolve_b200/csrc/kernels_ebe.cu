@@ -426,6 +426,13 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_rg_resid64(const RgSys* __re
     const RgItem I = items[it];
     if (!s.sreq[I.sys]) continue;  // the same for the whole CTA
     const RgSys S = Sys[I.sys];
+    if (I.G == 4) {  // four groups to an element-row load when all four run
+      const int grp = (S.goff + I.rb) / 32;
+      if (s.gact[grp] && s.gact[grp + 1] && s.gact[grp + 2] && s.gact[grp + 3]) {
+        rg_resid_groups<4>(S, I.blk, I.rb, sh);
+        continue;
+      }
+    }
     for (int g = 0; g < I.G; g += 2) {
       const int grp = (S.goff + I.rb) / 32 + g;
       const bool a0 = s.gact[grp] != 0, a1 = g + 1 < I.G && s.gact[grp + 1] != 0;
