@@ -3,9 +3,10 @@ oracle solves of the same inputs (the oracle restates SolverPCG and
 NewmarkDynamicAnalyzer; ISAAR.MSolve.Solvers/PCG/SolverPCG.cs:105-149,
 ISAAR.MSolve.Analyzers/NewmarkDynamicAnalyzer.cs:280-315).
 
-* Monte Carlo, 1024 realizations of the 32^3 block (50-term KL, sigma 0.3):
-  eight realizations spread over the batch within 1e-8 (max norm, relative to
-  the oracle's maximum) of oracle solves converged to 1e-12.
+* Monte Carlo, 1024 realizations of the 32^3 block (50-term KL, sigma 0.3),
+  each to the benchmark's FP64 true relative residual of 1e-9: eight
+  realizations spread over the batch within 1e-8 (max norm, relative to the
+  oracle's maximum) of oracle solves converged to 1e-12.
 * Single 64^3 static solve: the FP64 drop-in at the reference's stopping rule
   (1e-8) equals the oracle's PCG at the same rule to 1e-10 with the same
   iteration count (+-1); FP32 values + FP64 refinement to a 1e-10 relative
@@ -41,10 +42,10 @@ def test_mc_1024_realizations_32cube_against_oracle(ctx):
     kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 16)
     xi = np.random.default_rng(31).standard_normal((R, K))
     mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=K, simulations=R, mode="mixed",
-                                                    tolerance=1e-10)
+                                                    tolerance=1e-9)
     mc.RandomNumbers = xi
     mc.Solve()
-    assert (mc.Residuals < 1e-10).all()
+    assert (mc.Residuals < 1e-9).all()
     P = O.block_problem(n, K, 16)
     assert np.array_equal(P["b"], model.subdomains[0].RHS)
     rows = np.linspace(0, R - 1, 8).astype(int)
