@@ -1008,71 +1008,100 @@ static int rg_results(Context* ctx, const std::vector<RgInput>& in, const std::v
   return status;
 }
 
-int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol) {
-  NvtxRange range("msg: batched element-by-element solve");
-  if (in.empty() || max_it <= 0 || !(tol > 0))
-    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid arguments");
-  cudaStream_t st = ctx->stream;
-  const auto t_setup = std::chrono::steady_clock::now();
-  const int S = (int)in.size();
-  std::vector<RgBuf> bufs(S);
-  std::vector<RgSys> sys(S);
-  int Rtot = 0, max_ne = 0;
-  for (int i = 0; i < S; ++i) {
-    if (!in[i].m || in[i].m->ctx != ctx)
-      return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: system %d has no mesh of this context", i);
-    MSG_TRY(rg_plan(ctx, in[i], bufs[i]));
-    sys[i].goff = Rtot;
-    Rtot += bufs[i].Rp;
-    max_ne = std::max(max_ne, in[i].m->n_elems);
-  }
-  int G = 8;  // one G for the batch: the smallest of the systems' (each divides the next)
-  for (int i = 0; i < S; ++i) G = std::min(G, bufs[i].G);
-  for (int i = 0; i < S; ++i) bufs[i].G = G;
-  // work items: per system and node block, the realization ranges one after
-  // another (operator passes: 64 nodes and G groups; update: 256 nodes and one
-  // group), so that CTAs running at the same time cover whole rows
-  // [node * 3 + c][0 .. Rp) of the vectors
+// The device state of an element-by-element batch: each system's buffers
+// carved from one arena (workspace slot 34, kept by the context between calls;
+// slot 35: the packed element matrices of one system at a time), the system
+// table, the work items and the per-realization scalars.
+struct RgBatch {
+  int S = 0, Rtot = 0, n_items = 0, n_items_u = 0;
+  std::vector<RgBuf> bufs;
+  std::vector<RgSys> sys;
   std::vector<RgItem> items, items_u;
-  std::vector<int> rsys(Rtot);
-  for (int i = 0; i < S; ++i) {
-    const RgBuf& B = bufs[i];
-    for (int blk = 0; blk < B.n_blk; ++blk)
-      for (int rb = 0; rb < B.Rp; rb += 32 * B.G) items.push_back(RgItem{i, blk, rb, B.G});
-    for (int blk = 0; blk < B.n_blk_u; ++blk)
-      for (int rb = 0; rb < B.Rp; rb += 32) items_u.push_back(RgItem{i, blk, rb, 1});
-    for (int r = 0; r < B.Rp; ++r) rsys[sys[i].goff + r] = i;
-  }
-  const int n_items = (int)items.size(), n_items_u = (int)items_u.size();
-  // one arena for the batch, kept by the context between calls (workspace slot
-  // 34; slot 35: the packed element matrices of one system at a time)
-  const size_t scal_bytes = (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 3) * (size_t)Rtot +
-                            sizeof(int) * (S + Rtot / 32 + 2);
+  std::vector<int> rsys;
+  std::vector<float*> z;  // z [n_nodes * 3][Rp] of the systems that asked for one
   RgSys* d_sys = nullptr;
   RgItem *d_items = nullptr, *d_items_u = nullptr;
   unsigned char* scal_base = nullptr;
   int* d_status = nullptr;
+  double* k300 = nullptr;
+  RgScal s;
+};
+
+// Plan and carve a batch: per-system sizes (Rp a multiple of rp_multiple[i]),
+// one realization-group count G for all systems (the smallest of theirs; each
+// divides the next), the work items (per system and node block, the
+// realization ranges one after another: operator passes 64 nodes and G groups,
+// the update 256 nodes and one group, so that CTAs running at the same time
+// cover whole rows [node * 3 + c][0 .. Rp) of the vectors) and the arena, with
+// a z vector for each system with want_z[i].
+static int rg_batch_plan(Context* ctx, const std::vector<RgInput>& in, const std::vector<int>& rp_multiple,
+                         const std::vector<int>& want_z, RgBatch& b) {
+  const int S = (int)in.size();
+  b.S = S;
+  b.bufs.assign(S, RgBuf());
+  b.sys.assign(S, RgSys());
+  b.z.assign(S, nullptr);
+  b.Rtot = 0;
+  int max_ne = 0;
+  for (int i = 0; i < S; ++i) {
+    if (!in[i].m || in[i].m->ctx != ctx)
+      return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: system %d has no mesh of this context", i);
+    MSG_TRY(rg_plan(ctx, in[i], b.bufs[i], rp_multiple[i]));
+    b.sys[i].goff = b.Rtot;
+    b.Rtot += b.bufs[i].Rp;
+    max_ne = std::max(max_ne, in[i].m->n_elems);
+  }
+  int G = 8;
+  for (int i = 0; i < S; ++i) G = std::min(G, b.bufs[i].G);
+  for (int i = 0; i < S; ++i) b.bufs[i].G = G;
+  b.items.clear();
+  b.items_u.clear();
+  b.rsys.assign(b.Rtot, 0);
+  for (int i = 0; i < S; ++i) {
+    const RgBuf& B = b.bufs[i];
+    for (int blk = 0; blk < B.n_blk; ++blk)
+      for (int rb = 0; rb < B.Rp; rb += 32 * B.G) b.items.push_back(RgItem{i, blk, rb, B.G});
+    for (int blk = 0; blk < B.n_blk_u; ++blk)
+      for (int rb = 0; rb < B.Rp; rb += 32) b.items_u.push_back(RgItem{i, blk, rb, 1});
+    for (int r = 0; r < B.Rp; ++r) b.rsys[b.sys[i].goff + r] = i;
+  }
+  b.n_items = (int)b.items.size();
+  b.n_items_u = (int)b.items_u.size();
+  const size_t scal_bytes = (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 3) * (size_t)b.Rtot +
+                            sizeof(int) * (S + b.Rtot / 32 + 2);
   auto carve_all = [&](Carver& c) {
-    for (int i = 0; i < S; ++i) rg_carve(in[i], bufs[i], c);
-    d_sys = c.take<RgSys>(S);
-    d_items = c.take<RgItem>(items.size());
-    d_items_u = c.take<RgItem>(items_u.size());
-    scal_base = c.take<unsigned char>(scal_bytes);
-    d_status = c.take<int>(1);
+    for (int i = 0; i < S; ++i) {
+      rg_carve(in[i], b.bufs[i], c);
+      if (want_z[i]) b.z[i] = c.take<float>(3 * (size_t)in[i].m->n_nodes * b.bufs[i].Rp);
+    }
+    b.d_sys = c.take<RgSys>(S);
+    b.d_items = c.take<RgItem>(b.items.size());
+    b.d_items_u = c.take<RgItem>(b.items_u.size());
+    b.scal_base = c.take<unsigned char>(scal_bytes);
+    b.d_status = c.take<int>(1);
   };
   Carver count;
   carve_all(count);
   void *arena = nullptr, *k300 = nullptr;
   MSG_TRY(workspace(ctx, 34, count.off, &arena));
   MSG_TRY(workspace(ctx, 35, sizeof(double) * 300 * (size_t)max_ne, &k300));
+  b.k300 = static_cast<double*>(k300);
   Carver c;
   c.base = static_cast<unsigned char*>(arena);
   carve_all(c);
-  for (int i = 0; i < S; ++i) {
-    RgBuf& B = bufs[i];
-    MSG_TRY(rg_setup(ctx, in[i], B, static_cast<double*>(k300), d_status));
+  return MSG_OK;
+}
+
+// Per-system device setup (element matrices, E field, load, Jacobi diagonal),
+// the system table (fields a caller set before, z, rl and lmap, are kept), the
+// work items and the scalars' layout on the device.
+static int rg_batch_upload(Context* ctx, const std::vector<RgInput>& in, RgBatch& b) {
+  cudaStream_t st = ctx->stream;
+  for (int i = 0; i < b.S; ++i) {
+    RgBuf& B = b.bufs[i];
+    MSG_TRY(rg_setup(ctx, in[i], B, b.k300, b.d_status));
     Mesh* m = in[i].m;
-    RgSys& Y = sys[i];
+    RgSys& Y = b.sys[i];
     Y.n_nodes = m->n_nodes;
     Y.Rp = B.Rp;
     Y.n_blk = B.n_blk;
@@ -1094,13 +1123,16 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
     Y.dinv = B.dinv;
     Y.part = B.part;
     Y.part_u = B.part_u;
+    if (b.z[i]) Y.z = b.z[i];
   }
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys) * S, cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(RgItem) * items.size(), cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_items_u, items_u.data(), sizeof(RgItem) * items_u.size(), cudaMemcpyHostToDevice,
+  MSG_CUDA(ctx, cudaMemcpyAsync(b.d_sys, b.sys.data(), sizeof(RgSys) * b.S, cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(b.d_items, b.items.data(), sizeof(RgItem) * b.items.size(), cudaMemcpyHostToDevice,
                                 st));
-  RgScal s;
-  s.gamma = reinterpret_cast<double*>(scal_base);
+  MSG_CUDA(ctx, cudaMemcpyAsync(b.d_items_u, b.items_u.data(), sizeof(RgItem) * b.items_u.size(),
+                                cudaMemcpyHostToDevice, st));
+  const int Rtot = b.Rtot;
+  RgScal& s = b.s;
+  s.gamma = reinterpret_cast<double*>(b.scal_base);
   s.rr_ref = s.gamma + Rtot;
   s.bnorm = s.rr_ref + Rtot;
   s.res = s.bnorm + Rtot;
@@ -1110,10 +1142,27 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   s.its = s.done + Rtot;
   s.rsys = s.its + Rtot;
   s.sreq = s.rsys + Rtot;
-  s.gact = s.sreq + S;
+  s.gact = s.sreq + b.S;
   s.flags = s.gact + Rtot / 32;
-  MSG_CUDA(ctx, cudaMemcpyAsync(s.rsys, rsys.data(), sizeof(int) * Rtot, cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
+  MSG_CUDA(ctx, cudaMemcpyAsync(s.rsys, b.rsys.data(), sizeof(int) * Rtot, cudaMemcpyHostToDevice, st));
+  MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * b.S, st));
+  return MSG_OK;
+}
+
+int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, double tol) {
+  NvtxRange range("msg: batched element-by-element solve");
+  if (in.empty() || max_it <= 0 || !(tol > 0))
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: invalid arguments");
+  cudaStream_t st = ctx->stream;
+  const auto t_setup = std::chrono::steady_clock::now();
+  const int S = (int)in.size();
+  RgBatch b;
+  MSG_TRY(rg_batch_plan(ctx, in, std::vector<int>(S, 32), std::vector<int>(S, 0), b));
+  MSG_TRY(rg_batch_upload(ctx, in, b));
+  const std::vector<RgBuf>& bufs = b.bufs;
+  const std::vector<RgSys>& sys = b.sys;
+  const int Rtot = b.Rtot, n_items = b.n_items, n_items_u = b.n_items_u;
+  const RgScal s = b.s;
   for (int i = 0; i < S; ++i) {
     const dim3 g(bufs[i].n_blk, bufs[i].Rp / 32);
     k_rg_init<<<g, 32 * kEbeWarps, 0, st>>>(sys[i]);
@@ -1133,9 +1182,9 @@ int ebe_ragged_solve(Context* ctx, const std::vector<RgInput>& in, int max_it, d
   const int g_apply = grid_of(occ_apply, n_items), g_update = n_items_u;
   const int g_resid = grid_of(occ_resid, n_items), g_fold = grid_of(occ_update, n_items);
   const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
-  const RgSys* dS = d_sys;
-  const RgItem* dI = d_items;
-  const RgItem* dIu = d_items_u;
+  const RgSys* dS = b.d_sys;
+  const RgItem* dI = b.d_items;
+  const RgItem* dIu = b.d_items_u;
   const double delta2 = ctx->reliable_delta * ctx->reliable_delta, tol2 = 0.25 * tol * tol;
   // one chunk of kEbeCheck iterations, captured once as a CUDA graph
   cudaGraph_t graph = nullptr;
@@ -1209,62 +1258,20 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   const auto t_setup = std::chrono::steady_clock::now();
   const int S = (int)in.size();
   if (S > 1000) return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: more than 1000 systems");
-  std::vector<RgBuf> bufs(S);
-  std::vector<RgSys> sys(S);
   std::vector<Mesh*> lats(S, nullptr);
-  int Rtot = 0;
+  std::vector<int> rp_multiple(S), want_z(S);
   for (int i = 0; i < S; ++i) {
     if (!in[i].m || in[i].m->ctx != ctx)
       return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "element-by-element batch: system %d has no mesh of this context", i);
     if (use_vcycle[i]) MSG_TRY(lattice_shadow(ctx, in[i].m, &lats[i]));
-    // the packed level-0 operator of a V-cycle takes pairs of realization groups
-    MSG_TRY(rg_plan(ctx, in[i], bufs[i], use_vcycle[i] ? 64 : 32));
-    sys[i].goff = Rtot;
-    Rtot += bufs[i].Rp;
+    // the packed level-0 operator of a V-cycle takes pairs of realization groups;
+    // z of a V-cycle system is the lattice's own buffer
+    rp_multiple[i] = use_vcycle[i] ? 64 : 32;
+    want_z[i] = use_vcycle[i] ? 0 : 1;
   }
-  int G = 8;
-  for (int i = 0; i < S; ++i) G = std::min(G, bufs[i].G);
-  for (int i = 0; i < S; ++i) bufs[i].G = G;
-  std::vector<RgItem> items, items_u;
-  std::vector<int> rsys(Rtot);
-  for (int i = 0; i < S; ++i) {
-    const RgBuf& B = bufs[i];
-    for (int blk = 0; blk < B.n_blk; ++blk)
-      for (int rb = 0; rb < B.Rp; rb += 32 * B.G) items.push_back(RgItem{i, blk, rb, B.G});
-    for (int blk = 0; blk < B.n_blk_u; ++blk)
-      for (int rb = 0; rb < B.Rp; rb += 32) items_u.push_back(RgItem{i, blk, rb, 1});
-    for (int r = 0; r < B.Rp; ++r) rsys[sys[i].goff + r] = i;
-  }
-  const int n_items = (int)items.size(), n_items_u = (int)items_u.size();
-  const size_t scal_bytes = (sizeof(double) * 4 + sizeof(float) * 2 + sizeof(int) * 3) * (size_t)Rtot +
-                            sizeof(int) * (S + Rtot / 32 + 2);
-  RgSys* d_sys = nullptr;
-  RgItem *d_items = nullptr, *d_items_u = nullptr;
-  unsigned char* scal_base = nullptr;
-  int* d_status = nullptr;
-  std::vector<float*> zs(S, nullptr);
-  int max_ne = 0;
-  for (int i = 0; i < S; ++i) max_ne = std::max(max_ne, in[i].m->n_elems);
-  auto carve_all = [&](Carver& c) {
-    for (int i = 0; i < S; ++i) {
-      rg_carve(in[i], bufs[i], c);
-      // z of a V-cycle system is the lattice's own buffer
-      zs[i] = c.take<float>(use_vcycle[i] ? 1 : 3 * (size_t)in[i].m->n_nodes * bufs[i].Rp);
-    }
-    d_sys = c.take<RgSys>(S);
-    d_items = c.take<RgItem>(items.size());
-    d_items_u = c.take<RgItem>(items_u.size());
-    scal_base = c.take<unsigned char>(scal_bytes);
-    d_status = c.take<int>(1);
-  };
-  Carver count;
-  carve_all(count);
-  void *arena = nullptr, *k300 = nullptr;
-  MSG_TRY(workspace(ctx, 34, count.off, &arena));
-  MSG_TRY(workspace(ctx, 35, sizeof(double) * 300 * (size_t)max_ne, &k300));
-  Carver c;
-  c.base = static_cast<unsigned char*>(arena);
-  carve_all(c);
+  RgBatch b;
+  MSG_TRY(rg_batch_plan(ctx, in, rp_multiple, want_z, b));
+  const std::vector<RgBuf>& bufs = b.bufs;
   // preconditioners: the V-cycle of each system's cube lattice (lattice buffers
   // of their own when several systems hold one), E of every realization on the
   // lattice's elements; r and z of such a system live in the lattice's buffers
@@ -1280,70 +1287,29 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   } pguard{P};
   if (n_vc > 1)
     while ((int)ctx->vc_pool.size() < n_vc) ctx->vc_pool.push_back(new DevMem[kWorkSlots]);
-  for (int i = 0, k = 0; i < S; ++i)
-    if (use_vcycle[i]) {
-      DevMem* own = n_vc > 1 ? ctx->vc_pool[k++] : nullptr;
-      MSG_TRY(gmg_precond_create(ctx, lats[i], in[i].nu, in[i].kl, in[i].d_xi, in[i].R, bufs[i].Rp, own, &P[i]));
-      float *rl = nullptr, *zl = nullptr;
-      const int* lmap = nullptr;
-      int lrp = 0;
-      gmg_precond_buffers(P[i], &rl, &zl, &lmap, &lrp);
-      if (lrp != bufs[i].Rp)
-        return set_error(ctx, MSG_ERR_UNKNOWN, "element-by-element batch: lattice layout of %d realizations, not %d",
-                         lrp, bufs[i].Rp);
-      sys[i].rl = rl;
-      sys[i].z = zl;
-      sys[i].lmap = lmap;
-    }
-  for (int i = 0; i < S; ++i) {
-    RgBuf& B = bufs[i];
-    MSG_TRY(rg_setup(ctx, in[i], B, static_cast<double*>(k300), d_status));
-    Mesh* m = in[i].m;
-    RgSys& Y = sys[i];
-    Y.n_nodes = m->n_nodes;
-    Y.Rp = B.Rp;
-    Y.n_blk = B.n_blk;
-    Y.n_blk_u = B.n_blk_u;
-    Y.inc_ptr = B.ptr;
-    Y.inc = B.inc;
-    Y.conn = m->d_conn.as<int>();
-    Y.mask = m->d_mask.as<uint8_t>();
-    Y.K32 = B.K32;
-    Y.K64 = B.K64;
-    Y.E32 = B.E32;
-    Y.E64 = B.E64;
-    Y.b = B.bn;
-    Y.x = B.x;
-    Y.d = B.d;
-    Y.r = B.r;
-    Y.p = B.p;
-    Y.q = B.q;
-    Y.dinv = B.dinv;
-    Y.part = B.part;
-    Y.part_u = B.part_u;
-    Y.kind = use_vcycle[i] ? 1 : 0;
-    if (!use_vcycle[i]) Y.z = zs[i];
+  for (int i = 0, k = 0; i < S; ++i) {
+    b.sys[i].kind = use_vcycle[i] ? 1 : 0;
+    if (!use_vcycle[i]) continue;
+    DevMem* own = n_vc > 1 ? ctx->vc_pool[k++] : nullptr;
+    MSG_TRY(gmg_precond_create(ctx, lats[i], in[i].nu, in[i].kl, in[i].d_xi, in[i].R, bufs[i].Rp, own, &P[i]));
+    float *rl = nullptr, *zl = nullptr;
+    const int* lmap = nullptr;
+    int lrp = 0;
+    gmg_precond_buffers(P[i], &rl, &zl, &lmap, &lrp);
+    if (lrp != bufs[i].Rp)
+      return set_error(ctx, MSG_ERR_UNKNOWN, "element-by-element batch: lattice layout of %d realizations, not %d",
+                       lrp, bufs[i].Rp);
+    b.sys[i].rl = rl;
+    b.sys[i].z = zl;
+    b.sys[i].lmap = lmap;
   }
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_sys, sys.data(), sizeof(RgSys) * S, cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_items, items.data(), sizeof(RgItem) * items.size(), cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemcpyAsync(d_items_u, items_u.data(), sizeof(RgItem) * items_u.size(), cudaMemcpyHostToDevice,
-                                st));
-  RgScal s;
-  s.gamma = reinterpret_cast<double*>(scal_base);
-  s.rr_ref = s.gamma + Rtot;
-  s.bnorm = s.rr_ref + Rtot;
-  s.res = s.bnorm + Rtot;
-  s.alpha = reinterpret_cast<float*>(s.res + Rtot);
-  s.beta = s.alpha + Rtot;
-  s.done = reinterpret_cast<int*>(s.beta + Rtot);
-  s.its = s.done + Rtot;
-  s.rsys = s.its + Rtot;
-  s.sreq = s.rsys + Rtot;
-  s.gact = s.sreq + S;
-  s.flags = s.gact + Rtot / 32;
-  MSG_CUDA(ctx, cudaMemcpyAsync(s.rsys, rsys.data(), sizeof(int) * Rtot, cudaMemcpyHostToDevice, st));
-  MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
-  const RgSys* dS = d_sys;
+  MSG_TRY(rg_batch_upload(ctx, in, b));
+  const std::vector<RgSys>& sys = b.sys;
+  const int Rtot = b.Rtot, n_items = b.n_items, n_items_u = b.n_items_u;
+  const RgScal s = b.s;
+  const RgItem* d_items = b.d_items;
+  const RgItem* d_items_u = b.d_items_u;
+  const RgSys* dS = b.d_sys;
   const int n_groups = Rtot / 32, g_groups = (n_groups + kEbeWarps - 1) / kEbeWarps;
   const int g_scal = (Rtot + kEbeWarps - 1) / kEbeWarps;
   int occ_apply = 1, occ_resid = 1, occ_u = 1;
