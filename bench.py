@@ -370,6 +370,79 @@ def single_leg(args, ctx):
     return out
 
 
+def cantilever_leg(args, ctx):
+    """The plain small case: the linear-static cantilever of 10 x 4 x 4 unit
+    cubes (275 nodes, 750 free DOFs), E = 1, nu 0.3, x = 0 face clamped, total
+    load -1 in z split over the 25 nodes of the x = 10 face, FP64. The GPU FP64
+    drop-in (MSG_PCG_SOLVE, Jacobi-PCG to the recursive 1e-10, timed after one
+    warm-up solve) against the oracle on the host: skyline LDL^T (factorisation
+    and substitution) and CSR Jacobi-PCG to 1e-10, both built from the oracle's
+    own mesh, DOF and load functions."""
+    import torch
+    import msolve_b200 as M
+    import oracle as O
+    nx, ny, nz = 10, 4, 4
+    model = M.cantilever_model(nx, ny, nz)
+    xyz, conn = O.block_mesh(nx, ny, nz)
+    cons = O.clamp_face(xyz, 0)
+    dof, nd = O.enumerate_dofs(cons)
+    b = O.load_tip(xyz, dof, nd, axis_face=0, comp=2, total=-1.0)
+    assert nd == model.n_dofs and np.array_equal(b, model.subdomains[0].RHS)
+    mesh = M.GpuMesh(ctx, model)
+    A = mesh.assemble(np.ones(model.n_elems), model.poisson)
+    s = M.SolverPCG(ctx, model, max_iterations=20000, tolerance=1e-10, precision="fp64")
+    s.matrix = A
+    s.Solve()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    xg = s.Solve().copy()
+    ev1.record()
+    ev1.synchronize()
+    gpu_ms = ev0.elapsed_time(ev1)
+    A.close()
+    Ke = O.h8_stiffness_batch(O.element_xyz(xyz, conn), np.ones(conn.shape[0]), 0.3)[0]
+    t0 = time.perf_counter()
+    sk = O.Skyline(conn, dof, nd)
+    sk.assemble(Ke)
+    f, _ = sk.factorized()
+    xs = sk.solve(f, b)
+    sky_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    cs = O.CSR(xyz.shape[0], conn, dof, nd)
+    cs.assemble(Ke)
+    xp, info = cs.pcg_jacobi(b, tol=1e-10)
+    pcg_ms = (time.perf_counter() - t0) * 1e3
+    scale = np.abs(xs).max()
+    return {"workload": "linear-static cantilever, 10 x 4 x 4 unit cubes, 750 free DOFs, E 1, nu 0.3, total load -1 "
+                        "in z over the x = 10 face, FP64",
+            "gpu_fp64_pcg_ms": gpu_ms, "gpu_iterations": s.iterations,
+            "cpu_skyline_ldlt_ms": sky_ms, "cpu_csr_pcg_ms": pcg_ms, "cpu_pcg_iterations": info["iterations"],
+            "cpu_threads": O.num_threads(),
+            "rel_err_gpu_pcg_vs_skyline": float(np.abs(xg - xs).max() / scale),
+            "rel_err_cpu_pcg_vs_skyline": float(np.abs(xp - xs).max() / scale)}
+
+
+def cpu_serving_baseline(args, sides):
+    """The oracle on the host cores, one request at a time, for the serving
+    sides it solves within seconds (8 to 32; the 48^3 solve takes about half a
+    minute and is left out): KL field, element matrices, CSR assembly and
+    Jacobi-PCG to 1e-8, one realization of a fresh field per side."""
+    import oracle as O
+    per = {}
+    for n in sides:
+        if n > 32:
+            continue
+        P = O.block_problem(n, args.terms, 12)
+        xi = np.random.default_rng(500 + n).standard_normal((1, args.terms))
+        t0 = time.perf_counter()
+        E = oracle_fields(P, xi)
+        _, info = O.block_solve_pcg(n, n, n, P["constrained"], E[0], 0.3, P["b"], tol=1e-8, max_it=100000)
+        per[str(n)] = {"service_ms": (time.perf_counter() - t0) * 1e3, "iterations": info["iterations"]}
+    mean = float(np.mean([v["service_ms"] for v in per.values()])) if per else None
+    return {"sides": per, "mean_service_ms_sides_8_to_32": mean, "cores": O.num_threads(),
+            "max_throughput_per_s_sides_8_to_32": 1e3 / mean if mean else None}
+
+
 def ragged_leg(args, ctx):
     """Monte Carlo systems of uneven size in one batch (MSG_MC_SOLVE_RAGGED): the
     serving sides {8, 16, 24, 32, 48} (cube lattices) and a 24^3 block with its
@@ -554,6 +627,8 @@ def serving_leg(args, ctx):
                 "mean_iterations": float(np.mean(its))})
         out["fp64_one_at_a_time"] = fp64_serving_baseline(args, ctx, sides,
                                                            [float(v) for v in args.serve_rates.split(",") if v])
+        if not args.no_cpu:
+            out["cpu_oracle_one_at_a_time"] = cpu_serving_baseline(args, sides)
         if not args.no_parity and largest is not None:
             import oracle as O
             n = max(sides)
@@ -906,6 +981,7 @@ def main():
         serving = None if args.no_serving else serving_leg(args, ctx)
         single = None if args.no_single else single_leg(args, ctx)
         ragged = None if args.no_ragged else ragged_leg(args, ctx)
+        cantilever = None if args.no_cpu else cantilever_leg(args, ctx)
         distorted = None
         if not args.no_ragged:  # the same element-by-element loop on one mesh that is not a lattice
             dargs = argparse.Namespace(**vars(args))
@@ -955,6 +1031,7 @@ def main():
             "single_solve": single,
             "ragged": ragged,
             "distorted_mesh": distorted,
+            "cantilever": cantilever,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
