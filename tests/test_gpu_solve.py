@@ -134,3 +134,30 @@ def test_mixed_assembled_solve_reaches_fp64_true_residual(ctx):
     assert abs(mixed.rel_res - np.linalg.norm(r) / np.linalg.norm(b)) <= 1e-3 * mixed.rel_res + 1e-16
     assert np.abs(xm - xo).max() <= 1e-8 * np.abs(xo).max()
     assert mixed.iterations <= 1.3 * fp64.iterations + 16
+
+
+def test_mixed_zero_rhs_and_not_converged(ctx):
+    """The mixed loop keeps SolverPCG's guards: a zero right-hand side returns
+    x = 0 after no iteration; an iteration limit below what the tolerance needs
+    raises not-converged (-2001) with iterations = the limit, and the iterate it
+    leaves (the FP32 correction folded into the FP64 x) is the one the same
+    limit gives on a second call, and is closer to the solution than x = 0."""
+    model = M.clamped_block_model(6)
+    A = M.GpuMesh(ctx, model).assemble(model.E_elem, 0.3)
+    solver = M.SolverPCG(ctx, model, precision="mixed")
+    solver.matrix = A
+    model.subdomains[0].Forces = np.zeros(model.n_dofs)
+    x = solver.Solve(100, 1e-8)
+    assert solver.iterations == 0 and not x.any()
+    model.ConnectDataStructures()
+    b = model.subdomains[0].RHS
+    xs = []
+    for _ in range(2):
+        with pytest.raises(M.InvalidOperationError) as e:
+            solver.Solve(7, 1e-12)
+        assert e.value.code == -2001 and solver.iterations == 7
+        xs.append(model.subdomains[0].Solution.copy())
+    assert np.array_equal(xs[0], xs[1]) and np.abs(xs[0]).max() > 0
+    C, _ = oracle_csr(model, model.E_elem)
+    r = b - C.multiply(xs[0])
+    assert np.linalg.norm(r) < np.linalg.norm(b)
