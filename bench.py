@@ -977,13 +977,16 @@ def main():
             import oracle as O
             cpu = cpu_baseline(args, O.block_problem(args.n, K_terms, 16), xi_all[0].numpy())
         its_all = np.concatenate(iters)
-        newmark = None if args.no_newmark else newmark_leg(args, ctx)
-        serving = None if args.no_serving else serving_leg(args, ctx)
-        single = None if args.no_single else single_leg(args, ctx)
-        ragged = None if args.no_ragged else ragged_leg(args, ctx)
-        cantilever = None if args.no_cpu else cantilever_leg(args, ctx)
+        # the other configurations are single-GPU measurements: the 1-GPU run reports
+        # them, a multi-GPU run (the other ranks waiting) only the scaled batch
+        solo = ws == 1
+        newmark = newmark_leg(args, ctx) if solo and not args.no_newmark else None
+        serving = serving_leg(args, ctx) if solo and not args.no_serving else None
+        single = single_leg(args, ctx) if solo and not args.no_single else None
+        ragged = ragged_leg(args, ctx) if solo and not args.no_ragged else None
+        cantilever = cantilever_leg(args, ctx) if solo and not args.no_cpu else None
         distorted = None
-        if not args.no_ragged:  # the same element-by-element loop on one mesh that is not a lattice
+        if solo and not args.no_ragged:  # the same element-by-element loop on one mesh that is not a lattice
             dargs = argparse.Namespace(**vars(args))
             dargs.R, dargs.steps = 512, 2
             distorted = distorted_leg(dargs, ctx)
