@@ -2090,6 +2090,7 @@ __global__ void __launch_bounds__(kRThreads, 1)
 // Offsets are 32-bit and relative to the centre node (the 27 loads of a
 // component share one base address).
 constexpr int kXferThreads = 128;
+constexpr int kProlongNodes = 2;  // fine nodes of one k_prolong_add CTA
 __global__ void __launch_bounds__(kXferThreads, 8) k_restrict(Lattice Lf, Lattice Lc, const int* __restrict__ interior_c,
                                                               const uint8_t* __restrict__ mask_c,
                                                               const float* __restrict__ tf,
@@ -2141,7 +2142,7 @@ __global__ void __launch_bounds__(kXferThreads, 8) k_restrict(Lattice Lf, Lattic
 // arithmetic of the start pass (which then need not write it), and x_f is
 // written at every component (the constrained ones without the correction).
 __global__ void __launch_bounds__(kXferThreads, 8) k_prolong_add(Lattice Lf, Lattice Lc,
-                                                                 const int* __restrict__ interior_f,
+                                                                 const int* __restrict__ interior_f, int n_int,
                                                                  const uint8_t* __restrict__ mask_f,
                                                                  const float* __restrict__ xc, float* __restrict__ xf,
                                                                  const float* __restrict__ r0,
@@ -2149,53 +2150,59 @@ __global__ void __launch_bounds__(kXferThreads, 8) k_prolong_add(Lattice Lf, Lat
   const int Q = Lf.Rp >> 2;
   const int q = blockIdx.y * kXferThreads + threadIdx.x;
   if (q >= Q) return;
-  const int nf = interior_f[blockIdx.x];
-  const uint32_t mk = mask_f[nf];
-  if (mk == 7u && r0 == nullptr) return;
-  const int gi = nf % Lf.NXp - 1, gj = (nf / Lf.NXp) % Lf.NYp - 1, gk = nf / (Lf.NXp * Lf.NYp) - 1;
   const int sx = 3 * Q, sy = Lc.NXp * sx, sz = Lc.NYp * sy;  // float4 strides between coarse nodes
-  const int c0 = ((gi >> 1) + 1) + Lc.NXp * (((gj >> 1) + 1) + Lc.NYp * ((gk >> 1) + 1));
-  const int oi = (gi & 1) * sx, oj = (gj & 1) * sy, ok = (gk & 1) * sz;  // offset of the second neighbour (or 0)
-  const float wi[2] = {(gi & 1) ? 0.5f : 1.f, (gi & 1) ? 0.5f : 0.f};
-  const float wj[2] = {(gj & 1) ? 0.5f : 1.f, (gj & 1) ? 0.5f : 0.f};
-  const float wk[2] = {(gk & 1) ? 0.5f : 1.f, (gk & 1) ? 0.5f : 0.f};
-  const float4* c4 = reinterpret_cast<const float4*>(xc) + (size_t)c0 * sx + q;
-  float4* f4 = reinterpret_cast<float4*>(xf) + (size_t)nf * sx + q;
-  float4 wdv = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (r0 != nullptr) {
-    const float4 dv = reinterpret_cast<const float4*>(dinv0)[(size_t)nf * Q + q];
-    wdv = make_float4(omega * dv.x, omega * dv.y, omega * dv.z, omega * dv.w);
-  }
+  // kProlongNodes fine nodes a CTA, their loads in flight together
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    float4 s;
+  for (int u = 0; u < kProlongNodes; ++u) {
+    const int t = blockIdx.x * kProlongNodes + u;
+    if (t >= n_int) break;
+    const int nf = interior_f[t];
+    const uint32_t mk = mask_f[nf];
+    if (mk == 7u && r0 == nullptr) continue;
+    const int gi = nf % Lf.NXp - 1, gj = (nf / Lf.NXp) % Lf.NYp - 1, gk = nf / (Lf.NXp * Lf.NYp) - 1;
+    const int c0 = ((gi >> 1) + 1) + Lc.NXp * (((gj >> 1) + 1) + Lc.NYp * ((gk >> 1) + 1));
+    const int oi = (gi & 1) * sx, oj = (gj & 1) * sy, ok = (gk & 1) * sz;  // offset of the second neighbour (or 0)
+    const float wi[2] = {(gi & 1) ? 0.5f : 1.f, (gi & 1) ? 0.5f : 0.f};
+    const float wj[2] = {(gj & 1) ? 0.5f : 1.f, (gj & 1) ? 0.5f : 0.f};
+    const float wk[2] = {(gk & 1) ? 0.5f : 1.f, (gk & 1) ? 0.5f : 0.f};
+    const float4* c4 = reinterpret_cast<const float4*>(xc) + (size_t)c0 * sx + q;
+    float4* f4 = reinterpret_cast<float4*>(xf) + (size_t)nf * sx + q;
+    float4 wdv = make_float4(0.f, 0.f, 0.f, 0.f);
     if (r0 != nullptr) {
-      const float4 rv = reinterpret_cast<const float4*>(r0)[((size_t)nf * 3 + c) * Q + q];
-      s = make_float4(wdv.x * rv.x, wdv.y * rv.y, wdv.z * rv.z, wdv.w * rv.w);
-      if ((mk >> c) & 1) {
-        f4[c * Q] = s;
-        continue;
-      }
-    } else {
-      if ((mk >> c) & 1) continue;
-      s = f4[c * Q];
+      const float4 dv = reinterpret_cast<const float4*>(dinv0)[(size_t)nf * Q + q];
+      wdv = make_float4(omega * dv.x, omega * dv.y, omega * dv.z, omega * dv.w);
     }
 #pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          // an even coordinate has one coarse neighbour on that axis: skip the zero-weight loads
-          if ((e && !(gi & 1)) || (bb && !(gj & 1)) || (a && !(gk & 1))) continue;
-          const float wgt = wk[a] * wj[bb] * wi[e];
-          const float4 v = c4[(e ? oi : 0) + (bb ? oj : 0) + (a ? ok : 0) + c * Q];
-          s.x = fmaf(wgt, v.x, s.x);
-          s.y = fmaf(wgt, v.y, s.y);
-          s.z = fmaf(wgt, v.z, s.z);
-          s.w = fmaf(wgt, v.w, s.w);
+    for (int c = 0; c < 3; ++c) {
+      float4 s;
+      if (r0 != nullptr) {
+        const float4 rv = reinterpret_cast<const float4*>(r0)[((size_t)nf * 3 + c) * Q + q];
+        s = make_float4(wdv.x * rv.x, wdv.y * rv.y, wdv.z * rv.z, wdv.w * rv.w);
+        if ((mk >> c) & 1) {
+          f4[c * Q] = s;
+          continue;
         }
-    f4[c * Q] = s;
+      } else {
+        if ((mk >> c) & 1) continue;
+        s = f4[c * Q];
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            // an even coordinate has one coarse neighbour on that axis: skip the zero-weight loads
+            if ((e && !(gi & 1)) || (bb && !(gj & 1)) || (a && !(gk & 1))) continue;
+            const float wgt = wk[a] * wj[bb] * wi[e];
+            const float4 v = c4[(e ? oi : 0) + (bb ? oj : 0) + (a ? ok : 0) + c * Q];
+            s.x = fmaf(wgt, v.x, s.x);
+            s.y = fmaf(wgt, v.y, s.y);
+            s.z = fmaf(wgt, v.z, s.z);
+            s.w = fmaf(wgt, v.w, s.w);
+          }
+      f4[c * Q] = s;
+    }
   }
 }
 
@@ -2204,6 +2211,10 @@ inline dim3 xfer_grid(int n_int, int Rp) {
   return dim3((unsigned)n_int, (unsigned)((Rp / 4 + kXferThreads - 1) / kXferThreads));
 }
 inline int xfer_block(int Rp) { return std::min(kXferThreads, (Rp / 4 + 31) / 32 * 32); }
+inline dim3 prolong_grid(int n_int, int Rp) {
+  return dim3((unsigned)((n_int + kProlongNodes - 1) / kProlongNodes),
+              (unsigned)((Rp / 4 + kXferThreads - 1) / kXferThreads));
+}
 
 // Coarse element field: the mean of the 8 fine elements it covers (elements
 // are stored at their lower-corner padded node). One CTA per coarse element.
@@ -3590,15 +3601,17 @@ void gmg_vcycle(BlockSys* B, Scal& s, bool even, cudaStream_t st) {
   // up: prolongate into the level's iterate, one sweep (result in t)
   for (int l = nl - 2; l >= 1; --l) {
     GmgLevel& g = B->lv[l];
-    k_prolong_add<<<xfer_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(g.L, B->lv[l + 1].L, g.interior, g.mask, res_c,
-                                                                        g.x, nullptr, nullptr, 0.f);
+    k_prolong_add<<<prolong_grid(g.L.n_int, Rp), xfer_block(Rp), 0, st>>>(g.L, B->lv[l + 1].L, g.interior,
+                                                                          g.L.n_int, g.mask, res_c, g.x, nullptr,
+                                                                          nullptr, 0.f);
     lvlc(Smooth{}, g);
     res_c = g.t;
   }
   // level 0: x0 = omega dinv r' formed here (the start pass does not write it)
-  k_prolong_add<<<xfer_grid(B->L.n_int, Rp), xfer_block(Rp), 0, st>>>(B->L, B->lv[1].L, B->interior, B->mask, res_c,
-                                                                        B->xs.as<float>(), r_out, B->dinv.as<float>(),
-                                                                        om);
+  k_prolong_add<<<prolong_grid(B->L.n_int, Rp), xfer_block(Rp), 0, st>>>(B->L, B->lv[1].L, B->interior,
+                                                                          B->L.n_int, B->mask, res_c,
+                                                                          B->xs.as<float>(), r_out,
+                                                                          B->dinv.as<float>(), om);
   // level 0 post-sweep: z (into qB) and the partial z.r'
   lvl0(Smooth{}, B->tm_xs, B->tm_xs, B->tm2_xs, B->tm2_xs, r_out, B->dinv.as<float>(), qB, nullptr, nullptr, nullptr,
        part2 + 1, 2);
