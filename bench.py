@@ -898,41 +898,57 @@ def main():
     traffic = per_r * Rp if (per_r and args.n == 32) else None
 
     line = None
-    if rank == 0:
-        # e2e through the host-buffer entry points (pinned buffers): every step
-        # copies its xi in and every realization's displacements out. Blocking:
-        # MSG_MC_SOLVE_BATCH returns with X on the host. Pipelined (the e2e
-        # value): MSG_MC_SOLVE_BATCH_PIPELINED leaves each step's X copy in
-        # flight while the next step solves (two host buffers, flushed inside
-        # the timed region).
-        xi_h = torch.empty(R, K_terms, dtype=torch.float64).pin_memory()
-        b_h = torch.from_numpy(model.subdomains[0].RHS.copy()).pin_memory()
-        X_hs = [torch.empty(R, Nd, dtype=torch.float64).pin_memory() for _ in range(2)]
-        n_e2e = max(3, args.steps)
+    # e2e through the host-buffer entry points (pinned buffers), on every rank at
+    # once (each rank its own batch and host buffers; the slowest rank's time):
+    # every step copies its xi in and every realization's displacements out.
+    # Blocking: MSG_MC_SOLVE_BATCH returns with X on the host. Pipelined (the e2e
+    # value): MSG_MC_SOLVE_BATCH_PIPELINED leaves each step's X copy in flight
+    # while the next step solves (two host buffers, flushed inside the timed region).
+    xi_h = torch.empty(R, K_terms, dtype=torch.float64).pin_memory()
+    b_h = torch.from_numpy(model.subdomains[0].RHS.copy()).pin_memory()
+    X_hs = [torch.empty(R, Nd, dtype=torch.float64).pin_memory() for _ in range(2)]
+    n_e2e = max(3, args.steps)
 
-        def host_call(fn, X_h):
-            stt = fn(mesh.handle, model.poisson, C.byref(kls), R, C.cast(C.c_void_p(xi_h.data_ptr()), N._d),
-                     C.cast(C.c_void_p(b_h.data_ptr()), N._d), N.MSG_MODE_MIXED_BATCHED, 200000, args.tol, tip,
-                     C.cast(C.c_void_p(X_h.data_ptr()), N._d), N.ptr(tip_h), N.ptr(its_h, N._i), N.ptr(res_h))
-            N.check(stt, ctx.handle, "MC batch (host buffers)")
+    def host_call(fn, X_h):
+        stt = fn(mesh.handle, model.poisson, C.byref(kls), R, C.cast(C.c_void_p(xi_h.data_ptr()), N._d),
+                 C.cast(C.c_void_p(b_h.data_ptr()), N._d), N.MSG_MODE_MIXED_BATCHED, 200000, args.tol, tip,
+                 C.cast(C.c_void_p(X_h.data_ptr()), N._d), N.ptr(tip_h), N.ptr(its_h, N._i), N.ptr(res_h))
+        N.check(stt, ctx.handle, "MC batch (host buffers)")
 
-        e2e_lat = []
-        for s in range(1 + n_e2e):  # one untimed call, then at least 3 timed
-            xi_h.copy_(xi_all[steps_total])
-            t0 = time.perf_counter()
-            host_call(L.MSG_MC_SOLVE_BATCH, X_hs[0])
-            if s > 0:
-                e2e_lat.append(1e3 * (time.perf_counter() - t0))
-        e2e_blocking = R / (np.mean(e2e_lat) / 1e3)
-        host_call(L.MSG_MC_SOLVE_BATCH_PIPELINED, X_hs[1])  # untimed
-        N.check(L.MSG_MC_FLUSH(ctx.handle), ctx.handle, "MSG_MC_FLUSH")
+    def slowest(ms):  # the slowest rank's time (every rank calls it, in the same order)
+        if ws == 1:
+            return ms
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def start_together():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    e2e_lat = []
+    for s in range(1 + n_e2e):  # one untimed call, then at least 3 timed
+        xi_h.copy_(xi_all[steps_total])
+        start_together()
         t0 = time.perf_counter()
-        for s in range(n_e2e):
-            xi_h.copy_(xi_all[steps_total])
-            host_call(L.MSG_MC_SOLVE_BATCH_PIPELINED, X_hs[s % 2])
-        N.check(L.MSG_MC_FLUSH(ctx.handle), ctx.handle, "MSG_MC_FLUSH")
-        e2e_ms = 1e3 * (time.perf_counter() - t0) / n_e2e
-        e2e_value = R / (e2e_ms / 1e3)
+        host_call(L.MSG_MC_SOLVE_BATCH, X_hs[0])
+        if s > 0:
+            e2e_lat.append(slowest(1e3 * (time.perf_counter() - t0)))
+    e2e_blocking = ws * R / (np.mean(e2e_lat) / 1e3)
+    host_call(L.MSG_MC_SOLVE_BATCH_PIPELINED, X_hs[1])  # untimed
+    N.check(L.MSG_MC_FLUSH(ctx.handle), ctx.handle, "MSG_MC_FLUSH")
+    start_together()
+    t0 = time.perf_counter()
+    for s in range(n_e2e):
+        xi_h.copy_(xi_all[steps_total])
+        host_call(L.MSG_MC_SOLVE_BATCH_PIPELINED, X_hs[s % 2])
+    N.check(L.MSG_MC_FLUSH(ctx.handle), ctx.handle, "MSG_MC_FLUSH")
+    e2e_ms = slowest(1e3 * (time.perf_counter() - t0) / n_e2e)
+    e2e_value = ws * R / (e2e_ms / 1e3)
+    if rank == 0:
         X_h = X_hs[(n_e2e - 1) % 2]
         # parity: realizations of the e2e batch (host outputs of the public entry
         # point) against FP64 oracle solves of the same fields converged to 1e-12
