@@ -343,8 +343,9 @@ __global__ void __launch_bounds__(32 * kS * kSpmvWarps) k_pcg_dir_spmv_rows(int 
 // On a pause the host runs k_pcgm_fold (x += d, d = 0), y = K64 x with the FP64
 // values and k_pcgm_true (r = b - y into the FP32 r, gamma = (D r).r; stop
 // when ||r||/||b|| < tol in FP64). The direction is kept across the
-// replacement. Per iteration the vectors cost 36 bytes a DOF besides the
-// matrix (FP64 vectors and a separate direction pass: 100).
+// replacement. Per iteration the vectors cost 48 bytes a DOF besides the
+// matrix (16 in the SpMV pass, 32 in the update; with FP64 vectors and a
+// separate direction pass they would cost 108).
 // A warp owns one slice at a time; with kSpmvWarps = 1 the CTAs are persistent
 // (the grid fills the SMs once) and a warp strides over the slices, summing its
 // partials across them; with kSpmvWarps > 1 (small matrices) a CTA takes one

@@ -663,7 +663,7 @@ __global__ void k_ebe_tip(int R, int Rp, int row, const double* __restrict__ x, 
   if (r < R) tip[r] = x[(size_t)row * Rp + r];
 }
 
-// ---------------------------------------------------------------- multigrid-preconditioned loop (one system)
+// ---------------------------------------------------------------- preconditioned loop (V-cycle or diagonal per system)
 // Standard PCG with z = M^-1 r: M^-1 the V-cycle of the system's cube lattice
 // (gmg_precond_apply) or the diagonal (k_vc_jacobi_z):
 // operator (k_rg_apply: q = K p, partial p.q), alpha, update (r, d and r.r),

@@ -323,8 +323,8 @@ int launch_node_to_dof(Context* ctx, const Mesh* m, const double* d_in, double* 
                        int64_t out_stride);
 // FP32 copy b[0..n) of FP64 a on the context's stream.
 int launch_to_f32(Context* ctx, size_t n, const double* a, float* b);
-// mixed: FP32 matrix values in the loop's SpMV, FP64 vectors, FP64 true-residual
-// replacement (reliable updates), stop on the FP64 true residual.
+// mixed: FP32 matrix values and vectors in the loop, the iterate in FP64, FP64
+// true-residual replacement (reliable updates), stop on the FP64 true residual.
 int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b_node, double* d_x_node, int max_it, double tol,
                      int* iterations, double* rel_res, int* status, bool mixed = false);
 
