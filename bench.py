@@ -445,22 +445,22 @@ def cpu_serving_baseline(args, sides):
 
 def ragged_leg(args, ctx):
     """Monte Carlo systems of uneven size in one batch (MSG_MC_SOLVE_RAGGED): the
-    serving sides {8, 16, 24, 32, 48} (cube lattices) and a 24^3 block with its
-    interior nodes moved (not a lattice), args.ragged_R realizations each with
-    its own 50-term KL field (sigma 0.3, l 0.2 * side), PCG with the FP32
-    element-by-element operator and the FP64 true residual < 1e-8, each system
-    preconditioned by the V-cycle of its cube lattice (the diagonal with the
-    multigrid option 0). Timed
-    (device time of the call) as one ragged batch after a warm-up, and as the
-    same systems one call each, and each system through its own
-    MSG_MC_SOLVE_BATCH call; each batch is built and solved once first (its
-    meshes, their lattices and the workspace then exist), the time of a call is
-    the median of three calls on the host clock (xi and b in, X of the 48^3 and
-    the distorted 24^3 and every tip value out); the oracle solves one realization of the 48^3
-    lattice and of the distorted 24^3 (FP64 CSR Jacobi-PCG to 1e-12)."""
+    serving sides {8, 16, 24, 32, 48} (cube lattices) and blocks of side 16, 24
+    and 32 with their interior nodes moved by up to 0.2 (not lattices),
+    args.ragged_R realizations each with its own 50-term KL field (sigma 0.3,
+    l 0.2 * side), to the FP64 true residual < 1e-8; the cube lattices run the
+    lattice loop, the moved-node blocks share the element-by-element batch, each
+    system preconditioned by the V-cycle of its cube lattice (the diagonal with
+    the multigrid option 0). Timed as one ragged batch, as the same systems one
+    ragged call each, and as one MSG_MC_SOLVE_BATCH call (the analyzer) per
+    system; each batch is built and solved once first (its meshes, their
+    lattices and the workspace then exist), the time of a call is the median of
+    three calls on the host clock (xi and b in, X of the 48^3 lattice and the
+    distorted 24^3 and every tip value out); the oracle solves one realization
+    of the 48^3 lattice and of the distorted 24^3 (FP64 CSR Jacobi-PCG to 1e-12)."""
     import msolve_b200 as M
     R, tol = args.ragged_R, 1e-8
-    specs = [(8, False), (16, False), (24, False), (32, False), (48, False), (24, True)]
+    specs = [(8, False), (16, False), (24, False), (32, False), (48, False), (16, True), (24, True), (32, True)]
     systems = []
     for i, (n, dist) in enumerate(specs):
         model = M.clamped_block_model(n)
@@ -471,7 +471,7 @@ def ragged_leg(args, ctx):
         kl = M.LognormalStochasticCoefficientsProvider([n] * 3, 0.2 * n, args.terms, 16)
         xi = np.random.default_rng(1000 + i).standard_normal((R, args.terms))
         systems.append((n, dist, model, kl, xi))
-    keep = {4, 5}
+    keep = {4, 6}  # the 48^3 lattice and the distorted 24^3
 
     def batch(sel):
         b = M.RaggedMonteCarloBatch(ctx, tolerance=tol)
@@ -507,7 +507,7 @@ def ragged_leg(args, ctx):
     dof_its = sum(systems[j][2].n_dofs * float(res[j]["Iterations"].sum()) for j in idx)
     prec = "Jacobi-PCG" if ctx.get_option("multigrid") == 0 else "PCG preconditioned by each system's V-cycle"
     out = {"workload": f"{len(specs)} Monte Carlo systems in one batch: cube lattices of side 8, 16, 24, 32, 48 and "
-                       f"a 24^3 block with interior nodes moved by up to 0.2, {R} realizations each, "
+                       f"16^3, 24^3, 32^3 blocks with interior nodes moved by up to 0.2, {R} realizations each, "
                        f"{args.terms}-term KL lognormal E, {prec} (FP32 element-by-element operator, FP64 "
                        f"iterate) to the FP64 true relative residual < {tol:g}",
            "systems": [{"mesh": f"{n}^3" + (" distorted" if dist else ""), "free_dofs": model.n_dofs,
