@@ -61,8 +61,9 @@ typedef struct msg_svs* MSG_SVS;
  * beyond the device's free memory. The batched entry points keep their device
  * buffers in the context from one call to the next (grown to the largest call,
  * never shrunk; charged to the budget) so that repeated calls allocate
- * nothing; they are released with the context (MSG_DESTROY). No counterpart in the reference (which has no
- * device); the C# shim creates one per solver instance. */
+ * nothing; they are released with the context (MSG_DESTROY). No counterpart
+ * in the reference (which has no device); the C# shim creates one per solver
+ * instance. */
 int MSG_CREATE(int device, uint64_t mem_budget_bytes, MSG_CTX* out);
 int MSG_DESTROY(MSG_CTX ctx);
 /* Text of the last error on this context (valid until the next call on it). */
