@@ -458,7 +458,7 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * "multigrid_sweeps" (damped Jacobi sweeps on the coarsest level, default 20),
  * "multigrid_omega" (Jacobi damping of every level, 0 = derived from the
  * element stiffness, default), "multigrid_delta" (reliable-update factor of the
- * V-cycle loop, default 0.003; its inner chunk is 2 iterations), "multigrid_packed"
+ * V-cycle-preconditioned loops, default 0.001; their inner chunk is 2 iterations), "multigrid_packed"
  * (1, default: the three level-0 operator passes of an iteration work on two
  * realizations per thread with packed FP32 arithmetic; 0: one per thread),
  * "multigrid_fused_coarse" (1, default: every sweep of the coarsest level in

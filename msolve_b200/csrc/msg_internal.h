@@ -78,7 +78,7 @@ struct Context {
   int mg_levels = kGmgMaxLevels; // lattice levels at most, fine level included (2..kGmgMaxLevels)
   int mg_sweeps = 20;           // damped Jacobi sweeps on the coarsest level
   double mg_omega = 0.0;        // Jacobi damping; 0 = from the element stiffness
-  double mg_delta = 3e-3;       // reliable-update factor of the multigrid loop
+  double mg_delta = 1e-3;       // reliable-update factor of the V-cycle-preconditioned loops
   int mg_packed = 1;            // 1: level-0 operator with two realizations per lane (packed FP32)
   int mg_fused_coarse = 1;      // 1: all coarsest-level sweeps in one launch (when the level fits a CTA)
   int tensor_op = 0;            // 1: the multigrid loop's level-0 search-direction launch on the tensor cores
