@@ -4441,12 +4441,16 @@ int gmg_precond_apply(Context* ctx, void* handle, const float* r_node, float* z_
   return MSG_OK;
 }
 
-void gmg_precond_buffers(void* handle, float** r_lat, float** z_lat, const int** node_to_lattice, int* Rp) {
+void gmg_precond_buffers(void* handle, float** r_lat, float** z_lat, const int** node_to_lattice, int* Rp,
+                         const double** zr_part, int* zr_blocks) {
   GmgPrecondImpl* P = static_cast<GmgPrecondImpl*>(handle);
   *r_lat = P->B.r32.as<float>();
   *z_lat = P->B.qB.as<float>();
   *node_to_lattice = P->B.interior;
   *Rp = P->B.Rp;
+  // the level-0 post-sweep's partials z.r' ([tile][Rp][2], component 1)
+  *zr_part = P->B.part_op.as<double>() + 1;
+  *zr_blocks = P->B.pack ? P->B.n_tiles2 : P->B.n_tiles_m;
 }
 
 void gmg_precond_destroy(void* handle) { delete static_cast<GmgPrecondImpl*>(handle); }

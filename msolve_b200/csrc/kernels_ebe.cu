@@ -84,6 +84,10 @@ struct RgSys {
   // each node; z then is the lattice's z buffer, indexed the same way
   float* rl;
   const int* lmap;
+  // V-cycle systems: z.r of the last apply, from the V-cycle's own partials
+  // (lzr[(block * Rp + realization) * 2], lzr_blocks blocks)
+  const double* lzr;
+  int lzr_blocks;
 };
 struct RgItem {
   int sys, blk, rb, G;  // nodes blk * 64 .., realizations rb .. rb + 32 G - 1
@@ -460,6 +464,18 @@ __device__ __forceinline__ double rg_sum(const double* __restrict__ part, int n_
   return v;
 }
 
+// z.r of system-local realization r after z = M^-1 r: the V-cycle's partials
+// (two values a block and realization, z.r the second) or the diagonal pass's
+__device__ __forceinline__ double rg_sum_zr(const RgSys& S, int r) {
+  if (!S.lzr) return rg_sum(S.part_u, S.n_blk_u, S.Rp, r);
+  const int lane = threadIdx.x & 31;
+  double v = 0.0;
+  for (int i = lane; i < S.lzr_blocks; i += 32) v += S.lzr[((size_t)i * S.Rp + r) * 2];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __device__ __forceinline__ int rg_warp_index() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
 
 // A realization asks for a true residual of its system.
@@ -699,30 +715,6 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_update(const RgSys* __res
   }
 }
 
-// partial z.r (into part_u[0])
-__global__ void __launch_bounds__(32 * kEbeWarps) k_vc_zr(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items,
-                                                         int n_items, RgScal s) {
-  __shared__ double sh[kEbeWarps * 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const RgItem I = items[it];
-    const RgSys S = Sys[I.sys];
-    if (!s.gact[(S.goff + I.rb) / 32]) continue;
-    const int Rp = S.Rp, col = I.rb;
-    const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
-    double zr = 0.0;
-#pragma unroll 2
-    for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
-        const size_t oz = S.lmap ? ((size_t)__ldg(S.lmap + n) * 3 + c) * Rp + col + lane : o;
-        zr += (double)S.z[oz] * (double)S.r[o];
-      }
-    rg_block_partial(zr, sh, S.part_u + (size_t)I.blk * Rp + col);
-  }
-}
-
 // p = z + beta p
 __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_dir(const RgSys* __restrict__ Sys, const RgItem* __restrict__ items,
                                                           int n_items, RgScal s) {
@@ -745,10 +737,12 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_dir(const RgSys* __restri
   }
 }
 
-// z = D^-1 r for the systems with the diagonal preconditioner
+// z = D^-1 r and the partial z.r (into part_u[0]) for the systems with the
+// diagonal preconditioner; the V-cycle writes its own z.r partials
 __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_jacobi_z(const RgSys* __restrict__ Sys,
                                                                const RgItem* __restrict__ items, int n_items,
                                                                RgScal s) {
+  __shared__ double sh[kEbeWarps * 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
     const RgItem I = items[it];
@@ -756,13 +750,17 @@ __global__ void __launch_bounds__(32 * kEbeWarps) k_vc_jacobi_z(const RgSys* __r
     if (S.kind != 0 || !s.gact[(S.goff + I.rb) / 32]) continue;
     const int Rp = S.Rp, col = I.rb;
     const int n1 = min(S.n_nodes, (I.blk + 1) * kRgBlkU);
+    double zr = 0.0;
 #pragma unroll 2
     for (int n = I.blk * kRgBlkU + w; n < n1; n += kEbeWarps)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const size_t o = ((size_t)n * 3 + c) * Rp + col + lane;
-        S.z[o] = S.dinv[o] * S.r[o];
+        const float rv = S.r[o], zv = S.dinv[o] * rv;
+        S.z[o] = zv;
+        zr += (double)zv * (double)rv;
       }
+    rg_block_partial(zr, sh, S.part_u + (size_t)I.blk * Rp + col);
   }
 }
 
@@ -801,7 +799,7 @@ __global__ void k_vc_beta(const RgSys* __restrict__ Sys, int Rtot, RgScal s, dou
   const RgSys& S = Sys[s.rsys[g]];
   const int r = g - S.goff;
   const size_t Pu = (size_t)S.n_blk_u * S.Rp;
-  const double zr = rg_sum(S.part_u, S.n_blk_u, S.Rp, r), rr = rg_sum(S.part_u + Pu, S.n_blk_u, S.Rp, r);
+  const double zr = rg_sum_zr(S, r), rr = rg_sum(S.part_u + Pu, S.n_blk_u, S.Rp, r);
   if (lane != 0) return;
   s.beta[g] = s.gamma[g] > 0.0 ? (float)(zr / s.gamma[g]) : 0.f;
   s.gamma[g] = zr;
@@ -813,7 +811,7 @@ __global__ void k_vc_start(RgSys S, int R, RgScal s) {
   const int r = rg_warp_index();
   if (r >= S.Rp) return;
   const double bb = rg_sum(S.part + (size_t)kRr * S.n_blk * S.Rp, S.n_blk, S.Rp, r);
-  const double zr = rg_sum(S.part_u, S.n_blk_u, S.Rp, r);
+  const double zr = rg_sum_zr(S, r);
   if ((threadIdx.x & 31) != 0) return;
   const int g = S.goff + r;
   s.bnorm[g] = sqrt(bb);
@@ -838,7 +836,7 @@ __global__ void k_vc_true(const RgSys* __restrict__ Sys, int Rtot, RgScal s, dou
   const RgSys& S = Sys[s.rsys[g]];
   const int r = g - S.goff;
   const double rr = rg_sum(S.part + (size_t)kRr * S.n_blk * S.Rp, S.n_blk, S.Rp, r);
-  const double zr = rg_sum(S.part_u, S.n_blk_u, S.Rp, r);
+  const double zr = rg_sum_zr(S, r);
   if (lane != 0) return;
   const double err = s.bnorm[g] > 0.0 ? sqrt(rr) / s.bnorm[g] : 0.0;
   s.res[g] = err;
@@ -1294,14 +1292,17 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
     MSG_TRY(gmg_precond_create(ctx, lats[i], in[i].nu, in[i].kl, in[i].d_xi, in[i].R, bufs[i].Rp, own, &P[i]));
     float *rl = nullptr, *zl = nullptr;
     const int* lmap = nullptr;
-    int lrp = 0;
-    gmg_precond_buffers(P[i], &rl, &zl, &lmap, &lrp);
+    const double* lzr = nullptr;
+    int lrp = 0, lzr_blocks = 0;
+    gmg_precond_buffers(P[i], &rl, &zl, &lmap, &lrp, &lzr, &lzr_blocks);
     if (lrp != bufs[i].Rp)
       return set_error(ctx, MSG_ERR_UNKNOWN, "element-by-element batch: lattice layout of %d realizations, not %d",
                        lrp, bufs[i].Rp);
     b.sys[i].rl = rl;
     b.sys[i].z = zl;
     b.sys[i].lmap = lmap;
+    b.sys[i].lzr = lzr;
+    b.sys[i].lzr_blocks = lzr_blocks;
   }
   MSG_TRY(rg_batch_upload(ctx, in, b));
   const std::vector<RgSys>& sys = b.sys;
@@ -1340,11 +1341,10 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   }
   MSG_CUDA(ctx, cudaMemsetAsync(s.gact, 0xff, sizeof(int) * n_groups, st));  // every group until the start
   MSG_TRY(precondition(nullptr, true));
-  k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
   for (int i = 0; i < S; ++i) k_vc_start<<<bufs[i].Rp / kEbeWarps, 32 * kEbeWarps, 0, st>>>(sys[i], in[i].R, s);
   k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
   k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
-  count_launch(ctx, 3 + S);
+  count_launch(ctx, 2 + S);
   MSG_CUDA(ctx, cudaGetLastError());
   // two iterations to a graph launch (the multigrid loop's chunk), its reliable-update factor
   constexpr int kChunk = 2;
@@ -1358,7 +1358,6 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
     k_vc_alpha<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s);
     k_vc_update<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     precondition(nullptr, false);
-    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     k_vc_beta<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol2, delta2, max_it);
     k_vc_dir<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
   }
@@ -1382,7 +1381,7 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
   const int max_chunks = max_it / kChunk + 2;
   for (int chunk = 0; chunk < max_chunks; ++chunk) {
     MSG_CUDA(ctx, cudaGraphLaunch(exec, st));
-    count_launch(ctx, kChunk * (6 + n_vc + (n_vc < S ? 1 : 0)) + 1);
+    count_launch(ctx, kChunk * (5 + n_vc + (n_vc < S ? 1 : 0)) + 1);
     MSG_TRY(publish_flags(ctx, s.flags, 2, h, ctx->d_hflags, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));
     if (h[1] == 0) break;
@@ -1397,11 +1396,10 @@ int ebe_mg_solve(Context* ctx, const std::vector<RgInput>& in, const std::vector
     k_rg_fold<<<g_fold, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s, 0);
     k_rg_resid64<<<g_resid, 32 * kEbeWarps, 0, st>>>(dS, d_items, n_items, s);
     MSG_TRY(precondition(&req, true));
-    k_vc_zr<<<g_u, 32 * kEbeWarps, 0, st>>>(dS, d_items_u, n_items_u, s);
     k_vc_true<<<g_scal, 32 * kEbeWarps, 0, st>>>(dS, Rtot, s, tol, max_it);
     k_rg_active<<<g_groups, 32 * kEbeWarps, 0, st>>>(n_groups, s);
     MSG_CUDA(ctx, cudaMemsetAsync(s.sreq, 0, sizeof(int) * S, st));
-    count_launch(ctx, 5);
+    count_launch(ctx, 4);
     MSG_CUDA(ctx, cudaGetLastError());
     MSG_TRY(publish_flags(ctx, s.flags + 1, 1, h + 1, ctx->d_hflags ? ctx->d_hflags + 1 : nullptr, st));
     MSG_CUDA(ctx, cudaStreamSynchronize(st));

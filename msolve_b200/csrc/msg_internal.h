@@ -373,8 +373,10 @@ int gmg_precond_create(Context* ctx, Mesh* lattice, double nu, const MSG_KL* kl,
                        DevMem* own, void** out);
 int gmg_precond_apply(Context* ctx, void* P, const float* r_node, float* z_node, cudaStream_t st);
 // The lattice's r and z buffers ((padded node * 3 + c) * Rp + realization), the
-// padded index of each mesh node and the buffers' Rp.
-void gmg_precond_buffers(void* P, float** r_lat, float** z_lat, const int** node_to_lattice, int* Rp);
+// padded index of each mesh node and the buffers' Rp; the partials of z.r of the
+// last apply (zr_blocks blocks: zr_part[(block * Rp + realization) * 2]).
+void gmg_precond_buffers(void* P, float** r_lat, float** z_lat, const int** node_to_lattice, int* Rp,
+                         const double** zr_part, int* zr_blocks);
 void gmg_precond_destroy(void* P);
 
 // One system of a batched element-by-element solve (kernels_ebe.cu): a mesh
