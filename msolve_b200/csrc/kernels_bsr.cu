@@ -774,13 +774,32 @@ static void launch_pcgm_spmv(Context* ctx, const Mesh* m, const float* v32, cons
 #undef MSG_SPMV32
 }
 
-// Runs the device PCG on node-layout vectors. The loop body (2 kernels) is
-// captured once per matrix as a CUDA graph of `chunk` iterations; the host
-// launches the graph and reads back the state flags after each chunk.
-// Kernels after convergence return immediately, so the recorded iteration
-// count is exact. Mixed precision: the FP32 loop (k_pcgm_*); when it pauses
-// (need), x += d, y = K x with the FP64 values and k_pcgm_true replace the
-// recursive residual (or end the solve on the true residual).
+// The device loop's control (one thread each, inside the solve's graph):
+// another round of iterations while the solve runs, at most
+// max_it / chunk + 2 max_it + 4 rounds (every round but a paused one advances
+// the iteration count, every pause ends or advances it, so the bound is never
+// the reason to stop); and, in the mixed loop, the FP64 true-residual step
+// when the round paused for one.
+__global__ void k_pcg_loop_while(PcgState* st, cudaGraphConditionalHandle h, int chunk) {
+  const long long r = ++st->rounds;
+  const long long cap = (long long)st->max_it / chunk + 2LL * st->max_it + 4;
+  cudaGraphSetConditional(h, (!st->done && r < cap) ? 1u : 0u);
+}
+
+__global__ void k_pcg_loop_if(PcgState* st, cudaGraphConditionalHandle h) {
+  const int need = st->need;
+  if (need) st->pauses += 1;
+  cudaGraphSetConditional(h, need ? 1u : 0u);
+}
+
+// Runs the device PCG on node-layout vectors, the whole solve one graph
+// launch: a WHILE node repeats a round of `chunk` iterations (2 kernels each,
+// captured once per matrix) until the state says done, with no host round
+// trip between rounds. Kernels after convergence return immediately, so the
+// recorded iteration count is exact. Mixed precision: the FP32 loop
+// (k_pcgm_*); when it pauses (need), an IF node runs x += d, y = K x with the
+// FP64 values and k_pcgm_true, which replace the recursive residual (or end
+// the solve on the true residual).
 int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, int max_it, double tol, int* iterations,
                      double* rel_res, int* status, bool mixed) {
   Mesh* m = A->mesh;
@@ -838,9 +857,18 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
   }
   const int chunk = 8;
   const int graph_kind = mixed ? 1 + ctx->spmv32_shape : 0;  // the captured loop's kernels and shapes
-  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x || A->graph_mixed != graph_kind) {
+  if (!A->graph || A->graph_chunk != chunk || A->graph_x != (const void*)d_x || A->graph_mixed != graph_kind ||
+      (mixed && A->graph_b != (const void*)d_b)) {
     if (A->graph) { cudaGraphExecDestroy(A->graph); A->graph = nullptr; }
-    cudaGraph_t g;
+    struct Graphs {
+      cudaGraph_t round = nullptr, pause = nullptr, loop = nullptr;
+      ~Graphs() {
+        if (round) cudaGraphDestroy(round);
+        if (pause) cudaGraphDestroy(pause);
+        if (loop) cudaGraphDestroy(loop);
+      }
+    } G;
+    // one round: `chunk` iterations
     MSG_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; ++k) {
       if (mixed) {
@@ -854,34 +882,70 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
                                                     pa, st);
       }
     }
-    MSG_CUDA(ctx, cudaStreamEndCapture(s, &g));
-    cudaError_t e = cudaGraphInstantiate(&A->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphInstantiate");
-    A->graph_chunk = chunk;
-    A->graph_x = d_x;
-    A->graph_mixed = graph_kind;
-  }
-  int* h = ctx->h_flags;  // pinned, mapped: done and need
-  int* dh = ctx->d_hflags;
-  const int max_rounds = max_it / chunk + 2 * max_it + 4;  // chunks plus true-residual pauses
-  for (int round = 0; round < max_rounds; ++round) {
-    cudaError_t e = cudaGraphLaunch(A->graph, s);
-    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphLaunch");
-    count_launch(ctx, 2 * chunk);
-    MSG_TRY(publish_flags(ctx, &st->done, 2, h, dh, s));  // done, need
-    MSG_CUDA(ctx, cudaStreamSynchronize(s));
-    if (mixed && h[1]) {
-      // FP64 true residual r = b - K x (x += d in FP64 first), then resume or stop
+    MSG_CUDA(ctx, cudaStreamEndCapture(s, &G.round));
+    if (mixed) {
+      // the pause: x += d in FP64, y = K x, the true residual (resume or stop)
+      MSG_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       k_pcgm_fold<<<grid_v, kPcgThreads, 0, s>>>(n, d_x, d32);
       k_bsr_spmv3<<<m->pat.n_slices, 96, 0, s>>>(nr, m->d_slice_ptr.as<int64_t>(), m->d_col.as<int>(),
                                                   A->d_val.as<double>(), d_x, A->d_tmp.as<double>());
       k_pcgm_true<<<grid_v, kPcgThreads, 0, s>>>(n, d_b, A->d_tmp.as<double>(), dinv32, r32, pa, st);
-      count_launch(ctx, 3);
-      MSG_TRY(publish_flags(ctx, &st->done, 1, h, dh, s));
-      MSG_CUDA(ctx, cudaStreamSynchronize(s));
+      MSG_CUDA(ctx, cudaStreamEndCapture(s, &G.pause));
     }
-    if (h[0]) break;
+    MSG_CUDA(ctx, cudaGraphCreate(&G.loop, 0));
+    cudaGraphConditionalHandle h_while = 0, h_if = 0;
+    MSG_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_while, G.loop, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = h_while;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wn = nullptr, last = nullptr;
+    MSG_CUDA(ctx, cudaGraphAddNode(&wn, G.loop, nullptr, 0, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    MSG_CUDA(ctx, cudaGraphAddChildGraphNode(&last, body, nullptr, 0, G.round));
+    auto add_kernel = [&](void* fn, void** args) -> int {
+      cudaKernelNodeParams kp = {};
+      kp.func = fn;
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(1);
+      kp.kernelParams = args;
+      cudaGraphNode_t kn = nullptr;
+      MSG_CUDA(ctx, cudaGraphAddKernelNode(&kn, body, &last, 1, &kp));
+      last = kn;
+      return MSG_OK;
+    };
+    if (mixed) {
+      MSG_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_if, body, 0, 0));
+      void* a_if[] = {&st, &h_if};
+      MSG_TRY(add_kernel((void*)k_pcg_loop_if, a_if));
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = h_if;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t in = nullptr, pn = nullptr;
+      MSG_CUDA(ctx, cudaGraphAddNode(&in, body, &last, 1, &ip));
+      MSG_CUDA(ctx, cudaGraphAddChildGraphNode(&pn, ip.conditional.phGraph_out[0], nullptr, 0, G.pause));
+      last = in;
+    }
+    int chunk_arg = chunk;
+    void* a_while[] = {&st, &h_while, &chunk_arg};
+    MSG_TRY(add_kernel((void*)k_pcg_loop_while, a_while));
+    cudaError_t e = cudaGraphInstantiate(&A->graph, G.loop, 0);
+    if (e != cudaSuccess) {
+      A->graph = nullptr;
+      return cuda_error(ctx, e, "cudaGraphInstantiate");
+    }
+    A->graph_chunk = chunk;
+    A->graph_x = d_x;
+    A->graph_b = d_b;
+    A->graph_mixed = graph_kind;
+  }
+  MSG_CUDA(ctx, cudaMemsetAsync(&st->rounds, 0, 2 * sizeof(int), s));  // rounds, pauses
+  {
+    cudaError_t e = cudaGraphLaunch(A->graph, s);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cudaGraphLaunch");
   }
   if (mixed) {  // a correction left by a solve that ended without a true residual
     k_pcgm_fold<<<grid_v, kPcgThreads, 0, s>>>(n, d_x, d32);
@@ -891,6 +955,7 @@ int pcg_solve_device(Context* ctx, Matrix* A, const double* d_b, double* d_x, in
   PcgState hs;
   MSG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
   MSG_CUDA(ctx, cudaStreamSynchronize(s));
+  count_launch(ctx, hs.rounds * (2 * chunk + (mixed ? 2 : 1)) + 3 * hs.pauses);
   if (iterations) *iterations = hs.iterations;
   if (rel_res) *rel_res = hs.err;
   if (status) *status = hs.done ? hs.status : MSG_ERR_NOT_CONVERGED;
@@ -908,6 +973,7 @@ constexpr size_t kNoAllocVecBytes = sizeof(double) * 3 * (size_t)kNoAllocMaxNode
 constexpr size_t kNoAllocPartials = 2 * 4096;  // >= max(2 * update CTAs, slices of 65536 nodes)
 constexpr size_t kNoAllocStateOff = 6 * kNoAllocVecBytes + sizeof(double) * kNoAllocPartials;
 constexpr size_t kNoAllocBytes = kNoAllocStateOff + 256;
+static_assert(sizeof(PcgState) <= 256, "the scalar state fits its slot of the scratch");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 

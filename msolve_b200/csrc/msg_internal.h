@@ -259,7 +259,10 @@ struct PcgState {
   // pauses (need = 1) when the recursive residual has dropped by delta since
   // err_ref or below tol, and the host replaces it with the FP64 true residual
   double delta, err_ref;
-  int mixed, pad;
+  int mixed;
+  // rounds of the graph's device loop (chunks of iterations) and the FP64
+  // true-residual pauses among them
+  int rounds, pauses, pad;
 };
 
 struct Matrix {
@@ -275,6 +278,7 @@ struct Matrix {
   int graph_chunk = 0;
   int graph_mixed = 0;
   const void* graph_x = nullptr;  // output vector the captured graph writes (not owned)
+  const void* graph_b = nullptr;  // right-hand side its true-residual steps read (not owned)
   ~Matrix();
 };
 
