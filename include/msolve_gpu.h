@@ -342,7 +342,13 @@ typedef struct {
  * (ISAAR.MSolve.Analyzers/MonteCarloAnalyzerWithStochasticMaterial.cs:232-296)
  * for several systems of uneven mesh size at once. Structured cube lattices go
  * through the lattice loop of MSG_MC_SOLVE_BATCH (mixed mode, the same results
- * as that call) unless the "ragged_lattice_loop" option is 0; for the other
+ * as that call) unless the "ragged_lattice_loop" option is 0: with the
+ * "ragged_side_by_side" option on (the default) their loops are stepped side
+ * by side, each on its own stream with its own buffers and loop graph (kept in
+ * the context for the next call), on a second host thread while the calling
+ * thread runs the other systems' batch, each lattice taking the steps it
+ * takes alone (the same bits); with it off, one lattice after another and
+ * then the other systems. For the other
  * systems every iteration of every realization runs in the same three persistent launches
  * (element-by-element FP32 operator over each element's stiffness at E = 1
  * scaled by E per realization, per-realization scalars, fused vector update),
@@ -489,8 +495,11 @@ int MSG_SERVE_STOP(MSG_CTX ctx);
  * starts from the Newmark predictor u + dt v + (1/2 - alpha) dt^2 a; 0: from
  * the last displacement), "ragged_lattice_loop" (MSG_MC_SOLVE_RAGGED: 1, default, structured cube
  * lattices of the batch are solved by the lattice loop of
- * MSG_MC_SOLVE_BATCH, one after another, the other systems together in the
- * element-by-element batch; 0: every system in the element-by-element batch).
+ * MSG_MC_SOLVE_BATCH, the other systems together in the element-by-element
+ * batch; 0: every system in the element-by-element batch),
+ * "ragged_side_by_side" (MSG_MC_SOLVE_RAGGED: 1, default, the lattice loops
+ * side by side on their own streams alongside the element-by-element batch;
+ * 0: one after another, then the element-by-element batch; the same results).
  * Batched realization counts are padded to a multiple of 64.
  * In the multigrid loop t[5] below is the duration of one search-direction +
  * operator launch and t[6] that of one whole iteration. */

@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -40,6 +41,7 @@
 #include <utility>
 
 #include "khat_classes.h"
+
 #include "msg_internal.h"
 
 namespace msg {
@@ -3827,6 +3829,25 @@ int block_bnorm(Context* ctx, BlockSys* B, const double* b, bool b_per_r) {
   return MSG_OK;
 }
 
+// The start of a batched solve (enqueued on the batch's stream): scalars,
+// directions, the operator outputs and the correction zero (x too unless
+// warm), ||b|| per realization, the loop's configuration and graph.
+int block_solve_start(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool warm, double tol, int chunk_cap,
+                      LoopCfg* c, cudaGraphExec_t* gexec) {
+  cudaStream_t st = B->X.st;
+  const size_t nvec = B->nvec;
+  MSG_CUDA(ctx, cudaMemsetAsync(B->scal.ptr, 0, B->scal_bytes, st));
+  if (!warm) MSG_CUDA(ctx, cudaMemsetAsync(B->x.ptr, 0, sizeof(double) * nvec, st));
+  // directions, operator outputs and the correction start from zero
+  const WSlot* z32[] = {&B->p, &B->q, &B->d, &B->pB, &B->qB};
+  for (const WSlot* w : z32)
+    if (w->ptr) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(float) * nvec, st));
+  MSG_TRY(block_bnorm(ctx, B, b, b_per_r));
+  *c = loop_cfg(ctx, B, tol, chunk_cap);
+  MSG_TRY(block_graph(ctx, B, *c, gexec));
+  return MSG_OK;
+}
+
 // Solve A x = b for every realization of the batch to the FP64 true relative
 // residual tol: b is one vector (blat layout) or one per realization; x (slot 0)
 // starts from zero, or from its content when warm. Per-realization results stay
@@ -3836,19 +3857,11 @@ int block_solve(Context* ctx, BlockSys* B, const double* b, bool b_per_r, bool w
   NvtxRange range("msg: batched solve");
   cudaStream_t st = B->X.st;
   Scal& s = B->s;
-  const size_t nvec = B->nvec;
-  MSG_CUDA(ctx, cudaMemsetAsync(B->scal.ptr, 0, B->scal_bytes, st));
-  if (!warm) MSG_CUDA(ctx, cudaMemsetAsync(B->x.ptr, 0, sizeof(double) * nvec, st));
-  // directions, operator outputs and the correction start from zero
-  const WSlot* z32[] = {&B->p, &B->q, &B->d, &B->pB, &B->qB};
-  for (const WSlot* w : z32)
-    if (w->ptr) MSG_CUDA(ctx, cudaMemsetAsync(w->ptr, 0, sizeof(float) * nvec, st));
-  MSG_TRY(block_bnorm(ctx, B, b, b_per_r));
-  const LoopCfg c = loop_cfg(ctx, B, tol, chunk_cap);
+  LoopCfg c;
+  cudaGraphExec_t gexec = nullptr;
+  MSG_TRY(block_solve_start(ctx, B, b, b_per_r, warm, tol, chunk_cap, &c, &gexec));
   cudaEvent_t* ev = B->X.ev;
   float t_resid = 0.f, t_inner = 0.f;
-  cudaGraphExec_t gexec = nullptr;
-  MSG_TRY(block_graph(ctx, B, c, &gexec));
 
   int* h_flags = B->X.h_flags;  // [0] active, [4] update requests, [8] wait timeout (pinned)
   int status = MSG_OK;
@@ -4055,6 +4068,176 @@ int block_mixed_solve(Context* ctx, Mesh* m, double nu, const KLDevice* kl, cons
     return set_error(ctx, status, "mixed batched solve: %s",
                      status == MSG_ERR_BREAKDOWN ? "PCG breakdown" : "not converged");
   return MSG_OK;
+}
+
+LatticeRunner::~LatticeRunner() {
+  if (st) cudaStreamSynchronize(st);
+  if (graph) cudaGraphExecDestroy(graph);
+  for (cudaEvent_t& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (st) cudaStreamDestroy(st);
+  delete[] pool;
+}
+
+// Several cube-lattice batches side by side. Each batch has its own stream,
+// events, flag words (mapped words 512 + 16 k of the context's), loop graph and
+// buffer set (ctx->lat_runners[k]); the set-ups run on the context's stream one
+// after another (the KL table's device copy is the context's). Then one host
+// thread steps every batch's loop in turn: a round enqueues the next step of
+// every running batch (its FP64 true residual or a chunk of iterations, then
+// its flags) before it waits for any, so that one batch's host round trip and
+// small launches overlap the other batches' kernels. Each batch takes exactly
+// the steps block_solve takes for it alone, so its results are the same.
+int block_mixed_solve_many(Context* ctx, std::vector<LatticeJob>& jobs, int max_it, double tol,
+                           const std::function<int()>& alongside) {
+  NvtxRange range("msg: cube-lattice batches side by side");
+  const int n = (int)jobs.size();
+  constexpr int kMaxSideBySide = 32;  // flag words 512 ... 1023 of the context's 1024
+  if (n > kMaxSideBySide)
+    return set_error(ctx, MSG_ERR_INVALID_ARGUMENT, "at most %d cube lattices side by side", kMaxSideBySide);
+  MSG_TRY(context_resources(ctx));
+  while ((int)ctx->lat_runners.size() < n) {
+    std::unique_ptr<LatticeRunner> r(new LatticeRunner());
+    MSG_CUDA(ctx, cudaStreamCreateWithFlags(&r->st, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : r->ev) MSG_CUDA(ctx, cudaEventCreate(&e));
+    r->pool = new DevMem[kWorkSlots];
+    ctx->lat_runners.push_back(r.release());
+  }
+  std::vector<std::unique_ptr<BlockSys>> Bs(n);
+  std::vector<LoopCfg> cfg(n);
+  std::vector<cudaGraphExec_t> gx(n, nullptr);
+  cudaStream_t cs = ctx->stream;
+  for (int i = 0; i < n; ++i) {
+    LatticeJob& J = jobs[i];
+    LatticeRunner* run = ctx->lat_runners[i];
+    if (!J.m->structured) return set_error(ctx, MSG_ERR_NOT_STRUCTURED, "mesh is not a structured cube lattice");
+    BlockExec X;
+    X.st = run->st;
+    X.ev = run->ev;
+    X.h_flags = ctx->h_flags + 512 + 16 * i;
+    X.d_hflags = ctx->d_hflags ? ctx->d_hflags + 512 + 16 * i : nullptr;
+    X.graph = &run->graph;
+    X.graph_key = &run->graph_key;
+    X.ctx_stats = false;
+    Bs[i].reset(new BlockSys());
+    BlockSys* B = Bs[i].get();
+    const int Rp = (J.R + 63) / 64 * 64;
+    MSG_TRY(block_setup(ctx, J.m, J.nu, 1.0, 1.0, 0.0, J.R, Rp, B, run->pool, &X));
+    B->fixed = ctx->fixed_updates != 0;
+    MSG_CUDA(ctx, cudaStreamSynchronize(run->st));
+    KLDevice kd;
+    MSG_TRY(kl_prepare(ctx, J.m, J.kl, &kd));
+    MSG_TRY(block_field(ctx, J.m, B, &kd, J.d_xi));
+    k_lattice_rhs<<<(J.m->n_dofs + 255) / 256, 256, 0, cs>>>(J.m->n_dofs, J.m->d_pad_free_rows.as<int>(), J.d_b,
+                                                             B->blat.as<double>());
+    count_launch(ctx);
+    MSG_CUDA(ctx, cudaStreamSynchronize(cs));  // before the next batch's KL table replaces this one's
+    MSG_TRY(block_solve_start(ctx, B, B->blat.as<double>(), false, false, tol, 0, &cfg[i], &gx[i]));
+    if (J.h_tip && run->tip.bytes < sizeof(double) * Rp) {
+      run->tip.release();
+      MSG_TRY(run->tip.alloc(ctx, sizeof(double) * Rp));
+    }
+  }
+  // the loops, stepped in turn (block_solve's decisions, batch by batch), and
+  // the outputs: on a second host thread while `alongside` runs on this one
+  auto run_loops = [&]() -> int {
+  struct Step {
+    bool need_update = true, first = true, live = true;
+    int total_inner = 0, status = MSG_OK, kind = 0;  // kind: 1 true residual, 2 chunk
+  };
+  std::vector<Step> sp(n);
+  for (int round = 0; round < 1000000; ++round) {
+    bool any = false;
+    for (int i = 0; i < n; ++i) {
+      Step& u = sp[i];
+      if (!u.live) continue;
+      BlockSys* B = Bs[i].get();
+      if (u.need_update) {
+        u.kind = 1;
+        MSG_TRY(block_update(ctx, B, cfg[i], B->blat.as<double>(), false, tol, u.first, 0x7fffffff,
+                             B->gmg && u.first));
+      } else {
+        u.kind = 2;
+        const cudaError_t e = cudaGraphLaunch(gx[i], B->X.st);
+        if (e != cudaSuccess) return cuda_error(ctx, e, "inner chunk");
+        count_launch(ctx, (B->gmg ? gmg_launches(B) : 2) * cfg[i].chunk);
+        u.total_inner += cfg[i].chunk;
+      }
+      MSG_TRY(publish_flags(ctx, B->s.n_active, 9, B->X.h_flags, B->X.d_hflags, B->X.st));
+      any = true;
+    }
+    if (!any) break;
+    for (int i = 0; i < n; ++i) {
+      Step& u = sp[i];
+      if (!u.live) continue;
+      BlockSys* B = Bs[i].get();
+      MSG_CUDA(ctx, cudaStreamSynchronize(B->X.st));
+      const int* h = B->X.h_flags;
+      if (u.kind == 1) {
+        u.first = false;
+        if (h[0] == 0) {  // every realization converged (or broke down)
+          u.live = false;
+          continue;
+        }
+        u.need_update = false;
+      } else {
+        if (h[8]) {
+          u.status = set_error(ctx, MSG_ERR_TIMEOUT, "a bounded wait of the staged operator expired");
+          u.live = false;
+          continue;
+        }
+        u.need_update = B->fixed || (h[4] > 0) || (h[0] == 0);
+      }
+      if (!u.need_update && u.total_inner >= max_it) {
+        u.status = MSG_ERR_NOT_CONVERGED;
+        u.live = false;
+      }
+    }
+  }
+  // outputs, batch by batch
+  for (int i = 0; i < n; ++i) {
+    LatticeJob& J = jobs[i];
+    BlockSys* B = Bs[i].get();
+    cudaStream_t st = B->X.st;
+    Mesh* m = J.m;
+    int status = sp[i].status;
+    if (status == MSG_ERR_TIMEOUT) {
+      J.status = status;
+      continue;
+    }
+    if (J.d_X) {
+      dim3 g((m->n_dofs + 31) / 32, B->Rp / 32);
+      k_gather_solution<<<g, dim3(32, 8), 0, st>>>(m->n_dofs, J.R, B->Rp, m->d_pad_free_rows.as<int>(),
+                                                   B->x.as<double>(), J.d_X);
+      count_launch(ctx);
+    }
+    if (J.h_tip && J.tip_dof >= 0 && J.tip_dof < m->n_dofs) {
+      int row = 0;
+      MSG_CUDA(ctx, cudaMemcpyAsync(&row, m->d_pad_free_rows.as<int>() + J.tip_dof, sizeof(int),
+                                    cudaMemcpyDeviceToHost, st));
+      MSG_CUDA(ctx, cudaStreamSynchronize(st));
+      DevMem& tip = ctx->lat_runners[i]->tip;  // sized in the set-up
+      k_gather_tip<<<(J.R + 127) / 128, 128, 0, st>>>(J.R, B->Rp, row, B->x.as<double>(), tip.as<double>());
+      count_launch(ctx);
+      MSG_CUDA(ctx, cudaMemcpyAsync(J.h_tip, tip.ptr, sizeof(double) * J.R, cudaMemcpyDeviceToHost, st));
+    }
+    status = block_results(ctx, B, status, J.h_its, J.h_res);  // synchronises the batch's stream
+    if (status != MSG_OK)
+      set_error(ctx, status, "mixed batched solve: %s", status == MSG_ERR_BREAKDOWN ? "PCG breakdown" : "not converged");
+    J.status = status;
+  }
+  for (int i = 0; i < n; ++i) MSG_CUDA(ctx, cudaStreamSynchronize(ctx->lat_runners[i]->st));
+  return MSG_OK;
+  };
+  if (!alongside) return run_loops();
+  int loop_status = MSG_OK;
+  std::thread worker([&] {
+    const cudaError_t e = cudaSetDevice(ctx->device);
+    loop_status = e == cudaSuccess ? run_loops() : cuda_error(ctx, e, "cudaSetDevice");
+  });
+  const int a_status = alongside();
+  worker.join();
+  return loop_status != MSG_OK ? loop_status : a_status;
 }
 
 int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,

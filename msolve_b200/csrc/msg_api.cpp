@@ -19,6 +19,7 @@ int set_error(Context* ctx, int code, const char* fmt, ...) {
     va_start(ap, fmt);
     vsnprintf(buf, sizeof(buf), fmt, ap);
     va_end(ap);
+    std::lock_guard<std::mutex> g(ctx->err_mu);
     ctx->last_error = buf;
   }
   return code;
@@ -76,6 +77,8 @@ Context::~Context() {
   }
   for (DevMem* set : vc_pool) delete[] set;
   vc_pool.clear();
+  for (LatticeRunner* r : lat_runners) delete r;
+  lat_runners.clear();
   if (batch_graph) cudaGraphExecDestroy(batch_graph);
   for (auto& e : ev)
     if (e) cudaEventDestroy(e);
@@ -740,6 +743,10 @@ int MSG_SET_OPTION(MSG_CTX ctx, const char* key, double value) {
     ctx->ragged_lattice_loop = (int)value;
     return MSG_OK;
   }
+  if (!std::strcmp(key, "ragged_side_by_side") && (value == 0 || value == 1)) {
+    ctx->ragged_side_by_side = (int)value;
+    return MSG_OK;
+  }
   if (!std::strcmp(key, "newmark_predictor") && (value == 0 || value == 1)) {
     ctx->nm_predictor = (int)value;
     return MSG_OK;
@@ -786,6 +793,7 @@ int MSG_GET_OPTION(MSG_CTX ctx, const char* key, double* value) {
               {"element_batch", (double)ctx->element_batch},
               {"element_groups", (double)ctx->element_groups},
               {"ragged_lattice_loop", (double)ctx->ragged_lattice_loop},
+              {"ragged_side_by_side", (double)ctx->ragged_side_by_side},
               {"newmark_predictor", (double)ctx->nm_predictor},
               {"multigrid_fused_coarse", (double)ctx->mg_fused_coarse},
               {"serve_persistent", (double)ctx->serve_persistent},
@@ -1366,13 +1374,46 @@ int MSG_MC_SOLVE_RAGGED(MSG_CTX ctx, int n_systems, const MSG_RAGGED_SYSTEM* sys
     if (worst == MSG_OK) worst = st;
     return true;
   };
-  for (int i : lattice) {
-    const MSG_RAGGED_SYSTEM& y = systems[i];
-    const int st = mc_batch(ctx, y.mesh, y.nu, y.kl, y.R, reinterpret_cast<double*>(base + off[3 * i]),
-                            reinterpret_cast<double*>(base + off[3 * i + 1]), MSG_MODE_MIXED_BATCHED, max_it, tol,
-                            y.tip ? y.tip_dof : -1, y.X ? reinterpret_cast<double*>(base + off[3 * i + 2]) : nullptr,
-                            y.tip, y.iterations, y.rel_res);
-    if (!outcome(st)) return st;
+  if (ctx->ragged_side_by_side && !lattice.empty() && (lattice.size() > 1 || !in.empty())) {
+    // the cube lattices' loops stepped side by side, each on its own stream, on
+    // a second host thread while this one runs the element-by-element batch
+    std::vector<LatticeJob> jobs;
+    for (int i : lattice) {
+      const MSG_RAGGED_SYSTEM& y = systems[i];
+      LatticeJob J;
+      J.m = y.mesh;
+      J.nu = y.nu;
+      J.kl = y.kl;
+      J.R = y.R;
+      J.d_xi = reinterpret_cast<double*>(base + off[3 * i]);
+      J.d_b = reinterpret_cast<double*>(base + off[3 * i + 1]);
+      J.d_X = y.X ? reinterpret_cast<double*>(base + off[3 * i + 2]) : nullptr;
+      J.h_tip = y.tip;
+      J.tip_dof = y.tip ? y.tip_dof : -1;
+      J.h_its = y.iterations;
+      J.h_res = y.rel_res;
+      jobs.push_back(J);
+    }
+    int ebe_status = MSG_OK;
+    std::function<int()> ebe;
+    if (!in.empty()) ebe = [&] { return ebe_status = ebe_solve(ctx, in, max_it, tol); };
+    const int st = block_mixed_solve_many(ctx, jobs, max_it, tol, ebe);
+    // a status of the element-by-element batch is its outcome, any other a failure
+    if (st != MSG_OK && st != ebe_status) return st;
+    for (const LatticeJob& J : jobs)
+      if (!outcome(J.status)) return J.status;
+    if (!in.empty() && !outcome(ebe_status)) return ebe_status;
+    in.clear();  // solved
+  } else {
+    for (int i : lattice) {
+      const MSG_RAGGED_SYSTEM& y = systems[i];
+      const int st = mc_batch(ctx, y.mesh, y.nu, y.kl, y.R, reinterpret_cast<double*>(base + off[3 * i]),
+                              reinterpret_cast<double*>(base + off[3 * i + 1]), MSG_MODE_MIXED_BATCHED, max_it, tol,
+                              y.tip ? y.tip_dof : -1,
+                              y.X ? reinterpret_cast<double*>(base + off[3 * i + 2]) : nullptr, y.tip, y.iterations,
+                              y.rel_res);
+      if (!outcome(st)) return st;
+    }
   }
   if (!in.empty()) {
     const int st = ebe_solve(ctx, in, max_it, tol);

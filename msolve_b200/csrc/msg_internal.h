@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <memory>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -52,6 +53,8 @@ struct DevMem {
 // mesh, so the caller may destroy them in any order (a garbage-collected host
 // such as .NET finalises in arbitrary order); the object is freed with its
 // last reference.
+struct LatticeRunner;
+
 struct Context {
   std::atomic<int> refs{1};
   int device = 0;
@@ -60,6 +63,7 @@ struct Context {
   std::atomic<uint64_t> used{0};
   std::recursive_mutex mu;
   std::string last_error;
+  std::mutex err_mu;  // last_error: a ragged batch's lattice loops run on a second host thread
   std::atomic<int64_t> launches{0};
   double t_phase[5] = {0, 0, 0, 0, 0};
   // live per-launch samples of the inner operator / update kernels (event
@@ -86,6 +90,7 @@ struct Context {
   int element_batch = 1;        // mixed mode on non-lattice meshes: 1 batched element-by-element loop, 0 per realization
   int element_groups = 0;       // realization groups of 32 per CTA of the element-by-element FP32 operator (0 auto)
   int ragged_lattice_loop = 1;  // ragged batches: cube lattices through the lattice loop (1) or the shared loop (0)
+  int ragged_side_by_side = 1;  // ragged batches: the cube lattices' loops side by side (1) or one after another (0)
   int nm_predictor = 1;         // Newmark steps start from the Newmark predictor (1) or the last displacement (0)
   int serve_persistent = 1;     // serving lanes: 1 persistent grids, 0 one CTA per work item
   int serve_priority = 0;       // serving lanes: 1 stream priority grows as the model shrinks, 0 all equal
@@ -97,6 +102,10 @@ struct Context {
   // element-by-element batch with several of them: set k for the k-th such
   // system, kept (and grown) across calls like the workspace slots
   std::vector<DevMem*> vc_pool;
+  // the ragged batch's cube lattices, solved side by side: runner k (a stream,
+  // 12 events, the loop graph and a lattice buffer set) serves the k-th of them,
+  // kept across calls
+  std::vector<LatticeRunner*> lat_runners;
   // per-context host/driver resources reused by every batch (created lazily)
   int* h_flags = nullptr;           // 4 KB of pinned host memory, mapped into the device
   int* d_hflags = nullptr;          // the device's address of h_flags
@@ -426,6 +435,37 @@ struct NewmarkParams {
 int block_newmark(Context* ctx, Mesh* m, double nu, const KLDevice* kl, const double* d_xi, int R, int Rp,
                   const NewmarkParams& nm, const double* d_f_dof, int max_it, double tol, int tip_dof,
                   double* tip_hist, double* d_U, int* its_total);
+
+// Cube-lattice batches solved side by side (kernels_block.cu): the ragged
+// batch's lattices, each with the outputs of MSG_MC_SOLVE_BATCH_DEVICE (X and
+// the tip on the device and the host, iterations and residuals on the host);
+// status is each batch's outcome.
+struct LatticeJob {
+  Mesh* m = nullptr;
+  double nu = 0.0;
+  const MSG_KL* kl = nullptr;
+  const double* d_xi = nullptr;
+  const double* d_b = nullptr;
+  int R = 0, tip_dof = -1;
+  double* d_X = nullptr;
+  double* h_tip = nullptr;
+  int* h_its = nullptr;
+  double* h_res = nullptr;
+  int status = 0;
+};
+struct LatticeRunner {
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[12] = {};
+  cudaGraphExec_t graph = nullptr;
+  size_t graph_key = 0;
+  DevMem* pool = nullptr;  // kWorkSlots buffers
+  DevMem tip;              // the tip displacement of every realization
+  ~LatticeRunner();
+};
+// alongside (optional) runs on the calling thread while a second host thread
+// steps the lattices' loops; its status is returned when theirs is MSG_OK.
+int block_mixed_solve_many(Context* ctx, std::vector<LatticeJob>& jobs, int max_it, double tol,
+                           const std::function<int()>& alongside);
 
 // Serving lanes (kernels_block.cu): continuous batching of one model's requests.
 struct Lane;

@@ -172,3 +172,71 @@ def test_ragged_batch_rejects_invalid_systems(ctx):
         batch.Solve()  # mesh of another context
     with pytest.raises(M.ArgumentError):
         M.RaggedMonteCarloBatch(ctx).Solve()  # no systems
+
+
+MIX = ((4, 3, 5, False, 4), (6, 40, 8, False, 5), (5, 2, 6, True, 6), (8, 70, 10, False, 7))
+MIX_SIDES = [row[0] for row in MIX]
+
+
+def lattice_mix():
+    """Three cube lattices (4^3 with 3 realizations, 6^3 with 40, 8^3 with 70:
+    two 64-wide groups, the second mostly padding) and a distorted 5^3 block."""
+    out = []
+    for n, R, K, distort, seed in MIX:
+        model = distorted_model(n, seed) if distort else M.clamped_block_model(n)
+        kl = M.LognormalStochasticCoefficientsProvider([n, n, n], 0.2 * n, K, 4)
+        xi = np.random.default_rng(20 + seed).standard_normal((R, K))
+        out.append((model, kl, xi))
+    return out
+
+
+@pytest.fixture
+def side_by_side(ctx):
+    yield
+    ctx.set_option("ragged_side_by_side", 1)
+
+
+def test_lattices_side_by_side_equal_one_after_another(ctx, side_by_side):
+    """The ragged_side_by_side option (default 1) steps the loops of a batch's
+    cube lattices side by side, each on its own stream: every lattice takes the
+    steps it takes alone, so the results are the same bits as with the lattices
+    solved one after another, call after call, and as the analyzer's own call."""
+    syss = lattice_mix()
+    ctx.set_option("ragged_side_by_side", 0)
+    ref = solve(ctx, syss)
+    ctx.set_option("ragged_side_by_side", 1)
+    for _ in range(2):  # the second call reuses the streams, buffers and loop graphs
+        got = solve(ctx, syss)
+        for a, b in zip(got, ref):
+            for key in ("Solutions", "TipValues", "Iterations", "Residuals"):
+                assert np.array_equal(a[key], b[key]), key
+    model, kl, xi = syss[3]
+    mc = M.MonteCarloAnalyzerWithStochasticMaterial(ctx, model, kl, expansion_order=kl.n_terms,
+                                                    simulations=xi.shape[0], mode="mixed", tolerance=1e-10)
+    mc.RandomNumbers = xi
+    mc.Solve()
+    assert np.array_equal(got[3]["Solutions"], mc.Solutions)
+    assert np.array_equal(got[3]["Iterations"], mc.Iterations)
+    for k, ((model, kl, xi), n) in enumerate(zip(syss, MIX_SIDES)):
+        assert got[k]["Residuals"].max() < 1e-10
+        xo, _ = oracle_solution(model, kl, xi[-1], n)
+        assert np.abs(got[k]["Solutions"][-1] - xo).max() <= 1e-8 * np.abs(xo).max()
+
+
+def test_lattices_side_by_side_not_converged(ctx, side_by_side):
+    """An iteration limit that stops every lattice: the same outcome (not
+    converged), iteration counts and partial solutions either way."""
+    syss = lattice_mix()
+    outs = []
+    for opt in (0, 1):
+        ctx.set_option("ragged_side_by_side", opt)
+        batch = M.RaggedMonteCarloBatch(ctx, max_iterations=2, tolerance=1e-12)
+        for model, kl, xi in syss:
+            batch.add(model, kl, xi)
+        with pytest.raises(M.InvalidOperationError) as e:
+            batch.Solve()
+        outs.append((e.value.code, batch.Results))
+    assert outs[0][0] == outs[1][0]
+    for a, b in zip(outs[0][1], outs[1][1]):
+        for key in ("Solutions", "Iterations", "Residuals"):
+            assert np.array_equal(a[key], b[key]), key
