@@ -4235,6 +4235,12 @@ int block_mixed_solve_many(Context* ctx, std::vector<LatticeJob>& jobs, int max_
     const cudaError_t e = cudaSetDevice(ctx->device);
     loop_status = e == cudaSuccess ? run_loops() : cuda_error(ctx, e, "cudaSetDevice");
   });
+  struct Join {  // joined on every way out, an exception from `alongside` included
+    std::thread& t;
+    ~Join() {
+      if (t.joinable()) t.join();
+    }
+  } join{worker};
   const int a_status = alongside();
   worker.join();
   return loop_status != MSG_OK ? loop_status : a_status;
