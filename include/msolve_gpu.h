@@ -143,7 +143,9 @@ int MSG_MAT_DESTROY(MSG_MAT mat);
  * (ISAAR.MSolve.Solvers/PCG/SolverPCG.cs:105-149, simple search vector
  * SolverPCGSimpleSearchVectorCalculator.cs:18-41): x0 = 0, r0 = b, stop when
  * ||r_k|| / ||b|| < tol on the recursively updated r, skip if ||b|| <= 1e-25.
- * The whole loop runs on the device (no host round trip per iteration).
+ * The whole loop runs on the device: one CUDA graph launch a solve, whose
+ * conditional WHILE node repeats 8-iteration rounds until the solve ends (no
+ * host round trip between iterations or rounds).
  * iterations = the reference's count (loop index at the break); rel_res = last
  * ||r||/||b||. Returns MSG_ERR_NOT_CONVERGED if max_it was reached. */
 int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
@@ -158,8 +160,9 @@ int MSG_PCG_SOLVE(MSG_MAT mat, const double* b, double* x, int max_it, double to
  * replaced by the FP64 true residual b - K x computed with the FP64 values,
  * the search direction is kept, and the solve stops only when
  * ||b - K x|| / ||b|| < tol in FP64 (rel_res). iterations counts as
- * MSG_PCG_SOLVE. The FP32 copy of the values is built on first use. No
- * counterpart in the reference. */
+ * MSG_PCG_SOLVE. The FP32 copy of the values is built on first use. Like
+ * MSG_PCG_SOLVE, one CUDA graph launch a solve; the true-residual step is a
+ * conditional node of that graph. No counterpart in the reference. */
 int MSG_PCG_SOLVE_MIXED(MSG_MAT mat, const double* b, double* x, int max_it, double tol, int* iterations,
                         double* rel_res);
 
